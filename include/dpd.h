@@ -1,0 +1,225 @@
+/*
+ * dpd.h -- C ABI of libdpd.so, the B200 (sm_100a) implementation of the 2D
+ * DPD step with lipid chemistry of the Oercel engine.
+ *
+ * The reference runs its step inside the engine process (cel/engine/oercel.c,
+ * main loop :2300-2361) and is driven from Python only through a subprocess
+ * CLI (cel/pc/pclib.py:973-986).  This ABI exposes the same step and its
+ * phases in-process, for ctypes/cffi callers, with plain pointers and sizes:
+ *
+ *   reference phase (file:line)                       entry point here
+ *   ------------------------------------------------  ---------------------------
+ *   Params/PDEFS + finalize_params  oercel.c:178-299,578-619  dpd_params_default, dpd_create
+ *   sys_alloc                       oercel.c:714-759   dpd_create
+ *   init_soup + set_velocities      oercel.c:1757-1814 dpd_set_state (host-made soup)
+ *   initial sort/forces/half kick   oercel.c:2203-2211 dpd_prime
+ *   integrate block of main         oercel.c:2303-2334 dpd_integrate
+ *   sort_cells                      oercel.c:832-933   dpd_build_cells
+ *   pair_forces                     oercel.c:1198-1216 dpd_forces (pair part)
+ *   bonded_forces                   oercel.c:1322-1343 dpd_forces (bond part)
+ *   chemistry                       oercel.c:1565-1701 dpd_chemistry
+ *   one loop iteration              oercel.c:2300-2361 dpd_step
+ *   kinetic_T / count_types         oercel.c:2053-2071 dpd_observables
+ *   write_snapshot/ckpt state read  oercel.c:1830-1936 dpd_get_state, dpd_get_cells
+ *   add_event / flush_events        oercel.c:788-798,2036-2047 dpd_get_events
+ *   die() error path                oercel.c:74-90     negative return + dpd_last_error
+ *
+ * Conventions
+ *   - Every call returns DPD_OK (0) or a negative DPD_E_* code; the message of
+ *     the last failure on the calling thread is dpd_last_error().  Nothing
+ *     calls exit().
+ *   - Array arguments may be host or device pointers (CUDA unified
+ *     addressing decides); the caller owns them.  The library owns its device
+ *     state and scratch.  Arrays are in "slot" order (cell-sorted order, as
+ *     the reference's Sys arrays) unless a function says otherwise.
+ *   - One handle = one CUDA stream; a handle is not thread safe.
+ *   - Bead types: 0 W, 1 H, 2 T, 3 P (the reference's N), 4..7 free.  Lipid
+ *     bonds are prev/next links (slot indices, -1 = none); the reference's
+ *     nxt[] is next[] and mpos is implied by the chain.
+ *   - Cells: ncx = ncy = floor(L), column-major c = cx * ncy + cy: the
+ *     reference with nsub = 1 (oercel.c:739-745,779-786).
+ */
+#ifndef DPD_H
+#define DPD_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DPD_API __attribute__((visibility("default")))
+#else
+#define DPD_API
+#endif
+
+#define DPD_OK 0
+#define DPD_E_ARG (-1)            /* bad argument or parameter (reference: die() on params) */
+#define DPD_E_CUDA (-2)           /* CUDA runtime error */
+#define DPD_E_SORT_OVERFLOW (-3)  /* cell sort could not place every bead (reference GPU: ERR_SORT) */
+#define DPD_E_CHAIN (-4)          /* broken lipid chain (reference GPU: ERR_CHAIN) */
+#define DPD_E_EVENT_OVERFLOW (-5) /* event buffer full (reference GPU: ERR_EVOVF) */
+#define DPD_E_TIMEOUT (-6)        /* a bounded device wait gave up */
+#define DPD_E_STATE (-7)          /* a bead left the box or a value is not finite */
+#define DPD_E_NOMEM (-8)          /* device allocation failed */
+
+#define DPD_MAXT 8
+
+/* Physics and chemistry of one replica.  Defaults (dpd_params_default) are the
+ * reference's PDEFS defaults where the reference has the key
+ * (cel/engine/oercel.c:237-299) and the 1M-bead chemistry rules otherwise. */
+typedef struct {
+    double L;                  /* box side; ncx = ncy = floor(L) >= 3 */
+    double dt;                 /* time step (reference key dt) */
+    double lambda;             /* Groot-Warren lambda (lambda) */
+    double gamma;              /* friction (gamma) */
+    double kT;                 /* temperature; sigma = sqrt(2 gamma kT) (kT) */
+    double a[DPD_MAXT * DPD_MAXT]; /* repulsion a_ij, symmetric (a_X_Y) */
+    double k_bond;             /* harmonic bond constant (k_bond) */
+    double r0;                 /* bond rest length (r0) */
+    uint64_t seed;             /* noise and chemistry key (seed) */
+    int32_t noise;             /* 0 = Philox4x32-10 (default), 1 = the reference's mix13 hash */
+    int32_t chem;              /* 1 = run the chemistry pass */
+    int32_t n_chem;            /* chemistry every n_chem steps (n_chem) */
+    int32_t n_t_min;           /* T beads a P needs within r_grow */
+    int32_t max_chain;         /* longest chain growth may produce */
+    int32_t pad;
+    double p_break;            /* H-T bond break probability per check */
+    double p_grow;             /* P -> T chain growth probability per check */
+    double p_bond;             /* free T + free H bonding probability per check */
+    double r_grow;             /* growth reaction radius (r_c) */
+    double r_bond;             /* free T - free H bonding radius */
+} dpd_params;
+
+/* One chemistry event, the reference's events.csv row (oercel.c:788-798)
+ * with the partner bead added.  kind: 0 grow, 1 brk, 2 bond. */
+typedef struct {
+    int64_t step;
+    int32_t kind;
+    uint32_t gid;
+    uint32_t partner;
+    float x, y;
+    int32_t replica;
+} dpd_event;
+
+typedef struct dpd_handle dpd_handle;
+
+/* message of the last failed call on this thread ("" if none) */
+DPD_API const char *dpd_last_error(void);
+/* library version string */
+DPD_API const char *dpd_version(void);
+
+/* Fill *p with the defaults. */
+DPD_API int dpd_params_default(dpd_params *p);
+
+/* Create a simulation of n_replicas independent boxes packed into one set of
+ * device arrays.  params[r] and n_beads[r] describe replica r.  The step
+ * counter starts at 0.  Replaces sys_alloc + finalize_params. */
+DPD_API int dpd_create(const dpd_params *params, int32_t n_replicas, const int32_t *n_beads, dpd_handle **out);
+DPD_API int dpd_destroy(dpd_handle *h);
+
+/* sizes: total beads, beads of replica r, cells of replica r */
+DPD_API int dpd_sizes(const dpd_handle *h, int32_t replica, int64_t *n_total, int32_t *n_beads, int32_t *n_cells);
+
+/* Load replica r's state.  x, y in [0, L); vx, vy: velocity (see dpd_prime);
+ * type in 0..7; gid: permanent bead ids 0..n-1 (NULL = 0..n-1); prev/next:
+ * link slot indices within the replica, -1 = none (NULL = no links).  The
+ * slot order is the caller's; dpd_prime or dpd_build_cells sorts it. */
+DPD_API int dpd_set_state(dpd_handle *h, int32_t replica, const float *x, const float *y, const float *vx, const float *vy,
+                  const uint8_t *type, const uint32_t *gid, const int32_t *prev, const int32_t *next);
+
+/* Read replica r's state in slot order.  Any pointer may be NULL. vhx/vhy is
+ * the stored half-step velocity, vtx/vty the predicted velocity, fx/fy the
+ * force of the current configuration (the reference's vx/vy, vtx/vty, fx/fy). */
+DPD_API int dpd_get_state(dpd_handle *h, int32_t replica, float *x, float *y, float *vhx, float *vhy, float *vtx, float *vty,
+                  float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev, int32_t *next);
+
+/* Overwrite the stored half-step velocity and force of replica r (slot
+ * order), e.g. to continue from a checkpoint.  NULL leaves a field as is. */
+DPD_API int dpd_set_dynamics(dpd_handle *h, int32_t replica, const float *vhx, const float *vhy, const float *fx,
+                     const float *fy);
+
+/* Fresh start as the reference's main() (oercel.c:2203-2211): take the loaded
+ * velocity as the full velocity v, sort by cell, compute the forces of the
+ * current step, store vh = v - dt/2 f, and prepare the next sort. */
+DPD_API int dpd_prime(dpd_handle *h);
+
+/* Continue from a loaded (x, vh, f) state without recomputing forces: sort by
+ * cell and prepare the next sort. */
+DPD_API int dpd_resume(dpd_handle *h);
+
+/* current step number (the step of the stored forces) */
+DPD_API int dpd_get_step(const dpd_handle *h, int64_t *step);
+DPD_API int dpd_set_step(dpd_handle *h, int64_t step);
+
+/* Advance nsteps full steps: integrate, cell sort, chemistry (when due),
+ * pair + bond forces (oercel.c:2300-2361), launched as CUDA graphs. */
+DPD_API int dpd_step(dpd_handle *h, int64_t nsteps);
+
+/* dpd_step without the final status check: enqueues the steps on the
+ * handle's stream and returns; dpd_sync waits for them and reports any
+ * device-side error flag (as dpd_step does). */
+DPD_API int dpd_step_async(dpd_handle *h, int64_t nsteps);
+DPD_API int dpd_sync(dpd_handle *h);
+/* steps per captured CUDA graph (default: about 4M bead-steps per replay) */
+DPD_API int dpd_set_graph_steps(dpd_handle *h, int32_t steps);
+/* One real step launched kernel by kernel with CUDA events around each launch
+ * on the handle's stream: ms[k] = device time of kernel k in launch order
+ * (scan1, scan2, place, cellfix, permute, [5 chemistry kernels], forces);
+ * *n_out = number of kernels. */
+DPD_API int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_out);
+
+/* The reference's random soup (init_soup + set_velocities,
+ * cel/engine/oercel.c:1757-1814) with the same xoshiro256** draws, on the
+ * host: linear lipids of nH heads + nT tails at spacing r0 from uniform head
+ * positions, then nKa = round(f_Ka N) beads of type 4, nKb of type 5,
+ * round(c_N N) of type 3 (P), the rest W; Gaussian velocities with the mean
+ * removed, rescaled to exactly kT.  HOST arrays of N entries in gid order.
+ * *n_lipid_beads receives the number of beads placed in lipids. */
+DPD_API int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, double r0, int32_t nH, int32_t nT,
+                          double f_lip, double f_Ka, double f_Kb, double c_N, double *x, double *y, double *vx,
+                          double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads);
+
+/* ---- phases, for testing and custom loops ---- */
+
+/* Stable counting sort of every replica by the cell of the CURRENT positions
+ * (oercel.c:832-933); carries all per-bead arrays along, remaps links. */
+DPD_API int dpd_build_cells(dpd_handle *h);
+/* cell starts of replica r (n_cells + 1 entries, slot offsets within the replica) */
+DPD_API int dpd_get_cells(dpd_handle *h, int32_t replica, int32_t *cstart);
+/* pair + bond forces of the current configuration at the given step, stored
+ * as the current forces (requires a sorted state) */
+DPD_API int dpd_forces(dpd_handle *h, int64_t step);
+/* pair part only / bond part only, written to fx, fy (slot order, replica r) */
+DPD_API int dpd_pair_forces(dpd_handle *h, int32_t replica, int64_t step, float *fx, float *fy);
+DPD_API int dpd_bond_forces(dpd_handle *h, int32_t replica, float *fx, float *fy, float *maxbond);
+/* the Groot-Warren update in place, without sorting (oercel.c:2303-2334) */
+DPD_API int dpd_integrate(dpd_handle *h);
+/* one chemistry pass at the given step on the current sorted state */
+DPD_API int dpd_chemistry(dpd_handle *h, int64_t step);
+
+/* events recorded since the last call, in device order; *n_out = count
+ * returned (<= cap); the buffer is then cleared. */
+DPD_API int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out);
+
+/* Observables of replica r (reference stats row, oercel.c:2364-2372):
+ * out[0] T_kin = sum v^2 / (2N - 2) with v = vh + dt/2 f; out[1..2] total
+ * momentum; out[3] conservative virial (1/L^2) sum_{i<j} a_ij (1-r) r;
+ * out[4] largest bond length; out[5] number of chains (heads with a bond);
+ * out[8 + t] number of beads of type t (t < 8).  out has 16 entries. */
+DPD_API int dpd_observables(dpd_handle *h, int32_t replica, double *out);
+
+/* Histogram (nbin bins on [0, rmax), rmax <= 3) of distances between beads of
+ * types ta and tb of replica r, each unordered pair once. */
+DPD_API int dpd_pair_hist(dpd_handle *h, int32_t replica, int32_t ta, int32_t tb, double rmax, int32_t nbin, double *hist);
+
+/* the CUDA stream (cudaStream_t) this handle enqueues its work on */
+DPD_API int dpd_get_stream(const dpd_handle *h, void **stream);
+/* kernels one step of dpd_step launches: *n_plain in total, of which *n_chem
+ * belong to the chemistry pass (they return at once on non-chemistry steps) */
+DPD_API int dpd_kernels_per_step(const dpd_handle *h, int32_t *n_plain, int32_t *n_chem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

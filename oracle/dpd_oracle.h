@@ -1,0 +1,61 @@
+/*
+ * dpd_oracle.h -- CPU restatement of the 2D DPD step (TEST INFRASTRUCTURE ONLY).
+ *
+ * This library is the checker for the CUDA path: only the tests, the smoke
+ * check and the CPU-baseline leg of bench.py may load it.  The product
+ * (libdpd.so) never links or calls it.
+ *
+ * Every function restates one piece of the reference engine
+ * cel/engine/oercel.c (file:line cited at each definition in dpd_oracle.c),
+ * with two deliberate extensions that the reference does not have:
+ *   - Philox4x32-10 pair noise (Salmon et al., SC'11) next to the
+ *     reference's mix13 hash noise (selected by ora_params.noise);
+ *   - the three-rule lipid chemistry of the 1M-bead workload (chain growth
+ *     from P, H-T bond breaking, free T + free H bonding), whose parity is
+ *     UNPINNED by the reference (it has no such reactions).
+ *
+ * Conventions shared with the CUDA library:
+ *   cells: ncx = ncy = floor(L), column-major c = cx * ncy + cy (the
+ *          reference with nsub = 1, oercel.c:739-745, 779-786);
+ *   links: prev/next slot of the bonded neighbour towards the chain head /
+ *          tail, -1 if none (the reference's nxt[] is next[]).
+ */
+#ifndef DPD_ORACLE_H
+#define DPD_ORACLE_H
+#include <stdint.h>
+
+#define ORA_MAXT 8
+
+typedef struct {
+    double L;
+    int32_t ncx, ncy;
+    double icsx, icsy;      /* ncx / L, ncy / L */
+    double dt, lambda, gamma, kT;
+    double a[ORA_MAXT * ORA_MAXT];
+    double k_bond, r0;
+    uint64_t seed;
+    int32_t noise;          /* 0 = Philox4x32-10, 1 = reference mix13 hash */
+    int32_t pad;
+} ora_params;
+
+typedef struct {
+    float dt, dt2, cvt, L; /* FP32 integrator constants exactly as the kernel gets them */
+} ora_f32c;
+
+typedef struct {
+    uint32_t thr_break, thr_grow, thr_bond; /* decision u32 < thr */
+    float r2_grow, r2_bond;                  /* squared reaction radii (FP32) */
+    int32_t n_t_min;                         /* T beads within r_grow needed by a P */
+    int32_t max_chain;                       /* chains never grow beyond this many beads */
+} ora_chem;
+
+typedef struct {
+    int64_t step;
+    int32_t kind;      /* 0 = grow, 1 = brk, 2 = bond */
+    uint32_t gid;      /* reacting bead */
+    uint32_t partner;  /* gid of the bead it bonded to / unbonded from */
+    float x, y;        /* position of the reacting bead */
+    int32_t pad;
+} ora_event;
+
+#endif

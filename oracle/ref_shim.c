@@ -1,0 +1,188 @@
+/*
+ * ref_shim.c -- ctypes entry points into the reference engine itself
+ * (TEST INFRASTRUCTURE ONLY: used to pin the oracle restatement and to
+ * generate tests/golden/ fixtures; never part of the product).
+ *
+ * The reference source cel/engine/oercel.c is compiled unmodified from where
+ * it lies, with the include trick of cel/engine/tests/forcetest.c:3-5.
+ * oracle/Makefile passes its directory with -I.  Every function below only
+ * calls the reference's own routines, except ref_integrate, which restates
+ * the integrator block that the reference keeps inline in main()
+ * (oercel.c:2303-2334).
+ */
+#define main oercel_main
+#include "oercel.c"
+#undef main
+
+typedef struct {
+    Params P;
+    Sys S;
+} ref_t;
+
+/* Parameters: the reference defaults (oercel.c:2139-2140), then the
+ * "key=value" lines of kv, generic a_K_X keys first (oercel.c:2155-2158),
+ * then finalize_params. */
+static void ref_params(Params *P, const char *kv) {
+    memset(P, 0, sizeof *P);
+    for (int k = 0; k < NPDEFS; k++) set_param(P, PDEFS[k].key, PDEFS[k].def);
+    default_amatrix(P);
+    char *buf = strdup(kv ? kv : "");
+    kv_t items[256];
+    int n = 0;
+    for (char *line = strtok(buf, "\n"); line && n < 256; line = strtok(NULL, "\n")) {
+        char *eq = strchr(line, '=');
+        if (!eq) continue;
+        *eq = 0;
+        snprintf(items[n].key, sizeof items[n].key, "%s", trim(line));
+        snprintf(items[n].val, sizeof items[n].val, "%s", trim(eq + 1));
+        n++;
+    }
+    for (int pass = 0; pass < 2; pass++)
+        for (int k = 0; k < n; k++)
+            if (is_generic_akey(items[k].key) == (pass == 0)) set_param(P, items[k].key, items[k].val);
+    free(buf);
+    finalize_params(P);
+}
+
+/* A fresh soup exactly as main() builds it (oercel.c:2185-2202), without the
+ * initial force evaluation (ref_prime does that). */
+void *ref_create(const char *kv) {
+    ref_t *r = calloc(1, sizeof *r);
+    ref_params(&r->P, kv);
+    Params *P = &r->P;
+    Sys *s = &r->S;
+    omp_set_num_threads(P->threads);
+    omp_set_dynamic(0);
+    const int N = (int)lround(P->rho * P->L * P->L);
+    sys_alloc(s, N, P->L, g_mol.mlen, g_mol.nH, P->threads, P->nsub);
+    s->seed = P->seed;
+    s->soup_seed = P->seed;
+    rng_seed(&s->rng, P->seed);
+    init_soup(s, P);
+    set_velocities(s, P);
+    g_warm_end = P->warmup;
+    for (int i = 0; i < N; i++) {
+        s->vtx[i] = s->vx[i];
+        s->vty[i] = s->vy[i];
+    }
+    s->step = 0;
+    s->time = 0.0;
+    s->t_anchor = 0.0;
+    s->step_anchor = 0;
+    s->dt_anchor = P->dt;
+    return r;
+}
+
+/* initial sort, forces at step 0 and the half kick vh = v - dt/2 f (oercel.c:2203-2211) */
+void ref_prime(void *h) {
+    ref_t *r = h;
+    Sys *s = &r->S;
+    sort_cells(s);
+    pair_forces(s, &r->P, 0, 0.0);
+    bonded_forces(s, &r->P);
+    for (int i = 0; i < s->N; i++) {
+        s->vx[i] -= 0.5 * r->P.dt * s->fx[i];
+        s->vy[i] -= 0.5 * r->P.dt * s->fy[i];
+    }
+}
+
+int32_t ref_n(void *h) { return ((ref_t *)h)->S.N; }
+int32_t ref_ncell(void *h) { return ((ref_t *)h)->S.ncell; }
+int32_t ref_ncy(void *h) { return ((ref_t *)h)->S.ncy; }
+
+void ref_get(void *h, double *x, double *y, double *vx, double *vy, double *vtx, double *vty, double *fx, double *fy,
+             uint8_t *type, uint32_t *gid, int32_t *nxt, int8_t *mpos) {
+    Sys *s = &((ref_t *)h)->S;
+    const size_t N = (size_t)s->N;
+    memcpy(x, s->x, N * 8); memcpy(y, s->y, N * 8);
+    memcpy(vx, s->vx, N * 8); memcpy(vy, s->vy, N * 8);
+    memcpy(vtx, s->vtx, N * 8); memcpy(vty, s->vty, N * 8);
+    memcpy(fx, s->fx, N * 8); memcpy(fy, s->fy, N * 8);
+    memcpy(type, s->type, N); memcpy(gid, s->gid, N * 4);
+    memcpy(nxt, s->nxt, N * 4); memcpy(mpos, s->mpos, N);
+}
+
+void ref_set(void *h, const double *x, const double *y, const double *vx, const double *vy, const double *vtx,
+             const double *vty, const double *fx, const double *fy, const uint8_t *type, const uint32_t *gid,
+             const int32_t *nxt, const int8_t *mpos) {
+    Sys *s = &((ref_t *)h)->S;
+    const size_t N = (size_t)s->N;
+    memcpy(s->x, x, N * 8); memcpy(s->y, y, N * 8);
+    memcpy(s->vx, vx, N * 8); memcpy(s->vy, vy, N * 8);
+    memcpy(s->vtx, vtx, N * 8); memcpy(s->vty, vty, N * 8);
+    memcpy(s->fx, fx, N * 8); memcpy(s->fy, fy, N * 8);
+    memcpy(s->type, type, N); memcpy(s->gid, gid, N * 4);
+    memcpy(s->nxt, nxt, N * 4); memcpy(s->mpos, mpos, N);
+}
+
+void ref_sort(void *h) { sort_cells(&((ref_t *)h)->S); }
+
+void ref_cells(void *h, int32_t *cstart) {
+    Sys *s = &((ref_t *)h)->S;
+    memcpy(cstart, s->cstart, (size_t)(s->ncell + 1) * sizeof(int32_t));
+}
+
+int32_t ref_cell_of(void *h, double x, double y) { return cell_of_pos(&((ref_t *)h)->S, x, y); }
+
+void ref_pair(void *h, int64_t step) {
+    ref_t *r = h;
+    pair_forces(&r->S, &r->P, step, r->S.t_anchor + (double)(step - r->S.step_anchor) * r->P.dt);
+}
+
+double ref_bonded(void *h) {
+    ref_t *r = h;
+    r->S.maxbond = 0.0;
+    bonded_forces(&r->S, &r->P);
+    return r->S.maxbond;
+}
+
+/* the integrator block of main(), oercel.c:2303-2334 */
+void ref_integrate(void *h) {
+    ref_t *r = h;
+    Sys *s = &r->S;
+    const double dt = r->P.dt, dt2 = dt * dt, cvt = (0.5 + r->P.lambda) * dt, L = s->L;
+    for (int i = 0; i < s->N; i++) {
+        const double ddx = dt * s->vx[i] + dt2 * s->fx[i], ddy = dt * s->vy[i] + dt2 * s->fy[i];
+        double xi = s->x[i] + ddx, yi = s->y[i] + ddy;
+        xi = xi < 0.0 ? xi + L : xi;
+        yi = yi < 0.0 ? yi + L : yi;
+        xi = xi >= L ? xi - L : xi;
+        yi = yi >= L ? yi - L : yi;
+        s->x[i] = xi;
+        s->y[i] = yi;
+        s->vtx[i] = s->vx[i] + cvt * s->fx[i];
+        s->vty[i] = s->vy[i] + cvt * s->fy[i];
+        s->vx[i] += dt * s->fx[i];
+        s->vy[i] += dt * s->fy[i];
+    }
+}
+
+/* nsteps plain steps (no chemistry, no IO) in main()'s order: integrate,
+ * sort, pair forces of the new step, bonded forces (oercel.c:2300-2361). */
+void ref_run(void *h, int64_t nsteps) {
+    ref_t *r = h;
+    Sys *s = &r->S;
+    for (int64_t k = 0; k < nsteps; k++) {
+        const int64_t ns = s->step + 1;
+        ref_integrate(h);
+        sort_cells(s);
+        const double tn = s->t_anchor + (double)(ns - s->step_anchor) * r->P.dt;
+        pair_forces(s, &r->P, ns, tn);
+        bonded_forces(s, &r->P);
+        s->step = ns;
+        s->time = tn;
+    }
+}
+
+int64_t ref_step(void *h) { return ((ref_t *)h)->S.step; }
+
+double ref_theta(uint64_t seed, int64_t step, uint32_t gi, uint32_t gj) {
+    return pair_theta(step_seed(seed, step), gi, gj);
+}
+
+double ref_kinetic_T(void *h, double *px, double *py) {
+    ref_t *r = h;
+    return kinetic_T(&r->S, r->P.dt, px, py);
+}
+
+void ref_destroy(void *h) { free(h); /* per-bead arrays are never freed by the reference either */ }

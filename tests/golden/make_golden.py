@@ -1,0 +1,153 @@
+"""Generate the golden fixtures of this directory from the reference engine itself.
+
+    python tests/golden/make_golden.py
+
+Runs the reference's own routines (cel/engine/oercel.c compiled by
+oracle/Makefile into oracle/_ref/libref_oercel.so with FMA contraction off) and
+stores their outputs as small .npz files.  The reference has no data files of
+its own: its tests regenerate inputs from seeds (cel/engine/tests/forcetest.c),
+and so does this script, with the reference's own soup initialisation.
+Needs the reference sources (only in the build container); the fixtures are
+committed so that the tests run anywhere.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import oracle as O  # noqa: E402
+
+# configuration 1 of the workload table mapped onto the reference's keys (P is the reference's N)
+CONFIG1 = dict(L=32, rho=4, dt=0.02, gamma=4.5, kT=1, k_bond=100, r0=0.5, k_angle=0, lip_nH=1, lip_nT=2,
+               f_lip=0.15, f_Ka=0, f_Kb=0, c_N=0.05, chem=0, events=0, warmup=0, seed=0, threads=1, nsub=1,
+               a_W_H=25, a_W_T=75, a_H_T=50, a_W_N=25, a_H_N=25, a_N_T=75)
+
+
+def f32(a):
+    return np.asarray(a, np.float64).astype(np.float32).astype(np.float64)
+
+
+def soup_fixture():
+    r = O.Ref(**CONFIG1)
+    a = r.get()
+    np.savez_compressed(os.path.join(HERE, "soup_L32_seed0.npz"), x=a["x"], y=a["y"], vx=a["vx"], vy=a["vy"],
+                        type=a["type"], nxt=a["nxt"])
+
+
+def step_fixture(L, seed, name, steps=(12345,)):
+    """one state at non-trivial L, sorted by the reference with nsub = 1, its
+    pair forces (mix13 noise), bonded forces, and one integrator update"""
+    kv = dict(CONFIG1, L=L, seed=seed, f_lip=0.15, c_N=0.1)
+    r = O.Ref(**kv)
+    a = r.get()
+    rng = np.random.default_rng(seed)
+    n = len(a["x"])
+    for k in ("x", "y", "vx", "vy"):
+        a[k] = f32(a[k])
+    a["vtx"] = f32(a["vx"] + 0.3 * rng.standard_normal(n))
+    a["vty"] = f32(a["vy"])
+    # beads on cell edges and the box edge (cel/engine/tests/forcetest.c:46)
+    Lf = float(np.float32(L))
+    a["x"][0] = 0.0
+    a["y"][1] = float(np.nextafter(np.float32(Lf), np.float32(0)))
+    a["x"][2] = float(np.float32(3 * Lf / np.floor(L)))
+    r.set(a)
+    r.sort()
+    b = r.get()
+    cs = r.cells()
+    out = dict(x0=a["x"], y0=a["y"], vx0=a["vx"], vy0=a["vy"], vtx0=a["vtx"], vty0=a["vty"], type0=a["type"],
+               nxt0=a["nxt"], gid=b["gid"], cstart=cs, L=np.float64(L))
+    for s in steps:
+        r.pair(s)
+        f = r.get()
+        out[f"fx_{s}"] = f["fx"]
+        out[f"fy_{s}"] = f["fy"]
+    r.pair(steps[0])
+    f0 = r.get()
+    mb = r.bonded()
+    f1 = r.get()
+    out["bfx"] = f1["fx"] - f0["fx"]
+    out["bfy"] = f1["fy"] - f0["fy"]
+    out["maxbond"] = np.float64(mb)
+    r.integrate()
+    g = r.get()
+    for k in ("x", "y", "vx", "vy", "vtx", "vty"):
+        out[f"int_{k}"] = g[k]
+    out["int_fx"], out["int_fy"] = f1["fx"], f1["fy"]
+    np.savez_compressed(os.path.join(HERE, name), **out)
+
+
+def theta_fixture():
+    lib = O.Ref.lib()
+    rows = []
+    for seed in (0, 1, 99, 2**63 + 5):
+        for step in (0, 1, 7, 12345, 2**40 + 3):
+            for gi, gj in ((0, 1), (5, 9), (9, 5), (123456, 7), (2**28, 2**29 - 1)):
+                rows.append((seed, step, gi, gj, lib.ref_theta(seed, step, gi, gj)))
+    arr = np.array(rows, dtype=[("seed", "u8"), ("step", "i8"), ("gi", "u4"), ("gj", "u4"), ("theta", "f8")])
+    np.save(os.path.join(HERE, "theta_mix13.npy"), arr)
+
+
+def trajectory_fixture():
+    """the reference's own primed start and 20 plain steps at L = 16 (kinetic T per step)"""
+    kv = dict(CONFIG1, L=16, seed=5)
+    r = O.Ref(**kv)
+    r.prime()
+    T = []
+    for _ in range(20):
+        r.run(1)
+        T.append(r.kinetic_T(None, None))
+    a = r.get()
+    np.savez_compressed(os.path.join(HERE, "traj_L16_seed5.npz"), T=np.array(T), gid=a["gid"], x=a["x"], y=a["y"])
+
+
+def stats_fixture(nsteps=10000, equil=1000, every=10):
+    """time averages of the reference at configuration 1: kinetic temperature,
+    conservative virial and the T-T pair histogram (64 bins on [0, 2)), with
+    block standard errors (20 blocks)"""
+    r = O.Ref(**CONFIG1)
+    r.prime()
+    r.run(equil)
+    amat = np.full((8, 8), 25.0)
+    for (i, j, v) in ((0, 2, 75.0), (3, 2, 75.0), (1, 2, 50.0)):
+        amat[i, j] = amat[j, i] = v
+    p = O.params(32.0, amat)
+    T, vir, hist = [], [], []
+    for _ in range((nsteps - equil) // every):
+        r.run(every)
+        T.append(r.kinetic_T(None, None))
+        a = r.get()
+        x, y = a["x"].astype(np.float32), a["y"].astype(np.float32)
+        key, cs, src = O.sort(p, x, y)
+        st = dict(x=x[src], y=y[src], vhx=np.zeros(len(x), np.float32), vhy=np.zeros(len(x), np.float32),
+                  fx=np.zeros(len(x), np.float32), fy=np.zeros(len(x), np.float32), type=a["type"][src].copy(),
+                  next=np.full(len(x), -1, np.int32))
+        vir.append(O.observables(p, st, cs)["virial"])
+        hist.append(O.pair_hist(p, st, cs, 2, 2, 2.0, 64))
+    T, vir, hist = np.array(T), np.array(vir), np.array(hist)
+
+    def blocks(v):
+        b = np.array([c.mean(axis=0) for c in np.array_split(v, 20)])
+        return v.mean(axis=0), b.std(axis=0, ddof=1) / np.sqrt(20)
+
+    (Tm, Te), (Vm, Ve), (Hm, He) = blocks(T), blocks(vir), blocks(hist)
+    np.savez_compressed(os.path.join(HERE, "stats_config1.npz"), T=Tm, T_err=Te, virial=Vm, virial_err=Ve,
+                        tt_hist=Hm, tt_hist_err=He, nsteps=nsteps, equil=equil, every=every,
+                        n_t=int((r.get()["type"] == 2).sum()))
+
+
+if __name__ == "__main__":
+    if not O.Ref.available():
+        sys.exit("oracle/_ref/libref_oercel.so is missing: run make -C oracle with the reference sources present")
+    soup_fixture()
+    step_fixture(12.5, 99, "step_L12p5_seed99.npz")
+    step_fixture(9.0, 7, "step_L9_seed7.npz", steps=(3,))
+    theta_fixture()
+    trajectory_fixture()
+    stats_fixture()
+    for f in sorted(os.listdir(HERE)):
+        print(f, os.path.getsize(os.path.join(HERE, f)))

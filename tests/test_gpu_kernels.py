@@ -1,0 +1,131 @@
+"""Parity of each CUDA phase with the oracle and the reference (through the C ABI).
+
+Criteria: cell assignment, cell starts, the sort permutation, link topology and
+the FP32 integrator are bit-exact; forces are within 1e-5 relative to the
+largest force (max |F_gpu - F_ref| <= 1e-5 max |F_ref|), FP32 against FP64.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden
+from gpu_util import (engine_with, links_from_next, oracle_params, oracle_state, params, rel_err)
+
+pytestmark = pytest.mark.gpu
+FORCE_TOL = 1e-5
+
+CASES = [("step_L12p5_seed99.npz", 12.5, 99, 12345), ("step_L9_seed7.npz", 9.0, 7, 3)]
+
+
+def fixture_engine(name, L, seed, noise="mix13", use_vt=True, **kv):
+    g = golden(name)
+    p = params(L=L, seed=seed, noise=noise, **kv)
+    prev, nxt = links_from_next(g["nxt0"])
+    v = (g["vtx0"], g["vty0"]) if use_vt else (g["vx0"], g["vy0"])
+    e = engine_with(p, g["x0"], g["y0"], v[0], v[1], g["type0"], prev, nxt)
+    return g, p, e
+
+
+@pytest.mark.parametrize("name,L,seed,step", CASES)
+def test_build_cells_matches_reference(cuda_ok, name, L, seed, step):
+    g, p, e = fixture_engine(name, L, seed)
+    e.build_cells()
+    s = e.state()
+    assert np.array_equal(e.cells(), g["cstart"])
+    assert np.array_equal(s["gid"], g["gid"])
+    # links follow the beads: next of slot d is the slot holding nxt0[gid[d]]
+    nxt0 = g["nxt0"]
+    slot = np.empty(len(s["gid"]), np.int64)
+    slot[s["gid"]] = np.arange(len(slot))
+    want = np.where(nxt0[s["gid"]] >= 0, slot[np.maximum(nxt0[s["gid"]], 0)], -1)
+    assert np.array_equal(s["next"], want)
+    assert np.array_equal(s["x"], g["x0"][s["gid"]].astype(np.float32))
+
+
+@pytest.mark.parametrize("name,L,seed,step", CASES)
+def test_pair_forces_match_reference(cuda_ok, name, L, seed, step):
+    g, p, e = fixture_engine(name, L, seed, noise="mix13")
+    e.build_cells()
+    fx, fy = e.pair_forces(0, step)
+    assert rel_err(fx, g[f"fx_{step}"]) < FORCE_TOL
+    assert rel_err(fy, g[f"fy_{step}"]) < FORCE_TOL
+
+
+@pytest.mark.parametrize("noise", ["philox", "mix13"])
+def test_pair_forces_match_oracle(cuda_ok, noise):
+    g, p, e = fixture_engine("step_L12p5_seed99.npz", 12.5, 99, noise=noise)
+    e.build_cells()
+    s = oracle_state(e.state())
+    op = oracle_params(p)
+    for step in (0, 1, 777):
+        fx, fy = e.pair_forces(0, step)
+        rx, ry = O.pair_forces(op, s, e.cells(), step, noise=True)
+        assert rel_err(fx, rx) < FORCE_TOL and rel_err(fy, ry) < FORCE_TOL, step
+
+
+def test_pair_forces_without_noise(cuda_ok):
+    """sigma -> 0 (kT = 1e-20): conservative + dissipative forces only"""
+    g, p, e = fixture_engine("step_L12p5_seed99.npz", 12.5, 99, noise="philox", kT=1e-20)
+    e.build_cells()
+    s = oracle_state(e.state())
+    fx, fy = e.pair_forces(0, 5)
+    rx, ry = O.pair_forces(oracle_params(p), s, e.cells(), 5, noise=False)
+    assert rel_err(fx, rx) < FORCE_TOL and rel_err(fy, ry) < FORCE_TOL
+
+
+@pytest.mark.parametrize("name,L,seed,step", CASES)
+def test_bond_forces_match_reference(cuda_ok, name, L, seed, step):
+    g, p, e = fixture_engine(name, L, seed)
+    e.build_cells()
+    bx, by, mb = e.bond_forces(0)
+    assert rel_err(bx, g["bfx"]) < FORCE_TOL and rel_err(by, g["bfy"]) < FORCE_TOL
+    assert mb == pytest.approx(float(g["maxbond"]), rel=1e-6)
+
+
+def test_forces_deterministic_and_momentum_free(cuda_ok):
+    g, p, e = fixture_engine("step_L12p5_seed99.npz", 12.5, 99, noise="philox")
+    e.build_cells()
+    e.forces(42)
+    a = e.state()
+    e.forces(42)
+    b = e.state()
+    assert np.array_equal(a["fx"], b["fx"]) and np.array_equal(a["fy"], b["fy"])
+    # pair and bond terms cancel exactly in fixed point; what is left is the
+    # final FP32 rounding of each bead's sum (<= 1/2 ulp each)
+    ulp = np.spacing(np.abs(a["fx"]).astype(np.float32)).astype(np.float64)
+    assert abs(a["fx"].astype(np.float64).sum()) <= 0.5 * ulp.sum()
+    pair_plus_bond = e.pair_forces(0, 42)[0].astype(np.float64) + e.bond_forces(0)[0]
+    assert np.abs(pair_plus_bond - a["fx"]).max() <= 4 * np.spacing(np.float32(np.abs(a["fx"]).max()))
+
+
+def test_integrate_bit_exact_against_fp32_oracle(cuda_ok):
+    g, p, e = fixture_engine("step_L12p5_seed99.npz", 12.5, 99)
+    e.build_cells()
+    rng = np.random.default_rng(3)
+    n = len(g["x0"])
+    vh = rng.normal(size=(2, n)).astype(np.float32)
+    f = (80 * rng.normal(size=(2, n))).astype(np.float32)
+    e.set_dynamics(0, vh[0], vh[1], f[0], f[1])
+    before = e.state()
+    e.integrate()
+    after = e.state()
+    st = dict(x=before["x"].copy(), y=before["y"].copy(), vhx=before["vhx"].copy(), vhy=before["vhy"].copy(),
+              vtx=np.zeros(n, np.float32), vty=np.zeros(n, np.float32), fx=before["fx"], fy=before["fy"])
+    assert O.integrate_f32(oracle_params(p), st) == 0
+    for k in ("x", "y", "vhx", "vhy", "vtx", "vty"):
+        assert np.array_equal(after[k], st[k]), k
+
+
+def test_sort_at_one_million_beads(cuda_ok):
+    """size-independent properties at the 1M-bead size: the sort is the oracle's
+    stable counting sort, bit for bit, and every bead lies in its cell"""
+    import oercel_b200 as ob
+    p = params(L=512, seed=1)
+    s = ob.soup_for(p)
+    e = engine_with(p, s["x"], s["y"], s["vx"], s["vy"], s["type"], s["prev"], s["next"])
+    e.build_cells()
+    st = e.state()
+    key, cs, src = O.sort(oracle_params(p), s["x"], s["y"])
+    assert np.array_equal(e.cells(), cs)
+    assert np.array_equal(st["gid"], src.astype(np.uint32))
+    assert np.all(np.diff(key[src]) >= 0)

@@ -1,0 +1,714 @@
+// dpd_capi.cu -- the C ABI of libdpd.so (include/dpd.h): handles, device
+// memory, CUDA graphs of the step, state in/out, error reporting.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dpd.h"
+#include "dpd_internal.h"
+
+static_assert(sizeof(dpd_event) == sizeof(EventDev), "event layout");
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) return fail(DPD_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                         \
+    } while (0)
+
+struct dpd_handle {
+    int nrep = 0;
+    std::vector<dpd_params> params;
+    std::vector<RepDev> rh;
+    int64_t N = 0, C = 0;
+    int nmax = 0;
+    cudaStream_t s = nullptr;
+    RepDev *d_rep = nullptr;
+    Chunk *d_bch = nullptr, *d_cch = nullptr;
+    int nbch = 0, ncch = 0;
+    Bufs b{};
+    int cur = 0;
+    bool any_chem = false;
+    bool keys_valid = false;
+    int64_t step = 0;
+    // CUDA graphs of gsteps consecutive steps, one per starting buffer parity
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int gsteps = 0;
+    // staging for state in/out
+    char *stage = nullptr;
+    std::vector<void *> allocs;
+};
+
+extern "C" const char *dpd_last_error(void) { return g_err.c_str(); }
+extern "C" const char *dpd_version(void) { return "libdpd 0.1 (sm_100a)"; }
+
+extern "C" int dpd_params_default(dpd_params *p) {
+    if (!p) return fail(DPD_E_ARG, "null params");
+    memset(p, 0, sizeof *p);
+    p->L = 64.0;   // reference defaults: cel/engine/oercel.c:237-299
+    p->dt = 0.03;
+    p->lambda = 0.65;
+    p->gamma = 4.5;
+    p->kT = 1.0;
+    for (int i = 0; i < DPD_MAXT * DPD_MAXT; i++) p->a[i] = 25.0;
+    p->k_bond = 100.0;
+    p->r0 = 0.5;
+    p->seed = 1;
+    p->noise = 0;
+    p->chem = 0;
+    p->n_chem = 1;
+    p->n_t_min = 2;
+    p->max_chain = 12;  // reference MAXMLEN, oercel.c:50
+    p->p_break = 1e-5;
+    p->p_grow = 1e-3;
+    p->p_bond = 1e-2;
+    p->r_grow = 1.0;
+    p->r_bond = 0.6;
+    return DPD_OK;
+}
+
+static uint32_t threshold(double p) {
+    const double t = std::floor(p * 4294967296.0);
+    if (!(t > 0.0)) return 0u;
+    if (t >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)t;
+}
+
+static int make_rep(const dpd_params &p, int b0, int n, int c0, RepDev &R) {
+    memset(&R, 0, sizeof R);
+    if (!(p.L >= 3.0) || !std::isfinite(p.L)) return fail(DPD_E_ARG, "L must be >= 3 (got %g)", p.L);
+    if (!(p.dt > 0.0)) return fail(DPD_E_ARG, "dt must be > 0");
+    if (!(p.kT > 0.0)) return fail(DPD_E_ARG, "kT must be > 0");
+    if (p.gamma < 0.0) return fail(DPD_E_ARG, "gamma must be >= 0");
+    if (p.noise != 0 && p.noise != 1) return fail(DPD_E_ARG, "noise must be 0 (philox) or 1 (mix13)");
+    if (p.chem && p.n_chem < 1) return fail(DPD_E_ARG, "n_chem must be >= 1");
+    if (p.chem && (p.max_chain < 2 || p.max_chain > 1000)) return fail(DPD_E_ARG, "max_chain must be 2..1000");
+    if (p.chem && !(p.r_grow > 0.0 && p.r_grow <= 1.0 && p.r_bond > 0.0 && p.r_bond <= 1.0))
+        return fail(DPD_E_ARG, "reaction radii must lie in (0, 1]");
+    for (int i = 0; i < DPD_MAXT; i++)
+        for (int j = 0; j < DPD_MAXT; j++)
+            if (p.a[i * DPD_MAXT + j] != p.a[j * DPD_MAXT + i]) return fail(DPD_E_ARG, "a_ij must be symmetric");
+    R.L = (float)p.L;
+    R.halfL = 0.5f * R.L;
+    R.ncx = R.ncy = (int)std::floor((double)R.L);
+    R.icsx = R.ncx / (double)R.L;
+    R.icsy = R.ncy / (double)R.L;
+    R.b0 = b0;
+    R.n = n;
+    R.c0 = c0;
+    R.ncell = R.ncx * R.ncy;
+    R.dt = (float)p.dt;
+    R.dt2 = (float)(p.dt * p.dt);
+    R.cvt = (float)((0.5 + p.lambda) * p.dt);
+    R.hdt = (float)(0.5 * p.dt);
+    R.gamma = (float)p.gamma;
+    R.sdt = (float)(std::sqrt(2.0 * p.gamma * p.kT) / std::sqrt(p.dt));
+    R.kb = (float)p.k_bond;
+    R.r0 = (float)p.r0;
+    for (int i = 0; i < DPD_MAXT * DPD_MAXT; i++) R.a[i] = (float)p.a[i];
+    R.seed = p.seed;
+    R.noise = p.noise;
+    R.chem = p.chem;
+    R.n_chem = p.n_chem;
+    R.thr_break = threshold(p.p_break);
+    R.thr_grow = threshold(p.p_grow);
+    R.thr_bond = threshold(p.p_bond);
+    R.r2_grow = (float)(p.r_grow * p.r_grow);
+    R.r2_bond = (float)(p.r_bond * p.r_bond);
+    R.n_t_min = p.n_t_min;
+    R.max_chain = p.max_chain;
+    return DPD_OK;
+}
+
+template <typename T>
+static int dalloc(dpd_handle *h, T **p, size_t count) {
+    void *q = nullptr;
+    const size_t bytes = count * sizeof(T) + 64;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return fail(DPD_E_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    h->allocs.push_back(q);
+    *p = (T *)q;
+    return DPD_OK;
+}
+
+#define TRY(x)                       \
+    do {                             \
+        int r_ = (x);                \
+        if (r_ != DPD_OK) return r_; \
+    } while (0)
+
+static void drop_graphs(dpd_handle *h) {
+    for (int k = 0; k < 2; k++)
+        if (h->gexec[k]) {
+            cudaGraphExecDestroy(h->gexec[k]);
+            h->gexec[k] = nullptr;
+        }
+}
+
+static void free_all(dpd_handle *h) {
+    drop_graphs(h);
+    for (void *p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    if (h->s) cudaStreamDestroy(h->s);
+}
+
+static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, const int32_t *n_beads) {
+    h->nrep = nrep;
+    h->params.assign(params, params + nrep);
+    h->rh.resize(nrep);
+    int64_t b0 = 0, c0 = 0;
+    for (int r = 0; r < nrep; r++) {
+        if (n_beads[r] < 2) return fail(DPD_E_ARG, "replica %d: need at least 2 beads", r);
+        TRY(make_rep(params[r], (int)b0, n_beads[r], (int)c0, h->rh[r]));
+        h->any_chem = h->any_chem || params[r].chem;
+        b0 += n_beads[r];
+        c0 += h->rh[r].ncell;
+        h->nmax = std::max(h->nmax, (int)n_beads[r]);
+        if (b0 > (int64_t)GID_MASK || c0 > (int64_t)0x7fffffff - 8)
+            return fail(DPD_E_ARG, "too many beads or cells (beads < 2^29 in total)");
+    }
+    h->N = b0;
+    h->C = c0;
+    // work chunks: CTAs never straddle replicas
+    std::vector<Chunk> bch, cch;
+    for (int r = 0; r < nrep; r++) {
+        const RepDev &R = h->rh[r];
+        for (int k = 0; k < R.n; k += BEAD_TPB) bch.push_back({r, R.b0 + k, R.b0 + std::min(R.n, k + BEAD_TPB), 0});
+        for (int k = 0; k < R.ncell; k += CELL_TPB)
+            cch.push_back({r, R.c0 + k, R.c0 + std::min(R.ncell, k + CELL_TPB), 0});
+    }
+    h->nbch = (int)bch.size();
+    h->ncch = (int)cch.size();
+    CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+    TRY(dalloc(h, &h->d_rep, nrep));
+    TRY(dalloc(h, &h->d_bch, bch.size()));
+    TRY(dalloc(h, &h->d_cch, cch.size()));
+    CK(cudaMemcpy(h->d_rep, h->rh.data(), nrep * sizeof(RepDev), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_bch, bch.data(), bch.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_cch, cch.data(), cch.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+    Bufs &b = h->b;
+    const size_t N = (size_t)h->N, C = (size_t)h->C;
+    for (int k = 0; k < 2; k++) {
+        TRY(dalloc(h, &b.pos[k], N));
+        TRY(dalloc(h, &b.vh[k], N));
+        TRY(dalloc(h, &b.vt[k], N));
+        TRY(dalloc(h, &b.f[k], N));
+        TRY(dalloc(h, &b.tg[k], N));
+        TRY(dalloc(h, &b.link[k], N));
+    }
+    TRY(dalloc(h, &b.key, N));
+    TRY(dalloc(h, &b.rank, N));
+    TRY(dalloc(h, &b.src, N));
+    TRY(dalloc(h, &b.dest, N));
+    TRY(dalloc(h, &b.count, C + 4));
+    TRY(dalloc(h, &b.cstart, C + 4));
+    TRY(dalloc(h, &b.bsum, C / SCAN_PER_BLOCK + 2));
+    TRY(dalloc(h, &b.claim, N));
+    TRY(dalloc(h, &b.req, N));
+    b.evcap = 1 << 20;
+    TRY(dalloc(h, &b.events, (size_t)b.evcap));
+    TRY(dalloc(h, &b.status, 1));
+    TRY(dalloc(h, &b.step, 1));
+    TRY(dalloc(h, &b.obs, (size_t)nrep * OBS_N));
+    TRY(dalloc(h, &b.hist, 4096));
+    // staging for set/get state: 8 float + 3 int32 + 1 byte arrays of nmax
+    TRY(dalloc(h, &h->stage, (size_t)h->nmax * (8 * 4 + 3 * 4 + 1) + 16 * 256));
+    CK(cudaMemset(b.count, 0, (C + 4) * sizeof(uint32_t)));
+    CK(cudaMemset(b.claim, 0xFF, N * sizeof(uint32_t)));
+    CK(cudaMemset(b.req, 0xFF, N * sizeof(int32_t)));
+    CK(cudaMemset(b.status, 0, sizeof(DevStatus)));
+    CK(cudaMemset(b.step, 0, sizeof(long long)));
+    CK(cudaMemset(b.obs, 0, (size_t)nrep * OBS_N * sizeof(unsigned long long)));
+    for (int k = 0; k < 2; k++) {
+        CK(cudaMemset(b.pos[k], 0, N * sizeof(float2)));
+        CK(cudaMemset(b.vh[k], 0, N * sizeof(float2)));
+        CK(cudaMemset(b.vt[k], 0, N * sizeof(float2)));
+        CK(cudaMemset(b.f[k], 0, N * sizeof(float2)));
+        CK(cudaMemset(b.tg[k], 0, N * sizeof(uint32_t)));
+        CK(cudaMemset(b.link[k], 0xFF, N * sizeof(int2)));
+    }
+    // graph length: even (the buffers alternate every step), ~4M bead-steps per replay
+    int g = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 << 20) / std::max<int64_t>(1, h->N)));
+    if (const char *e = getenv("DPD_GRAPH_STEPS")) g = atoi(e);
+    h->gsteps = std::max(1, g);
+    return DPD_OK;
+}
+
+extern "C" int dpd_create(const dpd_params *params, int32_t n_replicas, const int32_t *n_beads, dpd_handle **out) {
+    if (!params || !n_beads || !out || n_replicas < 1) return fail(DPD_E_ARG, "bad arguments to dpd_create");
+    *out = nullptr;
+    dpd_handle *h = new dpd_handle();
+    const int r = create_impl(h, params, n_replicas, n_beads);
+    if (r != DPD_OK) {
+        free_all(h);
+        delete h;
+        return r;
+    }
+    *out = h;
+    return DPD_OK;
+}
+
+extern "C" int dpd_destroy(dpd_handle *h) {
+    if (!h) return DPD_OK;
+    cudaStreamSynchronize(h->s);
+    free_all(h);
+    delete h;
+    return DPD_OK;
+}
+
+extern "C" int dpd_sizes(const dpd_handle *h, int32_t r, int64_t *n_total, int32_t *n_beads, int32_t *n_cells) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    if (n_total) *n_total = h->N;
+    if (r >= 0 && r < h->nrep) {
+        if (n_beads) *n_beads = h->rh[r].n;
+        if (n_cells) *n_cells = h->rh[r].ncell;
+    } else if (n_beads || n_cells) {
+        return fail(DPD_E_ARG, "replica %d out of range", r);
+    }
+    return DPD_OK;
+}
+
+// ---------------------------------------------------------------- status
+
+static int check_status(dpd_handle *h) {
+    DevStatus st;
+    CK(cudaMemcpyAsync(&st, h->b.status, sizeof st, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    if (st.flags) {
+        CK(cudaMemsetAsync(&h->b.status->flags, 0, sizeof(unsigned), h->s));
+        CK(cudaStreamSynchronize(h->s));
+        if (st.flags & DPD_F_NONFINITE) return fail(DPD_E_STATE, "non-finite force (flags 0x%x)", st.flags);
+        if (st.flags & DPD_F_OUTSIDE)
+            return fail(DPD_E_STATE, "a bead moved more than one box length in one step (flags 0x%x)", st.flags);
+        if (st.flags & DPD_F_EVENTS)
+            return fail(DPD_E_EVENT_OVERFLOW, "event buffer full (%u events since the last read)", st.nevents);
+        if (st.flags & DPD_F_CHAIN) return fail(DPD_E_CHAIN, "broken lipid chain");
+    }
+    return DPD_OK;
+}
+
+static int ensure_replica(const dpd_handle *h, int r) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    if (r < 0 || r >= h->nrep) return fail(DPD_E_ARG, "replica %d out of range (0..%d)", r, h->nrep - 1);
+    return DPD_OK;
+}
+
+// ---------------------------------------------------------------- state in/out
+
+extern "C" int dpd_set_state(dpd_handle *h, int32_t r, const float *x, const float *y, const float *vx,
+                             const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
+                             const int32_t *next) {
+    TRY(ensure_replica(h, r));
+    if (!x || !y || !vx || !vy || !type) return fail(DPD_E_ARG, "x, y, vx, vy and type are required");
+    const RepDev &R = h->rh[r];
+    const size_t n = (size_t)R.n, a = ((n * 4 + 255) / 256) * 256;
+    char *p = h->stage;
+    float *sx = (float *)p, *sy = (float *)(p + a), *svx = (float *)(p + 2 * a), *svy = (float *)(p + 3 * a);
+    uint32_t *sg = (uint32_t *)(p + 4 * a);
+    int32_t *sp = (int32_t *)(p + 5 * a), *sn = (int32_t *)(p + 6 * a);
+    uint8_t *st = (uint8_t *)(p + 7 * a);
+    CK(cudaMemcpyAsync(sx, x, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaMemcpyAsync(sy, y, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaMemcpyAsync(svx, vx, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaMemcpyAsync(svy, vy, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaMemcpyAsync(st, type, n, cudaMemcpyDefault, h->s));
+    if (gid) CK(cudaMemcpyAsync(sg, gid, n * 4, cudaMemcpyDefault, h->s));
+    if (prev) CK(cudaMemcpyAsync(sp, prev, n * 4, cudaMemcpyDefault, h->s));
+    if (next) CK(cudaMemcpyAsync(sn, next, n * 4, cudaMemcpyDefault, h->s));
+    launch_pack(h->b, h->cur, R.b0, (int)n, sx, sy, svx, svy, st, gid ? sg : nullptr, prev ? sp : nullptr,
+                next ? sn : nullptr, h->s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s));
+    h->keys_valid = false;
+    return DPD_OK;
+}
+
+extern "C" int dpd_get_state(dpd_handle *h, int32_t r, float *x, float *y, float *vhx, float *vhy, float *vtx,
+                             float *vty, float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev,
+                             int32_t *next) {
+    TRY(ensure_replica(h, r));
+    const RepDev &R = h->rh[r];
+    const size_t n = (size_t)R.n, a = ((n * 4 + 255) / 256) * 256;
+    char *p = h->stage;
+    float *f8[8];
+    for (int k = 0; k < 8; k++) f8[k] = (float *)(p + k * a);
+    uint32_t *sg = (uint32_t *)(p + 8 * a);
+    int32_t *sp = (int32_t *)(p + 9 * a), *sn = (int32_t *)(p + 10 * a);
+    uint8_t *st = (uint8_t *)(p + 11 * a);
+    launch_unpack(h->b, h->cur, R.b0, (int)n, f8[0], f8[1], f8[2], f8[3], f8[4], f8[5], f8[6], f8[7], st, sg, sp,
+                  sn, h->s);
+    CK(cudaGetLastError());
+    float *outs[8] = {x, y, vhx, vhy, vtx, vty, fx, fy};
+    for (int k = 0; k < 8; k++)
+        if (outs[k]) CK(cudaMemcpyAsync(outs[k], f8[k], n * 4, cudaMemcpyDefault, h->s));
+    if (type) CK(cudaMemcpyAsync(type, st, n, cudaMemcpyDefault, h->s));
+    if (gid) CK(cudaMemcpyAsync(gid, sg, n * 4, cudaMemcpyDefault, h->s));
+    if (prev) CK(cudaMemcpyAsync(prev, sp, n * 4, cudaMemcpyDefault, h->s));
+    if (next) CK(cudaMemcpyAsync(next, sn, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return DPD_OK;
+}
+
+extern "C" int dpd_set_dynamics(dpd_handle *h, int32_t r, const float *vhx, const float *vhy, const float *fx,
+                                const float *fy) {
+    TRY(ensure_replica(h, r));
+    const RepDev &R = h->rh[r];
+    const size_t n = (size_t)R.n, a = ((n * 4 + 255) / 256) * 256;
+    const float *in[4] = {vhx, vhy, fx, fy};
+    float *sg[4];
+    for (int k = 0; k < 4; k++) {
+        sg[k] = (float *)(h->stage + k * a);
+        if (in[k]) CK(cudaMemcpyAsync(sg[k], in[k], n * 4, cudaMemcpyDefault, h->s));
+    }
+    launch_set_dynamics(h->b, h->cur, R.b0, (int)n, vhx ? sg[0] : nullptr, vhy ? sg[1] : nullptr,
+                        fx ? sg[2] : nullptr, fy ? sg[3] : nullptr, h->s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s));
+    h->keys_valid = false;
+    return DPD_OK;
+}
+
+// ---------------------------------------------------------------- phases
+
+static void enqueue_sort(dpd_handle *h, PermuteMode mode) {
+    // counts of the CURRENT positions
+    cudaMemsetAsync(h->b.count, 0, (size_t)(h->C + 4) * sizeof(uint32_t), h->s);
+    launch_keys(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, false, h->s);
+    launch_scan(h->b, h->C, false, h->s);
+    launch_place(h->b, h->d_bch, h->nbch, h->s);
+    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, mode, h->s);
+    h->cur ^= 1;
+}
+
+static int set_device_step(dpd_handle *h, int64_t step) {
+    long long v = (long long)step;
+    CK(cudaMemcpyAsync(h->b.step, &v, sizeof v, cudaMemcpyHostToDevice, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    h->step = step;
+    return DPD_OK;
+}
+
+static void enqueue_next_keys(dpd_handle *h) {
+    cudaMemsetAsync(h->b.count, 0, (size_t)(h->C + 4) * sizeof(uint32_t), h->s);
+    launch_keys(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, h->s);
+    h->keys_valid = true;
+}
+
+extern "C" int dpd_prime(dpd_handle *h) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    enqueue_sort(h, PERM_PRIME);
+    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, false, h->s);
+    launch_halfkick(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
+    enqueue_next_keys(h);
+    CK(cudaGetLastError());
+    return check_status(h);
+}
+
+extern "C" int dpd_resume(dpd_handle *h) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    enqueue_sort(h, PERM_SORT);
+    enqueue_next_keys(h);
+    CK(cudaGetLastError());
+    return check_status(h);
+}
+
+extern "C" int dpd_get_step(const dpd_handle *h, int64_t *step) {
+    if (!h || !step) return fail(DPD_E_ARG, "null argument");
+    *step = h->step;
+    return DPD_OK;
+}
+
+extern "C" int dpd_set_step(dpd_handle *h, int64_t step) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    return set_device_step(h, step);
+}
+
+extern "C" int dpd_build_cells(dpd_handle *h) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    enqueue_sort(h, PERM_SORT);
+    h->keys_valid = false;
+    CK(cudaGetLastError());
+    return check_status(h);
+}
+
+extern "C" int dpd_get_cells(dpd_handle *h, int32_t r, int32_t *cstart) {
+    TRY(ensure_replica(h, r));
+    if (!cstart) return fail(DPD_E_ARG, "null cstart");
+    const RepDev &R = h->rh[r];
+    std::vector<int32_t> tmp(R.ncell + 1);
+    CK(cudaMemcpyAsync(tmp.data(), h->b.cstart + R.c0, (R.ncell + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       h->s));
+    CK(cudaStreamSynchronize(h->s));
+    for (auto &v : tmp) v -= R.b0;
+    CK(cudaMemcpy(cstart, tmp.data(), tmp.size() * sizeof(int32_t), cudaMemcpyDefault));
+    return DPD_OK;
+}
+
+extern "C" int dpd_forces(dpd_handle *h, int64_t step) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    TRY(set_device_step(h, step));
+    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, false, h->s);
+    h->keys_valid = false;
+    CK(cudaGetLastError());
+    return check_status(h);
+}
+
+static int partial_forces(dpd_handle *h, int32_t r, bool pair, bool bond, float *fx, float *fy) {
+    // computed into the spare force buffer so the stored forces stay untouched
+    Bufs b = h->b;
+    b.f[h->cur] = h->b.f[h->cur ^ 1];
+    launch_forces(b, h->cur, h->d_rep, h->d_bch, h->nbch, pair, bond, false, h->s);
+    CK(cudaGetLastError());
+    const RepDev &R = h->rh[r];
+    const size_t n = (size_t)R.n, a = ((n * 4 + 255) / 256) * 256;
+    float *sx = (float *)h->stage, *sy = (float *)(h->stage + a);
+    Bufs u = h->b;
+    u.f[h->cur] = b.f[h->cur];
+    launch_unpack(u, h->cur, R.b0, (int)n, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, sx, sy, nullptr,
+                  nullptr, nullptr, nullptr, h->s);
+    CK(cudaGetLastError());
+    if (fx) CK(cudaMemcpyAsync(fx, sx, n * 4, cudaMemcpyDefault, h->s));
+    if (fy) CK(cudaMemcpyAsync(fy, sy, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return check_status(h);
+}
+
+extern "C" int dpd_pair_forces(dpd_handle *h, int32_t r, int64_t step, float *fx, float *fy) {
+    TRY(ensure_replica(h, r));
+    TRY(set_device_step(h, step));
+    return partial_forces(h, r, true, false, fx, fy);
+}
+
+extern "C" int dpd_bond_forces(dpd_handle *h, int32_t r, float *fx, float *fy, float *maxbond) {
+    TRY(ensure_replica(h, r));
+    unsigned long long *slot = h->b.obs + (size_t)r * OBS_N + 4;
+    CK(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), h->s));
+    TRY(partial_forces(h, r, false, true, fx, fy));
+    if (maxbond) {
+        unsigned long long v = 0;
+        CK(cudaMemcpy(&v, slot, sizeof v, cudaMemcpyDeviceToHost));
+        uint32_t bits = (uint32_t)v;
+        memcpy(maxbond, &bits, 4);
+    }
+    return DPD_OK;
+}
+
+extern "C" int dpd_integrate(dpd_handle *h) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    launch_integrate(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
+    h->keys_valid = false;
+    CK(cudaGetLastError());
+    return check_status(h);
+}
+
+extern "C" int dpd_chemistry(dpd_handle *h, int64_t step) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    TRY(set_device_step(h, step));
+    launch_chemistry(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
+    CK(cudaGetLastError());
+    return check_status(h);
+}
+
+// ---------------------------------------------------------------- the step
+
+static void enqueue_step(dpd_handle *h) {
+    launch_scan(h->b, h->C, true, h->s);
+    launch_place(h->b, h->d_bch, h->nbch, h->s);
+    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
+    h->cur ^= 1;
+    if (h->any_chem) launch_chemistry(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
+    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, true, h->s);
+}
+
+// capture gsteps steps starting from the current buffer parity
+static int build_graph(dpd_handle *h) {
+    const int cur0 = h->cur;
+    if (h->gexec[cur0]) {
+        CK(cudaGraphExecDestroy(h->gexec[cur0]));
+        h->gexec[cur0] = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < h->gsteps; k++) enqueue_step(h);
+    const cudaError_t e = cudaStreamEndCapture(h->s, &g);
+    h->cur = cur0;  // capture only recorded the launches
+    if (e != cudaSuccess) return fail(DPD_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    const cudaError_t e2 = cudaGraphInstantiate(&h->gexec[cur0], g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) return fail(DPD_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e2));
+    return DPD_OK;
+}
+
+// enqueue nsteps steps: whole graphs while they fit, eager launches for the rest
+static int enqueue_steps(dpd_handle *h, int64_t nsteps) {
+    if (nsteps < 0) return fail(DPD_E_ARG, "nsteps must be >= 0");
+    if (nsteps == 0) return DPD_OK;
+    if (!h->keys_valid) enqueue_next_keys(h);
+    int64_t left = nsteps;
+    const bool graphs = getenv("DPD_NO_GRAPH") == nullptr;
+    while (graphs && left >= h->gsteps) {
+        if (!h->gexec[h->cur]) TRY(build_graph(h));
+        CK(cudaGraphLaunch(h->gexec[h->cur], h->s));
+        left -= h->gsteps;
+        if (h->gsteps & 1) h->cur ^= 1;
+    }
+    for (; left > 0; left--) enqueue_step(h);
+    CK(cudaGetLastError());
+    h->step += nsteps;
+    return DPD_OK;
+}
+
+extern "C" int dpd_step(dpd_handle *h, int64_t nsteps) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    TRY(enqueue_steps(h, nsteps));
+    return check_status(h);
+}
+
+extern "C" int dpd_step_async(dpd_handle *h, int64_t nsteps) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    return enqueue_steps(h, nsteps);
+}
+
+extern "C" int dpd_sync(dpd_handle *h) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    return check_status(h);
+}
+
+extern "C" int dpd_set_graph_steps(dpd_handle *h, int32_t steps) {
+    if (!h || steps < 1) return fail(DPD_E_ARG, "graph length must be >= 1");
+    CK(cudaStreamSynchronize(h->s));
+    drop_graphs(h);
+    h->gsteps = steps;
+    return DPD_OK;
+}
+
+// One step launched kernel by kernel with CUDA events between the launches on
+// the handle's stream; ms[k] = device time of kernel k (scan1, scan2, place,
+// cellfix, permute, [5 chemistry], forces).  The step is a real step.
+extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_out) {
+    if (!h || !ms || !n_out) return fail(DPD_E_ARG, "null argument");
+    if (!h->keys_valid) enqueue_next_keys(h);
+    const int nk = 6 + (h->any_chem ? chem_kernel_count() : 0);
+    if (cap < nk) return fail(DPD_E_ARG, "need room for %d kernel times", nk);
+    std::vector<cudaEvent_t> ev(nk + 1);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    int k = 0;
+    const int nb = (int)((h->C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
+    (void)nb;
+    CK(cudaEventRecord(ev[k++], h->s));
+    launch_scan_part(h->b, h->C, true, 1, h->s);
+    CK(cudaEventRecord(ev[k++], h->s));
+    launch_scan_part(h->b, h->C, true, 2, h->s);
+    CK(cudaEventRecord(ev[k++], h->s));
+    launch_place(h->b, h->d_bch, h->nbch, h->s);
+    CK(cudaEventRecord(ev[k++], h->s));
+    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    CK(cudaEventRecord(ev[k++], h->s));
+    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
+    CK(cudaEventRecord(ev[k++], h->s));
+    h->cur ^= 1;
+    if (h->any_chem)
+        for (int c = 0; c < chem_kernel_count(); c++) {
+            launch_chemistry_part(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, c, h->s);
+            CK(cudaEventRecord(ev[k++], h->s));
+        }
+    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, true, h->s);
+    CK(cudaEventRecord(ev[k++], h->s));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[nk]));
+    for (int q = 0; q < nk; q++) CK(cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]));
+    for (auto &e : ev) cudaEventDestroy(e);
+    h->step += 1;
+    *n_out = nk;
+    return check_status(h);
+}
+
+extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out) {
+    if (!h || !n_out) return fail(DPD_E_ARG, "null argument");
+    DevStatus st;
+    CK(cudaMemcpyAsync(&st, h->b.status, sizeof st, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    const int have = (int)std::min<unsigned>(st.nevents, (unsigned)h->b.evcap);
+    const int n = std::min(have, cap < 0 ? 0 : cap);
+    if (n > 0 && out) CK(cudaMemcpy(out, h->b.events, (size_t)n * sizeof(dpd_event), cudaMemcpyDefault));
+    *n_out = n;
+    CK(cudaMemset(&h->b.status->nevents, 0, sizeof(unsigned)));
+    if (st.nevents > (unsigned)h->b.evcap)
+        return fail(DPD_E_EVENT_OVERFLOW, "%u events were recorded, %d kept", st.nevents, h->b.evcap);
+    return DPD_OK;
+}
+
+extern "C" int dpd_observables(dpd_handle *h, int32_t r, double *out) {
+    TRY(ensure_replica(h, r));
+    if (!out) return fail(DPD_E_ARG, "null out");
+    unsigned long long *o = h->b.obs + (size_t)r * OBS_N;
+    CK(cudaMemsetAsync(o, 0, 4 * sizeof(unsigned long long), h->s));
+    CK(cudaMemsetAsync(o + 5, 0, (OBS_N - 5) * sizeof(unsigned long long), h->s));
+    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, h->s);
+    CK(cudaGetLastError());
+    unsigned long long v[OBS_N];
+    CK(cudaMemcpyAsync(v, o, sizeof v, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    CK(cudaMemsetAsync(o + 4, 0, sizeof(unsigned long long), h->s));  // max bond restarts per stats row
+    const RepDev &R = h->rh[r];
+    for (int k = 0; k < 16; k++) out[k] = 0.0;
+    out[0] = (double)(long long)v[2] / OBS_FIX / (2.0 * R.n - 2.0);
+    out[1] = (double)(long long)v[0] / OBS_FIX;
+    out[2] = (double)(long long)v[1] / OBS_FIX;
+    out[3] = (double)(long long)v[3] / OBS_FIX / ((double)R.L * (double)R.L);
+    uint32_t bits = (uint32_t)v[4];
+    float mb;
+    memcpy(&mb, &bits, 4);
+    out[4] = mb;
+    out[5] = (double)v[5];
+    for (int t = 0; t < 8; t++) out[8 + t] = (double)v[8 + t];
+    CK(cudaStreamSynchronize(h->s));
+    return DPD_OK;
+}
+
+extern "C" int dpd_pair_hist(dpd_handle *h, int32_t r, int32_t ta, int32_t tb, double rmax, int32_t nbin,
+                             double *hist) {
+    TRY(ensure_replica(h, r));
+    if (!hist || nbin < 1 || nbin > 4096 || !(rmax > 0.0 && rmax <= 3.0))
+        return fail(DPD_E_ARG, "need 1 <= nbin <= 4096 and 0 < rmax <= 3");
+    CK(cudaMemsetAsync(h->b.hist, 0, nbin * sizeof(unsigned long long), h->s));
+    launch_pair_hist(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, ta, tb, (float)rmax, nbin, h->s);
+    CK(cudaGetLastError());
+    std::vector<unsigned long long> v(nbin);
+    CK(cudaMemcpyAsync(v.data(), h->b.hist, nbin * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    for (int k = 0; k < nbin; k++) hist[k] = (double)v[k];
+    return DPD_OK;
+}
+
+extern "C" int dpd_get_stream(const dpd_handle *h, void **stream) {
+    if (!h || !stream) return fail(DPD_E_ARG, "null argument");
+    *stream = (void *)h->s;
+    return DPD_OK;
+}
+
+extern "C" int dpd_kernels_per_step(const dpd_handle *h, int32_t *n_plain, int32_t *n_chem) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    // scan1, scan2, place, cellfix, permute, forces (+ the chemistry kernels)
+    if (n_plain) *n_plain = 6 + (h->any_chem ? chem_kernel_count() : 0);
+    if (n_chem) *n_chem = chem_kernel_count();
+    return DPD_OK;
+}

@@ -1,0 +1,143 @@
+// dpd_device.cuh -- device helpers shared by the kernels of libdpd.so.
+#pragma once
+#include "dpd_internal.h"
+
+// ---------------------------------------------------------------- counter-based RNGs
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), first output word.
+// Counter (c0, c1, c2, c3), key (k0, k1); constants from the paper.
+__device__ __forceinline__ uint32_t philox_w0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                              uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+    }
+    return c0;
+}
+
+// splitmix64 finaliser of the reference (cel/engine/oercel.c:124-128)
+__device__ __forceinline__ uint64_t mix13(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+// per-step noise key of the reference (oercel.c:131-133)
+__device__ __forceinline__ uint64_t step_seed(uint64_t seed, long long step) {
+    return mix13(mix13(seed ^ 0x5851f42d4c957f2dULL) ^ mix13((uint64_t)step + 0x632be59bd9b4e019ULL));
+}
+
+#define THETA_SCALE (3.4641016151377545870548926830117f / 4294967296.0f)  // sqrt(12) / 2^32
+
+// symmetric pair noise theta, uniform on [-sqrt3, sqrt3).
+// noise 0: Philox word 0 at counter (min gid, max gid, step), key = seed;
+// noise 1: the reference's mix13 pair hash (oercel.c:137-141), top 32 bits.
+struct NoiseKey {
+    uint32_t k0, k1, s0, s1;   // Philox key and step words
+    uint64_t sseed;            // mix13 per-step key
+    int mode;
+};
+
+__device__ __forceinline__ NoiseKey make_noise_key(const RepDev &R, long long step) {
+    NoiseKey k;
+    k.k0 = (uint32_t)R.seed;
+    k.k1 = (uint32_t)(R.seed >> 32);
+    k.s0 = (uint32_t)(unsigned long long)step;
+    k.s1 = (uint32_t)((unsigned long long)step >> 32);
+    k.mode = R.noise;
+    k.sseed = R.noise == 1 ? step_seed(R.seed, step) : 0ull;
+    return k;
+}
+
+__device__ __forceinline__ float pair_theta(const NoiseKey &k, uint32_t gi, uint32_t gj) {
+    const uint32_t lo = min(gi, gj), hi = max(gi, gj);
+    int32_t u;
+    if (k.mode == 1) {
+        const uint64_t key = ((uint64_t)lo << 32) | hi;
+        u = (int32_t)(uint32_t)(mix13((key * 0x9e3779b97f4a7c15ULL) ^ k.sseed) >> 32);
+    } else {
+        u = (int32_t)philox_w0(lo, hi, k.s0, k.s1, k.k0, k.k1);
+    }
+    return __fmul_rn(__int2float_rn(u), THETA_SCALE);
+}
+
+// keyed decision word for the chemistry: Philox word 0 at counter (gid, salt, step), key = seed
+__device__ __forceinline__ uint32_t decision_word(const RepDev &R, long long step, uint32_t salt, uint32_t gid) {
+    return philox_w0(gid, salt, (uint32_t)(unsigned long long)step, (uint32_t)((unsigned long long)step >> 32),
+                     (uint32_t)R.seed, (uint32_t)(R.seed >> 32));
+}
+
+// ---------------------------------------------------------------- fixed-point force sums
+
+// Each pair or bond term is rounded once to a multiple of 2^-32 and summed in
+// int64: the sum does not depend on the order of the terms, and the two
+// halves of a pair, computed with exactly negated operands, cancel exactly.
+__device__ __forceinline__ long long f2fix(float v) { return __float2ll_rn(__fmul_rn(v, 4294967296.0f)); }
+__device__ __forceinline__ float fix2f(long long a) { return __fmul_rn(__ll2float_rn(a), 2.3283064365386963e-10f); }
+
+// ---------------------------------------------------------------- cells and the integrator
+
+// cell of a position: the reference's cell_of_pos (oercel.c:779-786) with nsub = 1
+__device__ __forceinline__ int cell_xy(const RepDev &R, float x, float y, int &cx, int &cy) {
+    cx = (int)((double)x * R.icsx);
+    cy = (int)((double)y * R.icsy);
+    cx = cx >= R.ncx ? R.ncx - 1 : cx;
+    cy = cy >= R.ncy ? R.ncy - 1 : cy;
+    cx = cx < 0 ? 0 : cx;
+    cy = cy < 0 ? 0 : cy;
+    return cx * R.ncy + cy;
+}
+
+// Groot-Warren position update x + dt vh + dt^2 f, wrapped into [0, L)
+// (oercel.c:2314-2324); every rounding spelled out so that the copy in the
+// force kernel's next-key epilogue and the one in the permute kernel agree.
+__device__ __forceinline__ float advance1(float x, float vh, float f, float dt, float dt2, float L) {
+    const float dd = __fmaf_rn(dt2, f, __fmul_rn(dt, vh));
+    float xi = __fadd_rn(x, dd);
+    xi = xi < 0.0f ? __fadd_rn(xi, L) : xi;
+    xi = xi >= L ? __fsub_rn(xi, L) : xi;
+    return xi;
+}
+
+__device__ __forceinline__ float minimg(float d, float L, float h) {
+    return d > h ? __fsub_rn(d, L) : (d < -h ? __fadd_rn(d, L) : d);
+}
+
+// ---------------------------------------------------------------- warp helpers
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// warp-aggregated atomic count: every active lane gets its provisional rank
+// in the cell `key`; all 32 lanes of the warp must call this together.
+__device__ __forceinline__ uint32_t count_key(uint32_t *count, uint32_t key, bool active) {
+    const unsigned valid = __ballot_sync(0xffffffffu, active);
+    uint32_t rank = 0;
+    if (active) {
+        const unsigned peers = __match_any_sync(valid, key);
+        const int lane = (int)lane_id();
+        const int leader = __ffs(peers) - 1;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(count + key, (unsigned)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        rank = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
+    }
+    return rank;
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void raise_flag(DevStatus *st, unsigned f) { atomicOr(&st->flags, f); }

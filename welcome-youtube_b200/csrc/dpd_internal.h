@@ -1,0 +1,130 @@
+// dpd_internal.h -- device data layout shared by the kernels and the C ABI of libdpd.so.
+//
+// Layout in HBM (one set of arrays for all replicas, replica r owning the bead
+// range [b0, b0 + n) and the cell range [c0, c0 + ncell)):
+//   per bead, double-buffered (the cell sort permutes buffer cur -> 1 - cur):
+//     pos  float2  x, y in [0, L)
+//     vh   float2  stored half-step velocity (reference Sys.vx/vy)
+//     vt   float2  Groot-Warren predicted velocity (reference Sys.vtx/vty)
+//     f    float2  force of the current configuration
+//     tg   u32     type << 29 | gid  (gid < 2^29)
+//     link int2    prev, next slot of the bonded neighbours (-1 = none)
+//   per bead, single: key (cell of the next position), rank (provisional
+//     place in that cell), src (old slot of each new slot), dest (inverse),
+//     req/claim (chemistry requests)
+//   per cell: count (beads whose next position falls in the cell), cstart
+//     (exclusive scan of count; cstart of the packed cell C_total = N)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define DPD_MAXT 8
+#define TYPE_SHIFT 29
+#define GID_MASK 0x1FFFFFFFu
+
+#define BEAD_TPB 256
+#define CELL_TPB 256
+#define SCAN_TPB 1024
+#define SCAN_PER_THREAD 4
+#define SCAN_PER_BLOCK (SCAN_TPB * SCAN_PER_THREAD)
+
+// status flags raised by kernels (read back once per API call)
+#define DPD_F_OUTSIDE 0x1u      // a bead left [0, L) after integration
+#define DPD_F_NONFINITE 0x2u    // non-finite force or position
+#define DPD_F_EVENTS 0x4u       // event buffer overflow
+#define DPD_F_CHAIN 0x8u        // broken chain link found
+#define DPD_F_BIGCELL 0x10u     // a cell held more beads than the in-register sort handles (slow path used)
+
+struct RepDev {                 // constants of one replica, read by every kernel
+    float L, halfL;
+    int32_t ncx, ncy;
+    double icsx, icsy;          // ncx / L, ncy / L (cell index product in FP64, as the reference)
+    int32_t b0, n, c0, ncell;   // packed bead and cell offsets
+    float dt, dt2, cvt, hdt;    // dt, dt^2, (1/2 + lambda) dt, dt / 2 (FP32)
+    float gamma, sdt;           // gamma, sigma / sqrt(dt)
+    float kb, r0;
+    float a[DPD_MAXT * DPD_MAXT];
+    uint64_t seed;
+    int32_t noise;              // 0 Philox4x32-10, 1 reference mix13
+    int32_t chem, n_chem;
+    uint32_t thr_break, thr_grow, thr_bond;
+    float r2_grow, r2_bond;
+    int32_t n_t_min, max_chain;
+    int32_t pad;
+};
+
+struct Chunk {                  // one CTA's work: packed indices [begin, end) of replica rep
+    int32_t rep, begin, end, pad;
+};
+
+struct DevStatus {
+    unsigned int flags;
+    unsigned int nevents;       // events appended (may exceed the capacity)
+    unsigned int bigcell;       // largest cell population seen by the sort fix-up
+    unsigned int pad;
+};
+
+struct EventDev {
+    long long step;
+    int kind;
+    unsigned int gid, partner;
+    float x, y;
+    int replica;
+};
+
+#define OBS_N 16
+// per-replica observable accumulators (fixed point, integer atomics => deterministic)
+//   0: sum vx * 2^24   1: sum vy * 2^24   2: sum v^2 * 2^24   3: virial sum a w r * 2^24
+//   4: max bond length (float bits)   5: chain heads   8..15: type counts
+#define OBS_FIX 16777216.0
+
+struct Bufs {
+    float2 *pos[2], *vh[2], *vt[2], *f[2];
+    uint32_t *tg[2];
+    int2 *link[2];
+    uint32_t *key, *rank;
+    int32_t *src, *dest;
+    uint32_t *count;
+    int32_t *cstart;            // C + 1
+    int32_t *bsum;              // scan block totals
+    uint32_t *claim;            // per bead, 0xFFFFFFFF when unclaimed
+    int32_t *req;               // per bead chemistry request target (-1 none)
+    EventDev *events;
+    int32_t evcap;
+    DevStatus *status;
+    long long *step;            // step number of the forces being computed
+    unsigned long long *obs;    // OBS_N per replica
+    unsigned long long *hist;   // pair histogram scratch
+};
+
+// launchers (dpd_kernels.cu, dpd_chem.cu); every launcher enqueues on stream s
+enum PermuteMode { PERM_STEP = 0, PERM_PRIME = 1, PERM_SORT = 2 };
+
+void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool integrate,
+                 cudaStream_t s);
+void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s);
+void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s);
+void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s);
+void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s);
+void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
+                    cudaStream_t s);
+void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool pair, bool bond,
+                   bool next_keys, cudaStream_t s);
+void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
+void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
+void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
+                        cudaStream_t s);
+void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
+                      int tb, float rmax, int nbin, cudaStream_t s);
+void launch_pack(const Bufs &b, int cur, int b0, int n, const float *x, const float *y, const float *vx,
+                 const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
+                 const int32_t *next, cudaStream_t s);
+void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, float *vhx, float *vhy, float *vtx,
+                   float *vty, float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev, int32_t *next,
+                   cudaStream_t s);
+void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
+                         const float *fx, const float *fy, cudaStream_t s);
+int chem_kernel_count();
+void launch_chemistry(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
+void launch_chemistry_part(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int part,
+                           cudaStream_t s);

@@ -1,0 +1,660 @@
+// dpd_kernels.cu -- cell sort, integrator, pair + bond forces and observables (sm_100a).
+//
+// One step of the production path (dpd_step) is
+//   k_scan1, k_scan2   exclusive scan of the per-cell counts of the NEXT positions
+//   k_place            provisional slot of every bead: cstart[key] + rank
+//   k_cellfix          per cell: order its beads by old slot (stable sort), dest[]
+//   k_permute          gather the old slots into the new order AND apply the
+//                      Groot-Warren update (fused; oercel.c:2303-2334 + 832-933)
+//   [chemistry]        dpd_chem.cu
+//   k_forces           pair + bond forces of the new configuration; epilogue:
+//                      cell of the next position and its atomic count
+// so the bead state is read and written once per kernel and the sort keys for
+// step n+1 come out of the force kernel of step n.
+#include "dpd_device.cuh"
+
+// ---------------------------------------------------------------- keys (prime / build_cells)
+
+template <bool INTEG>
+__global__ void __launch_bounds__(BEAD_TPB) k_keys(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                   const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    const int i = c.begin + (int)threadIdx.x;
+    const bool act = i < c.end;
+    uint32_t key = 0;
+    if (act) {
+        float2 p = b.pos[cur][i];
+        if (INTEG) {
+            const float2 v = b.vh[cur][i], f = b.f[cur][i];
+            p.x = advance1(p.x, v.x, f.x, R.dt, R.dt2, R.L);
+            p.y = advance1(p.y, v.y, f.y, R.dt, R.dt2, R.L);
+        }
+        int cx, cy;
+        key = (uint32_t)(R.c0 + cell_xy(R, p.x, p.y, cx, cy));
+    }
+    const uint32_t rank = count_key(b.count, key, act);
+    if (act) {
+        b.key[i] = key;
+        b.rank[i] = rank;
+    }
+}
+
+// ---------------------------------------------------------------- scan of the cell counts
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *total) {
+    __shared__ int ws[SCAN_TPB / 32];
+    const int lane = (int)lane_id(), w = (int)threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < (SCAN_TPB / 32) ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < (SCAN_TPB / 32)) ws[lane] = s;
+    }
+    __syncthreads();
+    const int before = w > 0 ? ws[w - 1] : 0;
+    *total = ws[SCAN_TPB / 32 - 1];
+    return before + x - v;
+}
+
+// block-local exclusive scan; counts are consumed and zeroed for the next step
+__global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count, int32_t *__restrict__ cstart,
+                                                    int32_t *__restrict__ bsum, long long C,
+                                                    long long *__restrict__ step, int step_inc) {
+    const long long base = (long long)blockIdx.x * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
+    int v[SCAN_PER_THREAD];
+    int s = 0;
+    if (base + SCAN_PER_THREAD <= C) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(count + base);
+        v[0] = (int)q.x;
+        v[1] = (int)q.y;
+        v[2] = (int)q.z;
+        v[3] = (int)q.w;
+        *reinterpret_cast<uint4 *>(count + base) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; k++) {
+            v[k] = base + k < C ? (int)count[base + k] : 0;
+            if (base + k < C) count[base + k] = 0u;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; k++) s += v[k];
+    int total;
+    int ex = block_exclusive_scan(s, &total);
+    if (base + SCAN_PER_THREAD <= C) {
+        int4 o;
+        o.x = ex;
+        o.y = ex + v[0];
+        o.z = o.y + v[1];
+        o.w = o.z + v[2];
+        *reinterpret_cast<int4 *>(cstart + base) = o;
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; k++) {
+            if (base + k < C) cstart[base + k] = ex;
+            ex += v[k];
+        }
+    }
+    if (threadIdx.x == 0) {
+        bsum[blockIdx.x] = total;
+        if (step_inc && blockIdx.x == 0) *step += 1;
+    }
+}
+
+// add the totals of all earlier blocks; the last block writes cstart[C]
+__global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart, const int32_t *__restrict__ bsum,
+                                                    long long C, int nblocks) {
+    __shared__ int red[SCAN_TPB / 32];
+    int part = 0;
+    for (int k = (int)threadIdx.x; k < (int)blockIdx.x; k += SCAN_TPB) part += bsum[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if (lane_id() == 0) red[threadIdx.x >> 5] = part;
+    __syncthreads();
+    int prefix = 0;
+#pragma unroll
+    for (int w = 0; w < SCAN_TPB / 32; w++) prefix += red[w];
+    const long long base = (long long)blockIdx.x * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
+    if (prefix != 0) {
+        if (base + SCAN_PER_THREAD <= C) {
+            int4 o = *reinterpret_cast<const int4 *>(cstart + base);
+            o.x += prefix;
+            o.y += prefix;
+            o.z += prefix;
+            o.w += prefix;
+            *reinterpret_cast<int4 *>(cstart + base) = o;
+        } else {
+#pragma unroll
+            for (int k = 0; k < SCAN_PER_THREAD; k++)
+                if (base + k < C) cstart[base + k] += prefix;
+        }
+    }
+    if ((int)blockIdx.x == nblocks - 1 && threadIdx.x == 0) cstart[C] = prefix + bsum[nblocks - 1];
+}
+
+// ---------------------------------------------------------------- placement and the stable fix-up
+
+__global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int i = c.begin + (int)threadIdx.x;
+    if (i >= c.end) return;
+    b.src[b.cstart[b.key[i]] + (int)b.rank[i]] = i;
+}
+
+// bitonic sort of NP register values (static indexing only)
+template <int NP>
+__device__ __forceinline__ void bitonic(int (&v)[NP]) {
+#pragma unroll
+    for (int k = 2; k <= NP; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < NP; i++) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const int a = v[i], c = v[l];
+                    const bool sw = up ? (a > c) : (a < c);
+                    v[i] = sw ? c : a;
+                    v[l] = sw ? a : c;
+                }
+            }
+}
+
+template <int NP>
+__device__ __forceinline__ void fix_cell(int32_t *__restrict__ src, int32_t *__restrict__ dest, int s, int m) {
+    int v[NP];
+#pragma unroll
+    for (int k = 0; k < NP; k++) v[k] = k < m ? src[s + k] : 0x7fffffff;
+    bitonic<NP>(v);
+#pragma unroll
+    for (int k = 0; k < NP; k++)
+        if (k < m) {
+            src[s + k] = v[k];
+            dest[v[k]] = s + k;
+        }
+}
+
+// Beads that land in one cell keep their old slot order (the reference's
+// stable counting sort, oercel.c:832-933): the atomics gave each bead some
+// place in its cell; here every cell orders its beads by old slot.
+__global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int cell = c.begin + (int)threadIdx.x;
+    if (cell >= c.end) return;
+    const int s = b.cstart[cell], m = b.cstart[cell + 1] - s;
+    if (m <= 1) {
+        if (m == 1) b.dest[b.src[s]] = s;
+        return;
+    }
+    if (m <= 8) {
+        fix_cell<8>(b.src, b.dest, s, m);
+    } else if (m <= 16) {
+        fix_cell<16>(b.src, b.dest, s, m);
+    } else {
+        // crowded cell: in-place insertion sort in global memory
+        atomicMax(&b.status->bigcell, (unsigned)m);
+        for (int k = 1; k < m; k++) {
+            const int t = b.src[s + k];
+            int q = k - 1;
+            while (q >= 0 && b.src[s + q] > t) {
+                b.src[s + q + 1] = b.src[s + q];
+                q--;
+            }
+            b.src[s + q + 1] = t;
+        }
+        for (int k = 0; k < m; k++) b.dest[b.src[s + k]] = s + k;
+    }
+}
+
+// ---------------------------------------------------------------- permute (+ integrate)
+
+// new slot d takes old bead src[d].  PERM_STEP applies the Groot-Warren update
+// on the way (x += dt vh + dt^2 f; vt = vh + (1/2 + lambda) dt f; vh += dt f);
+// PERM_PRIME takes the loaded velocity as the full velocity (vt = v);
+// PERM_SORT moves everything unchanged.
+template <int MODE>
+__global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                      const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const int nxt = cur ^ 1;
+    const int i = b.src[d];
+    float2 p = b.pos[cur][i], vh = b.vh[cur][i];
+    const uint32_t tg = b.tg[cur][i];
+    const int2 lk = b.link[cur][i];
+    if (MODE == PERM_STEP) {
+        const RepDev &R = reps[c.rep];
+        const float2 f = b.f[cur][i];
+        const float2 q = make_float2(advance1(p.x, vh.x, f.x, R.dt, R.dt2, R.L),
+                                     advance1(p.y, vh.y, f.y, R.dt, R.dt2, R.L));
+        if (!(q.x >= 0.0f && q.x < R.L && q.y >= 0.0f && q.y < R.L)) raise_flag(b.status, DPD_F_OUTSIDE);
+        b.vt[nxt][d] = make_float2(__fmaf_rn(R.cvt, f.x, vh.x), __fmaf_rn(R.cvt, f.y, vh.y));
+        vh = make_float2(__fmaf_rn(R.dt, f.x, vh.x), __fmaf_rn(R.dt, f.y, vh.y));
+        p = q;
+    } else if (MODE == PERM_PRIME) {
+        b.vt[nxt][d] = vh;
+    } else {
+        b.vt[nxt][d] = b.vt[cur][i];
+        b.f[nxt][d] = b.f[cur][i];
+    }
+    b.pos[nxt][d] = p;
+    b.vh[nxt][d] = vh;
+    b.tg[nxt][d] = tg;
+    b.link[nxt][d] = make_int2(lk.x >= 0 ? b.dest[lk.x] : -1, lk.y >= 0 ? b.dest[lk.y] : -1);
+}
+
+// ---------------------------------------------------------------- pair + bond forces
+
+// Per bead d: F_d = sum_j w [a_ij - gamma w (rhat . vt_ij) + sigma theta_ij / sqrt(dt)] rhat
+// over the 3x3 neighbour cells (w = 1 - r, r < 1; oercel.c:970-981) plus the
+// harmonic bonds to prev/next (oercel.c:1272-1308).  Every pair is evaluated
+// by both of its beads with exactly negated operands and summed in fixed point,
+// so F_ij = -F_ji and sum F = 0 hold exactly and the result does not depend on
+// the order of the loops.  NEXTKEY: also the cell of x + dt vh + dt^2 F and
+// its count, i.e. the first half of the next step's sort.
+template <bool PAIR, bool BOND, bool NEXTKEY>
+__global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                     const Chunk *__restrict__ ch) {
+    __shared__ float a_sh[DPD_MAXT * DPD_MAXT];
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    if (threadIdx.x < DPD_MAXT * DPD_MAXT) a_sh[threadIdx.x] = R.a[threadIdx.x];
+    __syncthreads();
+    const int d = c.begin + (int)threadIdx.x;
+    const bool act = d < c.end;
+    const float2 *__restrict__ pos = b.pos[cur];
+    uint32_t key = 0;
+    float mb = 0.0f;
+    if (act) {
+        long long ax = 0, ay = 0;
+        const float2 pi = pos[d];
+        const float L = R.L;
+        if (PAIR) {
+            const float2 *__restrict__ vt = b.vt[cur];
+            const uint32_t *__restrict__ tg = b.tg[cur];
+            const float2 vi = vt[d];
+            const uint32_t tgi = tg[d];
+            const uint32_t gi = tgi & GID_MASK;
+            const float *arow = a_sh + (tgi >> TYPE_SHIFT) * DPD_MAXT;
+            const NoiseKey nk = make_noise_key(R, *b.step);
+            const float gam = R.gamma, sdt = R.sdt;
+            const int ncx = R.ncx, ncy = R.ncy;
+            const int32_t *__restrict__ cs = b.cstart + R.c0;
+            int cx, cy;
+            cell_xy(R, pi.x, pi.y, cx, cy);
+#pragma unroll 1
+            for (int ox = -1; ox <= 1; ox++) {
+                int nx = cx + ox;
+                float sx = 0.0f;
+                if (nx < 0) {
+                    nx += ncx;
+                    sx = L;
+                } else if (nx >= ncx) {
+                    nx -= ncx;
+                    sx = -L;
+                }
+                const int col = nx * ncy;
+                // rows cy-1 .. cy+1 of this column: one or two contiguous slot ranges
+                int s0, e0, s1 = 0, e1 = 0;
+                float sy0 = 0.0f, sy1 = 0.0f;
+                if (cy >= 1 && cy + 1 < ncy) {
+                    s0 = cs[col + cy - 1];
+                    e0 = cs[col + cy + 2];
+                } else if (cy == 0) {
+                    s0 = cs[col + ncy - 1];
+                    e0 = cs[col + ncy];
+                    sy0 = L;
+                    s1 = cs[col];
+                    e1 = cs[col + 2];
+                } else {
+                    s0 = cs[col + cy - 1];
+                    e0 = cs[col + ncy];
+                    s1 = cs[col];
+                    e1 = cs[col + 1];
+                    sy1 = -L;
+                }
+#pragma unroll 1
+                for (int seg = 0; seg < 2; seg++) {
+                    const int js = seg ? s1 : s0, je = seg ? e1 : e0;
+                    const float sy = seg ? sy1 : sy0;
+#pragma unroll 1
+                    for (int j = js; j < je; j++) {
+                        const float2 pj = pos[j];
+                        const float dx = __fadd_rn(__fsub_rn(pi.x, pj.x), sx);
+                        const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
+                        const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                        if (r2 < 1.0f && r2 > 1e-24f && j != d) {
+                            const float2 vj = vt[j];
+                            const uint32_t tgj = tg[j];
+                            const float r = __fsqrt_rn(r2);
+                            const float ir = __frcp_rn(r);
+                            const float w = __fsub_rn(1.0f, r);
+                            const float dvx = __fsub_rn(vi.x, vj.x), dvy = __fsub_rn(vi.y, vj.y);
+                            const float rv = __fmul_rn(__fmaf_rn(dx, dvx, __fmul_rn(dy, dvy)), ir);
+                            const float th = pair_theta(nk, gi, tgj & GID_MASK);
+                            const float inner = __fmaf_rn(sdt, th, __fmaf_rn(-__fmul_rn(gam, w), rv,
+                                                                            arow[tgj >> TYPE_SHIFT]));
+                            const float fm = __fmul_rn(__fmul_rn(w, inner), ir);
+                            ax += f2fix(__fmul_rn(fm, dx));
+                            ay += f2fix(__fmul_rn(fm, dy));
+                        }
+                    }
+                }
+            }
+        }
+        if (BOND) {
+            const int2 lk = b.link[cur][d];
+            const float h = R.halfL, kb = R.kb, r0 = R.r0;
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int j = q ? lk.y : lk.x;
+                if (j < 0) continue;
+                const float2 pj = pos[j];
+                const float dx = minimg(__fsub_rn(pj.x, pi.x), L, h), dy = minimg(__fsub_rn(pj.y, pi.y), L, h);
+                const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+                mb = fmaxf(mb, r);
+                const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
+                ax += f2fix(__fmul_rn(fb, dx));
+                ay += f2fix(__fmul_rn(fb, dy));
+            }
+        }
+        const float2 fs = make_float2(fix2f(ax), fix2f(ay));
+        if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);
+        b.f[cur][d] = fs;
+        if (NEXTKEY) {
+            const float2 v = b.vh[cur][d];
+            int cx, cy;
+            key = (uint32_t)(R.c0 + cell_xy(R, advance1(pi.x, v.x, fs.x, R.dt, R.dt2, L),
+                                            advance1(pi.y, v.y, fs.y, R.dt, R.dt2, L), cx, cy));
+        }
+    }
+    if (BOND) {
+        // running max bond length of the replica (obs slot 4, float bits; r >= 0)
+        const unsigned mbb = __reduce_max_sync(0xffffffffu, __float_as_uint(mb));
+        if (lane_id() == 0 && mbb != 0u) atomicMax(b.obs + (size_t)c.rep * OBS_N + 4, (unsigned long long)mbb);
+    }
+    if (NEXTKEY) {
+        const uint32_t rank = count_key(b.count, key, act);
+        if (act) {
+            b.key[d] = key;
+            b.rank[d] = rank;
+        }
+    }
+}
+
+// vh = v - dt/2 f after the first force evaluation (oercel.c:2207-2211)
+__global__ void __launch_bounds__(BEAD_TPB) k_halfkick(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                       const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const float h = reps[c.rep].hdt;
+    const float2 v = b.vh[cur][d], f = b.f[cur][d];
+    b.vh[cur][d] = make_float2(__fmaf_rn(-h, f.x, v.x), __fmaf_rn(-h, f.y, v.y));
+}
+
+// the Groot-Warren update in place, no sort (phase entry point dpd_integrate)
+__global__ void __launch_bounds__(BEAD_TPB) k_integrate(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                        const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const RepDev &R = reps[c.rep];
+    const float2 p = b.pos[cur][d], vh = b.vh[cur][d], f = b.f[cur][d];
+    const float2 q = make_float2(advance1(p.x, vh.x, f.x, R.dt, R.dt2, R.L), advance1(p.y, vh.y, f.y, R.dt, R.dt2, R.L));
+    if (!(q.x >= 0.0f && q.x < R.L && q.y >= 0.0f && q.y < R.L)) raise_flag(b.status, DPD_F_OUTSIDE);
+    b.pos[cur][d] = q;
+    b.vt[cur][d] = make_float2(__fmaf_rn(R.cvt, f.x, vh.x), __fmaf_rn(R.cvt, f.y, vh.y));
+    b.vh[cur][d] = make_float2(__fmaf_rn(R.dt, f.x, vh.x), __fmaf_rn(R.dt, f.y, vh.y));
+}
+
+// ---------------------------------------------------------------- observables
+
+// per-bead sums (momentum, kinetic energy, type counts, chain heads) and the
+// conservative virial over each unordered pair once; fixed-point integer
+// atomics make the result independent of the launch shape.
+__global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                          const Chunk *__restrict__ ch, int rep_index) {
+    const Chunk c = ch[blockIdx.x];
+    if (c.rep != rep_index) return;
+    const RepDev &R = reps[c.rep];
+    const int d = c.begin + (int)threadIdx.x;
+    const bool act = d < c.end;
+    long long sx = 0, sy = 0, s2 = 0, vir = 0, heads = 0;
+    int ty = -1;
+    if (act) {
+        const float2 v = b.vh[cur][d], f = b.f[cur][d];
+        const double vx = (double)v.x + (double)R.hdt * (double)f.x, vy = (double)v.y + (double)R.hdt * (double)f.y;
+        sx = __double2ll_rn(vx * OBS_FIX);
+        sy = __double2ll_rn(vy * OBS_FIX);
+        s2 = __double2ll_rn((vx * vx + vy * vy) * OBS_FIX);
+        const uint32_t tgi = b.tg[cur][d];
+        ty = (int)(tgi >> TYPE_SHIFT);
+        const int2 lk = b.link[cur][d];
+        heads = (lk.x < 0 && lk.y >= 0) ? 1 : 0;
+        // virial: pairs (d, j) with j > d inside the cutoff
+        const float2 *__restrict__ pos = b.pos[cur];
+        const float2 pi = pos[d];
+        const int ncx = R.ncx, ncy = R.ncy;
+        const int32_t *cs = b.cstart + R.c0;
+        int cx, cy;
+        cell_xy(R, pi.x, pi.y, cx, cy);
+        double accv = 0.0;
+        for (int ox = -1; ox <= 1; ox++)
+            for (int oy = -1; oy <= 1; oy++) {
+                const int nx = (cx + ox + ncx) % ncx, ny = (cy + oy + ncy) % ncy;
+                const int cc = nx * ncy + ny;
+                for (int j = cs[cc]; j < cs[cc + 1]; j++) {
+                    if (j <= d) continue;
+                    const float2 pj = pos[j];
+                    const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
+                    const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
+                    const double r2 = dx * dx + dy * dy;
+                    if (!(r2 < 1.0 && r2 > 1e-24)) continue;
+                    const double r = sqrt(r2);
+                    accv += (double)R.a[ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT)] * (1.0 - r) * r;
+                }
+            }
+        vir = __double2ll_rn(accv * OBS_FIX);
+    }
+    unsigned long long *o = b.obs + (size_t)rep_index * OBS_N;
+    sx = warp_sum_ll(sx);
+    sy = warp_sum_ll(sy);
+    s2 = warp_sum_ll(s2);
+    vir = warp_sum_ll(vir);
+    heads = warp_sum_ll(heads);
+    if (lane_id() == 0) {
+        atomicAdd(o + 0, (unsigned long long)sx);
+        atomicAdd(o + 1, (unsigned long long)sy);
+        atomicAdd(o + 2, (unsigned long long)s2);
+        atomicAdd(o + 3, (unsigned long long)vir);
+        atomicAdd(o + 5, (unsigned long long)heads);
+    }
+    for (int t = 0; t < DPD_MAXT; t++) {
+        const unsigned m = __ballot_sync(0xffffffffu, ty == t);
+        if (lane_id() == 0 && m) atomicAdd(o + 8 + t, (unsigned long long)__popc(m));
+    }
+}
+
+// distances between types ta and tb within rmax (<= 3 cells), each unordered pair once
+__global__ void __launch_bounds__(BEAD_TPB) k_pair_hist(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                        const Chunk *__restrict__ ch, int rep_index, int ta, int tb,
+                                                        float rmax, int nbin) {
+    const Chunk c = ch[blockIdx.x];
+    if (c.rep != rep_index) return;
+    const RepDev &R = reps[c.rep];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const uint32_t ti = b.tg[cur][d] >> TYPE_SHIFT;
+    if ((int)ti != ta && (int)ti != tb) return;
+    const float2 *__restrict__ pos = b.pos[cur];
+    const float2 pi = pos[d];
+    const int ncx = R.ncx, ncy = R.ncy;
+    const int rc = (int)ceil((double)rmax * R.icsx);
+    const int rx = min(rc, (ncx - 1) / 2), ry = min(rc, (ncy - 1) / 2);
+    const int32_t *cs = b.cstart + R.c0;
+    int cx, cy;
+    cell_xy(R, pi.x, pi.y, cx, cy);
+    for (int ox = -rx; ox <= rx; ox++)
+        for (int oy = -ry; oy <= ry; oy++) {
+            const int nx = (cx + ox + ncx) % ncx, ny = (cy + oy + ncy) % ncy;
+            const int cc = nx * ncy + ny;
+            for (int j = cs[cc]; j < cs[cc + 1]; j++) {
+                if (j <= d) continue;
+                const uint32_t tj = b.tg[cur][j] >> TYPE_SHIFT;
+                if (!(((int)ti == ta && (int)tj == tb) || ((int)ti == tb && (int)tj == ta))) continue;
+                const float2 pj = pos[j];
+                const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
+                const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
+                const double r = sqrt(dx * dx + dy * dy);
+                if (r >= (double)rmax) continue;
+                const int bin = (int)(r / (double)rmax * nbin);
+                if (bin >= 0 && bin < nbin) atomicAdd(b.hist + bin, 1ull);
+            }
+        }
+}
+
+// ---------------------------------------------------------------- state in/out
+
+__global__ void k_pack(Bufs b, int cur, int b0, int n, const float *x, const float *y, const float *vx, const float *vy,
+                       const uint8_t *type, const uint32_t *gid, const int32_t *prev, const int32_t *next) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int d = b0 + k;
+    b.pos[cur][d] = make_float2(x[k], y[k]);
+    b.vh[cur][d] = make_float2(vx[k], vy[k]);
+    b.vt[cur][d] = make_float2(vx[k], vy[k]);
+    b.f[cur][d] = make_float2(0.0f, 0.0f);
+    const uint32_t g = gid ? gid[k] : (uint32_t)k;
+    b.tg[cur][d] = ((uint32_t)type[k] << TYPE_SHIFT) | (g & GID_MASK);
+    const int p = prev ? prev[k] : -1, q = next ? next[k] : -1;
+    b.link[cur][d] = make_int2(p >= 0 ? b0 + p : -1, q >= 0 ? b0 + q : -1);
+}
+
+__global__ void k_unpack(Bufs b, int cur, int b0, int n, float *x, float *y, float *vhx, float *vhy, float *vtx,
+                         float *vty, float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev,
+                         int32_t *next) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int d = b0 + k;
+    const float2 p = b.pos[cur][d], vh = b.vh[cur][d], vt = b.vt[cur][d], f = b.f[cur][d];
+    if (x) x[k] = p.x;
+    if (y) y[k] = p.y;
+    if (vhx) vhx[k] = vh.x;
+    if (vhy) vhy[k] = vh.y;
+    if (vtx) vtx[k] = vt.x;
+    if (vty) vty[k] = vt.y;
+    if (fx) fx[k] = f.x;
+    if (fy) fy[k] = f.y;
+    const uint32_t tg = b.tg[cur][d];
+    if (type) type[k] = (uint8_t)(tg >> TYPE_SHIFT);
+    if (gid) gid[k] = tg & GID_MASK;
+    const int2 lk = b.link[cur][d];
+    if (prev) prev[k] = lk.x >= 0 ? lk.x - b0 : -1;
+    if (next) next[k] = lk.y >= 0 ? lk.y - b0 : -1;
+}
+
+__global__ void k_set_dynamics(Bufs b, int cur, int b0, int n, const float *vhx, const float *vhy, const float *fx,
+                               const float *fy) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int d = b0 + k;
+    float2 v = b.vh[cur][d], f = b.f[cur][d];
+    if (vhx) v.x = vhx[k];
+    if (vhy) v.y = vhy[k];
+    if (fx) f.x = fx[k];
+    if (fy) f.y = fy[k];
+    b.vh[cur][d] = v;
+    b.f[cur][d] = f;
+}
+
+// ---------------------------------------------------------------- launchers
+
+void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool integrate,
+                 cudaStream_t s) {
+    if (integrate) k_keys<true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else k_keys<false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s) {
+    const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
+    if (part == 1) k_scan1<<<nb, SCAN_TPB, 0, s>>>(b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0);
+    else k_scan2<<<nb, SCAN_TPB, 0, s>>>(b.cstart, b.bsum, (long long)C, nb);
+}
+
+void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
+    launch_scan_part(b, C, step_inc, 1, s);
+    launch_scan_part(b, C, step_inc, 2, s);
+}
+
+void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s) {
+    k_place<<<nbch, BEAD_TPB, 0, s>>>(b, bch);
+}
+
+void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s) {
+    k_cellfix<<<ncch, CELL_TPB, 0, s>>>(b, cch);
+}
+
+void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
+                    cudaStream_t s) {
+    if (mode == PERM_STEP) k_permute<PERM_STEP><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else if (mode == PERM_PRIME) k_permute<PERM_PRIME><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else k_permute<PERM_SORT><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool pair, bool bond,
+                   bool next_keys, cudaStream_t s) {
+    if (pair && bond && next_keys) k_forces<true, true, true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else if (pair && bond) k_forces<true, true, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else if (pair) k_forces<true, false, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else k_forces<false, true, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
+    k_halfkick<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
+    k_integrate<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
+                        cudaStream_t s) {
+    k_observables<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
+}
+
+void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
+                      int tb, float rmax, int nbin, cudaStream_t s) {
+    k_pair_hist<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, ta, tb, rmax, nbin);
+}
+
+void launch_pack(const Bufs &b, int cur, int b0, int n, const float *x, const float *y, const float *vx,
+                 const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
+                 const int32_t *next, cudaStream_t s) {
+    k_pack<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, x, y, vx, vy, type, gid, prev, next);
+}
+
+void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, float *vhx, float *vhy, float *vtx,
+                   float *vty, float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev, int32_t *next,
+                   cudaStream_t s) {
+    k_unpack<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, x, y, vhx, vhy, vtx, vty, fx, fy, type, gid, prev, next);
+}
+
+void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
+                         const float *fx, const float *fy, cudaStream_t s) {
+    k_set_dynamics<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, vhx, vhy, fx, fy);
+}

@@ -1,0 +1,142 @@
+"""ctypes binding of libdpd.so (include/dpd.h).
+
+The library is the product: there is no Python or CPU implementation of the
+step behind this module.  Loading fails loudly when libdpd.so is missing, and
+every call that returns a negative code raises DpdError with the library's
+message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdpd.so")
+MAXT = 8
+
+ERRORS = {
+    -1: "DPD_E_ARG", -2: "DPD_E_CUDA", -3: "DPD_E_SORT_OVERFLOW", -4: "DPD_E_CHAIN",
+    -5: "DPD_E_EVENT_OVERFLOW", -6: "DPD_E_TIMEOUT", -7: "DPD_E_STATE", -8: "DPD_E_NOMEM",
+}
+
+
+class DpdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class DpdParams(C.Structure):
+    _fields_ = [
+        ("L", C.c_double), ("dt", C.c_double), ("lam", C.c_double), ("gamma", C.c_double), ("kT", C.c_double),
+        ("a", C.c_double * (MAXT * MAXT)), ("k_bond", C.c_double), ("r0", C.c_double), ("seed", C.c_uint64),
+        ("noise", C.c_int32), ("chem", C.c_int32), ("n_chem", C.c_int32), ("n_t_min", C.c_int32),
+        ("max_chain", C.c_int32), ("pad", C.c_int32),
+        ("p_break", C.c_double), ("p_grow", C.c_double), ("p_bond", C.c_double),
+        ("r_grow", C.c_double), ("r_bond", C.c_double),
+    ]
+
+
+class DpdEvent(C.Structure):
+    _fields_ = [("step", C.c_int64), ("kind", C.c_int32), ("gid", C.c_uint32), ("partner", C.c_uint32),
+                ("x", C.c_float), ("y", C.c_float), ("replica", C.c_int32)]
+
+
+EXPORTS = [
+    "dpd_last_error", "dpd_version", "dpd_params_default", "dpd_create", "dpd_destroy", "dpd_sizes",
+    "dpd_set_state", "dpd_get_state", "dpd_set_dynamics", "dpd_prime", "dpd_resume", "dpd_get_step",
+    "dpd_set_step", "dpd_step", "dpd_init_soup", "dpd_build_cells", "dpd_get_cells", "dpd_forces",
+    "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events",
+    "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
+    "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step",
+]
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libdpd.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if path == LIB_PATH:
+        try:
+            import importlib.util
+            spec = importlib.util.spec_from_file_location("_dpd_build", os.path.join(os.path.dirname(HERE),
+                                                                                       "build.py"))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            if mod.stale() and os.path.exists("/usr/local/cuda/bin/nvcc"):
+                mod.build()
+        except FileNotFoundError:
+            pass
+    if not os.path.exists(path):
+        raise OSError(f"libdpd.so not found at {path}: build it with welcome-youtube_b200/build.py")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    fp = C.c_void_p  # data pointers are passed as integers (host or device)
+    i32, i64, u64, dbl = C.c_int32, C.c_int64, C.c_uint64, C.c_double
+    sig = {
+        "dpd_last_error": ([], C.c_char_p),
+        "dpd_version": ([], C.c_char_p),
+        "dpd_params_default": ([C.POINTER(DpdParams)], C.c_int),
+        "dpd_create": ([C.POINTER(DpdParams), i32, C.POINTER(C.c_int32), C.POINTER(vp)], C.c_int),
+        "dpd_destroy": ([vp], C.c_int),
+        "dpd_sizes": ([vp, i32, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "dpd_set_state": ([vp, i32] + [fp] * 8, C.c_int),
+        "dpd_get_state": ([vp, i32] + [fp] * 12, C.c_int),
+        "dpd_set_dynamics": ([vp, i32] + [fp] * 4, C.c_int),
+        "dpd_prime": ([vp], C.c_int),
+        "dpd_resume": ([vp], C.c_int),
+        "dpd_get_step": ([vp, C.POINTER(C.c_int64)], C.c_int),
+        "dpd_set_step": ([vp, i64], C.c_int),
+        "dpd_step": ([vp, i64], C.c_int),
+        "dpd_init_soup": ([dbl, i32, u64, dbl, dbl, i32, i32, dbl, dbl, dbl, dbl] + [fp] * 7
+                          + [C.POINTER(C.c_int32)], C.c_int),
+        "dpd_build_cells": ([vp], C.c_int),
+        "dpd_get_cells": ([vp, i32, fp], C.c_int),
+        "dpd_forces": ([vp, i64], C.c_int),
+        "dpd_pair_forces": ([vp, i32, i64, fp, fp], C.c_int),
+        "dpd_bond_forces": ([vp, i32, fp, fp, C.POINTER(C.c_float)], C.c_int),
+        "dpd_integrate": ([vp], C.c_int),
+        "dpd_chemistry": ([vp, i64], C.c_int),
+        "dpd_get_events": ([vp, C.POINTER(DpdEvent), i32, C.POINTER(C.c_int32)], C.c_int),
+        "dpd_observables": ([vp, i32, fp], C.c_int),
+        "dpd_pair_hist": ([vp, i32, i32, i32, dbl, i32, fp], C.c_int),
+        "dpd_get_stream": ([vp, C.POINTER(vp)], C.c_int),
+        "dpd_kernels_per_step": ([vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+        "dpd_step_async": ([vp, i64], C.c_int),
+        "dpd_sync": ([vp], C.c_int),
+        "dpd_set_graph_steps": ([vp, i32], C.c_int),
+        "dpd_profile_step": ([vp, C.POINTER(C.c_float), i32, C.POINTER(C.c_int32)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def check(rc: int):
+    if rc != 0:
+        raise DpdError(rc, load().dpd_last_error().decode(errors="replace"))
+    return rc
+
+
+def ptr(a) -> int | None:
+    """data pointer of a numpy array or torch tensor (None passes NULL)"""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")

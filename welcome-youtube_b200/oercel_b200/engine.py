@@ -1,0 +1,216 @@
+"""In-process engine: the reference engine's step / parameter / state interface
+over libdpd.so.
+
+The reference engine (cel/engine/oercel.c) owns its state in one process and
+advances it with the loop of main() (:2300-2361).  Engine does the same on
+the GPU: one handle holds one or more replicas (independent boxes packed into
+one set of device arrays) and every method is one C-ABI call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import DpdEvent, check, load, ptr
+from .params import Params
+
+EVENT_KINDS = ("grow", "brk", "bond")
+
+
+def make_soup(L, N, seed, *, kT=1.0, r0=0.5, nH=1, nT=3, f_lip=0.10, f_Ka=0.0, f_Kb=0.0, c_N=0.12):
+    """The reference's random soup (same draws as init_soup/set_velocities) from
+    libdpd's host routine; float64 arrays in gid order."""
+    lib = load()
+    x, y, vx, vy = (np.empty(N, np.float64) for _ in range(4))
+    t = np.empty(N, np.uint8)
+    pv = np.empty(N, np.int32)
+    nx = np.empty(N, np.int32)
+    nl = C.c_int32(0)
+    check(lib.dpd_init_soup(float(L), int(N), int(seed) & 0xFFFFFFFFFFFFFFFF, float(kT), float(r0), int(nH),
+                            int(nT), float(f_lip), float(f_Ka), float(f_Kb), float(c_N), ptr(x), ptr(y), ptr(vx),
+                            ptr(vy), ptr(t), ptr(pv), ptr(nx), C.byref(nl)))
+    return dict(x=x, y=y, vx=vx, vy=vy, type=t, prev=pv, next=nx, n_lipid_beads=nl.value)
+
+
+def soup_for(p: Params, seed=None):
+    """soup of a parameter set (positions rounded to FP32 inside [0, L))"""
+    s = make_soup(np.float32(p.L), p.n_beads(), p.seed if seed is None else seed, kT=p.kT, r0=p.r0,
+                  nH=p.lip_nH, nT=p.lip_nT, f_lip=p.f_lip, f_Ka=p.f_Ka, f_Kb=p.f_Kb, c_N=p.c_N)
+    L = np.float32(p.L)
+    for k in ("x", "y"):
+        v = s[k].astype(np.float32)
+        v[v >= L] = np.float32(0.0)   # a coordinate that rounds up to L wraps to 0
+        s[k] = v
+    s["vx"] = s["vx"].astype(np.float32)
+    s["vy"] = s["vy"].astype(np.float32)
+    return s
+
+
+class Engine:
+    """GPU simulation of one or more replicas.
+
+    params: a Params (one replica) or a list of Params (one per replica).
+    n_beads: bead count per replica (default round(rho L^2))."""
+
+    def __init__(self, params, n_beads=None):
+        self.lib = load()
+        plist = list(params) if isinstance(params, (list, tuple)) else [params]
+        self.params = plist
+        self.nrep = len(plist)
+        if n_beads is None:
+            n_beads = [p.n_beads() for p in plist]
+        n_beads = [int(n) for n in (n_beads if hasattr(n_beads, "__len__") else [n_beads])]
+        structs = (_capi.DpdParams * self.nrep)(*[p.to_struct() for p in plist])
+        nb = (C.c_int32 * self.nrep)(*n_beads)
+        self.h = C.c_void_p()
+        check(self.lib.dpd_create(structs, self.nrep, nb, C.byref(self.h)))
+        self.n_beads = n_beads
+
+    # ---------------------------------------------------------------- lifetime
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.dpd_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------------------------------------------------------- state
+    def set_state(self, replica, x, y, vx, vy, type, gid=None, prev=None, next=None):
+        f32 = lambda a: np.ascontiguousarray(a, np.float32) if isinstance(a, np.ndarray) else a
+        args = [f32(x), f32(y), f32(vx), f32(vy)]
+        t = np.ascontiguousarray(type, np.uint8) if isinstance(type, np.ndarray) else type
+        g = np.ascontiguousarray(gid, np.uint32) if isinstance(gid, np.ndarray) else gid
+        pv = np.ascontiguousarray(prev, np.int32) if isinstance(prev, np.ndarray) else prev
+        nx = np.ascontiguousarray(next, np.int32) if isinstance(next, np.ndarray) else next
+        check(self.lib.dpd_set_state(self.h, replica, *[ptr(a) for a in args], ptr(t), ptr(g), ptr(pv), ptr(nx)))
+
+    def load_soup(self, replica=0, seed=None):
+        s = soup_for(self.params[replica], seed)
+        self.set_state(replica, s["x"], s["y"], s["vx"], s["vy"], s["type"], None, s["prev"], s["next"])
+        return s
+
+    def state(self, replica=0):
+        n = self.n_beads[replica]
+        out = {k: np.empty(n, np.float32) for k in ("x", "y", "vhx", "vhy", "vtx", "vty", "fx", "fy")}
+        out["type"] = np.empty(n, np.uint8)
+        out["gid"] = np.empty(n, np.uint32)
+        out["prev"] = np.empty(n, np.int32)
+        out["next"] = np.empty(n, np.int32)
+        o = out
+        check(self.lib.dpd_get_state(self.h, replica, ptr(o["x"]), ptr(o["y"]), ptr(o["vhx"]), ptr(o["vhy"]),
+                                     ptr(o["vtx"]), ptr(o["vty"]), ptr(o["fx"]), ptr(o["fy"]), ptr(o["type"]),
+                                     ptr(o["gid"]), ptr(o["prev"]), ptr(o["next"])))
+        return out
+
+    def set_dynamics(self, replica, vhx=None, vhy=None, fx=None, fy=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        a = [c(vhx), c(vhy), c(fx), c(fy)]
+        check(self.lib.dpd_set_dynamics(self.h, replica, *[ptr(v) for v in a]))
+
+    def cells(self, replica=0):
+        nc = C.c_int32()
+        check(self.lib.dpd_sizes(self.h, replica, None, None, C.byref(nc)))
+        cs = np.empty(nc.value + 1, np.int32)
+        check(self.lib.dpd_get_cells(self.h, replica, ptr(cs)))
+        return cs
+
+    # ---------------------------------------------------------------- stepping
+    def prime(self):
+        check(self.lib.dpd_prime(self.h))
+
+    def resume(self):
+        check(self.lib.dpd_resume(self.h))
+
+    def step(self, n=1):
+        check(self.lib.dpd_step(self.h, int(n)))
+
+    def step_async(self, n=1):
+        check(self.lib.dpd_step_async(self.h, int(n)))
+
+    def sync(self):
+        check(self.lib.dpd_sync(self.h))
+
+    def set_graph_steps(self, n):
+        check(self.lib.dpd_set_graph_steps(self.h, int(n)))
+
+    def profile_step(self):
+        """device time (ms) of each kernel of one real step, in launch order"""
+        ms = (C.c_float * 32)()
+        n = C.c_int32()
+        check(self.lib.dpd_profile_step(self.h, ms, 32, C.byref(n)))
+        return [ms[k] for k in range(n.value)]
+
+    @property
+    def step_no(self):
+        s = C.c_int64()
+        check(self.lib.dpd_get_step(self.h, C.byref(s)))
+        return s.value
+
+    def set_step(self, s):
+        check(self.lib.dpd_set_step(self.h, int(s)))
+
+    # ---------------------------------------------------------------- phases
+    def build_cells(self):
+        check(self.lib.dpd_build_cells(self.h))
+
+    def forces(self, step):
+        check(self.lib.dpd_forces(self.h, int(step)))
+
+    def pair_forces(self, replica, step):
+        n = self.n_beads[replica]
+        fx, fy = np.empty(n, np.float32), np.empty(n, np.float32)
+        check(self.lib.dpd_pair_forces(self.h, replica, int(step), ptr(fx), ptr(fy)))
+        return fx, fy
+
+    def bond_forces(self, replica):
+        n = self.n_beads[replica]
+        fx, fy = np.empty(n, np.float32), np.empty(n, np.float32)
+        mb = C.c_float()
+        check(self.lib.dpd_bond_forces(self.h, replica, ptr(fx), ptr(fy), C.byref(mb)))
+        return fx, fy, mb.value
+
+    def integrate(self):
+        check(self.lib.dpd_integrate(self.h))
+
+    def chemistry(self, step):
+        check(self.lib.dpd_chemistry(self.h, int(step)))
+
+    # ---------------------------------------------------------------- outputs
+    def events(self, cap=1 << 20):
+        buf = (DpdEvent * cap)()
+        n = C.c_int32()
+        check(self.lib.dpd_get_events(self.h, buf, cap, C.byref(n)))
+        return [(e.step, e.kind, e.gid, e.partner, e.x, e.y, e.replica) for e in buf[: n.value]]
+
+    def observables(self, replica=0):
+        o = np.zeros(16)
+        check(self.lib.dpd_observables(self.h, replica, ptr(o)))
+        return dict(T=o[0], px=o[1], py=o[2], virial=o[3], maxbond=o[4], n_chains=int(o[5]),
+                    counts=o[8:16].astype(np.int64))
+
+    def pair_hist(self, replica, ta, tb, rmax, nbin):
+        h = np.zeros(nbin)
+        check(self.lib.dpd_pair_hist(self.h, replica, ta, tb, float(rmax), nbin, ptr(h)))
+        return h
+
+    def stream(self):
+        s = C.c_void_p()
+        check(self.lib.dpd_get_stream(self.h, C.byref(s)))
+        return s.value
+
+    def kernels_per_step(self):
+        a, b = C.c_int32(), C.c_int32()
+        check(self.lib.dpd_kernels_per_step(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value

@@ -1,0 +1,313 @@
+"""Parameters with the reference engine's keys, defaults and parsing rules.
+
+The reference keeps one table of (key, type, default, help) that drives ini
+parsing, defaults, validation and the `--params` listing
+(cel/engine/oercel.c:226-299, set_param :338-395, read_ini :409-434).  The
+drop-in front end must accept the same keys with the same defaults, so the
+key names and default values below are the reference's; the table itself and
+the help texts are written here.  Keys marked NEW exist only in this engine.
+"""
+from __future__ import annotations
+
+import math
+import re
+
+TYPE_NAMES = ["W", "H", "T", "N", "Ka", "Kb", "Z"]   # reference TNAME, oercel.c:49
+TYPE_ALIASES = {"P": 3}                              # the precursor of the lipid chemistry is type 3
+MAXT = 8
+
+# (key, kind, default, help); kinds: int, long, float, str, u64
+PDEFS = [
+    ("L", "float", "64", "box side; beads N = round(rho L^2)"),
+    ("rho", "float", "3", "number density"),
+    ("dt", "float", "0.03", "time step"),
+    ("lambda", "float", "0.65", "Groot-Warren predictor lambda"),
+    ("gamma", "float", "4.5", "friction; sigma = sqrt(2 gamma kT)"),
+    ("kT", "float", "1", "temperature"),
+    ("k_bond", "float", "100", "bond constant, U = k/2 (r - r0)^2"),
+    ("r0", "float", "0.5", "bond rest length"),
+    ("k_angle", "float", "10", "angle constant (only 0 is supported here)"),
+    ("lip_nH", "int", "1", "head beads per lipid"),
+    ("lip_nT", "int", "3", "tail beads per lipid"),
+    ("lip_arch", "str", "linear", "lipid shape (only linear is supported here)"),
+    ("r0_head", "float", "0.5", "branched lipids only (unused)"),
+    ("k_head", "float", "0", "branched lipids only (unused)"),
+    ("cos_head", "float", "0", "branched lipids only (unused)"),
+    ("lip_tie", "int", "0", "branched lipids only (unused)"),
+    ("syn_nN", "int", "0", "catalyst chemistry only (unused)"),
+    ("steps", "long", "10000", "run until this step number"),
+    ("snap_every", "long", "1000", "snapshot interval (0 = none)"),
+    ("stats_every", "long", "100", "stats.csv interval (0 = none)"),
+    ("ckpt_every", "long", "10000", "checkpoint interval (0 = at the end only)"),
+    ("ckpt_keep", "int", "0", "1 = keep ckpt_<step>.bin copies"),
+    ("log_every", "long", "1000", "log line interval"),
+    ("warmup", "long", "1000", "repulsion ramp on fresh starts (only 0 is supported here)"),
+    ("threads", "int", "2", "host threads (the step runs on the GPU)"),
+    ("nsub", "int", "4", "reference sub-cells per cell (the GPU grid is 1x1)"),
+    ("seed", "u64", "1", "random seed"),
+    ("init", "str", "soup", "soup or restart"),
+    ("restart", "str", "", "checkpoint to continue from"),
+    ("restart_reseed", "int", "0", "1 = branch with this seed on restart"),
+    ("walltime", "float", "0", "stop cleanly after this many seconds (0 = off)"),
+    ("chem", "int", "1", "1 = run the chemistry pass"),
+    ("n_chem", "long", "10", "chemistry interval in steps"),
+    ("r_cat", "float", "1.2", "catalyst chemistry only (unused)"),
+    ("syn_tries", "int", "8", "catalyst chemistry only (unused)"),
+    ("syn_relax", "int", "20", "catalyst chemistry only (unused)"),
+    ("p_syn_a", "float", "0.02", "catalyst chemistry only (unused)"),
+    ("p_syn_b", "float", "0.06", "catalyst chemistry only (unused)"),
+    ("p_rep_a", "float", "0.001", "catalyst chemistry only (unused)"),
+    ("p_rep_b", "float", "0.001", "catalyst chemistry only (unused)"),
+    ("mu", "float", "0.02", "catalyst chemistry only (unused)"),
+    ("p_ld", "float", "2e-4", "catalyst chemistry only (unused)"),
+    ("p_kd", "float", "5e-4", "catalyst chemistry only (unused)"),
+    ("p_nd", "float", "1e-4", "catalyst chemistry only (unused)"),
+    ("feed", "str", "uniform", "catalyst chemistry only (unused)"),
+    ("p_feed", "float", "1e-3", "catalyst chemistry only (unused)"),
+    ("feed_cap", "float", "0.12", "catalyst chemistry only (unused)"),
+    ("vent_shape", "str", "disk", "catalyst chemistry only (unused)"),
+    ("vent_x", "float", "-1", "catalyst chemistry only (unused)"),
+    ("vent_y", "float", "-1", "catalyst chemistry only (unused)"),
+    ("vent_r", "float", "5", "catalyst chemistry only (unused)"),
+    ("vent_w", "float", "4", "catalyst chemistry only (unused)"),
+    ("events", "int", "1", "1 = write events.csv"),
+    ("stir_A", "float", "0", "stirring force (only 0 is supported here)"),
+    ("stir_n", "int", "1", "stirring periods"),
+    ("kT_amp", "float", "0", "temperature cycle (only 0 is supported here)"),
+    ("kT_period", "float", "1000", "temperature cycle period"),
+    ("f_lip", "float", "0.10", "soup: fraction of beads in lipids"),
+    ("f_Ka", "float", "0.005", "soup: fraction of Ka beads"),
+    ("f_Kb", "float", "0", "soup: fraction of Kb beads"),
+    ("c_N", "float", "0.12", "soup: fraction of N (P) beads"),
+    # NEW: this engine's noise generator and lipid chemistry
+    ("noise", "str", "philox", "NEW pair noise: philox (Philox4x32-10) or mix13 (the reference's hash)"),
+    ("p_grow", "float", "1e-3", "NEW P -> T growth probability per check"),
+    ("p_break", "float", "1e-5", "NEW H-T bond break probability per check"),
+    ("p_bond", "float", "1e-2", "NEW free T + free H bonding probability per check"),
+    ("r_grow", "float", "1.0", "NEW growth radius"),
+    ("r_bond", "float", "0.6", "NEW bonding radius"),
+    ("n_t_min", "int", "2", "NEW T beads a P needs within r_grow"),
+    ("max_chain", "int", "12", "NEW longest chain growth may produce"),
+]
+PKEYS = {k: (t, d, h) for k, t, d, h in PDEFS}
+REMOVED = {"seed_R", "seed_spacing", "seed_cN_in", "seed_nKa", "feed_every", "feed_grid", "feed_tmin"}
+
+
+class ParamError(ValueError):
+    pass
+
+
+def default_amatrix():
+    """the reference's default repulsions (oercel.c:303-320)"""
+    a = [[25.0] * MAXT for _ in range(MAXT)]
+
+    def s(i, j, v):
+        a[i][j] = a[j][i] = v
+
+    s(0, 1, 20.0)
+    s(0, 2, 80.0)
+    s(1, 2, 50.0)
+    s(3, 0, 25.0)
+    s(3, 1, 25.0)
+    s(3, 2, 40.0)
+    for k in (4, 5):
+        s(k, 0, 25.0)
+        s(k, 1, 30.0)
+        s(k, 2, 120.0)
+        s(k, 3, 25.0)
+    return a
+
+
+def _type_index(name):
+    if name in TYPE_NAMES:
+        return [TYPE_NAMES.index(name)]
+    if name in TYPE_ALIASES:
+        return [TYPE_ALIASES[name]]
+    if name == "K":
+        return [4, 5]
+    return None
+
+
+def _parse(kind, key, val):
+    val = val.strip()
+    try:
+        if kind == "int":
+            if not re.fullmatch(r"[+-]?\d+", val):
+                raise ValueError
+            return int(val)
+        if kind == "long":
+            return int(round(float(val)))
+        if kind == "u64":
+            return int(val, 0)
+        if kind == "float":
+            return float(val)
+        return val
+    except ValueError:
+        raise ParamError(f"bad value for {key}: '{val}'") from None
+
+
+class Params:
+    """Parameter set; attribute access by key (p.L, p["lambda"])."""
+
+    def __init__(self, **overrides):
+        self.v = {k: _parse(t, k, d) for k, t, d, _ in PDEFS}
+        self.a = default_amatrix()
+        for k, val in overrides.items():
+            self.set(k, str(val))
+
+    def __getattr__(self, k):
+        v = self.__dict__.get("v")
+        if v is not None and k in v:
+            return v[k]
+        raise AttributeError(k)
+
+    def __getitem__(self, k):
+        return self.v[k]
+
+    def set(self, key: str, val: str):
+        key = key.strip()
+        if key.startswith("a_"):
+            parts = key[2:].split("_")
+            if len(parts) != 2:
+                raise ParamError(f"bad repulsion key '{key}' (use a_X_Y)")
+            t1, t2 = _type_index(parts[0]), _type_index(parts[1])
+            if t1 is None or t2 is None:
+                raise ParamError(f"bad repulsion key '{key}'")
+            x = _parse("float", key, val)
+            for i in t1:
+                for j in t2:
+                    self.a[i][j] = self.a[j][i] = x
+            return
+        if key in PKEYS:
+            self.v[key] = _parse(PKEYS[key][0], key, val)
+            return
+        if key in REMOVED:
+            raise ParamError(f"parameter '{key}' was removed in the reference engine")
+        raise ParamError(f"unknown parameter '{key}'")
+
+    def update(self, items):
+        """apply (key, value) pairs: generic catalyst keys a_K_X first (oercel.c:2155-2158)"""
+        items = list(items)
+        gen = [kv for kv in items if _generic(kv[0])]
+        for k, v in gen + [kv for kv in items if not _generic(kv[0])]:
+            self.set(k, v)
+        return self
+
+    @classmethod
+    def from_ini(cls, path, overrides=()):
+        p = cls()
+        return p.update(read_ini(path) + [parse_override(o) for o in overrides])
+
+    def n_beads(self):
+        return int(round(self.rho * self.L * self.L))
+
+    def validate(self):
+        """the reference's finalize_params checks that apply here, plus this engine's limits"""
+        if self.L < 8:
+            raise ParamError("L must be >= 8")
+        if self.dt <= 0:
+            raise ParamError("dt must be > 0")
+        if self.kT <= 0:
+            raise ParamError("kT must be > 0")
+        if self.lip_arch != "linear":
+            raise ParamError("only lip_arch = linear is supported")
+        if self.k_angle != 0:
+            raise ParamError("angle terms are not supported: set k_angle = 0")
+        if self.stir_A != 0 or self.kT_amp != 0:
+            raise ParamError("stirring and the temperature cycle are not supported: set stir_A = 0, kT_amp = 0")
+        if self.warmup != 0 and self.init == "soup":
+            raise ParamError("the repulsion warm-up ramp is not supported: set warmup = 0")
+        if self.noise not in ("philox", "mix13"):
+            raise ParamError("noise must be philox or mix13")
+        if self.init not in ("soup", "restart"):
+            raise ParamError("init must be soup or restart")
+        if self.chem and (self.f_Ka > 0 or self.f_Kb > 0):
+            raise ParamError("the catalyst chemistry (Ka/Kb) is not implemented; set f_Ka = f_Kb = 0")
+        return self
+
+    def sigma(self):
+        return math.sqrt(2.0 * self.gamma * self.kT)
+
+    def to_struct(self, seed=None):
+        from ._capi import DpdParams, load
+        s = DpdParams()
+        load().dpd_params_default(s)
+        s.L = float(self.L)
+        s.dt = float(self.dt)
+        s.lam = float(self["lambda"])
+        s.gamma = float(self.gamma)
+        s.kT = float(self.kT)
+        for i in range(MAXT):
+            for j in range(MAXT):
+                s.a[i * MAXT + j] = float(self.a[i][j])
+        s.k_bond = float(self.k_bond)
+        s.r0 = float(self.r0)
+        s.seed = int(self.seed if seed is None else seed) & 0xFFFFFFFFFFFFFFFF
+        s.noise = 0 if self.noise == "philox" else 1
+        s.chem = int(self.chem)
+        s.n_chem = int(self.n_chem)
+        s.n_t_min = int(self.n_t_min)
+        s.max_chain = int(self.max_chain)
+        s.p_break, s.p_grow, s.p_bond = float(self.p_break), float(self.p_grow), float(self.p_bond)
+        s.r_grow, s.r_bond = float(self.r_grow), float(self.r_bond)
+        return s
+
+    def write(self, path, overrides=()):
+        """params.ini with every key (reference write_params, oercel.c:626-653)"""
+        with open(path, "w") as f:
+            f.write("# oercel_b200 parameters actually used (all keys, defaults filled in)\n")
+            if overrides:
+                f.write("# command-line overrides: " + " ".join(overrides) + "\n")
+            for k, t, _, h in PDEFS:
+                v = self.v[k]
+                vs = repr(float(v)) if t == "float" else str(v)
+                f.write(f"{k} = {vs}    # {h}\n")
+            f.write(f"# derived: sigma = {self.sigma()!r}\n# repulsion matrix a_ij (symmetric)\n")
+            for i in range(len(TYPE_NAMES)):
+                for j in range(i, len(TYPE_NAMES)):
+                    f.write(f"a_{TYPE_NAMES[i]}_{TYPE_NAMES[j]} = {self.a[i][j]!r}\n")
+
+
+def _generic(key):
+    if not key.startswith("a_"):
+        return False
+    parts = key[2:].split("_")
+    return len(parts) == 2 and "K" in parts
+
+
+def read_ini(path):
+    """key = value lines, '#' comments (reference read_ini, oercel.c:409-434)"""
+    out = []
+    with open(path) as f:
+        for ln, line in enumerate(f, 1):
+            line = line.split("#", 1)[0].strip()
+            if not line:
+                continue
+            if "=" not in line:
+                raise ParamError(f"{path}:{ln}: expected key = value")
+            k, v = line.split("=", 1)
+            out.append((k.strip(), v.strip()))
+    return out
+
+
+def parse_override(o):
+    if "=" not in o:
+        raise ParamError(f"override '{o}' is not key=value")
+    k, v = o.split("=", 1)
+    return k.strip(), v.strip()
+
+
+def param_table():
+    """markdown table of every key, as the reference's --params (oercel.c:2107-2123)"""
+    lines = ["| key | default | meaning |", "|---|---|---|"]
+    for k, _, d, h in PDEFS:
+        lines.append(f"| `{k}` | {d if d else '(empty)'} | {h} |")
+    a = default_amatrix()
+    lines.append("")
+    lines.append("Default repulsion matrix a_ij (key `a_X_Y`, symmetric; `a_K_X` sets Ka and Kb at once):")
+    lines.append("")
+    lines.append("|    |" + "".join(f" {n} |" for n in TYPE_NAMES))
+    lines.append("|---|" + "---|" * len(TYPE_NAMES))
+    for i, n in enumerate(TYPE_NAMES):
+        lines.append(f"| **{n}** |" + "".join(f" {a[i][j]:g} |" for j in range(len(TYPE_NAMES))))
+    return "\n".join(lines)
