@@ -1,0 +1,383 @@
+"""Benchmark of the 2D DPD step with lipid chemistry on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one box per GPU, "replicas only": the single box does not shard):
+the 1,048,576-bead box at L = 512, rho = 4 with the lipid chemistry every
+step (oercel_b200.workloads.config2), FP32, synthetic seeded soup.
+
+ours: W untimed steps, then K steps, each a one-step CUDA graph timed with
+CUDA events on the engine's stream, with a 256 MiB buffer written between
+timed steps to flush L2 (outside the events); value = beads x K x N / max over
+ranks of the summed step times.  Also: a live kernel-by-kernel profile of a
+real step (roofline of the dominant kernel), the end-to-end rate through the
+C ABI with host buffers, the batched 256-replica ensemble against the same
+replicas one at a time, the reference CPU engine on the host cores, and the
+SM clocks sampled during the timed loop.
+reference: the reference engine's own CLI (oracle/_ref/oercel, built from
+cel/engine/oercel.c) on the same box size with all host threads, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "welcome-youtube_b200"))
+
+METRIC = "DPD bead-steps/s at 1M beads & 256-replica batch; adjoint/forward time ratio"
+UNIT = "bead-steps/s"
+# algorithmic bytes per bead of each kernel of the step (FP32 SoA; derivation in DESIGN.md)
+KERNEL_BYTES = {"scan1": 3, "scan2": 2, "place": 13, "cellfix": 14, "permute": 88, "chem_break": 4,
+                "chem_grow_req": 8, "chem_grow_apply": 4, "chem_bond_req": 16, "chem_bond_apply": 4, "forces": 54}
+KERNELS_PLAIN = ["scan1", "scan2", "place", "cellfix", "permute"]
+KERNELS_CHEM = ["chem_break", "chem_grow_req", "chem_grow_apply", "chem_bond_req", "chem_bond_apply"]
+# algorithmic bytes per bead-step of the whole step (the workload table's figure: plain 138, with chemistry 147)
+STEP_BYTES_CHEM = 147
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws == 1:
+        return 0, 0, 1
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return dist.get_rank(), int(os.environ.get("LOCAL_RANK", "0")), ws
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed loop"""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def reference_binary():
+    flags = ""
+    try:
+        flags = open("/proc/cpuinfo").read()
+    except OSError:
+        pass
+    avx512 = all(f in flags for f in (" avx512f", " avx512dq", " avx512bw", " avx512vl"))
+    name = "oercel" if avx512 else "oercel_portable"
+    path = os.path.join(ROOT, "oracle", "_ref", name)
+    return path if os.path.exists(path) else None, ("avx512" if avx512 else "avx2")
+
+
+def run_reference(p, steps, threads):
+    """the reference CLI on the physics of p; returns (ms/step of the step phases, timing dict)"""
+    from oercel_b200.workloads import reference_ini
+    exe, isa = reference_binary()
+    if exe is None:
+        return None, {"error": "oracle/_ref/oercel not built"}
+    with tempfile.TemporaryDirectory() as td:
+        ini = os.path.join(td, "params.ini")
+        with open(ini, "w") as f:
+            f.write(reference_ini(p, steps, threads))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        r = subprocess.run([exe, ini, os.path.join(td, "out")], capture_output=True, text=True, env=env,
+                           timeout=1800)
+    m = re.search(r"timing: (\d+) steps, ([\d.]+) ms/step \(integrate ([\d.]+), sort ([\d.]+), pair ([\d.]+), "
+                  r"bonded ([\d.]+), chem ([\d.]+), io ([\d.]+)\)", r.stdout)
+    if not m:
+        return None, {"error": (r.stdout + r.stderr)[-400:]}
+    t = dict(zip(["steps", "total", "integrate", "sort", "pair", "bonded", "chem", "io"],
+                 [float(v) for v in m.groups()]))
+    step_ms = t["integrate"] + t["sort"] + t["pair"] + t["bonded"] + t["chem"]
+    t["isa"] = isa
+    return step_ms, t
+
+
+def reference_arm(args, rank, ws):
+    if rank != 0:
+        return
+    from oercel_b200 import workloads
+    p = workloads.config2()
+    threads = os.cpu_count() or 1
+    step_ms, t = run_reference(p, min(args.steps, 300), threads)
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "L=512 rho=4 box, 1,048,576 beads, W/H/T/P lipid soup (reference physics step; "
+                                   "the lipid chemistry does not exist in the reference)",
+                       "beads": p.n_beads(), "parallelism": f"openmp{threads}"}}
+    if step_ms is None:
+        base.update({"unavailable": t.get("error", "reference run failed")})
+        print(json.dumps(base))
+        return
+    v = p.n_beads() * 1000.0 / step_ms * 1.0  # one box, the reference runs on the host
+    base.update({"value": v, "ms_per_step": step_ms,
+                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                                  "sample": f"{int(t['steps'])} steps of the 1,048,576-bead box, "
+                                            f"ms/step of integrate+sort+pair+bonded ({t['isa']} build)"},
+                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "reference_timing_ms": t})
+    print(json.dumps(base))
+
+
+def time_steps(torch, eng, K, flush):
+    """K steps, each a one-step graph between CUDA events on the engine's stream"""
+    stream = torch.cuda.ExternalStream(eng.stream())
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            starts[k].record(stream)
+            eng.step_async(1)
+            ends[k].record(stream)
+    stream.synchronize()
+    eng.sync()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+
+def batched_rates(torch, steps=64):
+    """256-replica ensemble in one engine vs the same replicas one engine at a
+    time; both run graphs of `steps` steps (captured before timing)"""
+    from oercel_b200 import Engine, workloads
+    reps = workloads.config3()
+    plist = [p for p, _ in reps]
+    nb = [n for _, n in reps]
+    total = sum(nb)
+    e = Engine(plist, nb)
+    for r in range(len(plist)):
+        e.load_soup(r)
+    e.prime()
+    e.set_graph_steps(steps)
+    e.step(steps)
+    stream = torch.cuda.ExternalStream(e.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    e.step_async(steps)
+    b.record(stream)
+    stream.synchronize()
+    e.sync()
+    t_batched = a.elapsed_time(b)
+    e.close()
+    # one at a time: each replica its own engine (plain GPU step, CUDA graphs), run back to back
+    singles = []
+    for p, n in reps:
+        s = Engine(p, n)
+        s.load_soup(0)
+        s.prime()
+        s.set_graph_steps(steps)
+        s.step(steps)
+        singles.append(s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in singles:
+        s.step_async(steps)
+    for s in singles:
+        s.sync()
+    t_single = (time.perf_counter() - t0) * 1000.0
+    for s in singles:
+        s.close()
+    return {"value": total * steps / (t_batched / 1000.0), "one_at_a_time": total * steps / (t_single / 1000.0),
+            "ratio": t_single / t_batched, "replicas": len(reps), "beads": total, "steps": steps,
+            "timing": "batched: CUDA events on the engine stream; one at a time: host clock around all engines"}
+
+
+def e2e_rate(eng_cls, p, K):
+    """the public API from host memory: load the soup from pinned host buffers,
+    prime, K steps each followed by the stats row and the event log read back,
+    the final state read back; wall clock around all of it"""
+    import numpy as np
+    import torch
+
+    from oercel_b200 import soup_for
+    s = soup_for(p)
+    n = len(s["x"])
+    pin = {}
+    for k in ("x", "y", "vx", "vy"):
+        t = torch.empty(n, dtype=torch.float32, pin_memory=True)
+        t.numpy()[:] = s[k]
+        pin[k] = t.numpy()
+    for k, dt in (("type", torch.uint8), ("prev", torch.int32), ("next", torch.int32)):
+        t = torch.empty(n, dtype=dt, pin_memory=True)
+        t.numpy()[:] = s[k]
+        pin[k] = t.numpy()
+    out = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
+    eng = eng_cls(p)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.set_state(0, pin["x"], pin["y"], pin["vx"], pin["vy"], pin["type"], None, pin["prev"], pin["next"])
+    eng.prime()
+    nev = 0
+    for _ in range(K):
+        eng.step(1)
+        eng.observables(0)
+        nev += len(eng.events())
+    st = eng.state(0)
+    el = time.perf_counter() - t0
+    eng.close()
+    h2d = n * (4 * 4 + 1 + 4 + 4)
+    d2h = 16 * 8 + nev * 32 / max(K, 1) + n * (8 * 4 + 1 + 3 * 4)
+    return {"value": n * K / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d / K),
+            "d2h_bytes_per_step": int(d2h / K + 16 * 8), "steps": K,
+            "note": "state upload and final read-back amortised over the steps; stats row and events every step"}
+
+
+def ours(args, rank, local_rank, ws):
+    import numpy as np
+    import torch
+
+    from oercel_b200 import Engine, workloads
+    torch.cuda.set_device(local_rank)
+    p = workloads.config2(seed=1 + rank)
+    eng = Engine(p)
+    eng.load_soup(0)
+    eng.prime()
+    eng.step(max(args.warmup, 3))
+    eng.set_graph_steps(1)
+    eng.step(2)  # capture the one-step graphs of both buffer parities before timing
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    nb = p.n_beads()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        total_ms = time_steps(torch, eng, args.steps, flush)
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = nb * args.steps * ws / (total_ms / 1000.0)
+    # live kernel profile of real steps (median of 5)
+    prof = np.median(np.array([eng.profile_step() for _ in range(5)]), axis=0)
+    names = KERNELS_PLAIN + (KERNELS_CHEM if len(prof) > 6 else []) + ["forces"]
+    kernels = {n: float(ms) for n, ms in zip(names, prof)}
+    top = max(kernels, key=kernels.get)
+    peak, peak_kind = peaks()
+    ach = KERNEL_BYTES[top] * nb / (kernels[top] / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"{top}_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    n_plain, _ = eng.kernels_per_step()
+    eng.close()
+    del flush
+    res = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "L=512 rho=4 box, 1,048,576 beads, W/H/T/P lipid soup, lipid chemistry every "
+                                  "step, one box per GPU", "beads_per_gpu": nb, "parallelism": f"replicas{ws}",
+                      "l2": "flushed between timed steps (256 MiB write, outside the events)", "noise": "philox"},
+           "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
+                        "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
+                        "bytes_per_bead": KERNEL_BYTES[top]},
+           "step_roofline": {"bytes_per_bead_step": STEP_BYTES_CHEM,
+                             "achieved": value / ws * STEP_BYTES_CHEM / 1e9, "peak": peak,
+                             "frac": value / ws * STEP_BYTES_CHEM / 1e9 / peak},
+           "kernels_ms": kernels, "gpu_launches": n_plain * args.steps, "clocks": clk.summary()}
+    if rank == 0:
+        res["e2e"] = e2e_rate(Engine, p, args.e2e_steps)
+        if not args.skip_batched and ws == 1:
+            res["batched"] = batched_rates(torch)
+        if ws == 1 and not args.skip_cpu:
+            threads = os.cpu_count() or 1
+            step_ms, t = run_reference(p, args.cpu_steps, threads)
+            if step_ms is not None:
+                res["cpu_baseline"] = {"value": nb * 1000.0 / step_ms, "unit": UNIT, "cores": threads,
+                                       "kind": "reference",
+                                       "sample": f"{args.cpu_steps} steps of the 1,048,576-bead box, reference CLI, "
+                                                 f"integrate+sort+pair+bonded ms/step ({t['isa']} build); the "
+                                                 f"lipid chemistry does not exist in the reference"}
+            else:
+                res["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                                       "sample": t.get("error", "")}
+        print(json.dumps(res))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--cpu-steps", type=int, default=100)
+    ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, local_rank, ws = dist_init()
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, ws)
+        else:
+            ours(args, rank, local_rank, ws)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -521,19 +521,21 @@ void ora_observables(const ora_params *P, int32_t n, const float *x, const float
 
 /* Histogram of minimum-image distances between beads of types ta and tb
  * (each unordered pair once; ta == tb allowed) in nbin bins on [0, rmax),
- * rmax <= 1 so the 3x3 cells suffice.  Pattern of
+ * over the (2R+1)^2 cells with R = ceil(rmax * ncx / L).  Pattern of
  * cel/engine/tests/snapcheck.py:86-117. */
 void ora_pair_hist(const ora_params *P, int32_t n, const float *x, const float *y, const uint8_t *type,
                    const int32_t *cstart, int32_t ta, int32_t tb, double rmax, int32_t nbin, double *hist) {
     const int ncx = P->ncx, ncy = P->ncy;
     const double L = P->L;
+    int R = (int)ceil(rmax * P->icsx);
+    if (2 * R + 1 > ncx) R = (ncx - 1) / 2;
     (void)n;
     for (int cx = 0; cx < ncx; cx++)
         for (int cy = 0; cy < ncy; cy++) {
             const int c = cx * ncy + cy;
             for (int i = cstart[c]; i < cstart[c + 1]; i++)
-                for (int ox = -1; ox <= 1; ox++)
-                    for (int oy = -1; oy <= 1; oy++) {
+                for (int ox = -R; ox <= R; ox++)
+                    for (int oy = -R; oy <= R; oy++) {
                         const int cc = ((cx + ox + ncx) % ncx) * ncy + (cy + oy + ncy) % ncy;
                         for (int j = cstart[cc]; j < cstart[cc + 1]; j++) {
                             if (j <= i) continue;

@@ -150,3 +150,24 @@ def test_reference_trajectory_fixture_relaxes():
     g = golden("traj_L16_seed5.npz")
     T = g["T"]
     assert T.max() > 2.0 and T[-1] < T.max() and np.all(np.diff(T[T.argmax():]) < 0)
+
+
+def test_pair_hist_matches_brute_force():
+    rng = np.random.default_rng(0)
+    L, n = 12.0, 600
+    x = rng.uniform(0, L, n).astype(np.float32)
+    y = rng.uniform(0, L, n).astype(np.float32)
+    t = rng.integers(0, 3, n).astype(np.uint8)
+    p = O.params(L, np.full((8, 8), 25.0))
+    key, cs, src = O.sort(p, x, y)
+    st = dict(x=x[src], y=y[src], type=t[src])
+    h = O.pair_hist(p, st, cs, 2, 2, 2.0, 64)
+    X, Y = st["x"].astype(float), st["y"].astype(float)
+    idx = np.nonzero(st["type"] == 2)[0]
+    dx = X[idx][:, None] - X[idx][None, :]
+    dy = Y[idx][:, None] - Y[idx][None, :]
+    dx -= L * np.round(dx / L)
+    dy -= L * np.round(dy / L)
+    r = np.hypot(dx, dy)[np.triu_indices(len(idx), 1)]
+    hb, _ = np.histogram(r[r < 2.0], bins=64, range=(0, 2))
+    assert np.array_equal(h, hb)
