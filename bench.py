@@ -35,10 +35,10 @@ sys.path.insert(0, os.path.join(ROOT, "welcome-youtube_b200"))
 METRIC = "DPD bead-steps/s at 1M beads & 256-replica batch; adjoint/forward time ratio"
 UNIT = "bead-steps/s"
 # algorithmic bytes per bead of each kernel of the step (FP32 SoA; derivation in DESIGN.md)
-KERNEL_BYTES = {"scan1": 3, "scan2": 2, "place": 13, "cellfix": 14, "permute": 88, "chem_break": 4,
-                "chem_grow_req": 8, "chem_grow_apply": 4, "chem_bond_req": 16, "chem_bond_apply": 4, "forces": 54}
+KERNEL_BYTES = {"scan1": 3, "scan2": 2, "place": 13, "cellfix": 14, "permute": 88, "chem_grow_req": 0,
+                "chem_grow_apply": 0, "chem_bond_req": 0, "chem_bond_apply": 0, "forces": 54}
 KERNELS_PLAIN = ["scan1", "scan2", "place", "cellfix", "permute"]
-KERNELS_CHEM = ["chem_break", "chem_grow_req", "chem_grow_apply", "chem_bond_req", "chem_bond_apply"]
+KERNELS_CHEM = ["chem_grow_req", "chem_grow_apply", "chem_bond_req", "chem_bond_apply"]
 # algorithmic bytes per bead-step of the whole step (the workload table's figure: plain 138, with chemistry 147)
 STEP_BYTES_CHEM = 147
 
@@ -228,9 +228,8 @@ def batched_rates(torch, steps=64):
         singles.append(s)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for s in singles:
+    for s in singles:  # strictly one replica after the other
         s.step_async(steps)
-    for s in singles:
         s.sync()
     t_single = (time.perf_counter() - t0) * 1000.0
     for s in singles:
@@ -268,7 +267,7 @@ def e2e_rate(eng_cls, p, K):
     nev = 0
     for _ in range(K):
         eng.step(1)
-        eng.observables(0)
+        eng.observables(0, virial=False)
         nev += len(eng.events())
     st = eng.state(0)
     el = time.perf_counter() - t0
@@ -337,6 +336,9 @@ def ours(args, rank, local_rank, ws):
                              "achieved": value / ws * STEP_BYTES_CHEM / 1e9, "peak": peak,
                              "frac": value / ws * STEP_BYTES_CHEM / 1e9 / peak},
            "kernels_ms": kernels, "gpu_launches": n_plain * args.steps, "clocks": clk.summary()}
+    if rank == 0 and args.quick:
+        print(json.dumps(res))
+        return
     if rank == 0:
         res["e2e"] = e2e_rate(Engine, p, args.e2e_steps)
         if not args.skip_batched and ws == 1:
@@ -366,6 +368,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=100)
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="timed loop and kernel profile only (for profiler runs)")
     args = ap.parse_args()
     rank, local_rank, ws = dist_init()
     try:

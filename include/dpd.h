@@ -104,6 +104,17 @@ typedef struct {
 
 typedef struct dpd_handle dpd_handle;
 
+/* Launch choices of a handle (the autotuner's knobs).  force_kernel 0: cell
+ * tiles of tile_w x tile_h cells staged in shared memory, each pair evaluated
+ * once (default); 1: one thread per bead over its 3x3 cells, each pair
+ * evaluated by both beads.  Both give bit-identical forces.  graph_steps:
+ * steps per captured CUDA graph. */
+typedef struct {
+    int32_t force_kernel;
+    int32_t tile_w, tile_h;   /* (tile_w + 2) * (tile_h + 2) <= 256 */
+    int32_t graph_steps;
+} dpd_tuning;
+
 /* message of the last failed call on this thread ("" if none) */
 DPD_API const char *dpd_last_error(void);
 /* library version string */
@@ -161,6 +172,8 @@ DPD_API int dpd_step(dpd_handle *h, int64_t nsteps);
  * device-side error flag (as dpd_step does). */
 DPD_API int dpd_step_async(dpd_handle *h, int64_t nsteps);
 DPD_API int dpd_sync(dpd_handle *h);
+DPD_API int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t);
+DPD_API int dpd_get_tuning(const dpd_handle *h, dpd_tuning *t);
 /* steps per captured CUDA graph (default: about 4M bead-steps per replay) */
 DPD_API int dpd_set_graph_steps(dpd_handle *h, int32_t steps);
 /* One real step launched kernel by kernel with CUDA events around each launch
@@ -198,8 +211,10 @@ DPD_API int dpd_integrate(dpd_handle *h);
 /* one chemistry pass at the given step on the current sorted state */
 DPD_API int dpd_chemistry(dpd_handle *h, int64_t step);
 
-/* events recorded since the last call, in device order; *n_out = count
- * returned (<= cap); the buffer is then cleared. */
+/* Events recorded since the last call, in device order; *n_out = count
+ * returned (<= cap); the buffer is then cleared (events beyond cap are
+ * dropped and reported as DPD_E_EVENT_OVERFLOW).  out == NULL only reports
+ * the pending count in *n_out and clears nothing. */
 DPD_API int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out);
 
 /* Observables of replica r (reference stats row, oercel.c:2364-2372):
@@ -208,6 +223,8 @@ DPD_API int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *
  * out[4] largest bond length; out[5] number of chains (heads with a bond);
  * out[8 + t] number of beads of type t (t < 8).  out has 16 entries. */
 DPD_API int dpd_observables(dpd_handle *h, int32_t replica, double *out);
+/* the stats row only (out[3], the virial, is left 0): no pair loop */
+DPD_API int dpd_stats(dpd_handle *h, int32_t replica, double *out);
 
 /* Histogram (nbin bins on [0, rmax), rmax <= 3) of distances between beads of
  * types ta and tb of replica r, each unordered pair once. */

@@ -44,6 +44,11 @@ struct dpd_handle {
     int nbch = 0, ncch = 0;
     Bufs b{};
     int cur = 0;
+    // force kernel: 0 = cell tiles in shared memory (half shell), 1 = one thread per bead (full shell)
+    int force_kernel = 0;
+    int tile_w = 8, tile_h = 16;
+    TileDesc *d_tiles = nullptr;
+    int ntiles = 0;
     bool any_chem = false;
     bool keys_valid = false;
     int64_t step = 0;
@@ -168,6 +173,35 @@ static void free_all(dpd_handle *h) {
     if (h->s) cudaStreamDestroy(h->s);
 }
 
+// cell tiles of every replica: w x h cells (narrower boxes get narrower tiles,
+// so that a tile and its halo never hold the same column or row twice)
+static int build_tiles(dpd_handle *h) {
+    if (h->tile_w < 1 || h->tile_h < 1 || (h->tile_w + 2) * (h->tile_h + 2) > 256)
+        return fail(DPD_E_ARG, "tile shape %dx%d: need (w+2)(h+2) <= 256", h->tile_w, h->tile_h);
+    std::vector<TileDesc> t;
+    for (int r = 0; r < h->nrep; r++) {
+        const RepDev &R = h->rh[r];
+        const int w = std::min(h->tile_w, R.ncx - 2), hh = std::min(h->tile_h, R.ncy - 2);
+        for (int cx = 0; cx < R.ncx; cx += w)
+            for (int cy = 0; cy < R.ncy; cy += hh)
+                t.push_back({r, cx, cy, std::min(w, R.ncx - cx), std::min(hh, R.ncy - cy), 0, 0, 0});
+    }
+    if (h->d_tiles) {
+        cudaFree(h->d_tiles);
+        for (auto &p : h->allocs)
+            if (p == (void *)h->d_tiles) p = nullptr;
+    }
+    TRY(dalloc(h, &h->d_tiles, t.size()));
+    CK(cudaMemcpy(h->d_tiles, t.data(), t.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
+    h->ntiles = (int)t.size();
+    return DPD_OK;
+}
+
+static void enqueue_forces(dpd_handle *h, bool next_keys) {
+    if (h->force_kernel == 0) launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
+    else launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, next_keys, h->s);
+}
+
 static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, const int32_t *n_beads) {
     h->nrep = nrep;
     h->params.assign(params, params + nrep);
@@ -196,6 +230,8 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     h->nbch = (int)bch.size();
     h->ncch = (int)cch.size();
     CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+    if (tile_setup() != 0) return fail(DPD_E_CUDA, "cannot reserve %zu bytes of shared memory per CTA", tile_smem_bytes());
+    if (const char *e = getenv("DPD_FORCES")) h->force_kernel = strcmp(e, "bead") == 0 ? 1 : 0;
     TRY(dalloc(h, &h->d_rep, nrep));
     TRY(dalloc(h, &h->d_bch, bch.size()));
     TRY(dalloc(h, &h->d_cch, cch.size()));
@@ -221,6 +257,8 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.bsum, C / SCAN_PER_BLOCK + 2));
     TRY(dalloc(h, &b.claim, N));
     TRY(dalloc(h, &b.req, N));
+    TRY(dalloc(h, &b.grow_list, N));
+    TRY(dalloc(h, &b.bond_list, N));
     b.evcap = 1 << 20;
     TRY(dalloc(h, &b.events, (size_t)b.evcap));
     TRY(dalloc(h, &b.status, 1));
@@ -247,6 +285,7 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     int g = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 << 20) / std::max<int64_t>(1, h->N)));
     if (const char *e = getenv("DPD_GRAPH_STEPS")) g = atoi(e);
     h->gsteps = std::max(1, g);
+    TRY(build_tiles(h));
     return DPD_OK;
 }
 
@@ -293,6 +332,9 @@ static int check_status(dpd_handle *h) {
     if (st.flags) {
         CK(cudaMemsetAsync(&h->b.status->flags, 0, sizeof(unsigned), h->s));
         CK(cudaStreamSynchronize(h->s));
+        if (st.flags & DPD_F_TILE)
+            return fail(DPD_E_SORT_OVERFLOW, "a cell tile and its halo held more beads than fit in shared memory");
+        if (st.flags & DPD_F_FORCE) return fail(DPD_E_STATE, "a pair or bond force above 2048 (fixed-point range)");
         if (st.flags & DPD_F_NONFINITE) return fail(DPD_E_STATE, "non-finite force (flags 0x%x)", st.flags);
         if (st.flags & DPD_F_OUTSIDE)
             return fail(DPD_E_STATE, "a bead moved more than one box length in one step (flags 0x%x)", st.flags);
@@ -414,7 +456,7 @@ static void enqueue_next_keys(dpd_handle *h) {
 extern "C" int dpd_prime(dpd_handle *h) {
     if (!h) return fail(DPD_E_ARG, "null handle");
     enqueue_sort(h, PERM_PRIME);
-    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, false, h->s);
+    enqueue_forces(h, false);
     launch_halfkick(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     enqueue_next_keys(h);
     CK(cudaGetLastError());
@@ -464,7 +506,7 @@ extern "C" int dpd_get_cells(dpd_handle *h, int32_t r, int32_t *cstart) {
 extern "C" int dpd_forces(dpd_handle *h, int64_t step) {
     if (!h) return fail(DPD_E_ARG, "null handle");
     TRY(set_device_step(h, step));
-    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, false, h->s);
+    enqueue_forces(h, false);
     h->keys_valid = false;
     CK(cudaGetLastError());
     return check_status(h);
@@ -521,7 +563,9 @@ extern "C" int dpd_integrate(dpd_handle *h) {
 extern "C" int dpd_chemistry(dpd_handle *h, int64_t step) {
     if (!h) return fail(DPD_E_ARG, "null handle");
     TRY(set_device_step(h, step));
-    launch_chemistry(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
+    CK(cudaMemsetAsync(&h->b.status->n_grow, 0, 2 * sizeof(unsigned), h->s));
+    launch_chem_scan(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
+    launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
     CK(cudaGetLastError());
     return check_status(h);
 }
@@ -534,8 +578,8 @@ static void enqueue_step(dpd_handle *h) {
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
     h->cur ^= 1;
-    if (h->any_chem) launch_chemistry(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
-    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, true, h->s);
+    if (h->any_chem) launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
+    enqueue_forces(h, true);
 }
 
 // capture gsteps steps starting from the current buffer parity
@@ -592,6 +636,36 @@ extern "C" int dpd_sync(dpd_handle *h) {
     return check_status(h);
 }
 
+extern "C" int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t) {
+    if (!h || !t) return fail(DPD_E_ARG, "null argument");
+    if (t->force_kernel != 0 && t->force_kernel != 1) return fail(DPD_E_ARG, "force_kernel must be 0 or 1");
+    if (t->graph_steps < 1) return fail(DPD_E_ARG, "graph_steps must be >= 1");
+    CK(cudaStreamSynchronize(h->s));
+    const int ow = h->tile_w, oh = h->tile_h;
+    h->tile_w = t->tile_w;
+    h->tile_h = t->tile_h;
+    const int r = build_tiles(h);
+    if (r != DPD_OK) {
+        h->tile_w = ow;
+        h->tile_h = oh;
+        build_tiles(h);
+        return r;
+    }
+    h->force_kernel = t->force_kernel;
+    h->gsteps = t->graph_steps;
+    drop_graphs(h);
+    return DPD_OK;
+}
+
+extern "C" int dpd_get_tuning(const dpd_handle *h, dpd_tuning *t) {
+    if (!h || !t) return fail(DPD_E_ARG, "null argument");
+    t->force_kernel = h->force_kernel;
+    t->tile_w = h->tile_w;
+    t->tile_h = h->tile_h;
+    t->graph_steps = h->gsteps;
+    return DPD_OK;
+}
+
 extern "C" int dpd_set_graph_steps(dpd_handle *h, int32_t steps) {
     if (!h || steps < 1) return fail(DPD_E_ARG, "graph length must be >= 1");
     CK(cudaStreamSynchronize(h->s));
@@ -627,10 +701,10 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     h->cur ^= 1;
     if (h->any_chem)
         for (int c = 0; c < chem_kernel_count(); c++) {
-            launch_chemistry_part(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, c, h->s);
+            launch_chem_lists(h->b, h->cur, h->d_rep, c, h->s);
             CK(cudaEventRecord(ev[k++], h->s));
         }
-    launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, true, h->s);
+    enqueue_forces(h, true);
     CK(cudaEventRecord(ev[k++], h->s));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(ev[nk]));
@@ -647,22 +721,27 @@ extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_
     CK(cudaMemcpyAsync(&st, h->b.status, sizeof st, cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
     const int have = (int)std::min<unsigned>(st.nevents, (unsigned)h->b.evcap);
+    if (!out) {  // count only, nothing is cleared
+        *n_out = have;
+        return DPD_OK;
+    }
     const int n = std::min(have, cap < 0 ? 0 : cap);
-    if (n > 0 && out) CK(cudaMemcpy(out, h->b.events, (size_t)n * sizeof(dpd_event), cudaMemcpyDefault));
+    if (n > 0) CK(cudaMemcpy(out, h->b.events, (size_t)n * sizeof(dpd_event), cudaMemcpyDefault));
     *n_out = n;
     CK(cudaMemset(&h->b.status->nevents, 0, sizeof(unsigned)));
     if (st.nevents > (unsigned)h->b.evcap)
         return fail(DPD_E_EVENT_OVERFLOW, "%u events were recorded, %d kept", st.nevents, h->b.evcap);
+    if (have > n) return fail(DPD_E_EVENT_OVERFLOW, "%d events pending, %d copied: the rest were dropped", have, n);
     return DPD_OK;
 }
 
-extern "C" int dpd_observables(dpd_handle *h, int32_t r, double *out) {
+static int observables_impl(dpd_handle *h, int32_t r, bool virial, double *out) {
     TRY(ensure_replica(h, r));
     if (!out) return fail(DPD_E_ARG, "null out");
     unsigned long long *o = h->b.obs + (size_t)r * OBS_N;
     CK(cudaMemsetAsync(o, 0, 4 * sizeof(unsigned long long), h->s));
     CK(cudaMemsetAsync(o + 5, 0, (OBS_N - 5) * sizeof(unsigned long long), h->s));
-    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, h->s);
+    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, h->s);
     CK(cudaGetLastError());
     unsigned long long v[OBS_N];
     CK(cudaMemcpyAsync(v, o, sizeof v, cudaMemcpyDeviceToHost, h->s));
@@ -683,6 +762,10 @@ extern "C" int dpd_observables(dpd_handle *h, int32_t r, double *out) {
     CK(cudaStreamSynchronize(h->s));
     return DPD_OK;
 }
+
+extern "C" int dpd_observables(dpd_handle *h, int32_t r, double *out) { return observables_impl(h, r, true, out); }
+
+extern "C" int dpd_stats(dpd_handle *h, int32_t r, double *out) { return observables_impl(h, r, false, out); }
 
 extern "C" int dpd_pair_hist(dpd_handle *h, int32_t r, int32_t ta, int32_t tb, double rmax, int32_t nbin,
                              double *hist) {

@@ -6,7 +6,11 @@
 // (cel/engine/oercel.c:819-826) -- and every conflict resolved by the lowest
 // requesting gid (atomicMin claim, then a check by each requester; the
 // reference GPU port resolves its lock rounds the same way, lowest rank wins,
-// cel/engine_gpu/oercel_gpu.cu:1746-1757):
+// cel/engine_gpu/oercel_gpu.cu:1746-1757).  The draws do not depend on the
+// state, so one pass over the beads (fused into the permute kernel of the step,
+// or k_chem_scan for the phase entry point) applies the breaks and lists the
+// few beads whose growth or bonding draw succeeded; the later stages run over
+// those lists only.
 //   1 brk : an H whose next bead is T breaks the bond with p_break;
 //   2 grow: a P with >= n_t_min T beads within r_grow, with p_grow, becomes a
 //           T bonded behind its nearest growable H-terminated chain end
@@ -15,47 +19,32 @@
 //   3 bond: a free T, with p_bond, bonds to its nearest free H within r_bond.
 // Nearest = smallest squared FP32 distance, ties to the lower gid
 // (oercel.c:1387-1396).
-#include "dpd_device.cuh"
+#include "dpd_chem.cuh"
 
-#define T_W 0
-#define T_H 1
-#define T_T 2
-#define T_P 3
-#define SALT_BREAK 1u
-#define SALT_GROW 2u
-#define SALT_BOND 3u
-
-__device__ __forceinline__ bool chem_due(const RepDev &R, long long step) {
-    return R.chem && R.n_chem > 0 && (step % R.n_chem) == 0;
-}
-
-__device__ __forceinline__ int type_of(uint32_t tg) { return (int)(tg >> TYPE_SHIFT); }
-
-__device__ __forceinline__ float dist2(float xa, float ya, float xb, float yb, float L, float h) {
-    const float dx = minimg(__fsub_rn(xb, xa), L, h), dy = minimg(__fsub_rn(yb, ya), L, h);
-    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-}
-
-__device__ void push_event(const Bufs &b, long long step, int kind, uint32_t gid, uint32_t partner, float x, float y,
-                           int rep) {
-    const unsigned k = atomicAdd(&b.status->nevents, 1u);
-    if ((int)k < b.evcap) {
-        EventDev e;
-        e.step = step;
-        e.kind = kind;
-        e.gid = gid;
-        e.partner = partner;
-        e.x = x;
-        e.y = y;
-        e.replica = rep;
-        b.events[k] = e;
-    } else {
-        raise_flag(b.status, DPD_F_EVENTS);
+// stage 1 on a sorted state in place (the phase entry point dpd_chemistry)
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_scan(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                        const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    const long long step = *b.step;
+    if (!chem_due(R, step)) return;
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const uint32_t *tg = b.tg[cur];
+    int2 *link = b.link[cur];
+    const uint32_t t0 = tg[d];
+    const int t = link[d].y;
+    if (type_of(t0) == T_H && t >= 0 && h_breaks(R, step, t0, tg[t])) {
+        link[d].y = -1;
+        link[t].x = -1;
+        const float2 p = b.pos[cur][d];
+        push_event(b, step, 1, t0 & GID_MASK, tg[t] & GID_MASK, p.x, p.y, c.rep);
     }
+    chem_candidate(b, R, step, c.rep, d, t0);
 }
 
 // tail end e of a chain headed by H that is shorter than max_chain, or a lone H
-__device__ bool growable_end(const uint32_t *tg, const int2 *link, int e, int max_chain, DevStatus *st) {
+__device__ bool growable_end(const uint32_t *tg, const int2 *link, int e, int max_chain) {
     const int2 le = link[e];
     if (le.y >= 0) return false;
     const int te = type_of(tg[e]);
@@ -72,28 +61,7 @@ __device__ bool growable_end(const uint32_t *tg, const int2 *link, int e, int ma
     return type_of(tg[c]) == T_H && len < max_chain;
 }
 
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_break(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                         const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const RepDev &R = reps[c.rep];
-    const long long step = *b.step;
-    if (!chem_due(R, step)) return;
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end) return;
-    const uint32_t *tg = b.tg[cur];
-    int2 *link = b.link[cur];
-    const uint32_t t0 = tg[d];
-    if (type_of(t0) != T_H) return;
-    const int t = link[d].y;
-    if (t < 0 || type_of(tg[t]) != T_T) return;
-    if (decision_word(R, step, SALT_BREAK, t0 & GID_MASK) >= R.thr_break) return;
-    link[d].y = -1;
-    link[t].x = -1;
-    const float2 p = b.pos[cur][d];
-    push_event(b, step, 1, t0 & GID_MASK, tg[t] & GID_MASK, p.x, p.y, c.rep);
-}
-
-// the 3x3 cells around bead d: calls body(j) for every other bead j
+// the 3x3 cells around position pi: calls body(j) for every bead j there
 template <typename F>
 __device__ __forceinline__ void for_neighbours(const Bufs &b, const RepDev &R, float2 pi, F body) {
     const int ncx = R.ncx, ncy = R.ncy;
@@ -109,151 +77,139 @@ __device__ __forceinline__ void for_neighbours(const Bufs &b, const RepDev &R, f
     }
 }
 
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_req(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                            const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const RepDev &R = reps[c.rep];
-    const long long step = *b.step;
-    if (!chem_due(R, step)) return;
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end) return;
-    b.req[d] = -1;
+#define LIST_GRID 148
+
+// stage 2 requests: a listed P with >= n_t_min T beads within r_grow claims its
+// nearest growable end within r_grow (req[k] = end slot or -1)
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    const int n = (int)b.status->n_grow;
     const uint32_t *tg = b.tg[cur];
-    const uint32_t t0 = tg[d];
-    if (type_of(t0) != T_P) return;
-    const uint32_t g = t0 & GID_MASK;
-    if (decision_word(R, step, SALT_GROW, g) >= R.thr_grow) return;
     const float2 *pos = b.pos[cur];
     const int2 *link = b.link[cur];
-    const float2 pi = pos[d];
-    const float L = R.L, h = R.halfL, r2 = R.r2_grow;
-    int nt = 0;
-    for_neighbours(b, R, pi, [&](int j) {
-        if (j != d && type_of(tg[j]) == T_T) {
-            const float2 pj = pos[j];
-            if (dist2(pi.x, pi.y, pj.x, pj.y, L, h) < r2) nt++;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int2 it = b.grow_list[k];
+        const int d = it.x;
+        const RepDev &R = reps[it.y];
+        const uint32_t g = tg[d] & GID_MASK;
+        const float2 pi = pos[d];
+        const float L = R.L, h = R.halfL, r2 = R.r2_grow;
+        int nt = 0;
+        for_neighbours(b, R, pi, [&](int j) {
+            if (j != d && type_of(tg[j]) == T_T) {
+                const float2 pj = pos[j];
+                if (dist2(pi.x, pi.y, pj.x, pj.y, L, h) < r2) nt++;
+            }
+        });
+        int best = -1;
+        if (nt >= R.n_t_min) {
+            float bd = 0.0f;
+            uint32_t bg = 0;
+            for_neighbours(b, R, pi, [&](int j) {
+                if (j == d) return;
+                const float2 pj = pos[j];
+                const float q = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+                if (!(q < r2)) return;
+                const uint32_t gj = tg[j] & GID_MASK;
+                if (best >= 0 && !(q < bd || (q == bd && gj < bg))) return;
+                if (!growable_end(tg, link, j, R.max_chain)) return;
+                best = j;
+                bd = q;
+                bg = gj;
+            });
         }
-    });
-    if (nt < R.n_t_min) return;
-    int best = -1;
-    float bd = 0.0f;
-    uint32_t bg = 0;
-    for_neighbours(b, R, pi, [&](int j) {
-        if (j == d) return;
-        const float2 pj = pos[j];
-        const float q = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
-        if (!(q < r2)) return;
-        const uint32_t gj = tg[j] & GID_MASK;
-        if (best >= 0 && !(q < bd || (q == bd && gj < bg))) return;
-        if (!growable_end(tg, link, j, R.max_chain, b.status)) return;
-        best = j;
-        bd = q;
-        bg = gj;
-    });
-    if (best < 0) return;
-    b.req[d] = best;
-    atomicMin(b.claim + best, g);
-}
-
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                              const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const RepDev &R = reps[c.rep];
-    const long long step = *b.step;
-    if (!chem_due(R, step)) return;
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end) return;
-    const int e = b.req[d];
-    if (e < 0) return;
-    uint32_t *tg = b.tg[cur];
-    const uint32_t g = tg[d] & GID_MASK;
-    if (b.claim[e] != g) return;  // a lower gid claimed this end
-    b.claim[e] = 0xFFFFFFFFu;
-    int2 *link = b.link[cur];
-    tg[d] = ((uint32_t)T_T << TYPE_SHIFT) | g;
-    link[d] = make_int2(e, -1);
-    link[e].y = d;
-    const float2 p = b.pos[cur][d];
-    push_event(b, step, 0, g, tg[e] & GID_MASK, p.x, p.y, c.rep);
-}
-
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_req(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                            const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const RepDev &R = reps[c.rep];
-    const long long step = *b.step;
-    if (!chem_due(R, step)) return;
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end) return;
-    b.req[d] = -1;
-    const uint32_t *tg = b.tg[cur];
-    const int2 *link = b.link[cur];
-    const uint32_t t0 = tg[d];
-    if (type_of(t0) != T_T) return;
-    const int2 lk = link[d];
-    if (lk.x >= 0 || lk.y >= 0) return;
-    const uint32_t g = t0 & GID_MASK;
-    if (decision_word(R, step, SALT_BOND, g) >= R.thr_bond) return;
-    const float2 *pos = b.pos[cur];
-    const float2 pi = pos[d];
-    const float L = R.L, h = R.halfL, r2 = R.r2_bond;
-    int best = -1;
-    float bd = 0.0f;
-    uint32_t bg = 0;
-    for_neighbours(b, R, pi, [&](int j) {
-        if (j == d) return;
-        const uint32_t tj = tg[j];
-        if (type_of(tj) != T_H) return;
-        const int2 lj = link[j];
-        if (lj.x >= 0 || lj.y >= 0) return;
-        const float2 pj = pos[j];
-        const float q = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
-        if (!(q < r2)) return;
-        const uint32_t gj = tj & GID_MASK;
-        if (best >= 0 && !(q < bd || (q == bd && gj < bg))) return;
-        best = j;
-        bd = q;
-        bg = gj;
-    });
-    if (best < 0) return;
-    b.req[d] = best;
-    atomicMin(b.claim + best, g);
-}
-
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_apply(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                              const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const RepDev &R = reps[c.rep];
-    const long long step = *b.step;
-    if (!chem_due(R, step)) return;
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end) return;
-    const int h = b.req[d];
-    if (h < 0) return;
-    const uint32_t *tg = b.tg[cur];
-    const uint32_t g = tg[d] & GID_MASK;
-    if (b.claim[h] != g) return;
-    b.claim[h] = 0xFFFFFFFFu;
-    int2 *link = b.link[cur];
-    link[h].y = d;
-    link[d].x = h;
-    const float2 p = b.pos[cur][d];
-    push_event(b, step, 2, g, tg[h] & GID_MASK, p.x, p.y, c.rep);
-}
-
-int chem_kernel_count() { return 5; }
-
-void launch_chemistry_part(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int part,
-                           cudaStream_t s) {
-    switch (part) {
-    case 0: k_chem_break<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch); break;
-    case 1: k_chem_grow_req<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch); break;
-    case 2: k_chem_grow_apply<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch); break;
-    case 3: k_chem_bond_req<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch); break;
-    default: k_chem_bond_apply<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch); break;
+        b.req[k] = best;
+        if (best >= 0) atomicMin(b.claim + best, g);
     }
 }
 
-void launch_chemistry(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
-    for (int k = 0; k < chem_kernel_count(); k++) launch_chemistry_part(b, cur, rep, bch, nbch, k, s);
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    const int n = (int)b.status->n_grow;
+    const long long step = *b.step;
+    uint32_t *tg = b.tg[cur];
+    int2 *link = b.link[cur];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int e = b.req[k];
+        if (e < 0) continue;
+        const int2 it = b.grow_list[k];
+        const int d = it.x;
+        const uint32_t g = tg[d] & GID_MASK;
+        if (b.claim[e] != g) continue;  // a lower gid claimed this end
+        b.claim[e] = 0xFFFFFFFFu;
+        tg[d] = ((uint32_t)T_T << TYPE_SHIFT) | g;
+        link[d] = make_int2(e, -1);
+        link[e].y = d;
+        const float2 p = b.pos[cur][d];
+        push_event(b, step, 0, g, tg[e] & GID_MASK, p.x, p.y, it.y);
+    }
+}
+
+// stage 3 requests: a listed T that is still free claims its nearest free H within r_bond
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    const int n = (int)b.status->n_bond;
+    const uint32_t *tg = b.tg[cur];
+    const float2 *pos = b.pos[cur];
+    const int2 *link = b.link[cur];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int2 it = b.bond_list[k];
+        const int d = it.x;
+        int best = -1;
+        const int2 lk = link[d];
+        if (type_of(tg[d]) == T_T && lk.x < 0 && lk.y < 0) {
+            const RepDev &R = reps[it.y];
+            const float2 pi = pos[d];
+            const float L = R.L, h = R.halfL, r2 = R.r2_bond;
+            float bd = 0.0f;
+            uint32_t bg = 0;
+            for_neighbours(b, R, pi, [&](int j) {
+                if (j == d) return;
+                const uint32_t tj = tg[j];
+                if (type_of(tj) != T_H) return;
+                const int2 lj = link[j];
+                if (lj.x >= 0 || lj.y >= 0) return;
+                const float2 pj = pos[j];
+                const float q = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+                if (!(q < r2)) return;
+                const uint32_t gj = tj & GID_MASK;
+                if (best >= 0 && !(q < bd || (q == bd && gj < bg))) return;
+                best = j;
+                bd = q;
+                bg = gj;
+            });
+            if (best >= 0) atomicMin(b.claim + best, tg[d] & GID_MASK);
+        }
+        b.req[k] = best;
+    }
+}
+
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_apply(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    const int n = (int)b.status->n_bond;
+    const long long step = *b.step;
+    const uint32_t *tg = b.tg[cur];
+    int2 *link = b.link[cur];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int h = b.req[k];
+        if (h < 0) continue;
+        const int2 it = b.bond_list[k];
+        const int d = it.x;
+        const uint32_t g = tg[d] & GID_MASK;
+        if (b.claim[h] != g) continue;
+        b.claim[h] = 0xFFFFFFFFu;
+        link[h].y = d;
+        link[d].x = h;
+        const float2 p = b.pos[cur][d];
+        push_event(b, step, 2, g, tg[h] & GID_MASK, p.x, p.y, it.y);
+    }
+}
+
+int chem_kernel_count() { return 4; }
+
+void launch_chem_scan(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
+    k_chem_scan<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+void launch_chem_lists(const Bufs &b, int cur, const RepDev *rep, int part, cudaStream_t s) {
+    if (part < 0 || part == 0) k_chem_grow_req<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur, rep);
+    if (part < 0 || part == 1) k_chem_grow_apply<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur, rep);
+    if (part < 0 || part == 2) k_chem_bond_req<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur, rep);
+    if (part < 0 || part == 3) k_chem_bond_apply<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur, rep);
 }

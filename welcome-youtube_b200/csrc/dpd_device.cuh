@@ -5,24 +5,41 @@
 // ---------------------------------------------------------------- counter-based RNGs
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), first output word.
-// Counter (c0, c1, c2, c3), key (k0, k1); constants from the paper.
-__device__ __forceinline__ uint32_t philox_w0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
-                                              uint32_t k1) {
+// Counter (c0, c1, c2, c3); the round keys (k0 + r W0, k1 + r W1) come
+// precomputed in ks (see PhiloxKeys); constants from the paper.
+struct PhiloxKeys {
+    uint32_t k0[10], k1[10];
+};
+
+__device__ __forceinline__ PhiloxKeys philox_keys(uint32_t k0, uint32_t k1) {
+    PhiloxKeys ks;
 #pragma unroll
     for (int r = 0; r < 10; r++) {
-        if (r > 0) {
-            k0 += 0x9E3779B9u;
-            k1 += 0xBB67AE85u;
-        }
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
-        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        ks.k0[r] = k0 + (uint32_t)r * 0x9E3779B9u;
+        ks.k1[r] = k1 + (uint32_t)r * 0xBB67AE85u;
+    }
+    return ks;
+}
+
+__device__ __forceinline__ uint32_t philox_w0k(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                               const PhiloxKeys &ks) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ ks.k0[r];
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ ks.k1[r];
+        c1 = (uint32_t)p1;
+        c3 = (uint32_t)p0;
         c0 = n0;
-        c1 = lo1;
         c2 = n2;
-        c3 = lo0;
     }
     return c0;
+}
+
+__device__ __forceinline__ uint32_t philox_w0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                              uint32_t k1) {
+    return philox_w0k(c0, c1, c2, c3, philox_keys(k0, k1));
 }
 
 // splitmix64 finaliser of the reference (cel/engine/oercel.c:124-128)
@@ -43,15 +60,15 @@ __device__ __forceinline__ uint64_t step_seed(uint64_t seed, long long step) {
 // noise 0: Philox word 0 at counter (min gid, max gid, step), key = seed;
 // noise 1: the reference's mix13 pair hash (oercel.c:137-141), top 32 bits.
 struct NoiseKey {
-    uint32_t k0, k1, s0, s1;   // Philox key and step words
+    PhiloxKeys ks;             // Philox round keys of the seed
+    uint32_t s0, s1;           // step words of the counter
     uint64_t sseed;            // mix13 per-step key
     int mode;
 };
 
 __device__ __forceinline__ NoiseKey make_noise_key(const RepDev &R, long long step) {
     NoiseKey k;
-    k.k0 = (uint32_t)R.seed;
-    k.k1 = (uint32_t)(R.seed >> 32);
+    k.ks = philox_keys((uint32_t)R.seed, (uint32_t)(R.seed >> 32));
     k.s0 = (uint32_t)(unsigned long long)step;
     k.s1 = (uint32_t)((unsigned long long)step >> 32);
     k.mode = R.noise;
@@ -66,7 +83,7 @@ __device__ __forceinline__ float pair_theta(const NoiseKey &k, uint32_t gi, uint
         const uint64_t key = ((uint64_t)lo << 32) | hi;
         u = (int32_t)(uint32_t)(mix13((key * 0x9e3779b97f4a7c15ULL) ^ k.sseed) >> 32);
     } else {
-        u = (int32_t)philox_w0(lo, hi, k.s0, k.s1, k.k0, k.k1);
+        u = (int32_t)philox_w0k(lo, hi, k.s0, k.s1, k.ks);
     }
     return __fmul_rn(__int2float_rn(u), THETA_SCALE);
 }
@@ -77,13 +94,25 @@ __device__ __forceinline__ uint32_t decision_word(const RepDev &R, long long ste
                      (uint32_t)R.seed, (uint32_t)(R.seed >> 32));
 }
 
+// ---------------------------------------------------------------- the pair force
+
+// 1/r and r from r^2 with the hardware reciprocal square root: r^2 -> (r, 1/r)
+__device__ __forceinline__ void r_and_ir(float r2, float &r, float &ir) {
+    ir = rsqrtf(r2);
+    r = __fmul_rn(r2, ir);
+}
+
 // ---------------------------------------------------------------- fixed-point force sums
 
-// Each pair or bond term is rounded once to a multiple of 2^-32 and summed in
-// int64: the sum does not depend on the order of the terms, and the two
-// halves of a pair, computed with exactly negated operands, cancel exactly.
-__device__ __forceinline__ long long f2fix(float v) { return __float2ll_rn(__fmul_rn(v, 4294967296.0f)); }
-__device__ __forceinline__ float fix2f(long long a) { return __fmul_rn(__ll2float_rn(a), 2.3283064365386963e-10f); }
+// Each pair or bond term is rounded once to a multiple of 2^-16 (a 32-bit
+// integer) and the terms are summed in integers: the sum does not depend on the
+// order of the terms, and the two halves of a pair, computed with exactly
+// negated operands, cancel exactly.  A bead's sum stays far below 2^31 (|F| <
+// 32768) for any physical state; a single term above 2048 raises a flag.
+#define FIX_TERM_LIMIT (1 << 27)
+__device__ __forceinline__ int f2fix16(float v) { return __float2int_rn(__fmul_rn(v, 65536.0f)); }
+__device__ __forceinline__ float fix16_to_f(int a) { return __fmul_rn(__int2float_rn(a), 1.52587890625e-05f); }
+__device__ __forceinline__ float fix16_to_f(long long a) { return __fmul_rn(__ll2float_rn(a), 1.52587890625e-05f); }
 
 // ---------------------------------------------------------------- cells and the integrator
 

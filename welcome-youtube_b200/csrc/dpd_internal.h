@@ -34,6 +34,8 @@
 #define DPD_F_EVENTS 0x4u       // event buffer overflow
 #define DPD_F_CHAIN 0x8u        // broken chain link found
 #define DPD_F_BIGCELL 0x10u     // a cell held more beads than the in-register sort handles (slow path used)
+#define DPD_F_TILE 0x20u        // a cell tile held more beads than its shared-memory capacity
+#define DPD_F_FORCE 0x40u       // a single pair or bond force term above the fixed-point range
 
 struct RepDev {                 // constants of one replica, read by every kernel
     float L, halfL;
@@ -57,11 +59,17 @@ struct Chunk {                  // one CTA's work: packed indices [begin, end) o
     int32_t rep, begin, end, pad;
 };
 
+struct TileDesc {               // one CTA of the tiled force kernel: cells [cx0, cx0+w) x [cy0, cy0+h)
+    int32_t rep, cx0, cy0, w, h, pad0, pad1, pad2;
+};
+
 struct DevStatus {
     unsigned int flags;
     unsigned int nevents;       // events appended (may exceed the capacity)
     unsigned int bigcell;       // largest cell population seen by the sort fix-up
-    unsigned int pad;
+    unsigned int n_grow;        // chemistry candidate lists of this step
+    unsigned int n_bond;
+    unsigned int pad[3];
 };
 
 struct EventDev {
@@ -88,7 +96,9 @@ struct Bufs {
     int32_t *cstart;            // C + 1
     int32_t *bsum;              // scan block totals
     uint32_t *claim;            // per bead, 0xFFFFFFFF when unclaimed
-    int32_t *req;               // per bead chemistry request target (-1 none)
+    int32_t *req;               // per candidate chemistry request target (-1 none)
+    int2 *grow_list;            // (slot, replica) of P beads whose growth draw succeeded
+    int2 *bond_list;            // (slot, replica) of T beads whose bonding draw succeeded
     EventDev *events;
     int32_t evcap;
     DevStatus *status;
@@ -113,7 +123,7 @@ void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
 void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
-                        cudaStream_t s);
+                        bool virial, cudaStream_t s);
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
                       int tb, float rmax, int nbin, cudaStream_t s);
 void launch_pack(const Bufs &b, int cur, int b0, int n, const float *x, const float *y, const float *vx,
@@ -124,7 +134,12 @@ void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, fl
                    cudaStream_t s);
 void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
                          const float *fx, const float *fy, cudaStream_t s);
+void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
+                        bool next_keys, cudaStream_t s);
+int tile_setup();
+size_t tile_smem_bytes();
 int chem_kernel_count();
-void launch_chemistry(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
-void launch_chemistry_part(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int part,
-                           cudaStream_t s);
+// the break stage and the candidate draws on the current sorted state (phase entry point)
+void launch_chem_scan(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
+// the growth and bonding stages over the candidate lists (part 0..3, or all with part < 0)
+void launch_chem_lists(const Bufs &b, int cur, const RepDev *rep, int part, cudaStream_t s);

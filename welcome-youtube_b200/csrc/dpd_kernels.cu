@@ -11,7 +11,7 @@
 //                      cell of the next position and its atomic count
 // so the bead state is read and written once per kernel and the sort keys for
 // step n+1 come out of the force kernel of step n.
-#include "dpd_device.cuh"
+#include "dpd_chem.cuh"
 
 // ---------------------------------------------------------------- keys (prime / build_cells)
 
@@ -71,7 +71,8 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *total) {
 // block-local exclusive scan; counts are consumed and zeroed for the next step
 __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count, int32_t *__restrict__ cstart,
                                                     int32_t *__restrict__ bsum, long long C,
-                                                    long long *__restrict__ step, int step_inc) {
+                                                    long long *__restrict__ step, int step_inc,
+                                                    DevStatus *__restrict__ status) {
     const long long base = (long long)blockIdx.x * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
     int v[SCAN_PER_THREAD];
     int s = 0;
@@ -109,7 +110,11 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count
     }
     if (threadIdx.x == 0) {
         bsum[blockIdx.x] = total;
-        if (step_inc && blockIdx.x == 0) *step += 1;
+        if (step_inc && blockIdx.x == 0) {
+            *step += 1;
+            status->n_grow = 0u;  // the chemistry candidate lists of the new step start empty
+            status->n_bond = 0u;
+        }
     }
 }
 
@@ -251,10 +256,16 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
         b.vt[nxt][d] = b.vt[cur][i];
         b.f[nxt][d] = b.f[cur][i];
     }
+    int2 nl = make_int2(lk.x >= 0 ? b.dest[lk.x] : -1, lk.y >= 0 ? b.dest[lk.y] : -1);
+    if (MODE == PERM_STEP) {
+        const RepDev &R = reps[c.rep];
+        const long long step = *b.step;
+        if (chem_due(R, step)) chem_in_permute(b, cur, R, step, c.rep, d, p, tg, lk, nl);
+    }
     b.pos[nxt][d] = p;
     b.vh[nxt][d] = vh;
     b.tg[nxt][d] = tg;
-    b.link[nxt][d] = make_int2(lk.x >= 0 ? b.dest[lk.x] : -1, lk.y >= 0 ? b.dest[lk.y] : -1);
+    b.link[nxt][d] = nl;
 }
 
 // ---------------------------------------------------------------- pair + bond forces
@@ -266,10 +277,55 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
 // so F_ij = -F_ji and sum F = 0 hold exactly and the result does not depend on
 // the order of the loops.  NEXTKEY: also the cell of x + dt vh + dt^2 F and
 // its count, i.e. the first half of the next step's sort.
+// one pair term on bead i from bead j in fixed point; dx = minimg(x_i - x_j),
+// which equals (x_i - x_j) + shift of the cell stencil bit for bit
+struct PairCtx {
+    const float2 *__restrict__ pos;
+    const float2 *__restrict__ vt;
+    const uint32_t *__restrict__ tg;
+    const float *arow;
+    NoiseKey nk;
+    float2 pi, vi;
+    uint32_t gi;
+    float L, h, gam, sdt;
+};
+
+__device__ __forceinline__ void pair_term(const PairCtx &c, int j, long long &ax, long long &ay) {
+    const float2 pj = c.pos[j];
+    const float dx = minimg(__fsub_rn(c.pi.x, pj.x), c.L, c.h);
+    const float dy = minimg(__fsub_rn(c.pi.y, pj.y), c.L, c.h);
+    const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+    const float2 vj = c.vt[j];
+    const uint32_t tgj = c.tg[j];
+    float r, ir;
+    r_and_ir(r2, r, ir);
+    const float w = __fsub_rn(1.0f, r);
+    const float dvx = __fsub_rn(c.vi.x, vj.x), dvy = __fsub_rn(c.vi.y, vj.y);
+    const float rv = __fmul_rn(__fmaf_rn(dx, dvx, __fmul_rn(dy, dvy)), ir);
+    const float th = pair_theta(c.nk, c.gi, tgj & GID_MASK);
+    const float inner = __fmaf_rn(c.sdt, th, __fmaf_rn(-__fmul_rn(c.gam, w), rv, c.arow[tgj >> TYPE_SHIFT]));
+    const float fm = __fmul_rn(__fmul_rn(w, inner), ir);
+    ax += f2fix16(__fmul_rn(fm, dx));
+    ay += f2fix16(__fmul_rn(fm, dy));
+}
+
+#define MAXHIT 32
+
+// Per bead d: F_d = sum_j w [a_ij - gamma w (rhat . vt_ij) + sigma theta_ij / sqrt(dt)] rhat
+// over the 3x3 neighbour cells (w = 1 - r, r < 1; oercel.c:970-981) plus the
+// harmonic bonds to prev/next (oercel.c:1272-1308).  Every pair is evaluated
+// by both of its beads with exactly negated operands and summed in fixed point,
+// so F_ij = -F_ji and sum F = 0 hold exactly and the result does not depend on
+// the order of the loops.  The candidates of a thread are first screened
+// (r < 1) into a per-thread list in shared memory, then the list is evaluated,
+// so the expensive part (noise + force) runs without warp divergence on the
+// cutoff test.  NEXTKEY: also the cell of x + dt vh + dt^2 F and its count,
+// i.e. the first half of the next step's sort.
 template <bool PAIR, bool BOND, bool NEXTKEY>
 __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                      const Chunk *__restrict__ ch) {
     __shared__ float a_sh[DPD_MAXT * DPD_MAXT];
+    __shared__ int hl[PAIR ? MAXHIT : 1][BEAD_TPB];
     const Chunk c = ch[blockIdx.x];
     const RepDev &R = reps[c.rep];
     if (threadIdx.x < DPD_MAXT * DPD_MAXT) a_sh[threadIdx.x] = R.a[threadIdx.x];
@@ -284,18 +340,25 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
         const float2 pi = pos[d];
         const float L = R.L;
         if (PAIR) {
-            const float2 *__restrict__ vt = b.vt[cur];
-            const uint32_t *__restrict__ tg = b.tg[cur];
-            const float2 vi = vt[d];
-            const uint32_t tgi = tg[d];
-            const uint32_t gi = tgi & GID_MASK;
-            const float *arow = a_sh + (tgi >> TYPE_SHIFT) * DPD_MAXT;
-            const NoiseKey nk = make_noise_key(R, *b.step);
-            const float gam = R.gamma, sdt = R.sdt;
+            PairCtx pc;
+            pc.pos = pos;
+            pc.vt = b.vt[cur];
+            pc.tg = b.tg[cur];
+            pc.pi = pi;
+            pc.vi = pc.vt[d];
+            const uint32_t tgi = pc.tg[d];
+            pc.gi = tgi & GID_MASK;
+            pc.arow = a_sh + (tgi >> TYPE_SHIFT) * DPD_MAXT;
+            pc.nk = make_noise_key(R, *b.step);
+            pc.L = L;
+            pc.h = R.halfL;
+            pc.gam = R.gamma;
+            pc.sdt = R.sdt;
             const int ncx = R.ncx, ncy = R.ncy;
             const int32_t *__restrict__ cs = b.cstart + R.c0;
             int cx, cy;
             cell_xy(R, pi.x, pi.y, cx, cy);
+            int nh = 0;
 #pragma unroll 1
             for (int ox = -1; ox <= 1; ox++) {
                 int nx = cx + ox;
@@ -331,30 +394,23 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
                 for (int seg = 0; seg < 2; seg++) {
                     const int js = seg ? s1 : s0, je = seg ? e1 : e0;
                     const float sy = seg ? sy1 : sy0;
-#pragma unroll 1
+#pragma unroll 4
                     for (int j = js; j < je; j++) {
                         const float2 pj = pos[j];
                         const float dx = __fadd_rn(__fsub_rn(pi.x, pj.x), sx);
                         const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
                         const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
                         if (r2 < 1.0f && r2 > 1e-24f && j != d) {
-                            const float2 vj = vt[j];
-                            const uint32_t tgj = tg[j];
-                            const float r = __fsqrt_rn(r2);
-                            const float ir = __frcp_rn(r);
-                            const float w = __fsub_rn(1.0f, r);
-                            const float dvx = __fsub_rn(vi.x, vj.x), dvy = __fsub_rn(vi.y, vj.y);
-                            const float rv = __fmul_rn(__fmaf_rn(dx, dvx, __fmul_rn(dy, dvy)), ir);
-                            const float th = pair_theta(nk, gi, tgj & GID_MASK);
-                            const float inner = __fmaf_rn(sdt, th, __fmaf_rn(-__fmul_rn(gam, w), rv,
-                                                                            arow[tgj >> TYPE_SHIFT]));
-                            const float fm = __fmul_rn(__fmul_rn(w, inner), ir);
-                            ax += f2fix(__fmul_rn(fm, dx));
-                            ay += f2fix(__fmul_rn(fm, dy));
+                            if (nh < MAXHIT) hl[nh][threadIdx.x] = j;
+                            else pair_term(pc, j, ax, ay);  // crowded neighbourhood: evaluate at once
+                            nh++;
                         }
                     }
                 }
             }
+            const int nl = min(nh, MAXHIT);
+#pragma unroll 1
+            for (int k = 0; k < nl; k++) pair_term(pc, hl[k][threadIdx.x], ax, ay);
         }
         if (BOND) {
             const int2 lk = b.link[cur][d];
@@ -368,11 +424,11 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
                 const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
                 mb = fmaxf(mb, r);
                 const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
-                ax += f2fix(__fmul_rn(fb, dx));
-                ay += f2fix(__fmul_rn(fb, dy));
+                ax += f2fix16(__fmul_rn(fb, dx));
+                ay += f2fix16(__fmul_rn(fb, dy));
             }
         }
-        const float2 fs = make_float2(fix2f(ax), fix2f(ay));
+        const float2 fs = make_float2(fix16_to_f(ax), fix16_to_f(ay));
         if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);
         b.f[cur][d] = fs;
         if (NEXTKEY) {
@@ -427,6 +483,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_integrate(Bufs b, int cur, const R
 // per-bead sums (momentum, kinetic energy, type counts, chain heads) and the
 // conservative virial over each unordered pair once; fixed-point integer
 // atomics make the result independent of the launch shape.
+template <bool VIRIAL>
 __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const Chunk *__restrict__ ch, int rep_index) {
     const Chunk c = ch[blockIdx.x];
@@ -447,6 +504,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
         const int2 lk = b.link[cur][d];
         heads = (lk.x < 0 && lk.y >= 0) ? 1 : 0;
         // virial: pairs (d, j) with j > d inside the cutoff
+        if (VIRIAL) {
         const float2 *__restrict__ pos = b.pos[cur];
         const float2 pi = pos[d];
         const int ncx = R.ncx, ncy = R.ncy;
@@ -470,6 +528,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
                 }
             }
         vir = __double2ll_rn(accv * OBS_FIX);
+        }
     }
     unsigned long long *o = b.obs + (size_t)rep_index * OBS_N;
     sx = warp_sum_ll(sx);
@@ -592,7 +651,8 @@ void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, in
 
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s) {
     const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
-    if (part == 1) k_scan1<<<nb, SCAN_TPB, 0, s>>>(b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0);
+    if (part == 1)
+        k_scan1<<<nb, SCAN_TPB, 0, s>>>(b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0, b.status);
     else k_scan2<<<nb, SCAN_TPB, 0, s>>>(b.cstart, b.bsum, (long long)C, nb);
 }
 
@@ -633,8 +693,9 @@ void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bc
 }
 
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
-                        cudaStream_t s) {
-    k_observables<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
+                        bool virial, cudaStream_t s) {
+    if (virial) k_observables<true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
+    else k_observables<false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
 }
 
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,

@@ -39,6 +39,11 @@ class DpdParams(C.Structure):
     ]
 
 
+class DpdTuning(C.Structure):
+    _fields_ = [("force_kernel", C.c_int32), ("tile_w", C.c_int32), ("tile_h", C.c_int32),
+                ("graph_steps", C.c_int32)]
+
+
 class DpdEvent(C.Structure):
     _fields_ = [("step", C.c_int64), ("kind", C.c_int32), ("gid", C.c_uint32), ("partner", C.c_uint32),
                 ("x", C.c_float), ("y", C.c_float), ("replica", C.c_int32)]
@@ -50,7 +55,7 @@ EXPORTS = [
     "dpd_set_step", "dpd_step", "dpd_init_soup", "dpd_build_cells", "dpd_get_cells", "dpd_forces",
     "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events",
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
-    "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step",
+    "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
 ]
 
 _lib = None
@@ -61,7 +66,7 @@ def load(path: str | None = None):
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    path = path or os.environ.get("DPD_LIB") or LIB_PATH
     if path == LIB_PATH:
         try:
             import importlib.util
@@ -105,6 +110,9 @@ def load(path: str | None = None):
         "dpd_chemistry": ([vp, i64], C.c_int),
         "dpd_get_events": ([vp, C.POINTER(DpdEvent), i32, C.POINTER(C.c_int32)], C.c_int),
         "dpd_observables": ([vp, i32, fp], C.c_int),
+        "dpd_stats": ([vp, i32, fp], C.c_int),
+        "dpd_set_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),
+        "dpd_get_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),
         "dpd_pair_hist": ([vp, i32, i32, i32, dbl, i32, fp], C.c_int),
         "dpd_get_stream": ([vp, C.POINTER(vp)], C.c_int),
         "dpd_kernels_per_step": ([vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),

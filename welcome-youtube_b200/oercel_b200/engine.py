@@ -145,6 +145,17 @@ class Engine:
     def set_graph_steps(self, n):
         check(self.lib.dpd_set_graph_steps(self.h, int(n)))
 
+    def tuning(self):
+        t = _capi.DpdTuning()
+        check(self.lib.dpd_get_tuning(self.h, C.byref(t)))
+        return dict(force_kernel=t.force_kernel, tile_w=t.tile_w, tile_h=t.tile_h, graph_steps=t.graph_steps)
+
+    def set_tuning(self, **kv):
+        cur = self.tuning()
+        cur.update(kv)
+        t = _capi.DpdTuning(int(cur["force_kernel"]), int(cur["tile_w"]), int(cur["tile_h"]), int(cur["graph_steps"]))
+        check(self.lib.dpd_set_tuning(self.h, C.byref(t)))
+
     def profile_step(self):
         """device time (ms) of each kernel of one real step, in launch order"""
         ms = (C.c_float * 32)()
@@ -188,15 +199,19 @@ class Engine:
         check(self.lib.dpd_chemistry(self.h, int(step)))
 
     # ---------------------------------------------------------------- outputs
-    def events(self, cap=1 << 20):
-        buf = (DpdEvent * cap)()
+    def events(self):
+        """(step, kind, gid, partner gid, x, y, replica) of the events since the last call"""
         n = C.c_int32()
+        check(self.lib.dpd_get_events(self.h, None, 0, C.byref(n)))
+        cap = max(n.value, 1)
+        buf = (DpdEvent * cap)()
         check(self.lib.dpd_get_events(self.h, buf, cap, C.byref(n)))
         return [(e.step, e.kind, e.gid, e.partner, e.x, e.y, e.replica) for e in buf[: n.value]]
 
-    def observables(self, replica=0):
+    def observables(self, replica=0, virial=True):
         o = np.zeros(16)
-        check(self.lib.dpd_observables(self.h, replica, ptr(o)))
+        f = self.lib.dpd_observables if virial else self.lib.dpd_stats
+        check(f(self.h, replica, ptr(o)))
         return dict(T=o[0], px=o[1], py=o[2], virial=o[3], maxbond=o[4], n_chains=int(o[5]),
                     counts=o[8:16].astype(np.int64))
 
