@@ -47,3 +47,16 @@ def test_tuning_validation(cuda_ok):
     with pytest.raises(ob.DpdError):
         e.set_tuning(tile_w=20, tile_h=20)
     assert e.tuning()["tile_w"] == 8
+
+
+def test_autotune_picks_a_valid_choice(cuda_ok, tmp_path):
+    from oercel_b200.autotune import autotune
+    p = params(L=48.0, seed=2, noise="philox")
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    out = autotune(e, repeats=1, cache_path=str(tmp_path / "t.json"))
+    assert out["tuning"]["force_kernel"] in (0, 1) and out["forces_ms"] > 0
+    again = autotune(e, cache_path=str(tmp_path / "t.json"))  # from the cache
+    assert again["tuning"] == out["tuning"]
+    e.step(5)

@@ -249,7 +249,7 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
         TRY(dalloc(h, &b.link[k], N));
     }
     TRY(dalloc(h, &b.key, N));
-    TRY(dalloc(h, &b.rank, N));
+    TRY(dalloc(h, &b.fill, C + 4));
     TRY(dalloc(h, &b.src, N));
     TRY(dalloc(h, &b.dest, N));
     TRY(dalloc(h, &b.count, C + 4));

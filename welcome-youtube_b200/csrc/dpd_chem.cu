@@ -61,67 +61,114 @@ __device__ bool growable_end(const uint32_t *tg, const int2 *link, int e, int ma
     return type_of(tg[c]) == T_H && len < max_chain;
 }
 
-// the 3x3 cells around position pi: calls body(j) for every bead j there
-template <typename F>
-__device__ __forceinline__ void for_neighbours(const Bufs &b, const RepDev &R, float2 pi, F body) {
+// the 3x3 cells around position pi as contiguous slot ranges: per column the
+// rows cy-1..cy+1 are one range, or two where the rows wrap
+struct NbrRanges {
+    int s[6], e[6];
+    int n, total;
+};
+
+__device__ __forceinline__ NbrRanges nbr_ranges(const Bufs &b, const RepDev &R, float2 pi) {
+    NbrRanges q;
     const int ncx = R.ncx, ncy = R.ncy;
     const int32_t *cs = b.cstart + R.c0;
     int cx, cy;
     cell_xy(R, pi.x, pi.y, cx, cy);
+    q.n = 0;
+    q.total = 0;
+#pragma unroll
     for (int ox = -1; ox <= 1; ox++) {
-        const int nx = (cx + ox + ncx) % ncx;
-        for (int oy = -1; oy <= 1; oy++) {
-            const int cc = nx * ncy + (cy + oy + ncy) % ncy;
-            for (int j = cs[cc]; j < cs[cc + 1]; j++) body(j);
+        const int col = ((cx + ox + ncx) % ncx) * ncy;
+        if (cy >= 1 && cy + 1 < ncy) {
+            q.s[q.n] = cs[col + cy - 1];
+            q.e[q.n++] = cs[col + cy + 2];
+        } else if (cy == 0) {
+            q.s[q.n] = cs[col + ncy - 1];
+            q.e[q.n++] = cs[col + ncy];
+            q.s[q.n] = cs[col];
+            q.e[q.n++] = cs[col + 2];
+        } else {
+            q.s[q.n] = cs[col + cy - 1];
+            q.e[q.n++] = cs[col + ncy];
+            q.s[q.n] = cs[col];
+            q.e[q.n++] = cs[col + 1];
         }
     }
+    for (int k = 0; k < q.n; k++) q.total += q.e[k] - q.s[k];
+    return q;
+}
+
+// slot of the f-th bead of the ranges
+__device__ __forceinline__ int nbr_slot(const NbrRanges &q, int f) {
+    int k = 0;
+    while (f >= q.e[k] - q.s[k]) {
+        f -= q.e[k] - q.s[k];
+        k++;
+    }
+    return q.s[k] + f;
+}
+
+// warp minimum of a 64-bit key (distance bits, gid): the lexicographic nearest
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
 }
 
 #define LIST_GRID 148
+#define NONE_KEY 0xFFFFFFFFFFFFFFFFull
 
-// stage 2 requests: a listed P with >= n_t_min T beads within r_grow claims its
-// nearest growable end within r_grow (req[k] = end slot or -1)
+// stage 2 requests, one warp per listed P: it needs >= n_t_min T beads within
+// r_grow and claims its nearest growable end within r_grow (req[k] = end or -1)
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
     const int n = (int)b.status->n_grow;
     const uint32_t *tg = b.tg[cur];
     const float2 *pos = b.pos[cur];
     const int2 *link = b.link[cur];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int lane = (int)lane_id();
+    const int nw = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < n; k += nw) {
         const int2 it = b.grow_list[k];
         const int d = it.x;
         const RepDev &R = reps[it.y];
-        const uint32_t g = tg[d] & GID_MASK;
         const float2 pi = pos[d];
         const float L = R.L, h = R.halfL, r2 = R.r2_grow;
+        const NbrRanges q = nbr_ranges(b, R, pi);
         int nt = 0;
-        for_neighbours(b, R, pi, [&](int j) {
-            if (j != d && type_of(tg[j]) == T_T) {
-                const float2 pj = pos[j];
-                if (dist2(pi.x, pi.y, pj.x, pj.y, L, h) < r2) nt++;
-            }
-        });
-        int best = -1;
-        if (nt >= R.n_t_min) {
-            float bd = 0.0f;
-            uint32_t bg = 0;
-            for_neighbours(b, R, pi, [&](int j) {
-                if (j == d) return;
-                const float2 pj = pos[j];
-                const float q = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
-                if (!(q < r2)) return;
-                const uint32_t gj = tg[j] & GID_MASK;
-                if (best >= 0 && !(q < bd || (q == bd && gj < bg))) return;
-                if (!growable_end(tg, link, j, R.max_chain)) return;
-                best = j;
-                bd = q;
-                bg = gj;
-            });
+        unsigned long long best = NONE_KEY;
+        for (int f = lane; f < q.total; f += 32) {
+            const int j = nbr_slot(q, f);
+            if (j == d) continue;
+            const float2 pj = pos[j];
+            const float dd = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+            if (!(dd < r2)) continue;
+            const uint32_t tj = tg[j];
+            nt += type_of(tj) == T_T;
+            const unsigned long long key = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
+            if (key < best && growable_end(tg, link, j, R.max_chain)) best = key;
         }
-        b.req[k] = best;
-        if (best >= 0) atomicMin(b.claim + best, g);
+        nt = (int)__reduce_add_sync(0xffffffffu, (unsigned)nt);
+        best = warp_min_u64(best);
+        int e = -1;
+        if (nt >= R.n_t_min && best != NONE_KEY) {
+            // the slot of the winning end: the lane that holds it reports it
+            for (int f = lane; f < q.total; f += 32) {
+                const int j = nbr_slot(q, f);
+                if (j != d && (tg[j] & GID_MASK) == (uint32_t)(best & 0xFFFFFFFFu)) e = j;
+            }
+            e = (int)__reduce_max_sync(0xffffffffu, (unsigned)(e + 1)) - 1;
+        }
+        if (lane == 0) {
+            b.req[k] = e;
+            if (e >= 0) atomicMin(b.claim + e, tg[d] & GID_MASK);
+        }
     }
 }
 
+// stage 2 application, one thread per listed P: the lowest claiming gid wins its end
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur, const RepDev *__restrict__ reps) {
     const int n = (int)b.status->n_grow;
     const long long step = *b.step;
@@ -143,41 +190,51 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur, c
     }
 }
 
-// stage 3 requests: a listed T that is still free claims its nearest free H within r_bond
+// stage 3 requests, one warp per listed T: if still free it claims its nearest
+// free H within r_bond
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
     const int n = (int)b.status->n_bond;
     const uint32_t *tg = b.tg[cur];
     const float2 *pos = b.pos[cur];
     const int2 *link = b.link[cur];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int lane = (int)lane_id();
+    const int nw = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < n; k += nw) {
         const int2 it = b.bond_list[k];
         const int d = it.x;
-        int best = -1;
         const int2 lk = link[d];
+        int e = -1;
         if (type_of(tg[d]) == T_T && lk.x < 0 && lk.y < 0) {
             const RepDev &R = reps[it.y];
             const float2 pi = pos[d];
             const float L = R.L, h = R.halfL, r2 = R.r2_bond;
-            float bd = 0.0f;
-            uint32_t bg = 0;
-            for_neighbours(b, R, pi, [&](int j) {
-                if (j == d) return;
+            const NbrRanges q = nbr_ranges(b, R, pi);
+            unsigned long long best = NONE_KEY;
+            int bj = -1;
+            for (int f = lane; f < q.total; f += 32) {
+                const int j = nbr_slot(q, f);
+                if (j == d) continue;
                 const uint32_t tj = tg[j];
-                if (type_of(tj) != T_H) return;
+                if (type_of(tj) != T_H) continue;
                 const int2 lj = link[j];
-                if (lj.x >= 0 || lj.y >= 0) return;
+                if (lj.x >= 0 || lj.y >= 0) continue;
                 const float2 pj = pos[j];
-                const float q = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
-                if (!(q < r2)) return;
-                const uint32_t gj = tj & GID_MASK;
-                if (best >= 0 && !(q < bd || (q == bd && gj < bg))) return;
-                best = j;
-                bd = q;
-                bg = gj;
-            });
-            if (best >= 0) atomicMin(b.claim + best, tg[d] & GID_MASK);
+                const float dd = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+                if (!(dd < r2)) continue;
+                const unsigned long long key = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
+                if (key < best) {
+                    best = key;
+                    bj = j;
+                }
+            }
+            const unsigned long long wbest = warp_min_u64(best);
+            const int mine = (best == wbest && wbest != NONE_KEY) ? bj : -1;
+            e = (int)__reduce_max_sync(0xffffffffu, (unsigned)(mine + 1)) - 1;
         }
-        b.req[k] = best;
+        if (lane == 0) {
+            b.req[k] = e;
+            if (e >= 0) atomicMin(b.claim + e, tg[d] & GID_MASK);
+        }
     }
 }
 

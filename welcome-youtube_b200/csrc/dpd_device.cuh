@@ -146,21 +146,9 @@ __device__ __forceinline__ float minimg(float d, float L, float h) {
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
-// warp-aggregated atomic count: every active lane gets its provisional rank
-// in the cell `key`; all 32 lanes of the warp must call this together.
-__device__ __forceinline__ uint32_t count_key(uint32_t *count, uint32_t key, bool active) {
-    const unsigned valid = __ballot_sync(0xffffffffu, active);
-    uint32_t rank = 0;
-    if (active) {
-        const unsigned peers = __match_any_sync(valid, key);
-        const int lane = (int)lane_id();
-        const int leader = __ffs(peers) - 1;
-        unsigned base = 0;
-        if (lane == leader) base = atomicAdd(count + key, (unsigned)__popc(peers));
-        base = __shfl_sync(peers, base, leader);
-        rank = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
-    }
-    return rank;
+// count a bead into its next cell (no value returned: the add is fire-and-forget)
+__device__ __forceinline__ void count_key(uint32_t *count, uint32_t key, bool active) {
+    if (active) atomicAdd(count + key, 1u);
 }
 
 __device__ __forceinline__ long long warp_sum_ll(long long v) {

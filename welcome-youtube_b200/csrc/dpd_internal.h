@@ -9,11 +9,11 @@
 //     f    float2  force of the current configuration
 //     tg   u32     type << 29 | gid  (gid < 2^29)
 //     link int2    prev, next slot of the bonded neighbours (-1 = none)
-//   per bead, single: key (cell of the next position), rank (provisional
-//     place in that cell), src (old slot of each new slot), dest (inverse),
-//     req/claim (chemistry requests)
+//   per bead, single: key (cell of the next position), src (old slot of each
+//     new slot), dest (inverse), req/claim (chemistry requests)
 //   per cell: count (beads whose next position falls in the cell), cstart
-//     (exclusive scan of count; cstart of the packed cell C_total = N)
+//     (exclusive scan of count; cstart of the packed cell C_total = N), fill
+//     (placement cursor)
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -90,7 +90,8 @@ struct Bufs {
     float2 *pos[2], *vh[2], *vt[2], *f[2];
     uint32_t *tg[2];
     int2 *link[2];
-    uint32_t *key, *rank;
+    uint32_t *key;
+    uint32_t *fill;             // per cell: next free slot while beads are placed (cstart + count so far)
     int32_t *src, *dest;
     uint32_t *count;
     int32_t *cstart;            // C + 1

@@ -2,7 +2,7 @@
 //
 // One step of the production path (dpd_step) is
 //   k_scan1, k_scan2   exclusive scan of the per-cell counts of the NEXT positions
-//   k_place            provisional slot of every bead: cstart[key] + rank
+//   k_place            provisional slot of every bead: an atomic cursor per cell
 //   k_cellfix          per cell: order its beads by old slot (stable sort), dest[]
 //   k_permute          gather the old slots into the new order AND apply the
 //                      Groot-Warren update (fused; oercel.c:2303-2334 + 832-933)
@@ -33,11 +33,8 @@ __global__ void __launch_bounds__(BEAD_TPB) k_keys(Bufs b, int cur, const RepDev
         int cx, cy;
         key = (uint32_t)(R.c0 + cell_xy(R, p.x, p.y, cx, cy));
     }
-    const uint32_t rank = count_key(b.count, key, act);
-    if (act) {
-        b.key[i] = key;
-        b.rank[i] = rank;
-    }
+    count_key(b.count, key, act);
+    if (act) b.key[i] = key;
 }
 
 // ---------------------------------------------------------------- scan of the cell counts
@@ -119,8 +116,8 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count
 }
 
 // add the totals of all earlier blocks; the last block writes cstart[C]
-__global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart, const int32_t *__restrict__ bsum,
-                                                    long long C, int nblocks) {
+__global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart, uint32_t *__restrict__ fill,
+                                                    const int32_t *__restrict__ bsum, long long C, int nblocks) {
     __shared__ int red[SCAN_TPB / 32];
     int part = 0;
     for (int k = (int)threadIdx.x; k < (int)blockIdx.x; k += SCAN_TPB) part += bsum[k];
@@ -132,19 +129,21 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart
 #pragma unroll
     for (int w = 0; w < SCAN_TPB / 32; w++) prefix += red[w];
     const long long base = (long long)blockIdx.x * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
-    if (prefix != 0) {
-        if (base + SCAN_PER_THREAD <= C) {
-            int4 o = *reinterpret_cast<const int4 *>(cstart + base);
-            o.x += prefix;
-            o.y += prefix;
-            o.z += prefix;
-            o.w += prefix;
-            *reinterpret_cast<int4 *>(cstart + base) = o;
-        } else {
+    if (base + SCAN_PER_THREAD <= C) {
+        int4 o = *reinterpret_cast<const int4 *>(cstart + base);
+        o.x += prefix;
+        o.y += prefix;
+        o.z += prefix;
+        o.w += prefix;
+        if (prefix != 0) *reinterpret_cast<int4 *>(cstart + base) = o;
+        *reinterpret_cast<int4 *>(fill + base) = o;
+    } else {
 #pragma unroll
-            for (int k = 0; k < SCAN_PER_THREAD; k++)
-                if (base + k < C) cstart[base + k] += prefix;
-        }
+        for (int k = 0; k < SCAN_PER_THREAD; k++)
+            if (base + k < C) {
+                cstart[base + k] += prefix;
+                fill[base + k] = (uint32_t)cstart[base + k];
+            }
     }
     if ((int)blockIdx.x == nblocks - 1 && threadIdx.x == 0) cstart[C] = prefix + bsum[nblocks - 1];
 }
@@ -155,7 +154,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restr
     const Chunk c = ch[blockIdx.x];
     const int i = c.begin + (int)threadIdx.x;
     if (i >= c.end) return;
-    b.src[b.cstart[b.key[i]] + (int)b.rank[i]] = i;
+    b.src[atomicAdd(b.fill + b.key[i], 1u)] = i;
 }
 
 // bitonic sort of NP register values (static indexing only)
@@ -444,11 +443,8 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
         if (lane_id() == 0 && mbb != 0u) atomicMax(b.obs + (size_t)c.rep * OBS_N + 4, (unsigned long long)mbb);
     }
     if (NEXTKEY) {
-        const uint32_t rank = count_key(b.count, key, act);
-        if (act) {
-            b.key[d] = key;
-            b.rank[d] = rank;
-        }
+        count_key(b.count, key, act);
+        if (act) b.key[d] = key;
     }
 }
 
@@ -653,7 +649,7 @@ void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStr
     const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
     if (part == 1)
         k_scan1<<<nb, SCAN_TPB, 0, s>>>(b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0, b.status);
-    else k_scan2<<<nb, SCAN_TPB, 0, s>>>(b.cstart, b.bsum, (long long)C, nb);
+    else k_scan2<<<nb, SCAN_TPB, 0, s>>>(b.cstart, b.fill, b.bsum, (long long)C, nb);
 }
 
 void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {

@@ -151,9 +151,13 @@ __device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int
             const uint8_t ft = S.flag[t];
             const bool tok = tv && (aown || (ft & 1u));
             const int tin = k < na ? A0 + k : -1;  // t's slot when t lies in A (only s < t pairs there)
+            if (qn + 32 * na > TILE_QCAP) {  // room for every pair of this source cell and chunk
+                flush_queue<WRAP, NOISE>(S, pc, wq, qn, lane, qmax);
+                qn = 0;
+            }
             // four sources per round: independent screening chains for the scheduler
             for (int s0 = A0; s0 < A1; s0 += 4) {
-                if (qn > TILE_QCAP - 128) {
+                if (qn > TILE_QCAP - 128) {  // only for cells of more than QCAP / 32 beads
                     flush_queue<WRAP, NOISE>(S, pc, wq, qn, lane, qmax);
                     qn = 0;
                 }
@@ -304,11 +308,8 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
             }
         }
         if (NEXTKEY) {
-            const uint32_t rank = count_key(b.count, key, act);
-            if (act) {
-                b.key[g] = key;
-                b.rank[g] = rank;
-            }
+            count_key(b.count, key, act);
+            if (act) b.key[g] = key;
         }
     }
     const unsigned mbb = __reduce_max_sync(0xffffffffu, __float_as_uint(mb));
