@@ -236,6 +236,24 @@ DPD_API int dpd_get_stream(const dpd_handle *h, void **stream);
  * belong to the chemistry pass (they return at once on non-chemistry steps) */
 DPD_API int dpd_kernels_per_step(const dpd_handle *h, int32_t *n_plain, int32_t *n_chem);
 
+/* ---- the cell sort without any allocation ----
+ * No counterpart in the reference (its sort always runs inside the engine,
+ * oercel.c:832-933, on buffers the engine allocated).  For callers that must
+ * not allocate device memory, e.g. code inside another framework's operator
+ * or plugin hook, where cudaMalloc's device-wide synchronisation is not
+ * allowed: the stable cell sort of n positions (x, y: DEVICE arrays in [0, L))
+ * with the cell grid of the handle API, writing cstart (floor(L)^2 + 1 DEVICE
+ * entries) and order (n DEVICE entries: input index of each sorted slot).
+ * Scratch lives in one fixed device array of the library (8.0 MiB per GPU):
+ * n <= DPD_NOALLOC_MAX_BEADS and floor(L)^2 <= DPD_NOALLOC_MAX_CELLS, else
+ * DPD_E_ARG.  Calls whose work overlaps on the GPU race on that array.  The
+ * first call on a device looks up the array's address: make it before any
+ * stream capture.  stream: a cudaStream_t (NULL = the default stream). */
+#define DPD_NOALLOC_MAX_BEADS 1048576
+#define DPD_NOALLOC_MAX_CELLS 524288
+DPD_API int dpd_sort_cells_noalloc(const float *x, const float *y, int32_t n, double L, int32_t *cstart,
+                                   int32_t *order, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

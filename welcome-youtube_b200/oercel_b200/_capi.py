@@ -56,6 +56,7 @@ EXPORTS = [
     "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events",
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
+    "dpd_sort_cells_noalloc",
 ]
 
 _lib = None
@@ -113,6 +114,7 @@ def load(path: str | None = None):
         "dpd_stats": ([vp, i32, fp], C.c_int),
         "dpd_set_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),
         "dpd_get_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),
+        "dpd_sort_cells_noalloc": ([fp, fp, i32, dbl, fp, fp, vp], C.c_int),
         "dpd_pair_hist": ([vp, i32, i32, i32, dbl, i32, fp], C.c_int),
         "dpd_get_stream": ([vp, C.POINTER(vp)], C.c_int),
         "dpd_kernels_per_step": ([vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
