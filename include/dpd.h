@@ -236,6 +236,41 @@ DPD_API int dpd_get_stream(const dpd_handle *h, void **stream);
  * belong to the chemistry pass (they return at once on non-chemistry steps) */
 DPD_API int dpd_kernels_per_step(const dpd_handle *h, int32_t *n_plain, int32_t *n_chem);
 
+/* ---- parameters in place, and reverse mode (no counterpart in the reference) ---- */
+
+/* Replace replica r's physics and chemistry parameters (same box size); a fit
+ * updates its repulsions this way between windows. */
+DPD_API int dpd_set_params(dpd_handle *h, int32_t replica, const dpd_params *p);
+
+/* Structural loss of a differentiated window: the pair distribution g(r) of
+ * types ta and tb on nbin bins of [0, rmax), smoothed with a Gaussian of width
+ * sigma, averaged over the last last_steps steps of the window;
+ * loss = mean over bins of (g - target)^2, per replica. */
+typedef struct {
+    int32_t ta, tb, nbin, last_steps;
+    double rmax, sigma;
+} dpd_rdf_spec;
+
+#define DPD_NGRAD 66 /* gradient layout per replica: d loss / d a_ij (64, entry [i*8+j] with i <= j holds the
+                        symmetric pair's total), d loss / d gamma, d loss / d k_bond */
+
+/* Advance every replica nsteps steps (chemistry must be off) and return the
+ * loss (nrep values) and, if rdf_out, the averaged g(r) (nrep x nbin). */
+DPD_API int dpd_window_loss(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec, const double *target,
+                            double *loss, double *rdf_out);
+/* The same window, then its adjoint: the pair noise is replayed from its key,
+ * the state is checkpointed every ckpt_every steps and each segment is
+ * recomputed in reverse.  grad: nrep x DPD_NGRAD.  The handle ends at the end
+ * of the window, as after dpd_window_loss. */
+DPD_API int dpd_window_adjoint(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
+                               const double *target, double *loss, double *grad, double *rdf_out);
+/* Vector-Jacobian product of the pair + bond forces of replica r's current
+ * configuration at `step` (noise key): given the force cotangent (gx, gy, slot
+ * order), the gradients with respect to positions (xbar), predicted velocities
+ * (vbar) and parameters (grad, DPD_NGRAD values). */
+DPD_API int dpd_force_vjp(dpd_handle *h, int32_t replica, int64_t step, const float *gx, const float *gy,
+                          float *xbar_x, float *xbar_y, float *vbar_x, float *vbar_y, double *grad);
+
 /* ---- the cell sort without any allocation ----
  * No counterpart in the reference (its sort always runs inside the engine,
  * oercel.c:832-933, on buffers the engine allocated).  For callers that must

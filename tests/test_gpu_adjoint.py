@@ -1,0 +1,123 @@
+"""Reverse mode: the force VJP against torch autograd of a naive all-pairs model,
+and the window adjoint (checkpoints + recomputation, replayed noise) against
+central finite differences of the same window."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+import oercel_b200 as ob
+from gpu_util import engine_with, oracle_params, params
+
+pytestmark = pytest.mark.gpu
+
+MAXT = 8
+
+
+def naive_forces(torch, x, v, P, gamma, kb, types, theta, nxt, L, kT, dt, r0):
+    """all-pairs DPD + bond forces in float64 (the template of cel/engine/tests/forcetest.c:91-101)"""
+    n = x.shape[0]
+    a = torch.triu(P) + torch.triu(P, 1).T
+    d = x[:, None, :] - x[None, :, :]
+    d = d - L * torch.round(d / L)
+    r2 = (d * d).sum(-1)
+    eye = torch.eye(n, dtype=torch.bool)
+    mask = (r2 < 1.0) & (r2 > 1e-24) & ~eye
+    r = torch.sqrt(torch.where(mask, r2, torch.ones_like(r2)))
+    w = 1.0 - r
+    dv = v[:, None, :] - v[None, :, :]
+    rv = (d * dv).sum(-1) / r
+    s = torch.sqrt(2.0 * gamma * kT / dt)
+    A = a[types][:, types] - gamma * w * rv + s * theta
+    fm = torch.where(mask, w * A / r, torch.zeros_like(r))
+    F = (fm[..., None] * d).sum(1)
+    i = np.nonzero(nxt >= 0)[0]
+    j = nxt[i]
+    db = x[j] - x[i]
+    db = db - L * torch.round(db / L)
+    rb = torch.sqrt((db * db).sum(-1))
+    fb = kb * (1.0 - r0 / rb)[:, None] * db
+    F = F.index_add(0, torch.as_tensor(i), fb)
+    F = F.index_add(0, torch.as_tensor(j), -fb)
+    return F
+
+
+def test_force_vjp_matches_torch_autograd(cuda_ok):
+    import torch
+    p = params(L=8.0, seed=21, noise="philox", f_lip=0.3, c_N=0.1)
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(5)
+    step = e.step_no
+    s = e.state()
+    n = len(s["x"])
+    rng = np.random.default_rng(0)
+    gx, gy = rng.normal(size=(2, n)).astype(np.float32)
+    xbx, xby, vbx, vby, grad = e.force_vjp(0, step, gx, gy)
+    op = oracle_params(p)
+    th = np.zeros((n, n))
+    for a_ in range(n):
+        for b_ in range(a_ + 1, n):
+            th[a_, b_] = th[b_, a_] = O.lib().ora_theta(C.byref(op), step, int(s["gid"][a_]), int(s["gid"][b_]))
+    dt = torch.float64
+    x = torch.tensor(np.c_[s["x"], s["y"]], dtype=dt, requires_grad=True)
+    v = torch.tensor(np.c_[s["vtx"], s["vty"]], dtype=dt, requires_grad=True)
+    P = torch.tensor(np.array(p.a, dtype=np.float64), dtype=dt, requires_grad=True)
+    gam = torch.tensor(p.gamma, dtype=dt, requires_grad=True)
+    kb = torch.tensor(p.k_bond, dtype=dt, requires_grad=True)
+    F = naive_forces(torch, x, v, P, gam, kb, torch.as_tensor(s["type"].astype(np.int64)), torch.tensor(th), s["next"],
+                     float(np.float32(p.L)), p.kT, p.dt, p.r0)
+    # the GPU forces themselves agree with the model
+    assert np.abs(F.detach().numpy() - np.c_[s["fx"], s["fy"]]).max() < 1e-5 * np.abs(F.detach().numpy()).max()
+    lam = (F * torch.tensor(np.c_[gx, gy], dtype=dt)).sum()
+    gxv, gvv, gP, gg, gk = torch.autograd.grad(lam, [x, v, P, gam, kb])
+
+    def rel(a, b):
+        return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-30)
+
+    assert rel(np.c_[xbx, xby], gxv.numpy()) < 1e-3
+    assert rel(np.c_[vbx, vby], gvv.numpy()) < 1e-3
+    gP = gP.numpy()
+    up = np.array([[gP[i, j] if i <= j else 0.0 for j in range(MAXT)] for i in range(MAXT)])
+    assert rel(grad[:64].reshape(MAXT, MAXT), up) < 1e-3
+    assert grad[64] == pytest.approx(gg.item(), rel=1e-3)
+    assert grad[65] == pytest.approx(gk.item(), rel=1e-3)
+
+
+def _window_engine(p, s0, step0):
+    e = engine_with(p, s0["x"], s0["y"], s0["vhx"], s0["vhy"], s0["type"], s0["prev"], s0["next"], gid=s0["gid"])
+    e.build_cells()
+    e.forces(step0)
+    return e
+
+
+def test_window_adjoint_matches_finite_differences(cuda_ok):
+    base = params(L=12.0, seed=5, noise="philox", f_lip=0.3, c_N=0.1)
+    e = ob.Engine(base)
+    e.load_soup(0)
+    e.prime()
+    e.step(40)
+    s0, step0 = e.state(), e.step_no
+    spec = ob.Engine.rdf_spec(ta=2, tb=2, nbin=32, rmax=2.0, sigma=0.1, last_steps=5)
+    target = np.linspace(0.5, 1.5, 32)
+    nsteps, ckpt = 12, 5
+    e = _window_engine(base, s0, step0)
+    loss, grad, rdf = e.window_adjoint(nsteps, ckpt, spec, target)
+    assert loss[0] > 0 and np.all(np.isfinite(grad))
+    # the adjoint run leaves the engine at the end of the window, like the plain window
+    e2 = _window_engine(base, s0, step0)
+    loss2, rdf2 = e2.window_loss(nsteps, spec, target)
+    assert loss2[0] == loss[0] and np.array_equal(rdf, rdf2)
+    assert np.array_equal(e.state()["x"], e2.state()["x"])
+
+    def loss_at(**kv):
+        pp = params(L=12.0, seed=5, noise="philox", f_lip=0.3, c_N=0.1, **kv)
+        return _window_engine(pp, s0, step0).window_loss(nsteps, spec, target)[0][0]
+
+    checks = [("a_W_T", 75.0, 0.5, 0 * 8 + 2), ("a_H_T", 50.0, 0.5, 1 * 8 + 2), ("gamma", 4.5, 0.05, 64),
+              ("k_bond", 100.0, 1.0, 65)]
+    for key, val, h, idx in checks:
+        fd = (loss_at(**{key: val + h}) - loss_at(**{key: val - h})) / (2 * h)
+        assert grad[0][idx] == pytest.approx(fd, rel=0.05, abs=1e-3 * np.abs(grad[0]).max()), key

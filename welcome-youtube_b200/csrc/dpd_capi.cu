@@ -55,6 +55,10 @@ struct dpd_handle {
     // CUDA graphs of gsteps consecutive steps, one per starting buffer parity
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
+    // reverse-mode storage, grown on demand (full checkpoints, the states of one
+    // recomputed segment, adjoint arrays in gid order)
+    std::vector<void *> adj_allocs;
+    int adj_nck = 0, adj_nseg = 0;
     // staging for state in/out
     char *stage = nullptr;
     std::vector<void *> allocs;
@@ -166,8 +170,15 @@ static void drop_graphs(dpd_handle *h) {
         }
 }
 
+static void free_adj(dpd_handle *h) {
+    for (void *p : h->adj_allocs) cudaFree(p);
+    h->adj_allocs.clear();
+    h->adj_nck = h->adj_nseg = 0;
+}
+
 static void free_all(dpd_handle *h) {
     drop_graphs(h);
+    free_adj(h);
     for (void *p : h->allocs) cudaFree(p);
     h->allocs.clear();
     if (h->s) cudaStreamDestroy(h->s);
@@ -793,5 +804,309 @@ extern "C" int dpd_kernels_per_step(const dpd_handle *h, int32_t *n_plain, int32
     // scan1, scan2, place, cellfix, permute, forces (+ the chemistry kernels)
     if (n_plain) *n_plain = 6 + (h->any_chem ? chem_kernel_count() : 0);
     if (n_chem) *n_chem = chem_kernel_count();
+    return DPD_OK;
+}
+
+// ---------------------------------------------------------------- parameters in place
+
+extern "C" int dpd_set_params(dpd_handle *h, int32_t r, const dpd_params *p) {
+    TRY(ensure_replica(h, r));
+    if (!p) return fail(DPD_E_ARG, "null params");
+    RepDev R;
+    const RepDev &old = h->rh[r];
+    TRY(make_rep(*p, old.b0, old.n, old.c0, R));
+    if (R.ncx != old.ncx || R.L != old.L) return fail(DPD_E_ARG, "dpd_set_params cannot change the box size");
+    CK(cudaStreamSynchronize(h->s));
+    h->rh[r] = R;
+    h->params[r] = *p;
+    CK(cudaMemcpy(h->d_rep + r, &R, sizeof R, cudaMemcpyHostToDevice));
+    bool any = false;
+    for (auto &q : h->params) any = any || q.chem;
+    if (any != h->any_chem) {
+        h->any_chem = any;
+        drop_graphs(h);
+    }
+    return DPD_OK;
+}
+
+// ---------------------------------------------------------------- reverse mode
+
+namespace {
+struct FullCk {  // a full configuration of the engine's current buffer
+    float2 *pos, *vh, *vt, *f;
+    uint32_t *tg;
+    int2 *link;
+    int32_t *cstart;
+};
+struct SegState {  // what a force VJP needs of one configuration
+    float2 *pos, *vt;
+    uint32_t *tg;
+    int2 *link;
+    int32_t *cstart;
+};
+struct AdjBufs {
+    std::vector<FullCk> ck;  // checkpoints + the end of the window (last)
+    std::vector<SegState> seg;
+    float2 *X, *V, *F, *g, *xb, *vb;
+    double *hist, *wgt, *grad;
+};
+}  // namespace
+
+template <typename T>
+static int adj_alloc(dpd_handle *h, T **p, size_t count) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 64);
+    if (e != cudaSuccess) return fail(DPD_E_NOMEM, "cudaMalloc for the adjoint: %s", cudaGetErrorString(e));
+    h->adj_allocs.push_back(q);
+    *p = (T *)q;
+    return DPD_OK;
+}
+
+static int adj_setup(dpd_handle *h, int nck, int nseg, int nbin, AdjBufs &A) {
+    // storage is rebuilt each call (cheap next to the window)
+    free_adj(h);
+    const size_t N = (size_t)h->N, C = (size_t)h->C;
+    A.ck.resize(nck);
+    for (auto &c : A.ck) {
+        TRY(adj_alloc(h, &c.pos, N));
+        TRY(adj_alloc(h, &c.vh, N));
+        TRY(adj_alloc(h, &c.vt, N));
+        TRY(adj_alloc(h, &c.f, N));
+        TRY(adj_alloc(h, &c.tg, N));
+        TRY(adj_alloc(h, &c.link, N));
+        TRY(adj_alloc(h, &c.cstart, C + 1));
+    }
+    A.seg.resize(nseg);
+    for (auto &c : A.seg) {
+        TRY(adj_alloc(h, &c.pos, N));
+        TRY(adj_alloc(h, &c.vt, N));
+        TRY(adj_alloc(h, &c.tg, N));
+        TRY(adj_alloc(h, &c.link, N));
+        TRY(adj_alloc(h, &c.cstart, C + 1));
+    }
+    TRY(adj_alloc(h, &A.X, N));
+    TRY(adj_alloc(h, &A.V, N));
+    TRY(adj_alloc(h, &A.F, N));
+    TRY(adj_alloc(h, &A.g, N));
+    TRY(adj_alloc(h, &A.xb, N));
+    TRY(adj_alloc(h, &A.vb, N));
+    TRY(adj_alloc(h, &A.hist, (size_t)h->nrep * nbin));
+    TRY(adj_alloc(h, &A.wgt, (size_t)h->nrep * nbin));
+    TRY(adj_alloc(h, &A.grad, (size_t)h->nrep * DPD_NGRAD));
+    return DPD_OK;
+}
+
+static void ck_save(dpd_handle *h, const FullCk &c) {
+    const size_t N = (size_t)h->N, C = (size_t)h->C;
+    const int k = h->cur;
+    cudaMemcpyAsync(c.pos, h->b.pos[k], N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(c.vh, h->b.vh[k], N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(c.vt, h->b.vt[k], N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(c.f, h->b.f[k], N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(c.tg, h->b.tg[k], N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(c.link, h->b.link[k], N * sizeof(int2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(c.cstart, h->b.cstart, (C + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->s);
+}
+
+static void ck_restore(dpd_handle *h, const FullCk &c) {
+    const size_t N = (size_t)h->N, C = (size_t)h->C;
+    const int k = h->cur;
+    cudaMemcpyAsync(h->b.pos[k], c.pos, N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(h->b.vh[k], c.vh, N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(h->b.vt[k], c.vt, N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(h->b.f[k], c.f, N * sizeof(float2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(h->b.tg[k], c.tg, N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(h->b.link[k], c.link, N * sizeof(int2), cudaMemcpyDeviceToDevice, h->s);
+    cudaMemcpyAsync(h->b.cstart, c.cstart, (C + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->s);
+    h->keys_valid = false;
+}
+
+static void seg_save(dpd_handle *h, const SegState &c) {
+    const int k = h->cur;
+    launch_adj_save((int)h->N, h->b.pos[k], h->b.vt[k], h->b.tg[k], h->b.link[k], c.pos, c.vt, c.tg, c.link, h->s);
+    cudaMemcpyAsync(c.cstart, h->b.cstart, (size_t)(h->C + 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, h->s);
+}
+
+static StateView view_of(const SegState &c) { return StateView{c.pos, c.vt, c.tg, c.link, c.cstart}; }
+
+static StateView view_cur(dpd_handle *h) {
+    const int k = h->cur;
+    return StateView{h->b.pos[k], h->b.vt[k], h->b.tg[k], h->b.link[k], h->b.cstart};
+}
+
+static void enqueue_plain_step(dpd_handle *h) {  // one step without chemistry (windows require chem off)
+    launch_scan(h->b, h->C, true, h->s);
+    launch_place(h->b, h->d_bch, h->nbch, h->s);
+    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
+    h->cur ^= 1;
+    enqueue_forces(h, true);
+}
+
+static int check_window(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec, const double *target) {
+    if (nsteps < 1) return fail(DPD_E_ARG, "window of at least one step");
+    if (!spec || !target) return fail(DPD_E_ARG, "null loss specification");
+    if (spec->nbin < 1 || spec->nbin > 4096 || !(spec->rmax > 0.0) || !(spec->sigma > 0.0) || spec->last_steps < 1 ||
+        spec->last_steps > nsteps)
+        return fail(DPD_E_ARG, "bad loss specification");
+    for (auto &p : h->params)
+        if (p.chem) return fail(DPD_E_ARG, "chemistry must be off inside a differentiated window");
+    return DPD_OK;
+}
+
+// host side of the loss: mean histogram -> rdf, loss and the weights dL/dh of every bin
+static void rdf_loss(dpd_handle *h, const dpd_rdf_spec *spec, const std::vector<double> &hist,
+                     const std::vector<long long> &npairs, const double *target, double *loss, double *rdf_out,
+                     std::vector<double> *wgt) {
+    const int nb = spec->nbin;
+    const double dr = spec->rmax / nb;
+    for (int r = 0; r < h->nrep; r++) {
+        const double L = (double)h->rh[r].L, area = L * L;
+        double sum = 0.0;
+        for (int b = 0; b < nb; b++) {
+            const double rb = (b + 0.5) * dr;
+            const double norm = (npairs[r] > 0) ? area / ((double)npairs[r] * 2.0 * M_PI * rb * dr) : 0.0;
+            const double g = hist[(size_t)r * nb + b] / spec->last_steps * norm;
+            if (rdf_out) rdf_out[(size_t)r * nb + b] = g;
+            const double e = g - target[(size_t)r * nb + b];
+            sum += e * e;
+            if (wgt) (*wgt)[(size_t)r * nb + b] = 2.0 * e / nb * norm / spec->last_steps;
+        }
+        if (loss) loss[r] = sum / nb;
+    }
+}
+
+// unordered pairs of the loss types per replica (the types do not change in a window)
+static int count_pairs(dpd_handle *h, const dpd_rdf_spec *spec, std::vector<long long> &npairs) {
+    npairs.assign(h->nrep, 0);
+    for (int r = 0; r < h->nrep; r++) {
+        double o[16];
+        TRY(observables_impl(h, r, false, o));
+        const long long na = (long long)o[8 + spec->ta], nb = (long long)o[8 + spec->tb];
+        npairs[r] = spec->ta == spec->tb ? na * (na - 1) / 2 : na * nb;
+    }
+    return DPD_OK;
+}
+
+static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rdf_spec *spec, const double *target,
+                       double *loss, double *grad, double *rdf_out, bool backward) {
+    TRY(check_window(h, nsteps, spec, target));
+    if (ckpt < 1) ckpt = (int32_t)nsteps;
+    const int nseg = (int)((nsteps + ckpt - 1) / ckpt);
+    const int nb = spec->nbin;
+    const float rmax = (float)spec->rmax, sig = (float)spec->sigma;
+    std::vector<long long> npairs;
+    TRY(count_pairs(h, spec, npairs));
+    AdjBufs A;
+    TRY(adj_setup(h, backward ? nseg + 1 : 0, backward ? ckpt + 1 : 0, nb, A));
+    if (!h->keys_valid) enqueue_next_keys(h);
+    const int64_t step0 = h->step;
+    const int64_t first_loss = nsteps - spec->last_steps + 1;  // window steps whose state enters the loss
+    CK(cudaMemsetAsync(A.hist, 0, (size_t)h->nrep * nb * sizeof(double), h->s));
+    // ---- forward, with a full checkpoint at the start of every segment
+    for (int64_t k = 1; k <= nsteps; k++) {
+        if (backward && (k - 1) % ckpt == 0) ck_save(h, A.ck[(k - 1) / ckpt]);
+        enqueue_plain_step(h);
+        if (k >= first_loss) launch_rdf(view_cur(h), h->d_rep, h->d_bch, h->nbch, spec->ta, spec->tb, nb, rmax, sig, A.hist, h->s);
+    }
+    CK(cudaGetLastError());
+    h->step = step0 + nsteps;
+    std::vector<double> hist((size_t)h->nrep * nb), wgt((size_t)h->nrep * nb);
+    CK(cudaMemcpyAsync(hist.data(), A.hist, hist.size() * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    TRY(check_status(h));
+    rdf_loss(h, spec, hist, npairs, target, loss, rdf_out, &wgt);
+    if (!backward) return DPD_OK;
+    const FullCk &end = A.ck[nseg];
+    ck_save(h, end);
+    const int cur_end = h->cur;
+    CK(cudaMemcpyAsync(A.wgt, wgt.data(), wgt.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    const size_t N = (size_t)h->N;
+    CK(cudaMemsetAsync(A.X, 0, N * sizeof(float2), h->s));
+    CK(cudaMemsetAsync(A.V, 0, N * sizeof(float2), h->s));
+    CK(cudaMemsetAsync(A.F, 0, N * sizeof(float2), h->s));
+    CK(cudaMemsetAsync(A.grad, 0, (size_t)h->nrep * DPD_NGRAD * sizeof(double), h->s));
+    // ---- reverse, segment by segment, recomputing each segment's states
+    for (int sg = nseg - 1; sg >= 0; sg--) {
+        const int64_t k0 = (int64_t)sg * ckpt;
+        const int len = (int)std::min<int64_t>(ckpt, nsteps - k0);
+        ck_restore(h, A.ck[sg]);
+        TRY(set_device_step(h, step0 + k0));
+        enqueue_next_keys(h);
+        seg_save(h, A.seg[0]);
+        for (int s = 1; s <= len; s++) {
+            enqueue_plain_step(h);
+            seg_save(h, A.seg[s]);
+        }
+        for (int s = len; s >= 1; s--) {
+            const int64_t k = k0 + s;
+            const StateView v = view_of(A.seg[s]);
+            if (k >= first_loss)
+                launch_rdf_vjp(v, h->d_rep, h->d_bch, h->nbch, spec->ta, spec->tb, nb, rmax, sig, A.wgt, A.X, h->s);
+            launch_adj_gather(v.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
+            launch_force_vjp(v, step0 + k, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+            launch_adj_update(v.tg, h->d_rep, h->d_bch, h->nbch, A.xb, A.vb, A.X, A.V, A.F, h->s);
+        }
+    }
+    // the forces stored at the window start were computed with the same parameters
+    const StateView v0 = view_of(A.seg[0]);
+    launch_adj_gather(v0.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
+    launch_force_vjp(v0, step0, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+    CK(cudaGetLastError());
+    if (grad) {
+        CK(cudaMemcpyAsync(grad, A.grad, (size_t)h->nrep * DPD_NGRAD * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    }
+    // back to the end of the window
+    h->cur = cur_end;
+    ck_restore(h, end);
+    TRY(set_device_step(h, step0 + nsteps));
+    CK(cudaStreamSynchronize(h->s));
+    return check_status(h);
+}
+
+extern "C" int dpd_window_loss(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec, const double *target,
+                               double *loss, double *rdf_out) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    return window_impl(h, nsteps, (int32_t)nsteps, spec, target, loss, nullptr, rdf_out, false);
+}
+
+extern "C" int dpd_window_adjoint(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
+                                  const double *target, double *loss, double *grad, double *rdf_out) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    return window_impl(h, nsteps, ckpt_every, spec, target, loss, grad, rdf_out, true);
+}
+
+extern "C" int dpd_force_vjp(dpd_handle *h, int32_t r, int64_t step, const float *gx, const float *gy, float *xbar_x,
+                             float *xbar_y, float *vbar_x, float *vbar_y, double *grad) {
+    TRY(ensure_replica(h, r));
+    if (!gx || !gy) return fail(DPD_E_ARG, "null cotangent");
+    const RepDev &R = h->rh[r];
+    const size_t n = (size_t)R.n, N = (size_t)h->N, a = ((n * 4 + 255) / 256) * 256;
+    AdjBufs A;
+    TRY(adj_setup(h, 0, 0, 1, A));
+    CK(cudaMemsetAsync(A.g, 0, N * sizeof(float2), h->s));
+    CK(cudaMemsetAsync(A.grad, 0, (size_t)h->nrep * DPD_NGRAD * sizeof(double), h->s));
+    float *sx = (float *)h->stage, *sy = (float *)(h->stage + a);
+    CK(cudaMemcpyAsync(sx, gx, n * 4, cudaMemcpyDefault, h->s));
+    CK(cudaMemcpyAsync(sy, gy, n * 4, cudaMemcpyDefault, h->s));
+    // pack the cotangent into the replica's slots via the state packer's force field
+    Bufs u = h->b;
+    u.f[h->cur] = A.g;
+    launch_set_dynamics(u, h->cur, R.b0, (int)n, nullptr, nullptr, sx, sy, h->s);
+    launch_force_vjp(view_cur(h), step, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+    CK(cudaGetLastError());
+    float *outs[4] = {xbar_x, xbar_y, vbar_x, vbar_y};
+    float *st[4];
+    for (int k = 0; k < 4; k++) st[k] = (float *)(h->stage + k * a);
+    Bufs w = h->b;
+    w.f[h->cur] = A.xb;
+    w.vh[h->cur] = A.vb;
+    launch_unpack(w, h->cur, R.b0, (int)n, nullptr, nullptr, st[2], st[3], nullptr, nullptr, st[0], st[1], nullptr,
+                  nullptr, nullptr, nullptr, h->s);
+    CK(cudaGetLastError());
+    for (int k = 0; k < 4; k++)
+        if (outs[k]) CK(cudaMemcpyAsync(outs[k], st[k], n * 4, cudaMemcpyDefault, h->s));
+    if (grad) CK(cudaMemcpyAsync(grad, A.grad + (size_t)r * DPD_NGRAD, DPD_NGRAD * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
     return DPD_OK;
 }

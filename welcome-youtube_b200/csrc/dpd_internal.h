@@ -108,7 +108,18 @@ struct Bufs {
     unsigned long long *hist;   // pair histogram scratch
 };
 
-// launchers (dpd_kernels.cu, dpd_chem.cu); every launcher enqueues on stream s
+struct StateView {              // one stored configuration (slot order of its own step)
+    const float2 *pos, *vt;
+    const uint32_t *tg;
+    const int2 *link;
+    const int32_t *cstart;      // packed cells (C + 1)
+};
+
+#ifndef DPD_NGRAD
+#define DPD_NGRAD (DPD_MAXT * DPD_MAXT + 2)
+#endif
+
+// launchers (dpd_kernels.cu, dpd_chem.cu, dpd_adjoint.cu); every launcher enqueues on stream s
 enum PermuteMode { PERM_STEP = 0, PERM_PRIME = 1, PERM_SORT = 2 };
 
 void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool integrate,
@@ -139,6 +150,18 @@ void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDes
                         bool next_keys, cudaStream_t s);
 int tile_setup();
 size_t tile_smem_bytes();
+void launch_force_vjp(const StateView &sv, long long step, const RepDev *rep, const Chunk *bch, int nbch,
+                      const float2 *g, float2 *xbar, float2 *vbar, double *grad, cudaStream_t s);
+void launch_rdf(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,
+                float rmax, float sigma, double *hist, cudaStream_t s);
+void launch_rdf_vjp(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,
+                    float rmax, float sigma, const double *wgt, float2 *xadd_gid, cudaStream_t s);
+void launch_adj_update(const uint32_t *tg, const RepDev *rep, const Chunk *bch, int nbch, const float2 *xb,
+                       const float2 *vb, float2 *X, float2 *V, float2 *F, cudaStream_t s);
+void launch_adj_gather(const uint32_t *tg, const RepDev *rep, const Chunk *bch, int nbch, const float2 *F, float2 *g,
+                       cudaStream_t s);
+void launch_adj_save(int n, const float2 *pos, const float2 *vt, const uint32_t *tg, const int2 *link, float2 *opos,
+                     float2 *ovt, uint32_t *otg, int2 *olink, cudaStream_t s);
 int chem_kernel_count();
 // the break stage and the candidate draws on the current sorted state (phase entry point)
 void launch_chem_scan(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);

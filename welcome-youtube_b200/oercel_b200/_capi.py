@@ -44,6 +44,11 @@ class DpdTuning(C.Structure):
                 ("graph_steps", C.c_int32)]
 
 
+class DpdRdfSpec(C.Structure):
+    _fields_ = [("ta", C.c_int32), ("tb", C.c_int32), ("nbin", C.c_int32), ("last_steps", C.c_int32),
+                ("rmax", C.c_double), ("sigma", C.c_double)]
+
+
 class DpdEvent(C.Structure):
     _fields_ = [("step", C.c_int64), ("kind", C.c_int32), ("gid", C.c_uint32), ("partner", C.c_uint32),
                 ("x", C.c_float), ("y", C.c_float), ("replica", C.c_int32)]
@@ -56,8 +61,9 @@ EXPORTS = [
     "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events",
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
-    "dpd_sort_cells_noalloc",
+    "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
 ]
+NGRAD = 66
 
 _lib = None
 
@@ -115,6 +121,10 @@ def load(path: str | None = None):
         "dpd_set_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),
         "dpd_get_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),
         "dpd_sort_cells_noalloc": ([fp, fp, i32, dbl, fp, fp, vp], C.c_int),
+        "dpd_set_params": ([vp, i32, C.POINTER(DpdParams)], C.c_int),
+        "dpd_window_loss": ([vp, i64, C.POINTER(DpdRdfSpec), fp, fp, fp], C.c_int),
+        "dpd_window_adjoint": ([vp, i64, i32, C.POINTER(DpdRdfSpec), fp, fp, fp, fp], C.c_int),
+        "dpd_force_vjp": ([vp, i32, i64, fp, fp, fp, fp, fp, fp, fp], C.c_int),
         "dpd_pair_hist": ([vp, i32, i32, i32, dbl, i32, fp], C.c_int),
         "dpd_get_stream": ([vp, C.POINTER(vp)], C.c_int),
         "dpd_kernels_per_step": ([vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),

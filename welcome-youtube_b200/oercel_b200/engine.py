@@ -220,6 +220,42 @@ class Engine:
         check(self.lib.dpd_pair_hist(self.h, replica, ta, tb, float(rmax), nbin, ptr(h)))
         return h
 
+    # ---------------------------------------------------------------- parameters and reverse mode
+    def set_params(self, replica, p: Params):
+        self.params[replica] = p
+        check(self.lib.dpd_set_params(self.h, replica, C.byref(p.to_struct())))
+
+    @staticmethod
+    def rdf_spec(ta=2, tb=2, nbin=64, rmax=2.0, sigma=0.05, last_steps=50):
+        return _capi.DpdRdfSpec(int(ta), int(tb), int(nbin), int(last_steps), float(rmax), float(sigma))
+
+    def window_loss(self, nsteps, spec, target):
+        """advance nsteps (chemistry off); per-replica loss and averaged g(r)"""
+        tgt = np.ascontiguousarray(np.broadcast_to(target, (self.nrep, spec.nbin)), np.float64)
+        loss = np.zeros(self.nrep)
+        rdf = np.zeros((self.nrep, spec.nbin))
+        check(self.lib.dpd_window_loss(self.h, int(nsteps), C.byref(spec), ptr(tgt), ptr(loss), ptr(rdf)))
+        return loss, rdf
+
+    def window_adjoint(self, nsteps, ckpt_every, spec, target):
+        """window loss and its gradient (nrep x 66: a_ij upper triangle, gamma, k_bond)"""
+        tgt = np.ascontiguousarray(np.broadcast_to(target, (self.nrep, spec.nbin)), np.float64)
+        loss = np.zeros(self.nrep)
+        rdf = np.zeros((self.nrep, spec.nbin))
+        grad = np.zeros((self.nrep, _capi.NGRAD))
+        check(self.lib.dpd_window_adjoint(self.h, int(nsteps), int(ckpt_every), C.byref(spec), ptr(tgt), ptr(loss),
+                                          ptr(grad), ptr(rdf)))
+        return loss, grad, rdf
+
+    def force_vjp(self, replica, step, gx, gy):
+        n = self.n_beads[replica]
+        g = [np.ascontiguousarray(v, np.float32) for v in (gx, gy)]
+        out = [np.empty(n, np.float32) for _ in range(4)]
+        grad = np.zeros(_capi.NGRAD)
+        check(self.lib.dpd_force_vjp(self.h, replica, int(step), ptr(g[0]), ptr(g[1]), *[ptr(o) for o in out],
+                                     ptr(grad)))
+        return out[0], out[1], out[2], out[3], grad
+
     def stream(self):
         s = C.c_void_p()
         check(self.lib.dpd_get_stream(self.h, C.byref(s)))
