@@ -239,6 +239,35 @@ def batched_rates(torch, steps=64):
             "timing": "batched: CUDA events on the engine stream; one at a time: host clock around all engines"}
 
 
+def adjoint_ratio(torch, window=200, ckpt=20, last=50, reps=3):
+    """cost of the differentiated 200-step window against its forward (configuration 4 size)"""
+    import numpy as np
+
+    from oercel_b200 import Engine, workloads
+    p = workloads.config4()
+    e = Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(200)
+    spec = Engine.rdf_spec(nbin=64, rmax=2.0, sigma=0.05, last_steps=last)
+    target = np.ones(64)
+    tf, ta = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.window_loss(window, spec, target)
+        torch.cuda.synchronize()
+        tf.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        e.window_adjoint(window, ckpt, spec, target)
+        torch.cuda.synchronize()
+        ta.append(time.perf_counter() - t0)
+    e.close()
+    f, a = float(np.median(tf)), float(np.median(ta))
+    return {"ratio": a / f, "forward_s": f, "adjoint_s": a, "window": window, "ckpt_every": ckpt, "beads": p.n_beads(),
+            "timing": "host clock around each call, device synchronised; forward = the same window with its loss"}
+
+
 def e2e_rate(eng_cls, p, K):
     """the public API from host memory: load the soup from pinned host buffers,
     prime, K steps each followed by the stats row and the event log read back,
@@ -346,6 +375,7 @@ def ours(args, rank, local_rank, ws):
         res["e2e"] = e2e_rate(Engine, p, args.e2e_steps)
         if not args.skip_batched and ws == 1:
             res["batched"] = batched_rates(torch)
+            res["adjoint"] = adjoint_ratio(torch)
         if ws == 1 and not args.skip_cpu:
             threads = os.cpu_count() or 1
             step_ms, t = run_reference(p, args.cpu_steps, threads)

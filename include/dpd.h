@@ -245,10 +245,16 @@ DPD_API int dpd_set_params(dpd_handle *h, int32_t replica, const dpd_params *p);
 /* Structural loss of a differentiated window: the pair distribution g(r) of
  * types ta and tb on nbin bins of [0, rmax), smoothed with a Gaussian of width
  * sigma, averaged over the last last_steps steps of the window;
- * loss = mean over bins of (g - target)^2, per replica. */
+ * loss = mean over bins of (g - target)^2, per replica.
+ * horizon: the reverse pass runs back only `horizon` steps before the first
+ * step that enters the loss (0 = through the whole window).  The exact
+ * gradient through a long chaotic trajectory grows exponentially with the
+ * window; a horizon of a few tens of steps keeps it bounded (truncated
+ * backpropagation) and saves the recomputation of the earlier segments. */
 typedef struct {
     int32_t ta, tb, nbin, last_steps;
     double rmax, sigma;
+    int32_t horizon, pad;
 } dpd_rdf_spec;
 
 #define DPD_NGRAD 66 /* gradient layout per replica: d loss / d a_ij (64, entry [i*8+j] with i <= j holds the

@@ -121,3 +121,39 @@ def test_window_adjoint_matches_finite_differences(cuda_ok):
     for key, val, h, idx in checks:
         fd = (loss_at(**{key: val + h}) - loss_at(**{key: val - h})) / (2 * h)
         assert grad[0][idx] == pytest.approx(fd, rel=0.05, abs=1e-3 * np.abs(grad[0]).max()), key
+
+
+def test_horizon_truncates_the_reverse_pass(cuda_ok):
+    base = params(L=12.0, seed=6, noise="philox", f_lip=0.3, c_N=0.1)
+    e = ob.Engine(base)
+    e.load_soup(0)
+    e.prime()
+    e.step(30)
+    s0, step0 = e.state(), e.step_no
+    target = np.linspace(0.5, 1.5, 32)
+    full = _window_engine(base, s0, step0).window_adjoint(
+        16, 4, ob.Engine.rdf_spec(nbin=32, rmax=2.0, sigma=0.1, last_steps=4), target)
+    longh = _window_engine(base, s0, step0).window_adjoint(
+        16, 4, ob.Engine.rdf_spec(nbin=32, rmax=2.0, sigma=0.1, last_steps=4, horizon=100), target)
+    short = _window_engine(base, s0, step0).window_adjoint(
+        16, 4, ob.Engine.rdf_spec(nbin=32, rmax=2.0, sigma=0.1, last_steps=4, horizon=3), target)
+    assert np.array_equal(full[1], longh[1])  # a horizon past the window start changes nothing
+    assert full[0][0] == short[0][0] and np.all(np.isfinite(short[1]))
+    assert not np.array_equal(full[1], short[1])
+
+
+def test_fit_moves_repulsion_toward_target(cuda_ok):
+    """configuration-4 pattern on a small box: target g_TT(r) made at a_W_T = 75, fit from 60"""
+    from oercel_b200 import fit
+    truth = params(L=20.0, seed=8, noise="philox", f_lip=0.3, c_N=0.05)
+    e = ob.Engine(truth)
+    e.load_soup(0)
+    e.prime()
+    e.step(200)
+    spec = ob.Engine.rdf_spec(nbin=32, rmax=2.0, sigma=0.1, last_steps=20, horizon=10)
+    _, target = e.window_loss(60, spec, np.zeros(32))
+    start = params(L=20.0, seed=8, noise="philox", f_lip=0.3, c_N=0.05, a_W_T=60)
+    e.set_params(0, start)
+    hist = fit.fit(e, ["a_W_T"], target[0], iters=6, window=60, ckpt=20, spec=spec, lr=2.0)
+    assert hist[-1]["values"][0] > 60.0
+    assert all(np.isfinite(h["loss"]) for h in hist)

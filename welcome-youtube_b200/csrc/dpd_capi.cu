@@ -947,7 +947,7 @@ static int check_window(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec,
     if (nsteps < 1) return fail(DPD_E_ARG, "window of at least one step");
     if (!spec || !target) return fail(DPD_E_ARG, "null loss specification");
     if (spec->nbin < 1 || spec->nbin > 4096 || !(spec->rmax > 0.0) || !(spec->sigma > 0.0) || spec->last_steps < 1 ||
-        spec->last_steps > nsteps)
+        spec->last_steps > nsteps || spec->horizon < 0)
         return fail(DPD_E_ARG, "bad loss specification");
     for (auto &p : h->params)
         if (p.chem) return fail(DPD_E_ARG, "chemistry must be off inside a differentiated window");
@@ -1026,8 +1026,11 @@ static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rd
     CK(cudaMemsetAsync(A.V, 0, N * sizeof(float2), h->s));
     CK(cudaMemsetAsync(A.F, 0, N * sizeof(float2), h->s));
     CK(cudaMemsetAsync(A.grad, 0, (size_t)h->nrep * DPD_NGRAD * sizeof(double), h->s));
-    // ---- reverse, segment by segment, recomputing each segment's states
-    for (int sg = nseg - 1; sg >= 0; sg--) {
+    // ---- reverse, segment by segment, recomputing each segment's states, down to k_stop
+    const int64_t k_stop = spec->horizon > 0 ? std::max<int64_t>(0, first_loss - 1 - spec->horizon) : 0;
+    const int sg_stop = (int)(k_stop / ckpt);
+    int stop_slot = 0;  // slot of the configuration k_stop in the last recomputed segment
+    for (int sg = nseg - 1; sg >= sg_stop; sg--) {
         const int64_t k0 = (int64_t)sg * ckpt;
         const int len = (int)std::min<int64_t>(ckpt, nsteps - k0);
         ck_restore(h, A.ck[sg]);
@@ -1038,7 +1041,9 @@ static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rd
             enqueue_plain_step(h);
             seg_save(h, A.seg[s]);
         }
-        for (int s = len; s >= 1; s--) {
+        const int s_low = sg == sg_stop ? (int)(k_stop - k0) : 0;
+        stop_slot = s_low;
+        for (int s = len; s > s_low; s--) {
             const int64_t k = k0 + s;
             const StateView v = view_of(A.seg[s]);
             if (k >= first_loss)
@@ -1048,10 +1053,10 @@ static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rd
             launch_adj_update(v.tg, h->d_rep, h->d_bch, h->nbch, A.xb, A.vb, A.X, A.V, A.F, h->s);
         }
     }
-    // the forces stored at the window start were computed with the same parameters
-    const StateView v0 = view_of(A.seg[0]);
+    // the forces stored at step k_stop (the window start without a horizon) depend on the parameters too
+    const StateView v0 = view_of(A.seg[stop_slot]);
     launch_adj_gather(v0.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
-    launch_force_vjp(v0, step0, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+    launch_force_vjp(v0, step0 + k_stop, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
     CK(cudaGetLastError());
     if (grad) {
         CK(cudaMemcpyAsync(grad, A.grad, (size_t)h->nrep * DPD_NGRAD * sizeof(double), cudaMemcpyDeviceToHost, h->s));

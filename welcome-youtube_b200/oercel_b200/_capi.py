@@ -46,7 +46,7 @@ class DpdTuning(C.Structure):
 
 class DpdRdfSpec(C.Structure):
     _fields_ = [("ta", C.c_int32), ("tb", C.c_int32), ("nbin", C.c_int32), ("last_steps", C.c_int32),
-                ("rmax", C.c_double), ("sigma", C.c_double)]
+                ("rmax", C.c_double), ("sigma", C.c_double), ("horizon", C.c_int32), ("pad", C.c_int32)]
 
 
 class DpdEvent(C.Structure):

@@ -226,8 +226,9 @@ class Engine:
         check(self.lib.dpd_set_params(self.h, replica, C.byref(p.to_struct())))
 
     @staticmethod
-    def rdf_spec(ta=2, tb=2, nbin=64, rmax=2.0, sigma=0.05, last_steps=50):
-        return _capi.DpdRdfSpec(int(ta), int(tb), int(nbin), int(last_steps), float(rmax), float(sigma))
+    def rdf_spec(ta=2, tb=2, nbin=64, rmax=2.0, sigma=0.05, last_steps=50, horizon=0):
+        return _capi.DpdRdfSpec(int(ta), int(tb), int(nbin), int(last_steps), float(rmax), float(sigma),
+                                int(horizon), 0)
 
     def window_loss(self, nsteps, spec, target):
         """advance nsteps (chemistry off); per-replica loss and averaged g(r)"""

@@ -59,6 +59,18 @@ def config3(n_replicas=256, seed=2026, nmin=2048, nmax=65536, chem=True):
     return out
 
 
+def config4(a_wt=75.0, seed=4):
+    """the differentiated fit: L = 64 (16384 beads), chemistry frozen"""
+    return Params(**dict(PHYSICS, L=64, seed=seed, chem=0, a_W_T=a_wt))
+
+
+def config5(n_replicas=64, seed=2027, a_wt=75.0):
+    """the batched adjoint: 64 boxes of L = 128 (65536 beads), lipid fraction U(0.1, 0.3)"""
+    rng = np.random.default_rng(seed)
+    return [Params(**dict(PHYSICS, L=128, seed=3000 + b, chem=0, a_W_T=a_wt, f_lip=float(rng.uniform(0.1, 0.3))))
+            for b in range(n_replicas)]
+
+
 def reference_ini(p: Params, steps: int, threads: int) -> str:
     """the reference engine's ini for the physics of p (type 3 is its N; its
     catalyst chemistry is switched off: the lipid rules do not exist there)"""
