@@ -89,6 +89,8 @@ typedef struct {
     double p_bond;             /* free T + free H bonding probability per check */
     double r_grow;             /* growth reaction radius (r_c) */
     double r_bond;             /* free T - free H bonding radius */
+    int64_t warmup;            /* repulsion ramp length (warmup; 0 = off) */
+    int64_t warm_end;          /* step at which the ramp ends (a fresh soup: = warmup) */
 } dpd_params;
 
 /* One chemistry event, the reference's events.csv row (oercel.c:788-798)

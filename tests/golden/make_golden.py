@@ -140,6 +140,40 @@ def stats_fixture(nsteps=10000, equil=1000, every=10):
                         n_t=int((r.get()["type"] == 2).sum()))
 
 
+RUN_INI = dict(L=10, rho=4, dt=0.02, gamma=4.5, kT=1, k_bond=100, r0=0.5, k_angle=0, lip_nH=1, lip_nT=2,
+               f_lip=0.15, f_Ka=0, f_Kb=0, c_N=0.05, chem=0, events=0, warmup=8, seed=3, threads=1, steps=24,
+               snap_every=12, stats_every=4, ckpt_every=24, log_every=0, a_W_H=25, a_W_T=75, a_H_T=50, a_W_N=25,
+               a_H_N=25, a_N_T=75)
+
+
+def run_fixture():
+    """two runs of the reference engine's executable (oracle/_ref/oercel_portable):
+    a fresh soup with the repulsion warm-up for 24 steps, then a restart from its
+    checkpoint to step 36.  Stores the ini, stats.csv texts, snapshots and the
+    checkpoint as bytes."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "..", "..", "oracle", "_ref", "oercel_portable")
+    with tempfile.TemporaryDirectory() as td:
+        ini = os.path.join(td, "p.ini")
+        text = "".join(f"{k} = {v}\n" for k, v in RUN_INI.items())
+        with open(ini, "w") as f:
+            f.write(text)
+        a, b = os.path.join(td, "a"), os.path.join(td, "b")
+        subprocess.run([exe, ini, a], check=True, capture_output=True)
+        subprocess.run([exe, ini, b, f"restart={a}/ckpt.bin", "steps=36"], check=True, capture_output=True)
+
+        def rd(path):
+            with open(path, "rb") as f:
+                return np.frombuffer(f.read(), np.uint8)
+
+        np.savez_compressed(os.path.join(HERE, "run_L10_seed3.npz"), ini=np.frombuffer(text.encode(), np.uint8),
+                            stats_a=rd(f"{a}/stats.csv"), stats_b=rd(f"{b}/stats.csv"),
+                            snap_0=rd(f"{a}/snap_0000000000.bin"), snap_12=rd(f"{a}/snap_0000000012.bin"),
+                            snap_24=rd(f"{a}/snap_0000000024.bin"), snap_36=rd(f"{b}/snap_0000000036.bin"),
+                            ckpt_24=rd(f"{a}/ckpt.bin"))
+
+
 if __name__ == "__main__":
     if not O.Ref.available():
         sys.exit("oracle/_ref/libref_oercel.so is missing: run make -C oracle with the reference sources present")
@@ -149,5 +183,6 @@ if __name__ == "__main__":
     theta_fixture()
     trajectory_fixture()
     stats_fixture()
+    run_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,136 @@
+"""The drop-in front end without a GPU: command-line contract, file formats
+against the reference engine's own files (tests/golden/run_L10_seed3.npz, made
+by the reference executable), checkpoint round trip, csv truncation."""
+import os
+import struct
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import PKG, golden
+from oercel_b200 import cli
+
+EXE = os.path.join(PKG, "bin", "oercel_b200")
+
+
+def fixture_bytes(key):
+    return bytes(golden("run_L10_seed3.npz")[key])
+
+
+def test_usage_and_params_listing(capsys):
+    assert cli.run(["oercel_b200"]) == 2
+    assert "usage" in capsys.readouterr().err
+    assert cli.run(["oercel_b200", "--params"]) == 0
+    out = capsys.readouterr().out
+    for key in ("`L`", "`warmup`", "`restart_reseed`", "`p_grow`"):
+        assert key in out
+    assert "**W**" in out  # the default repulsion matrix
+
+
+def test_errors_exit_1(tmp_path, capsys):
+    ini = tmp_path / "p.ini"
+    ini.write_text("L = 16\nfoo = 3\n")
+    assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
+    assert "unknown parameter 'foo'" in capsys.readouterr().err
+    ini.write_text("L = 16\nk_angle = 10\n")
+    assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
+    assert "k_angle" in capsys.readouterr().err
+    ini.write_text("L = 16\nk_angle = 0\nf_Ka = 0\ninit = restart\n")
+    assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
+    assert "needs restart" in capsys.readouterr().err
+    ini.write_text("L = 16\nk_angle = 0\n")  # the catalyst beads of the default soup
+    assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
+    assert "catalyst" in capsys.readouterr().err
+    ini.write_text("L = 16\nk_angle = 0\n")
+    assert cli.run(["x", str(ini), str(tmp_path / "o"), "seed"]) == 1
+    assert "not key=value" in capsys.readouterr().err
+    assert cli.run(["x", str(tmp_path / "missing.ini"), str(tmp_path / "o")]) == 1
+
+
+def test_executable_wrapper():
+    r = subprocess.run([sys.executable, EXE, "--params"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "`seed`" in r.stdout
+    r = subprocess.run([sys.executable, EXE], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2
+
+
+def test_read_reference_snapshot(tmp_path):
+    p = tmp_path / "snap.bin"
+    p.write_bytes(fixture_bytes("snap_24"))
+    s = cli.read_snapshot(str(p))
+    assert (s["version"], s["N"], s["step"], s["L"]) == (1, 400, 24, 10.0)
+    assert s["time"] == pytest.approx(0.48)
+    assert np.bincount(s["type"], minlength=4)[:4].tolist() == [320, 20, 40, 20]
+    assert s["bonds"].shape == (40, 2) and np.all(s["bonds"][:, 0] < s["bonds"][:, 1])
+
+
+def test_snapshot_writer_is_byte_identical_to_the_reference(tmp_path):
+    """the reference checkpoint at step 24, read and written as a snapshot,
+    gives the reference's own snap_0000000024.bin byte for byte"""
+    ck_path = tmp_path / "ckpt.bin"
+    ck_path.write_bytes(fixture_bytes("ckpt_24"))
+    ck = cli.read_ckpt(str(ck_path))
+    assert (ck["N"], ck["step"], ck["L"], ck["seed"], ck["warm_end"]) == (400, 24, 10.0, 3, 8)
+    out = tmp_path / "snap.bin"
+    cli.write_snapshot(str(out), ck, ck["step"], ck["time"], ck["L"])
+    assert out.read_bytes() == fixture_bytes("snap_24")
+
+
+def test_reference_checkpoint_links_are_consistent(tmp_path):
+    ck_path = tmp_path / "ckpt.bin"
+    ck_path.write_bytes(fixture_bytes("ckpt_24"))
+    ck = cli.read_ckpt(str(ck_path))
+    n = ck["N"]
+    assert sorted(ck["gid"].tolist()) == list(range(n))
+    has = ck["next"] >= 0
+    assert np.array_equal(ck["prev"][ck["next"][has]], np.nonzero(has)[0])
+    # every link joins lipid beads (H or T)
+    assert np.all(np.isin(ck["type"][has], [1, 2])) and np.all(np.isin(ck["type"][ck["next"][has]], [1, 2]))
+    assert ck["anchor"] == (0.0, 0, 0.02)
+
+
+def test_checkpoint_round_trip(tmp_path):
+    rng = np.random.default_rng(1)
+    n = 50
+    st = dict(gid=rng.permutation(n).astype(np.uint32), type=rng.integers(0, 4, n).astype(np.uint8),
+              prev=np.full(n, -1, np.int32), next=np.full(n, -1, np.int32))
+    st["next"][3], st["prev"][7] = 7, 3
+    for k in ("x", "y", "vhx", "vhy", "fx", "fy"):
+        st[k] = rng.random(n).astype(np.float32)
+    path = str(tmp_path / "ckpt.bin")
+    cli.write_ckpt(path, st, 1234, 24.68, 16.0, 2**63 + 5, 1000, (0.0, 0, 0.02), keep_copy=str(tmp_path / "k.bin"))
+    for p in (path, str(tmp_path / "k.bin")):
+        ck = cli.read_ckpt(p)
+        assert (ck["N"], ck["step"], ck["time"], ck["L"], ck["seed"], ck["warm_end"]) == \
+            (n, 1234, 24.68, 16.0, 2**63 + 5, 1000)
+        for k in st:
+            assert np.array_equal(ck[k], st[k]), k
+    raw = open(path, "rb").read()
+    with open(path, "wb") as f:
+        f.write(raw[:-2])
+    with pytest.raises(cli.EngineError):
+        cli.read_ckpt(path)
+
+
+def test_truncate_csv_after(tmp_path):
+    p = tmp_path / "stats.csv"
+    p.write_text("step,a\n0,1\n10,2\n20,3\n30,4\n40,5")  # the last line is partial
+    cli.truncate_csv_after(str(p), 20)
+    assert p.read_text() == "step,a\n0,1\n10,2\n20,3\n"
+    p.write_text("step,a\n0,1\n10,2\n10,3\n")
+    cli.truncate_csv_after(str(p), 10)
+    assert p.read_text() == "step,a\n0,1\n10,2\n10,3\n"
+    cli.truncate_csv_after(str(tmp_path / "none.csv"), 5)  # a missing file is left alone
+
+
+def test_snapshot_header_layout(tmp_path):
+    st = dict(x=np.array([1.5, 0.25], np.float32), y=np.array([2.0, 3.0], np.float32),
+              type=np.array([2, 1], np.uint8), gid=np.array([1, 0], np.uint32), next=np.array([-1, 0], np.int32))
+    p = str(tmp_path / "s.bin")
+    cli.write_snapshot(p, st, 7, 0.14, 8.0)
+    b = open(p, "rb").read()
+    assert b[:4] == b"OCEL" and struct.unpack_from("<iiiqdd", b, 4) == (1, 2, 1, 7, 0.14, 8.0)
+    s = cli.read_snapshot(p)
+    assert s["x"].tolist() == [0.25, 1.5] and s["type"].tolist() == [1, 2] and s["bonds"].tolist() == [[0, 1]]

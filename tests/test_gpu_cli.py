@@ -1,0 +1,157 @@
+"""The drop-in executable on the GPU against runs of the reference executable
+(tests/golden/run_L10_seed3.npz: a fresh soup with the repulsion warm-up, 24
+steps, and a restart from its checkpoint to step 36), plus the continuation,
+walltime and SIGTERM contract.
+
+Criteria: the step-0 snapshot (the soup) is byte-identical; stats rows agree in
+step, time, counts and chain numbers exactly and in T_kin and max_bond within
+2e-3 relative (FP32 state against FP64 over <= 36 steps); snapshot positions
+within 1e-3 (minimum image).  A continuation from this engine's own checkpoint
+is bit-identical to the uninterrupted run."""
+import os
+import shutil
+import signal
+import subprocess
+import sys
+import time
+
+import numpy as np
+import pytest
+
+from conftest import PKG, golden
+from oercel_b200 import cli
+
+pytestmark = pytest.mark.gpu
+EXE = os.path.join(PKG, "bin", "oercel_b200")
+G = "run_L10_seed3.npz"
+
+
+def fixture_bytes(key):
+    return bytes(golden(G)[key])
+
+
+def run_exe(ini, out, *over, timeout=600):
+    r = subprocess.run([sys.executable, EXE, str(ini), str(out), *over], capture_output=True, text=True,
+                       timeout=timeout)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return r
+
+
+@pytest.fixture
+def ini(tmp_path):
+    p = tmp_path / "p.ini"
+    p.write_bytes(fixture_bytes("ini"))
+    return p
+
+
+def rows(text):
+    lines = text.strip().split("\n")
+    return [ln.split(",") for ln in lines[1:]]
+
+
+def check_stats(got_text, ref_text):
+    got, ref = rows(got_text), rows(ref_text)
+    assert len(got) == len(ref)
+    for g, r in zip(got, ref):
+        assert g[0] == r[0] and g[1] == r[1], (g, r)             # step, time
+        assert g[3:11] == r[3:11], (g, r)                        # type counts, n_lipids
+        assert float(g[2]) == pytest.approx(float(r[2]), rel=2e-3), (g, r)   # T_kin
+        assert float(g[11]) == pytest.approx(float(r[11]), rel=2e-3), (g, r)  # max_bond
+
+
+def check_snapshot(path, ref_key):
+    ref_path = path + ".ref"
+    with open(ref_path, "wb") as f:
+        f.write(fixture_bytes(ref_key))
+    a, b = cli.read_snapshot(path), cli.read_snapshot(ref_path)
+    assert (a["N"], a["step"], a["L"]) == (b["N"], b["step"], b["L"])
+    assert a["time"] == pytest.approx(b["time"], abs=1e-12)
+    assert np.array_equal(a["type"], b["type"]) and np.array_equal(a["bonds"], b["bonds"])
+    L = b["L"]
+    for k in ("x", "y"):
+        d = a[k].astype(np.float64) - b[k]
+        d -= L * np.round(d / L)
+        assert np.abs(d).max() < 1e-3, k
+
+
+def test_run_matches_the_reference_executable(cuda_ok, ini, tmp_path):
+    out = tmp_path / "run"
+    run_exe(ini, out, "noise=mix13")
+    assert (out / "snap_0000000000.bin").read_bytes() == fixture_bytes("snap_0")
+    check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_a").decode())
+    check_snapshot(str(out / "snap_0000000012.bin"), "snap_12")
+    check_snapshot(str(out / "snap_0000000024.bin"), "snap_24")
+    log = (out / "log.txt").read_text()
+    assert log.rstrip().endswith("done at step 24") and "timing:" in log
+    assert "warmup = 8" in (out / "params.ini").read_text()
+    assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] == 24
+
+
+def test_restart_from_a_reference_checkpoint(cuda_ok, ini, tmp_path):
+    ck = tmp_path / "ref_ckpt.bin"
+    ck.write_bytes(fixture_bytes("ckpt_24"))
+    out = tmp_path / "cont"
+    run_exe(ini, out, "noise=mix13", f"restart={ck}", "steps=36")
+    check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_b").decode())
+    check_snapshot(str(out / "snap_0000000036.bin"), "snap_36")
+    assert "restart from" in (out / "log.txt").read_text()
+
+
+CHEM = ("chem=1", "n_chem=1", "p_grow=0.05", "p_bond=0.3", "p_break=0.02", "noise=philox", "ckpt_every=12",
+        "ckpt_keep=1", "snap_every=6")
+
+
+def test_own_checkpoint_continuation_is_bitwise(cuda_ok, ini, tmp_path):
+    a = tmp_path / "a"
+    run_exe(ini, a, *CHEM)
+    events = (a / "events.csv").read_text()
+    assert events.startswith("step,kind,i,x,y,variant\n")
+    kinds = {r[1] for r in rows(events)}
+    assert kinds and kinds <= {"grow", "brk", "bond"}
+    # into a fresh directory
+    b = tmp_path / "b"
+    run_exe(ini, b, *CHEM, f"restart={a}/ckpt_0000000012.bin")
+    for s in (18, 24):
+        assert (b / f"snap_{s:010d}.bin").read_bytes() == (a / f"snap_{s:010d}.bin").read_bytes()
+    sa = (a / "stats.csv").read_text().split("\n")
+    sb = (b / "stats.csv").read_text().split("\n")
+    assert sb[1:] == [ln for ln in sa[1:] if not ln or int(ln.split(",")[0]) > 12]
+    # into the same directory: stats.csv and events.csv are truncated after step 12 and rewritten identically
+    saved = {f: (a / f).read_text() for f in ("stats.csv", "events.csv")}
+    shutil.copy(a / "ckpt_0000000012.bin", tmp_path / "c12.bin")
+    run_exe(ini, a, *CHEM, f"restart={tmp_path}/c12.bin")
+    for f, text in saved.items():
+        assert (a / f).read_text() == text, f
+
+
+def test_walltime_stop_writes_a_checkpoint(cuda_ok, ini, tmp_path):
+    out = tmp_path / "w"
+    run_exe(ini, out, "noise=philox", "steps=100000", "walltime=1e-9", "stats_every=5", "snap_every=0")
+    log = (out / "log.txt").read_text()
+    assert "(walltime), checkpoint written" in log and "stopped early; restart to continue" in log
+    st = cli.read_ckpt(str(out / "ckpt.bin"))["step"]
+    assert 0 < st < 100000 and f"stopping at step {st} " in log
+
+
+def test_sigterm_stops_cleanly(cuda_ok, ini, tmp_path):
+    out = tmp_path / "s"
+    p = subprocess.Popen([sys.executable, EXE, str(ini), str(out), "noise=philox", "steps=100000000",
+                          "stats_every=1000", "snap_every=0", "log_every=1000"], stdout=subprocess.PIPE,
+                         stderr=subprocess.PIPE, text=True)
+    try:
+        t0 = time.time()
+        while time.time() - t0 < 300:
+            line = p.stdout.readline()
+            if not line or line.startswith("step "):
+                break
+        time.sleep(0.5)
+        p.send_signal(signal.SIGTERM)
+        rc = p.wait(timeout=120)
+    finally:
+        if p.poll() is None:
+            p.kill()
+            p.wait()
+    assert rc == 0
+    log = (out / "log.txt").read_text()
+    assert "(signal), checkpoint written" in log
+    assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] > 0

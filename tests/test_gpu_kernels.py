@@ -129,3 +129,48 @@ def test_sort_at_one_million_beads(cuda_ok):
     assert np.array_equal(e.cells(), cs)
     assert np.array_equal(st["gid"], src.astype(np.uint32))
     assert np.all(np.diff(key[src]) >= 0)
+
+
+def a_eff(a, warmup, warm_end, step):
+    """the warm-up repulsion of the reference (cel/engine/oercel.c:1124-1129), rounded to FP32 like the engine's table"""
+    a = np.asarray(a, np.float64)
+    if warmup <= 0 or step >= warm_end:
+        return a
+    f = max(0.0, 1.0 - (warm_end - step) / warmup)
+    return np.where(a > 25.0, 25.0 + (a - 25.0) * f, a).astype(np.float32).astype(np.float64)
+
+
+def test_warmup_ramp_matches_oracle(cuda_ok):
+    g, p, e = fixture_engine("step_L12p5_seed99.npz", 12.5, 99, noise="philox", warmup=100)
+    e.build_cells()
+    s = oracle_state(e.state())
+    for step in (0, 1, 37, 99, 100, 5000):
+        op = O.params(float(np.float32(p.L)), a_eff(p.a, 100, 100, step), dt=p.dt, lam=p["lambda"], gamma=p.gamma,
+                      kT=p.kT, k_bond=p.k_bond, r0=p.r0, seed=p.seed, noise=0)
+        fx, fy = e.pair_forces(0, step)
+        rx, ry = O.pair_forces(op, s, e.cells(), step, noise=True)
+        assert rel_err(fx, rx) < FORCE_TOL and rel_err(fy, ry) < FORCE_TOL, step
+    # the ramp really changes the forces
+    f0 = e.pair_forces(0, 0)[0]
+    f1 = e.pair_forces(0, 100)[0]
+    assert rel_err(f0, f1) > 1e-2
+
+
+@pytest.mark.parametrize("force_kernel", [0, 1])   # cell tiles, per bead
+def test_warmup_in_the_fused_step(cuda_ok, force_kernel):
+    """the production step through the ramp: stored forces at step s use a_eff(s)"""
+    import oercel_b200 as ob
+    p = params(L=16.0, seed=4, noise="philox", warmup=30)
+    e = ob.Engine(p)
+    e.set_tuning(force_kernel=force_kernel)
+    e.load_soup(0)
+    e.prime()
+    for n in (7, 13, 20):   # steps 7, 20 (inside the ramp) and 40 (after it)
+        e.step(n)
+        st = e.step_no
+        s = oracle_state(e.state())
+        op = O.params(float(np.float32(p.L)), a_eff(p.a, 30, 30, st), dt=p.dt, lam=p["lambda"], gamma=p.gamma,
+                      kT=p.kT, k_bond=p.k_bond, r0=p.r0, seed=p.seed, noise=0)
+        rx, ry = O.pair_forces(op, s, e.cells(), st, noise=True)
+        rx, ry, _ = O.bond_forces(op, s, rx, ry)
+        assert rel_err(s["fx"], rx) < FORCE_TOL and rel_err(s["fy"], ry) < FORCE_TOL, st

@@ -142,6 +142,9 @@ static int make_rep(const dpd_params &p, int b0, int n, int c0, RepDev &R) {
     R.r2_bond = (float)(p.r_bond * p.r_bond);
     R.n_t_min = p.n_t_min;
     R.max_chain = p.max_chain;
+    if (p.warmup < 0) return fail(DPD_E_ARG, "warmup must be >= 0");
+    R.warm_end = (long long)p.warm_end;
+    R.warm_inv = p.warmup > 0 ? 1.0 / (double)p.warmup : 0.0;
     return DPD_OK;
 }
 
@@ -949,8 +952,11 @@ static int check_window(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec,
     if (spec->nbin < 1 || spec->nbin > 4096 || !(spec->rmax > 0.0) || !(spec->sigma > 0.0) || spec->last_steps < 1 ||
         spec->last_steps > nsteps || spec->horizon < 0)
         return fail(DPD_E_ARG, "bad loss specification");
-    for (auto &p : h->params)
+    for (auto &p : h->params) {
         if (p.chem) return fail(DPD_E_ARG, "chemistry must be off inside a differentiated window");
+        if (p.warmup > 0 && h->step < p.warm_end)
+            return fail(DPD_E_ARG, "the repulsion warm-up must be over before a differentiated window");
+    }
     return DPD_OK;
 }
 

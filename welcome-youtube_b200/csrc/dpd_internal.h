@@ -53,7 +53,19 @@ struct RepDev {                 // constants of one replica, read by every kerne
     float r2_grow, r2_bond;
     int32_t n_t_min, max_chain;
     int32_t pad;
+    long long warm_end;         // repulsions above 25 ramp in until this step (oercel.c:1124-1129)
+    double warm_inv;            // 1 / warmup, 0 = no ramp
 };
+
+// the repulsion in force at `step`: during the warm-up of a fresh soup the part
+// of a_ij above the water value 25 is ramped in linearly (oercel.c:1124-1129)
+__device__ __forceinline__ float a_at(const RepDev &R, int k, long long step) {
+    const float a = R.a[k];
+    if (R.warm_inv == 0.0 || step >= R.warm_end || a <= 25.0f) return a;
+    double f = 1.0 - (double)(R.warm_end - step) * R.warm_inv;
+    f = f < 0.0 ? 0.0 : f;
+    return (float)(25.0 + ((double)a - 25.0) * f);
+}
 
 struct Chunk {                  // one CTA's work: packed indices [begin, end) of replica rep
     int32_t rep, begin, end, pad;

@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
     __shared__ int hl[PAIR ? MAXHIT : 1][BEAD_TPB];
     const Chunk c = ch[blockIdx.x];
     const RepDev &R = reps[c.rep];
-    if (threadIdx.x < DPD_MAXT * DPD_MAXT) a_sh[threadIdx.x] = R.a[threadIdx.x];
+    if (threadIdx.x < DPD_MAXT * DPD_MAXT) a_sh[threadIdx.x] = a_at(R, threadIdx.x, *b.step);
     __syncthreads();
     const int d = c.begin + (int)threadIdx.x;
     const bool act = d < c.end;
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
                     const double r2 = dx * dx + dy * dy;
                     if (!(r2 < 1.0 && r2 > 1e-24)) continue;
                     const double r = sqrt(r2);
-                    accv += (double)R.a[ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT)] * (1.0 - r) * r;
+                    accv += (double)a_at(R, ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT), *b.step) * (1.0 - r) * r;
                 }
             }
         vir = __double2ll_rn(accv * OBS_FIX);

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
     const int LW = td.w + 2, LH = td.h + 2, nl = LW * LH;
     const int32_t *__restrict__ cs = b.cstart + R.c0;
     const int tid = (int)threadIdx.x;
-    if (tid < DPD_MAXT * DPD_MAXT) S.a[tid] = R.a[tid];
+    if (tid < DPD_MAXT * DPD_MAXT) S.a[tid] = a_at(R, tid, *b.step);
     // ---- phase 0: local cells, their bead counts, exclusive scan, copy in
     int cnt = 0;
     if (tid < nl) {

@@ -35,7 +35,7 @@ class DpdParams(C.Structure):
         ("noise", C.c_int32), ("chem", C.c_int32), ("n_chem", C.c_int32), ("n_t_min", C.c_int32),
         ("max_chain", C.c_int32), ("pad", C.c_int32),
         ("p_break", C.c_double), ("p_grow", C.c_double), ("p_bond", C.c_double),
-        ("r_grow", C.c_double), ("r_bond", C.c_double),
+        ("r_grow", C.c_double), ("r_bond", C.c_double), ("warmup", C.c_int64), ("warm_end", C.c_int64),
     ]
 
 

@@ -41,7 +41,7 @@ PDEFS = [
     ("ckpt_every", "long", "10000", "checkpoint interval (0 = at the end only)"),
     ("ckpt_keep", "int", "0", "1 = keep ckpt_<step>.bin copies"),
     ("log_every", "long", "1000", "log line interval"),
-    ("warmup", "long", "1000", "repulsion ramp on fresh starts (only 0 is supported here)"),
+    ("warmup", "long", "1000", "fresh soups: repulsions above 25 ramp in linearly over the first warmup steps"),
     ("threads", "int", "2", "host threads (the step runs on the GPU)"),
     ("nsub", "int", "4", "reference sub-cells per cell (the GPU grid is 1x1)"),
     ("seed", "u64", "1", "random seed"),
@@ -215,8 +215,6 @@ class Params:
             raise ParamError("angle terms are not supported: set k_angle = 0")
         if self.stir_A != 0 or self.kT_amp != 0:
             raise ParamError("stirring and the temperature cycle are not supported: set stir_A = 0, kT_amp = 0")
-        if self.warmup != 0 and self.init == "soup":
-            raise ParamError("the repulsion warm-up ramp is not supported: set warmup = 0")
         if self.noise not in ("philox", "mix13"):
             raise ParamError("noise must be philox or mix13")
         if self.init not in ("soup", "restart"):
@@ -228,7 +226,7 @@ class Params:
     def sigma(self):
         return math.sqrt(2.0 * self.gamma * self.kT)
 
-    def to_struct(self, seed=None):
+    def to_struct(self, seed=None, warm_end=None):
         from ._capi import DpdParams, load
         s = DpdParams()
         load().dpd_params_default(s)
@@ -250,6 +248,8 @@ class Params:
         s.max_chain = int(self.max_chain)
         s.p_break, s.p_grow, s.p_bond = float(self.p_break), float(self.p_grow), float(self.p_bond)
         s.r_grow, s.r_bond = float(self.r_grow), float(self.r_bond)
+        s.warmup = max(int(self.warmup), 0)
+        s.warm_end = int(self.warmup if warm_end is None else warm_end)
         return s
 
     def write(self, path, overrides=()):
