@@ -97,7 +97,7 @@ def test_restart_from_a_reference_checkpoint(cuda_ok, ini, tmp_path):
     assert "restart from" in (out / "log.txt").read_text()
 
 
-CHEM = ("chem=1", "n_chem=1", "p_grow=0.05", "p_bond=0.3", "p_break=0.02", "noise=philox", "ckpt_every=12",
+CHEM = ("chem=1", "events=1", "n_chem=1", "p_grow=0.05", "p_bond=0.3", "p_break=0.02", "noise=philox", "ckpt_every=12",
         "ckpt_keep=1", "snap_every=6")
 
 
