@@ -60,3 +60,38 @@ def test_autotune_picks_a_valid_choice(cuda_ok, tmp_path):
     again = autotune(e, cache_path=str(tmp_path / "t.json"))  # from the cache
     assert again["tuning"] == out["tuning"]
     e.step(5)
+
+
+@pytest.mark.parametrize("noise", ["philox", "mix13"])
+def test_tile_noise_modes(cuda_ok, noise):
+    p = params(L=20.0, seed=3, noise=noise)
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.set_tuning(force_kernel=1)
+    e.forces(77)
+    a = e.state()
+    e.set_tuning(force_kernel=0, tile_w=6, tile_h=10)
+    e.forces(77)
+    b = e.state()
+    assert np.array_equal(a["fx"], b["fx"]) and np.array_equal(a["fy"], b["fy"])
+
+
+def test_crowded_tile_falls_back_to_direct_sums(cuda_ok):
+    """a tile whose beads overflow shared memory computes them straight from HBM, same bits"""
+    from gpu_util import engine_with
+    p = params(L=32.0, seed=9, noise="philox")
+    s = ob.soup_for(p)
+    rng = np.random.default_rng(0)
+    x, y = s["x"].copy(), s["y"].copy()
+    free = np.nonzero(s["prev"] + s["next"] == -2)[0][:1600]   # unbonded beads packed into a 6 x 6 patch
+    x[free] = rng.uniform(1.0, 7.0, len(free)).astype(np.float32)
+    y[free] = rng.uniform(1.0, 7.0, len(free)).astype(np.float32)
+    runs = []
+    for fk in (1, 0):
+        e = engine_with(p, x, y, s["vx"], s["vy"], s["type"], s["prev"], s["next"])
+        e.set_tuning(force_kernel=fk, tile_w=14, tile_h=14)
+        e.build_cells()
+        e.forces(5)
+        runs.append(e.state())
+    assert np.array_equal(runs[0]["fx"], runs[1]["fx"]) and np.array_equal(runs[0]["fy"], runs[1]["fy"])

@@ -76,3 +76,203 @@ __device__ __forceinline__ void chem_in_permute(const Bufs &b, int cur, const Re
     chem_candidate(b, R, step, rep, d, tg);
 }
 
+// tail end e of a chain headed by H that is shorter than max_chain, or a lone H
+__device__ __forceinline__ bool growable_end(const uint32_t *tg, const int2 *link, int e, int max_chain) {
+    const int2 le = link[e];
+    if (le.y >= 0) return false;
+    const int te = type_of(tg[e]);
+    if (te == T_H) return le.x < 0;
+    if (te != T_T || le.x < 0) return false;
+    int len = 1, c = e;
+    while (true) {
+        const int p = link[c].x;
+        if (p < 0) break;
+        c = p;
+        len++;
+        if (len > max_chain) return false;  // chain already full (or a loop): not growable
+    }
+    return type_of(tg[c]) == T_H && len < max_chain;
+}
+
+// the 3x3 cells around position pi as contiguous slot ranges: per column the
+// rows cy-1..cy+1 are one range, or two where the rows wrap
+struct NbrRanges {
+    int s[6], e[6];
+    int n, total;
+};
+
+__device__ __forceinline__ NbrRanges nbr_ranges(const Bufs &b, const RepDev &R, float2 pi) {
+    NbrRanges q;
+    const int ncx = R.ncx, ncy = R.ncy;
+    const int32_t *cs = b.cstart + R.c0;
+    int cx, cy;
+    cell_xy(R, pi.x, pi.y, cx, cy);
+    q.n = 0;
+    q.total = 0;
+#pragma unroll
+    for (int ox = -1; ox <= 1; ox++) {
+        const int col = ((cx + ox + ncx) % ncx) * ncy;
+        if (cy >= 1 && cy + 1 < ncy) {
+            q.s[q.n] = cs[col + cy - 1];
+            q.e[q.n++] = cs[col + cy + 2];
+        } else if (cy == 0) {
+            q.s[q.n] = cs[col + ncy - 1];
+            q.e[q.n++] = cs[col + ncy];
+            q.s[q.n] = cs[col];
+            q.e[q.n++] = cs[col + 2];
+        } else {
+            q.s[q.n] = cs[col + cy - 1];
+            q.e[q.n++] = cs[col + ncy];
+            q.s[q.n] = cs[col];
+            q.e[q.n++] = cs[col + 1];
+        }
+    }
+    for (int k = 0; k < q.n; k++) q.total += q.e[k] - q.s[k];
+    return q;
+}
+
+// slot of the f-th bead of the ranges
+__device__ __forceinline__ int nbr_slot(const NbrRanges &q, int f) {
+    int k = 0;
+    while (f >= q.e[k] - q.s[k]) {
+        f -= q.e[k] - q.s[k];
+        k++;
+    }
+    return q.s[k] + f;
+}
+
+// warp minimum of a 64-bit key (distance bits, gid): the lexicographic nearest
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+
+#define NONE_LIST_KEY 0xFFFFFFFFFFFFFFFFull
+
+// stage 2 request of list entry k, by one whole warp: the listed P needs
+// >= n_t_min T beads within r_grow and claims its nearest growable end within
+// r_grow (req[k] = end or -1)
+__device__ __forceinline__ void chem_grow_req_one(const Bufs &b, int cur, const RepDev *__restrict__ reps, int k,
+                                                  int lane) {
+    const uint32_t *tg = b.tg[cur];
+    const float2 *pos = b.pos[cur];
+    const int2 *link = b.link[cur];
+    const int2 it = b.grow_list[k];
+    const int d = it.x;
+    const RepDev &R = reps[it.y];
+    const float2 pi = pos[d];
+    const float L = R.L, h = R.halfL, r2 = R.r2_grow;
+    const NbrRanges q = nbr_ranges(b, R, pi);
+    int nt = 0;
+    unsigned long long best = NONE_LIST_KEY;
+    for (int f = lane; f < q.total; f += 32) {
+        const int j = nbr_slot(q, f);
+        if (j == d) continue;
+        const float2 pj = pos[j];
+        const float dd = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+        if (!(dd < r2)) continue;
+        const uint32_t tj = tg[j];
+        nt += type_of(tj) == T_T;
+        const unsigned long long key = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
+        if (key < best && growable_end(tg, link, j, R.max_chain)) best = key;
+    }
+    nt = (int)__reduce_add_sync(0xffffffffu, (unsigned)nt);
+    best = warp_min_u64(best);
+    int e = -1;
+    if (nt >= R.n_t_min && best != NONE_LIST_KEY) {
+        // the slot of the winning end: the lane that holds it reports it
+        for (int f = lane; f < q.total; f += 32) {
+            const int j = nbr_slot(q, f);
+            if (j != d && (tg[j] & GID_MASK) == (uint32_t)(best & 0xFFFFFFFFu)) e = j;
+        }
+        e = (int)__reduce_max_sync(0xffffffffu, (unsigned)(e + 1)) - 1;
+    }
+    if (lane == 0) {
+        b.req[k] = e;
+        if (e >= 0) atomicMin(b.claim + e, tg[d] & GID_MASK);
+    }
+}
+
+// stage 2 application of list entry k: the lowest claiming gid wins its end
+__device__ __forceinline__ void chem_grow_apply_one(const Bufs &b, int cur, int k, long long step) {
+    const int e = b.req[k];
+    if (e < 0) return;
+    uint32_t *tg = b.tg[cur];
+    int2 *link = b.link[cur];
+    const int2 it = b.grow_list[k];
+    const int d = it.x;
+    const uint32_t g = tg[d] & GID_MASK;
+    if (b.claim[e] != g) return;  // a lower gid claimed this end
+    b.claim[e] = 0xFFFFFFFFu;
+    tg[d] = ((uint32_t)T_T << TYPE_SHIFT) | g;
+    link[d] = make_int2(e, -1);
+    link[e].y = d;
+    const float2 p = b.pos[cur][d];
+    push_event(b, step, 0, g, tg[e] & GID_MASK, p.x, p.y, it.y);
+}
+
+// stage 3 request of list entry k, by one whole warp: a T that is still free
+// claims its nearest free H within r_bond
+__device__ __forceinline__ void chem_bond_req_one(const Bufs &b, int cur, const RepDev *__restrict__ reps, int k,
+                                                  int lane) {
+    const uint32_t *tg = b.tg[cur];
+    const float2 *pos = b.pos[cur];
+    const int2 *link = b.link[cur];
+    const int2 it = b.bond_list[k];
+    const int d = it.x;
+    const int2 lk = link[d];
+    int e = -1;
+    if (type_of(tg[d]) == T_T && lk.x < 0 && lk.y < 0) {
+        const RepDev &R = reps[it.y];
+        const float2 pi = pos[d];
+        const float L = R.L, h = R.halfL, r2 = R.r2_bond;
+        const NbrRanges q = nbr_ranges(b, R, pi);
+        unsigned long long best = NONE_LIST_KEY;
+        int bj = -1;
+        for (int f = lane; f < q.total; f += 32) {
+            const int j = nbr_slot(q, f);
+            if (j == d) continue;
+            const uint32_t tj = tg[j];
+            if (type_of(tj) != T_H) continue;
+            const int2 lj = link[j];
+            if (lj.x >= 0 || lj.y >= 0) continue;
+            const float2 pj = pos[j];
+            const float dd = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+            if (!(dd < r2)) continue;
+            const unsigned long long key = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
+            if (key < best) {
+                best = key;
+                bj = j;
+            }
+        }
+        const unsigned long long wbest = warp_min_u64(best);
+        const int mine = (best == wbest && wbest != NONE_LIST_KEY) ? bj : -1;
+        e = (int)__reduce_max_sync(0xffffffffu, (unsigned)(mine + 1)) - 1;
+    }
+    if (lane == 0) {
+        b.req[k] = e;
+        if (e >= 0) atomicMin(b.claim + e, tg[d] & GID_MASK);
+    }
+}
+
+// stage 3 application of list entry k
+__device__ __forceinline__ void chem_bond_apply_one(const Bufs &b, int cur, int k, long long step) {
+    const int h = b.req[k];
+    if (h < 0) return;
+    const uint32_t *tg = b.tg[cur];
+    int2 *link = b.link[cur];
+    const int2 it = b.bond_list[k];
+    const int d = it.x;
+    const uint32_t g = tg[d] & GID_MASK;
+    if (b.claim[h] != g) return;
+    b.claim[h] = 0xFFFFFFFFu;
+    link[h].y = d;
+    link[d].x = h;
+    const float2 p = b.pos[cur][d];
+    push_event(b, step, 2, g, tg[h] & GID_MASK, p.x, p.y, it.y);
+}

@@ -142,6 +142,82 @@ __device__ __forceinline__ float minimg(float d, float L, float h) {
     return d > h ? __fsub_rn(d, L) : (d < -h ? __fadd_rn(d, L) : d);
 }
 
+// ---------------------------------------------------------------- the pair term
+
+// one pair term on bead i from bead j in fixed point; dx = minimg(x_i - x_j),
+// which equals (x_i - x_j) + shift of the cell stencil bit for bit
+struct PairCtx {
+    const float2 *__restrict__ pos;
+    const float2 *__restrict__ vt;
+    const uint32_t *__restrict__ tg;
+    const float *arow;
+    NoiseKey nk;
+    float2 pi, vi;
+    uint32_t gi;
+    float L, h, gam, sdt;
+};
+
+__device__ __forceinline__ void pair_term(const PairCtx &c, int j, long long &ax, long long &ay) {
+    const float2 pj = c.pos[j];
+    const float dx = minimg(__fsub_rn(c.pi.x, pj.x), c.L, c.h);
+    const float dy = minimg(__fsub_rn(c.pi.y, pj.y), c.L, c.h);
+    const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+    const float2 vj = c.vt[j];
+    const uint32_t tgj = c.tg[j];
+    float r, ir;
+    r_and_ir(r2, r, ir);
+    const float w = __fsub_rn(1.0f, r);
+    const float dvx = __fsub_rn(c.vi.x, vj.x), dvy = __fsub_rn(c.vi.y, vj.y);
+    const float rv = __fmul_rn(__fmaf_rn(dx, dvx, __fmul_rn(dy, dvy)), ir);
+    const float th = pair_theta(c.nk, c.gi, tgj & GID_MASK);
+    const float inner = __fmaf_rn(c.sdt, th, __fmaf_rn(-__fmul_rn(c.gam, w), rv, c.arow[tgj >> TYPE_SHIFT]));
+    const float fm = __fmul_rn(__fmul_rn(w, inner), ir);
+    ax += f2fix16(__fmul_rn(fm, dx));
+    ay += f2fix16(__fmul_rn(fm, dy));
+}
+
+
+// The full-shell pair sum of bead d straight from HBM (3 x 3 cells around its
+// own, every term evaluated on the spot): the force kernels' slow path for
+// tiles too crowded for shared memory.  Same terms and roundings as k_forces.
+__device__ __forceinline__ void bead_pairs_direct(const PairCtx &pc, const RepDev &R, const int32_t *__restrict__ cs,
+                                                  int d, long long &ax, long long &ay) {
+    const int ncx = R.ncx, ncy = R.ncy;
+    const float L = R.L;
+    int cx, cy;
+    cell_xy(R, pc.pi.x, pc.pi.y, cx, cy);
+    for (int ox = -1; ox <= 1; ox++) {
+        int nx = cx + ox;
+        float sx = 0.0f;
+        if (nx < 0) {
+            nx += ncx;
+            sx = L;
+        } else if (nx >= ncx) {
+            nx -= ncx;
+            sx = -L;
+        }
+        for (int oy = -1; oy <= 1; oy++) {
+            int ny = cy + oy;
+            float sy = 0.0f;
+            if (ny < 0) {
+                ny += ncy;
+                sy = L;
+            } else if (ny >= ncy) {
+                ny -= ncy;
+                sy = -L;
+            }
+            const int cc = nx * ncy + ny;
+            for (int j = cs[cc]; j < cs[cc + 1]; j++) {
+                const float2 pj = pc.pos[j];
+                const float dx = __fadd_rn(__fsub_rn(pc.pi.x, pj.x), sx);
+                const float dy = __fadd_rn(__fsub_rn(pc.pi.y, pj.y), sy);
+                const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                if (r2 < 1.0f && r2 > 1e-24f && j != d) pair_term(pc, j, ax, ay);
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- warp helpers
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

@@ -24,7 +24,7 @@
 
 #define BEAD_TPB 256
 #define CELL_TPB 256
-#define SCAN_TPB 1024
+#define SCAN_TPB 256
 #define SCAN_PER_THREAD 4
 #define SCAN_PER_BLOCK (SCAN_TPB * SCAN_PER_THREAD)
 
@@ -137,6 +137,7 @@ enum PermuteMode { PERM_STEP = 0, PERM_PRIME = 1, PERM_SORT = 2 };
 void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool integrate,
                  cudaStream_t s);
 void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s);
+
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s);
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s);

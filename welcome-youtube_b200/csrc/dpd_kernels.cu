@@ -150,11 +150,24 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart
 
 // ---------------------------------------------------------------- placement and the stable fix-up
 
+// Called by all lanes of a warp: the beads of the warp that go to the same cell
+// share one atomic on its cursor and take consecutive places in lane (= old
+// slot) order.
+__device__ __forceinline__ void place_warp(const Bufs &b, int i, bool act) {
+    const unsigned lane = lane_id();
+    const uint32_t key = act ? b.key[i] : 0xFFFFFFFFu;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(grp) - 1;
+    uint32_t base = 0;
+    if (act && (int)lane == leader) base = atomicAdd(b.fill + key, (unsigned)__popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (act) b.src[base + __popc(grp & ((1u << lane) - 1u))] = i;
+}
+
 __global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch) {
     const Chunk c = ch[blockIdx.x];
     const int i = c.begin + (int)threadIdx.x;
-    if (i >= c.end) return;
-    b.src[atomicAdd(b.fill + b.key[i], 1u)] = i;
+    place_warp(b, i, i < c.end);
 }
 
 // bitonic sort of NP register values (static indexing only)
@@ -180,13 +193,17 @@ __device__ __forceinline__ void bitonic(int (&v)[NP]) {
 template <int NP>
 __device__ __forceinline__ void fix_cell(int32_t *__restrict__ src, int32_t *__restrict__ dest, int s, int m) {
     int v[NP];
+    bool sorted = true;
 #pragma unroll
-    for (int k = 0; k < NP; k++) v[k] = k < m ? src[s + k] : 0x7fffffff;
-    bitonic<NP>(v);
+    for (int k = 0; k < NP; k++) {
+        v[k] = k < m ? src[s + k] : 0x7fffffff;
+        if (k > 0) sorted = sorted && v[k - 1] <= v[k];
+    }
+    if (!sorted) bitonic<NP>(v);
 #pragma unroll
     for (int k = 0; k < NP; k++)
         if (k < m) {
-            src[s + k] = v[k];
+            if (!sorted) src[s + k] = v[k];
             dest[v[k]] = s + k;
         }
 }
@@ -194,16 +211,15 @@ __device__ __forceinline__ void fix_cell(int32_t *__restrict__ src, int32_t *__r
 // Beads that land in one cell keep their old slot order (the reference's
 // stable counting sort, oercel.c:832-933): the atomics gave each bead some
 // place in its cell; here every cell orders its beads by old slot.
-__global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const int cell = c.begin + (int)threadIdx.x;
-    if (cell >= c.end) return;
+__device__ __forceinline__ void cellfix_one(const Bufs &b, int cell) {
     const int s = b.cstart[cell], m = b.cstart[cell + 1] - s;
     if (m <= 1) {
         if (m == 1) b.dest[b.src[s]] = s;
         return;
     }
-    if (m <= 8) {
+    if (m <= 4) {
+        fix_cell<4>(b.src, b.dest, s, m);
+    } else if (m <= 8) {
         fix_cell<8>(b.src, b.dest, s, m);
     } else if (m <= 16) {
         fix_cell<16>(b.src, b.dest, s, m);
@@ -223,6 +239,12 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
     }
 }
 
+__global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int cell = c.begin + (int)threadIdx.x;
+    if (cell < c.end) cellfix_one(b, cell);
+}
+
 // ---------------------------------------------------------------- permute (+ integrate)
 
 // new slot d takes old bead src[d].  PERM_STEP applies the Groot-Warren update
@@ -230,18 +252,14 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
 // PERM_PRIME takes the loaded velocity as the full velocity (vt = v);
 // PERM_SORT moves everything unchanged.
 template <int MODE>
-__global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                      const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end) return;
+__device__ __forceinline__ void permute_one(const Bufs &b, int cur, const RepDev *__restrict__ reps, int rep, int d) {
     const int nxt = cur ^ 1;
     const int i = b.src[d];
     float2 p = b.pos[cur][i], vh = b.vh[cur][i];
     const uint32_t tg = b.tg[cur][i];
     const int2 lk = b.link[cur][i];
     if (MODE == PERM_STEP) {
-        const RepDev &R = reps[c.rep];
+        const RepDev &R = reps[rep];
         const float2 f = b.f[cur][i];
         const float2 q = make_float2(advance1(p.x, vh.x, f.x, R.dt, R.dt2, R.L),
                                      advance1(p.y, vh.y, f.y, R.dt, R.dt2, R.L));
@@ -257,14 +275,22 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
     }
     int2 nl = make_int2(lk.x >= 0 ? b.dest[lk.x] : -1, lk.y >= 0 ? b.dest[lk.y] : -1);
     if (MODE == PERM_STEP) {
-        const RepDev &R = reps[c.rep];
+        const RepDev &R = reps[rep];
         const long long step = *b.step;
-        if (chem_due(R, step)) chem_in_permute(b, cur, R, step, c.rep, d, p, tg, lk, nl);
+        if (chem_due(R, step)) chem_in_permute(b, cur, R, step, rep, d, p, tg, lk, nl);
     }
     b.pos[nxt][d] = p;
     b.vh[nxt][d] = vh;
     b.tg[nxt][d] = tg;
     b.link[nxt][d] = nl;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                      const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d < c.end) permute_one<MODE>(b, cur, reps, c.rep, d);
 }
 
 // ---------------------------------------------------------------- pair + bond forces
@@ -276,38 +302,6 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
 // so F_ij = -F_ji and sum F = 0 hold exactly and the result does not depend on
 // the order of the loops.  NEXTKEY: also the cell of x + dt vh + dt^2 F and
 // its count, i.e. the first half of the next step's sort.
-// one pair term on bead i from bead j in fixed point; dx = minimg(x_i - x_j),
-// which equals (x_i - x_j) + shift of the cell stencil bit for bit
-struct PairCtx {
-    const float2 *__restrict__ pos;
-    const float2 *__restrict__ vt;
-    const uint32_t *__restrict__ tg;
-    const float *arow;
-    NoiseKey nk;
-    float2 pi, vi;
-    uint32_t gi;
-    float L, h, gam, sdt;
-};
-
-__device__ __forceinline__ void pair_term(const PairCtx &c, int j, long long &ax, long long &ay) {
-    const float2 pj = c.pos[j];
-    const float dx = minimg(__fsub_rn(c.pi.x, pj.x), c.L, c.h);
-    const float dy = minimg(__fsub_rn(c.pi.y, pj.y), c.L, c.h);
-    const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-    const float2 vj = c.vt[j];
-    const uint32_t tgj = c.tg[j];
-    float r, ir;
-    r_and_ir(r2, r, ir);
-    const float w = __fsub_rn(1.0f, r);
-    const float dvx = __fsub_rn(c.vi.x, vj.x), dvy = __fsub_rn(c.vi.y, vj.y);
-    const float rv = __fmul_rn(__fmaf_rn(dx, dvx, __fmul_rn(dy, dvy)), ir);
-    const float th = pair_theta(c.nk, c.gi, tgj & GID_MASK);
-    const float inner = __fmaf_rn(c.sdt, th, __fmaf_rn(-__fmul_rn(c.gam, w), rv, c.arow[tgj >> TYPE_SHIFT]));
-    const float fm = __fmul_rn(__fmul_rn(w, inner), ir);
-    ax += f2fix16(__fmul_rn(fm, dx));
-    ay += f2fix16(__fmul_rn(fm, dy));
-}
-
 #define MAXHIT 32
 
 // Per bead d: F_d = sum_j w [a_ij - gamma w (rhat . vt_ij) + sigma theta_ij / sqrt(dt)] rhat

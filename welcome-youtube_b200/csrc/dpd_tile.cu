@@ -1,67 +1,72 @@
 // dpd_tile.cu -- pair + bond forces over cell tiles staged in shared memory (sm_100a).
 //
 // One CTA owns a tile of w x h cells of one replica.  It copies the beads of
-// the tile and of a one-cell halo around it into shared memory, enumerates
+// the tile and of a one-cell halo around it into shared memory and enumerates
 // every pair that touches an owned bead ONCE (half shell: a cell pairs with
-// itself and with its 4 forward neighbours (x, y+1), (x+1, y-1..y+1)), and adds
-// +q to one bead and -q to the other (q = the pair force rounded to a multiple
-// of 2^-16, 32-bit shared atomics).  A pair between an owned bead and a halo
+// itself and with its 4 forward neighbours (x, y+1), (x+1, y-1..y+1)).  The
+// pair force q, rounded to a multiple of 2^-16, goes +q to one bead and -q to
+// the other (32-bit shared atomics).  A pair between an owned bead and a halo
 // bead is computed by both CTAs, each keeping its own side; the operands are
 // exactly negated, so both sides agree bit for bit and sum F = 0 holds exactly.
 // The sums equal those of the per-bead kernel (k_forces) bit for bit: the same
 // terms, rounded the same way, added in integers.
 //
-// Per warp the candidate pairs are screened (r < 1) into a queue in shared
-// memory and the queue is evaluated 32 pairs at a time, so the noise and force
-// arithmetic runs on full warps.  Epilogue per owned bead: harmonic bonds to
-// prev/next, the force written to HBM, and the cell of the next position with
-// its count (the first half of the next step's sort).
+// Screening: cells are column-major, so for a source bead s in local cell
+// (lx, ly) its half-shell partners are two contiguous index ranges of the
+// local arrays: the rest of its own cell plus the cell above, and cells
+// ly-1..ly+1 of the next column.  A lane owns one source and walks its two
+// ranges; hits (r < 1) go through a warp ballot into a per-warp ring buffer,
+// which is drained 64 pairs at a time (two per lane), so the noise and force
+// arithmetic always runs on full warps.  Halo sources only pair with owned
+// beads: their ranges are clipped to the owned rows of the column.
+//
+// Epilogue per owned bead: harmonic bonds to prev/next, the force written to
+// HBM, and the cell of the next position with its count (the first half of
+// the next step's sort).  A tile whose beads do not fit in shared memory
+// computes its owned beads straight from HBM instead (bead_pairs_direct).
 #include "dpd_device.cuh"
 
 #define TILE_TPB 256
 #define TILE_WARPS (TILE_TPB / 32)
-#define TILE_MAXB 1536
+#define TILE_MAXB 1408
 #define TILE_MAXC 256
-#define TILE_QCAP 512
+#define TILE_QCAP 128  // per-warp ring; < 64 entries wait between drains, at most 64 arrive per round
 
 struct TileSmem {
     float2 pos[TILE_MAXB];
     float2 vt[TILE_MAXB];
     uint32_t tg[TILE_MAXB];
-    int32_t gslot[TILE_MAXB];
-    int2 acc[TILE_MAXB];
-    uint16_t lcell[TILE_MAXB];
-    uint8_t flag[TILE_MAXB];      // bit 0 owned; bits 1-2 x image code + 1; bits 3-4 y image code + 1
+    int32_t accx[TILE_MAXB];      // fixed-point force sums (separate arrays: 32 banks for the atomics)
+    int32_t accy[TILE_MAXB];
+    uint16_t lxy[TILE_MAXB];      // local cell of each bead: lx << 8 | ly
+    uint8_t img[TILE_MAXB];       // periodic image code: (ix + 1) | (iy + 1) << 2
     int32_t lcs[TILE_MAXC + 1];   // local cell starts (column-major over (w+2) x (h+2))
     int32_t gst[TILE_MAXC];       // global slot of each local cell's first bead
     uint32_t q[TILE_WARPS][TILE_QCAP];
     float a[DPD_MAXT * DPD_MAXT];
-    int32_t scan[TILE_TPB / 32];
+    int32_t scan[TILE_WARPS];
     int32_t n;
+    int32_t next_chunk;           // source chunks are handed to warps as they finish their last one
 };
 
-__device__ __forceinline__ int img_x(uint8_t f) { return (int)((f >> 1) & 3u) - 1; }
-__device__ __forceinline__ int img_y(uint8_t f) { return (int)((f >> 3) & 3u) - 1; }
-
-// periodic image shift of a pair: (code_s - code_t) L, exactly 0 or +-L
+// periodic image shift of a pair along one axis: (code_s - code_t) L, exactly 0 or +-L
 __device__ __forceinline__ float img_shift(int dc, float L) { return dc == 0 ? 0.0f : (dc > 0 ? L : -L); }
 
 struct PairConst {
     NoiseKey nk;
     float L, gam, sdt;
-    DevStatus *status;
 };
 
-// the pair force on s from t as fixed-point terms; only called for queued
-// pairs, which the screen already found inside the cutoff with the same r^2
+// the pair force on s from t as fixed-point terms (a queued pair: inside the cutoff)
 template <bool WRAP, int NOISE>
-__device__ __forceinline__ void tile_pair(const TileSmem &S, const PairConst &pc, int s, int t, int &qx, int &qy) {
+__device__ __forceinline__ void tile_pair(const TileSmem &S, const PairConst &pc, int s, int t, int &qx, int &qy,
+                                          float &fmax) {
     const float2 ps = S.pos[s], pt = S.pos[t];
     float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
     if (WRAP) {
-        const uint8_t fs = S.flag[s], ft = S.flag[t];
-        dx = __fadd_rn(dx, img_shift(img_x(fs) - img_x(ft), pc.L));
-        dy = __fadd_rn(dy, img_shift(img_y(fs) - img_y(ft), pc.L));
+        const int is = S.img[s], it = S.img[t];
+        dx = __fadd_rn(dx, img_shift((is & 3) - (it & 3), pc.L));
+        dy = __fadd_rn(dy, img_shift((is >> 2) - (it >> 2), pc.L));
     }
     const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
     const float2 vs = S.vt[s], vtt = S.vt[t];
@@ -83,109 +88,156 @@ __device__ __forceinline__ void tile_pair(const TileSmem &S, const PairConst &pc
     const float a = S.a[(tgs >> TYPE_SHIFT) * DPD_MAXT + (tgt >> TYPE_SHIFT)];
     const float inner = __fmaf_rn(pc.sdt, th, __fmaf_rn(-__fmul_rn(pc.gam, w), rv, a));
     const float fm = __fmul_rn(__fmul_rn(w, inner), ir);
-    qx = f2fix16(__fmul_rn(fm, dx));
-    qy = f2fix16(__fmul_rn(fm, dy));
+    const float tx = __fmul_rn(fm, dx), ty = __fmul_rn(fm, dy);
+    fmax = fmaxf(fmax, fmaxf(fabsf(tx), fabsf(ty)));
+    qx = f2fix16(tx);
+    qy = f2fix16(ty);
 }
 
 // +q to s, -q to t; halo accumulators take their share too and are ignored
-__device__ __forceinline__ void tile_add(TileSmem &S, int s, int t, int qx, int qy) {
-    atomicAdd(&S.acc[s].x, qx);
-    atomicAdd(&S.acc[s].y, qy);
-    atomicAdd(&S.acc[t].x, -qx);
-    atomicAdd(&S.acc[t].y, -qy);
+__device__ __forceinline__ void tile_add(TileSmem &S, uint32_t v, int qx, int qy) {
+    const int s = (int)(v >> 16), t = (int)(v & 0xFFFFu);
+    atomicAdd(&S.accx[s], qx);
+    atomicAdd(&S.accy[s], qy);
+    atomicAdd(&S.accx[t], -qx);
+    atomicAdd(&S.accy[t], -qy);
 }
 
+// evaluate ring entries [head, head + cnt), cnt <= 64: two independent chains per lane
 template <bool WRAP, int NOISE>
-__device__ __forceinline__ void flush_queue(TileSmem &S, const PairConst &pc, int wq, int qn, int lane,
-                                            int &qmax) {
-    // two queue entries per lane per round: two independent noise + force chains
-    for (int e = lane; e < qn; e += 64) {
-        const int e2 = e + 32;
-        const uint32_t v = S.q[wq][e];
-        const bool two = e2 < qn;
-        const uint32_t v2 = two ? S.q[wq][e2] : v;
-        int qx, qy, qx2, qy2;
-        tile_pair<WRAP, NOISE>(S, pc, (int)(v >> 16), (int)(v & 0xFFFFu), qx, qy);
-        tile_pair<WRAP, NOISE>(S, pc, (int)(v2 >> 16), (int)(v2 & 0xFFFFu), qx2, qy2);
-        qx2 = two ? qx2 : 0;
-        qy2 = two ? qy2 : 0;
-        qmax = max(qmax, max(max(abs(qx), abs(qy)), max(abs(qx2), abs(qy2))));
-        tile_add(S, (int)(v >> 16), (int)(v & 0xFFFFu), qx, qy);
-        tile_add(S, (int)(v2 >> 16), (int)(v2 & 0xFFFFu), qx2, qy2);
+__device__ __forceinline__ void drain(TileSmem &S, const PairConst &pc, const uint32_t *q, int head, int cnt,
+                                      int lane, float &fmax) {
+    const int e1 = lane, e2 = lane + 32;
+    const bool has1 = e1 < cnt, has2 = e2 < cnt;
+    if (has1) {
+        const uint32_t v1 = q[(head + e1) & (TILE_QCAP - 1)];
+        const uint32_t v2 = q[(head + (has2 ? e2 : e1)) & (TILE_QCAP - 1)];
+        int qx1, qy1, qx2, qy2;
+        tile_pair<WRAP, NOISE>(S, pc, (int)(v1 >> 16), (int)(v1 & 0xFFFFu), qx1, qy1, fmax);
+        tile_pair<WRAP, NOISE>(S, pc, (int)(v2 >> 16), (int)(v2 & 0xFFFFu), qx2, qy2, fmax);
+        tile_add(S, v1, qx1, qy1);
+        if (has2) tile_add(S, v2, qx2, qy2);
     }
     __syncwarp();
 }
 
-// Screening by cell: a warp takes a source cell A; its lanes hold up to 32
-// candidate beads t of the half-shell set of A (A itself, the cell above, and
-// the three cells of the next column) in registers and the warp walks the
-// beads s of A (a shared-memory broadcast), queueing every (s, t) inside the
-// cutoff that touches an owned bead.
-template <bool WRAP, int NOISE>
-__device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int tw, int th) {
-    const int lane = (int)lane_id(), wq = (int)threadIdx.x >> 5;
-    const int nl = LW * LH;
-    int qn = 0, qmax = 0;
-    for (int l = wq; l < nl; l += TILE_WARPS) {
-        const int A0 = S.lcs[l], A1 = S.lcs[l + 1];
-        if (A0 == A1) continue;
-        const int lx = l / LH, ly = l - lx * LH;
-        const bool aown = lx >= 1 && lx <= tw && ly >= 1 && ly <= th;
-        if (!aown) {  // a halo cell matters only if its half-shell set holds an owned cell
-            const bool up = lx >= 1 && lx <= tw && ly + 1 >= 1 && ly + 1 <= th;
-            const bool right = lx + 1 >= 1 && lx + 1 <= tw && ly + 1 >= 1 && ly - 1 <= th;
-            if (!up && !right) continue;
-        }
-        const int b1s = A0, b1e = S.lcs[ly + 1 < LH ? l + 2 : l + 1];
-        int b2s = 0, b2e = 0;
-        if (lx + 1 < LW) {
-            b2s = S.lcs[(lx + 1) * LH + (ly > 0 ? ly - 1 : 0)];
-            b2e = S.lcs[(lx + 1) * LH + (ly + 1 < LH ? ly + 1 : LH - 1) + 1];
-        }
-        const int nb1 = b1e - b1s, nb = nb1 + (b2e - b2s), na = A1 - A0;
-        for (int c0 = 0; c0 < nb; c0 += 32) {
-            const int k = c0 + lane;
-            const bool tv = k < nb;
-            const int t = tv ? (k < nb1 ? b1s + k : b2s + (k - nb1)) : 0;
-            const float2 pt = S.pos[t];
-            const uint8_t ft = S.flag[t];
-            const bool tok = tv && (aown || (ft & 1u));
-            const int tin = k < na ? A0 + k : -1;  // t's slot when t lies in A (only s < t pairs there)
-            if (qn + 32 * na > TILE_QCAP) {  // room for every pair of this source cell and chunk
-                flush_queue<WRAP, NOISE>(S, pc, wq, qn, lane, qmax);
-                qn = 0;
-            }
-            // four sources per round: independent screening chains for the scheduler
-            for (int s0 = A0; s0 < A1; s0 += 4) {
-                if (qn > TILE_QCAP - 128) {  // only for cells of more than QCAP / 32 beads
-                    flush_queue<WRAP, NOISE>(S, pc, wq, qn, lane, qmax);
-                    qn = 0;
-                }
-                bool hit[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int s = min(s0 + u, A1 - 1);  // past the cell end: repeat the last bead, masked below
-                    const float2 ps = S.pos[s];
-                    float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
-                    if (WRAP) {
-                        const uint8_t fs = S.flag[s];
-                        dx = __fadd_rn(dx, img_shift(img_x(fs) - img_x(ft), pc.L));
-                        dy = __fadd_rn(dy, img_shift(img_y(fs) - img_y(ft), pc.L));
-                    }
-                    const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
-                    hit[u] = (s0 + u < A1) && tok && (tin < 0 || tin > s) && r2 < 1.0f && r2 > 1e-24f;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const unsigned hm = __ballot_sync(0xffffffffu, hit[u]);
-                    if (hit[u]) S.q[wq][qn + __popc(hm & ((1u << lane) - 1u))] = ((uint32_t)(s0 + u) << 16) | (uint32_t)t;
-                    qn += __popc(hm);
-                }
-            }
-        }
+// rows [lo, hi] of local column c that hold owned cells, as a bead index range
+__device__ __forceinline__ void owned_rows(const TileSmem &S, int c, int LH, int tw, int th, int &b0, int &b1) {
+    if (c >= 1 && c <= tw) {
+        b0 = S.lcs[c * LH + 1];
+        b1 = S.lcs[c * LH + th + 1];
+    } else {
+        b0 = b1 = 0;
     }
-    flush_queue<WRAP, NOISE>(S, pc, wq, qn, lane, qmax);
-    if (qmax > FIX_TERM_LIMIT) raise_flag(pc.status, DPD_F_FORCE);
+}
+
+template <bool WRAP, int NOISE>
+__device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int tw, int th, DevStatus *status) {
+    const int lane = (int)lane_id(), wq = (int)threadIdx.x >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t *q = S.q[wq];
+    const int nsrc = S.lcs[(LW - 1) * LH];  // the last column (right halo) holds no sources
+    int head = 0, tail = 0;
+    float fmax = 0.0f;
+    for (int base = wq * 32; base < nsrc;) {
+        const int s = base + lane;
+        int r1s = 0, len1 = 0, r2s = 0, len = 0;
+        float2 ps = make_float2(0.0f, 0.0f);
+        int is = 0;
+        if (s < nsrc) {
+            const int v = S.lxy[s], lx = v >> 8, ly = v & 255, l = lx * LH + ly;
+            ps = S.pos[s];
+            if (WRAP) is = S.img[s];
+            int r1e = S.lcs[l + (ly + 1 < LH ? 2 : 1)];
+            r1s = s + 1;
+            const int c2 = (lx + 1) * LH;
+            r2s = S.lcs[c2 + (ly > 0 ? ly - 1 : 0)];
+            int r2e = S.lcs[c2 + (ly + 1 < LH ? ly + 1 : LH - 1) + 1];
+            if (!(lx >= 1 && lx <= tw && ly >= 1 && ly <= th)) {  // halo source: owned partners only
+                int o0, o1;
+                owned_rows(S, lx, LH, tw, th, o0, o1);
+                r1s = max(r1s, o0);
+                r1e = min(r1e, o1);
+                owned_rows(S, lx + 1, LH, tw, th, o0, o1);
+                r2s = max(r2s, o0);
+                r2e = min(r2e, o1);
+            }
+            len1 = max(r1e - r1s, 0);
+            len = len1 + max(r2e - r2s, 0);
+        }
+        const int s2m = r2s - len1;
+        const int maxlen = __reduce_max_sync(0xffffffffu, len);
+        for (int k = 0; k < maxlen; k += 2) {
+            bool hit[2];
+            int tt[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int kk = k + u;
+                const int t = kk + (kk < len1 ? r1s : s2m);
+                tt[u] = t;
+                const int tc = kk < len ? t : 0;  // past the end: a harmless in-range read
+                const float2 pt = S.pos[tc];
+                float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
+                if (WRAP) {
+                    const int it = S.img[tc];
+                    dx = __fadd_rn(dx, img_shift((is & 3) - (it & 3), pc.L));
+                    dy = __fadd_rn(dy, img_shift((is >> 2) - (it >> 2), pc.L));
+                }
+                const float r2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                hit[u] = kk < len && r2 < 1.0f && r2 > 1e-24f;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const uint32_t hm = __ballot_sync(0xffffffffu, hit[u]);
+                if (hit[u]) q[(tail + __popc(hm & below)) & (TILE_QCAP - 1)] = ((uint32_t)s << 16) | (uint32_t)tt[u];
+                tail += __popc(hm);
+            }
+            __syncwarp();
+            if (tail - head >= 64) {
+                drain<WRAP, NOISE>(S, pc, q, head, 64, lane, fmax);
+                head += 64;
+            }
+        }
+        int nxt = 0;
+        if (lane == 0) nxt = atomicAdd(&S.next_chunk, 1);
+        base = __shfl_sync(0xffffffffu, nxt, 0) * 32;
+    }
+    while (tail > head) {
+        const int cnt = min(tail - head, 64);
+        drain<WRAP, NOISE>(S, pc, q, head, cnt, lane, fmax);
+        head += cnt;
+    }
+    if (fmax > 2048.0f) raise_flag(status, DPD_F_FORCE);
+}
+
+// bonds, the force to HBM, the next cell key and its count of one owned bead
+template <bool NEXTKEY>
+__device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev &R, int g, float2 pi, long long qx,
+                                            long long qy, float &mb, uint32_t &key) {
+    const float2 *__restrict__ pos = b.pos[cur];
+    const float L = R.L, h = R.halfL, kb = R.kb, r0 = R.r0;
+    const int2 lk = b.link[cur][g];
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+        const int j = e ? lk.y : lk.x;
+        if (j < 0) continue;
+        const float2 pj = pos[j];
+        const float dx = minimg(__fsub_rn(pj.x, pi.x), L, h), dy = minimg(__fsub_rn(pj.y, pi.y), L, h);
+        const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+        mb = fmaxf(mb, r);
+        const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
+        qx += f2fix16(__fmul_rn(fb, dx));
+        qy += f2fix16(__fmul_rn(fb, dy));
+    }
+    const float2 fs = make_float2(fix16_to_f(qx), fix16_to_f(qy));
+    if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);
+    b.f[cur][g] = fs;
+    if (NEXTKEY) {
+        const float2 v = b.vh[cur][g];
+        int cx, cy;
+        key = (uint32_t)(R.c0 + cell_xy(R, advance1(pi.x, v.x, fs.x, R.dt, R.dt2, L),
+                                        advance1(pi.y, v.y, fs.y, R.dt, R.dt2, L), cx, cy));
+    }
 }
 
 template <bool NEXTKEY>
@@ -198,122 +250,133 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
     const int ncx = R.ncx, ncy = R.ncy;
     const int LW = td.w + 2, LH = td.h + 2, nl = LW * LH;
     const int32_t *__restrict__ cs = b.cstart + R.c0;
-    const int tid = (int)threadIdx.x;
-    if (tid < DPD_MAXT * DPD_MAXT) S.a[tid] = a_at(R, tid, *b.step);
-    // ---- phase 0: local cells, their bead counts, exclusive scan, copy in
-    int cnt = 0;
+    const int tid = (int)threadIdx.x, lane = (int)lane_id(), wq = tid >> 5;
+    const long long step = *b.step;
+    if (tid < DPD_MAXT * DPD_MAXT) S.a[tid] = a_at(R, tid, step);
+    // ---- phase 0: local cells, their bead counts, exclusive scan
+    int cnt = 0, lx = 0, ly = 0, code = 0;
     if (tid < nl) {
-        const int lx = tid / LH, ly = tid - lx * LH;
+        lx = tid / LH;
+        ly = tid - lx * LH;
         int gx = td.cx0 - 1 + lx, gy = td.cy0 - 1 + ly;
-        gx += gx < 0 ? ncx : (gx >= ncx ? -ncx : 0);
-        gy += gy < 0 ? ncy : (gy >= ncy ? -ncy : 0);
+        const int ix = gx < 0 ? -1 : (gx >= ncx ? 1 : 0), iy = gy < 0 ? -1 : (gy >= ncy ? 1 : 0);
+        gx -= ix * ncx;
+        gy -= iy * ncy;
+        code = (ix + 1) | ((iy + 1) << 2);
         const int gc = gx * ncy + gy;
         S.gst[tid] = cs[gc];
         cnt = cs[gc + 1] - cs[gc];
     }
+    int before;
     {   // block exclusive scan of cnt (nl <= TILE_TPB)
-        const int lane = (int)lane_id(), w = tid >> 5;
         int x = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
-        if (lane == 31) S.scan[w] = x;
+        if (lane == 31) S.scan[wq] = x;
         __syncthreads();
-        int before = 0;
-        for (int k = 0; k < w; k++) before += S.scan[k];
-        if (tid < nl) S.lcs[tid] = before + x - cnt;
+        before = 0;
+        for (int k = 0; k < wq; k++) before += S.scan[k];
+        before += x - cnt;
+        if (tid < nl) S.lcs[tid] = before;
         if (tid == TILE_TPB - 1) {
-            S.n = before + x;
-            S.lcs[nl] = before + x;
+            S.n = before + cnt;
+            S.lcs[nl] = before + cnt;
         }
         __syncthreads();
     }
     const int n = S.n;
-    if (n > TILE_MAXB) {  // tile too crowded for shared memory: report, leave the forces to the host check
-        if (tid == 0) raise_flag(b.status, DPD_F_TILE);
-        return;
-    }
-    const bool wrap = td.cx0 == 0 || td.cy0 == 0 || td.cx0 + td.w >= ncx || td.cy0 + td.h >= ncy;
-    for (int k = tid; k < n; k += TILE_TPB) {
-        int lo = 0, hi = nl;  // last local cell with lcs <= k
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (S.lcs[mid] <= k) lo = mid;
-            else hi = mid;
-        }
-        const int l = lo, lx = l / LH, ly = l - lx * LH;
-        const int g = S.gst[l] + (k - S.lcs[l]);
-        const int gx = td.cx0 - 1 + lx, gy = td.cy0 - 1 + ly;
-        const int ix = gx < 0 ? -1 : (gx >= ncx ? 1 : 0), iy = gy < 0 ? -1 : (gy >= ncy ? 1 : 0);
-        const bool own = lx >= 1 && lx <= td.w && ly >= 1 && ly <= td.h;
-        S.pos[k] = b.pos[cur][g];
-        S.vt[k] = b.vt[cur][g];
-        S.tg[k] = b.tg[cur][g];
-        S.gslot[k] = g;
-        S.lcell[k] = (uint16_t)l;
-        S.flag[k] = (uint8_t)((own ? 1u : 0u) | ((uint32_t)(ix + 1) << 1) | ((uint32_t)(iy + 1) << 3));
-        S.acc[k] = make_int2(0, 0);
-    }
-    __syncthreads();
-    // ---- phases 1 + 2: screened pair queue per warp, evaluated on full warps
-    PairConst pc;
-    pc.nk = make_noise_key(R, *b.step);
-    pc.L = R.L;
-    pc.gam = R.gamma;
-    pc.sdt = R.sdt;
-    pc.status = b.status;
-    if (R.noise == 1) {
-        if (wrap) tile_pairs<true, 1>(S, pc, LW, LH, td.w, td.h);
-        else tile_pairs<false, 1>(S, pc, LW, LH, td.w, td.h);
-    } else {
-        if (wrap) tile_pairs<true, 0>(S, pc, LW, LH, td.w, td.h);
-        else tile_pairs<false, 0>(S, pc, LW, LH, td.w, td.h);
-    }
-    __syncthreads();
-    // ---- phase 3: bonds, the force to HBM, next cell key + count
-    const float2 *__restrict__ pos = b.pos[cur];
-    const float L = R.L, h = R.halfL, kb = R.kb, r0 = R.r0;
     float mb = 0.0f;
-    for (int base = 0; base < n; base += TILE_TPB) {
-        const int k = base + tid;
-        const bool act = k < n && (S.flag[k] & 1u);
-        uint32_t key = 0;
-        int g = 0;
-        if (act) {
-            g = S.gslot[k];
-            int2 q = S.acc[k];
-            const float2 pi = S.pos[k];
-            const int2 lk = b.link[cur][g];
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int j = e ? lk.y : lk.x;
-                if (j < 0) continue;
-                const float2 pj = pos[j];
-                const float dx = minimg(__fsub_rn(pj.x, pi.x), L, h), dy = minimg(__fsub_rn(pj.y, pi.y), L, h);
-                const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
-                mb = fmaxf(mb, r);
-                const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
-                q.x += f2fix16(__fmul_rn(fb, dx));
-                q.y += f2fix16(__fmul_rn(fb, dy));
-            }
-            const float2 fs = make_float2(fix16_to_f(q.x), fix16_to_f(q.y));
-            b.f[cur][g] = fs;
-            if (NEXTKEY) {
-                const float2 v = b.vh[cur][g];
-                int cx, cy;
-                key = (uint32_t)(R.c0 + cell_xy(R, advance1(pi.x, v.x, fs.x, R.dt, R.dt2, L),
-                                                advance1(pi.y, v.y, fs.y, R.dt, R.dt2, L), cx, cy));
+    if (n > TILE_MAXB) {
+        // too crowded for shared memory: the owned beads straight from HBM (rare; same bits)
+        PairConst pk;
+        pk.nk = make_noise_key(R, step);
+        for (int c = 1; c <= td.w; c++) {
+            const int gx = td.cx0 + c - 1, g0 = cs[gx * ncy + td.cy0], g1 = cs[gx * ncy + td.cy0 + td.h];
+            for (int base = g0; base < g1; base += TILE_TPB) {
+                const int g = base + tid;
+                const bool act = g < g1;
+                uint32_t key = 0;
+                if (act) {
+                    PairCtx pc;
+                    pc.pos = b.pos[cur];
+                    pc.vt = b.vt[cur];
+                    pc.tg = b.tg[cur];
+                    pc.pi = pc.pos[g];
+                    pc.vi = pc.vt[g];
+                    const uint32_t tgi = pc.tg[g];
+                    pc.gi = tgi & GID_MASK;
+                    pc.arow = S.a + (tgi >> TYPE_SHIFT) * DPD_MAXT;
+                    pc.nk = pk.nk;
+                    pc.L = R.L;
+                    pc.h = R.halfL;
+                    pc.gam = R.gamma;
+                    pc.sdt = R.sdt;
+                    long long ax = 0, ay = 0;
+                    bead_pairs_direct(pc, R, cs, g, ax, ay);
+                    finish_bead<NEXTKEY>(b, cur, R, g, pc.pi, ax, ay, mb, key);
+                }
+                if (NEXTKEY) {
+                    count_key(b.count, key, act);
+                    if (act) b.key[g] = key;
+                }
             }
         }
-        if (NEXTKEY) {
-            count_key(b.count, key, act);
-            if (act) b.key[g] = key;
+    } else {
+        // per local cell: its beads' cell and image code
+        if (tid < nl)
+            for (int k = before; k < before + cnt; k++) {
+                S.lxy[k] = (uint16_t)((lx << 8) | ly);
+                S.img[k] = (uint8_t)code;
+            }
+        __syncthreads();
+        // copy in: consecutive beads of a column are consecutive in HBM (coalesced)
+        for (int k = tid; k < n; k += TILE_TPB) {
+            const int v = S.lxy[k], l = (v >> 8) * LH + (v & 255);
+            const int g = S.gst[l] + (k - S.lcs[l]);
+            S.pos[k] = b.pos[cur][g];
+            S.vt[k] = b.vt[cur][g];
+            S.tg[k] = b.tg[cur][g];
+            S.accx[k] = 0;
+            S.accy[k] = 0;
+        }
+        if (tid == 0) S.next_chunk = TILE_WARPS;  // chunks 0..7 go to warps 0..7 first
+        __syncthreads();
+        // ---- screened pairs, evaluated on full warps
+        PairConst pc;
+        pc.nk = make_noise_key(R, step);
+        pc.L = R.L;
+        pc.gam = R.gamma;
+        pc.sdt = R.sdt;
+        const bool wrap = td.cx0 == 0 || td.cy0 == 0 || td.cx0 + td.w >= ncx || td.cy0 + td.h >= ncy;
+        if (R.noise == 1) {
+            if (wrap) tile_pairs<true, 1>(S, pc, LW, LH, td.w, td.h, b.status);
+            else tile_pairs<false, 1>(S, pc, LW, LH, td.w, td.h, b.status);
+        } else {
+            if (wrap) tile_pairs<true, 0>(S, pc, LW, LH, td.w, td.h, b.status);
+            else tile_pairs<false, 0>(S, pc, LW, LH, td.w, td.h, b.status);
+        }
+        __syncthreads();
+        // ---- epilogue: a warp per owned column (owned rows are contiguous in HBM)
+        for (int c = 1 + wq; c <= td.w; c += TILE_WARPS) {
+            const int k0 = S.lcs[c * LH + 1], k1 = S.lcs[c * LH + td.h + 1], g0 = S.gst[c * LH + 1];
+            for (int kb = k0; kb < k1; kb += 32) {
+                const int k = kb + lane;
+                const bool act = k < k1;
+                uint32_t key = 0;
+                const int g = g0 + (k - k0);
+                if (act) finish_bead<NEXTKEY>(b, cur, R, g, S.pos[k], S.accx[k], S.accy[k], mb, key);
+                if (NEXTKEY) {
+                    count_key(b.count, key, act);
+                    if (act) b.key[g] = key;
+                }
+            }
         }
     }
     const unsigned mbb = __reduce_max_sync(0xffffffffu, __float_as_uint(mb));
-    if (lane_id() == 0 && mbb != 0u) atomicMax(b.obs + (size_t)td.rep * OBS_N + 4, (unsigned long long)mbb);
+    if (lane == 0 && mbb != 0u) atomicMax(b.obs + (size_t)td.rep * OBS_N + 4, (unsigned long long)mbb);
 }
 
 size_t tile_smem_bytes() { return sizeof(TileSmem); }
