@@ -43,6 +43,20 @@ KERNELS_CHEM = ["chem_grow_req", "chem_grow_apply", "chem_bond_req", "chem_bond_
 STEP_BYTES_CHEM = 147
 
 
+def profiled_traffic(kernel):
+    """DRAM bytes (read + write) per launch of a kernel of the step, from the
+    ncu summary in profiles/<kernel>_1M.md (line "dram_bytes_per_launch: N")"""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_1M.md")
+    try:
+        for line in open(path):
+            m = re.search(r"dram_bytes_per_launch:\s*([0-9]+)", line)
+            if m:
+                return int(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws == 1:
@@ -344,13 +358,7 @@ def ours(args, rank, local_rank, ws):
     top = max(kernels, key=kernels.get)
     peak, peak_kind = peaks()
     ach = KERNEL_BYTES[top] * nb / (kernels[top] / 1000.0) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"{top}_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(top)
     n_plain, _ = eng.kernels_per_step()
     eng.close()
     del flush

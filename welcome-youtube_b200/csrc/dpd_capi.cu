@@ -246,6 +246,11 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
     if (tile_setup() != 0) return fail(DPD_E_CUDA, "cannot reserve %zu bytes of shared memory per CTA", tile_smem_bytes());
     if (const char *e = getenv("DPD_FORCES")) h->force_kernel = strcmp(e, "bead") == 0 ? 1 : 0;
+    // default tile: 8 x 16 cells, smaller when that would leave SMs idle (at least ~4 tiles per SM)
+    while (h->C / ((int64_t)h->tile_w * h->tile_h) < 4 * 148 && h->tile_w * h->tile_h > 4) {
+        if (h->tile_h > h->tile_w) h->tile_h /= 2;
+        else h->tile_w /= 2;
+    }
     TRY(dalloc(h, &h->d_rep, nrep));
     TRY(dalloc(h, &h->d_bch, bch.size()));
     TRY(dalloc(h, &h->d_cch, cch.size()));

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_scan(Bufs b, int cur, const R
 
 // the list stages as separate kernels (phase entry points and the multi-kernel step)
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    pdl_begin();
     const int n = (int)b.status->n_grow;
     const int nw = (int)(gridDim.x * blockDim.x) >> 5;
     for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < n; k += nw)
@@ -54,6 +55,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_req(Bufs b, int cur, con
 }
 
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur) {
+    pdl_begin();
     const int n = (int)b.status->n_grow;
     const long long step = *b.step;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
@@ -61,6 +63,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur) {
 }
 
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    pdl_begin();
     const int n = (int)b.status->n_bond;
     const int nw = (int)(gridDim.x * blockDim.x) >> 5;
     for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < n; k += nw)
@@ -68,6 +71,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_req(Bufs b, int cur, con
 }
 
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_apply(Bufs b, int cur) {
+    pdl_begin();
     const int n = (int)b.status->n_bond;
     const long long step = *b.step;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
@@ -81,8 +85,8 @@ void launch_chem_scan(const Bufs &b, int cur, const RepDev *rep, const Chunk *bc
 }
 
 void launch_chem_lists(const Bufs &b, int cur, const RepDev *rep, int part, cudaStream_t s) {
-    if (part < 0 || part == 0) k_chem_grow_req<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur, rep);
-    if (part < 0 || part == 1) k_chem_grow_apply<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur);
-    if (part < 0 || part == 2) k_chem_bond_req<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur, rep);
-    if (part < 0 || part == 3) k_chem_bond_apply<<<LIST_GRID, BEAD_TPB, 0, s>>>(b, cur);
+    if (part < 0 || part == 0) launch_pdl(k_chem_grow_req, LIST_GRID, BEAD_TPB, 0, s, b, cur, rep);
+    if (part < 0 || part == 1) launch_pdl(k_chem_grow_apply, LIST_GRID, BEAD_TPB, 0, s, b, cur);
+    if (part < 0 || part == 2) launch_pdl(k_chem_bond_req, LIST_GRID, BEAD_TPB, 0, s, b, cur, rep);
+    if (part < 0 || part == 3) launch_pdl(k_chem_bond_apply, LIST_GRID, BEAD_TPB, 0, s, b, cur);
 }

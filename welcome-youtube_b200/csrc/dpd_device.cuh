@@ -218,6 +218,17 @@ __device__ __forceinline__ void bead_pairs_direct(const PairCtx &pc, const RepDe
     }
 }
 
+// ---------------------------------------------------------------- programmatic dependent launch
+
+// The kernels of a step are launched with programmatic stream serialization
+// (launch_pdl): a kernel may be scheduled while its predecessor drains.  It
+// waits for the predecessor's completion (and its memory) before touching
+// anything, and lets its own successor be scheduled once all its CTAs run.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- warp helpers
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

@@ -131,6 +131,24 @@ struct StateView {              // one stored configuration (slot order of its o
 #define DPD_NGRAD (DPD_MAXT * DPD_MAXT + 2)
 #endif
 
+// launch a kernel of the step with programmatic dependent launch allowed (the
+// kernel begins with pdl_begin(), which waits for its predecessor)
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, (KArgs)args...);
+}
+
 // launchers (dpd_kernels.cu, dpd_chem.cu, dpd_adjoint.cu); every launcher enqueues on stream s
 enum PermuteMode { PERM_STEP = 0, PERM_PRIME = 1, PERM_SORT = 2 };
 

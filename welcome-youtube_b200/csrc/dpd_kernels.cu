@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count
                                                     int32_t *__restrict__ bsum, long long C,
                                                     long long *__restrict__ step, int step_inc,
                                                     DevStatus *__restrict__ status) {
+    pdl_begin();
     const long long base = (long long)blockIdx.x * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
     int v[SCAN_PER_THREAD];
     int s = 0;
@@ -118,6 +119,7 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count
 // add the totals of all earlier blocks; the last block writes cstart[C]
 __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart, uint32_t *__restrict__ fill,
                                                     const int32_t *__restrict__ bsum, long long C, int nblocks) {
+    pdl_begin();
     __shared__ int red[SCAN_TPB / 32];
     int part = 0;
     for (int k = (int)threadIdx.x; k < (int)blockIdx.x; k += SCAN_TPB) part += bsum[k];
@@ -165,6 +167,7 @@ __device__ __forceinline__ void place_warp(const Bufs &b, int i, bool act) {
 }
 
 __global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch) {
+    pdl_begin();
     const Chunk c = ch[blockIdx.x];
     const int i = c.begin + (int)threadIdx.x;
     place_warp(b, i, i < c.end);
@@ -240,6 +243,7 @@ __device__ __forceinline__ void cellfix_one(const Bufs &b, int cell) {
 }
 
 __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch) {
+    pdl_begin();
     const Chunk c = ch[blockIdx.x];
     const int cell = c.begin + (int)threadIdx.x;
     if (cell < c.end) cellfix_one(b, cell);
@@ -288,6 +292,7 @@ __device__ __forceinline__ void permute_one(const Bufs &b, int cur, const RepDev
 template <int MODE>
 __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                       const Chunk *__restrict__ ch) {
+    pdl_begin();
     const Chunk c = ch[blockIdx.x];
     const int d = c.begin + (int)threadIdx.x;
     if (d < c.end) permute_one<MODE>(b, cur, reps, c.rep, d);
@@ -317,6 +322,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
 template <bool PAIR, bool BOND, bool NEXTKEY>
 __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                      const Chunk *__restrict__ ch) {
+    pdl_begin();
     __shared__ float a_sh[DPD_MAXT * DPD_MAXT];
     __shared__ int hl[PAIR ? MAXHIT : 1][BEAD_TPB];
     const Chunk c = ch[blockIdx.x];
@@ -642,8 +648,8 @@ void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, in
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s) {
     const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
     if (part == 1)
-        k_scan1<<<nb, SCAN_TPB, 0, s>>>(b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0, b.status);
-    else k_scan2<<<nb, SCAN_TPB, 0, s>>>(b.cstart, b.fill, b.bsum, (long long)C, nb);
+        launch_pdl(k_scan1, nb, SCAN_TPB, 0, s, b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0, b.status);
+    else launch_pdl(k_scan2, nb, SCAN_TPB, 0, s, b.cstart, b.fill, b.bsum, (long long)C, nb);
 }
 
 void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
@@ -652,23 +658,23 @@ void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
 }
 
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s) {
-    k_place<<<nbch, BEAD_TPB, 0, s>>>(b, bch);
+    launch_pdl(k_place, nbch, BEAD_TPB, 0, s, b, bch);
 }
 
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s) {
-    k_cellfix<<<ncch, CELL_TPB, 0, s>>>(b, cch);
+    launch_pdl(k_cellfix, ncch, CELL_TPB, 0, s, b, cch);
 }
 
 void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
                     cudaStream_t s) {
-    if (mode == PERM_STEP) k_permute<PERM_STEP><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    if (mode == PERM_STEP) launch_pdl(k_permute<PERM_STEP>, nbch, BEAD_TPB, 0, s, b, cur, rep, bch);
     else if (mode == PERM_PRIME) k_permute<PERM_PRIME><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
     else k_permute<PERM_SORT><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
 }
 
 void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool pair, bool bond,
                    bool next_keys, cudaStream_t s) {
-    if (pair && bond && next_keys) k_forces<true, true, true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    if (pair && bond && next_keys) launch_pdl(k_forces<true, true, true>, nbch, BEAD_TPB, 0, s, b, cur, rep, bch);
     else if (pair && bond) k_forces<true, true, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
     else if (pair) k_forces<true, false, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
     else k_forces<false, true, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);

@@ -243,6 +243,7 @@ __device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev
 template <bool NEXTKEY>
 __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const TileDesc *__restrict__ tiles) {
+    pdl_begin();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
     const TileDesc td = tiles[blockIdx.x];
@@ -392,6 +393,6 @@ int tile_setup() {
 void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
                         bool next_keys, cudaStream_t s) {
     const size_t bytes = sizeof(TileSmem);
-    if (next_keys) k_forces_tile<true><<<ntiles, TILE_TPB, bytes, s>>>(b, cur, rep, tiles);
+    if (next_keys) launch_pdl(k_forces_tile<true>, ntiles, TILE_TPB, bytes, s, b, cur, rep, tiles);
     else k_forces_tile<false><<<ntiles, TILE_TPB, bytes, s>>>(b, cur, rep, tiles);
 }

@@ -21,6 +21,8 @@ FORCE_CANDIDATES = [
     dict(force_kernel=0, tile_w=14, tile_h=14),
     dict(force_kernel=0, tile_w=6, tile_h=30),
     dict(force_kernel=0, tile_w=10, tile_h=18),
+    dict(force_kernel=0, tile_w=4, tile_h=8),
+    dict(force_kernel=0, tile_w=2, tile_h=4),
 ]
 
 
