@@ -35,10 +35,10 @@ sys.path.insert(0, os.path.join(ROOT, "welcome-youtube_b200"))
 METRIC = "DPD bead-steps/s at 1M beads & 256-replica batch; adjoint/forward time ratio"
 UNIT = "bead-steps/s"
 # algorithmic bytes per bead of each kernel of the step (FP32 SoA; derivation in DESIGN.md)
-KERNEL_BYTES = {"scan1": 3, "scan2": 2, "place": 13, "cellfix": 14, "permute": 88, "chem_grow_req": 0,
-                "chem_grow_apply": 0, "chem_bond_req": 0, "chem_bond_apply": 0, "forces": 54}
+KERNEL_BYTES = {"scan1": 3, "scan2": 2, "place": 13, "cellfix": 14, "permute": 88, "chem_grow": 0,
+                "chem_bond": 0, "forces": 54}
 KERNELS_PLAIN = ["scan1", "scan2", "place", "cellfix", "permute"]
-KERNELS_CHEM = ["chem_grow_req", "chem_grow_apply", "chem_bond_req", "chem_bond_apply"]
+KERNELS_CHEM = ["chem_grow", "chem_bond"]
 # algorithmic bytes per bead-step of the whole step (the workload table's figure: plain 138, with chemistry 147)
 STEP_BYTES_CHEM = 147
 

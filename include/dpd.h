@@ -180,7 +180,7 @@ DPD_API int dpd_get_tuning(const dpd_handle *h, dpd_tuning *t);
 DPD_API int dpd_set_graph_steps(dpd_handle *h, int32_t steps);
 /* One real step launched kernel by kernel with CUDA events around each launch
  * on the handle's stream: ms[k] = device time of kernel k in launch order
- * (scan1, scan2, place, cellfix, permute, [4 chemistry kernels], forces);
+ * (scan1, scan2, place, cellfix, permute, [2 chemistry kernels], forces);
  * *n_out = number of kernels. */
 DPD_API int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_out);
 

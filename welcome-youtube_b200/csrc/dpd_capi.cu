@@ -695,7 +695,7 @@ extern "C" int dpd_set_graph_steps(dpd_handle *h, int32_t steps) {
 
 // One step launched kernel by kernel with CUDA events between the launches on
 // the handle's stream; ms[k] = device time of kernel k (scan1, scan2, place,
-// cellfix, permute, [5 chemistry], forces).  The step is a real step.
+// cellfix, permute, [2 chemistry], forces).  The step is a real step.
 extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_out) {
     if (!h || !ms || !n_out) return fail(DPD_E_ARG, "null argument");
     if (!h->keys_valid) enqueue_next_keys(h);

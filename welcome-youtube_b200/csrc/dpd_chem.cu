@@ -45,48 +45,53 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_scan(Bufs b, int cur, const R
 
 #define LIST_GRID 148
 
-// the list stages as separate kernels (phase entry points and the multi-kernel step)
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
+// True in the last CTA of the grid to get here, after every CTA's writes are
+// visible to it (fence, then a counter; nothing waits).  The last CTA resets
+// the counter for the next launch.
+__device__ __forceinline__ bool last_cta(unsigned int *done) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+        if (last) *done = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// stage 2: requests, one warp per listed P, then the claims applied by the last CTA
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow(Bufs b, int cur, const RepDev *__restrict__ reps) {
     pdl_begin();
     const int n = (int)b.status->n_grow;
     const int nw = (int)(gridDim.x * blockDim.x) >> 5;
     for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < n; k += nw)
         chem_grow_req_one(b, cur, reps, k, (int)lane_id());
-}
-
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_grow_apply(Bufs b, int cur) {
-    pdl_begin();
-    const int n = (int)b.status->n_grow;
+    if (!last_cta(&b.status->done)) return;
     const long long step = *b.step;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        chem_grow_apply_one(b, cur, k, step);
+    for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) chem_grow_apply_one(b, cur, k, step);
 }
 
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_req(Bufs b, int cur, const RepDev *__restrict__ reps) {
+// stage 3: requests, one warp per listed T, then the claims applied by the last CTA
+__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond(Bufs b, int cur, const RepDev *__restrict__ reps) {
     pdl_begin();
     const int n = (int)b.status->n_bond;
     const int nw = (int)(gridDim.x * blockDim.x) >> 5;
     for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < n; k += nw)
         chem_bond_req_one(b, cur, reps, k, (int)lane_id());
-}
-
-__global__ void __launch_bounds__(BEAD_TPB) k_chem_bond_apply(Bufs b, int cur) {
-    pdl_begin();
-    const int n = (int)b.status->n_bond;
+    if (!last_cta(&b.status->done)) return;
     const long long step = *b.step;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        chem_bond_apply_one(b, cur, k, step);
+    for (int k = (int)threadIdx.x; k < n; k += (int)blockDim.x) chem_bond_apply_one(b, cur, k, step);
 }
 
-int chem_kernel_count() { return 4; }
+int chem_kernel_count() { return 2; }
 
 void launch_chem_scan(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
     k_chem_scan<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
 }
 
 void launch_chem_lists(const Bufs &b, int cur, const RepDev *rep, int part, cudaStream_t s) {
-    if (part < 0 || part == 0) launch_pdl(k_chem_grow_req, LIST_GRID, BEAD_TPB, 0, s, b, cur, rep);
-    if (part < 0 || part == 1) launch_pdl(k_chem_grow_apply, LIST_GRID, BEAD_TPB, 0, s, b, cur);
-    if (part < 0 || part == 2) launch_pdl(k_chem_bond_req, LIST_GRID, BEAD_TPB, 0, s, b, cur, rep);
-    if (part < 0 || part == 3) launch_pdl(k_chem_bond_apply, LIST_GRID, BEAD_TPB, 0, s, b, cur);
+    if (part < 0 || part == 0) launch_pdl(k_chem_grow, LIST_GRID, BEAD_TPB, 0, s, b, cur, rep);
+    if (part < 0 || part == 1) launch_pdl(k_chem_bond, LIST_GRID, BEAD_TPB, 0, s, b, cur, rep);
 }

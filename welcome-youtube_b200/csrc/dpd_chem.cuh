@@ -60,20 +60,47 @@ __device__ __forceinline__ void chem_candidate(const Bufs &b, const RepDev &R, l
 
 // stage 1 for new slot d inside the permute of a step (links already remapped
 // to new slots in *nl): the H side drops its next and logs the event, the T
-// side drops its prev; both evaluate the same draw (the H bead's).
+// side drops its prev; both evaluate the same draw (the H bead's).  Each lane
+// makes at most two draws, each at one call site, so a warp runs the Philox
+// rounds at most twice whatever its mix of bead types.
 __device__ __forceinline__ void chem_in_permute(const Bufs &b, int cur, const RepDev &R, long long step, int rep, int d, float2 p,
                                 uint32_t tg, int2 lk_old, int2 &nl) {
     const uint32_t *tg_old = b.tg[cur];
-    if (type_of(tg) == T_H && lk_old.y >= 0) {
-        const uint32_t tn = tg_old[lk_old.y];
-        if (h_breaks(R, step, tg, tn)) {
-            nl.y = -1;
-            push_event(b, step, 1, tg & GID_MASK, tn & GID_MASK, p.x, p.y, rep);
+    const int ty = type_of(tg);
+    const uint32_t g = tg & GID_MASK;
+    // the H-T bond this bead is part of, if any: its H bead's gid decides
+    uint32_t hgid = 0, partner = 0;
+    int side = 0;  // 1: this bead is the H, 2: this bead is the T
+    if (ty == T_H && lk_old.y >= 0) {
+        partner = tg_old[lk_old.y];
+        if (type_of(partner) == T_T) {
+            side = 1;
+            hgid = g;
         }
-    } else if (type_of(tg) == T_T && lk_old.x >= 0) {
-        if (h_breaks(R, step, tg_old[lk_old.x], tg)) nl.x = -1;
+    } else if (ty == T_T && lk_old.x >= 0) {
+        partner = tg_old[lk_old.x];
+        if (type_of(partner) == T_H) {
+            side = 2;
+            hgid = partner & GID_MASK;
+        }
     }
-    chem_candidate(b, R, step, rep, d, tg);
+    if (side != 0 && decision_word(R, step, SALT_BREAK, hgid) < R.thr_break) {
+        if (side == 1) {
+            nl.y = -1;
+            push_event(b, step, 1, g, partner & GID_MASK, p.x, p.y, rep);
+        } else {
+            nl.x = -1;
+        }
+    }
+    // the growth (P) or bonding (T) draw; only a free T can bond (nothing in the
+    // later stages of the step gives a free T a link before its bond request)
+    if (ty == T_P || (ty == T_T && nl.x < 0 && nl.y < 0)) {
+        const bool grow = ty == T_P;
+        if (decision_word(R, step, grow ? SALT_GROW : SALT_BOND, g) < (grow ? R.thr_grow : R.thr_bond)) {
+            if (grow) b.grow_list[atomicAdd(&b.status->n_grow, 1u)] = make_int2(d, rep);
+            else b.bond_list[atomicAdd(&b.status->n_bond, 1u)] = make_int2(d, rep);
+        }
+    }
 }
 
 // tail end e of a chain headed by H that is shorter than max_chain, or a lone H
@@ -200,14 +227,14 @@ __device__ __forceinline__ void chem_grow_req_one(const Bufs &b, int cur, const 
 
 // stage 2 application of list entry k: the lowest claiming gid wins its end
 __device__ __forceinline__ void chem_grow_apply_one(const Bufs &b, int cur, int k, long long step) {
-    const int e = b.req[k];
+    const int e = __ldcg(b.req + k);
     if (e < 0) return;
     uint32_t *tg = b.tg[cur];
     int2 *link = b.link[cur];
     const int2 it = b.grow_list[k];
     const int d = it.x;
     const uint32_t g = tg[d] & GID_MASK;
-    if (b.claim[e] != g) return;  // a lower gid claimed this end
+    if (__ldcg(b.claim + e) != g) return;  // a lower gid claimed this end
     b.claim[e] = 0xFFFFFFFFu;
     tg[d] = ((uint32_t)T_T << TYPE_SHIFT) | g;
     link[d] = make_int2(e, -1);
@@ -262,14 +289,14 @@ __device__ __forceinline__ void chem_bond_req_one(const Bufs &b, int cur, const 
 
 // stage 3 application of list entry k
 __device__ __forceinline__ void chem_bond_apply_one(const Bufs &b, int cur, int k, long long step) {
-    const int h = b.req[k];
+    const int h = __ldcg(b.req + k);
     if (h < 0) return;
     const uint32_t *tg = b.tg[cur];
     int2 *link = b.link[cur];
     const int2 it = b.bond_list[k];
     const int d = it.x;
     const uint32_t g = tg[d] & GID_MASK;
-    if (b.claim[h] != g) return;
+    if (__ldcg(b.claim + h) != g) return;
     b.claim[h] = 0xFFFFFFFFu;
     link[h].y = d;
     link[d].x = h;

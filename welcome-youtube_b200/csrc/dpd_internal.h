@@ -81,7 +81,8 @@ struct DevStatus {
     unsigned int bigcell;       // largest cell population seen by the sort fix-up
     unsigned int n_grow;        // chemistry candidate lists of this step
     unsigned int n_bond;
-    unsigned int pad[3];
+    unsigned int done;          // CTAs finished in the current chemistry list kernel (the last one applies)
+    unsigned int pad[2];
 };
 
 struct EventDev {

@@ -152,25 +152,39 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart
 
 // ---------------------------------------------------------------- placement and the stable fix-up
 
-// Called by all lanes of a warp: the beads of the warp that go to the same cell
-// share one atomic on its cursor and take consecutive places in lane (= old
-// slot) order.
-__device__ __forceinline__ void place_warp(const Bufs &b, int i, bool act) {
-    const unsigned lane = lane_id();
-    const uint32_t key = act ? b.key[i] : 0xFFFFFFFFu;
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(grp) - 1;
-    uint32_t base = 0;
-    if (act && (int)lane == leader) base = atomicAdd(b.fill + key, (unsigned)__popc(grp));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (act) b.src[base + __popc(grp & ((1u << lane) - 1u))] = i;
-}
+// The beads of a warp that go to the same cell share one atomic on its cursor
+// and take consecutive places in lane (= old slot) order.
+#ifndef PLACE_ITEMS
+#define PLACE_ITEMS 4
+#endif
 
-__global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch) {
+// PLACE_ITEMS chunks per CTA: all keys are loaded before the first atomic
+__global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch, int nch) {
     pdl_begin();
-    const Chunk c = ch[blockIdx.x];
-    const int i = c.begin + (int)threadIdx.x;
-    place_warp(b, i, i < c.end);
+    const unsigned lane = lane_id();
+    uint32_t key[PLACE_ITEMS];
+    int idx[PLACE_ITEMS];
+#pragma unroll
+    for (int k = 0; k < PLACE_ITEMS; k++) {
+        const int c = (int)blockIdx.x * PLACE_ITEMS + k;
+        idx[k] = -1;
+        if (c < nch) {
+            const Chunk q = ch[c];
+            const int i = q.begin + (int)threadIdx.x;
+            if (i < q.end) idx[k] = i;
+        }
+        key[k] = idx[k] >= 0 ? b.key[idx[k]] : 0xFFFFFFFFu;
+    }
+#pragma unroll
+    for (int k = 0; k < PLACE_ITEMS; k++) {
+        const bool act = idx[k] >= 0;
+        const unsigned grp = __match_any_sync(0xffffffffu, key[k]);
+        const int leader = __ffs(grp) - 1;
+        uint32_t base = 0;
+        if (act && (int)lane == leader) base = atomicAdd(b.fill + key[k], (unsigned)__popc(grp));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (act) b.src[base + __popc(grp & ((1u << lane) - 1u))] = idx[k];
+    }
 }
 
 // bitonic sort of NP register values (static indexing only)
@@ -251,51 +265,87 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
 
 // ---------------------------------------------------------------- permute (+ integrate)
 
+#ifndef PERM_ITEMS
+#define PERM_ITEMS 1
+#endif
+
 // new slot d takes old bead src[d].  PERM_STEP applies the Groot-Warren update
 // on the way (x += dt vh + dt^2 f; vt = vh + (1/2 + lambda) dt f; vh += dt f);
 // PERM_PRIME takes the loaded velocity as the full velocity (vt = v);
 // PERM_SORT moves everything unchanged.
-template <int MODE>
-__device__ __forceinline__ void permute_one(const Bufs &b, int cur, const RepDev *__restrict__ reps, int rep, int d) {
-    const int nxt = cur ^ 1;
-    const int i = b.src[d];
-    float2 p = b.pos[cur][i], vh = b.vh[cur][i];
-    const uint32_t tg = b.tg[cur][i];
-    const int2 lk = b.link[cur][i];
-    if (MODE == PERM_STEP) {
-        const RepDev &R = reps[rep];
-        const float2 f = b.f[cur][i];
-        const float2 q = make_float2(advance1(p.x, vh.x, f.x, R.dt, R.dt2, R.L),
-                                     advance1(p.y, vh.y, f.y, R.dt, R.dt2, R.L));
-        if (!(q.x >= 0.0f && q.x < R.L && q.y >= 0.0f && q.y < R.L)) raise_flag(b.status, DPD_F_OUTSIDE);
-        b.vt[nxt][d] = make_float2(__fmaf_rn(R.cvt, f.x, vh.x), __fmaf_rn(R.cvt, f.y, vh.y));
-        vh = make_float2(__fmaf_rn(R.dt, f.x, vh.x), __fmaf_rn(R.dt, f.y, vh.y));
-        p = q;
-    } else if (MODE == PERM_PRIME) {
-        b.vt[nxt][d] = vh;
-    } else {
-        b.vt[nxt][d] = b.vt[cur][i];
-        b.f[nxt][d] = b.f[cur][i];
-    }
-    int2 nl = make_int2(lk.x >= 0 ? b.dest[lk.x] : -1, lk.y >= 0 ? b.dest[lk.y] : -1);
-    if (MODE == PERM_STEP) {
-        const RepDev &R = reps[rep];
-        const long long step = *b.step;
-        if (chem_due(R, step)) chem_in_permute(b, cur, R, step, rep, d, p, tg, lk, nl);
-    }
-    b.pos[nxt][d] = p;
-    b.vh[nxt][d] = vh;
-    b.tg[nxt][d] = tg;
-    b.link[nxt][d] = nl;
-}
-
-template <int MODE>
+// ITEMS chunks per CTA, one bead of each per thread; the loads of all items
+// are issued phase by phase (slots, state, partner slots) so that each thread
+// has several independent gathers in flight.
+template <int MODE, int ITEMS>
 __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                      const Chunk *__restrict__ ch) {
+                                                      const Chunk *__restrict__ ch, int nch) {
     pdl_begin();
-    const Chunk c = ch[blockIdx.x];
-    const int d = c.begin + (int)threadIdx.x;
-    if (d < c.end) permute_one<MODE>(b, cur, reps, c.rep, d);
+    const int nxt = cur ^ 1;
+    const int32_t *__restrict__ src = b.src;
+    const int32_t *__restrict__ dest = b.dest;
+    const float2 *__restrict__ pos0 = b.pos[cur];
+    const float2 *__restrict__ vh0 = b.vh[cur];
+    const float2 *__restrict__ f0 = b.f[cur];
+    const uint32_t *__restrict__ tg0 = b.tg[cur];
+    const int2 *__restrict__ lk0 = b.link[cur];
+    int d[ITEMS], i[ITEMS], rep[ITEMS];
+    bool act[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+        const int c = (int)blockIdx.x * ITEMS + k;
+        act[k] = false;
+        d[k] = 0;
+        rep[k] = 0;
+        if (c < nch) {
+            const Chunk q = ch[c];
+            d[k] = q.begin + (int)threadIdx.x;
+            rep[k] = q.rep;
+            act[k] = d[k] < q.end;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) i[k] = act[k] ? src[d[k]] : 0;
+    float2 p[ITEMS], vh[ITEMS], f[ITEMS];
+    uint32_t tg[ITEMS];
+    int2 lk[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+        if (!act[k]) continue;
+        p[k] = pos0[i[k]];
+        vh[k] = vh0[i[k]];
+        tg[k] = tg0[i[k]];
+        lk[k] = lk0[i[k]];
+        f[k] = MODE == PERM_PRIME ? make_float2(0.0f, 0.0f) : f0[i[k]];
+    }
+    int2 nl[ITEMS];
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++)
+        if (act[k]) nl[k] = make_int2(lk[k].x >= 0 ? dest[lk[k].x] : -1, lk[k].y >= 0 ? dest[lk[k].y] : -1);
+    const long long step = MODE == PERM_STEP ? *b.step : 0;
+#pragma unroll
+    for (int k = 0; k < ITEMS; k++) {
+        if (!act[k]) continue;
+        const int dd = d[k];
+        float2 q = p[k], v = vh[k];
+        if (MODE == PERM_STEP) {
+            const RepDev &R = reps[rep[k]];
+            const float2 ff = f[k];
+            q = make_float2(advance1(q.x, v.x, ff.x, R.dt, R.dt2, R.L), advance1(q.y, v.y, ff.y, R.dt, R.dt2, R.L));
+            if (!(q.x >= 0.0f && q.x < R.L && q.y >= 0.0f && q.y < R.L)) raise_flag(b.status, DPD_F_OUTSIDE);
+            b.vt[nxt][dd] = make_float2(__fmaf_rn(R.cvt, ff.x, v.x), __fmaf_rn(R.cvt, ff.y, v.y));
+            v = make_float2(__fmaf_rn(R.dt, ff.x, v.x), __fmaf_rn(R.dt, ff.y, v.y));
+            if (chem_due(R, step)) chem_in_permute(b, cur, R, step, rep[k], dd, q, tg[k], lk[k], nl[k]);
+        } else if (MODE == PERM_PRIME) {
+            b.vt[nxt][dd] = v;
+        } else {
+            b.vt[nxt][dd] = b.vt[cur][i[k]];
+            b.f[nxt][dd] = f[k];
+        }
+        b.pos[nxt][dd] = q;
+        b.vh[nxt][dd] = v;
+        b.tg[nxt][dd] = tg[k];
+        b.link[nxt][dd] = nl[k];
+    }
 }
 
 // ---------------------------------------------------------------- pair + bond forces
@@ -658,7 +708,7 @@ void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
 }
 
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s) {
-    launch_pdl(k_place, nbch, BEAD_TPB, 0, s, b, bch);
+    launch_pdl(k_place, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch);
 }
 
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s) {
@@ -667,9 +717,10 @@ void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s) {
 
 void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
                     cudaStream_t s) {
-    if (mode == PERM_STEP) launch_pdl(k_permute<PERM_STEP>, nbch, BEAD_TPB, 0, s, b, cur, rep, bch);
-    else if (mode == PERM_PRIME) k_permute<PERM_PRIME><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
-    else k_permute<PERM_SORT><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    const int g4 = (nbch + PERM_ITEMS - 1) / PERM_ITEMS;
+    if (mode == PERM_STEP) launch_pdl(k_permute<PERM_STEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch);
+    else if (mode == PERM_PRIME) k_permute<PERM_PRIME, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch);
+    else k_permute<PERM_SORT, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch);
 }
 
 void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool pair, bool bond,
