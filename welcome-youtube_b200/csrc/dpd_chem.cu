@@ -45,22 +45,6 @@ __global__ void __launch_bounds__(BEAD_TPB) k_chem_scan(Bufs b, int cur, const R
 
 #define LIST_GRID 148
 
-// True in the last CTA of the grid to get here, after every CTA's writes are
-// visible to it (fence, then a counter; nothing waits).  The last CTA resets
-// the counter for the next launch.
-__device__ __forceinline__ bool last_cta(unsigned int *done) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        last = atomicAdd(done, 1u) == gridDim.x - 1;
-        if (last) *done = 0u;
-    }
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
-}
-
 // stage 2: requests, one warp per listed P, then the claims applied by the last CTA
 __global__ void __launch_bounds__(BEAD_TPB) k_chem_grow(Bufs b, int cur, const RepDev *__restrict__ reps) {
     pdl_begin();

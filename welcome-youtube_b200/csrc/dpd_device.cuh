@@ -229,6 +229,24 @@ __device__ __forceinline__ void pdl_begin() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// ---------------------------------------------------------------- grid helpers
+
+// True in the last CTA of the grid to get here, after every CTA's writes are
+// visible to it (fence, then a counter; nothing waits).  The last CTA resets
+// the counter for the next launch.
+__device__ __forceinline__ bool last_cta(unsigned int *done) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+        if (last) *done = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
 // ---------------------------------------------------------------- warp helpers
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }

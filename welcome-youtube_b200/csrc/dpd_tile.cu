@@ -210,19 +210,19 @@ __device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int
     if (fmax > 2048.0f) raise_flag(status, DPD_F_FORCE);
 }
 
-// bonds, the force to HBM, the next cell key and its count of one owned bead
+// bonds, the force to HBM and the next cell key of one owned bead, from its
+// links lk, its bond partners' positions pj[2] and its half-step velocity v
+// (loaded by the caller)
 template <bool NEXTKEY>
-__device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev &R, int g, float2 pi, long long qx,
-                                            long long qy, float &mb, uint32_t &key) {
-    const float2 *__restrict__ pos = b.pos[cur];
+__device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepDev &R, int g, float2 pi, long long qx,
+                                              long long qy, int2 lk, const float2 (&pj)[2], float2 v, float &mb,
+                                              uint32_t &key) {
     const float L = R.L, h = R.halfL, kb = R.kb, r0 = R.r0;
-    const int2 lk = b.link[cur][g];
 #pragma unroll
     for (int e = 0; e < 2; e++) {
         const int j = e ? lk.y : lk.x;
         if (j < 0) continue;
-        const float2 pj = pos[j];
-        const float dx = minimg(__fsub_rn(pj.x, pi.x), L, h), dy = minimg(__fsub_rn(pj.y, pi.y), L, h);
+        const float dx = minimg(__fsub_rn(pj[e].x, pi.x), L, h), dy = minimg(__fsub_rn(pj[e].y, pi.y), L, h);
         const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
         mb = fmaxf(mb, r);
         const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
@@ -233,12 +233,25 @@ __device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev
     if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);
     b.f[cur][g] = fs;
     if (NEXTKEY) {
-        const float2 v = b.vh[cur][g];
         int cx, cy;
         key = (uint32_t)(R.c0 + cell_xy(R, advance1(pi.x, v.x, fs.x, R.dt, R.dt2, L),
                                         advance1(pi.y, v.y, fs.y, R.dt, R.dt2, L), cx, cy));
     }
 }
+
+// the same with its own loads (the crowded-tile path)
+template <bool NEXTKEY>
+__device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev &R, int g, float2 pi, long long qx,
+                                            long long qy, float &mb, uint32_t &key) {
+    const int2 lk = b.link[cur][g];
+    float2 pj[2];
+    pj[0] = lk.x >= 0 ? b.pos[cur][lk.x] : pi;
+    pj[1] = lk.y >= 0 ? b.pos[cur][lk.y] : pi;
+    const float2 v = NEXTKEY ? b.vh[cur][g] : make_float2(0.0f, 0.0f);
+    finish_loaded<NEXTKEY>(b, cur, R, g, pi, qx, qy, lk, pj, v, mb, key);
+}
+
+#define EPI_ITEMS 2  // owned beads per thread per round of the epilogue
 
 template <bool NEXTKEY>
 __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
@@ -360,18 +373,47 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
             else tile_pairs<false, 0>(S, pc, LW, LH, td.w, td.h, b.status);
         }
         __syncthreads();
-        // ---- epilogue: a warp per owned column (owned rows are contiguous in HBM)
-        for (int c = 1 + wq; c <= td.w; c += TILE_WARPS) {
-            const int k0 = S.lcs[c * LH + 1], k1 = S.lcs[c * LH + td.h + 1], g0 = S.gst[c * LH + 1];
-            for (int kb = k0; kb < k1; kb += 32) {
-                const int k = kb + lane;
-                const bool act = k < k1;
+        // ---- epilogue over the local index range of the owned columns; halo beads
+        // (rows 0 and h + 1) in that range are skipped.  Loads of a round first.
+        const int e0 = S.lcs[LH + 1], e1 = S.lcs[td.w * LH + td.h + 1];
+        const float2 *__restrict__ gpos = b.pos[cur];
+        for (int base = e0; base < e1; base += EPI_ITEMS * TILE_TPB) {
+            int gg[EPI_ITEMS];
+            bool own[EPI_ITEMS];
+#pragma unroll
+            for (int j = 0; j < EPI_ITEMS; j++) {
+                const int k = base + j * TILE_TPB + tid;
+                own[j] = false;
+                gg[j] = 0;
+                if (k < e1) {
+                    const int v = S.lxy[k], ly = v & 255, l = (v >> 8) * LH + ly;
+                    own[j] = ly >= 1 && ly <= td.h;
+                    gg[j] = S.gst[l] + (k - S.lcs[l]);
+                }
+            }
+            int2 lk[EPI_ITEMS];
+            float2 vv[EPI_ITEMS];
+#pragma unroll
+            for (int j = 0; j < EPI_ITEMS; j++) {
+                lk[j] = own[j] ? b.link[cur][gg[j]] : make_int2(-1, -1);
+                vv[j] = (NEXTKEY && own[j]) ? b.vh[cur][gg[j]] : make_float2(0.0f, 0.0f);
+            }
+            float2 pj[EPI_ITEMS][2];
+#pragma unroll
+            for (int j = 0; j < EPI_ITEMS; j++) {
+                pj[j][0] = lk[j].x >= 0 ? gpos[lk[j].x] : make_float2(0.0f, 0.0f);
+                pj[j][1] = lk[j].y >= 0 ? gpos[lk[j].y] : make_float2(0.0f, 0.0f);
+            }
+#pragma unroll
+            for (int j = 0; j < EPI_ITEMS; j++) {
+                const int k = base + j * TILE_TPB + tid;
                 uint32_t key = 0;
-                const int g = g0 + (k - k0);
-                if (act) finish_bead<NEXTKEY>(b, cur, R, g, S.pos[k], S.accx[k], S.accy[k], mb, key);
+                if (own[j])
+                    finish_loaded<NEXTKEY>(b, cur, R, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j], vv[j], mb,
+                                           key);
                 if (NEXTKEY) {
-                    count_key(b.count, key, act);
-                    if (act) b.key[g] = key;
+                    count_key(b.count, key, own[j]);
+                    if (own[j]) b.key[gg[j]] = key;
                 }
             }
         }
