@@ -91,6 +91,14 @@ typedef struct {
     double r_bond;             /* free T - free H bonding radius */
     int64_t warmup;            /* repulsion ramp length (warmup; 0 = off) */
     int64_t warm_end;          /* step at which the ramp ends (a fresh soup: = warmup) */
+    double k_angle;            /* U = k_angle (1 - cos theta) on consecutive chain triplets (k_angle) */
+    double stir_A;             /* body force f_x = stir_A sin(2 pi stir_n y / L), net force removed (stir_A) */
+    int32_t stir_n;            /* sine periods across the box (stir_n) */
+    int32_t pad2;
+    double kT_amp;             /* kT(t) = kT + kT_amp sin(2 pi t / kT_period) in the noise (kT_amp) */
+    double kT_period;          /* (kT_period) */
+    double t_anchor;           /* time of step step_anchor: t(step) = t_anchor + (step - step_anchor) dt */
+    int64_t step_anchor;
 } dpd_params;
 
 /* One chemistry event, the reference's events.csv row (oercel.c:788-798)

@@ -26,6 +26,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
 #define SQRT12 3.4641016151377545870548926830117
 
 /* ------------------------------------------------------------------ counter-based RNGs */
@@ -156,6 +160,26 @@ static inline void pair_term(const ora_params *P, double sdt, int64_t step, doub
 /* sigma / sqrt(dt) with sigma = sqrt(2 gamma kT), oercel.c:579, 1204 */
 double ora_sdt(const ora_params *P) { return sqrt(2.0 * P->gamma * P->kT) / sqrt(P->dt); }
 
+/* sigma / sqrt(dt) of a step with the temperature cycle: kT_at (oercel.c:622-624)
+ * at t = t_anchor + (step - step_anchor) dt (oercel.c:2353), then oercel.c:1204 */
+double ora_sdt_at(const ora_params *P, int64_t step) {
+    if (P->kT_amp == 0.0) return ora_sdt(P);
+    const double t = P->t_anchor + (double)(step - P->step_anchor) * P->dt;
+    const double kT = P->kT + P->kT_amp * sin(2.0 * M_PI * t / P->kT_period);
+    return sqrt(2.0 * P->gamma * kT) / sqrt(P->dt);
+}
+
+/* Stirring body force (oercel.c:1166-1195): f_x = A sin(2 pi n y / L) on every
+ * bead, minus the mean over the beads so that the net force is zero. Added to fx. */
+void ora_stir_forces(const ora_params *P, int32_t n, const float *y, double *fx) {
+    if (P->stir_A == 0.0 || n < 1) return;
+    const double kn = (double)P->stir_n / P->L;
+    double sum = 0.0;
+    for (int i = 0; i < n; i++) sum += P->stir_A * sin(2.0 * M_PI * kn * (double)y[i]);
+    const double mean = sum / n;
+    for (int i = 0; i < n; i++) fx[i] += P->stir_A * sin(2.0 * M_PI * kn * (double)y[i]) - mean;
+}
+
 /* Pair forces through the cell list (input sorted by ora_sort): every bead
  * sums over the 3x3 neighbour cells (reference stencil oercel.c:1060-1120
  * visits the same pairs once each; here each pair is seen from both ends). */
@@ -163,7 +187,7 @@ void ora_pair_forces(const ora_params *P, int32_t n, const float *x, const float
                      const float *vty, const uint8_t *type, const uint32_t *gid, const int32_t *cstart, int64_t step,
                      int32_t with_noise, double *fx, double *fy) {
     const int ncx = P->ncx, ncy = P->ncy;
-    const double L = P->L, sdt = with_noise ? ora_sdt(P) : 0.0;
+    const double L = P->L, sdt = with_noise ? ora_sdt_at(P, step) : 0.0;
     (void)n;
     for (int cx = 0; cx < ncx; cx++)
         for (int cy = 0; cy < ncy; cy++) {
@@ -192,7 +216,7 @@ void ora_pair_forces(const ora_params *P, int32_t n, const float *x, const float
 void ora_pair_forces_brute(const ora_params *P, int32_t n, const float *x, const float *y, const float *vtx,
                            const float *vty, const uint8_t *type, const uint32_t *gid, int64_t step,
                            int32_t with_noise, double *fx, double *fy) {
-    const double L = P->L, sdt = with_noise ? ora_sdt(P) : 0.0;
+    const double L = P->L, sdt = with_noise ? ora_sdt_at(P, step) : 0.0;
     for (int i = 0; i < n; i++) {
         double ax = 0.0, ay = 0.0;
         for (int j = 0; j < n; j++) {
@@ -207,7 +231,7 @@ void ora_pair_forces_brute(const ora_params *P, int32_t n, const float *x, const
 }
 
 /* Harmonic bonds U = k/2 (r - r0)^2 along the prev/next links, added to
- * fx/fy (oercel.c:1272-1308 without angle terms).  Returns the largest bond
+ * fx/fy (oercel.c:1272-1308), and the angle terms when k_angle != 0.  Returns the largest bond
  * length in *maxbond (running max, oercel.c:1292). */
 void ora_bond_forces(const ora_params *P, int32_t n, const float *x, const float *y, const int32_t *next,
                      double *fx, double *fy, double *maxbond) {
@@ -224,6 +248,35 @@ void ora_bond_forces(const ora_params *P, int32_t n, const float *x, const float
         fy[j] += f * dy;
         fx[i] -= f * dx;
         fy[i] -= f * dy;
+    }
+    /* angle terms U = k (1 - cos theta) of every consecutive triplet (prev, j,
+     * next) along the links (chain_forces_linear, oercel.c:1290-1307) */
+    if (P->k_angle != 0.0) {
+        int32_t *prev = (int32_t *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int32_t));
+        for (int i = 0; i < n; i++) prev[i] = -1;
+        for (int i = 0; i < n; i++)
+            if (next[i] >= 0) prev[next[i]] = i;
+        const double ka = P->k_angle;
+        for (int j = 0; j < n; j++) {
+            const int i = prev[j], k = next[j];
+            if (i < 0 || k < 0) continue;
+            const double ax = minimg((double)x[j] - (double)x[i], L), ay = minimg((double)y[j] - (double)y[i], L);
+            const double cx = minimg((double)x[k] - (double)x[j], L), cy = minimg((double)y[k] - (double)y[j], L);
+            const double la = sqrt(ax * ax + ay * ay), lc = sqrt(cx * cx + cy * cy);
+            const double ilac = 1.0 / (la * lc);
+            const double cs = (ax * cx + ay * cy) * ilac;
+            const double dUax = -ka * (cx * ilac - cs * ax / (la * la));
+            const double dUay = -ka * (cy * ilac - cs * ay / (la * la));
+            const double dUcx = -ka * (ax * ilac - cs * cx / (lc * lc));
+            const double dUcy = -ka * (ay * ilac - cs * cy / (lc * lc));
+            fx[i] += dUax;
+            fy[i] += dUay;
+            fx[j] += -dUax + dUcx;
+            fy[j] += -dUay + dUcy;
+            fx[k] -= dUcx;
+            fy[k] -= dUcy;
+        }
+        free(prev);
     }
     *maxbond = mb;
 }

@@ -36,6 +36,12 @@ typedef struct {
     uint64_t seed;
     int32_t noise;          /* 0 = Philox4x32-10, 1 = reference mix13 hash */
     int32_t pad;
+    double k_angle;         /* U = k_angle (1 - cos) on consecutive chain triplets */
+    double stir_A;          /* stirring f_x = stir_A sin(2 pi stir_n y / L), mean removed */
+    int32_t stir_n, pad2;
+    double kT_amp, kT_period; /* kT(t) = kT + kT_amp sin(2 pi t / kT_period) */
+    double t_anchor;        /* t(step) = t_anchor + (step - step_anchor) dt */
+    int64_t step_anchor;
 } ora_params;
 
 typedef struct {

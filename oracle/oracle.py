@@ -33,7 +33,10 @@ class OraParams(C.Structure):
                 ("icsx", C.c_double), ("icsy", C.c_double),
                 ("dt", C.c_double), ("lam", C.c_double), ("gamma", C.c_double), ("kT", C.c_double),
                 ("a", C.c_double * (MAXT * MAXT)), ("k_bond", C.c_double), ("r0", C.c_double),
-                ("seed", C.c_uint64), ("noise", C.c_int32), ("pad", C.c_int32)]
+                ("seed", C.c_uint64), ("noise", C.c_int32), ("pad", C.c_int32),
+                ("k_angle", C.c_double), ("stir_A", C.c_double), ("stir_n", C.c_int32), ("pad2", C.c_int32),
+                ("kT_amp", C.c_double), ("kT_period", C.c_double), ("t_anchor", C.c_double),
+                ("step_anchor", C.c_int64)]
 
 
 class OraF32(C.Structure):
@@ -75,6 +78,9 @@ def _load():
     lib.ora_cell_of.argtypes = [P, C.c_float, C.c_float]
     lib.ora_cell_of.restype = C.c_int32
     lib.ora_sort.argtypes = [P, C.c_int32, f32p, f32p, i32p, i32p, i32p]
+    lib.ora_stir_forces.argtypes = [P, C.c_int32, f32p, f64p]
+    lib.ora_sdt_at.argtypes = [P, C.c_int64]
+    lib.ora_sdt_at.restype = C.c_double
     lib.ora_pair_forces.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u8p, u32p, i32p, C.c_int64, C.c_int32,
                                     f64p, f64p]
     lib.ora_pair_forces_brute.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u8p, u32p, C.c_int64, C.c_int32,
@@ -108,9 +114,12 @@ def lib():
     return _lib
 
 
-def params(L, amat, *, dt=0.02, lam=0.65, gamma=4.5, kT=1.0, k_bond=100.0, r0=0.5, seed=0, noise=0):
+def params(L, amat, *, dt=0.02, lam=0.65, gamma=4.5, kT=1.0, k_bond=100.0, r0=0.5, seed=0, noise=0, k_angle=0.0,
+           stir_A=0.0, stir_n=1, kT_amp=0.0, kT_period=1000.0, t_anchor=0.0, step_anchor=0):
     """Oracle parameter block; amat is a square array of up to 8x8 repulsions."""
     p = OraParams()
+    p.k_angle, p.stir_A, p.stir_n = float(k_angle), float(stir_A), int(stir_n)
+    p.kT_amp, p.kT_period, p.t_anchor, p.step_anchor = float(kT_amp), float(kT_period), float(t_anchor), int(step_anchor)
     p.L = float(L)
     p.ncx = p.ncy = int(math.floor(L))
     p.icsx = p.ncx / p.L
@@ -183,6 +192,16 @@ def bond_forces(p, st, fx=None, fy=None):
     mb = C.c_double(0.0)
     lib().ora_bond_forces(C.byref(p), n, st["x"], st["y"], st["next"], fx, fy, C.byref(mb))
     return fx, fy, mb.value
+
+
+def stir_forces(p, st, fx):
+    """add the stirring body force (mean removed) to fx in place"""
+    lib().ora_stir_forces(C.byref(p), len(st["y"]), st["y"], fx)
+    return fx
+
+
+def sdt_at(p, step):
+    return lib().ora_sdt_at(C.byref(p), int(step))
 
 
 def integrate_f32(p, st):

@@ -81,6 +81,42 @@ def step_fixture(L, seed, name, steps=(12345,)):
     np.savez_compressed(os.path.join(HERE, name), **out)
 
 
+EXTRAS = dict(k_angle=10, lip_nT=3, stir_A=1.5, stir_n=2, kT_amp=0.4, kT_period=37)
+
+
+def extras_fixture(L=12.5, seed=21, step=777):
+    """angle terms, stirring and the temperature cycle: one sorted state
+    (nsub = 1), the reference's pair forces at `step` (stirring body force and
+    kT(t) noise included) and its bonded forces (bonds + angles)"""
+    kv = dict(CONFIG1, L=L, seed=seed, f_lip=0.3, c_N=0.1, **EXTRAS)
+    r = O.Ref(**kv)
+    a = r.get()
+    rng = np.random.default_rng(seed)
+    n = len(a["x"])
+    Lf = float(np.float32(L))
+    for k in ("x", "y"):  # bent, stretched chains: bonds and angles under load
+        a[k] = np.mod(a[k] + 0.12 * rng.standard_normal(n) * (a["mpos"] >= 0), Lf)
+    for k in ("x", "y", "vx", "vy"):
+        a[k] = f32(a[k])
+        if k in ("x", "y"):
+            a[k][a[k] >= Lf] = 0.0
+    a["vtx"] = f32(a["vx"] + 0.3 * rng.standard_normal(n))
+    a["vty"] = f32(a["vy"])
+    r.set(a)
+    r.sort()
+    b = r.get()
+    out = dict(x0=a["x"], y0=a["y"], vtx0=a["vtx"], vty0=a["vty"], type0=a["type"], nxt0=a["nxt"], gid=b["gid"],
+               cstart=r.cells(), L=np.float64(L), step=np.int64(step), seed=np.int64(seed))
+    r.pair(step)
+    f = r.get()
+    out["fx"], out["fy"] = f["fx"], f["fy"]
+    mb = r.bonded()
+    g = r.get()
+    out["bfx"], out["bfy"] = g["fx"] - f["fx"], g["fy"] - f["fy"]
+    out["maxbond"] = np.float64(mb)
+    np.savez_compressed(os.path.join(HERE, f"extras_L{str(L).replace('.', 'p')}_seed{seed}.npz"), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -146,17 +182,17 @@ RUN_INI = dict(L=10, rho=4, dt=0.02, gamma=4.5, kT=1, k_bond=100, r0=0.5, k_angl
                a_H_N=25, a_N_T=75)
 
 
-def run_fixture():
+def run_fixture(name="run_L10_seed3.npz", **over):
     """two runs of the reference engine's executable (oracle/_ref/oercel_portable):
     a fresh soup with the repulsion warm-up for 24 steps, then a restart from its
     checkpoint to step 36.  Stores the ini, stats.csv texts, snapshots and the
-    checkpoint as bytes."""
+    checkpoint as bytes.  `over` replaces keys of RUN_INI."""
     import subprocess
     import tempfile
     exe = os.path.join(HERE, "..", "..", "oracle", "_ref", "oercel_portable")
     with tempfile.TemporaryDirectory() as td:
         ini = os.path.join(td, "p.ini")
-        text = "".join(f"{k} = {v}\n" for k, v in RUN_INI.items())
+        text = "".join(f"{k} = {v}\n" for k, v in dict(RUN_INI, **over).items())
         with open(ini, "w") as f:
             f.write(text)
         a, b = os.path.join(td, "a"), os.path.join(td, "b")
@@ -167,7 +203,7 @@ def run_fixture():
             with open(path, "rb") as f:
                 return np.frombuffer(f.read(), np.uint8)
 
-        np.savez_compressed(os.path.join(HERE, "run_L10_seed3.npz"), ini=np.frombuffer(text.encode(), np.uint8),
+        np.savez_compressed(os.path.join(HERE, name), ini=np.frombuffer(text.encode(), np.uint8),
                             stats_a=rd(f"{a}/stats.csv"), stats_b=rd(f"{b}/stats.csv"),
                             snap_0=rd(f"{a}/snap_0000000000.bin"), snap_12=rd(f"{a}/snap_0000000012.bin"),
                             snap_24=rd(f"{a}/snap_0000000024.bin"), snap_36=rd(f"{b}/snap_0000000036.bin"),
@@ -184,5 +220,8 @@ if __name__ == "__main__":
     trajectory_fixture()
     stats_fixture()
     run_fixture()
+    run_fixture("run_extras_L10_seed4.npz", seed=4, k_angle=10, lip_nT=3, stir_A=1.0, stir_n=1, kT_amp=0.3,
+                kT_period=5)
+    extras_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

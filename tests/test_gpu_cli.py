@@ -24,10 +24,12 @@ from oercel_b200 import cli
 pytestmark = pytest.mark.gpu
 EXE = os.path.join(PKG, "bin", "oercel_b200")
 G = "run_L10_seed3.npz"
+# the same runs with angle terms (k_angle = 10, H-T-T-T lipids), stirring and the temperature cycle
+G_EXTRAS = "run_extras_L10_seed4.npz"
 
 
-def fixture_bytes(key):
-    return bytes(golden(G)[key])
+def fixture_bytes(key, name=G):
+    return bytes(golden(name)[key])
 
 
 def run_exe(ini, out, *over, timeout=600):
@@ -41,6 +43,12 @@ def run_exe(ini, out, *over, timeout=600):
 def ini(tmp_path):
     p = tmp_path / "p.ini"
     p.write_bytes(fixture_bytes("ini"))
+    return p
+
+
+def write_ini(tmp_path, name):
+    p = tmp_path / "p.ini"
+    p.write_bytes(fixture_bytes("ini", name))
     return p
 
 
@@ -59,10 +67,10 @@ def check_stats(got_text, ref_text):
         assert float(g[11]) == pytest.approx(float(r[11]), rel=2e-3), (g, r)  # max_bond
 
 
-def check_snapshot(path, ref_key):
+def check_snapshot(path, ref_key, name=G):
     ref_path = path + ".ref"
     with open(ref_path, "wb") as f:
-        f.write(fixture_bytes(ref_key))
+        f.write(fixture_bytes(ref_key, name))
     a, b = cli.read_snapshot(path), cli.read_snapshot(ref_path)
     assert (a["N"], a["step"], a["L"]) == (b["N"], b["step"], b["L"])
     assert a["time"] == pytest.approx(b["time"], abs=1e-12)
@@ -74,26 +82,30 @@ def check_snapshot(path, ref_key):
         assert np.abs(d).max() < 1e-3, k
 
 
-def test_run_matches_the_reference_executable(cuda_ok, ini, tmp_path):
+@pytest.mark.parametrize("name", [G, G_EXTRAS])
+def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
+    ini = write_ini(tmp_path, name)
     out = tmp_path / "run"
     run_exe(ini, out, "noise=mix13")
-    assert (out / "snap_0000000000.bin").read_bytes() == fixture_bytes("snap_0")
-    check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_a").decode())
-    check_snapshot(str(out / "snap_0000000012.bin"), "snap_12")
-    check_snapshot(str(out / "snap_0000000024.bin"), "snap_24")
+    assert (out / "snap_0000000000.bin").read_bytes() == fixture_bytes("snap_0", name)
+    check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_a", name).decode())
+    check_snapshot(str(out / "snap_0000000012.bin"), "snap_12", name)
+    check_snapshot(str(out / "snap_0000000024.bin"), "snap_24", name)
     log = (out / "log.txt").read_text()
     assert log.rstrip().endswith("done at step 24") and "timing:" in log
     assert "warmup = 8" in (out / "params.ini").read_text()
     assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] == 24
 
 
-def test_restart_from_a_reference_checkpoint(cuda_ok, ini, tmp_path):
+@pytest.mark.parametrize("name", [G, G_EXTRAS])
+def test_restart_from_a_reference_checkpoint(cuda_ok, tmp_path, name):
+    ini = write_ini(tmp_path, name)
     ck = tmp_path / "ref_ckpt.bin"
-    ck.write_bytes(fixture_bytes("ckpt_24"))
+    ck.write_bytes(fixture_bytes("ckpt_24", name))
     out = tmp_path / "cont"
     run_exe(ini, out, "noise=mix13", f"restart={ck}", "steps=36")
-    check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_b").decode())
-    check_snapshot(str(out / "snap_0000000036.bin"), "snap_36")
+    check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_b", name).decode())
+    check_snapshot(str(out / "snap_0000000036.bin"), "snap_36", name)
     assert "restart from" in (out / "log.txt").read_text()
 
 

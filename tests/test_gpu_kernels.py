@@ -174,3 +174,50 @@ def test_warmup_in_the_fused_step(cuda_ok, force_kernel):
         rx, ry = O.pair_forces(op, s, e.cells(), st, noise=True)
         rx, ry, _ = O.bond_forces(op, s, rx, ry)
         assert rel_err(s["fx"], rx) < FORCE_TOL and rel_err(s["fy"], ry) < FORCE_TOL, st
+
+
+def extras_engine(force_kernel=0):
+    """the state of tests/golden/extras_L12p5_seed21.npz with angle terms,
+    stirring and the temperature cycle on (the reference's own forces there
+    pin the oracle, tests/test_oracle.py)"""
+    g = golden("extras_L12p5_seed21.npz")
+    p = params(L=float(g["L"]), seed=int(g["seed"]), noise="mix13", k_angle=10, stir_A=1.5, stir_n=2, kT_amp=0.4,
+               kT_period=37)
+    prev, nxt = links_from_next(g["nxt0"])
+    e = engine_with(p, g["x0"], g["y0"], g["vtx0"], g["vty0"], g["type0"], prev, nxt)
+    e.set_tuning(force_kernel=force_kernel)
+    e.build_cells()
+    op = O.params(float(np.float32(p.L)), np.array(p.a, dtype=np.float64), dt=p.dt, lam=p["lambda"], gamma=p.gamma,
+                  kT=p.kT, k_bond=p.k_bond, r0=p.r0, seed=p.seed, noise=1, k_angle=10, stir_A=1.5, stir_n=2,
+                  kT_amp=0.4, kT_period=37)
+    return g, p, e, op
+
+
+def test_angle_terms_match_oracle(cuda_ok):
+    g, p, e, op = extras_engine()
+    s = oracle_state(e.state())
+    bx, by, mb = e.bond_forces(0)
+    rx, ry, rmb = O.bond_forces(op, s)
+    assert rel_err(bx, rx) < FORCE_TOL and rel_err(by, ry) < FORCE_TOL
+    assert abs(mb - rmb) < 1e-6
+    assert abs(bx.astype(np.float64).sum()) < 1e-9  # the three shares of every angle term cancel exactly
+
+
+def test_stirring_and_temperature_cycle_match_oracle(cuda_ok):
+    g, p, e, op = extras_engine()
+    s = oracle_state(e.state())
+    step = int(g["step"])
+    fx, fy = e.pair_forces(0, step)
+    rx, ry = O.pair_forces(op, s, e.cells(), step, noise=True)
+    O.stir_forces(op, s, rx)
+    assert rel_err(fx, rx) < FORCE_TOL and rel_err(fy, ry) < FORCE_TOL
+    assert fx.astype(np.float64).sum() == 0.0  # net stirring force exactly zero in fixed point
+
+
+def test_extras_tile_and_bead_kernels_agree(cuda_ok):
+    runs = []
+    for fk in (0, 1):
+        g, p, e, op = extras_engine(fk)
+        e.forces(int(g["step"]))
+        runs.append(e.state())
+    assert np.array_equal(runs[0]["fx"], runs[1]["fx"]) and np.array_equal(runs[0]["fy"], runs[1]["fy"])

@@ -171,3 +171,32 @@ def test_pair_hist_matches_brute_force():
     r = np.hypot(dx, dy)[np.triu_indices(len(idx), 1)]
     hb, _ = np.histogram(r[r < 2.0], bins=64, range=(0, 2))
     assert np.array_equal(h, hb)
+
+
+def _extras_case():
+    g = golden("extras_L12p5_seed21.npz")
+    p = O.params(float(g["L"]), amat_config(), seed=int(g["seed"]), noise=1, k_angle=10, stir_A=1.5, stir_n=2,
+                 kT_amp=0.4, kT_period=37)
+    return g, p
+
+
+def test_angle_forces_match_reference():
+    """bonds + angle terms U = k (1 - cos theta) of the bent chains (chain_forces_linear)"""
+    g, p = _extras_case()
+    st = _sorted_state(g)
+    bx, by, mb = O.bond_forces(p, st)
+    assert np.abs(bx - g["bfx"]).max() < 1e-9 and np.abs(by - g["bfy"]).max() < 1e-9
+    assert mb == pytest.approx(float(g["maxbond"]), rel=1e-14)
+    p.k_angle = 0.0
+    assert np.abs(O.bond_forces(p, st)[0] - g["bfx"]).max() > 1.0  # the angles matter in this state
+
+
+def test_stirring_and_temperature_cycle_match_reference():
+    """pair forces with the kT(t) noise amplitude plus the stirring body force"""
+    g, p = _extras_case()
+    st = _sorted_state(g)
+    step = int(g["step"])
+    fx, fy = O.pair_forces(p, st, g["cstart"], step, noise=True)
+    O.stir_forces(p, st, fx)
+    assert np.abs(fx - g["fx"]).max() < 1e-9 and np.abs(fy - g["fy"]).max() < 1e-9
+    assert O.sdt_at(p, step) != pytest.approx(O.lib().ora_sdt(C.byref(p)))

@@ -50,6 +50,7 @@ struct dpd_handle {
     TileDesc *d_tiles = nullptr;
     int ntiles = 0;
     bool any_chem = false;
+    bool any_stir = false;      // some replica stirs: its term sums are cleared before each permute
     bool keys_valid = false;
     int64_t step = 0;
     // CUDA graphs of gsteps consecutive steps, one per starting buffer parity
@@ -78,6 +79,9 @@ extern "C" int dpd_params_default(dpd_params *p) {
     for (int i = 0; i < DPD_MAXT * DPD_MAXT; i++) p->a[i] = 25.0;
     p->k_bond = 100.0;
     p->r0 = 0.5;
+    p->k_angle = 10.0;
+    p->stir_n = 1;
+    p->kT_period = 1000.0;
     p->seed = 1;
     p->noise = 0;
     p->chem = 0;
@@ -145,6 +149,23 @@ static int make_rep(const dpd_params &p, int b0, int n, int c0, RepDev &R) {
     if (p.warmup < 0) return fail(DPD_E_ARG, "warmup must be >= 0");
     R.warm_end = (long long)p.warm_end;
     R.warm_inv = p.warmup > 0 ? 1.0 / (double)p.warmup : 0.0;
+    if (p.k_angle < 0.0 || !std::isfinite(p.k_angle)) return fail(DPD_E_ARG, "k_angle must be >= 0");
+    R.ka = (float)p.k_angle;
+    if (p.stir_A != 0.0 && p.stir_n < 1) return fail(DPD_E_ARG, "stir_n must be >= 1");
+    if (!std::isfinite(p.stir_A)) return fail(DPD_E_ARG, "stir_A must be finite");
+    R.stir_A = (float)p.stir_A;
+    R.stir_k = p.stir_A != 0.0 ? (double)p.stir_n / p.L : 0.0;
+    if (p.kT_amp != 0.0) {
+        if (!(p.kT_period > 0.0)) return fail(DPD_E_ARG, "kT_period must be > 0");
+        if (!(p.kT - std::fabs(p.kT_amp) > 0.0)) return fail(DPD_E_ARG, "kT - |kT_amp| must be > 0");
+    }
+    R.kT = p.kT;
+    R.kT_amp = p.kT_amp;
+    R.kT_w = p.kT_amp != 0.0 ? 2.0 * M_PI / p.kT_period : 0.0;
+    R.gamma_d = p.gamma;
+    R.dt_d = p.dt;
+    R.t_anchor = p.t_anchor;
+    R.step_anchor = (long long)p.step_anchor;
     return DPD_OK;
 }
 
@@ -225,6 +246,7 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
         if (n_beads[r] < 2) return fail(DPD_E_ARG, "replica %d: need at least 2 beads", r);
         TRY(make_rep(params[r], (int)b0, n_beads[r], (int)c0, h->rh[r]));
         h->any_chem = h->any_chem || params[r].chem;
+        h->any_stir = h->any_stir || params[r].stir_A != 0.0;
         b0 += n_beads[r];
         c0 += h->rh[r].ncell;
         h->nmax = std::max(h->nmax, (int)n_beads[r]);
@@ -284,6 +306,8 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.step, 1));
     TRY(dalloc(h, &b.obs, (size_t)nrep * OBS_N));
     TRY(dalloc(h, &b.hist, 4096));
+    TRY(dalloc(h, &b.stir, (size_t)nrep));
+    CK(cudaMemset(b.stir, 0, (size_t)nrep * sizeof(long long)));
     // staging for set/get state: 8 float + 3 int32 + 1 byte arrays of nmax
     TRY(dalloc(h, &h->stage, (size_t)h->nmax * (8 * 4 + 3 * 4 + 1) + 16 * 256));
     CK(cudaMemset(b.count, 0, (C + 4) * sizeof(uint32_t)));
@@ -447,6 +471,11 @@ extern "C" int dpd_set_dynamics(dpd_handle *h, int32_t r, const float *vhx, cons
 
 // ---------------------------------------------------------------- phases
 
+// the stirring sums are accumulated by the permute kernel and read by the forces
+static void clear_stir(dpd_handle *h) {
+    if (h->any_stir) cudaMemsetAsync(h->b.stir, 0, (size_t)h->nrep * sizeof(long long), h->s);
+}
+
 static void enqueue_sort(dpd_handle *h, PermuteMode mode) {
     // counts of the CURRENT positions
     cudaMemsetAsync(h->b.count, 0, (size_t)(h->C + 4) * sizeof(uint32_t), h->s);
@@ -454,6 +483,7 @@ static void enqueue_sort(dpd_handle *h, PermuteMode mode) {
     launch_scan(h->b, h->C, false, h->s);
     launch_place(h->b, h->d_bch, h->nbch, h->s);
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, mode, h->s);
     h->cur ^= 1;
 }
@@ -595,6 +625,7 @@ static void enqueue_step(dpd_handle *h) {
     launch_scan(h->b, h->C, true, h->s);
     launch_place(h->b, h->d_bch, h->nbch, h->s);
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
     h->cur ^= 1;
     if (h->any_chem) launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
@@ -715,6 +746,7 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     CK(cudaEventRecord(ev[k++], h->s));
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
+    clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
     h->cur ^= 1;
@@ -830,6 +862,16 @@ extern "C" int dpd_set_params(dpd_handle *h, int32_t r, const dpd_params *p) {
     CK(cudaMemcpy(h->d_rep + r, &R, sizeof R, cudaMemcpyHostToDevice));
     bool any = false;
     for (auto &q : h->params) any = any || q.chem;
+    bool stir = false;
+    for (auto &q : h->params) stir = stir || q.stir_A != 0.0;
+    if (stir && !h->any_stir) {
+        // the current sums were not kept: rebuild them with a sort in place
+        h->any_stir = true;
+        drop_graphs(h);
+        enqueue_sort(h, PERM_SORT);
+        h->keys_valid = false;
+    }
+    h->any_stir = stir;
     if (any != h->any_chem) {
         h->any_chem = any;
         drop_graphs(h);
@@ -946,6 +988,7 @@ static void enqueue_plain_step(dpd_handle *h) {  // one step without chemistry (
     launch_scan(h->b, h->C, true, h->s);
     launch_place(h->b, h->d_bch, h->nbch, h->s);
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
     h->cur ^= 1;
     enqueue_forces(h, true);
@@ -961,6 +1004,9 @@ static int check_window(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec,
         if (p.chem) return fail(DPD_E_ARG, "chemistry must be off inside a differentiated window");
         if (p.warmup > 0 && h->step < p.warm_end)
             return fail(DPD_E_ARG, "the repulsion warm-up must be over before a differentiated window");
+        if (p.k_angle != 0.0 || p.stir_A != 0.0 || p.kT_amp != 0.0)
+            return fail(DPD_E_ARG, "angle terms, stirring and the temperature cycle must be off in a differentiated "
+                                   "window (the force VJP has no terms for them)");
     }
     return DPD_OK;
 }

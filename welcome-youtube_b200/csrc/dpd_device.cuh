@@ -218,6 +218,84 @@ __device__ __forceinline__ void bead_pairs_direct(const PairCtx &pc, const RepDe
     }
 }
 
+// ---------------------------------------------------------------- angle terms and stirring
+
+// The outer shares of one angle term U = ka (1 - cos theta) of the chain
+// triplet (i, j, k), theta the angle between a = x_j - x_i and c = x_k - x_j
+// (chain_forces_linear, oercel.c:1290-1307), in fixed point: (qix, qiy) on
+// the end i, (qkx, qky) on the end k; the middle bead j takes -(qi + qk), so
+// the three shares cancel exactly.  Every rounding is explicit: each of the
+// three beads recomputes the term from the same positions and gets the same bits.
+__device__ __forceinline__ void angle_shares(float2 xi, float2 xj, float2 xk, float ka, float L, float h, int &qix,
+                                             int &qiy, int &qkx, int &qky) {
+    const float ax = minimg(__fsub_rn(xj.x, xi.x), L, h), ay = minimg(__fsub_rn(xj.y, xi.y), L, h);
+    const float cx = minimg(__fsub_rn(xk.x, xj.x), L, h), cy = minimg(__fsub_rn(xk.y, xj.y), L, h);
+    const float la2 = __fmaf_rn(ax, ax, __fmul_rn(ay, ay)), lc2 = __fmaf_rn(cx, cx, __fmul_rn(cy, cy));
+    const float ilac = __fdiv_rn(1.0f, __fmul_rn(__fsqrt_rn(la2), __fsqrt_rn(lc2)));
+    const float cs = __fmul_rn(__fmaf_rn(ax, cx, __fmul_rn(ay, cy)), ilac);
+    const float csa = __fdiv_rn(cs, la2), csc = __fdiv_rn(cs, lc2);
+    // on i: dU/da = -ka (c / (la lc) - cos a / la^2); on k: -dU/dc = ka (a / (la lc) - cos c / lc^2)
+    qix = f2fix16(__fmul_rn(-ka, __fsub_rn(__fmul_rn(cx, ilac), __fmul_rn(csa, ax))));
+    qiy = f2fix16(__fmul_rn(-ka, __fsub_rn(__fmul_rn(cy, ilac), __fmul_rn(csa, ay))));
+    qkx = f2fix16(__fmul_rn(ka, __fsub_rn(__fmul_rn(ax, ilac), __fmul_rn(csc, cx))));
+    qky = f2fix16(__fmul_rn(ka, __fsub_rn(__fmul_rn(ay, ilac), __fmul_rn(csc, cy))));
+}
+
+// The angle shares of bead g at position pg with chain neighbours p (prev),
+// n (next), pp (prev of p) and nn (next of n); has* say which exist.  g is
+// the middle of (p, g, n), the end k of (pp, p, g) and the end i of (g, n, nn).
+__device__ __forceinline__ void angle_sum(float ka, float L, float h, float2 pg, bool hp, float2 pp_, bool hn,
+                                          float2 pn, bool hpp, float2 ppp, bool hnn, float2 pnn, long long &qx,
+                                          long long &qy) {
+    int ix, iy, kx, ky;
+    if (hp && hn) {
+        angle_shares(pp_, pg, pn, ka, L, h, ix, iy, kx, ky);
+        qx -= (long long)ix + kx;
+        qy -= (long long)iy + ky;
+    }
+    if (hp && hpp) {
+        angle_shares(ppp, pp_, pg, ka, L, h, ix, iy, kx, ky);
+        qx += kx;
+        qy += ky;
+    }
+    if (hn && hnn) {
+        angle_shares(pg, pn, pnn, ka, L, h, ix, iy, kx, ky);
+        qx += ix;
+        qy += iy;
+    }
+}
+
+// The stirring term A sin(2 pi n y / L) of a bead at height y (oercel.c:1183),
+// in fixed point.
+__device__ __forceinline__ long long stir_fix(const RepDev &R, float y) {
+    return __double2ll_rn((double)R.stir_A * sinpi(2.0 * R.stir_k * (double)y) * 65536.0);
+}
+
+// The stirring force of bead gid (fixed point): its term minus its share of
+// the replica's sum S of all terms, the share being floor(S / n) plus one
+// for gids below the remainder, so the shares add up to S exactly and the net
+// stirring force is exactly zero (the reference subtracts the mean,
+// oercel.c:1191-1195).
+__device__ __forceinline__ long long stir_force(const RepDev &R, float y, uint32_t gid, long long S) {
+    long long base = S / R.n;
+    if (S - base * R.n < 0) base -= 1;
+    const long long rem = S - base * R.n;
+    return stir_fix(R, y) - base - ((long long)gid < rem ? 1 : 0);
+}
+
+// The angle terms of bead g (slot), added to its fixed-point force: pg its
+// position, lk its links, pp_/pn the positions of its prev/next (valid where
+// the link is).  Loads the second neighbours itself; nothing when ka = 0.
+__device__ __forceinline__ void angle_terms(const Bufs &b, int cur, const RepDev &R, float2 pg, int2 lk, float2 pp_,
+                                            float2 pn, long long &qx, long long &qy) {
+    if (R.ka == 0.0f || (lk.x < 0 && lk.y < 0)) return;
+    const int2 *__restrict__ link = b.link[cur];
+    const float2 *__restrict__ pos = b.pos[cur];
+    const int pp = lk.x >= 0 ? link[lk.x].x : -1, nn = lk.y >= 0 ? link[lk.y].y : -1;
+    const float2 ppp = pp >= 0 ? pos[pp] : pg, pnn = nn >= 0 ? pos[nn] : pg;
+    angle_sum(R.ka, R.L, R.halfL, pg, lk.x >= 0, pp_, lk.y >= 0, pn, pp >= 0, ppp, nn >= 0, pnn, qx, qy);
+}
+
 // ---------------------------------------------------------------- programmatic dependent launch
 
 // The kernels of a step are launched with programmatic stream serialization

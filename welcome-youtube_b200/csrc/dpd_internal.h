@@ -55,7 +55,23 @@ struct RepDev {                 // constants of one replica, read by every kerne
     int32_t pad;
     long long warm_end;         // repulsions above 25 ramp in until this step (oercel.c:1124-1129)
     double warm_inv;            // 1 / warmup, 0 = no ramp
+    float ka;                   // angle constant (0 = no angle terms)
+    float stir_A;               // stirring amplitude (0 = off)
+    double stir_k;              // stir_n / L (the argument of the sine is 2 pi stir_k y)
+    double kT, kT_amp, kT_w;    // kT(t) = kT + kT_amp sin(kT_w t)
+    double gamma_d, dt_d;       // gamma, dt in FP64 (sigma / sqrt(dt) of a step)
+    double t_anchor;            // t(step) = t_anchor + (step - step_anchor) dt
+    long long step_anchor;
 };
+
+// sigma / sqrt(dt) at `step`: constant, or with the temperature cycle
+// kT(t) = kT + kT_amp sin(2 pi t / kT_period) (oercel.c:622-624, 1204)
+__device__ __forceinline__ float sdt_at(const RepDev &R, long long step) {
+    if (R.kT_amp == 0.0) return R.sdt;
+    const double t = R.t_anchor + (double)(step - R.step_anchor) * R.dt_d;
+    const double kT = R.kT + R.kT_amp * sin(R.kT_w * t);
+    return (float)(sqrt(2.0 * R.gamma_d * kT) / sqrt(R.dt_d));
+}
 
 // the repulsion in force at `step`: during the warm-up of a fresh soup the part
 // of a_ij above the water value 25 is ramped in linearly (oercel.c:1124-1129)
@@ -119,6 +135,7 @@ struct Bufs {
     long long *step;            // step number of the forces being computed
     unsigned long long *obs;    // OBS_N per replica
     unsigned long long *hist;   // pair histogram scratch
+    long long *stir;            // per replica: sum of the stirring terms (fixed point) of the current positions
 };
 
 struct StateView {              // one stored configuration (slot order of its own step)

@@ -324,6 +324,18 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
     const long long step = MODE == PERM_STEP ? *b.step : 0;
 #pragma unroll
     for (int k = 0; k < ITEMS; k++) {
+        // the replica's sum of stirring terms at the new positions (warp sums, one atomic per warp)
+        const RepDev &Rk = reps[rep[k]];
+        if (Rk.stir_A != 0.0f) {  // uniform over the warp: its lanes share one chunk
+            long long st = 0;
+            if (act[k]) {
+                float yn = p[k].y;
+                if (MODE == PERM_STEP) yn = advance1(yn, vh[k].y, f[k].y, Rk.dt, Rk.dt2, Rk.L);
+                st = stir_fix(Rk, yn);
+            }
+            st = warp_sum_ll(st);
+            if (lane_id() == 0 && st != 0) atomicAdd((unsigned long long *)(b.stir + rep[k]), (unsigned long long)st);
+        }
         if (!act[k]) continue;
         const int dd = d[k];
         float2 q = p[k], v = vh[k];
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
             pc.L = L;
             pc.h = R.halfL;
             pc.gam = R.gamma;
-            pc.sdt = R.sdt;
+            pc.sdt = sdt_at(R, *b.step);
             const int ncx = R.ncx, ncy = R.ncy;
             const int32_t *__restrict__ cs = b.cstart + R.c0;
             int cx, cy;
@@ -460,15 +472,20 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
             const int nl = min(nh, MAXHIT);
 #pragma unroll 1
             for (int k = 0; k < nl; k++) pair_term(pc, hl[k][threadIdx.x], ax, ay);
+            // the stirring body force belongs to the pair forces, as in the reference (oercel.c:1159-1165)
+            if (R.stir_A != 0.0f) ax += stir_force(R, pi.y, pc.gi, b.stir[c.rep]);
         }
         if (BOND) {
             const int2 lk = b.link[cur][d];
             const float h = R.halfL, kb = R.kb, r0 = R.r0;
+            float2 pjs[2];
 #pragma unroll
             for (int q = 0; q < 2; q++) {
                 const int j = q ? lk.y : lk.x;
+                pjs[q] = pi;
                 if (j < 0) continue;
                 const float2 pj = pos[j];
+                pjs[q] = pj;
                 const float dx = minimg(__fsub_rn(pj.x, pi.x), L, h), dy = minimg(__fsub_rn(pj.y, pi.y), L, h);
                 const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
                 mb = fmaxf(mb, r);
@@ -476,6 +493,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
                 ax += f2fix16(__fmul_rn(fb, dx));
                 ay += f2fix16(__fmul_rn(fb, dy));
             }
+            angle_terms(b, cur, R, pi, lk, pjs[0], pjs[1], ax, ay);
         }
         const float2 fs = make_float2(fix16_to_f(ax), fix16_to_f(ay));
         if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);

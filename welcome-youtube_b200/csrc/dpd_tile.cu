@@ -214,9 +214,9 @@ __device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int
 // links lk, its bond partners' positions pj[2] and its half-step velocity v
 // (loaded by the caller)
 template <bool NEXTKEY>
-__device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepDev &R, int g, float2 pi, long long qx,
-                                              long long qy, int2 lk, const float2 (&pj)[2], float2 v, float &mb,
-                                              uint32_t &key) {
+__device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepDev &R, int rep, int g, float2 pi,
+                                              long long qx, long long qy, int2 lk, const float2 (&pj)[2], float2 v,
+                                              float &mb, uint32_t &key) {
     const float L = R.L, h = R.halfL, kb = R.kb, r0 = R.r0;
 #pragma unroll
     for (int e = 0; e < 2; e++) {
@@ -229,6 +229,8 @@ __device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepD
         qx += f2fix16(__fmul_rn(fb, dx));
         qy += f2fix16(__fmul_rn(fb, dy));
     }
+    angle_terms(b, cur, R, pi, lk, pj[0], pj[1], qx, qy);
+    if (R.stir_A != 0.0f) qx += stir_force(R, pi.y, b.tg[cur][g] & GID_MASK, b.stir[rep]);
     const float2 fs = make_float2(fix16_to_f(qx), fix16_to_f(qy));
     if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);
     b.f[cur][g] = fs;
@@ -241,14 +243,14 @@ __device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepD
 
 // the same with its own loads (the crowded-tile path)
 template <bool NEXTKEY>
-__device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev &R, int g, float2 pi, long long qx,
-                                            long long qy, float &mb, uint32_t &key) {
+__device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev &R, int rep, int g, float2 pi,
+                                            long long qx, long long qy, float &mb, uint32_t &key) {
     const int2 lk = b.link[cur][g];
     float2 pj[2];
     pj[0] = lk.x >= 0 ? b.pos[cur][lk.x] : pi;
     pj[1] = lk.y >= 0 ? b.pos[cur][lk.y] : pi;
     const float2 v = NEXTKEY ? b.vh[cur][g] : make_float2(0.0f, 0.0f);
-    finish_loaded<NEXTKEY>(b, cur, R, g, pi, qx, qy, lk, pj, v, mb, key);
+    finish_loaded<NEXTKEY>(b, cur, R, rep, g, pi, qx, qy, lk, pj, v, mb, key);
 }
 
 #define EPI_ITEMS 2  // owned beads per thread per round of the epilogue
@@ -327,10 +329,10 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
                     pc.L = R.L;
                     pc.h = R.halfL;
                     pc.gam = R.gamma;
-                    pc.sdt = R.sdt;
+                    pc.sdt = sdt_at(R, step);
                     long long ax = 0, ay = 0;
                     bead_pairs_direct(pc, R, cs, g, ax, ay);
-                    finish_bead<NEXTKEY>(b, cur, R, g, pc.pi, ax, ay, mb, key);
+                    finish_bead<NEXTKEY>(b, cur, R, td.rep, g, pc.pi, ax, ay, mb, key);
                 }
                 if (NEXTKEY) {
                     count_key(b.count, key, act);
@@ -363,7 +365,7 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
         pc.nk = make_noise_key(R, step);
         pc.L = R.L;
         pc.gam = R.gamma;
-        pc.sdt = R.sdt;
+        pc.sdt = sdt_at(R, step);
         const bool wrap = td.cx0 == 0 || td.cy0 == 0 || td.cx0 + td.w >= ncx || td.cy0 + td.h >= ncy;
         if (R.noise == 1) {
             if (wrap) tile_pairs<true, 1>(S, pc, LW, LH, td.w, td.h, b.status);
@@ -409,8 +411,8 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
                 const int k = base + j * TILE_TPB + tid;
                 uint32_t key = 0;
                 if (own[j])
-                    finish_loaded<NEXTKEY>(b, cur, R, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j], vv[j], mb,
-                                           key);
+                    finish_loaded<NEXTKEY>(b, cur, R, td.rep, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j],
+                                           vv[j], mb, key);
                 if (NEXTKEY) {
                     count_key(b.count, key, own[j]);
                     if (own[j]) b.key[gg[j]] = key;

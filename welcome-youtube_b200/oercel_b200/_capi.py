@@ -36,6 +36,8 @@ class DpdParams(C.Structure):
         ("max_chain", C.c_int32), ("pad", C.c_int32),
         ("p_break", C.c_double), ("p_grow", C.c_double), ("p_bond", C.c_double),
         ("r_grow", C.c_double), ("r_bond", C.c_double), ("warmup", C.c_int64), ("warm_end", C.c_int64),
+        ("k_angle", C.c_double), ("stir_A", C.c_double), ("stir_n", C.c_int32), ("pad2", C.c_int32),
+        ("kT_amp", C.c_double), ("kT_period", C.c_double), ("t_anchor", C.c_double), ("step_anchor", C.c_int64),
     ]
 
 

@@ -263,15 +263,16 @@ def _run(p, outdir, over):
                 log(f"restart: reseeded with seed={p.seed} (branch, not an exact continuation)")
             elif seed != p.seed:
                 log(f"note: using checkpoint seed {seed} (ini seed {p.seed} ignored; set restart_reseed=1 to branch)")
+            warm_end = ck["warm_end"]
+            ta, sa, da = ck["anchor"]
+            anchor = (ta, sa, da) if da == p.dt else (ck["time"], ck["step"], p.dt)  # dt changed: new anchor
             e = Engine(p, n_beads=ck["N"])
-            _set_seed_warm(e, p, seed, ck["warm_end"])
+            # the checkpoint's seed (unless restart_reseed), warm-up end and time anchor (oercel.c:1965-1990)
+            e.set_params(0, p, seed=seed, warm_end=warm_end, t_anchor=anchor[0], step_anchor=anchor[1])
             e.set_state(0, ck["x"], ck["y"], ck["vhx"], ck["vhy"], ck["type"], ck["gid"], ck["prev"], ck["next"])
             e.set_dynamics(0, ck["vhx"], ck["vhy"], ck["fx"], ck["fy"])
             e.resume()
             e.set_step(ck["step"])
-            warm_end = ck["warm_end"]
-            ta, sa, da = ck["anchor"]
-            anchor = (ta, sa, da) if da == p.dt else (ck["time"], ck["step"], p.dt)  # dt changed: new anchor
             log(f"restart from {p.restart} at step {ck['step']} (t={ck['time']:.4f}), N={ck['N']}")
         else:
             e = Engine(p)
@@ -310,6 +311,9 @@ def _run(p, outdir, over):
     nc = int(math.floor(L))
     log(f"oercel_b200: N={n} L={p.L:g} cells={nc}x{nc} dt={p.dt:g} gamma={p.gamma:g} sigma={p.sigma():g} "
         f"steps->{p.steps}")
+
+    def kT_at(t):
+        return p.kT + (p.kT_amp * math.sin(2.0 * math.pi * t / p.kT_period) if p.kT_amp != 0 else 0.0)
 
     def tnow(step):
         return anchor[0] + (step - anchor[1]) * p.dt
@@ -383,7 +387,7 @@ def _run(p, outdir, over):
             o = obs()
             now = time.time()
             c = o["counts"]
-            log(f"step {step} t={tnow(step):.2f} T={o['T']:.4f} (kT={p.kT:.4f}) p=({o['px']:.2e},{o['py']:.2e}) "
+            log(f"step {step} t={tnow(step):.2f} T={o['T']:.4f} (kT={kT_at(tnow(step)):.4f}) p=({o['px']:.2e},{o['py']:.2e}) "
                 f"lip={o['n_chains']} Ka={c[4]} Kb={c[5]} N={c[3]}  "
                 f"{1e3 * (now - t_last) / max(step - step_last, 1):.3f} ms/step")
             t_last, step_last = now, step
@@ -401,14 +405,6 @@ def _run(p, outdir, over):
     log(f"done at step {step}" + (" (stopped early; restart to continue)" if stopped else ""))
     e.close()
     return 0
-
-
-def _set_seed_warm(e, p, seed, warm_end):
-    """the checkpoint's seed (unless restart_reseed) and warm-up end (oercel.c:1965-1975)"""
-    from ._capi import check
-    import ctypes as C
-    s = p.to_struct(seed=seed, warm_end=warm_end)
-    check(e.lib.dpd_set_params(e.h, 0, C.byref(s)))
 
 
 def main():

@@ -221,9 +221,11 @@ class Engine:
         return h
 
     # ---------------------------------------------------------------- parameters and reverse mode
-    def set_params(self, replica, p: Params):
+    def set_params(self, replica, p: Params, **kv):
+        """replace the parameters of one replica (same box); kv go to Params.to_struct
+        (seed, warm_end, t_anchor, step_anchor)"""
         self.params[replica] = p
-        check(self.lib.dpd_set_params(self.h, replica, C.byref(p.to_struct())))
+        check(self.lib.dpd_set_params(self.h, replica, C.byref(p.to_struct(**kv))))
 
     @staticmethod
     def rdf_spec(ta=2, tb=2, nbin=64, rmax=2.0, sigma=0.05, last_steps=50, horizon=0):

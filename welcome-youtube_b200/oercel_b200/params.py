@@ -26,7 +26,7 @@ PDEFS = [
     ("kT", "float", "1", "temperature"),
     ("k_bond", "float", "100", "bond constant, U = k/2 (r - r0)^2"),
     ("r0", "float", "0.5", "bond rest length"),
-    ("k_angle", "float", "10", "angle constant (only 0 is supported here)"),
+    ("k_angle", "float", "10", "angle constant, U = k (1 - cos theta) on consecutive chain triplets"),
     ("lip_nH", "int", "1", "head beads per lipid"),
     ("lip_nT", "int", "3", "tail beads per lipid"),
     ("lip_arch", "str", "linear", "lipid shape (only linear is supported here)"),
@@ -71,9 +71,9 @@ PDEFS = [
     ("vent_r", "float", "5", "catalyst chemistry only (unused)"),
     ("vent_w", "float", "4", "catalyst chemistry only (unused)"),
     ("events", "int", "1", "1 = write events.csv"),
-    ("stir_A", "float", "0", "stirring force (only 0 is supported here)"),
+    ("stir_A", "float", "0", "stirring body force f_x = stir_A sin(2 pi stir_n y / L), net force removed"),
     ("stir_n", "int", "1", "stirring periods"),
-    ("kT_amp", "float", "0", "temperature cycle (only 0 is supported here)"),
+    ("kT_amp", "float", "0", "temperature cycle kT(t) = kT + kT_amp sin(2 pi t / kT_period) in the noise"),
     ("kT_period", "float", "1000", "temperature cycle period"),
     ("f_lip", "float", "0.10", "soup: fraction of beads in lipids"),
     ("f_Ka", "float", "0.005", "soup: fraction of Ka beads"),
@@ -211,10 +211,14 @@ class Params:
             raise ParamError("kT must be > 0")
         if self.lip_arch != "linear":
             raise ParamError("only lip_arch = linear is supported")
-        if self.k_angle != 0:
-            raise ParamError("angle terms are not supported: set k_angle = 0")
-        if self.stir_A != 0 or self.kT_amp != 0:
-            raise ParamError("stirring and the temperature cycle are not supported: set stir_A = 0, kT_amp = 0")
+        if self.k_angle < 0:
+            raise ParamError("k_angle must be >= 0")
+        if self.stir_n < 1:
+            raise ParamError("stir_n must be >= 1")
+        if self.kT_amp != 0 and self.kT_period <= 0:
+            raise ParamError("kT_period must be > 0")
+        if self.kT_amp != 0 and self.kT - abs(self.kT_amp) <= 0:
+            raise ParamError("kT - |kT_amp| must be > 0")
         if self.noise not in ("philox", "mix13"):
             raise ParamError("noise must be philox or mix13")
         if self.init not in ("soup", "restart"):
@@ -226,7 +230,7 @@ class Params:
     def sigma(self):
         return math.sqrt(2.0 * self.gamma * self.kT)
 
-    def to_struct(self, seed=None, warm_end=None):
+    def to_struct(self, seed=None, warm_end=None, t_anchor=0.0, step_anchor=0):
         from ._capi import DpdParams, load
         s = DpdParams()
         load().dpd_params_default(s)
@@ -250,6 +254,10 @@ class Params:
         s.r_grow, s.r_bond = float(self.r_grow), float(self.r_bond)
         s.warmup = max(int(self.warmup), 0)
         s.warm_end = int(self.warmup if warm_end is None else warm_end)
+        s.k_angle = float(self.k_angle)
+        s.stir_A, s.stir_n = float(self.stir_A), int(self.stir_n)
+        s.kT_amp, s.kT_period = float(self.kT_amp), float(self.kT_period)
+        s.t_anchor, s.step_anchor = float(t_anchor), int(step_anchor)
         return s
 
     def write(self, path, overrides=()):
