@@ -57,6 +57,20 @@ def profiled_traffic(kernel):
     return None
 
 
+def profiled_instructions(kernel):
+    """warp instructions per launch of a kernel of the step, from the ncu summary
+    in profiles/<kernel>_1M.md (line "warp_instructions_per_launch: N")"""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_1M.md")
+    try:
+        for line in open(path):
+            m = re.search(r"warp_instructions_per_launch:\s*([0-9]+)", line)
+            if m:
+                return int(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws == 1:
@@ -189,6 +203,21 @@ def reference_arm(args, rank, ws):
                  "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                  "reference_timing_ms": t})
     print(json.dumps(base))
+
+
+def issue_roofline(kernel, ms, clocks):
+    """The bound that binds the force kernel: instruction issue.  Warp
+    instructions of one launch (ncu) over 4 issues per SM cycle on all SMs at
+    the SM clock seen during the timed loop, against the measured duration."""
+    inst = profiled_instructions(kernel)
+    mhz = (clocks or {}).get("sm_mhz")
+    if not inst or not mhz:
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    t_min = inst / (4.0 * sms * mhz * 1e6)
+    return {"bound": "issue", "warp_instructions_per_launch": inst, "sms": sms, "sm_mhz": mhz,
+            "min_us": t_min * 1e6, "measured_us": ms * 1000.0, "frac": t_min / (ms / 1000.0)}
 
 
 def time_steps(torch, eng, K, flush):
@@ -371,6 +400,7 @@ def ours(args, rank, local_rank, ws):
            "roofline": {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
                         "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
                         "bytes_per_bead": KERNEL_BYTES[top]},
+           "issue_roofline": issue_roofline(top, kernels[top], clk.summary()),
            "step_roofline": {"bytes_per_bead_step": STEP_BYTES_CHEM,
                              "achieved": value / ws * STEP_BYTES_CHEM / 1e9, "peak": peak,
                              "frac": value / ws * STEP_BYTES_CHEM / 1e9 / peak},
