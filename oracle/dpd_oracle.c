@@ -716,3 +716,376 @@ int32_t ora_init_soup(double L, int32_t N, uint64_t seed, double kT, double r0, 
     }
     return nl;
 }
+
+/* ------------------------------------------------------------------ the catalyst chemistry */
+
+/* counter-based uniform deviate of the reference, oercel.c:819-826 */
+static uint64_t cat_hash_key(uint64_t seed, int64_t step, uint64_t salt) {
+    return ora_mix13(seed ^ ora_mix13((uint64_t)step * 0x9e3779b97f4a7c15ULL + salt));
+}
+static double cat_hash_u01(uint64_t key, uint32_t g) {
+    return (double)(ora_mix13(key ^ ((uint64_t)g * 0xd1b54a32d192ed03ULL)) >> 11) * 0x1.0p-53;
+}
+/* oercel.c:164-167 */
+static long cat_rng_below(rng_t *r, long n) {
+    long k = (long)(rng_unif(r) * (double)n);
+    return k >= n ? n - 1 : k;
+}
+
+/* cell of an FP64 position (cell_of_pos with nsub = 1, oercel.c:779-786) */
+static int cat_cell(const ora_params *P, double x, double y) {
+    int cx = (int)(x * P->icsx), cy = (int)(y * P->icsy);
+    cx = cx >= P->ncx ? P->ncx - 1 : (cx < 0 ? 0 : cx);
+    cy = cy >= P->ncy ? P->ncy - 1 : (cy < 0 ? 0 : cy);
+    return cx * P->ncy + cy;
+}
+
+#define CAT_MARGIN 0.5 /* oercel.c:1348 */
+typedef struct { int slot; double d2; } cat_nbr;
+
+/* beads of one type within rcut of (xk, yk), nearest first, ties by lower gid
+ * (find_type_near, oercel.c:1353-1398; at most maxout, counted in scan order) */
+static int cat_find(const ora_params *P, const float *x, const float *y, const uint8_t *type, const uint32_t *gid,
+                    const int32_t *cstart, int ks, double xk, double yk, double rcut, int want, cat_nbr *out,
+                    int maxout) {
+    const double L = P->L, r2c = rcut * rcut;
+    const int ncx = P->ncx, ncy = P->ncy;
+    const int c = cat_cell(P, xk, yk), cx = c / ncy, cy = c % ncy;
+    const int rx = (int)ceil((rcut + CAT_MARGIN) * P->icsx), ry = (int)ceil((rcut + CAT_MARGIN) * P->icsy);
+    int n = 0;
+    for (int ox = -rx; ox <= rx; ox++) {
+        int cxx = cx + ox;
+        cxx += cxx < 0 ? ncx : 0;
+        cxx -= cxx >= ncx ? ncx : 0;
+        const int base = cxx * ncy, lo = cy - ry, hi = cy + ry;
+        int r0[2], r1[2], nr = 0;
+        if (lo >= 0 && hi < ncy) { r0[nr] = cstart[base + lo]; r1[nr] = cstart[base + hi + 1]; nr++; }
+        else if (lo < 0) {
+            r0[nr] = cstart[base + lo + ncy]; r1[nr] = cstart[base + ncy]; nr++;
+            r0[nr] = cstart[base]; r1[nr] = cstart[base + hi + 1]; nr++;
+        } else {
+            r0[nr] = cstart[base + lo]; r1[nr] = cstart[base + ncy]; nr++;
+            r0[nr] = cstart[base]; r1[nr] = cstart[base + hi - ncy + 1]; nr++;
+        }
+        for (int q = 0; q < nr; q++)
+            for (int j = r0[q]; j < r1[q]; j++) {
+                if (type[j] != want || j == ks) continue;
+                const double dx = minimg((double)x[j] - xk, L), dy = minimg((double)y[j] - yk, L);
+                const double d2 = dx * dx + dy * dy;
+                if (d2 < r2c && n < maxout) { out[n].slot = j; out[n].d2 = d2; n++; }
+            }
+    }
+    for (int a = 1; a < n; a++) {
+        const cat_nbr t = out[a];
+        int b = a - 1;
+        while (b >= 0 && (out[b].d2 > t.d2 || (out[b].d2 == t.d2 && gid[out[b].slot] > gid[t.slot]))) {
+            out[b + 1] = out[b];
+            b--;
+        }
+        out[b + 1] = t;
+    }
+    return n;
+}
+
+/* overlap energy of a would-be straight chain (centre c0, direction u) with
+ * every bead outside it (chain_overlap_energy, oercel.c:1425-1468) */
+static double cat_chain_energy(const ora_params *P, const ora_cat *K, const float *x, const float *y,
+                               const uint8_t *type, const int32_t *cstart, double cx0, double cy0, double ux, double uy,
+                               const int *sl, int ml) {
+    const int ncx = P->ncx, ncy = P->ncy;
+    const double L = P->L;
+    double U = 0.0;
+    for (int b = 0; b < ml; b++) {
+        const double off = (b - 0.5 * (ml - 1)) * P->r0;
+        double px = cx0 + off * ux, py = cy0 + off * uy;
+        wrap1(&px, L);
+        wrap1(&py, L);
+        const int tb = b < K->nH ? 1 : 2;
+        const int c = cat_cell(P, px, py), cx = c / ncy, cy = c % ncy;
+        const int rx = (int)ceil((1.0 + CAT_MARGIN) * P->icsx), ry = (int)ceil((1.0 + CAT_MARGIN) * P->icsy);
+        for (int ox = -rx; ox <= rx; ox++) {
+            int cxx = cx + ox;
+            cxx += cxx < 0 ? ncx : 0;
+            cxx -= cxx >= ncx ? ncx : 0;
+            for (int oy = -ry; oy <= ry; oy++) {
+                int cyy = cy + oy;
+                cyy += cyy < 0 ? ncy : 0;
+                cyy -= cyy >= ncy ? ncy : 0;
+                const int cc = cxx * ncy + cyy;
+                for (int j = cstart[cc]; j < cstart[cc + 1]; j++) {
+                    int skip = 0;
+                    for (int q = 0; q < ml; q++) skip |= j == sl[q];
+                    if (skip) continue;
+                    const double dx = minimg((double)x[j] - px, L), dy = minimg((double)y[j] - py, L);
+                    const double r2 = dx * dx + dy * dy;
+                    if (r2 >= 1.0) continue;
+                    const double w = 1.0 - sqrt(r2);
+                    U += 0.5 * P->a[tb * ORA_MAXT + type[j]] * w * w;
+                }
+            }
+        }
+    }
+    return U;
+}
+
+/* steepest-descent relaxation of a new chain whose FP64 positions are
+ * (px, py)[0..ml) against its frozen surroundings (relax_new_chain,
+ * oercel.c:1473-1560, the linear-template branch) */
+static void cat_relax(const ora_params *P, const ora_cat *K, const float *x, const float *y, const uint8_t *type,
+                      const int32_t *cstart, const int *sl, int ml, double *px, double *py) {
+    const int ncx = P->ncx, ncy = P->ncy;
+    const double L = P->L, cap = 0.05, alpha = 0.002;
+    enum { MAXNB = 512 };
+    int nbj[MAXNB], nnb = 0;
+    const double reach = 1.0 + cap * K->syn_relax, reach2 = reach * reach;
+    for (int b = 0; b < ml && nnb < MAXNB; b++) {
+        const int c = cat_cell(P, px[b], py[b]), cx = c / ncy, cy = c % ncy;
+        const int rx = (int)ceil((reach + CAT_MARGIN) * P->icsx), ry = (int)ceil((reach + CAT_MARGIN) * P->icsy);
+        for (int ox = -rx; ox <= rx; ox++) {
+            int cxx = cx + ox;
+            cxx += cxx < 0 ? ncx : 0;
+            cxx -= cxx >= ncx ? ncx : 0;
+            for (int oy = -ry; oy <= ry; oy++) {
+                int cyy = cy + oy;
+                cyy += cyy < 0 ? ncy : 0;
+                cyy -= cyy >= ncy ? ncy : 0;
+                const int cc = cxx * ncy + cyy;
+                for (int j = cstart[cc]; j < cstart[cc + 1]; j++) {
+                    int skip = 0;
+                    for (int q = 0; q < ml; q++) skip |= j == sl[q];
+                    for (int q = 0; q < nnb && !skip; q++) skip |= nbj[q] == j;
+                    if (skip) continue;
+                    const double dx = minimg((double)x[j] - px[b], L), dy = minimg((double)y[j] - py[b], L);
+                    if (dx * dx + dy * dy < reach2 && nnb < MAXNB) nbj[nnb++] = j;
+                }
+            }
+        }
+    }
+    for (int it = 0; it < K->syn_relax; it++) {
+        double fx[64] = {0}, fy[64] = {0};
+        for (int b = 0; b < ml; b++) {
+            const int ti = b < K->nH ? 1 : 2;
+            for (int q = 0; q < nnb; q++) {
+                const int j = nbj[q];
+                const double dx = minimg(px[b] - (double)x[j], L), dy = minimg(py[b] - (double)y[j], L);
+                const double r2 = dx * dx + dy * dy;
+                if (r2 >= 1.0 || r2 < 1e-24) continue;
+                const double r = sqrt(r2);
+                const double f = P->a[ti * ORA_MAXT + type[j]] * (1.0 - r) / r;
+                fx[b] += f * dx;
+                fy[b] += f * dy;
+            }
+        }
+        double bx[64], by[64], bl[64];
+        for (int b = 0; b < ml - 1; b++) {
+            bx[b] = minimg(px[b + 1] - px[b], L);
+            by[b] = minimg(py[b + 1] - py[b], L);
+            bl[b] = sqrt(bx[b] * bx[b] + by[b] * by[b]);
+            const double f = -P->k_bond * (bl[b] - P->r0) / bl[b];
+            fx[b + 1] += f * bx[b]; fy[b + 1] += f * by[b];
+            fx[b] -= f * bx[b]; fy[b] -= f * by[b];
+        }
+        for (int b = 0; b < ml - 2 && P->k_angle != 0.0; b++) {
+            const double ax = bx[b], ay = by[b], cxv = bx[b + 1], cyv = by[b + 1], la = bl[b], lc = bl[b + 1];
+            const double ilac = 1.0 / (la * lc), cs = (ax * cxv + ay * cyv) * ilac, ka = P->k_angle;
+            const double dUax = -ka * (cxv * ilac - cs * ax / (la * la)), dUay = -ka * (cyv * ilac - cs * ay / (la * la));
+            const double dUcx = -ka * (ax * ilac - cs * cxv / (lc * lc)), dUcy = -ka * (ay * ilac - cs * cyv / (lc * lc));
+            fx[b] += dUax; fy[b] += dUay;
+            fx[b + 1] += -dUax + dUcx; fy[b + 1] += -dUay + dUcy;
+            fx[b + 2] -= dUcx; fy[b + 2] -= dUcy;
+        }
+        for (int b = 0; b < ml; b++) {
+            double mx = alpha * fx[b], my = alpha * fy[b];
+            const double m = sqrt(mx * mx + my * my);
+            if (m > cap) { mx *= cap / m; my *= cap / m; }
+            px[b] += mx;
+            py[b] += my;
+            wrap1(&px[b], L);
+            wrap1(&py[b], L);
+        }
+    }
+}
+
+static int cat_in_vent(const ora_cat *K, double L, double x, double y) {
+    if (K->vent_kind == 0) {
+        const double dx = minimg(x - K->vent_x, L), dy = minimg(y - K->vent_y, L);
+        return dx * dx + dy * dy < K->vent_r * K->vent_r;
+    }
+    if (K->vent_kind == 1) return fabs(minimg(x - K->vent_x, L)) < 0.5 * K->vent_w;
+    return fabs(minimg(y - K->vent_y, L)) < 0.5 * K->vent_w;
+}
+
+static void cat_event(ora_event *ev, int32_t evcap, int32_t *nev, int64_t step, int kind, uint32_t i, double x,
+                      double y, int variant) {
+    if (*nev < evcap) {
+        ora_event *e = &ev[*nev];
+        e->step = step;
+        e->kind = kind;
+        e->gid = i;
+        e->partner = (uint32_t)variant;
+        e->x = (float)x;
+        e->y = (float)y;
+        e->pad = 0;
+    }
+    (*nev)++;
+}
+
+/* One chemistry check of the reference (chemistry, oercel.c:1565-1700, and
+ * feed_supply, :1721-1753) on a state sorted into cells (cstart): catalysts
+ * in slot order shuffled with the serial generator rng, each with lipid
+ * synthesis (nearest N, best of syn_tries orientations, relaxation) and
+ * replication / mutation; then decay by keyed deviates; then the food
+ * supply.  Positions are FP32 in and out, computed in FP64.  Returns 1 if
+ * beads moved; *nev = number of events (those beyond evcap are dropped). */
+int32_t ora_catalyst_chemistry(const ora_params *P, const ora_cat *K, uint64_t *rng_state, int32_t n, float *x,
+                               float *y, float *vhx, float *vhy, float *vtx, float *vty, uint8_t *type,
+                               const uint32_t *gid, int32_t *prev, int32_t *next, const int32_t *cstart, int64_t step,
+                               ora_event *ev, int32_t evcap, int32_t *nev) {
+    rng_t rng;
+    memcpy(rng.s, rng_state, sizeof rng.s);
+    const int ml = K->nH + K->nT;
+    const double L = P->L;
+    int moved = 0;
+    *nev = 0;
+    int *ks = malloc((size_t)(n + 1) * sizeof(int));
+    int nk = 0;
+    for (int d = 0; d < n; d++)
+        if (type[d] == 4 || type[d] == 5) ks[nk++] = d;
+    for (int a = nk - 1; a > 0; a--) {
+        const int b = (int)cat_rng_below(&rng, a + 1);
+        const int t = ks[a]; ks[a] = ks[b]; ks[b] = t;
+    }
+    cat_nbr nb[256], nbw[256];
+    for (int q = 0; q < nk; q++) {
+        const int k = ks[q];
+        if (type[k] != 4 && type[k] != 5) continue;
+        const int var = type[k] == 5;
+        const double psyn = var ? K->p_syn_b : K->p_syn_a, prep = var ? K->p_rep_b : K->p_rep_a;
+        const double xk = x[k], yk = y[k];
+        const int nn = cat_find(P, x, y, type, gid, cstart, k, xk, yk, K->r_cat, 3, nb, 256);
+        if (nn < 2) continue;
+        int used = 0;
+        const int nsynN = K->syn_nN > 0 ? K->syn_nN : ml;
+        int nw = 0;
+        if (nn >= nsynN && nsynN < ml) nw = cat_find(P, x, y, type, gid, cstart, k, xk, yk, K->r_cat, 0, nbw, 256);
+        if (nn >= nsynN && nsynN + nw >= ml && rng_unif(&rng) < psyn) {
+            double cxm = 0, cym = 0, mvx = 0, mvy = 0, mtx = 0, mty = 0;
+            int sl[64];
+            for (int b = 0; b < ml; b++) {
+                const int j = b < nsynN ? nb[b].slot : nbw[b - nsynN].slot;
+                sl[b] = j;
+                cxm += minimg((double)x[j] - xk, L);
+                cym += minimg((double)y[j] - yk, L);
+                mvx += vhx[j]; mvy += vhy[j];
+                mtx += vtx[j]; mty += vty[j];
+            }
+            cxm = xk + cxm / ml; cym = yk + cym / ml;
+            mvx /= ml; mvy /= ml; mtx /= ml; mty /= ml;
+            double ux = 1.0, uy = 0.0, ubest = INFINITY;
+            for (int tr = 0; tr < K->syn_tries; tr++) {
+                const double phi = 2.0 * M_PI * rng_unif(&rng);
+                const double cx_ = cos(phi), cy_ = sin(phi);
+                const double U = K->syn_tries > 1 ? cat_chain_energy(P, K, x, y, type, cstart, cxm, cym, cx_, cy_, sl, ml)
+                                                  : 0.0;
+                if (U < ubest) { ubest = U; ux = cx_; uy = cy_; }
+            }
+            double px[64], py[64];
+            for (int b = 0; b < ml; b++) {
+                const int j = sl[b];
+                const double off = (b - 0.5 * (ml - 1)) * P->r0;
+                px[b] = cxm + off * ux;
+                py[b] = cym + off * uy;
+                wrap1(&px[b], L);
+                wrap1(&py[b], L);
+                vhx[j] = (float)mvx; vhy[j] = (float)mvy;
+                vtx[j] = (float)mtx; vty[j] = (float)mty;
+                type[j] = b < K->nH ? 1 : 2;
+            }
+            for (int b = 0; b < ml; b++) {
+                prev[sl[b]] = b > 0 ? sl[b - 1] : -1;
+                next[sl[b]] = b + 1 < ml ? sl[b + 1] : -1;
+            }
+            if (K->syn_relax > 0) cat_relax(P, K, x, y, type, cstart, sl, ml, px, py);
+            for (int b = 0; b < ml; b++) {
+                float fx_ = (float)px[b], fy_ = (float)py[b];
+                if (fx_ >= (float)L) fx_ = 0.0f;
+                if (fy_ >= (float)L) fy_ = 0.0f;
+                x[sl[b]] = fx_;
+                y[sl[b]] = fy_;
+            }
+            cat_event(ev, evcap, nev, step, ORA_EV_SYN, gid[k], xk, yk, var);
+            used = nsynN;
+            moved = 1;
+        }
+        if (nn - used >= 2 && rng_unif(&rng) < prep) {
+            int nv = var, mut = 0;
+            if (rng_unif(&rng) < K->mu) { nv = 1 - var; mut = 1; }
+            const int j1 = nb[used].slot, j2 = nb[used + 1].slot;
+            type[j1] = nv ? 5 : 4;
+            type[j2] = 0;
+            cat_event(ev, evcap, nev, step, mut ? ORA_EV_MUT : ORA_EV_REP, gid[j1], xk, yk, nv);
+        }
+    }
+    /* decay: keyed per-bead decisions in slot order, applied after the scan */
+    if (K->p_ld > 0 || K->p_kd > 0 || K->p_nd > 0) {
+        const uint64_t kl = cat_hash_key(P->seed, step, 11), kk = cat_hash_key(P->seed, step, 12),
+                       kn = cat_hash_key(P->seed, step, 13);
+        int nd = 0;
+        for (int d = 0; d < n; d++) {
+            const int head = prev[d] < 0 && next[d] >= 0;
+            if ((head && K->p_ld > 0 && cat_hash_u01(kl, gid[d]) < K->p_ld) ||
+                ((type[d] == 4 || type[d] == 5) && K->p_kd > 0 && cat_hash_u01(kk, gid[d]) < K->p_kd) ||
+                (type[d] == 3 && K->p_nd > 0 && cat_hash_u01(kn, gid[d]) < K->p_nd))
+                ks[nd++] = d;
+        }
+        for (int q = 0; q < nd; q++) {
+            const int d = ks[q], t = type[d];
+            if (prev[d] < 0 && next[d] >= 0) {
+                int c = d, m = 0;
+                while (c >= 0 && m < ml) {
+                    const int nx = next[c];
+                    type[c] = 0;
+                    prev[c] = -1;
+                    next[c] = -1;
+                    c = nx;
+                    m++;
+                }
+                cat_event(ev, evcap, nev, step, ORA_EV_DLIP, gid[d], x[d], y[d], -1);
+            } else if (t == 4 || t == 5) {
+                type[d] = 0;
+                cat_event(ev, evcap, nev, step, ORA_EV_DK, gid[d], x[d], y[d], t == 5);
+            } else if (t == 3) {
+                type[d] = 0;
+                cat_event(ev, evcap, nev, step, ORA_EV_DN, gid[d], x[d], y[d], -1);
+            }
+        }
+    }
+    /* food supply (feed_supply, oercel.c:1721-1753) */
+    if (K->feed_mode != 0 && K->p_feed > 0.0) {
+        const uint64_t kf = cat_hash_key(P->seed, step, 14);
+        int nc = 0;
+        for (int d = 0; d < n; d++)
+            if (type[d] == 0 && (K->feed_mode == 1 || cat_in_vent(K, L, x[d], y[d])) &&
+                cat_hash_u01(kf, gid[d]) < K->p_feed)
+                ks[nc++] = d;
+        long add = nc;
+        if (K->feed_cap > 0.0 && nc > 0) {
+            long nN = 0;
+            for (int i = 0; i < n; i++) nN += type[i] == 3;
+            long room = (long)floor(K->feed_cap * (double)n + 1e-9) - nN;
+            if (room < 0) room = 0;
+            if (add > room) {
+                for (long a = 0; a < room; a++) {
+                    const long b = a + cat_rng_below(&rng, nc - a);
+                    const int t = ks[a]; ks[a] = ks[b]; ks[b] = t;
+                }
+                add = room;
+            }
+        }
+        for (long a = 0; a < add; a++) type[ks[a]] = 3;
+        if (add > 0) cat_event(ev, evcap, nev, step, ORA_EV_FEED, (uint32_t)add, NAN, NAN, -1);
+    }
+    free(ks);
+    memcpy(rng_state, rng.s, sizeof rng.s);
+    return moved;
+}

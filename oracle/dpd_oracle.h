@@ -64,4 +64,26 @@ typedef struct {
     int32_t pad;
 } ora_event;
 
+/* the reference's catalyst chemistry (oercel.c:1345-1753): synthesis of
+ * lipids from N beads around Ka/Kb catalysts, replication and mutation of
+ * catalysts, decay, and the W -> N food supply */
+typedef struct {
+    double r_cat;                          /* catalyst reaction radius */
+    int32_t syn_tries, syn_relax, syn_nN;  /* orientation trials, relaxation iterations, N per lipid (0 = mlen) */
+    int32_t nH, nT;                        /* linear lipid template: nH heads then nT tails */
+    int32_t feed_mode, vent_kind;          /* 0 none, 1 uniform, 2 vent; 0 disk, 1 vstrip, 2 hstrip */
+    int32_t pad;
+    double p_syn_a, p_syn_b, p_rep_a, p_rep_b, mu, p_ld, p_kd, p_nd;
+    double p_feed, feed_cap, vent_x, vent_y, vent_r, vent_w;
+} ora_cat;
+
+/* event kinds of the catalyst chemistry (after the lipid chemistry's 0..2) */
+#define ORA_EV_SYN 3
+#define ORA_EV_REP 4
+#define ORA_EV_MUT 5
+#define ORA_EV_DLIP 6
+#define ORA_EV_DK 7
+#define ORA_EV_DN 8
+#define ORA_EV_FEED 9
+
 #endif

@@ -49,6 +49,15 @@ class OraChem(C.Structure):
                 ("max_chain", C.c_int32)]
 
 
+class OraCat(C.Structure):
+    _fields_ = [("r_cat", C.c_double), ("syn_tries", C.c_int32), ("syn_relax", C.c_int32), ("syn_nN", C.c_int32),
+                ("nH", C.c_int32), ("nT", C.c_int32), ("feed_mode", C.c_int32), ("vent_kind", C.c_int32),
+                ("pad", C.c_int32), ("p_syn_a", C.c_double), ("p_syn_b", C.c_double), ("p_rep_a", C.c_double),
+                ("p_rep_b", C.c_double), ("mu", C.c_double), ("p_ld", C.c_double), ("p_kd", C.c_double),
+                ("p_nd", C.c_double), ("p_feed", C.c_double), ("feed_cap", C.c_double), ("vent_x", C.c_double),
+                ("vent_y", C.c_double), ("vent_r", C.c_double), ("vent_w", C.c_double)]
+
+
 class OraEvent(C.Structure):
     _fields_ = [("step", C.c_int64), ("kind", C.c_int32), ("gid", C.c_uint32), ("partner", C.c_uint32),
                 ("x", C.c_float), ("y", C.c_float), ("pad", C.c_int32)]
@@ -79,6 +88,11 @@ def _load():
     lib.ora_cell_of.restype = C.c_int32
     lib.ora_sort.argtypes = [P, C.c_int32, f32p, f32p, i32p, i32p, i32p]
     lib.ora_stir_forces.argtypes = [P, C.c_int32, f32p, f64p]
+    u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+    lib.ora_catalyst_chemistry.argtypes = [P, C.POINTER(OraCat), u64p, C.c_int32, f32p, f32p, f32p, f32p, f32p,
+                                           f32p, u8p, u32p, i32p, i32p, i32p, C.c_int64, C.POINTER(OraEvent),
+                                           C.c_int32, C.POINTER(C.c_int32)]
+    lib.ora_catalyst_chemistry.restype = C.c_int32
     lib.ora_sdt_at.argtypes = [P, C.c_int64]
     lib.ora_sdt_at.restype = C.c_double
     lib.ora_pair_forces.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u8p, u32p, i32p, C.c_int64, C.c_int32,
@@ -194,6 +208,33 @@ def bond_forces(p, st, fx=None, fy=None):
     return fx, fy, mb.value
 
 
+CAT_DEFAULTS = dict(r_cat=1.2, syn_tries=8, syn_relax=20, syn_nN=0, nH=1, nT=3, feed_mode=1, vent_kind=0,
+                    p_syn_a=0.02, p_syn_b=0.06, p_rep_a=0.001, p_rep_b=0.001, mu=0.02, p_ld=2e-4, p_kd=5e-4,
+                    p_nd=1e-4, p_feed=1e-3, feed_cap=0.12, vent_x=-1.0, vent_y=-1.0, vent_r=5.0, vent_w=4.0)
+
+
+def cat(**kv):
+    """parameters of the catalyst chemistry (the reference's defaults, oercel.c:262-290)"""
+    c = OraCat()
+    for k, v in dict(CAT_DEFAULTS, **kv).items():
+        setattr(c, k, v)
+    return c
+
+
+def catalyst_chemistry(p, c, st, cstart, step, rng, evcap=1 << 14):
+    """one check of the reference's catalyst chemistry on the sorted state st
+    (dict of slot arrays, changed in place); rng (4 uint64) advanced in place.
+    Returns (moved, events as tuples (step, kind, i, variant, x, y))."""
+    ev = (OraEvent * evcap)()
+    nev = C.c_int32(0)
+    moved = lib().ora_catalyst_chemistry(C.byref(p), C.byref(c), rng, len(st["x"]), st["x"], st["y"], st["vhx"],
+                                         st["vhy"], st["vtx"], st["vty"], st["type"], st["gid"], st["prev"],
+                                         st["next"], cstart, int(step), ev, evcap, C.byref(nev))
+    out = [(e.step, e.kind, e.gid, (e.partner if e.partner < 2**31 else e.partner - 2**32), e.x, e.y)
+           for e in ev[: min(nev.value, evcap)]]
+    return moved, out
+
+
 def stir_forces(p, st, fx):
     """add the stirring body force (mean removed) to fx in place"""
     lib().ora_stir_forces(C.byref(p), len(st["y"]), st["y"], fx)
@@ -299,6 +340,15 @@ class Ref:
             lib.ref_theta.restype = C.c_double
             lib.ref_kinetic_T.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
             lib.ref_kinetic_T.restype = C.c_double
+            lib.ref_chemistry.argtypes = [vp, C.c_int64]
+            lib.ref_chemistry.restype = C.c_int32
+            lib.ref_nev.argtypes = [vp]
+            lib.ref_nev.restype = C.c_int32
+            i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+            u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+            lib.ref_events.argtypes = [vp, i64p, i32p, i64p, f64p, f64p, i32p]
+            lib.ref_get_rng.argtypes = [vp, u64p]
+            lib.ref_set_rng.argtypes = [vp, u64p]
             cls._lib = lib
         return cls._lib
 
@@ -329,6 +379,21 @@ class Ref:
         cs = np.empty(self.lib().ref_ncell(self.h) + 1, np.int32)
         self.lib().ref_cells(self.h, cs)
         return cs
+
+    def events(self):
+        n = self.lib().ref_nev(self.h)
+        st, kd, i, v = (np.empty(n, np.int64), np.empty(n, np.int32), np.empty(n, np.int64), np.empty(n, np.int32))
+        x, y = np.empty(n), np.empty(n)
+        self.lib().ref_events(self.h, st, kd, i, x, y, v)
+        return [(int(st[k]), int(kd[k]), int(i[k]), int(v[k]), float(x[k]), float(y[k])) for k in range(n)]
+
+    def rng(self):
+        r = np.empty(4, np.uint64)
+        self.lib().ref_get_rng(self.h, r)
+        return r
+
+    def set_rng(self, r):
+        self.lib().ref_set_rng(self.h, np.ascontiguousarray(r, np.uint64))
 
     def __getattr__(self, name):
         f = getattr(self.lib(), "ref_" + name)

@@ -186,3 +186,28 @@ double ref_kinetic_T(void *h, double *px, double *py) {
 }
 
 void ref_destroy(void *h) { free(h); /* per-bead arrays are never freed by the reference either */ }
+
+/* the reference's chemistry check at `step` (oercel.c:1565-1700), its event
+ * list and its serial generator state */
+int32_t ref_chemistry(void *h, int64_t step) {
+    ref_t *r = h;
+    r->S.nev = 0;
+    return chemistry(&r->S, &r->P, step);
+}
+
+int32_t ref_nev(void *h) { return ((ref_t *)h)->S.nev; }
+
+void ref_events(void *h, int64_t *step, int32_t *kind, int64_t *i, double *x, double *y, int32_t *variant) {
+    Sys *s = &((ref_t *)h)->S;
+    for (int k = 0; k < s->nev; k++) {
+        step[k] = s->ev[k].step;
+        kind[k] = s->ev[k].kind;
+        i[k] = s->ev[k].i;
+        x[k] = s->ev[k].x;
+        y[k] = s->ev[k].y;
+        variant[k] = s->ev[k].variant;
+    }
+}
+
+void ref_get_rng(void *h, uint64_t *s4) { memcpy(s4, ((ref_t *)h)->S.rng.s, 4 * sizeof(uint64_t)); }
+void ref_set_rng(void *h, const uint64_t *s4) { memcpy(((ref_t *)h)->S.rng.s, s4, 4 * sizeof(uint64_t)); }

@@ -117,6 +117,47 @@ def extras_fixture(L=12.5, seed=21, step=777):
     np.savez_compressed(os.path.join(HERE, f"extras_L{str(L).replace('.', 'p')}_seed{seed}.npz"), **out)
 
 
+CATALYST = dict(L=16, rho=4, dt=0.02, gamma=4.5, kT=1, k_bond=100, r0=0.5, k_angle=10, lip_nH=1, lip_nT=3,
+                f_lip=0.1, f_Ka=0.03, f_Kb=0.02, c_N=0.25, chem=1, n_chem=1, events=1, warmup=0, threads=1, nsub=1,
+                p_syn_a=0.5, p_syn_b=0.6, p_rep_a=0.4, p_rep_b=0.4, mu=0.3, p_ld=0.05, p_kd=0.05, p_nd=0.03,
+                feed="uniform", p_feed=0.05, feed_cap=0.27)
+
+
+def catalyst_fixture(name, seed, step, **over):
+    """one check of the reference's catalyst chemistry on a sorted soup state
+    with FP32 positions: the state before (slot order) and after, the serial
+    generator state before and after, and the events"""
+    kv = dict(CATALYST, seed=seed, **over)
+    r = O.Ref(**kv)
+    r.prime()
+    r.run(20)
+    a = r.get()
+    for k in ("x", "y", "vx", "vy", "vtx", "vty"):
+        a[k] = f32(a[k])
+    Lf = float(np.float32(kv["L"]))
+    for k in ("x", "y"):
+        a[k][a[k] >= Lf] = 0.0
+    r.set(a)
+    r.sort()
+    b = r.get()
+    out = {f"{k}0": b[k] for k in ("x", "y", "vx", "vy", "vtx", "vty", "type", "gid", "nxt", "mpos")}
+    out["cstart"] = r.cells()
+    out["rng0"] = r.rng()
+    moved = r.chemistry(step)
+    c = r.get()
+    out.update({f"{k}1": c[k] for k in ("x", "y", "vx", "vy", "vtx", "vty", "type", "nxt")})
+    out["rng1"] = r.rng()
+    ev = r.events()
+    out["events"] = np.array([(e[0], e[1], e[2], e[3], e[4], e[5]) for e in ev],
+                             dtype=[("step", "i8"), ("kind", "i4"), ("i", "i8"), ("variant", "i4"), ("x", "f8"),
+                                    ("y", "f8")])
+    out["moved"] = np.int32(moved)
+    out["step"] = np.int64(step)
+    out["seed"] = np.int64(seed)
+    out["ini"] = np.frombuffer("".join(f"{k} = {v}\n" for k, v in kv.items()).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -223,5 +264,8 @@ if __name__ == "__main__":
     run_fixture("run_extras_L10_seed4.npz", seed=4, k_angle=10, lip_nT=3, stir_A=1.0, stir_n=1, kT_amp=0.3,
                 kT_period=5)
     extras_fixture()
+    catalyst_fixture("catalyst_L16_seed12.npz", 12, 21)
+    catalyst_fixture("catalyst_vent_L16_seed13.npz", 13, 21, syn_nN=2, feed="vent", vent_shape="disk", vent_r=4,
+                     feed_cap=0.3)
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -200,3 +200,59 @@ def test_stirring_and_temperature_cycle_match_reference():
     O.stir_forces(p, st, fx)
     assert np.abs(fx - g["fx"]).max() < 1e-9 and np.abs(fy - g["fy"]).max() < 1e-9
     assert O.sdt_at(p, step) != pytest.approx(O.lib().ora_sdt(C.byref(p)))
+
+
+def _catalyst_case(name):
+    """the oracle's parameter blocks for a catalyst fixture (its ini) and the sorted state before the check"""
+    g = golden(name)
+    kv = dict(line.split(" = ", 1) for line in bytes(g["ini"]).decode().strip().split("\n"))
+    L = float(kv["L"])
+    p = O.params(L, np.full((8, 8), 25.0), dt=float(kv["dt"]), k_bond=float(kv["k_bond"]), r0=float(kv["r0"]),
+                 seed=int(kv["seed"]), k_angle=float(kv["k_angle"]))
+    # the reference's default repulsions (oercel.c:303-320): catalyst rows matter here
+    from oercel_b200.params import default_amatrix
+    for i, row in enumerate(default_amatrix()):
+        for j, v in enumerate(row):
+            p.a[i * 8 + j] = v
+    feed = {"none": 0, "uniform": 1, "vent": 2}[kv.get("feed", "uniform")]
+    vent = {"disk": 0, "vstrip": 1, "hstrip": 2}[kv.get("vent_shape", "disk")]
+    c = O.cat(syn_nN=int(kv.get("syn_nN", 0)), nH=int(kv["lip_nH"]), nT=int(kv["lip_nT"]), feed_mode=feed,
+              vent_kind=vent, p_syn_a=float(kv["p_syn_a"]), p_syn_b=float(kv["p_syn_b"]),
+              p_rep_a=float(kv["p_rep_a"]), p_rep_b=float(kv["p_rep_b"]), mu=float(kv["mu"]), p_ld=float(kv["p_ld"]),
+              p_kd=float(kv["p_kd"]), p_nd=float(kv["p_nd"]), p_feed=float(kv["p_feed"]),
+              feed_cap=float(kv["feed_cap"]), vent_x=0.5 * L, vent_y=0.5 * L, vent_r=float(kv.get("vent_r", 5)))
+    nxt = g["nxt0"].astype(np.int32)
+    prev = np.full_like(nxt, -1)
+    prev[nxt[nxt >= 0]] = np.nonzero(nxt >= 0)[0]
+    st = dict(x=g["x0"].astype(np.float32), y=g["y0"].astype(np.float32), vhx=g["vx0"].astype(np.float32),
+              vhy=g["vy0"].astype(np.float32), vtx=g["vtx0"].astype(np.float32), vty=g["vty0"].astype(np.float32),
+              type=g["type0"].astype(np.uint8), gid=g["gid0"].astype(np.uint32), prev=prev, next=nxt.copy())
+    return g, p, c, st
+
+
+@pytest.mark.parametrize("name", ["catalyst_L16_seed12.npz", "catalyst_vent_L16_seed13.npz"])
+def test_catalyst_chemistry_matches_reference(name):
+    """one check of the reference's catalyst chemistry: synthesis (orientation
+    trials, relaxation), replication and mutation, decay, capped food supply"""
+    g, p, c, st = _catalyst_case(name)
+    rng = g["rng0"].astype(np.uint64).copy()
+    moved, ev = O.catalyst_chemistry(p, c, st, g["cstart"].astype(np.int32), int(g["step"]), rng)
+    assert moved == int(g["moved"])
+    assert np.array_equal(rng, g["rng1"])          # the serial generator consumed exactly the same draws
+    assert np.array_equal(st["type"], g["type1"])
+    assert np.array_equal(st["next"], g["nxt1"])
+    L = float(p.L)
+    for k in ("x", "y"):
+        d = st[k].astype(np.float64) - g[f"{k}1"]
+        d -= L * np.round(d / L)
+        assert np.abs(d).max() < 2e-6, k
+    for k, r in (("vhx", "vx1"), ("vhy", "vy1"), ("vtx", "vtx1"), ("vty", "vty1")):
+        assert np.abs(st[k] - g[r]).max() < 1e-6, k
+    ref = g["events"]
+    assert len(ev) == len(ref)
+    for e, r in zip(ev, ref):
+        assert (e[0], e[1] - 3, e[2], e[3]) == (int(r["step"]), int(r["kind"]), int(r["i"]), int(r["variant"]))
+        if np.isfinite(r["x"]):
+            assert abs(e[4] - r["x"]) < 1e-5 and abs(e[5] - r["y"]) < 1e-5
+    kinds = {int(r["kind"]) for r in ref}
+    assert {0, 1}.issubset(kinds)  # synthesis and replication happened in this check
