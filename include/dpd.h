@@ -99,6 +99,24 @@ typedef struct {
     double kT_period;          /* (kT_period) */
     double t_anchor;           /* time of step step_anchor: t(step) = t_anchor + (step - step_anchor) dt */
     int64_t step_anchor;
+    /* which chemistry chem = 1 runs: 0 = the lipid chemistry above (p_grow,
+     * p_break, p_bond), 1 = the reference's catalyst chemistry (keys below,
+     * oercel.c:1565-1753), which needs the serial generator state of
+     * dpd_set_rng */
+    int32_t chem_kind;
+    int32_t syn_tries;         /* orientation trials of a new lipid (syn_tries) */
+    int32_t syn_relax;         /* relaxation iterations of a new lipid (syn_relax) */
+    int32_t syn_nN;            /* N beads consumed per lipid, 0 = all of it (syn_nN) */
+    int32_t lip_nH, lip_nT;    /* linear lipid template: heads, tails (lip_nH, lip_nT) */
+    int32_t feed_mode;         /* 0 none, 1 uniform, 2 vent (feed) */
+    int32_t vent_kind;         /* 0 disk, 1 vstrip, 2 hstrip (vent_shape) */
+    double r_cat;              /* catalyst reaction radius (r_cat) */
+    double p_syn_a, p_syn_b;   /* synthesis probability per check, Ka / Kb */
+    double p_rep_a, p_rep_b;   /* replication probability per check, Ka / Kb */
+    double mu;                 /* mutation probability per replication */
+    double p_ld, p_kd, p_nd;   /* decay probability per check: lipid, catalyst, N */
+    double p_feed, feed_cap;   /* W -> N probability per check, cap on the N fraction (0 = none) */
+    double vent_x, vent_y, vent_r, vent_w; /* vent region */
 } dpd_params;
 
 /* One chemistry event, the reference's events.csv row (oercel.c:788-798)
@@ -155,10 +173,11 @@ DPD_API int dpd_set_state(dpd_handle *h, int32_t replica, const float *x, const 
 DPD_API int dpd_get_state(dpd_handle *h, int32_t replica, float *x, float *y, float *vhx, float *vhy, float *vtx, float *vty,
                   float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev, int32_t *next);
 
-/* Overwrite the stored half-step velocity and force of replica r (slot
- * order), e.g. to continue from a checkpoint.  NULL leaves a field as is. */
+/* Overwrite the stored half-step velocity, the force and the predicted
+ * velocity of replica r (slot order), e.g. to continue from a checkpoint.
+ * NULL leaves a field as is. */
 DPD_API int dpd_set_dynamics(dpd_handle *h, int32_t replica, const float *vhx, const float *vhy, const float *fx,
-                     const float *fy);
+                             const float *fy, const float *vtx, const float *vty);
 
 /* Fresh start as the reference's main() (oercel.c:2203-2211): take the loaded
  * velocity as the full velocity v, sort by cell, compute the forces of the
@@ -188,8 +207,10 @@ DPD_API int dpd_get_tuning(const dpd_handle *h, dpd_tuning *t);
 DPD_API int dpd_set_graph_steps(dpd_handle *h, int32_t steps);
 /* One real step launched kernel by kernel with CUDA events around each launch
  * on the handle's stream: ms[k] = device time of kernel k in launch order
- * (scan1, scan2, place, cellfix, permute, [2 chemistry kernels], forces);
- * *n_out = number of kernels. */
+ * (scan1, scan2, place, cellfix, permute, [2 chemistry kernels], [catalyst
+ * check with its sort], forces); *n_out = number of kernels.  On a step with a
+ * catalyst check the first entry is a one-thread step-counter kernel and the
+ * next three are not launched (0 ms). */
 DPD_API int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_out);
 
 /* The reference's random soup (init_soup + set_velocities,
@@ -198,10 +219,18 @@ DPD_API int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_o
  * positions, then nKa = round(f_Ka N) beads of type 4, nKb of type 5,
  * round(c_N N) of type 3 (P), the rest W; Gaussian velocities with the mean
  * removed, rescaled to exactly kT.  HOST arrays of N entries in gid order.
- * *n_lipid_beads receives the number of beads placed in lipids. */
+ * *n_lipid_beads receives the number of beads placed in lipids; rng_out
+ * (4 words, may be NULL) the generator state after the soup, from which the
+ * reference's serial chemistry continues. */
 DPD_API int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, double r0, int32_t nH, int32_t nT,
                           double f_lip, double f_Ka, double f_Kb, double c_N, double *x, double *y, double *vx,
-                          double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads);
+                          double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads,
+                          uint64_t *rng_out);
+
+/* The serial xoshiro256** state of the catalyst chemistry of replica r
+ * (4 words; the reference's Sys.rng, checkpointed with the state). */
+DPD_API int dpd_set_rng(dpd_handle *h, int32_t replica, const uint64_t *state);
+DPD_API int dpd_get_rng(dpd_handle *h, int32_t replica, uint64_t *state);
 
 /* ---- phases, for testing and custom loops ---- */
 

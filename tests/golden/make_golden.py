@@ -244,7 +244,11 @@ def run_fixture(name="run_L10_seed3.npz", **over):
             with open(path, "rb") as f:
                 return np.frombuffer(f.read(), np.uint8)
 
-        np.savez_compressed(os.path.join(HERE, name), ini=np.frombuffer(text.encode(), np.uint8),
+        extra = {}
+        for tag, d in (("a", a), ("b", b)):
+            if os.path.exists(f"{d}/events.csv"):
+                extra[f"events_{tag}"] = rd(f"{d}/events.csv")
+        np.savez_compressed(os.path.join(HERE, name), **extra, ini=np.frombuffer(text.encode(), np.uint8),
                             stats_a=rd(f"{a}/stats.csv"), stats_b=rd(f"{b}/stats.csv"),
                             snap_0=rd(f"{a}/snap_0000000000.bin"), snap_12=rd(f"{a}/snap_0000000012.bin"),
                             snap_24=rd(f"{a}/snap_0000000024.bin"), snap_36=rd(f"{b}/snap_0000000036.bin"),
@@ -263,6 +267,9 @@ if __name__ == "__main__":
     run_fixture()
     run_fixture("run_extras_L10_seed4.npz", seed=4, k_angle=10, lip_nT=3, stir_A=1.0, stir_n=1, kT_amp=0.3,
                 kT_period=5)
+    run_fixture("run_cat_L16_seed5.npz", L=16, seed=5, chem=1, n_chem=4, events=1, nsub=1, k_angle=10, lip_nT=3,
+                f_Ka=0.03, f_Kb=0.02, c_N=0.25, p_syn_a=0.3, p_syn_b=0.3, p_rep_a=0.2, p_rep_b=0.2, mu=0.2,
+                p_ld=0.01, p_kd=0.01, p_nd=0.01, p_feed=0.02, feed_cap=0.27)
     extras_fixture()
     catalyst_fixture("catalyst_L16_seed12.npz", 12, 21)
     catalyst_fixture("catalyst_vent_L16_seed13.npz", 13, 21, syn_nN=2, feed="vent", vent_shape="disk", vent_r=4,

@@ -7,8 +7,8 @@ from conftest import amat_config
 
 # physics of the workloads (configuration 1 of the workload table)
 BASE = dict(rho=4, dt=0.02, gamma=4.5, kT=1, k_bond=100, r0=0.5, k_angle=0, lip_nH=1, lip_nT=2, f_lip=0.15,
-            f_Ka=0, f_Kb=0, c_N=0.05, chem=0, warmup=0, a_W_H=25, a_W_T=75, a_H_T=50, a_W_P=25, a_H_P=25,
-            a_P_T=75)
+            f_Ka=0, f_Kb=0, c_N=0.05, chem=0, chem_kind="lipid", warmup=0, a_W_H=25, a_W_T=75, a_H_T=50, a_W_P=25,
+            a_H_P=25, a_P_T=75)
 
 
 def params(**kv):

@@ -43,9 +43,9 @@ def test_errors_exit_1(tmp_path, capsys):
     ini.write_text("L = 16\nk_angle = 0\nf_Ka = 0\ninit = restart\n")
     assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
     assert "needs restart" in capsys.readouterr().err
-    ini.write_text("L = 16\nk_angle = 0\n")  # the catalyst beads of the default soup
+    ini.write_text("L = 16\nchem_kind = enzyme\n")
     assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
-    assert "catalyst" in capsys.readouterr().err
+    assert "chem_kind" in capsys.readouterr().err
     ini.write_text("L = 16\nk_angle = 0\n")
     assert cli.run(["x", str(ini), str(tmp_path / "o"), "seed"]) == 1
     assert "not key=value" in capsys.readouterr().err
@@ -103,13 +103,16 @@ def test_checkpoint_round_trip(tmp_path):
     for k in ("x", "y", "vhx", "vhy", "fx", "fy"):
         st[k] = rng.random(n).astype(np.float32)
     path = str(tmp_path / "ckpt.bin")
-    cli.write_ckpt(path, st, 1234, 24.68, 16.0, 2**63 + 5, 1000, (0.0, 0, 0.02), keep_copy=str(tmp_path / "k.bin"))
+    rng = np.array([1, 2**63, 3, 2**64 - 1], np.uint64)
+    cli.write_ckpt(path, st, 1234, 24.68, 16.0, 2**63 + 5, 1000, (0.0, 0, 0.02), keep_copy=str(tmp_path / "k.bin"),
+                   rng=rng)
     for p in (path, str(tmp_path / "k.bin")):
         ck = cli.read_ckpt(p)
         assert (ck["N"], ck["step"], ck["time"], ck["L"], ck["seed"], ck["warm_end"]) == \
             (n, 1234, 24.68, 16.0, 2**63 + 5, 1000)
         for k in st:
             assert np.array_equal(ck[k], st[k]), k
+        assert np.array_equal(ck["rng"], rng)
     raw = open(path, "rb").read()
     with open(path, "wb") as f:
         f.write(raw[:-2])

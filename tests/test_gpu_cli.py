@@ -1,13 +1,15 @@
 """The drop-in executable on the GPU against runs of the reference executable
 (tests/golden/run_L10_seed3.npz: a fresh soup with the repulsion warm-up, 24
-steps, and a restart from its checkpoint to step 36), plus the continuation,
-walltime and SIGTERM contract.
+steps, and a restart from its checkpoint to step 36; the same with the angle
+terms, stirring and the temperature cycle, and with the catalyst chemistry),
+plus the continuation, walltime and SIGTERM contract.
 
 Criteria: the step-0 snapshot (the soup) is byte-identical; stats rows agree in
 step, time, counts and chain numbers exactly and in T_kin and max_bond within
 2e-3 relative (FP32 state against FP64 over <= 36 steps); snapshot positions
 within 1e-3 (minimum image).  A continuation from this engine's own checkpoint
-is bit-identical to the uninterrupted run."""
+is bit-identical to the uninterrupted run.  With chemistry, the events are the
+reference's (step, kind, bead, variant)."""
 import os
 import shutil
 import signal
@@ -26,6 +28,8 @@ EXE = os.path.join(PKG, "bin", "oercel_b200")
 G = "run_L10_seed3.npz"
 # the same runs with angle terms (k_angle = 10, H-T-T-T lipids), stirring and the temperature cycle
 G_EXTRAS = "run_extras_L10_seed4.npz"
+# the same runs with the reference's catalyst chemistry every 4 steps (events on)
+G_CAT = "run_cat_L16_seed5.npz"
 
 
 def fixture_bytes(key, name=G):
@@ -67,6 +71,13 @@ def check_stats(got_text, ref_text):
         assert float(g[11]) == pytest.approx(float(r[11]), rel=2e-3), (g, r)  # max_bond
 
 
+def check_events(got_text, ref_text):
+    """the same events (step, kind, bead, variant) in any order within a step"""
+    key = lambda r: (int(r[0]), r[1], int(r[2]), r[5])
+    assert got_text.startswith("step,kind,i,x,y,variant\n")
+    assert sorted(map(key, rows(got_text))) == sorted(map(key, rows(ref_text)))
+
+
 def check_snapshot(path, ref_key, name=G):
     ref_path = path + ".ref"
     with open(ref_path, "wb") as f:
@@ -82,13 +93,15 @@ def check_snapshot(path, ref_key, name=G):
         assert np.abs(d).max() < 1e-3, k
 
 
-@pytest.mark.parametrize("name", [G, G_EXTRAS])
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT])
 def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
     ini = write_ini(tmp_path, name)
     out = tmp_path / "run"
     run_exe(ini, out, "noise=mix13")
     assert (out / "snap_0000000000.bin").read_bytes() == fixture_bytes("snap_0", name)
     check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_a", name).decode())
+    if "events_a" in golden(name):
+        check_events((out / "events.csv").read_text(), fixture_bytes("events_a", name).decode())
     check_snapshot(str(out / "snap_0000000012.bin"), "snap_12", name)
     check_snapshot(str(out / "snap_0000000024.bin"), "snap_24", name)
     log = (out / "log.txt").read_text()
@@ -97,7 +110,7 @@ def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
     assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] == 24
 
 
-@pytest.mark.parametrize("name", [G, G_EXTRAS])
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT])
 def test_restart_from_a_reference_checkpoint(cuda_ok, tmp_path, name):
     ini = write_ini(tmp_path, name)
     ck = tmp_path / "ref_ckpt.bin"
@@ -105,12 +118,14 @@ def test_restart_from_a_reference_checkpoint(cuda_ok, tmp_path, name):
     out = tmp_path / "cont"
     run_exe(ini, out, "noise=mix13", f"restart={ck}", "steps=36")
     check_stats((out / "stats.csv").read_text(), fixture_bytes("stats_b", name).decode())
+    if "events_b" in golden(name):
+        check_events((out / "events.csv").read_text(), fixture_bytes("events_b", name).decode())
     check_snapshot(str(out / "snap_0000000036.bin"), "snap_36", name)
     assert "restart from" in (out / "log.txt").read_text()
 
 
-CHEM = ("chem=1", "events=1", "n_chem=1", "p_grow=0.05", "p_bond=0.3", "p_break=0.02", "noise=philox", "ckpt_every=12",
-        "ckpt_keep=1", "snap_every=6")
+CHEM = ("chem=1", "chem_kind=lipid", "events=1", "n_chem=1", "p_grow=0.05", "p_bond=0.3", "p_break=0.02",
+        "noise=philox", "ckpt_every=12", "ckpt_keep=1", "snap_every=6")
 
 
 def test_own_checkpoint_continuation_is_bitwise(cuda_ok, ini, tmp_path):

@@ -1,11 +1,13 @@
 // dpd_capi.cu -- the C ABI of libdpd.so (include/dpd.h): handles, device
 // memory, CUDA graphs of the step, state in/out, error reporting.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <numeric>
 #include <vector>
 
 #include "../../include/dpd.h"
@@ -55,7 +57,11 @@ struct dpd_handle {
     int64_t step = 0;
     // CUDA graphs of gsteps consecutive steps, one per starting buffer parity
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int gflip[2] = {0, 0};      // buffer parity change of one replay (steps + the extra sorts of catalyst checks)
     int gsteps = 0;
+    // the reference's catalyst chemistry: replicas with chem_kind 1, the period of their checks
+    bool any_cat = false, any_lipid = false;
+    int64_t cat_period = 0;
     // reverse-mode storage, grown on demand (full checkpoints, the states of one
     // recomputed segment, adjoint arrays in gid order)
     std::vector<void *> adj_allocs;
@@ -82,6 +88,27 @@ extern "C" int dpd_params_default(dpd_params *p) {
     p->k_angle = 10.0;
     p->stir_n = 1;
     p->kT_period = 1000.0;
+    p->chem_kind = 0;
+    p->syn_tries = 8;   // catalyst chemistry: the reference's defaults, oercel.c:262-290
+    p->syn_relax = 20;
+    p->lip_nH = 1;
+    p->lip_nT = 3;
+    p->feed_mode = 1;
+    p->r_cat = 1.2;
+    p->p_syn_a = 0.02;
+    p->p_syn_b = 0.06;
+    p->p_rep_a = 0.001;
+    p->p_rep_b = 0.001;
+    p->mu = 0.02;
+    p->p_ld = 2e-4;
+    p->p_kd = 5e-4;
+    p->p_nd = 1e-4;
+    p->p_feed = 1e-3;
+    p->feed_cap = 0.12;
+    p->vent_x = -1.0;
+    p->vent_y = -1.0;
+    p->vent_r = 5.0;
+    p->vent_w = 4.0;
     p->seed = 1;
     p->noise = 0;
     p->chem = 0;
@@ -166,6 +193,51 @@ static int make_rep(const dpd_params &p, int b0, int n, int c0, RepDev &R) {
     R.dt_d = p.dt;
     R.t_anchor = p.t_anchor;
     R.step_anchor = (long long)p.step_anchor;
+    R.kb_d = p.k_bond;
+    R.r0_d = p.r0;
+    R.ka_d = p.k_angle;
+    R.chem_kind = p.chem_kind;
+    if (p.chem_kind != 0 && p.chem_kind != 1) return fail(DPD_E_ARG, "chem_kind must be 0 (lipid) or 1 (catalyst)");
+    if (p.chem && p.chem_kind == 1) {
+        const int ml = p.lip_nH + p.lip_nT;
+        if (p.lip_nH < 1 || p.lip_nT < 0 || ml < 2 || ml > 16) return fail(DPD_E_ARG, "lipids of 2..16 beads");
+        if (!(p.r_cat > 0.0) || p.syn_tries < 1 || p.syn_relax < 0 || p.syn_nN < 0 || p.syn_nN > ml)
+            return fail(DPD_E_ARG, "need r_cat > 0, syn_tries >= 1, syn_relax >= 0, 0 <= syn_nN <= mlen");
+        if (p.feed_mode < 0 || p.feed_mode > 2 || p.vent_kind < 0 || p.vent_kind > 2)
+            return fail(DPD_E_ARG, "feed_mode 0..2, vent_kind 0..2");
+        if (p.p_feed < 0.0 || p.p_feed > 1.0 || p.feed_cap < 0.0 || p.feed_cap >= 1.0)
+            return fail(DPD_E_ARG, "p_feed in [0, 1], feed_cap in [0, 1)");
+        // the cells a catalyst's visit can reach: the N window, the new chain's
+        // extent around the centroid, and the energy and relaxation windows
+        const double reach = 1.0 + 0.05 * p.syn_relax, ics = R.ncx / (double)R.L;
+        const int wmax = std::max({(int)std::ceil((p.r_cat + 0.5) * ics), (int)std::ceil(1.5 * ics),
+                                   (int)std::ceil((reach + 0.5) * ics)});
+        R.cat_E = (int)std::ceil((p.r_cat + 0.5 * (ml - 1) * p.r0) * ics) + 2 + wmax;
+        if (2 * (int)std::ceil((reach + 0.5) * ics) + 1 > R.ncx)
+            return fail(DPD_E_ARG, "box too small for the catalyst windows (L must exceed 2 (r_cat, reach) + 1)");
+    }
+    R.syn_tries = p.syn_tries;
+    R.syn_relax = p.syn_relax;
+    R.syn_nN = p.syn_nN;
+    R.lip_nH = p.lip_nH;
+    R.lip_nT = p.lip_nT;
+    R.feed_mode = p.feed_mode;
+    R.vent_kind = p.vent_kind;
+    R.r_cat = p.r_cat;
+    R.p_syn_a = p.p_syn_a;
+    R.p_syn_b = p.p_syn_b;
+    R.p_rep_a = p.p_rep_a;
+    R.p_rep_b = p.p_rep_b;
+    R.mu = p.mu;
+    R.p_ld = p.p_ld;
+    R.p_kd = p.p_kd;
+    R.p_nd = p.p_nd;
+    R.p_feed = p.p_feed;
+    R.feed_cap = p.feed_cap;
+    R.vent_x = p.vent_x < 0.0 ? 0.5 * p.L : p.vent_x;  // the reference centres an unset vent (oercel.c:607-608)
+    R.vent_y = p.vent_y < 0.0 ? 0.5 * p.L : p.vent_y;
+    R.vent_r = p.vent_r;
+    R.vent_w = p.vent_w;
     return DPD_OK;
 }
 
@@ -185,6 +257,15 @@ static int dalloc(dpd_handle *h, T **p, size_t count) {
         int r_ = (x);                \
         if (r_ != DPD_OK) return r_; \
     } while (0)
+
+// graph length: with catalyst chemistry a multiple of its period (so that a
+// replay starting on a multiple of the period holds the checks in place)
+static int graph_len(const dpd_handle *h, int g) {
+    g = std::max(1, g);
+    const int64_t P = h->cat_period;
+    if (P > 0 && P <= 1024) g = (int)(((g + P - 1) / P) * P);
+    return g;
+}
 
 static void drop_graphs(dpd_handle *h) {
     for (int k = 0; k < 2; k++)
@@ -246,6 +327,12 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
         if (n_beads[r] < 2) return fail(DPD_E_ARG, "replica %d: need at least 2 beads", r);
         TRY(make_rep(params[r], (int)b0, n_beads[r], (int)c0, h->rh[r]));
         h->any_chem = h->any_chem || params[r].chem;
+        h->any_lipid = h->any_lipid || (params[r].chem && params[r].chem_kind == 0);
+        if (params[r].chem && params[r].chem_kind == 1) {
+            h->any_cat = true;
+            const int64_t a = h->cat_period ? h->cat_period : 1, c = params[r].n_chem;
+            h->cat_period = a / std::gcd(a, c) * c;
+        }
         h->any_stir = h->any_stir || params[r].stir_A != 0.0;
         b0 += n_beads[r];
         c0 += h->rh[r].ncell;
@@ -259,7 +346,9 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     std::vector<Chunk> bch, cch;
     for (int r = 0; r < nrep; r++) {
         const RepDev &R = h->rh[r];
+        h->rh[r].ch0 = (int32_t)bch.size();
         for (int k = 0; k < R.n; k += BEAD_TPB) bch.push_back({r, R.b0 + k, R.b0 + std::min(R.n, k + BEAD_TPB), 0});
+        h->rh[r].nch = (int32_t)bch.size() - h->rh[r].ch0;
         for (int k = 0; k < R.ncell; k += CELL_TPB)
             cch.push_back({r, R.c0 + k, R.c0 + std::min(R.ncell, k + CELL_TPB), 0});
     }
@@ -307,6 +396,12 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.obs, (size_t)nrep * OBS_N));
     TRY(dalloc(h, &b.hist, 4096));
     TRY(dalloc(h, &b.stir, (size_t)nrep));
+    TRY(dalloc(h, &b.rng, (size_t)4 * nrep));
+    TRY(dalloc(h, &b.cat_list, N));
+    TRY(dalloc(h, &b.cat_cnt, (size_t)h->nbch + 1));
+    TRY(dalloc(h, &b.cat_ncnt, (size_t)h->nbch + 1));
+    CK(cudaMemset(b.rng, 0, (size_t)4 * nrep * sizeof(uint64_t)));
+    if (h->any_cat && catalyst_setup() != 0) return fail(DPD_E_CUDA, "cannot reserve shared memory for the catalyst kernel");
     CK(cudaMemset(b.stir, 0, (size_t)nrep * sizeof(long long)));
     // staging for set/get state: 8 float + 3 int32 + 1 byte arrays of nmax
     TRY(dalloc(h, &h->stage, (size_t)h->nmax * (8 * 4 + 3 * 4 + 1) + 16 * 256));
@@ -327,7 +422,7 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     // graph length: even (the buffers alternate every step), ~4M bead-steps per replay
     int g = (int)std::max<int64_t>(1, std::min<int64_t>(64, (4 << 20) / std::max<int64_t>(1, h->N)));
     if (const char *e = getenv("DPD_GRAPH_STEPS")) g = atoi(e);
-    h->gsteps = std::max(1, g);
+    h->gsteps = graph_len(h, g);
     TRY(build_tiles(h));
     return DPD_OK;
 }
@@ -375,6 +470,12 @@ static int check_status(dpd_handle *h) {
     if (st.flags) {
         CK(cudaMemsetAsync(&h->b.status->flags, 0, sizeof(unsigned), h->s));
         CK(cudaStreamSynchronize(h->s));
+        if (st.flags & DPD_F_MARGIN)
+            return fail(DPD_E_STATE, "a bead moved 0.5 or more in the step before a catalyst check, which uses the "
+                                     "previous cell index (the reference sorts again first); reduce dt");
+        if (st.flags & DPD_F_CATALYST)
+            return fail(DPD_E_STATE, "a catalyst's neighbourhood did not fit the staging area, or a search found "
+                                     "more than 256 candidates or 512 relaxation neighbours (too crowded)");
         if (st.flags & DPD_F_TILE)
             return fail(DPD_E_SORT_OVERFLOW, "a cell tile and its halo held more beads than fit in shared memory");
         if (st.flags & DPD_F_FORCE) return fail(DPD_E_STATE, "a pair or bond force above 2048 (fixed-point range)");
@@ -451,18 +552,19 @@ extern "C" int dpd_get_state(dpd_handle *h, int32_t r, float *x, float *y, float
 }
 
 extern "C" int dpd_set_dynamics(dpd_handle *h, int32_t r, const float *vhx, const float *vhy, const float *fx,
-                                const float *fy) {
+                                const float *fy, const float *vtx, const float *vty) {
     TRY(ensure_replica(h, r));
     const RepDev &R = h->rh[r];
     const size_t n = (size_t)R.n, a = ((n * 4 + 255) / 256) * 256;
-    const float *in[4] = {vhx, vhy, fx, fy};
-    float *sg[4];
-    for (int k = 0; k < 4; k++) {
+    const float *in[6] = {vhx, vhy, fx, fy, vtx, vty};
+    float *sg[6];
+    for (int k = 0; k < 6; k++) {
         sg[k] = (float *)(h->stage + k * a);
         if (in[k]) CK(cudaMemcpyAsync(sg[k], in[k], n * 4, cudaMemcpyDefault, h->s));
     }
     launch_set_dynamics(h->b, h->cur, R.b0, (int)n, vhx ? sg[0] : nullptr, vhy ? sg[1] : nullptr,
-                        fx ? sg[2] : nullptr, fy ? sg[3] : nullptr, h->s);
+                        fx ? sg[2] : nullptr, fy ? sg[3] : nullptr, vtx ? sg[4] : nullptr, vty ? sg[5] : nullptr,
+                        h->s);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s));
     h->keys_valid = false;
@@ -615,25 +717,52 @@ extern "C" int dpd_chemistry(dpd_handle *h, int64_t step) {
     CK(cudaMemsetAsync(&h->b.status->n_grow, 0, 2 * sizeof(unsigned), h->s));
     launch_chem_scan(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
+    // the catalyst chemistry as the reference's chemistry(): no sort afterwards
+    if (h->any_cat) launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->s);
     CK(cudaGetLastError());
     return check_status(h);
 }
 
 // ---------------------------------------------------------------- the step
 
-static void enqueue_step(dpd_handle *h) {
-    launch_scan(h->b, h->C, true, h->s);
-    launch_place(h->b, h->d_bch, h->nbch, h->s);
-    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+// does a catalyst check of some replica fall on step s
+static bool cat_at(const dpd_handle *h, int64_t s) {
+    if (!h->any_cat) return false;
+    for (const auto &p : h->params)
+        if (p.chem && p.chem_kind == 1 && p.n_chem > 0 && s % p.n_chem == 0) return true;
+    return false;
+}
+
+// one step producing step number s.  A step with a catalyst check follows the
+// reference's order (oercel.c:2337-2349): the update with every bead kept in
+// the slot of the last sort, the check on that order and cell index (the
+// catalysts and the food candidates are taken in slot order), then the sort of
+// the new configuration.  Other steps fuse the update into the sort whose
+// counts the previous force kernel made.
+static void enqueue_step(dpd_handle *h, int64_t s) {
+    const bool cat = cat_at(h, s);
+    if (!cat) {
+        launch_scan(h->b, h->C, true, h->s);
+        launch_place(h->b, h->d_bch, h->nbch, h->s);
+        launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    } else {
+        launch_step_begin(h->b, h->s);
+    }
     clear_stir(h);
-    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
+    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, cat ? PERM_KEEP : PERM_STEP, h->s);
     h->cur ^= 1;
-    if (h->any_chem) launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
+    if (h->any_lipid) launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
+    if (cat) {
+        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->s);
+        enqueue_sort(h, PERM_SORT);
+    }
     enqueue_forces(h, true);
 }
 
-// capture gsteps steps starting from the current buffer parity
-static int build_graph(dpd_handle *h) {
+// capture gsteps steps starting from the current buffer parity and step s0
+// (with catalyst chemistry s0 is a multiple of its period: the graph then
+// holds the checks at the same places on every replay)
+static int build_graph(dpd_handle *h, int64_t s0) {
     const int cur0 = h->cur;
     if (h->gexec[cur0]) {
         CK(cudaGraphExecDestroy(h->gexec[cur0]));
@@ -641,8 +770,9 @@ static int build_graph(dpd_handle *h) {
     }
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < h->gsteps; k++) enqueue_step(h);
+    for (int k = 0; k < h->gsteps; k++) enqueue_step(h, s0 + 1 + k);
     const cudaError_t e = cudaStreamEndCapture(h->s, &g);
+    h->gflip[cur0] = h->cur ^ cur0;
     h->cur = cur0;  // capture only recorded the launches
     if (e != cudaSuccess) return fail(DPD_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
     const cudaError_t e2 = cudaGraphInstantiate(&h->gexec[cur0], g, 0);
@@ -656,15 +786,22 @@ static int enqueue_steps(dpd_handle *h, int64_t nsteps) {
     if (nsteps < 0) return fail(DPD_E_ARG, "nsteps must be >= 0");
     if (nsteps == 0) return DPD_OK;
     if (!h->keys_valid) enqueue_next_keys(h);
-    int64_t left = nsteps;
-    const bool graphs = getenv("DPD_NO_GRAPH") == nullptr;
-    while (graphs && left >= h->gsteps) {
-        if (!h->gexec[h->cur]) TRY(build_graph(h));
-        CK(cudaGraphLaunch(h->gexec[h->cur], h->s));
-        left -= h->gsteps;
-        if (h->gsteps & 1) h->cur ^= 1;
+    int64_t left = nsteps, s = h->step;
+    const int64_t P = h->cat_period;
+    const bool graphs = getenv("DPD_NO_GRAPH") == nullptr && (P == 0 || h->gsteps % P == 0);
+    while (left > 0) {
+        if (graphs && left >= h->gsteps && (P == 0 || s % P == 0)) {
+            if (!h->gexec[h->cur]) TRY(build_graph(h, s));
+            CK(cudaGraphLaunch(h->gexec[h->cur], h->s));
+            h->cur ^= h->gflip[h->cur];
+            left -= h->gsteps;
+            s += h->gsteps;
+        } else {
+            enqueue_step(h, s + 1);
+            left--;
+            s++;
+        }
     }
-    for (; left > 0; left--) enqueue_step(h);
     CK(cudaGetLastError());
     h->step += nsteps;
     return DPD_OK;
@@ -702,7 +839,7 @@ extern "C" int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t) {
         return r;
     }
     h->force_kernel = t->force_kernel;
-    h->gsteps = t->graph_steps;
+    h->gsteps = graph_len(h, t->graph_steps);
     drop_graphs(h);
     return DPD_OK;
 }
@@ -720,41 +857,49 @@ extern "C" int dpd_set_graph_steps(dpd_handle *h, int32_t steps) {
     if (!h || steps < 1) return fail(DPD_E_ARG, "graph length must be >= 1");
     CK(cudaStreamSynchronize(h->s));
     drop_graphs(h);
-    h->gsteps = steps;
+    h->gsteps = graph_len(h, steps);
     return DPD_OK;
 }
 
 // One step launched kernel by kernel with CUDA events between the launches on
 // the handle's stream; ms[k] = device time of kernel k (scan1, scan2, place,
-// cellfix, permute, [2 chemistry], forces).  The step is a real step.
+// cellfix, permute, [2 chemistry], [catalyst check + its sort], forces).  The
+// step is a real step; on a step with a catalyst check the first entry is the
+// step counter's kernel, the next three are not launched (0 ms) and the
+// permute keeps the slot order.
 extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_out) {
     if (!h || !ms || !n_out) return fail(DPD_E_ARG, "null argument");
     if (!h->keys_valid) enqueue_next_keys(h);
-    const int nk = 6 + (h->any_chem ? chem_kernel_count() : 0);
+    const bool cat = cat_at(h, h->step + 1);
+    const int nk = 6 + (h->any_lipid ? chem_kernel_count() : 0) + (cat ? 1 : 0);
     if (cap < nk) return fail(DPD_E_ARG, "need room for %d kernel times", nk);
     std::vector<cudaEvent_t> ev(nk + 1);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     int k = 0;
-    const int nb = (int)((h->C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
-    (void)nb;
     CK(cudaEventRecord(ev[k++], h->s));
-    launch_scan_part(h->b, h->C, true, 1, h->s);
+    if (!cat) launch_scan_part(h->b, h->C, true, 1, h->s);
+    else launch_step_begin(h->b, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
-    launch_scan_part(h->b, h->C, true, 2, h->s);
+    if (!cat) launch_scan_part(h->b, h->C, true, 2, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
-    launch_place(h->b, h->d_bch, h->nbch, h->s);
+    if (!cat) launch_place(h->b, h->d_bch, h->nbch, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
-    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    if (!cat) launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
     clear_stir(h);
-    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
+    launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, cat ? PERM_KEEP : PERM_STEP, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
     h->cur ^= 1;
-    if (h->any_chem)
+    if (h->any_lipid)
         for (int c = 0; c < chem_kernel_count(); c++) {
             launch_chem_lists(h->b, h->cur, h->d_rep, c, h->s);
             CK(cudaEventRecord(ev[k++], h->s));
         }
+    if (cat) {
+        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->s);
+        enqueue_sort(h, PERM_SORT);
+        CK(cudaEventRecord(ev[k++], h->s));
+    }
     enqueue_forces(h, true);
     CK(cudaEventRecord(ev[k++], h->s));
     CK(cudaGetLastError());
@@ -839,10 +984,26 @@ extern "C" int dpd_get_stream(const dpd_handle *h, void **stream) {
     return DPD_OK;
 }
 
+extern "C" int dpd_set_rng(dpd_handle *h, int32_t r, const uint64_t *state) {
+    TRY(ensure_replica(h, r));
+    if (!state) return fail(DPD_E_ARG, "null state");
+    CK(cudaMemcpyAsync(h->b.rng + 4 * r, state, 4 * sizeof(uint64_t), cudaMemcpyDefault, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return DPD_OK;
+}
+
+extern "C" int dpd_get_rng(dpd_handle *h, int32_t r, uint64_t *state) {
+    TRY(ensure_replica(h, r));
+    if (!state) return fail(DPD_E_ARG, "null state");
+    CK(cudaMemcpyAsync(state, h->b.rng + 4 * r, 4 * sizeof(uint64_t), cudaMemcpyDefault, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return DPD_OK;
+}
+
 extern "C" int dpd_kernels_per_step(const dpd_handle *h, int32_t *n_plain, int32_t *n_chem) {
     if (!h) return fail(DPD_E_ARG, "null handle");
     // scan1, scan2, place, cellfix, permute, forces (+ the chemistry kernels)
-    if (n_plain) *n_plain = 6 + (h->any_chem ? chem_kernel_count() : 0);
+    if (n_plain) *n_plain = 6 + (h->any_lipid ? chem_kernel_count() : 0);
     if (n_chem) *n_chem = chem_kernel_count();
     return DPD_OK;
 }
@@ -856,12 +1017,27 @@ extern "C" int dpd_set_params(dpd_handle *h, int32_t r, const dpd_params *p) {
     const RepDev &old = h->rh[r];
     TRY(make_rep(*p, old.b0, old.n, old.c0, R));
     if (R.ncx != old.ncx || R.L != old.L) return fail(DPD_E_ARG, "dpd_set_params cannot change the box size");
+    R.ch0 = old.ch0;
+    R.nch = old.nch;
+    if ((p->chem && p->chem_kind == 1) != (h->params[r].chem && h->params[r].chem_kind == 1) && !h->any_cat)
+        return fail(DPD_E_ARG, "dpd_set_params cannot switch the catalyst chemistry on: create the handle with it");
     CK(cudaStreamSynchronize(h->s));
     h->rh[r] = R;
     h->params[r] = *p;
     CK(cudaMemcpy(h->d_rep + r, &R, sizeof R, cudaMemcpyHostToDevice));
     bool any = false;
-    for (auto &q : h->params) any = any || q.chem;
+    h->any_lipid = false;
+    h->cat_period = 0;
+    for (auto &q : h->params) {
+        any = any || q.chem;
+        h->any_lipid = h->any_lipid || (q.chem && q.chem_kind == 0);
+        if (q.chem && q.chem_kind == 1) {
+            const int64_t a = h->cat_period ? h->cat_period : 1, c = q.n_chem;
+            h->cat_period = a / std::gcd(a, c) * c;
+        }
+    }
+    h->gsteps = graph_len(h, h->gsteps);
+    drop_graphs(h);
     bool stir = false;
     for (auto &q : h->params) stir = stir || q.stir_A != 0.0;
     if (stir && !h->any_stir) {
@@ -1154,7 +1330,7 @@ extern "C" int dpd_force_vjp(dpd_handle *h, int32_t r, int64_t step, const float
     // pack the cotangent into the replica's slots via the state packer's force field
     Bufs u = h->b;
     u.f[h->cur] = A.g;
-    launch_set_dynamics(u, h->cur, R.b0, (int)n, nullptr, nullptr, sx, sy, h->s);
+    launch_set_dynamics(u, h->cur, R.b0, (int)n, nullptr, nullptr, sx, sy, nullptr, nullptr, h->s);
     launch_force_vjp(view_cur(h), step, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
     CK(cudaGetLastError());
     float *outs[4] = {xbar_x, xbar_y, vbar_x, vbar_y};

@@ -1,0 +1,777 @@
+// dpd_catalyst.cu -- the reference's catalyst chemistry (chem_kind 1) on the GPU.
+//
+// One chemistry check of cel/engine/oercel.c:1565-1753, with its semantics:
+//   1. the catalysts (Ka, Kb) in slot order, shuffled with the serial
+//      xoshiro256** generator, are visited one after the other: lipid
+//      synthesis from the nearest N beads (centroid, best of syn_tries
+//      random orientations by overlap energy, steepest-descent relaxation of
+//      the new chain), then replication / mutation onto the next nearest N;
+//   2. decay of lipids, catalysts and N by keyed deviates of (seed, step, gid);
+//   3. the W -> N food supply, uniform or in a vent, with a cap on the N
+//      fraction that keeps a random subset (serial generator) of the candidates.
+// The catalysts of one replica form a chain of dependent decisions (each sees
+// what the earlier ones did, and all draw from one serial stream), so one CTA
+// per replica walks them in order.  Around each catalyst the CTA stages the
+// cells within reach of everything the visit can touch into shared memory and
+// does the neighbour searches, the overlap energies and the relaxation forces
+// there in parallel; one thread makes the decisions.  All geometry is FP64 on
+// the FP32 state, the reference's formulas in its order; sums over beads are
+// block reductions in a fixed order, so a run is deterministic.
+// Candidate sets are those of the reference: beads of the cells in the
+// reference's windows around the cells the reference uses (the cell index of
+// the last sort), then the distance tests.
+#include <algorithm>
+
+#include "dpd_chem.cuh"
+
+#define CAT_TPB 256
+#define CAT_WARPS (CAT_TPB / 32)
+#define CAT_MAXS 2048    // staged beads around one catalyst
+#define CAT_MAXC 1024    // staged cells
+#define CAT_MAXML 16     // beads of a lipid
+#define CAT_MAXNB 256    // N (or W) candidates of one catalyst (the reference keeps 256)
+#define CAT_MAXRN 512    // relaxation neighbours of a new chain (the reference keeps 512)
+#define CAT_MARGIN 0.5   // oercel.c:1348
+
+// event kinds after the lipid chemistry's 0..2
+#define EV_SYN 3
+#define EV_REP 4
+#define EV_MUT 5
+#define EV_DLIP 6
+#define EV_DK 7
+#define EV_DN 8
+#define EV_FEED 9
+
+struct CatSmem {
+    float2 pos[CAT_MAXS];
+    int32_t slot[CAT_MAXS];
+    uint32_t gid[CAT_MAXS];
+    int16_t cx[CAT_MAXS], cy[CAT_MAXS];  // cell of the bead's slot (the last sort)
+    uint8_t type[CAT_MAXS];
+    int32_t wstart[CAT_MAXC + 1];        // staged index of each window cell's first bead
+    int32_t wg[CAT_MAXC];                // global slot of each window cell's first bead
+    int16_t wcx[CAT_MAXC], wcy[CAT_MAXC];
+    int32_t ns, ncw;
+    int32_t nn, nw, nrn;
+    int32_t nb[CAT_MAXNB], nbw[CAT_MAXNB];
+    double nbd[CAT_MAXNB], nbwd[CAT_MAXNB];
+    int32_t sl[CAT_MAXML];               // staged index of each bead of a new chain
+    double px[CAT_MAXML], py[CAT_MAXML];
+    double fx[CAT_MAXML], fy[CAT_MAXML];
+    int32_t rn[CAT_MAXRN];
+    double red[2][CAT_WARPS];
+    int32_t scan[CAT_WARPS];
+    uint64_t rng[4];
+    int32_t go, k, var, ml;
+    int32_t over;                        // a search found more than CAT_MAXNB candidates
+    double xk, yk, ux, uy, cxm, cym;
+};
+
+// ---------------------------------------------------------------- serial generator (oercel.c:143-174)
+
+__device__ __forceinline__ uint64_t xo_rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+__device__ __forceinline__ uint64_t xo_next(uint64_t *s) {
+    const uint64_t r = xo_rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = xo_rotl(s[3], 45);
+    return r;
+}
+__device__ __forceinline__ double xo_unif(uint64_t *s) { return (double)(xo_next(s) >> 11) * 0x1.0p-53; }
+__device__ __forceinline__ long long xo_below(uint64_t *s, long long n) {
+    const long long k = (long long)(xo_unif(s) * (double)n);
+    return k >= n ? n - 1 : k;
+}
+
+// keyed uniform deviates of the parallel decisions (oercel.c:819-826)
+__device__ __forceinline__ uint64_t cat_key(uint64_t seed, long long step, uint64_t salt) {
+    return mix13(seed ^ mix13((uint64_t)step * 0x9e3779b97f4a7c15ULL + salt));
+}
+__device__ __forceinline__ double cat_u01(uint64_t key, uint32_t g) {
+    return (double)(mix13(key ^ ((uint64_t)g * 0xd1b54a32d192ed03ULL)) >> 11) * 0x1.0p-53;
+}
+
+// ---------------------------------------------------------------- FP64 geometry of the reference
+
+__device__ __forceinline__ double dmin(double d, double L) {
+    const double h = 0.5 * L;
+    return d > h ? d - L : (d < -h ? d + L : d);
+}
+__device__ __forceinline__ double dwrap(double v, double L) {
+    if (v < 0.0) {
+        v += L;
+        if (v >= L) v -= L;
+    } else if (v >= L) {
+        v -= L;
+        if (v >= L || v < 0.0) v = fmod(v, L);
+    }
+    return v;
+}
+__device__ __forceinline__ void dcell(const RepDev &R, double x, double y, int &cx, int &cy) {
+    cx = (int)(x * R.icsx);
+    cy = (int)(y * R.icsy);
+    cx = cx >= R.ncx ? R.ncx - 1 : (cx < 0 ? 0 : cx);
+    cy = cy >= R.ncy ? R.ncy - 1 : (cy < 0 ? 0 : cy);
+}
+// is cell column c within [c0 - r, c0 + r] (periodic, n columns, 2r + 1 <= n)
+__device__ __forceinline__ bool in_band(int c, int c0, int r, int n) {
+    int d = (c - c0 + r) % n;
+    d += d < 0 ? n : 0;
+    return d <= 2 * r;
+}
+
+// ---------------------------------------------------------------- block helpers
+
+// sum of v over the CTA, the same order every time; all threads get it
+__device__ __forceinline__ void block_sum2(CatSmem &S, double &a, double &b) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    __syncthreads();
+    if (lane_id() == 0) {
+        S.red[0][threadIdx.x >> 5] = a;
+        S.red[1][threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    a = 0.0;
+    b = 0.0;
+    for (int w = 0; w < CAT_WARPS; w++) {
+        a += S.red[0][w];
+        b += S.red[1][w];
+    }
+}
+
+__device__ __forceinline__ int block_excl_scan(CatSmem &S, int v, int &total) {
+    const int lane = (int)lane_id(), w = (int)threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) S.scan[w] = x;
+    __syncthreads();
+    int before = 0;
+    total = 0;
+    for (int k = 0; k < CAT_WARPS; k++) {
+        before += k < w ? S.scan[k] : 0;
+        total += S.scan[k];
+    }
+    return before + x - v;
+}
+
+// ---------------------------------------------------------------- staging
+
+// Stage the cells within R.cat_E of cell (cx0, cy0) (all columns / rows once
+// if the window covers the box).  Returns false if they do not fit.
+__device__ bool stage(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int cx0, int cy0) {
+    const int E = R.cat_E, ncx = R.ncx, ncy = R.ncy;
+    const int ncol = 2 * E + 1 >= ncx ? ncx : 2 * E + 1, nrow = 2 * E + 1 >= ncy ? ncy : 2 * E + 1;
+    const int c0 = 2 * E + 1 >= ncx ? 0 : cx0 - E, r0 = 2 * E + 1 >= ncy ? 0 : cy0 - E;
+    const int ncw = ncol * nrow;
+    if (ncw > CAT_MAXC) return false;
+    const int32_t *cs = b.cstart + R.c0;
+    int cnt[CAT_MAXC / CAT_TPB];
+    int mine = 0;
+    for (int q = 0; q < CAT_MAXC / CAT_TPB; q++) {
+        const int w = q * CAT_TPB + (int)threadIdx.x;
+        cnt[q] = 0;
+        if (w < ncw) {
+            int gx = c0 + w / nrow, gy = r0 + w % nrow;
+            gx += gx < 0 ? ncx : (gx >= ncx ? -ncx : 0);
+            gy += gy < 0 ? ncy : (gy >= ncy ? -ncy : 0);
+            const int gc = gx * ncy + gy;
+            const int g0 = __ldcg(cs + gc);
+            cnt[q] = __ldcg(cs + gc + 1) - g0;
+            S.wg[w] = g0;
+            S.wcx[w] = (int16_t)gx;
+            S.wcy[w] = (int16_t)gy;
+        }
+        mine += cnt[q];
+    }
+    // window cells of thread t are t, t + TPB, ...: scan them in window order
+    int base = 0;
+    for (int q = 0; q < CAT_MAXC / CAT_TPB; q++) {
+        int tot;
+        const int ex = block_excl_scan(S, cnt[q], tot);
+        const int w = q * CAT_TPB + (int)threadIdx.x;
+        if (w < ncw) S.wstart[w] = base + ex;
+        base += tot;
+    }
+    (void)mine;
+    if (threadIdx.x == 0) {
+        S.wstart[ncw] = base;
+        S.ns = base;
+        S.ncw = ncw;
+    }
+    __syncthreads();
+    const int ns = S.ns;
+    if (ns > CAT_MAXS) return false;
+    for (int i = (int)threadIdx.x; i < ns; i += CAT_TPB) {
+        int lo = 0, hi = ncw;  // last window cell with wstart <= i
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (S.wstart[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        const int g = S.wg[lo] + (i - S.wstart[lo]);
+        S.slot[i] = g;
+        S.pos[i] = __ldcg(b.pos[cur] + g);
+        const uint32_t tg = __ldcg(b.tg[cur] + g);
+        S.type[i] = (uint8_t)(tg >> TYPE_SHIFT);
+        S.gid[i] = tg & GID_MASK;
+        S.cx[i] = S.wcx[lo];
+        S.cy[i] = S.wcy[lo];
+    }
+    __syncthreads();
+    return true;
+}
+
+// beads of type `want` within rcut of (xk, yk) in the reference's cell window
+// (find_type_near, oercel.c:1353-1398), nearest first, ties by lower gid
+__device__ void find_near(CatSmem &S, const RepDev &R, int kslot, double xk, double yk, double rcut, int want,
+                          int32_t *out, double *outd, int32_t *nout) {
+    const double L = (double)R.L, r2c = rcut * rcut;
+    int cx, cy;
+    dcell(R, xk, yk, cx, cy);
+    const int rx = (int)ceil((rcut + CAT_MARGIN) * R.icsx), ry = (int)ceil((rcut + CAT_MARGIN) * R.icsy);
+    if (threadIdx.x == 0) *nout = 0;
+    __syncthreads();
+    for (int i = (int)threadIdx.x; i < S.ns; i += CAT_TPB) {
+        if (S.type[i] != want || S.slot[i] == kslot) continue;
+        if (!in_band(S.cx[i], cx, rx, R.ncx) || !in_band(S.cy[i], cy, ry, R.ncy)) continue;
+        const double dx = dmin((double)S.pos[i].x - xk, L), dy = dmin((double)S.pos[i].y - yk, L);
+        const double d2 = dx * dx + dy * dy;
+        if (d2 < r2c) {
+            const int q = atomicAdd(nout, 1);
+            if (q < CAT_MAXNB) {
+                out[q] = i;
+                outd[q] = d2;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        S.over |= *nout > CAT_MAXNB;  // which ones the atomics kept is arbitrary: reported, not used
+        const int n = min(*nout, CAT_MAXNB);
+        for (int a = 1; a < n; a++) {
+            const int ti = out[a];
+            const double td = outd[a];
+            int c = a - 1;
+            while (c >= 0 && (outd[c] > td || (outd[c] == td && S.gid[out[c]] > S.gid[ti]))) {
+                out[c + 1] = out[c];
+                outd[c + 1] = outd[c];
+                c--;
+            }
+            out[c + 1] = ti;
+            outd[c + 1] = td;
+        }
+        *nout = n;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool in_chain(const CatSmem &S, int i, int ml) {
+    bool r = false;
+    for (int q = 0; q < ml; q++) r |= S.sl[q] == i;
+    return r;
+}
+
+// overlap energy of the would-be straight chain (centre, direction u) with the
+// beads outside it (chain_overlap_energy, oercel.c:1425-1468)
+__device__ double chain_energy(CatSmem &S, const RepDev &R, double cx0, double cy0, double ux, double uy, int ml) {
+    const double L = (double)R.L;
+    const int rx = (int)ceil((1.0 + CAT_MARGIN) * R.icsx), ry = (int)ceil((1.0 + CAT_MARGIN) * R.icsy);
+    double U = 0.0, dummy = 0.0;
+    for (int bb = 0; bb < ml; bb++) {
+        const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
+        const double px = dwrap(cx0 + off * ux, L), py = dwrap(cy0 + off * uy, L);
+        const int tb = bb < R.lip_nH ? 1 : 2;
+        int cx, cy;
+        dcell(R, px, py, cx, cy);
+        for (int i = (int)threadIdx.x; i < S.ns; i += CAT_TPB) {
+            if (!in_band(S.cx[i], cx, rx, R.ncx) || !in_band(S.cy[i], cy, ry, R.ncy) || in_chain(S, i, ml)) continue;
+            const double dx = dmin((double)S.pos[i].x - px, L), dy = dmin((double)S.pos[i].y - py, L);
+            const double r2 = dx * dx + dy * dy;
+            if (r2 >= 1.0) continue;
+            const double w = 1.0 - sqrt(r2);
+            U += 0.5 * (double)R.a[tb * DPD_MAXT + S.type[i]] * w * w;
+        }
+    }
+    block_sum2(S, U, dummy);
+    return U;
+}
+
+// steepest-descent relaxation of the new chain S.px/py against its frozen
+// surroundings (relax_new_chain, oercel.c:1473-1560, the linear template)
+__device__ void relax_chain(CatSmem &S, const RepDev &R, int ml, bool &overflow) {
+    const double L = (double)R.L, cap = 0.05, alpha = 0.002;
+    const double reach = 1.0 + cap * R.syn_relax, reach2 = reach * reach;
+    const int rx = (int)ceil((reach + CAT_MARGIN) * R.icsx), ry = (int)ceil((reach + CAT_MARGIN) * R.icsy);
+    int ccx[CAT_MAXML], ccy[CAT_MAXML];
+    for (int bb = 0; bb < ml; bb++) dcell(R, S.px[bb], S.py[bb], ccx[bb], ccy[bb]);
+    // neighbours within reach of any chain bead, in staged order
+    int base = 0;
+    for (int i0 = 0; i0 < S.ns; i0 += CAT_TPB) {
+        const int i = i0 + (int)threadIdx.x;
+        bool take = false;
+        if (i < S.ns && !in_chain(S, i, ml))
+            for (int bb = 0; bb < ml && !take; bb++) {
+                if (!in_band(S.cx[i], ccx[bb], rx, R.ncx) || !in_band(S.cy[i], ccy[bb], ry, R.ncy)) continue;
+                const double dx = dmin((double)S.pos[i].x - S.px[bb], L), dy = dmin((double)S.pos[i].y - S.py[bb], L);
+                take = dx * dx + dy * dy < reach2;
+            }
+        int tot;
+        const int ex = block_excl_scan(S, take ? 1 : 0, tot);
+        if (take && base + ex < CAT_MAXRN) S.rn[base + ex] = i;
+        base += tot;
+    }
+    if (base > CAT_MAXRN) overflow = true;
+    const int nrn = min(base, CAT_MAXRN);
+    for (int it = 0; it < R.syn_relax; it++) {
+        for (int bb = 0; bb < ml; bb++) {
+            const int ti = bb < R.lip_nH ? 1 : 2;
+            double fx = 0.0, fy = 0.0;
+            for (int q = (int)threadIdx.x; q < nrn; q += CAT_TPB) {
+                const int j = S.rn[q];
+                const double dx = dmin(S.px[bb] - (double)S.pos[j].x, L), dy = dmin(S.py[bb] - (double)S.pos[j].y, L);
+                const double r2 = dx * dx + dy * dy;
+                if (r2 >= 1.0 || r2 < 1e-24) continue;
+                const double r = sqrt(r2);
+                const double f = (double)R.a[ti * DPD_MAXT + S.type[j]] * (1.0 - r) / r;
+                fx += f * dx;
+                fy += f * dy;
+            }
+            block_sum2(S, fx, fy);
+            if (threadIdx.x == 0) {
+                S.fx[bb] = fx;
+                S.fy[bb] = fy;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bx[CAT_MAXML], by[CAT_MAXML], bl[CAT_MAXML];
+            for (int bb = 0; bb < ml - 1; bb++) {
+                bx[bb] = dmin(S.px[bb + 1] - S.px[bb], L);
+                by[bb] = dmin(S.py[bb + 1] - S.py[bb], L);
+                bl[bb] = sqrt(bx[bb] * bx[bb] + by[bb] * by[bb]);
+                const double f = -R.kb_d * (bl[bb] - R.r0_d) / bl[bb];
+                S.fx[bb + 1] += f * bx[bb];
+                S.fy[bb + 1] += f * by[bb];
+                S.fx[bb] -= f * bx[bb];
+                S.fy[bb] -= f * by[bb];
+            }
+            for (int bb = 0; bb < ml - 2 && R.ka_d != 0.0; bb++) {
+                const double ax = bx[bb], ay = by[bb], cxv = bx[bb + 1], cyv = by[bb + 1], la = bl[bb], lc = bl[bb + 1];
+                const double ilac = 1.0 / (la * lc), cs = (ax * cxv + ay * cyv) * ilac, ka = R.ka_d;
+                const double dUax = -ka * (cxv * ilac - cs * ax / (la * la)), dUay = -ka * (cyv * ilac - cs * ay / (la * la));
+                const double dUcx = -ka * (ax * ilac - cs * cxv / (lc * lc)), dUcy = -ka * (ay * ilac - cs * cyv / (lc * lc));
+                S.fx[bb] += dUax;
+                S.fy[bb] += dUay;
+                S.fx[bb + 1] += -dUax + dUcx;
+                S.fy[bb + 1] += -dUay + dUcy;
+                S.fx[bb + 2] -= dUcx;
+                S.fy[bb + 2] -= dUcy;
+            }
+            for (int bb = 0; bb < ml; bb++) {
+                double mx = alpha * S.fx[bb], my = alpha * S.fy[bb];
+                const double m = sqrt(mx * mx + my * my);
+                if (m > cap) {
+                    mx *= cap / m;
+                    my *= cap / m;
+                }
+                S.px[bb] = dwrap(S.px[bb] + mx, L);
+                S.py[bb] = dwrap(S.py[bb] + my, L);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void set_type(const Bufs &b, int cur, int g, int t) {
+    uint32_t *tg = b.tg[cur];
+    tg[g] = ((uint32_t)t << TYPE_SHIFT) | (__ldcg(tg + g) & GID_MASK);
+}
+
+// ---------------------------------------------------------------- 1. the catalysts
+
+// per chunk: how many beads are catalysts (the list is built in slot order)
+__global__ void __launch_bounds__(BEAD_TPB) k_cat_count(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                        const Chunk *__restrict__ ch, int mode) {
+    __shared__ int red[BEAD_TPB / 32];
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    const long long step = *b.step;
+    const int d = c.begin + (int)threadIdx.x;
+    int v = 0, vn = 0;
+    if (cat_due(R, step) && d < c.end) {
+        const uint32_t tg = b.tg[cur][d];
+        const int t = (int)(tg >> TYPE_SHIFT);
+        if (mode == 0) {
+            v = t == 4 || t == 5;
+        } else {
+            const float2 p = b.pos[cur][d];
+            const uint64_t kf = cat_key(R.seed, step, 14);
+            bool in = true;
+            if (R.feed_mode == 2) {
+                const double L = (double)R.L;
+                if (R.vent_kind == 0) {
+                    const double dx = dmin((double)p.x - R.vent_x, L), dy = dmin((double)p.y - R.vent_y, L);
+                    in = dx * dx + dy * dy < R.vent_r * R.vent_r;
+                } else if (R.vent_kind == 1) {
+                    in = fabs(dmin((double)p.x - R.vent_x, L)) < 0.5 * R.vent_w;
+                } else {
+                    in = fabs(dmin((double)p.y - R.vent_y, L)) < 0.5 * R.vent_w;
+                }
+            }
+            v = R.feed_mode != 0 && R.p_feed > 0.0 && t == 0 && in && cat_u01(kf, tg & GID_MASK) < R.p_feed;
+            vn = t == 3;
+        }
+    }
+    v = __reduce_add_sync(0xffffffffu, v);
+    vn = __reduce_add_sync(0xffffffffu, vn);
+    if (lane_id() == 0) red[threadIdx.x >> 5] = v | (vn << 16);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0, sn = 0;
+        for (int w = 0; w < BEAD_TPB / 32; w++) {
+            s += red[w] & 0xFFFF;
+            sn += red[w] >> 16;
+        }
+        b.cat_cnt[blockIdx.x] = s;
+        b.cat_ncnt[blockIdx.x] = sn;
+    }
+}
+
+// per chunk: its candidates written to the replica's list in slot order
+__global__ void __launch_bounds__(BEAD_TPB) k_cat_list(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                       const Chunk *__restrict__ ch, int mode) {
+    __shared__ int ws[BEAD_TPB / 32];
+    __shared__ int pre;
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    const long long step = *b.step;
+    if (!cat_due(R, step) || b.cat_cnt[blockIdx.x] == 0) return;
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int k = R.ch0; k < (int)blockIdx.x; k++) s += b.cat_cnt[k];
+        pre = s;
+    }
+    const int d = c.begin + (int)threadIdx.x;
+    int v = 0;
+    if (d < c.end) {
+        const uint32_t tg = b.tg[cur][d];
+        const int t = (int)(tg >> TYPE_SHIFT);
+        if (mode == 0) {
+            v = t == 4 || t == 5;
+        } else {
+            const float2 p = b.pos[cur][d];
+            const uint64_t kf = cat_key(R.seed, step, 14);
+            bool in = true;
+            if (R.feed_mode == 2) {
+                const double L = (double)R.L;
+                if (R.vent_kind == 0) {
+                    const double dx = dmin((double)p.x - R.vent_x, L), dy = dmin((double)p.y - R.vent_y, L);
+                    in = dx * dx + dy * dy < R.vent_r * R.vent_r;
+                } else if (R.vent_kind == 1) {
+                    in = fabs(dmin((double)p.x - R.vent_x, L)) < 0.5 * R.vent_w;
+                } else {
+                    in = fabs(dmin((double)p.y - R.vent_y, L)) < 0.5 * R.vent_w;
+                }
+            }
+            v = R.feed_mode != 0 && R.p_feed > 0.0 && t == 0 && in && cat_u01(kf, tg & GID_MASK) < R.p_feed;
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, v);
+    if (lane_id() == 0) ws[threadIdx.x >> 5] = __popc(m);
+    __syncthreads();
+    int before = pre;
+    for (int w = 0; w < (int)(threadIdx.x >> 5); w++) before += ws[w];
+    if (v) b.cat_list[R.b0 + before + __popc(m & ((1u << lane_id()) - 1u))] = d;
+}
+
+// the catalysts of one replica, one after the other (oercel.c:1570-1655)
+__global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CatSmem &S = *reinterpret_cast<CatSmem *>(smem_raw);
+    const int rep = (int)blockIdx.x;
+    const RepDev &R = reps[rep];
+    const long long step = *b.step;
+    if (!cat_due(R, step)) return;
+    const int tid = (int)threadIdx.x;
+    const int ml = R.lip_nH + R.lip_nT;
+    const double L = (double)R.L;
+    if (tid == 0) S.over = 0;
+    // the catalysts in slot order
+    int nk = 0;
+    for (int k = tid; k < R.nch; k += CAT_TPB) nk += b.cat_cnt[R.ch0 + k];
+    {
+        double a = (double)nk, z = 0.0;
+        block_sum2(S, a, z);
+        nk = (int)a;
+    }
+    int32_t *list = b.cat_list + R.b0;
+    if (tid == 0) {
+        for (int q = 0; q < 4; q++) S.rng[q] = b.rng[4 * rep + q];
+        for (int a = nk - 1; a > 0; a--) {  // shuffled with the serial generator
+            const int c = (int)xo_below(S.rng, a + 1);
+            const int t = list[a];
+            list[a] = list[c];
+            list[c] = t;
+        }
+    }
+    __syncthreads();
+    bool overflow = false;
+    for (int q = 0; q < nk; q++) {
+        __syncthreads();  // everyone is done with the previous catalyst's shared state
+        if (tid == 0) {
+            const int k = list[q];
+            const int t = (int)(__ldcg(b.tg[cur] + k) >> TYPE_SHIFT);
+            const float2 pk = __ldcg(b.pos[cur] + k);
+            S.k = k;
+            S.go = t == 4 || t == 5;
+            S.var = t == 5;
+            S.xk = pk.x;
+            S.yk = pk.y;
+        }
+        __syncthreads();
+        if (!S.go) continue;
+        const int k = S.k, var = S.var;
+        const double xk = S.xk, yk = S.yk;
+        int cxk, cyk;
+        dcell(R, xk, yk, cxk, cyk);
+        if (!stage(S, b, cur, R, cxk, cyk)) {
+            overflow = true;
+            continue;
+        }
+        find_near(S, R, k, xk, yk, R.r_cat, 3, S.nb, S.nbd, &S.nn);
+        const int nn = S.nn;
+        if (nn < 2) continue;
+        const int nsynN = R.syn_nN > 0 ? R.syn_nN : ml;
+        if (nn >= nsynN && nsynN < ml) find_near(S, R, k, xk, yk, R.r_cat, 0, S.nbw, S.nbwd, &S.nw);
+        else if (tid == 0) S.nw = 0;
+        __syncthreads();
+        const int nw = S.nw;
+        int used = 0;
+        if (tid == 0) S.go = nn >= nsynN && nsynN + nw >= ml && xo_unif(S.rng) < (var ? R.p_syn_b : R.p_syn_a);
+        __syncthreads();
+        if (S.go) {
+            // synthesis: the nsynN nearest N, then the nearest W
+            if (tid == 0) {
+                double cxm = 0, cym = 0;
+                for (int bb = 0; bb < ml; bb++) {
+                    const int i = bb < nsynN ? S.nb[bb] : S.nbw[bb - nsynN];
+                    S.sl[bb] = i;
+                    cxm += dmin((double)S.pos[i].x - xk, L);
+                    cym += dmin((double)S.pos[i].y - yk, L);
+                }
+                S.cxm = xk + cxm / ml;
+                S.cym = yk + cym / ml;
+                S.ux = 1.0;
+                S.uy = 0.0;
+            }
+            __syncthreads();
+            double ubest = INFINITY;
+            for (int tr = 0; tr < R.syn_tries; tr++) {
+                if (tid == 0) {
+                    const double phi = 2.0 * M_PI * xo_unif(S.rng);
+                    S.fx[0] = cos(phi);
+                    S.fy[0] = sin(phi);
+                }
+                __syncthreads();
+                const double cu = S.fx[0], su = S.fy[0];
+                const double U = R.syn_tries > 1 ? chain_energy(S, R, S.cxm, S.cym, cu, su, ml) : 0.0;
+                if (tid == 0 && U < ubest) {
+                    ubest = U;
+                    S.ux = cu;
+                    S.uy = su;
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                double mvx = 0, mvy = 0, mtx = 0, mty = 0;
+                for (int bb = 0; bb < ml; bb++) {
+                    const int g = S.slot[S.sl[bb]];
+                    const float2 vh = __ldcg(b.vh[cur] + g), vt = __ldcg(b.vt[cur] + g);
+                    mvx += vh.x;
+                    mvy += vh.y;
+                    mtx += vt.x;
+                    mty += vt.y;
+                }
+                mvx /= ml;
+                mvy /= ml;
+                mtx /= ml;
+                mty /= ml;
+                for (int bb = 0; bb < ml; bb++) {
+                    const int i = S.sl[bb], g = S.slot[i];
+                    const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
+                    S.px[bb] = dwrap(S.cxm + off * S.ux, L);
+                    S.py[bb] = dwrap(S.cym + off * S.uy, L);
+                    b.vh[cur][g] = make_float2((float)mvx, (float)mvy);
+                    b.vt[cur][g] = make_float2((float)mtx, (float)mty);
+                    const int t = bb < R.lip_nH ? 1 : 2;
+                    set_type(b, cur, g, t);
+                    S.type[i] = (uint8_t)t;
+                    b.link[cur][g] = make_int2(bb > 0 ? S.slot[S.sl[bb - 1]] : -1,
+                                               bb + 1 < ml ? S.slot[S.sl[bb + 1]] : -1);
+                }
+            }
+            __syncthreads();
+            if (R.syn_relax > 0) relax_chain(S, R, ml, overflow);
+            if (tid == 0) {
+                const float Lf = R.L;
+                for (int bb = 0; bb < ml; bb++) {
+                    float x = (float)S.px[bb], y = (float)S.py[bb];
+                    x = x >= Lf ? 0.0f : x;
+                    y = y >= Lf ? 0.0f : y;
+                    b.pos[cur][S.slot[S.sl[bb]]] = make_float2(x, y);
+                }
+                push_event(b, step, EV_SYN, __ldcg(b.tg[cur] + k) & GID_MASK, (uint32_t)var, (float)xk, (float)yk,
+                           rep);
+            }
+            used = nsynN;
+        }
+        // replication onto the next two nearest N, with mutation
+        if (tid == 0 && nn - used >= 2 && xo_unif(S.rng) < (var ? R.p_rep_b : R.p_rep_a)) {
+            int nv = var, mut = 0;
+            if (xo_unif(S.rng) < R.mu) {
+                nv = 1 - var;
+                mut = 1;
+            }
+            const int g1 = S.slot[S.nb[used]], g2 = S.slot[S.nb[used + 1]];
+            set_type(b, cur, g1, nv ? 5 : 4);
+            set_type(b, cur, g2, 0);
+            push_event(b, step, mut ? EV_MUT : EV_REP, __ldcg(b.tg[cur] + g1) & GID_MASK, (uint32_t)nv, (float)xk,
+                       (float)yk, rep);
+        }
+        __syncthreads();
+    }
+    if (tid == 0)
+        for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = S.rng[q];
+    if ((overflow || S.over) && tid == 0) raise_flag(b.status, DPD_F_CATALYST);
+}
+
+// ---------------------------------------------------------------- 2. decay (oercel.c:1658-1694)
+
+__global__ void __launch_bounds__(BEAD_TPB) k_cat_decay(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                        const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    const long long step = *b.step;
+    if (!cat_due(R, step) || !(R.p_ld > 0 || R.p_kd > 0 || R.p_nd > 0)) return;
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const uint32_t tg = b.tg[cur][d];
+    const int t = (int)(tg >> TYPE_SHIFT);
+    const uint32_t g = tg & GID_MASK;
+    const int2 lk = b.link[cur][d];
+    const bool head = lk.x < 0 && lk.y >= 0;
+    const bool lip = head && R.p_ld > 0 && cat_u01(cat_key(R.seed, step, 11), g) < R.p_ld;
+    const bool kat = (t == 4 || t == 5) && R.p_kd > 0 && cat_u01(cat_key(R.seed, step, 12), g) < R.p_kd;
+    const bool nut = t == 3 && R.p_nd > 0 && cat_u01(cat_key(R.seed, step, 13), g) < R.p_nd;
+    const float2 p = b.pos[cur][d];
+    if (lip) {
+        // the whole chain becomes W (no other thread touches its beads)
+        const int ml = R.lip_nH + R.lip_nT;
+        int cc = d, m = 0;
+        while (cc >= 0 && m < ml) {
+            const int nx = b.link[cur][cc].y;
+            set_type(b, cur, cc, 0);
+            b.link[cur][cc] = make_int2(-1, -1);
+            cc = nx;
+            m++;
+        }
+        push_event(b, step, EV_DLIP, g, 0xFFFFFFFFu, p.x, p.y, c.rep);
+    } else if (kat) {
+        set_type(b, cur, d, 0);
+        push_event(b, step, EV_DK, g, t == 5 ? 1u : 0u, p.x, p.y, c.rep);
+    } else if (nut) {
+        set_type(b, cur, d, 0);
+        push_event(b, step, EV_DN, g, 0xFFFFFFFFu, p.x, p.y, c.rep);
+    }
+}
+
+// ---------------------------------------------------------------- 3. food supply (oercel.c:1721-1753)
+
+// candidates in slot order (k_cat_list, mode 1); the cap keeps a random subset
+__global__ void __launch_bounds__(CAT_TPB) k_cat_feed(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    __shared__ double red[2][CAT_WARPS];
+    __shared__ long long keep;
+    const int rep = (int)blockIdx.x;
+    const RepDev &R = reps[rep];
+    const long long step = *b.step;
+    if (!cat_due(R, step) || R.feed_mode == 0 || !(R.p_feed > 0.0)) return;
+    const int tid = (int)threadIdx.x;
+    long long nc = 0, nN = 0;
+    for (int k = tid; k < R.nch; k += CAT_TPB) {
+        nc += b.cat_cnt[R.ch0 + k];
+        nN += b.cat_ncnt[R.ch0 + k];
+    }
+    double a = (double)nc, z = (double)nN;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        z += __shfl_down_sync(0xffffffffu, z, o);
+    }
+    if (lane_id() == 0) {
+        red[0][tid >> 5] = a;
+        red[1][tid >> 5] = z;
+    }
+    __syncthreads();
+    int32_t *list = b.cat_list + R.b0;
+    if (tid == 0) {
+        double sa = 0, sz = 0;
+        for (int w = 0; w < CAT_WARPS; w++) {
+            sa += red[0][w];
+            sz += red[1][w];
+        }
+        const long long ncand = (long long)sa, nNt = (long long)sz;
+        long long add = ncand;
+        if (R.feed_cap > 0.0 && ncand > 0) {
+            long long room = (long long)floor(R.feed_cap * (double)R.n + 1e-9) - nNt;
+            if (room < 0) room = 0;
+            if (add > room) {
+                uint64_t s[4];
+                for (int q = 0; q < 4; q++) s[q] = b.rng[4 * rep + q];
+                for (long long c = 0; c < room; c++) {  // partial Fisher-Yates: a random subset of size room
+                    const long long d = c + xo_below(s, ncand - c);
+                    const int t = list[c];
+                    list[c] = list[d];
+                    list[d] = t;
+                }
+                for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = s[q];
+                add = room;
+            }
+        }
+        keep = add;
+        if (add > 0) push_event(b, step, EV_FEED, (uint32_t)add, 0xFFFFFFFFu, __int_as_float(0x7fc00000),
+                                __int_as_float(0x7fc00000), rep);
+    }
+    __syncthreads();
+    for (long long c = tid; c < keep; c += CAT_TPB) set_type(b, cur, list[c], 3);
+}
+
+// ---------------------------------------------------------------- launch
+
+int catalyst_setup() {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_cat_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CatSmem));
+    return e == cudaSuccess ? 0 : -1;
+}
+
+void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep,
+                     cudaStream_t s) {
+    k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
+    k_cat_list<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
+    k_cat_serial<<<nrep, CAT_TPB, sizeof(CatSmem), s>>>(b, cur, rep);
+    k_cat_decay<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 1);
+    k_cat_list<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 1);
+    k_cat_feed<<<nrep, CAT_TPB, 0, s>>>(b, cur, rep);
+}

@@ -11,8 +11,14 @@
 #define SALT_GROW 2u
 #define SALT_BOND 3u
 
+// the lipid chemistry (chem_kind 0) is due at this step
 __device__ __forceinline__ bool chem_due(const RepDev &R, long long step) {
-    return R.chem && R.n_chem > 0 && (step % R.n_chem) == 0;
+    return R.chem && R.chem_kind == 0 && R.n_chem > 0 && (step % R.n_chem) == 0;
+}
+
+// the reference's catalyst chemistry (chem_kind 1) is due at this step
+__device__ __forceinline__ bool cat_due(const RepDev &R, long long step) {
+    return R.chem && R.chem_kind == 1 && R.n_chem > 0 && (step % R.n_chem) == 0;
 }
 
 __device__ __forceinline__ int type_of(uint32_t tg) { return (int)(tg >> TYPE_SHIFT); }

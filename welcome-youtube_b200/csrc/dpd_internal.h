@@ -36,6 +36,8 @@
 #define DPD_F_BIGCELL 0x10u     // a cell held more beads than the in-register sort handles (slow path used)
 #define DPD_F_TILE 0x20u        // a cell tile held more beads than its shared-memory capacity
 #define DPD_F_FORCE 0x40u       // a single pair or bond force term above the fixed-point range
+#define DPD_F_CATALYST 0x80u    // a catalyst's neighbourhood exceeded the staging capacity
+#define DPD_F_MARGIN 0x100u     // a bead moved >= 0.5 in a step that ends with a catalyst check
 
 struct RepDev {                 // constants of one replica, read by every kernel
     float L, halfL;
@@ -62,6 +64,13 @@ struct RepDev {                 // constants of one replica, read by every kerne
     double gamma_d, dt_d;       // gamma, dt in FP64 (sigma / sqrt(dt) of a step)
     double t_anchor;            // t(step) = t_anchor + (step - step_anchor) dt
     long long step_anchor;
+    // the reference's catalyst chemistry (chem_kind 1, dpd_catalyst.cu)
+    int32_t chem_kind, syn_tries, syn_relax, syn_nN, lip_nH, lip_nT, feed_mode, vent_kind;
+    int32_t ch0, nch;           // this replica's chunks in the bead chunk table
+    int32_t cat_E, pad3;        // half-width in cells of the window staged around a catalyst
+    double r_cat, p_syn_a, p_syn_b, p_rep_a, p_rep_b, mu, p_ld, p_kd, p_nd, p_feed, feed_cap;
+    double vent_x, vent_y, vent_r, vent_w;
+    double kb_d, r0_d, ka_d;    // FP64 bond and angle constants for the relaxation of new chains
 };
 
 // sigma / sqrt(dt) at `step`: constant, or with the temperature cycle
@@ -136,6 +145,10 @@ struct Bufs {
     unsigned long long *obs;    // OBS_N per replica
     unsigned long long *hist;   // pair histogram scratch
     long long *stir;            // per replica: sum of the stirring terms (fixed point) of the current positions
+    uint64_t *rng;              // per replica: the serial xoshiro256** state of the catalyst chemistry (4 words)
+    int32_t *cat_list;          // per bead slot: catalyst / feed candidates of a replica in slot order (at b0)
+    int32_t *cat_cnt;           // per bead chunk: candidates in the chunk
+    int32_t *cat_ncnt;          // per bead chunk: N beads in the chunk (the feed cap)
 };
 
 struct StateView {              // one stored configuration (slot order of its own step)
@@ -167,8 +180,14 @@ inline void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_
     cudaLaunchKernelEx(&cfg, k, (KArgs)args...);
 }
 
+// the catalyst chemistry of one check (dpd_catalyst.cu): catalysts, decay, food supply
+int catalyst_setup();
+void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep,
+                     cudaStream_t s);
+
 // launchers (dpd_kernels.cu, dpd_chem.cu, dpd_adjoint.cu); every launcher enqueues on stream s
-enum PermuteMode { PERM_STEP = 0, PERM_PRIME = 1, PERM_SORT = 2 };
+// PERM_KEEP: the step's update with the slot order kept (source = destination)
+enum PermuteMode { PERM_STEP = 0, PERM_PRIME = 1, PERM_SORT = 2, PERM_KEEP = 3 };
 
 void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool integrate,
                  cudaStream_t s);
@@ -183,6 +202,7 @@ void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
                    bool next_keys, cudaStream_t s);
 void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
+void launch_step_begin(const Bufs &b, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
                         bool virial, cudaStream_t s);
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
@@ -194,7 +214,7 @@ void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, fl
                    float *vty, float *fx, float *fy, uint8_t *type, uint32_t *gid, int32_t *prev, int32_t *next,
                    cudaStream_t s);
 void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
-                         const float *fx, const float *fy, cudaStream_t s);
+                         const float *fx, const float *fy, const float *vtx, const float *vty, cudaStream_t s);
 void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
                         bool next_keys, cudaStream_t s);
 int tile_setup();

@@ -271,6 +271,8 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
 
 // new slot d takes old bead src[d].  PERM_STEP applies the Groot-Warren update
 // on the way (x += dt vh + dt^2 f; vt = vh + (1/2 + lambda) dt f; vh += dt f);
+// PERM_KEEP applies it with every bead kept in its slot (the order and cell
+// index of the last sort stay valid for a catalyst check that follows);
 // PERM_PRIME takes the loaded velocity as the full velocity (vt = v);
 // PERM_SORT moves everything unchanged.
 // ITEMS chunks per CTA, one bead of each per thread; the loads of all items
@@ -280,6 +282,7 @@ template <int MODE, int ITEMS>
 __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                       const Chunk *__restrict__ ch, int nch) {
     pdl_begin();
+    constexpr bool STEP = MODE == PERM_STEP || MODE == PERM_KEEP, KEEP = MODE == PERM_KEEP;
     const int nxt = cur ^ 1;
     const int32_t *__restrict__ src = b.src;
     const int32_t *__restrict__ dest = b.dest;
@@ -304,7 +307,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
         }
     }
 #pragma unroll
-    for (int k = 0; k < ITEMS; k++) i[k] = act[k] ? src[d[k]] : 0;
+    for (int k = 0; k < ITEMS; k++) i[k] = act[k] ? (KEEP ? d[k] : src[d[k]]) : 0;
     float2 p[ITEMS], vh[ITEMS], f[ITEMS];
     uint32_t tg[ITEMS];
     int2 lk[ITEMS];
@@ -320,8 +323,9 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
     int2 nl[ITEMS];
 #pragma unroll
     for (int k = 0; k < ITEMS; k++)
-        if (act[k]) nl[k] = make_int2(lk[k].x >= 0 ? dest[lk[k].x] : -1, lk[k].y >= 0 ? dest[lk[k].y] : -1);
-    const long long step = MODE == PERM_STEP ? *b.step : 0;
+        if (act[k])
+            nl[k] = KEEP ? lk[k] : make_int2(lk[k].x >= 0 ? dest[lk[k].x] : -1, lk[k].y >= 0 ? dest[lk[k].y] : -1);
+    const long long step = STEP ? *b.step : 0;
 #pragma unroll
     for (int k = 0; k < ITEMS; k++) {
         // the replica's sum of stirring terms at the new positions (warp sums, one atomic per warp)
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
             long long st = 0;
             if (act[k]) {
                 float yn = p[k].y;
-                if (MODE == PERM_STEP) yn = advance1(yn, vh[k].y, f[k].y, Rk.dt, Rk.dt2, Rk.L);
+                if (STEP) yn = advance1(yn, vh[k].y, f[k].y, Rk.dt, Rk.dt2, Rk.L);
                 st = stir_fix(Rk, yn);
             }
             st = warp_sum_ll(st);
@@ -339,9 +343,14 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
         if (!act[k]) continue;
         const int dd = d[k];
         float2 q = p[k], v = vh[k];
-        if (MODE == PERM_STEP) {
+        if (STEP) {
             const RepDev &R = reps[rep[k]];
             const float2 ff = f[k];
+            // the catalyst check uses the cell index of the last sort, valid while
+            // every bead moved less than 0.5 (the reference re-sorts otherwise)
+            if (KEEP && cat_due(R, step) &&
+                fmaxf(fabsf(__fmaf_rn(R.dt2, ff.x, R.dt * v.x)), fabsf(__fmaf_rn(R.dt2, ff.y, R.dt * v.y))) >= 0.5f)
+                raise_flag(b.status, DPD_F_MARGIN);
             q = make_float2(advance1(q.x, v.x, ff.x, R.dt, R.dt2, R.L), advance1(q.y, v.y, ff.y, R.dt, R.dt2, R.L));
             if (!(q.x >= 0.0f && q.x < R.L && q.y >= 0.0f && q.y < R.L)) raise_flag(b.status, DPD_F_OUTSIDE);
             b.vt[nxt][dd] = make_float2(__fmaf_rn(R.cvt, ff.x, v.x), __fmaf_rn(R.cvt, ff.y, v.y));
@@ -527,6 +536,15 @@ __global__ void __launch_bounds__(BEAD_TPB) k_halfkick(Bufs b, int cur, const Re
     b.vh[cur][d] = make_float2(__fmaf_rn(-h, f.x, v.x), __fmaf_rn(-h, f.y, v.y));
 }
 
+// the start of a step whose update keeps the slot order (the scan that does
+// this on other steps is not launched): the step counter, and empty chemistry
+// candidate lists
+__global__ void k_step_begin(long long *__restrict__ step, DevStatus *__restrict__ status) {
+    *step += 1;
+    status->n_grow = 0u;
+    status->n_bond = 0u;
+}
+
 // the Groot-Warren update in place, no sort (phase entry point dpd_integrate)
 __global__ void __launch_bounds__(BEAD_TPB) k_integrate(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                         const Chunk *__restrict__ ch) {
@@ -692,17 +710,20 @@ __global__ void k_unpack(Bufs b, int cur, int b0, int n, float *x, float *y, flo
 }
 
 __global__ void k_set_dynamics(Bufs b, int cur, int b0, int n, const float *vhx, const float *vhy, const float *fx,
-                               const float *fy) {
+                               const float *fy, const float *vtx, const float *vty) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int d = b0 + k;
-    float2 v = b.vh[cur][d], f = b.f[cur][d];
+    float2 v = b.vh[cur][d], f = b.f[cur][d], t = b.vt[cur][d];
     if (vhx) v.x = vhx[k];
     if (vhy) v.y = vhy[k];
     if (fx) f.x = fx[k];
     if (fy) f.y = fy[k];
+    if (vtx) t.x = vtx[k];
+    if (vty) t.y = vty[k];
     b.vh[cur][d] = v;
     b.f[cur][d] = f;
+    b.vt[cur][d] = t;
 }
 
 // ---------------------------------------------------------------- launchers
@@ -737,6 +758,7 @@ void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch,
                     cudaStream_t s) {
     const int g4 = (nbch + PERM_ITEMS - 1) / PERM_ITEMS;
     if (mode == PERM_STEP) launch_pdl(k_permute<PERM_STEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch);
+    else if (mode == PERM_KEEP) launch_pdl(k_permute<PERM_KEEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch);
     else if (mode == PERM_PRIME) k_permute<PERM_PRIME, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch);
     else k_permute<PERM_SORT, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch);
 }
@@ -752,6 +774,8 @@ void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
 void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
     k_halfkick<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
 }
+
+void launch_step_begin(const Bufs &b, cudaStream_t s) { k_step_begin<<<1, 1, 0, s>>>(b.step, b.status); }
 
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
     k_integrate<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
@@ -781,6 +805,6 @@ void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, fl
 }
 
 void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
-                         const float *fx, const float *fy, cudaStream_t s) {
-    k_set_dynamics<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, vhx, vhy, fx, fy);
+                         const float *fx, const float *fy, const float *vtx, const float *vty, cudaStream_t s) {
+    k_set_dynamics<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, vhx, vhy, fx, fy, vtx, vty);
 }

@@ -59,7 +59,8 @@ double wrap(double v, double L) {
 
 extern "C" int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, double r0, int32_t nH, int32_t nT,
                              double f_lip, double f_Ka, double f_Kb, double c_N, double *x, double *y, double *vx,
-                             double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads) {
+                             double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads,
+                             uint64_t *rng_out) {
     if (!x || !y || !vx || !vy || !type || N < 2 || nH < 1 || nT < 0 || !(L > 0.0) || !(kT > 0.0))
         return DPD_E_ARG;
     const int ml = nH + nT;
@@ -110,5 +111,7 @@ extern "C" int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, doub
         vx[i] *= sc;
         vy[i] *= sc;
     }
+    if (rng_out)
+        for (int k = 0; k < 4; k++) rng_out[k] = rng.s[k];
     return DPD_OK;
 }

@@ -38,6 +38,12 @@ class DpdParams(C.Structure):
         ("r_grow", C.c_double), ("r_bond", C.c_double), ("warmup", C.c_int64), ("warm_end", C.c_int64),
         ("k_angle", C.c_double), ("stir_A", C.c_double), ("stir_n", C.c_int32), ("pad2", C.c_int32),
         ("kT_amp", C.c_double), ("kT_period", C.c_double), ("t_anchor", C.c_double), ("step_anchor", C.c_int64),
+        ("chem_kind", C.c_int32), ("syn_tries", C.c_int32), ("syn_relax", C.c_int32), ("syn_nN", C.c_int32),
+        ("lip_nH", C.c_int32), ("lip_nT", C.c_int32), ("feed_mode", C.c_int32), ("vent_kind", C.c_int32),
+        ("r_cat", C.c_double), ("p_syn_a", C.c_double), ("p_syn_b", C.c_double), ("p_rep_a", C.c_double),
+        ("p_rep_b", C.c_double), ("mu", C.c_double), ("p_ld", C.c_double), ("p_kd", C.c_double),
+        ("p_nd", C.c_double), ("p_feed", C.c_double), ("feed_cap", C.c_double), ("vent_x", C.c_double),
+        ("vent_y", C.c_double), ("vent_r", C.c_double), ("vent_w", C.c_double),
     ]
 
 
@@ -64,6 +70,7 @@ EXPORTS = [
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
+    "dpd_set_rng", "dpd_get_rng",
 ]
 NGRAD = 66
 
@@ -102,14 +109,16 @@ def load(path: str | None = None):
         "dpd_sizes": ([vp, i32, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
         "dpd_set_state": ([vp, i32] + [fp] * 8, C.c_int),
         "dpd_get_state": ([vp, i32] + [fp] * 12, C.c_int),
-        "dpd_set_dynamics": ([vp, i32] + [fp] * 4, C.c_int),
+        "dpd_set_dynamics": ([vp, i32] + [fp] * 6, C.c_int),
         "dpd_prime": ([vp], C.c_int),
         "dpd_resume": ([vp], C.c_int),
         "dpd_get_step": ([vp, C.POINTER(C.c_int64)], C.c_int),
         "dpd_set_step": ([vp, i64], C.c_int),
         "dpd_step": ([vp, i64], C.c_int),
         "dpd_init_soup": ([dbl, i32, u64, dbl, dbl, i32, i32, dbl, dbl, dbl, dbl] + [fp] * 7
-                          + [C.POINTER(C.c_int32)], C.c_int),
+                          + [C.POINTER(C.c_int32), fp], C.c_int),
+        "dpd_set_rng": ([vp, i32, fp], C.c_int),
+        "dpd_get_rng": ([vp, i32, fp], C.c_int),
         "dpd_build_cells": ([vp], C.c_int),
         "dpd_get_cells": ([vp, i32, fp], C.c_int),
         "dpd_forces": ([vp, i64], C.c_int),

@@ -32,9 +32,9 @@ import numpy as np
 
 from .params import PDEFS, ParamError, Params, param_table, parse_override, read_ini
 
-KINDS = ("grow", "brk", "bond")
+KINDS = ("grow", "brk", "bond", "syn", "rep", "mut", "dlip", "dK", "dN", "feed")
 CKPT_MAGIC = b"OCKB"
-CKPT_VERSION = 1
+CKPT_VERSION = 2
 MAX_CHUNK = 1000   # steps per engine call: bounds the signal latency and the events held on the device
 
 
@@ -95,11 +95,12 @@ def read_snapshot(path):
 CKPT_HEAD = "<iiqddQqdqd"
 
 
-def write_ckpt(path, st, step, time_, L, seed, warm_end, anchor, keep_copy=None):
-    """OCKB v1 (little endian): magic, int32 version, int32 N, int64 step,
+def write_ckpt(path, st, step, time_, L, seed, warm_end, anchor, keep_copy=None, rng=None):
+    """OCKB v2 (little endian): magic, int32 version, int32 N, int64 step,
     float64 time, float64 L, uint64 seed, int64 warm_end, float64 t_anchor,
     int64 step_anchor, float64 dt_anchor (time = t_anchor + (step -
-    step_anchor) dt while dt = dt_anchor, oercel.c:1984-1985), then in slot order
+    step_anchor) dt while dt = dt_anchor, oercel.c:1984-1985), uint64 rng[4]
+    (the serial generator of the catalyst chemistry), then in slot order
     uint32 gid[N], uint8 type[N], int32 prev[N], int32 next[N], float32
     x, y, vhx, vhy, fx, fy [N each], "END!".  Written to a temporary file,
     synced and renamed (oercel.c:1891-1936)."""
@@ -109,6 +110,7 @@ def write_ckpt(path, st, step, time_, L, seed, warm_end, anchor, keep_copy=None)
         f.write(CKPT_MAGIC)
         f.write(struct.pack(CKPT_HEAD, CKPT_VERSION, n, int(step), float(time_), float(L), int(seed) & (2**64 - 1),
                             int(warm_end), float(anchor[0]), int(anchor[1]), float(anchor[2])))
+        f.write(np.ascontiguousarray(np.zeros(4, np.uint64) if rng is None else rng, np.uint64).tobytes())
         for k, dt in (("gid", np.uint32), ("type", np.uint8), ("prev", np.int32), ("next", np.int32)):
             f.write(np.ascontiguousarray(st[k], dt).tobytes())
         for k in ("x", "y", "vhx", "vhy", "fx", "fy"):
@@ -132,10 +134,14 @@ def read_ckpt(path):
     if b[:4] != CKPT_MAGIC:
         raise EngineError(f"{path} is not an oercel_b200 checkpoint")
     ver, n, step, time_, L, seed, warm_end, ta, sa, da = struct.unpack_from(CKPT_HEAD, b, 4)
-    if ver != CKPT_VERSION:
+    if ver not in (1, 2):
         raise EngineError(f"unsupported checkpoint version {ver}")
     o = 4 + struct.calcsize(CKPT_HEAD)
-    out = dict(N=n, step=step, time=time_, L=L, seed=seed, warm_end=warm_end, anchor=(ta, sa, da))
+    out = dict(N=n, step=step, time=time_, L=L, seed=seed, warm_end=warm_end, anchor=(ta, sa, da),
+               rng=np.zeros(4, np.uint64))
+    if ver >= 2:
+        out["rng"] = np.frombuffer(b, np.uint64, 4, o).copy()
+        o += 32
     for k, dt in (("gid", np.uint32), ("type", np.uint8), ("prev", np.int32), ("next", np.int32)):
         a = np.frombuffer(b, dt, n, o)
         out[k] = a.copy()
@@ -156,6 +162,7 @@ def read_reference_ckpt(path, b):
     if ver != 2:
         raise EngineError(f"{path}: reference checkpoint version {ver} (only version 2, linear lipids, is read)")
     step, time_, L, seed = struct.unpack_from("<qddQ", b, 20)
+    rng = np.frombuffer(b, np.uint64, 4, 52).copy()
     o = 20 + 32 + 32 + 8          # rng state, maxbond
     warm_end, ta, sa, da = struct.unpack_from("<qdqd", b, o)
     o += 32 + 8                   # warm_end, anchors, soup seed
@@ -166,14 +173,14 @@ def read_reference_ckpt(path, b):
     nxt = np.frombuffer(b, np.int32, n, o).copy()
     o += 4 * n
     out = dict(N=n, step=step, time=time_, L=L, seed=seed, warm_end=warm_end, anchor=(ta, sa, da), gid=gid,
-               type=typ, next=nxt)
+               type=typ, next=nxt, rng=rng)
     for k, ref in (("x", "x"), ("y", "y"), ("vhx", "vx"), ("vhy", "vy"), ("fx", "fx"), ("fy", "fy")):
         out[k] = np.frombuffer(b, np.float64, n, o).astype(np.float32)
         o += 8 * n
     if b[o:o + 4] != b"END!":
         raise EngineError("checkpoint end marker missing")
-    if np.any(typ >= 4):
-        raise EngineError(f"{path}: catalyst beads (Ka/Kb/Z) are not supported by this engine")
+    if np.any(typ >= 6):
+        raise EngineError(f"{path}: bead type Z is not used (SPEC section 6)")
     Lf = np.float32(L)
     for k in ("x", "y"):
         out[k][out[k] >= Lf] = np.float32(0.0)
@@ -271,6 +278,8 @@ def _run(p, outdir, over):
             e.set_params(0, p, seed=seed, warm_end=warm_end, t_anchor=anchor[0], step_anchor=anchor[1])
             e.set_state(0, ck["x"], ck["y"], ck["vhx"], ck["vhy"], ck["type"], ck["gid"], ck["prev"], ck["next"])
             e.set_dynamics(0, ck["vhx"], ck["vhy"], ck["fx"], ck["fy"])
+            # the serial generator: the checkpoint's, or reseeded for a branch (oercel.c:2177-2180)
+            e.set_rng(0, reseeded_rng(p.seed, ck["step"]) if p.restart_reseed else ck["rng"])
             e.resume()
             e.set_step(ck["step"])
             log(f"restart from {p.restart} at step {ck['step']} (t={ck['time']:.4f}), N={ck['N']}")
@@ -278,6 +287,7 @@ def _run(p, outdir, over):
             e = Engine(p)
             s = soup_for(p)
             e.set_state(0, s["x"], s["y"], s["vx"], s["vy"], s["type"], None, s["prev"], s["next"])
+            e.set_rng(0, s["rng"])
             e.prime()
             warm_end, seed, anchor = p.warmup, p.seed, (0.0, 0, p.dt)
             log(f"init soup: N={len(s['x'])} lipid beads={s['n_lipid_beads']}")
@@ -322,15 +332,17 @@ def _run(p, outdir, over):
         if ef is None:
             e.events()
             return
-        rows = sorted(e.events())
+        rows = sorted(e.events(), key=lambda r: r[:4])
         for (st, k, g, pg, x, y, _) in rows:
-            ef.write(f"{st},{KINDS[k]},{g},{x:.4f},{y:.4f},-\n")
+            var = "-" if k < 3 else {0: "a", 1: "b"}.get(pg, "-")  # the reference's variant column
+            xy = "nan,nan" if math.isnan(x) else f"{x:.4f},{y:.4f}"
+            ef.write(f"{st},{KINDS[k]},{g},{xy},{var}\n")
         ef.flush()
 
     def ckpt(step):
         st = e.state(0)
         keep = os.path.join(outdir, f"ckpt_{step:010d}.bin") if p.ckpt_keep else None
-        write_ckpt(os.path.join(outdir, "ckpt.bin"), st, step, tnow(step), L, seed, warm_end, anchor, keep)
+        write_ckpt(os.path.join(outdir, "ckpt.bin"), st, step, tnow(step), L, seed, warm_end, anchor, keep, e.rng(0))
 
     # max_bond of a stats row is the largest bond length since the previous row
     # (oercel.c:2365-2369); every device read restarts the device maximum
@@ -405,6 +417,24 @@ def _run(p, outdir, over):
     log(f"done at step {step}" + (" (stopped early; restart to continue)" if stopped else ""))
     e.close()
     return 0
+
+
+def _mix13(z):
+    m = (1 << 64) - 1
+    z = ((z ^ (z >> 30)) * 0xbf58476d1ce4e5b9) & m
+    z = ((z ^ (z >> 27)) * 0x94d049bb133111eb) & m
+    return z ^ (z >> 31)
+
+
+def reseeded_rng(seed, step):
+    """rng_seed(seed ^ mix13(step)) of a branching restart (oercel.c:143-174, 2177-2180)"""
+    m = (1 << 64) - 1
+    z = (int(seed) ^ _mix13(int(step) & m)) & m
+    out = []
+    for _ in range(4):
+        z = (z + 0x9e3779b97f4a7c15) & m
+        out.append(_mix13(z))
+    return np.array(out, np.uint64)
 
 
 def main():

@@ -16,7 +16,8 @@ from . import _capi
 from ._capi import DpdEvent, check, load, ptr
 from .params import Params
 
-EVENT_KINDS = ("grow", "brk", "bond")
+# lipid chemistry 0..2, then the reference's catalyst chemistry (its EVNAME, oercel.c:659)
+EVENT_KINDS = ("grow", "brk", "bond", "syn", "rep", "mut", "dlip", "dK", "dN", "feed")
 
 
 def make_soup(L, N, seed, *, kT=1.0, r0=0.5, nH=1, nT=3, f_lip=0.10, f_Ka=0.0, f_Kb=0.0, c_N=0.12):
@@ -28,10 +29,11 @@ def make_soup(L, N, seed, *, kT=1.0, r0=0.5, nH=1, nT=3, f_lip=0.10, f_Ka=0.0, f
     pv = np.empty(N, np.int32)
     nx = np.empty(N, np.int32)
     nl = C.c_int32(0)
+    rng = np.zeros(4, np.uint64)
     check(lib.dpd_init_soup(float(L), int(N), int(seed) & 0xFFFFFFFFFFFFFFFF, float(kT), float(r0), int(nH),
                             int(nT), float(f_lip), float(f_Ka), float(f_Kb), float(c_N), ptr(x), ptr(y), ptr(vx),
-                            ptr(vy), ptr(t), ptr(pv), ptr(nx), C.byref(nl)))
-    return dict(x=x, y=y, vx=vx, vy=vy, type=t, prev=pv, next=nx, n_lipid_beads=nl.value)
+                            ptr(vy), ptr(t), ptr(pv), ptr(nx), C.byref(nl), ptr(rng)))
+    return dict(x=x, y=y, vx=vx, vy=vy, type=t, prev=pv, next=nx, n_lipid_beads=nl.value, rng=rng)
 
 
 def soup_for(p: Params, seed=None):
@@ -97,9 +99,20 @@ class Engine:
         check(self.lib.dpd_set_state(self.h, replica, *[ptr(a) for a in args], ptr(t), ptr(g), ptr(pv), ptr(nx)))
 
     def load_soup(self, replica=0, seed=None):
+        """the reference's soup for this replica's parameters; the serial
+        generator continues from where the soup left it"""
         s = soup_for(self.params[replica], seed)
         self.set_state(replica, s["x"], s["y"], s["vx"], s["vy"], s["type"], None, s["prev"], s["next"])
+        self.set_rng(replica, s["rng"])
         return s
+
+    def set_rng(self, replica, state):
+        check(self.lib.dpd_set_rng(self.h, replica, ptr(np.ascontiguousarray(state, np.uint64))))
+
+    def rng(self, replica=0):
+        r = np.zeros(4, np.uint64)
+        check(self.lib.dpd_get_rng(self.h, replica, ptr(r)))
+        return r
 
     def state(self, replica=0):
         n = self.n_beads[replica]
@@ -114,9 +127,9 @@ class Engine:
                                      ptr(o["gid"]), ptr(o["prev"]), ptr(o["next"])))
         return out
 
-    def set_dynamics(self, replica, vhx=None, vhy=None, fx=None, fy=None):
+    def set_dynamics(self, replica, vhx=None, vhy=None, fx=None, fy=None, vtx=None, vty=None):
         c = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
-        a = [c(vhx), c(vhy), c(fx), c(fy)]
+        a = [c(vhx), c(vhy), c(fx), c(fy), c(vtx), c(vty)]
         check(self.lib.dpd_set_dynamics(self.h, replica, *[ptr(v) for v in a]))
 
     def cells(self, replica=0):

@@ -34,7 +34,7 @@ PDEFS = [
     ("k_head", "float", "0", "branched lipids only (unused)"),
     ("cos_head", "float", "0", "branched lipids only (unused)"),
     ("lip_tie", "int", "0", "branched lipids only (unused)"),
-    ("syn_nN", "int", "0", "catalyst chemistry only (unused)"),
+    ("syn_nN", "int", "0", "N consumed per new lipid (0 = one per lipid bead; the rest are the nearest W)"),
     ("steps", "long", "10000", "run until this step number"),
     ("snap_every", "long", "1000", "snapshot interval (0 = none)"),
     ("stats_every", "long", "100", "stats.csv interval (0 = none)"),
@@ -49,27 +49,27 @@ PDEFS = [
     ("restart", "str", "", "checkpoint to continue from"),
     ("restart_reseed", "int", "0", "1 = branch with this seed on restart"),
     ("walltime", "float", "0", "stop cleanly after this many seconds (0 = off)"),
-    ("chem", "int", "1", "1 = run the chemistry pass"),
+    ("chem", "int", "1", "1 = run the chemistry pass (chem_kind picks which)"),
     ("n_chem", "long", "10", "chemistry interval in steps"),
-    ("r_cat", "float", "1.2", "catalyst chemistry only (unused)"),
-    ("syn_tries", "int", "8", "catalyst chemistry only (unused)"),
-    ("syn_relax", "int", "20", "catalyst chemistry only (unused)"),
-    ("p_syn_a", "float", "0.02", "catalyst chemistry only (unused)"),
-    ("p_syn_b", "float", "0.06", "catalyst chemistry only (unused)"),
-    ("p_rep_a", "float", "0.001", "catalyst chemistry only (unused)"),
-    ("p_rep_b", "float", "0.001", "catalyst chemistry only (unused)"),
-    ("mu", "float", "0.02", "catalyst chemistry only (unused)"),
-    ("p_ld", "float", "2e-4", "catalyst chemistry only (unused)"),
-    ("p_kd", "float", "5e-4", "catalyst chemistry only (unused)"),
-    ("p_nd", "float", "1e-4", "catalyst chemistry only (unused)"),
-    ("feed", "str", "uniform", "catalyst chemistry only (unused)"),
-    ("p_feed", "float", "1e-3", "catalyst chemistry only (unused)"),
-    ("feed_cap", "float", "0.12", "catalyst chemistry only (unused)"),
-    ("vent_shape", "str", "disk", "catalyst chemistry only (unused)"),
-    ("vent_x", "float", "-1", "catalyst chemistry only (unused)"),
-    ("vent_y", "float", "-1", "catalyst chemistry only (unused)"),
-    ("vent_r", "float", "5", "catalyst chemistry only (unused)"),
-    ("vent_w", "float", "4", "catalyst chemistry only (unused)"),
+    ("r_cat", "float", "1.2", "catalyst reaction radius"),
+    ("syn_tries", "int", "8", "new lipid: orientation = lowest overlap energy of this many random ones"),
+    ("syn_relax", "int", "20", "new lipid: steepest-descent iterations moving only its own beads"),
+    ("p_syn_a", "float", "0.02", "lipid synthesis probability per check, Ka"),
+    ("p_syn_b", "float", "0.06", "lipid synthesis probability per check, Kb"),
+    ("p_rep_a", "float", "0.001", "catalyst replication probability per check, Ka"),
+    ("p_rep_b", "float", "0.001", "catalyst replication probability per check, Kb"),
+    ("mu", "float", "0.02", "mutation probability per replication (a <-> b)"),
+    ("p_ld", "float", "2e-4", "lipid decay probability per molecule per check"),
+    ("p_kd", "float", "5e-4", "catalyst decay probability per check"),
+    ("p_nd", "float", "1e-4", "N decay probability per check"),
+    ("feed", "str", "uniform", "food supply W -> N: none, uniform or vent"),
+    ("p_feed", "float", "1e-3", "W -> N probability per check"),
+    ("feed_cap", "float", "0.12", "cap on the N fraction (0 = no cap)"),
+    ("vent_shape", "str", "disk", "vent: disk, vstrip or hstrip"),
+    ("vent_x", "float", "-1", "vent centre x (-1 = L/2)"),
+    ("vent_y", "float", "-1", "vent centre y (-1 = L/2)"),
+    ("vent_r", "float", "5", "vent disk radius"),
+    ("vent_w", "float", "4", "vent strip width"),
     ("events", "int", "1", "1 = write events.csv"),
     ("stir_A", "float", "0", "stirring body force f_x = stir_A sin(2 pi stir_n y / L), net force removed"),
     ("stir_n", "int", "1", "stirring periods"),
@@ -81,6 +81,7 @@ PDEFS = [
     ("c_N", "float", "0.12", "soup: fraction of N (P) beads"),
     # NEW: this engine's noise generator and lipid chemistry
     ("noise", "str", "philox", "NEW pair noise: philox (Philox4x32-10) or mix13 (the reference's hash)"),
+    ("chem_kind", "str", "catalyst", "NEW chemistry of chem = 1: catalyst (the reference's) or lipid (below)"),
     ("p_grow", "float", "1e-3", "NEW P -> T growth probability per check"),
     ("p_break", "float", "1e-5", "NEW H-T bond break probability per check"),
     ("p_bond", "float", "1e-2", "NEW free T + free H bonding probability per check"),
@@ -223,8 +224,16 @@ class Params:
             raise ParamError("noise must be philox or mix13")
         if self.init not in ("soup", "restart"):
             raise ParamError("init must be soup or restart")
-        if self.chem and (self.f_Ka > 0 or self.f_Kb > 0):
-            raise ParamError("the catalyst chemistry (Ka/Kb) is not implemented; set f_Ka = f_Kb = 0")
+        if self.chem_kind not in ("catalyst", "lipid"):
+            raise ParamError("chem_kind must be catalyst or lipid")
+        if self.feed not in ("none", "0", "uniform", "vent"):
+            raise ParamError("feed must be none, uniform or vent")
+        if self.vent_shape not in ("disk", "vstrip", "hstrip"):
+            raise ParamError("vent_shape must be disk, vstrip or hstrip")
+        if not (0 <= self.p_feed <= 1) or not (0 <= self.feed_cap < 1):
+            raise ParamError("p_feed must be in [0, 1] and feed_cap in [0, 1)")
+        if not (0 <= self.syn_nN <= self.lip_nH + self.lip_nT):
+            raise ParamError("syn_nN must be 0..mlen")
         return self
 
     def sigma(self):
@@ -258,6 +267,14 @@ class Params:
         s.stir_A, s.stir_n = float(self.stir_A), int(self.stir_n)
         s.kT_amp, s.kT_period = float(self.kT_amp), float(self.kT_period)
         s.t_anchor, s.step_anchor = float(t_anchor), int(step_anchor)
+        s.chem_kind = 1 if self.chem_kind == "catalyst" else 0
+        s.syn_tries, s.syn_relax, s.syn_nN = max(int(self.syn_tries), 1), int(self.syn_relax), int(self.syn_nN)
+        s.lip_nH, s.lip_nT = int(self.lip_nH), int(self.lip_nT)
+        s.feed_mode = {"none": 0, "0": 0, "uniform": 1, "vent": 2}[self.feed]
+        s.vent_kind = {"disk": 0, "vstrip": 1, "hstrip": 2}[self.vent_shape]
+        for k in ("r_cat", "p_syn_a", "p_syn_b", "p_rep_a", "p_rep_b", "mu", "p_ld", "p_kd", "p_nd", "p_feed",
+                  "feed_cap", "vent_x", "vent_y", "vent_r", "vent_w"):
+            setattr(s, k, float(self[k]))
         return s
 
     def write(self, path, overrides=()):

@@ -22,7 +22,8 @@ from .params import Params
 
 PHYSICS = dict(rho=4, dt=0.02, gamma=4.5, kT=1, k_bond=100, r0=0.5, k_angle=0, lip_nH=1, lip_nT=2, f_lip=0.15,
                f_Ka=0, f_Kb=0, c_N=0.05, warmup=0, a_W_H=25, a_W_T=75, a_H_T=50, a_W_P=25, a_H_P=25, a_P_T=75)
-CHEMISTRY = dict(chem=1, n_chem=1, p_grow=1e-3, p_break=1e-5, p_bond=1e-2, r_grow=1.0, r_bond=0.6, n_t_min=2)
+CHEMISTRY = dict(chem=1, chem_kind="lipid", n_chem=1, p_grow=1e-3, p_break=1e-5, p_bond=1e-2, r_grow=1.0, r_bond=0.6,
+                 n_t_min=2)
 
 
 def config1(seed=0, **kv):
