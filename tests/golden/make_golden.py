@@ -270,6 +270,10 @@ if __name__ == "__main__":
     run_fixture("run_cat_L16_seed5.npz", L=16, seed=5, chem=1, n_chem=4, events=1, nsub=1, k_angle=10, lip_nT=3,
                 f_Ka=0.03, f_Kb=0.02, c_N=0.25, p_syn_a=0.3, p_syn_b=0.3, p_rep_a=0.2, p_rep_b=0.2, mu=0.2,
                 p_ld=0.01, p_kd=0.01, p_nd=0.01, p_feed=0.02, feed_cap=0.27)
+    # a fresh soup without warm-up at dt = 0.05: the reference sorts again before the check of step 5
+    run_fixture("run_cat_resort_L16_seed5.npz", L=16, seed=5, chem=1, n_chem=1, events=1, nsub=1, k_angle=10,
+                lip_nT=3, f_Ka=0.03, f_Kb=0.02, c_N=0.25, p_syn_a=0.3, p_syn_b=0.3, p_rep_a=0.2, p_rep_b=0.2, mu=0.2,
+                p_ld=0.01, p_kd=0.01, p_nd=0.01, p_feed=0.02, feed_cap=0.27, warmup=0, dt=0.05)
     extras_fixture()
     catalyst_fixture("catalyst_L16_seed12.npz", 12, 21)
     catalyst_fixture("catalyst_vent_L16_seed13.npz", 13, 21, syn_nN=2, feed="vent", vent_shape="disk", vent_r=4,

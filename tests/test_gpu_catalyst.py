@@ -104,12 +104,18 @@ def oracle_blocks(p):
     return op, c
 
 
-@pytest.mark.parametrize("feed", ["uniform", "vent"])
-def test_catalyst_check_matches_the_oracle_on_a_large_box(cuda_ok, feed):
-    """a 40 x 40 box (4800 beads, about 240 catalysts) evolved by the engine:
-    one check on the GPU against the oracle's serial restatement on the same
-    sorted state, cell index and generator state"""
-    p = ob.Params(L=40, seed=7, n_chem=10, feed=feed, **CAT)
+# low rates: nearly every catalyst is decided from the counts found before the walk
+LOW = dict(p_syn_a=0.01, p_syn_b=0.03, p_rep_a=0.01, p_rep_b=0.01, mu=0.2, p_ld=0.002, p_kd=0.002, p_nd=0.002,
+           p_feed=0.01)
+
+
+@pytest.mark.parametrize("L, feed, rates", [(40, "uniform", {}), (40, "vent", {}), (100, "uniform", LOW)])
+def test_catalyst_check_matches_the_oracle_on_a_large_box(cuda_ok, L, feed, rates):
+    """a box evolved by the engine (L = 40: 4800 beads, about 240 catalysts, high
+    rates; L = 100: 30000 beads, about 1500 catalysts in two windows of the
+    walk, low rates): one check on the GPU against the oracle's serial
+    restatement on the same sorted state, cell index and generator state"""
+    p = ob.Params(L=L, seed=7, n_chem=10, feed=feed, **dict(CAT, **rates))
     e = ob.Engine(p)
     e.load_soup(0)
     e.prime()
@@ -131,6 +137,7 @@ def test_catalyst_check_matches_the_oracle_on_a_large_box(cuda_ok, feed):
     ref = sorted((ev[1], ev[2], ev[3]) for ev in oev)
     assert got == ref
     assert {k for k, _, _ in ref} >= {3, 4, 6, 7, 8, 9}  # syn, rep, decays and feed all happened
+    assert len([k for k, _, _ in ref if k in (3, 4, 5)]) < (100 if rates else 1000)
 
 
 def test_mixed_chemistries_in_one_batch_equal_solo_runs(cuda_ok):

@@ -30,6 +30,9 @@ G = "run_L10_seed3.npz"
 G_EXTRAS = "run_extras_L10_seed4.npz"
 # the same runs with the reference's catalyst chemistry every 4 steps (events on)
 G_CAT = "run_cat_L16_seed5.npz"
+# catalyst checks every step from a soup without warm-up at dt = 0.05: at step 5 a bead moves more
+# than 0.5 and the reference sorts again before its check
+G_CAT_RESORT = "run_cat_resort_L16_seed5.npz"
 
 
 def fixture_bytes(key, name=G):
@@ -78,6 +81,10 @@ def check_events(got_text, ref_text):
     assert sorted(map(key, rows(got_text))) == sorted(map(key, rows(ref_text)))
 
 
+# positions: FP32 against FP64; at dt = 0.05 the hot start amplifies the rounding differences more
+POS_TOL = {G_CAT_RESORT: 1e-2}
+
+
 def check_snapshot(path, ref_key, name=G):
     ref_path = path + ".ref"
     with open(ref_path, "wb") as f:
@@ -90,10 +97,10 @@ def check_snapshot(path, ref_key, name=G):
     for k in ("x", "y"):
         d = a[k].astype(np.float64) - b[k]
         d -= L * np.round(d / L)
-        assert np.abs(d).max() < 1e-3, k
+        assert np.abs(d).max() < POS_TOL.get(name, 1e-3), k
 
 
-@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT])
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_CAT_RESORT])
 def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
     ini = write_ini(tmp_path, name)
     out = tmp_path / "run"
@@ -106,11 +113,12 @@ def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
     check_snapshot(str(out / "snap_0000000024.bin"), "snap_24", name)
     log = (out / "log.txt").read_text()
     assert log.rstrip().endswith("done at step 24") and "timing:" in log
-    assert "warmup = 8" in (out / "params.ini").read_text()
+    warmup = dict(ln.split(" = ", 1) for ln in fixture_bytes("ini", name).decode().strip().split("\n"))["warmup"]
+    assert f"warmup = {warmup}" in (out / "params.ini").read_text()
     assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] == 24
 
 
-@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT])
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_CAT_RESORT])
 def test_restart_from_a_reference_checkpoint(cuda_ok, tmp_path, name):
     ini = write_ini(tmp_path, name)
     ck = tmp_path / "ref_ckpt.bin"

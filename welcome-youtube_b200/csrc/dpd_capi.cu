@@ -400,8 +400,15 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.cat_list, N));
     TRY(dalloc(h, &b.cat_cnt, (size_t)h->nbch + 1));
     TRY(dalloc(h, &b.cat_ncnt, (size_t)h->nbch + 1));
+    TRY(dalloc(h, &b.resort, (size_t)nrep + 1));
+    TRY(dalloc(h, &b.cat_nk, (size_t)nrep));
+    TRY(dalloc(h, &b.cat_near, N));
+    TRY(dalloc(h, &b.cat_cell, N));
+    TRY(dalloc(h, &b.cat_mark, C));
+    CK(cudaMemset(b.resort, 0, ((size_t)nrep + 1) * sizeof(int32_t)));
     CK(cudaMemset(b.rng, 0, (size_t)4 * nrep * sizeof(uint64_t)));
-    if (h->any_cat && catalyst_setup() != 0) return fail(DPD_E_CUDA, "cannot reserve shared memory for the catalyst kernel");
+    if (h->any_cat && catalyst_setup() != 0)
+        return fail(DPD_E_CUDA, "cannot reserve shared memory for the catalyst kernel");
     CK(cudaMemset(b.stir, 0, (size_t)nrep * sizeof(long long)));
     // staging for set/get state: 8 float + 3 int32 + 1 byte arrays of nmax
     TRY(dalloc(h, &h->stage, (size_t)h->nmax * (8 * 4 + 3 * 4 + 1) + 16 * 256));
@@ -470,9 +477,6 @@ static int check_status(dpd_handle *h) {
     if (st.flags) {
         CK(cudaMemsetAsync(&h->b.status->flags, 0, sizeof(unsigned), h->s));
         CK(cudaStreamSynchronize(h->s));
-        if (st.flags & DPD_F_MARGIN)
-            return fail(DPD_E_STATE, "a bead moved 0.5 or more in the step before a catalyst check, which uses the "
-                                     "previous cell index (the reference sorts again first); reduce dt");
         if (st.flags & DPD_F_CATALYST)
             return fail(DPD_E_STATE, "a catalyst's neighbourhood did not fit the staging area, or a search found "
                                      "more than 256 candidates or 512 relaxation neighbours (too crowded)");
@@ -718,7 +722,7 @@ extern "C" int dpd_chemistry(dpd_handle *h, int64_t step) {
     launch_chem_scan(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
     // the catalyst chemistry as the reference's chemistry(): no sort afterwards
-    if (h->any_cat) launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->s);
+    if (h->any_cat) launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->s);
     CK(cudaGetLastError());
     return check_status(h);
 }
@@ -737,8 +741,9 @@ static bool cat_at(const dpd_handle *h, int64_t s) {
 // reference's order (oercel.c:2337-2349): the update with every bead kept in
 // the slot of the last sort, the check on that order and cell index (the
 // catalysts and the food candidates are taken in slot order), then the sort of
-// the new configuration.  Other steps fuse the update into the sort whose
-// counts the previous force kernel made.
+// the new configuration.  A replica in which a bead moved 0.5 or more is
+// sorted before its check too (launch_resort, no-ops otherwise).  Other steps
+// fuse the update into the sort whose counts the previous force kernel made.
 static void enqueue_step(dpd_handle *h, int64_t s) {
     const bool cat = cat_at(h, s);
     if (!cat) {
@@ -746,14 +751,15 @@ static void enqueue_step(dpd_handle *h, int64_t s) {
         launch_place(h->b, h->d_bch, h->nbch, h->s);
         launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     } else {
-        launch_step_begin(h->b, h->s);
+        launch_step_begin(h->b, h->nrep, h->s);
     }
     clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, cat ? PERM_KEEP : PERM_STEP, h->s);
     h->cur ^= 1;
     if (h->any_lipid) launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
     if (cat) {
-        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->s);
+        launch_resort(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->d_cch, h->ncch, h->C, h->s);
+        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->s);
         enqueue_sort(h, PERM_SORT);
     }
     enqueue_forces(h, true);
@@ -878,7 +884,7 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     int k = 0;
     CK(cudaEventRecord(ev[k++], h->s));
     if (!cat) launch_scan_part(h->b, h->C, true, 1, h->s);
-    else launch_step_begin(h->b, h->s);
+    else launch_step_begin(h->b, h->nrep, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
     if (!cat) launch_scan_part(h->b, h->C, true, 2, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
@@ -896,7 +902,8 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
             CK(cudaEventRecord(ev[k++], h->s));
         }
     if (cat) {
-        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->s);
+        launch_resort(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->d_cch, h->ncch, h->C, h->s);
+        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->s);
         enqueue_sort(h, PERM_SORT);
         CK(cudaEventRecord(ev[k++], h->s));
     }

@@ -32,6 +32,8 @@
 #define CAT_MAXNB 256    // N (or W) candidates of one catalyst (the reference keeps 256)
 #define CAT_MAXRN 512    // relaxation neighbours of a new chain (the reference keeps 512)
 #define CAT_MARGIN 0.5   // oercel.c:1348
+#define CAT_WIN 1024     // catalysts per window of the walk
+#define CAT_SHUF_MAX 49152  // catalysts per replica shuffled in shared memory (more: in place in global memory)
 
 // event kinds after the lipid chemistry's 0..2
 #define EV_SYN 3
@@ -64,6 +66,11 @@ struct CatSmem {
     uint64_t rng[4];
     int32_t go, k, var, ml;
     int32_t over;                        // a search found more than CAT_MAXNB candidates
+    int32_t nchg;                        // beads whose type the current visit changed
+    float2 chg[CAT_MAXML + 2];           // and their positions before the change
+    int32_t wk[CAT_WIN];                 // the window of the walk: catalyst slots,
+    uint32_t wnear[CAT_WIN];             // their packed candidate counts,
+    uint8_t wdirty[CAT_WIN];             // and whether an earlier event changed a bead near them
     double xk, yk, ux, uy, cxm, cym;
 };
 
@@ -496,7 +503,226 @@ __global__ void __launch_bounds__(BEAD_TPB) k_cat_list(Bufs b, int cur, const Re
     if (v) b.cat_list[R.b0 + before + __popc(m & ((1u << lane_id()) - 1u))] = d;
 }
 
-// the catalysts of one replica, one after the other (oercel.c:1570-1655)
+// the catalyst list of one replica shuffled with its serial generator
+// (oercel.c:1571-1580): one warp per replica, the list in shared memory while
+// it fits (CAT_SHUF_MAX entries); also the replica's catalyst count
+__global__ void __launch_bounds__(32) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int shmax) {
+    extern __shared__ int32_t shl[];
+    const int rep = (int)blockIdx.x;
+    const RepDev &R = reps[rep];
+    if (!cat_due(R, *b.step)) return;
+    const int lane = (int)lane_id();
+    int nk = 0;
+    for (int k = lane; k < R.nch; k += 32) nk += b.cat_cnt[R.ch0 + k];
+    nk = __reduce_add_sync(0xffffffffu, nk);
+    int32_t *list = b.cat_list + R.b0;
+    const bool sh = nk <= shmax;
+    int32_t *a = sh ? shl : list;
+    if (sh)
+        for (int i = lane; i < nk; i += 32) shl[i] = list[i];
+    __syncwarp();
+    if (lane == 0) {
+        b.cat_nk[rep] = nk;
+        uint64_t s[4];
+        for (int q = 0; q < 4; q++) s[q] = b.rng[4 * rep + q];
+        for (int i = nk - 1; i > 0; i--) {
+            const int c = (int)xo_below(s, i + 1);
+            const int t = a[i];
+            a[i] = a[c];
+            a[c] = t;
+        }
+        for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = s[q];
+    }
+    __syncwarp();
+    if (sh)
+        for (int i = lane; i < nk; i += 32) list[i] = shl[i];
+}
+
+// per catalyst (thread per list entry): the N and W counts its searches will
+// find (the candidate rules of find_near on the cell index of the last sort),
+// its type and its cell.  Packed: nn | nw << 16 | Kb << 31 (counts saturate).
+__global__ void __launch_bounds__(BEAD_TPB) k_cat_near(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                       const Chunk *__restrict__ ch) {
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    if (!cat_due(R, *b.step)) return;
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end || d - R.b0 >= b.cat_nk[c.rep]) return;
+    const int k = b.cat_list[d];
+    const float2 pk = b.pos[cur][k];
+    const int t = (int)(b.tg[cur][k] >> TYPE_SHIFT);
+    const double L = (double)R.L, xk = pk.x, yk = pk.y, r2c = R.r_cat * R.r_cat;
+    int cx, cy;
+    dcell(R, xk, yk, cx, cy);
+    const int rx = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsx), ry = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsy);
+    const int ncol = 2 * rx + 1 >= R.ncx ? R.ncx : 2 * rx + 1, nrow = 2 * ry + 1 >= R.ncy ? R.ncy : 2 * ry + 1;
+    const int x0 = 2 * rx + 1 >= R.ncx ? 0 : cx - rx, y0 = 2 * ry + 1 >= R.ncy ? 0 : cy - ry;
+    const int32_t *cs = b.cstart + R.c0;
+    int nn = 0, nw = 0;
+    for (int u = 0; u < ncol; u++) {
+        int gx = x0 + u;
+        gx += gx < 0 ? R.ncx : (gx >= R.ncx ? -R.ncx : 0);
+        for (int v = 0; v < nrow; v++) {
+            int gy = y0 + v;
+            gy += gy < 0 ? R.ncy : (gy >= R.ncy ? -R.ncy : 0);
+            const int gc = gx * R.ncy + gy, e = cs[gc + 1];
+            for (int j = cs[gc]; j < e; j++) {
+                const int tj = (int)(b.tg[cur][j] >> TYPE_SHIFT);
+                if ((tj != 3 && tj != 0) || j == k) continue;
+                const float2 pj = b.pos[cur][j];
+                const double dx = dmin((double)pj.x - xk, L), dy = dmin((double)pj.y - yk, L);
+                if (dx * dx + dy * dy < r2c) {
+                    nn += tj == 3;
+                    nw += tj == 0;
+                }
+            }
+        }
+    }
+    b.cat_near[d] = (uint32_t)min(nn, 0x7FFF) | ((uint32_t)min(nw, 0x7FFF) << 16) | (t == 5 ? 0x80000000u : 0u);
+    b.cat_cell[d] = R.c0 + cx * R.ncy + cy;
+}
+
+// One catalyst visit with the whole CTA (oercel.c:1582-1653): staging, the
+// searches, synthesis and replication.  Thread 0 records in S.chg the old
+// positions of the beads whose type it changed.
+__device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int rep, long long step, int k,
+                      bool &overflow) {
+    const int tid = (int)threadIdx.x, ml = R.lip_nH + R.lip_nT;
+    const double L = (double)R.L;
+    if (tid == 0) {
+        const int t = (int)(__ldcg(b.tg[cur] + k) >> TYPE_SHIFT);
+        const float2 pk = __ldcg(b.pos[cur] + k);
+        S.go = t == 4 || t == 5;
+        S.var = t == 5;
+        S.xk = pk.x;
+        S.yk = pk.y;
+        S.nchg = 0;
+    }
+    __syncthreads();
+    if (!S.go) return;
+    const int var = S.var;
+    const double xk = S.xk, yk = S.yk;
+    int cxk, cyk;
+    dcell(R, xk, yk, cxk, cyk);
+    if (!stage(S, b, cur, R, cxk, cyk)) {
+        overflow = true;
+        return;
+    }
+    find_near(S, R, k, xk, yk, R.r_cat, 3, S.nb, S.nbd, &S.nn);
+    const int nn = S.nn;
+    if (nn < 2) return;
+    const int nsynN = R.syn_nN > 0 ? R.syn_nN : ml;
+    if (nn >= nsynN && nsynN < ml) find_near(S, R, k, xk, yk, R.r_cat, 0, S.nbw, S.nbwd, &S.nw);
+    else if (tid == 0) S.nw = 0;
+    __syncthreads();
+    const int nw = S.nw;
+    int used = 0;
+    if (tid == 0) S.go = nn >= nsynN && nsynN + nw >= ml && xo_unif(S.rng) < (var ? R.p_syn_b : R.p_syn_a);
+    __syncthreads();
+    if (S.go) {
+        // synthesis: the nsynN nearest N, then the nearest W
+        if (tid == 0) {
+            double cxm = 0, cym = 0;
+            for (int bb = 0; bb < ml; bb++) {
+                const int i = bb < nsynN ? S.nb[bb] : S.nbw[bb - nsynN];
+                S.sl[bb] = i;
+                S.chg[bb] = S.pos[i];
+                cxm += dmin((double)S.pos[i].x - xk, L);
+                cym += dmin((double)S.pos[i].y - yk, L);
+            }
+            S.nchg = ml;
+            S.cxm = xk + cxm / ml;
+            S.cym = yk + cym / ml;
+            S.ux = 1.0;
+            S.uy = 0.0;
+        }
+        __syncthreads();
+        double ubest = INFINITY;
+        for (int tr = 0; tr < R.syn_tries; tr++) {
+            if (tid == 0) {
+                const double phi = 2.0 * M_PI * xo_unif(S.rng);
+                S.fx[0] = cos(phi);
+                S.fy[0] = sin(phi);
+            }
+            __syncthreads();
+            const double cu = S.fx[0], su = S.fy[0];
+            const double U = R.syn_tries > 1 ? chain_energy(S, R, S.cxm, S.cym, cu, su, ml) : 0.0;
+            if (tid == 0 && U < ubest) {
+                ubest = U;
+                S.ux = cu;
+                S.uy = su;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            double mvx = 0, mvy = 0, mtx = 0, mty = 0;
+            for (int bb = 0; bb < ml; bb++) {
+                const int g = S.slot[S.sl[bb]];
+                const float2 vh = __ldcg(b.vh[cur] + g), vt = __ldcg(b.vt[cur] + g);
+                mvx += vh.x;
+                mvy += vh.y;
+                mtx += vt.x;
+                mty += vt.y;
+            }
+            mvx /= ml;
+            mvy /= ml;
+            mtx /= ml;
+            mty /= ml;
+            for (int bb = 0; bb < ml; bb++) {
+                const int i = S.sl[bb], g = S.slot[i];
+                const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
+                S.px[bb] = dwrap(S.cxm + off * S.ux, L);
+                S.py[bb] = dwrap(S.cym + off * S.uy, L);
+                b.vh[cur][g] = make_float2((float)mvx, (float)mvy);
+                b.vt[cur][g] = make_float2((float)mtx, (float)mty);
+                const int t = bb < R.lip_nH ? 1 : 2;
+                set_type(b, cur, g, t);
+                S.type[i] = (uint8_t)t;
+                b.link[cur][g] = make_int2(bb > 0 ? S.slot[S.sl[bb - 1]] : -1,
+                                           bb + 1 < ml ? S.slot[S.sl[bb + 1]] : -1);
+            }
+        }
+        __syncthreads();
+        if (R.syn_relax > 0) relax_chain(S, R, ml, overflow);
+        if (tid == 0) {
+            const float Lf = R.L;
+            for (int bb = 0; bb < ml; bb++) {
+                float x = (float)S.px[bb], y = (float)S.py[bb];
+                x = x >= Lf ? 0.0f : x;
+                y = y >= Lf ? 0.0f : y;
+                b.pos[cur][S.slot[S.sl[bb]]] = make_float2(x, y);
+            }
+            push_event(b, step, EV_SYN, __ldcg(b.tg[cur] + k) & GID_MASK, (uint32_t)var, (float)xk, (float)yk, rep);
+        }
+        used = nsynN;
+    }
+    // replication onto the next two nearest N, with mutation
+    if (tid == 0 && nn - used >= 2 && xo_unif(S.rng) < (var ? R.p_rep_b : R.p_rep_a)) {
+        int nv = var, mut = 0;
+        if (xo_unif(S.rng) < R.mu) {
+            nv = 1 - var;
+            mut = 1;
+        }
+        const int i1 = S.nb[used], i2 = S.nb[used + 1], g1 = S.slot[i1], g2 = S.slot[i2];
+        set_type(b, cur, g1, nv ? 5 : 4);
+        set_type(b, cur, g2, 0);
+        S.chg[S.nchg++] = S.pos[i1];
+        S.chg[S.nchg++] = S.pos[i2];
+        push_event(b, step, mut ? EV_MUT : EV_REP, __ldcg(b.tg[cur] + g1) & GID_MASK, (uint32_t)nv, (float)xk,
+                   (float)yk, rep);
+    }
+    __syncthreads();
+}
+
+// The catalysts of one replica, one after the other in the shuffled order
+// (oercel.c:1582-1655).  Most visits end without an event: their decisions
+// need only the draws and the two candidate counts, which k_cat_near found
+// before the walk.  So thread 0 walks a window of the list on those counts with
+// a copy of the generator, and hands a catalyst to the whole CTA (visit(), the
+// generator state from before its draws) when its draws give an event, or when
+// an earlier event in this check changed a bead near it (cell marks).  The
+// draws, their order and every decision are those of visiting each catalyst
+// in full.
 __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const RepDev *__restrict__ reps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CatSmem &S = *reinterpret_cast<CatSmem *>(smem_raw);
@@ -505,152 +731,70 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
     const long long step = *b.step;
     if (!cat_due(R, step)) return;
     const int tid = (int)threadIdx.x;
-    const int ml = R.lip_nH + R.lip_nT;
-    const double L = (double)R.L;
-    if (tid == 0) S.over = 0;
-    // the catalysts in slot order
-    int nk = 0;
-    for (int k = tid; k < R.nch; k += CAT_TPB) nk += b.cat_cnt[R.ch0 + k];
-    {
-        double a = (double)nk, z = 0.0;
-        block_sum2(S, a, z);
-        nk = (int)a;
-    }
-    int32_t *list = b.cat_list + R.b0;
+    const int ml = R.lip_nH + R.lip_nT, nsynN = R.syn_nN > 0 ? R.syn_nN : ml;
+    const int nk = b.cat_nk[rep];
+    const int32_t *list = b.cat_list + R.b0;
+    const uint32_t *near = b.cat_near + R.b0;
+    const int32_t *cell = b.cat_cell + R.b0;
+    uint8_t *mark = b.cat_mark;
+    // marking reach: the search radius in cells (a changed bead within r_cat of a
+    // catalyst lies within rx cells of it), plus one
+    const int mx = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsx) + 1, my = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsy) + 1;
+    const int mcol = 2 * mx + 1 >= R.ncx ? R.ncx : 2 * mx + 1, mrow = 2 * my + 1 >= R.ncy ? R.ncy : 2 * my + 1;
     if (tid == 0) {
+        S.over = 0;
         for (int q = 0; q < 4; q++) S.rng[q] = b.rng[4 * rep + q];
-        for (int a = nk - 1; a > 0; a--) {  // shuffled with the serial generator
-            const int c = (int)xo_below(S.rng, a + 1);
-            const int t = list[a];
-            list[a] = list[c];
-            list[c] = t;
-        }
     }
-    __syncthreads();
     bool overflow = false;
-    for (int q = 0; q < nk; q++) {
-        __syncthreads();  // everyone is done with the previous catalyst's shared state
-        if (tid == 0) {
-            const int k = list[q];
-            const int t = (int)(__ldcg(b.tg[cur] + k) >> TYPE_SHIFT);
-            const float2 pk = __ldcg(b.pos[cur] + k);
-            S.k = k;
-            S.go = t == 4 || t == 5;
-            S.var = t == 5;
-            S.xk = pk.x;
-            S.yk = pk.y;
+    for (int w0 = 0; w0 < nk; w0 += CAT_WIN) {
+        const int wn = min(CAT_WIN, nk - w0);
+        __syncthreads();
+        for (int i = tid; i < wn; i += CAT_TPB) {
+            S.wk[i] = list[w0 + i];
+            S.wnear[i] = near[w0 + i];
+            S.wdirty[i] = __ldcg(mark + cell[w0 + i]);
         }
         __syncthreads();
-        if (!S.go) continue;
-        const int k = S.k, var = S.var;
-        const double xk = S.xk, yk = S.yk;
-        int cxk, cyk;
-        dcell(R, xk, yk, cxk, cyk);
-        if (!stage(S, b, cur, R, cxk, cyk)) {
-            overflow = true;
-            continue;
-        }
-        find_near(S, R, k, xk, yk, R.r_cat, 3, S.nb, S.nbd, &S.nn);
-        const int nn = S.nn;
-        if (nn < 2) continue;
-        const int nsynN = R.syn_nN > 0 ? R.syn_nN : ml;
-        if (nn >= nsynN && nsynN < ml) find_near(S, R, k, xk, yk, R.r_cat, 0, S.nbw, S.nbwd, &S.nw);
-        else if (tid == 0) S.nw = 0;
-        __syncthreads();
-        const int nw = S.nw;
-        int used = 0;
-        if (tid == 0) S.go = nn >= nsynN && nsynN + nw >= ml && xo_unif(S.rng) < (var ? R.p_syn_b : R.p_syn_a);
-        __syncthreads();
-        if (S.go) {
-            // synthesis: the nsynN nearest N, then the nearest W
+        int i = 0;
+        while (true) {
             if (tid == 0) {
-                double cxm = 0, cym = 0;
-                for (int bb = 0; bb < ml; bb++) {
-                    const int i = bb < nsynN ? S.nb[bb] : S.nbw[bb - nsynN];
-                    S.sl[bb] = i;
-                    cxm += dmin((double)S.pos[i].x - xk, L);
-                    cym += dmin((double)S.pos[i].y - yk, L);
+                uint64_t r[4] = {S.rng[0], S.rng[1], S.rng[2], S.rng[3]};
+                for (; i < wn; i++) {
+                    const uint32_t v = S.wnear[i];
+                    const int nn = (int)(v & 0x7FFF), nw = (int)((v >> 16) & 0x7FFF), var = (int)(v >> 31);
+                    if (S.wdirty[i] || nn > CAT_MAXNB || nw > CAT_MAXNB) break;
+                    if (nn < 2) continue;
+                    uint64_t t[4] = {r[0], r[1], r[2], r[3]};
+                    const int nwe = nn >= nsynN && nsynN < ml ? nw : 0;
+                    if (nn >= nsynN && nsynN + nwe >= ml && xo_unif(t) < (var ? R.p_syn_b : R.p_syn_a)) break;
+                    if (xo_unif(t) < (var ? R.p_rep_b : R.p_rep_a)) break;
+                    for (int q = 0; q < 4; q++) r[q] = t[q];
                 }
-                S.cxm = xk + cxm / ml;
-                S.cym = yk + cym / ml;
-                S.ux = 1.0;
-                S.uy = 0.0;
+                for (int q = 0; q < 4; q++) S.rng[q] = r[q];
+                S.k = i;
             }
             __syncthreads();
-            double ubest = INFINITY;
-            for (int tr = 0; tr < R.syn_tries; tr++) {
-                if (tid == 0) {
-                    const double phi = 2.0 * M_PI * xo_unif(S.rng);
-                    S.fx[0] = cos(phi);
-                    S.fy[0] = sin(phi);
+            i = S.k;
+            if (i >= wn) break;
+            visit(S, b, cur, R, rep, step, S.wk[i], overflow);
+            // mark the cells around the beads it changed; re-test the rest of the window
+            const int nchg = S.nchg;
+            if (nchg > 0) {
+                for (int e = tid; e < nchg * mcol * mrow; e += CAT_TPB) {
+                    const int c = e / (mcol * mrow), u = (e / mrow) % mcol, w = e % mrow;
+                    int cx, cy;
+                    dcell(R, (double)S.chg[c].x, (double)S.chg[c].y, cx, cy);
+                    int gx = (2 * mx + 1 >= R.ncx ? 0 : cx - mx) + u, gy = (2 * my + 1 >= R.ncy ? 0 : cy - my) + w;
+                    gx += gx < 0 ? R.ncx : (gx >= R.ncx ? -R.ncx : 0);
+                    gy += gy < 0 ? R.ncy : (gy >= R.ncy ? -R.ncy : 0);
+                    mark[R.c0 + gx * R.ncy + gy] = 1;
                 }
                 __syncthreads();
-                const double cu = S.fx[0], su = S.fy[0];
-                const double U = R.syn_tries > 1 ? chain_energy(S, R, S.cxm, S.cym, cu, su, ml) : 0.0;
-                if (tid == 0 && U < ubest) {
-                    ubest = U;
-                    S.ux = cu;
-                    S.uy = su;
-                }
+                for (int j = i + 1 + tid; j < wn; j += CAT_TPB) S.wdirty[j] |= __ldcg(mark + cell[w0 + j]);
                 __syncthreads();
             }
-            if (tid == 0) {
-                double mvx = 0, mvy = 0, mtx = 0, mty = 0;
-                for (int bb = 0; bb < ml; bb++) {
-                    const int g = S.slot[S.sl[bb]];
-                    const float2 vh = __ldcg(b.vh[cur] + g), vt = __ldcg(b.vt[cur] + g);
-                    mvx += vh.x;
-                    mvy += vh.y;
-                    mtx += vt.x;
-                    mty += vt.y;
-                }
-                mvx /= ml;
-                mvy /= ml;
-                mtx /= ml;
-                mty /= ml;
-                for (int bb = 0; bb < ml; bb++) {
-                    const int i = S.sl[bb], g = S.slot[i];
-                    const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
-                    S.px[bb] = dwrap(S.cxm + off * S.ux, L);
-                    S.py[bb] = dwrap(S.cym + off * S.uy, L);
-                    b.vh[cur][g] = make_float2((float)mvx, (float)mvy);
-                    b.vt[cur][g] = make_float2((float)mtx, (float)mty);
-                    const int t = bb < R.lip_nH ? 1 : 2;
-                    set_type(b, cur, g, t);
-                    S.type[i] = (uint8_t)t;
-                    b.link[cur][g] = make_int2(bb > 0 ? S.slot[S.sl[bb - 1]] : -1,
-                                               bb + 1 < ml ? S.slot[S.sl[bb + 1]] : -1);
-                }
-            }
-            __syncthreads();
-            if (R.syn_relax > 0) relax_chain(S, R, ml, overflow);
-            if (tid == 0) {
-                const float Lf = R.L;
-                for (int bb = 0; bb < ml; bb++) {
-                    float x = (float)S.px[bb], y = (float)S.py[bb];
-                    x = x >= Lf ? 0.0f : x;
-                    y = y >= Lf ? 0.0f : y;
-                    b.pos[cur][S.slot[S.sl[bb]]] = make_float2(x, y);
-                }
-                push_event(b, step, EV_SYN, __ldcg(b.tg[cur] + k) & GID_MASK, (uint32_t)var, (float)xk, (float)yk,
-                           rep);
-            }
-            used = nsynN;
+            i++;
         }
-        // replication onto the next two nearest N, with mutation
-        if (tid == 0 && nn - used >= 2 && xo_unif(S.rng) < (var ? R.p_rep_b : R.p_rep_a)) {
-            int nv = var, mut = 0;
-            if (xo_unif(S.rng) < R.mu) {
-                nv = 1 - var;
-                mut = 1;
-            }
-            const int g1 = S.slot[S.nb[used]], g2 = S.slot[S.nb[used + 1]];
-            set_type(b, cur, g1, nv ? 5 : 4);
-            set_type(b, cur, g2, 0);
-            push_event(b, step, mut ? EV_MUT : EV_REP, __ldcg(b.tg[cur] + g1) & GID_MASK, (uint32_t)nv, (float)xk,
-                       (float)yk, rep);
-        }
-        __syncthreads();
     }
     if (tid == 0)
         for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = S.rng[q];
@@ -760,15 +904,22 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_feed(Bufs b, int cur, const Rep
 // ---------------------------------------------------------------- launch
 
 int catalyst_setup() {
-    const cudaError_t e =
+    cudaError_t e =
         cudaFuncSetAttribute(k_cat_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CatSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_cat_shuffle, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 CAT_SHUF_MAX * (int)sizeof(int32_t));
     return e == cudaSuccess ? 0 : -1;
 }
 
-void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep,
-                     cudaStream_t s) {
+void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep, int64_t C,
+                     int nmax, cudaStream_t s) {
+    const int shmax = std::min(nmax, CAT_SHUF_MAX);
     k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
     k_cat_list<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
+    k_cat_shuffle<<<nrep, 32, (size_t)shmax * sizeof(int32_t), s>>>(b, rep, shmax);
+    k_cat_near<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    cudaMemsetAsync(b.cat_mark, 0, (size_t)C, s);
     k_cat_serial<<<nrep, CAT_TPB, sizeof(CatSmem), s>>>(b, cur, rep);
     k_cat_decay<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
     k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 1);

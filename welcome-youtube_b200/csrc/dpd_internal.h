@@ -37,7 +37,6 @@
 #define DPD_F_TILE 0x20u        // a cell tile held more beads than its shared-memory capacity
 #define DPD_F_FORCE 0x40u       // a single pair or bond force term above the fixed-point range
 #define DPD_F_CATALYST 0x80u    // a catalyst's neighbourhood exceeded the staging capacity
-#define DPD_F_MARGIN 0x100u     // a bead moved >= 0.5 in a step that ends with a catalyst check
 
 struct RepDev {                 // constants of one replica, read by every kernel
     float L, halfL;
@@ -149,6 +148,11 @@ struct Bufs {
     int32_t *cat_list;          // per bead slot: catalyst / feed candidates of a replica in slot order (at b0)
     int32_t *cat_cnt;           // per bead chunk: candidates in the chunk
     int32_t *cat_ncnt;          // per bead chunk: N beads in the chunk (the feed cap)
+    int32_t *resort;            // [0]: some replica needs a sort before its catalyst check; [1 + r]: replica r
+    int32_t *cat_nk;            // per replica: catalysts of the current check
+    uint32_t *cat_near;         // per catalyst list entry: packed candidate counts (k_cat_near)
+    int32_t *cat_cell;          // per catalyst list entry: its cell
+    uint8_t *cat_mark;          // per cell: a bead near it changed type in the current check
 };
 
 struct StateView {              // one stored configuration (slot order of its own step)
@@ -182,8 +186,8 @@ inline void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_
 
 // the catalyst chemistry of one check (dpd_catalyst.cu): catalysts, decay, food supply
 int catalyst_setup();
-void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep,
-                     cudaStream_t s);
+void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep, int64_t C,
+                     int nmax, cudaStream_t s);
 
 // launchers (dpd_kernels.cu, dpd_chem.cu, dpd_adjoint.cu); every launcher enqueues on stream s
 // PERM_KEEP: the step's update with the slot order kept (source = destination)
@@ -202,7 +206,9 @@ void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
                    bool next_keys, cudaStream_t s);
 void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
-void launch_step_begin(const Bufs &b, cudaStream_t s);
+void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s);
+void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
+                   int64_t C, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
                         bool virial, cudaStream_t s);
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,

@@ -15,16 +15,21 @@
 
 // ---------------------------------------------------------------- keys (prime / build_cells)
 
-template <bool INTEG>
+// RESORT: the sort before a catalyst check (launch_resort), which runs only if
+// some replica is flagged; the other replicas are keyed by the positions of
+// the previous buffer, the ones their slot order was sorted by, so their
+// order does not change.
+template <bool INTEG, bool RESORT>
 __global__ void __launch_bounds__(BEAD_TPB) k_keys(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                    const Chunk *__restrict__ ch) {
+    if (RESORT && !b.resort[0]) return;
     const Chunk c = ch[blockIdx.x];
     const RepDev &R = reps[c.rep];
     const int i = c.begin + (int)threadIdx.x;
     const bool act = i < c.end;
     uint32_t key = 0;
     if (act) {
-        float2 p = b.pos[cur][i];
+        float2 p = b.pos[RESORT && !b.resort[1 + c.rep] ? cur ^ 1 : cur][i];
         if (INTEG) {
             const float2 v = b.vh[cur][i], f = b.f[cur][i];
             p.x = advance1(p.x, v.x, f.x, R.dt, R.dt2, R.L);
@@ -69,8 +74,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *total) {
 __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count, int32_t *__restrict__ cstart,
                                                     int32_t *__restrict__ bsum, long long C,
                                                     long long *__restrict__ step, int step_inc,
-                                                    DevStatus *__restrict__ status) {
+                                                    DevStatus *__restrict__ status, const int32_t *__restrict__ gate) {
     pdl_begin();
+    if (gate && !*gate) return;
     const long long base = (long long)blockIdx.x * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
     int v[SCAN_PER_THREAD];
     int s = 0;
@@ -118,8 +124,10 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count
 
 // add the totals of all earlier blocks; the last block writes cstart[C]
 __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart, uint32_t *__restrict__ fill,
-                                                    const int32_t *__restrict__ bsum, long long C, int nblocks) {
+                                                    const int32_t *__restrict__ bsum, long long C, int nblocks,
+                                                    const int32_t *__restrict__ gate) {
     pdl_begin();
+    if (gate && !*gate) return;
     __shared__ int red[SCAN_TPB / 32];
     int part = 0;
     for (int k = (int)threadIdx.x; k < (int)blockIdx.x; k += SCAN_TPB) part += bsum[k];
@@ -159,8 +167,10 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart
 #endif
 
 // PLACE_ITEMS chunks per CTA: all keys are loaded before the first atomic
-__global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch, int nch) {
+__global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch, int nch,
+                                                    const int32_t *__restrict__ gate) {
     pdl_begin();
+    if (gate && !*gate) return;
     const unsigned lane = lane_id();
     uint32_t key[PLACE_ITEMS];
     int idx[PLACE_ITEMS];
@@ -256,8 +266,10 @@ __device__ __forceinline__ void cellfix_one(const Bufs &b, int cell) {
     }
 }
 
-__global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch) {
+__global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch,
+                                                      const int32_t *__restrict__ gate) {
     pdl_begin();
+    if (gate && !*gate) return;
     const Chunk c = ch[blockIdx.x];
     const int cell = c.begin + (int)threadIdx.x;
     if (cell < c.end) cellfix_one(b, cell);
@@ -280,8 +292,10 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
 // has several independent gathers in flight.
 template <int MODE, int ITEMS>
 __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                      const Chunk *__restrict__ ch, int nch) {
+                                                      const Chunk *__restrict__ ch, int nch,
+                                                      const int32_t *__restrict__ gate) {
     pdl_begin();
+    if (gate && !*gate) return;
     constexpr bool STEP = MODE == PERM_STEP || MODE == PERM_KEEP, KEEP = MODE == PERM_KEEP;
     const int nxt = cur ^ 1;
     const int32_t *__restrict__ src = b.src;
@@ -346,11 +360,13 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
         if (STEP) {
             const RepDev &R = reps[rep[k]];
             const float2 ff = f[k];
-            // the catalyst check uses the cell index of the last sort, valid while
-            // every bead moved less than 0.5 (the reference re-sorts otherwise)
+            // the catalyst check uses the cell index of the last sort while every
+            // bead moved less than 0.5; otherwise its replica is sorted first
             if (KEEP && cat_due(R, step) &&
-                fmaxf(fabsf(__fmaf_rn(R.dt2, ff.x, R.dt * v.x)), fabsf(__fmaf_rn(R.dt2, ff.y, R.dt * v.y))) >= 0.5f)
-                raise_flag(b.status, DPD_F_MARGIN);
+                fmaxf(fabsf(__fmaf_rn(R.dt2, ff.x, R.dt * v.x)), fabsf(__fmaf_rn(R.dt2, ff.y, R.dt * v.y))) >= 0.5f) {
+                b.resort[0] = 1;
+                b.resort[1 + rep[k]] = 1;
+            }
             q = make_float2(advance1(q.x, v.x, ff.x, R.dt, R.dt2, R.L), advance1(q.y, v.y, ff.y, R.dt, R.dt2, R.L));
             if (!(q.x >= 0.0f && q.x < R.L && q.y >= 0.0f && q.y < R.L)) raise_flag(b.status, DPD_F_OUTSIDE);
             b.vt[nxt][dd] = make_float2(__fmaf_rn(R.cvt, ff.x, v.x), __fmaf_rn(R.cvt, ff.y, v.y));
@@ -539,10 +555,30 @@ __global__ void __launch_bounds__(BEAD_TPB) k_halfkick(Bufs b, int cur, const Re
 // the start of a step whose update keeps the slot order (the scan that does
 // this on other steps is not launched): the step counter, and empty chemistry
 // candidate lists
-__global__ void k_step_begin(long long *__restrict__ step, DevStatus *__restrict__ status) {
-    *step += 1;
-    status->n_grow = 0u;
-    status->n_bond = 0u;
+__global__ void k_step_begin(long long *__restrict__ step, DevStatus *__restrict__ status,
+                             int32_t *__restrict__ resort, int nrep) {
+    if (threadIdx.x == 0) {
+        *step += 1;
+        status->n_grow = 0u;
+        status->n_bond = 0u;
+    }
+    for (int r = (int)threadIdx.x; r <= nrep; r += (int)blockDim.x) resort[r] = 0;
+}
+
+// the sorted copy (next buffer) of a sort before a catalyst check back into the
+// current buffer, so that the buffer parity of the step does not depend on it
+__global__ void __launch_bounds__(BEAD_TPB) k_copy_back(Bufs b, int cur, const Chunk *__restrict__ ch) {
+    if (!b.resort[0]) return;
+    const Chunk c = ch[blockIdx.x];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const int n = cur ^ 1;
+    b.pos[cur][d] = b.pos[n][d];
+    b.vh[cur][d] = b.vh[n][d];
+    b.vt[cur][d] = b.vt[n][d];
+    b.f[cur][d] = b.f[n][d];
+    b.tg[cur][d] = b.tg[n][d];
+    b.link[cur][d] = b.link[n][d];
 }
 
 // the Groot-Warren update in place, no sort (phase entry point dpd_integrate)
@@ -730,15 +766,20 @@ __global__ void k_set_dynamics(Bufs b, int cur, int b0, int n, const float *vhx,
 
 void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool integrate,
                  cudaStream_t s) {
-    if (integrate) k_keys<true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
-    else k_keys<false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    if (integrate) k_keys<true, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    else k_keys<false, false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+}
+
+static void scan_part(const Bufs &b, int64_t C, bool step_inc, int part, const int32_t *gate, cudaStream_t s) {
+    const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
+    if (part == 1)
+        launch_pdl(k_scan1, nb, SCAN_TPB, 0, s, b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0,
+                   b.status, gate);
+    else launch_pdl(k_scan2, nb, SCAN_TPB, 0, s, b.cstart, b.fill, b.bsum, (long long)C, nb, gate);
 }
 
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s) {
-    const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
-    if (part == 1)
-        launch_pdl(k_scan1, nb, SCAN_TPB, 0, s, b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0, b.status);
-    else launch_pdl(k_scan2, nb, SCAN_TPB, 0, s, b.cstart, b.fill, b.bsum, (long long)C, nb);
+    scan_part(b, C, step_inc, part, nullptr, s);
 }
 
 void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
@@ -747,20 +788,41 @@ void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
 }
 
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s) {
-    launch_pdl(k_place, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch);
+    launch_pdl(k_place, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch,
+               (const int32_t *)nullptr);
 }
 
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s) {
-    launch_pdl(k_cellfix, ncch, CELL_TPB, 0, s, b, cch);
+    launch_pdl(k_cellfix, ncch, CELL_TPB, 0, s, b, cch, (const int32_t *)nullptr);
 }
 
 void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
                     cudaStream_t s) {
     const int g4 = (nbch + PERM_ITEMS - 1) / PERM_ITEMS;
-    if (mode == PERM_STEP) launch_pdl(k_permute<PERM_STEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch);
-    else if (mode == PERM_KEEP) launch_pdl(k_permute<PERM_KEEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch);
-    else if (mode == PERM_PRIME) k_permute<PERM_PRIME, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch);
-    else k_permute<PERM_SORT, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch);
+    const int32_t *no = nullptr;
+    if (mode == PERM_STEP) launch_pdl(k_permute<PERM_STEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch, no);
+    else if (mode == PERM_KEEP)
+        launch_pdl(k_permute<PERM_KEEP, PERM_ITEMS>, g4, BEAD_TPB, 0, s, b, cur, rep, bch, nbch, no);
+    else if (mode == PERM_PRIME) k_permute<PERM_PRIME, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch, no);
+    else k_permute<PERM_SORT, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch, no);
+}
+
+// The reference sorts again before a catalyst check when a bead moved 0.5 or
+// more in the step (oercel.c:2339-2344).  The kernels below run as no-ops
+// unless k_permute<PERM_KEEP> flagged a replica; then the flagged replicas are
+// sorted by their new positions (the others keep their order), and the sorted
+// state is copied back so the host's buffer parity stays the same.
+void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
+                   int64_t C, cudaStream_t s) {
+    const int32_t *gate = b.resort;
+    cudaMemsetAsync(b.count, 0, (size_t)(C + 4) * sizeof(uint32_t), s);
+    k_keys<false, true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    scan_part(b, C, false, 1, gate, s);
+    scan_part(b, C, false, 2, gate, s);
+    launch_pdl(k_place, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch, gate);
+    launch_pdl(k_cellfix, ncch, CELL_TPB, 0, s, b, cch, gate);
+    k_permute<PERM_SORT, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch, gate);
+    k_copy_back<<<nbch, BEAD_TPB, 0, s>>>(b, cur, bch);
 }
 
 void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, bool pair, bool bond,
@@ -775,7 +837,9 @@ void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch
     k_halfkick<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
 }
 
-void launch_step_begin(const Bufs &b, cudaStream_t s) { k_step_begin<<<1, 1, 0, s>>>(b.step, b.status); }
+void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s) {
+    k_step_begin<<<1, 128, 0, s>>>(b.step, b.status, b.resort, nrep);
+}
 
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s) {
     k_integrate<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
