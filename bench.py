@@ -154,8 +154,9 @@ def reference_binary():
     return path if os.path.exists(path) else None, ("avx512" if avx512 else "avx2")
 
 
-def run_reference(p, steps, threads):
-    """the reference CLI on the physics of p; returns (ms/step of the step phases, timing dict)"""
+def run_reference(p, steps, threads, ini_text=None):
+    """the reference CLI on the physics of p (or on ini_text); returns (ms/step of
+    the step phases, timing dict)"""
     from oercel_b200.workloads import reference_ini
     exe, isa = reference_binary()
     if exe is None:
@@ -163,7 +164,7 @@ def run_reference(p, steps, threads):
     with tempfile.TemporaryDirectory() as td:
         ini = os.path.join(td, "params.ini")
         with open(ini, "w") as f:
-            f.write(reference_ini(p, steps, threads))
+            f.write(ini_text if ini_text is not None else reference_ini(p, steps, threads))
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         r = subprocess.run([exe, ini, os.path.join(td, "out")], capture_output=True, text=True, env=env,
                            timeout=1800)
@@ -280,6 +281,53 @@ def batched_rates(torch, steps=64):
     return {"value": total * steps / (t_batched / 1000.0), "one_at_a_time": total * steps / (t_single / 1000.0),
             "ratio": t_single / t_batched, "replicas": len(reps), "beads": total, "steps": steps,
             "timing": "batched: CUDA events on the engine stream; one at a time: host clock around all engines"}
+
+
+def catalyst_rates(torch, steps=200, ref_steps=40):
+    """the reference's catalyst chemistry on its big-soup workload (786,432 beads,
+    a check every 10 steps): bead-steps/s of whole steps, checks included, the
+    check alone, and the reference executable on the same ini"""
+    import numpy as np
+
+    from oercel_b200 import Engine, workloads
+    p = workloads.catalyst_plan()
+    e = Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(40)  # past the hot start of the unrelaxed soup
+    while (e.step_no + 1) % p.n_chem:
+        e.step(1)
+    check_ms = float(e.profile_step()[-2])  # the catalyst entry of a step with a check
+    while e.step_no % p.n_chem:
+        e.step(1)
+    e.step(p.n_chem)  # capture the graphs
+    e.events()
+    stream = torch.cuda.ExternalStream(e.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    e.step_async(steps)
+    b.record(stream)
+    stream.synchronize()
+    e.sync()
+    ms = a.elapsed_time(b) / steps
+    nev = len(e.events())
+    nb = p.n_beads()
+    ncat = int(np.isin(e.state()["type"], (4, 5)).sum())
+    e.close()
+    threads = os.cpu_count() or 1
+    ref_ms, t = run_reference(p, ref_steps, threads, workloads.catalyst_plan_ini(p.seed, ref_steps, threads))
+    out = {"value": nb * 1000.0 / ms, "unit": UNIT, "ms_per_step": ms, "check_ms": check_ms, "steps": steps,
+           "events": nev, "beads": nb, "catalysts": ncat,
+           "workload": "L=512 soup, linear H-T-T-T lipids, catalyst chemistry with the big-soup rates of the "
+                       "reference's experiment plan, a check every 10 steps (CUDA events, graphs)"}
+    if ref_ms is not None:
+        out["reference"] = {"value": nb * 1000.0 / ref_ms, "ms_per_step": ref_ms, "cores": threads,
+                            "chem_ms_per_step": t["chem"],
+                            "sample": f"{ref_steps} steps of the same ini, reference CLI ({t['isa']} build)"}
+    else:
+        out["reference"] = {"value": None, "error": t.get("error", "")}
+    return out
 
 
 def adjoint_ratio(torch, window=200, ckpt=20, last=50, reps=3):
@@ -414,6 +462,7 @@ def ours(args, rank, local_rank, ws):
         if not args.skip_batched and ws == 1:
             res["batched"] = batched_rates(torch)
             res["adjoint"] = adjoint_ratio(torch)
+            res["catalyst"] = catalyst_rates(torch)
         if ws == 1 and not args.skip_cpu:
             threads = os.cpu_count() or 1
             step_ms, t = run_reference(p, args.cpu_steps, threads)

@@ -117,7 +117,41 @@ typedef struct {
     double p_ld, p_kd, p_nd;   /* decay probability per check: lipid, catalyst, N */
     double p_feed, feed_cap;   /* W -> N probability per check, cap on the N fraction (0 = none) */
     double vent_x, vent_y, vent_r, vent_w; /* vent region */
+    /* lipid shape (lip_arch, oercel.c:436-576): 0 linear (lip_nH heads, lip_nT
+     * tails), 1 pi (two bonded heads, a tail of lip_nT on each), 2 y (one head,
+     * two tails of lip_nT), 3 bola (head pair, two tails of lip_nT, a third head
+     * joining them); branched shapes take their bonds and angles from
+     * dpd_lipid_template */
+    int32_t lip_arch;
+    int32_t lip_tie;           /* pi / y / bola: rungs between the two tails (lip_tie) */
+    double r0_head;            /* pi / bola: head-head rest length (r0_head) */
+    double k_head, cos_head;   /* junction angle term U = k_head (cos - cos_head)^2 (k_head, cos_head) */
 } dpd_params;
+
+/* The molecule template of a lipid shape: bead types by position (heads
+ * first), bonds (position pairs with rest lengths, spring k_bond), angle terms
+ * (position triplets, j the middle bead; kind 0: U = K (1 - cos), kind 1:
+ * U = K (cos - c0)^2), the template coordinates (centroid at 0, long axis
+ * along +x) used to place a newly synthesised lipid, and the offsets from
+ * bead 0 used by the soup.  The beads of a molecule are linked prev/next in
+ * position order.  Same numbers, same order as the reference's mol_build
+ * (oercel.c:478-576). */
+#define DPD_MAXML 16
+#define DPD_MAXMB (2 * DPD_MAXML)
+typedef struct {
+    int32_t arch, mlen, nH, nb, na, pad;
+    int32_t bi[DPD_MAXMB], bj[DPD_MAXMB];
+    double br0[DPD_MAXMB];
+    int32_t ai[DPD_MAXMB], aj[DPD_MAXMB], ak[DPD_MAXMB], akind[DPD_MAXMB];
+    double aK[DPD_MAXMB], ac0[DPD_MAXMB];
+    double px[DPD_MAXML], py[DPD_MAXML];
+    double ix[DPD_MAXML], iy[DPD_MAXML];
+} dpd_template;
+
+/* The template of p's lipid shape (lip_arch, lip_nH, lip_nT, lip_tie, r0,
+ * r0_head, k_angle, k_head, cos_head).  No counterpart call in the
+ * reference, which builds it into a global (mol_build). */
+DPD_API int dpd_lipid_template(const dpd_params *p, dpd_template *t);
 
 /* One chemistry event, the reference's events.csv row (oercel.c:788-798)
  * with the partner bead added.  kind: 0 grow, 1 brk, 2 bond. */
@@ -216,16 +250,18 @@ DPD_API int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *n_o
 /* The reference's random soup (init_soup + set_velocities,
  * cel/engine/oercel.c:1757-1814) with the same xoshiro256** draws, on the
  * host: linear lipids of nH heads + nT tails at spacing r0 from uniform head
- * positions, then nKa = round(f_Ka N) beads of type 4, nKb of type 5,
- * round(c_N N) of type 3 (P), the rest W; Gaussian velocities with the mean
- * removed, rescaled to exactly kT.  HOST arrays of N entries in gid order.
- * *n_lipid_beads receives the number of beads placed in lipids; rng_out
- * (4 words, may be NULL) the generator state after the soup, from which the
- * reference's serial chemistry continues. */
+ * positions (or, with a template of a branched shape, its soup offsets turned
+ * by a random angle, its mlen beads and nH heads), then nKa = round(f_Ka N)
+ * beads of type 4, nKb of type 5, round(c_N N) of type 3 (P), the rest W;
+ * Gaussian velocities with the mean removed, rescaled to exactly kT.  HOST
+ * arrays of N entries in gid order.  *n_lipid_beads receives the number of
+ * beads placed in lipids; rng_out (4 words, may be NULL) the generator state
+ * after the soup, from which the reference's serial chemistry continues.
+ * mol may be NULL (linear lipids from nH, nT, r0). */
 DPD_API int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, double r0, int32_t nH, int32_t nT,
                           double f_lip, double f_Ka, double f_Kb, double c_N, double *x, double *y, double *vx,
                           double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads,
-                          uint64_t *rng_out);
+                          uint64_t *rng_out, const dpd_template *mol);
 
 /* The serial xoshiro256** state of the catalyst chemistry of replica r
  * (4 words; the reference's Sys.rng, checkpointed with the state). */

@@ -281,6 +281,56 @@ void ora_bond_forces(const ora_params *P, int32_t n, const float *x, const float
     *maxbond = mb;
 }
 
+/* Bonded forces of branched lipids from a molecule template (mol_forces,
+ * oercel.c:1221-1257): for every molecule (a bead with no prev and a next; its
+ * beads follow next in template order) each template bond (position pair,
+ * rest length, spring k_bond) and angle term (kind 0: U = K (1 - cos), kind 1:
+ * U = K (cos - c0)^2) is added to the beads it joins. */
+void ora_mol_forces(const ora_params *P, const ora_mol *M, int32_t n, const float *x, const float *y,
+                    const int32_t *next, double *fx, double *fy, double *maxbond) {
+    const double L = P->L;
+    double mb = *maxbond;
+    char *haspv = (char *)calloc((size_t)(n > 0 ? n : 1), 1);
+    for (int i = 0; i < n; i++)
+        if (next[i] >= 0) haspv[next[i]] = 1;
+    for (int h = 0; h < n; h++) {
+        if (haspv[h] || next[h] < 0) continue;
+        int sl[ORA_MAXML], m = 0;
+        for (int d = h; d >= 0 && m < M->mlen; d = next[d]) sl[m++] = d;
+        if (m != M->mlen) continue;
+        for (int q = 0; q < M->nb; q++) {
+            const int i = sl[M->bi[q]], j = sl[M->bj[q]];
+            const double dx = minimg((double)x[j] - (double)x[i], L), dy = minimg((double)y[j] - (double)y[i], L);
+            const double r = sqrt(dx * dx + dy * dy);
+            if (r > mb) mb = r;
+            const double f = -P->k_bond * (r - M->br0[q]) / r; /* force on j along (dx, dy) */
+            fx[j] += f * dx;
+            fy[j] += f * dy;
+            fx[i] -= f * dx;
+            fy[i] -= f * dy;
+        }
+        for (int q = 0; q < M->na; q++) {
+            const int i = sl[M->ai[q]], j = sl[M->aj[q]], k = sl[M->ak[q]];
+            const double ax = minimg((double)x[j] - (double)x[i], L), ay = minimg((double)y[j] - (double)y[i], L);
+            const double cx = minimg((double)x[k] - (double)x[j], L), cy = minimg((double)y[k] - (double)y[j], L);
+            const double la = sqrt(ax * ax + ay * ay), lc = sqrt(cx * cx + cy * cy);
+            const double ilac = 1.0 / (la * lc);
+            const double cs = (ax * cx + ay * cy) * ilac;
+            const double g = M->akind[q] == 0 ? -M->aK[q] : 2.0 * M->aK[q] * (cs - M->ac0[q]); /* dU/dcos */
+            const double dUax = g * (cx * ilac - cs * ax / (la * la)), dUay = g * (cy * ilac - cs * ay / (la * la));
+            const double dUcx = g * (ax * ilac - cs * cx / (lc * lc)), dUcy = g * (ay * ilac - cs * cy / (lc * lc));
+            fx[i] += dUax;
+            fy[i] += dUay;
+            fx[j] += -dUax + dUcx;
+            fy[j] += -dUay + dUcy;
+            fx[k] -= dUcx;
+            fy[k] -= dUcy;
+        }
+    }
+    free(haspv);
+    *maxbond = mb;
+}
+
 /* ------------------------------------------------------------------ integrator */
 
 /* Groot-Warren step with stored half-step velocity (oercel.c:2303-2334):

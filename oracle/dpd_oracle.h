@@ -64,6 +64,19 @@ typedef struct {
     int32_t pad;
 } ora_event;
 
+/* A lipid molecule template (the reference's mol_t, oercel.c:451-462): bonds
+ * as position pairs with rest lengths, angle terms as position triplets (j the
+ * middle) with kind 0 U = K (1 - cos) or kind 1 U = K (cos - c0)^2. */
+#define ORA_MAXML 16
+#define ORA_MAXMB (2 * ORA_MAXML)
+typedef struct {
+    int32_t mlen, nb, na, pad;
+    int32_t bi[ORA_MAXMB], bj[ORA_MAXMB];
+    double br0[ORA_MAXMB];
+    int32_t ai[ORA_MAXMB], aj[ORA_MAXMB], ak[ORA_MAXMB], akind[ORA_MAXMB];
+    double aK[ORA_MAXMB], ac0[ORA_MAXMB];
+} ora_mol;
+
 /* the reference's catalyst chemistry (oercel.c:1345-1753): synthesis of
  * lipids from N beads around Ka/Kb catalysts, replication and mutation of
  * catalysts, decay, and the W -> N food supply */

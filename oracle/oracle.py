@@ -100,6 +100,8 @@ def _load():
     lib.ora_pair_forces_brute.argtypes = [P, C.c_int32, f32p, f32p, f32p, f32p, u8p, u32p, C.c_int64, C.c_int32,
                                           f64p, f64p]
     lib.ora_bond_forces.argtypes = [P, C.c_int32, f32p, f32p, i32p, f64p, f64p, C.POINTER(C.c_double)]
+    lib.ora_mol_forces.argtypes = [P, C.POINTER(OraMol), C.c_int32, f32p, f32p, i32p, f64p, f64p,
+                                   C.POINTER(C.c_double)]
     lib.ora_integrate_f32.argtypes = [C.POINTER(OraF32), C.c_int32, f32p, f32p, f32p, f32p, f32p, f32p, f32p, f32p]
     lib.ora_integrate_f32.restype = C.c_int32
     lib.ora_integrate_f64.argtypes = [P, C.c_int32, f64p, f64p, f64p, f64p, f64p, f64p, f64p, f64p]
@@ -205,6 +207,34 @@ def bond_forces(p, st, fx=None, fy=None):
     fy = np.zeros(n) if fy is None else fy
     mb = C.c_double(0.0)
     lib().ora_bond_forces(C.byref(p), n, st["x"], st["y"], st["next"], fx, fy, C.byref(mb))
+    return fx, fy, mb.value
+
+
+class OraMol(C.Structure):
+    _fields_ = [("mlen", C.c_int32), ("nb", C.c_int32), ("na", C.c_int32), ("pad", C.c_int32),
+                ("bi", C.c_int32 * 32), ("bj", C.c_int32 * 32), ("br0", C.c_double * 32), ("ai", C.c_int32 * 32),
+                ("aj", C.c_int32 * 32), ("ak", C.c_int32 * 32), ("akind", C.c_int32 * 32), ("aK", C.c_double * 32),
+                ("ac0", C.c_double * 32)]
+
+
+def mol(t):
+    """oracle template from a dict of template fields (as Ref.template() gives)"""
+    m = OraMol()
+    m.mlen, m.nb, m.na = int(t["mlen"]), int(t["nb"]), int(t["na"])
+    for key in ("bi", "bj", "br0", "ai", "aj", "ak", "akind", "aK", "ac0"):
+        arr = getattr(m, key)
+        for q, v in enumerate(t[key]):
+            arr[q] = v
+    return m
+
+
+def mol_forces(p, m, st, fx=None, fy=None):
+    """bonded forces of branched lipids (template m) added to fx, fy"""
+    n = len(st["x"])
+    fx = np.zeros(n) if fx is None else fx
+    fy = np.zeros(n) if fy is None else fy
+    mb = C.c_double(0.0)
+    lib().ora_mol_forces(C.byref(p), C.byref(m), n, st["x"], st["y"], st["next"], fx, fy, C.byref(mb))
     return fx, fy, mb.value
 
 
@@ -349,6 +379,7 @@ class Ref:
             lib.ref_events.argtypes = [vp, i64p, i32p, i64p, f64p, f64p, i32p]
             lib.ref_get_rng.argtypes = [vp, u64p]
             lib.ref_set_rng.argtypes = [vp, u64p]
+            lib.ref_template.argtypes = [vp, i32p, f64p]
             cls._lib = lib
         return cls._lib
 
@@ -394,6 +425,20 @@ class Ref:
 
     def set_rng(self, r):
         self.lib().ref_set_rng(self.h, np.ascontiguousarray(r, np.uint64))
+
+    def template(self):
+        """the reference's lipid template for this handle's parameters (a dict)"""
+        ints, dbls = np.zeros(512, np.int32), np.zeros(512)
+        self.lib().ref_template(self.h, ints, dbls)
+        arch, ml, nh, nb, na = (int(v) for v in ints[:5])
+        k, d, t = 5, 0, dict(arch=arch, mlen=ml, nH=nh, nb=nb, na=na)
+        for key, n in (("bi", nb), ("bj", nb), ("ai", na), ("aj", na), ("ak", na), ("akind", na)):
+            t[key] = ints[k:k + n].copy()
+            k += n
+        for key, n in (("br0", nb), ("aK", na), ("ac0", na), ("px", ml), ("py", ml), ("ix", ml), ("iy", ml)):
+            t[key] = dbls[d:d + n].copy()
+            d += n
+        return t
 
     def __getattr__(self, name):
         f = getattr(self.lib(), "ref_" + name)

@@ -211,3 +211,27 @@ void ref_events(void *h, int64_t *step, int32_t *kind, int64_t *i, double *x, do
 
 void ref_get_rng(void *h, uint64_t *s4) { memcpy(s4, ((ref_t *)h)->S.rng.s, 4 * sizeof(uint64_t)); }
 void ref_set_rng(void *h, const uint64_t *s4) { memcpy(((ref_t *)h)->S.rng.s, s4, 4 * sizeof(uint64_t)); }
+
+/* the reference's lipid template g_mol (built by finalize_params from the
+ * parameters of ref_create): ints = arch, mlen, nH, nb, na, then bi, bj (nb
+ * each), ai, aj, ak, akind (na each); dbls = br0 (nb), aK, ac0 (na each), then
+ * px, py, ix, iy (mlen each) */
+void ref_template(void *h, int32_t *ints, double *dbls) {
+    (void)h;
+    const mol_t *M = &g_mol;
+    int k = 0, d = 0;
+    ints[k++] = M->arch; ints[k++] = M->mlen; ints[k++] = M->nH; ints[k++] = M->nb; ints[k++] = M->na;
+    for (int q = 0; q < M->nb; q++) ints[k++] = M->bi[q];
+    for (int q = 0; q < M->nb; q++) ints[k++] = M->bj[q];
+    for (int q = 0; q < M->na; q++) ints[k++] = M->ai[q];
+    for (int q = 0; q < M->na; q++) ints[k++] = M->aj[q];
+    for (int q = 0; q < M->na; q++) ints[k++] = M->ak[q];
+    for (int q = 0; q < M->na; q++) ints[k++] = M->akind[q];
+    for (int q = 0; q < M->nb; q++) dbls[d++] = M->br0[q];
+    for (int q = 0; q < M->na; q++) dbls[d++] = M->aK[q];
+    for (int q = 0; q < M->na; q++) dbls[d++] = M->ac0[q];
+    for (int b = 0; b < M->mlen; b++) dbls[d++] = M->px[b];
+    for (int b = 0; b < M->mlen; b++) dbls[d++] = M->py[b];
+    for (int b = 0; b < M->mlen; b++) dbls[d++] = M->ix[b];
+    for (int b = 0; b < M->mlen; b++) dbls[d++] = M->iy[b];
+}

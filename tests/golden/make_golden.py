@@ -158,6 +158,55 @@ def catalyst_fixture(name, seed, step, **over):
     np.savez_compressed(os.path.join(HERE, name), **out)
 
 
+# lipid shapes whose templates are checked against the reference's mol_build
+TEMPLATES = [dict(lip_arch="linear", lip_nH=2, lip_nT=3, k_angle=7), dict(lip_arch="pi", lip_nT=1),
+             dict(lip_arch="pi", lip_nT=3, lip_tie=2, k_head=4, cos_head=0.2, r0_head=0.7),
+             dict(lip_arch="y", lip_nT=2, lip_tie=1, k_head=3, cos_head=-0.3), dict(lip_arch="y", lip_nT=4, k_angle=0),
+             dict(lip_arch="bola", lip_nT=2, lip_tie=1, k_head=2, r0_head=0.6), dict(lip_arch="bola", lip_nT=4, lip_tie=3)]
+
+
+def template_fixture():
+    """the reference's template (g_mol) for each shape of TEMPLATES"""
+    import json
+    out = {}
+    for k, kv in enumerate(TEMPLATES):
+        t = O.Ref(L=8, f_lip=0.1, seed=1, threads=1, **kv).template()
+        for key, v in t.items():
+            out[f"c{k}_{key}"] = np.asarray(v)
+        out[f"c{k}_kv"] = np.frombuffer(json.dumps(kv).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "templates.npz"), **out)
+
+
+def mol_fixture(name, seed, **over):
+    """a soup of branched lipids (the reference's init_soup, gid order) and,
+    after 10 reference steps with FP32-rounded positions, its bonded forces
+    alone (bonded_forces with the template, maxbond)"""
+    kv = dict(L=12, rho=4, dt=0.02, k_angle=8, f_lip=0.3, f_Ka=0.02, f_Kb=0.0, c_N=0.05, seed=seed, threads=1,
+              nsub=1, warmup=0, **over)
+    r = O.Ref(**kv)
+    a0 = r.get()
+    out = {f"{k}_soup": a0[k] for k in ("x", "y", "vx", "vy", "type", "nxt", "mpos")}
+    out["rng_soup"] = r.rng()
+    r.prime()
+    r.run(10)
+    a = r.get()
+    for k in ("x", "y", "vx", "vy", "vtx", "vty"):
+        a[k] = f32(a[k])
+    Lf = float(np.float32(kv["L"]))
+    for k in ("x", "y"):
+        a[k][a[k] >= Lf] = 0.0
+    a["fx"] = np.zeros_like(a["fx"])
+    a["fy"] = np.zeros_like(a["fy"])
+    r.set(a)
+    mb = r.bonded()
+    b = r.get()
+    out.update({k: b[k] for k in ("x", "y", "type", "gid", "nxt", "mpos", "fx", "fy")})
+    out["maxbond"] = np.float64(mb)
+    out.update({f"t_{k}": np.asarray(v) for k, v in r.template().items()})
+    out["ini"] = np.frombuffer("".join(f"{k} = {v}\n" for k, v in kv.items()).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, name), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -275,6 +324,18 @@ if __name__ == "__main__":
                 lip_nT=3, f_Ka=0.03, f_Kb=0.02, c_N=0.25, p_syn_a=0.3, p_syn_b=0.3, p_rep_a=0.2, p_rep_b=0.2, mu=0.2,
                 p_ld=0.01, p_kd=0.01, p_nd=0.01, p_feed=0.02, feed_cap=0.27, warmup=0, dt=0.05)
     extras_fixture()
+    template_fixture()
+    mol_fixture("mol_pi_L12_seed31.npz", 31, lip_arch="pi", lip_nT=3, lip_tie=1, k_head=5, cos_head=0.1,
+                r0_head=0.7)
+    mol_fixture("mol_y_L12_seed32.npz", 32, lip_arch="y", lip_nT=2, lip_tie=1, k_head=3, cos_head=-0.3)
+    mol_fixture("mol_bola_L12_seed33.npz", 33, lip_arch="bola", lip_nT=3, lip_tie=2, k_head=2, r0_head=0.6)
+    catalyst_fixture("catalyst_pi_L16_seed14.npz", 14, 21, lip_arch="pi", lip_nT=2, lip_tie=1, k_head=5, cos_head=0.1,
+                     r0_head=0.7, k_bond=300)
+    # a membranes-like pi-lipid soup (tied H2T2 lipids, water-shy tails and catalysts) with catalyst chemistry
+    run_fixture("run_pi_L16_seed7.npz", L=16, seed=7, chem=1, n_chem=4, events=1, nsub=1, lip_arch="pi", lip_nT=1,
+                lip_tie=1, r0_head=0.7, k_bond=300, dt=0.02, f_lip=0.2, f_Ka=0.03, f_Kb=0.01, c_N=0.2, a_W_T=120,
+                a_W_N=45, a_H_N=22, a_N_T=120, p_syn_a=0.3, p_syn_b=0.3, p_rep_a=0.2, p_rep_b=0.2, mu=0.2, p_ld=0.01,
+                p_kd=0.01, p_nd=0.01, p_feed=0.02, feed_cap=0.25)
     catalyst_fixture("catalyst_L16_seed12.npz", 12, 21)
     catalyst_fixture("catalyst_vent_L16_seed13.npz", 13, 21, syn_nN=2, feed="vent", vent_shape="disk", vent_r=4,
                      feed_cap=0.3)

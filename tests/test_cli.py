@@ -37,7 +37,7 @@ def test_errors_exit_1(tmp_path, capsys):
     ini.write_text("L = 16\nf_Ka = 0\nkT_amp = 1.5\n")
     assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
     assert "kT_amp" in capsys.readouterr().err
-    ini.write_text("L = 16\nf_Ka = 0\nlip_arch = pi\n")
+    ini.write_text("L = 16\nf_Ka = 0\nlip_arch = star\n")
     assert cli.run(["x", str(ini), str(tmp_path / "o")]) == 1
     assert "lip_arch" in capsys.readouterr().err
     ini.write_text("L = 16\nk_angle = 0\nf_Ka = 0\ninit = restart\n")

@@ -16,7 +16,8 @@ from conftest import golden
 from gpu_util import params
 
 pytestmark = pytest.mark.gpu
-CASES = ["catalyst_L16_seed12.npz", "catalyst_vent_L16_seed13.npz"]
+# pi: two-headed lipids with one tail each, a rung and junction terms (the template's placement and relaxation)
+CASES = ["catalyst_L16_seed12.npz", "catalyst_vent_L16_seed13.npz", "catalyst_pi_L16_seed14.npz"]
 
 
 def ini_items(g):

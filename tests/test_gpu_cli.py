@@ -33,6 +33,8 @@ G_CAT = "run_cat_L16_seed5.npz"
 # catalyst checks every step from a soup without warm-up at dt = 0.05: at step 5 a bead moves more
 # than 0.5 and the reference sorts again before its check
 G_CAT_RESORT = "run_cat_resort_L16_seed5.npz"
+# pi lipids (the template's bonds, junction and rung) in a membranes-like soup with the catalyst chemistry
+G_PI = "run_pi_L16_seed7.npz"
 
 
 def fixture_bytes(key, name=G):
@@ -100,7 +102,7 @@ def check_snapshot(path, ref_key, name=G):
         assert np.abs(d).max() < POS_TOL.get(name, 1e-3), k
 
 
-@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_CAT_RESORT])
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_CAT_RESORT, G_PI])
 def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
     ini = write_ini(tmp_path, name)
     out = tmp_path / "run"
@@ -118,7 +120,7 @@ def test_run_matches_the_reference_executable(cuda_ok, tmp_path, name):
     assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] == 24
 
 
-@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_CAT_RESORT])
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_CAT_RESORT, G_PI])
 def test_restart_from_a_reference_checkpoint(cuda_ok, tmp_path, name):
     ini = write_ini(tmp_path, name)
     ck = tmp_path / "ref_ckpt.bin"

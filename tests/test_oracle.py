@@ -256,3 +256,25 @@ def test_catalyst_chemistry_matches_reference(name):
             assert abs(e[4] - r["x"]) < 1e-5 and abs(e[5] - r["y"]) < 1e-5
     kinds = {int(r["kind"]) for r in ref}
     assert {0, 1}.issubset(kinds)  # synthesis and replication happened in this check
+
+
+MOL_CASES = ["mol_pi_L12_seed31.npz", "mol_y_L12_seed32.npz", "mol_bola_L12_seed33.npz"]
+
+
+def mol_template(g):
+    return {k[2:]: g[k] for k in g.files if k.startswith("t_")}
+
+
+@pytest.mark.parametrize("name", MOL_CASES)
+def test_template_bonded_forces_match_reference(name):
+    """bonds and angle terms of pi, y and bola lipids (rungs, junction terms)
+    against the reference's bonded_forces on a state it evolved"""
+    g = golden(name)
+    kv = dict(line.split(" = ", 1) for line in bytes(g["ini"]).decode().strip().split("\n"))
+    p = O.params(float(kv["L"]), np.full((8, 8), 25.0), k_bond=100.0, r0=0.5)
+    st = dict(x=g["x"].astype(np.float32), y=g["y"].astype(np.float32), next=g["nxt"].astype(np.int32))
+    fx, fy, mb = O.mol_forces(p, O.mol(mol_template(g)), st)
+    scale = np.abs(g["fx"]).max()
+    assert np.abs(fx - g["fx"]).max() <= 1e-12 * scale and np.abs(fy - g["fy"]).max() <= 1e-12 * scale
+    assert mb == pytest.approx(float(g["maxbond"]), rel=1e-14)
+    assert abs(fx.sum()) < 1e-9 and abs(fy.sum()) < 1e-9

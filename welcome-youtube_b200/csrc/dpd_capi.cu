@@ -61,6 +61,7 @@ struct dpd_handle {
     int gsteps = 0;
     // the reference's catalyst chemistry: replicas with chem_kind 1, the period of their checks
     bool any_cat = false, any_lipid = false;
+    bool any_mol = false;       // some replica has branched lipids (k_mol_forces)
     int64_t cat_period = 0;
     // reverse-mode storage, grown on demand (full checkpoints, the states of one
     // recomputed segment, adjoint arrays in gid order)
@@ -108,6 +109,7 @@ extern "C" int dpd_params_default(dpd_params *p) {
     p->vent_x = -1.0;
     p->vent_y = -1.0;
     p->vent_r = 5.0;
+    p->r0_head = 0.5;
     p->vent_w = 4.0;
     p->seed = 1;
     p->noise = 0;
@@ -198,11 +200,24 @@ static int make_rep(const dpd_params &p, int b0, int n, int c0, RepDev &R) {
     R.ka_d = p.k_angle;
     R.chem_kind = p.chem_kind;
     if (p.chem_kind != 0 && p.chem_kind != 1) return fail(DPD_E_ARG, "chem_kind must be 0 (lipid) or 1 (catalyst)");
+    // the lipid template: branched shapes need it for their bonds, the catalyst chemistry for new lipids
+    dpd_template M;
+    const bool need_mol = p.lip_arch != 0 || (p.chem && p.chem_kind == 1);
+    if (dpd_lipid_template(&p, &M) != DPD_OK) {
+        if (need_mol) return fail(DPD_E_ARG, "lipid shape: lip_arch 0..3 with 2..%d beads (lip_nH >= 1, lip_nT >= 1 "
+                                             "for branched shapes)", DPD_MAXML);
+        M.mlen = p.lip_nH + p.lip_nT;
+        M.nH = p.lip_nH;
+    }
+    R.arch = p.lip_arch;
     if (p.chem && p.chem_kind == 1) {
-        const int ml = p.lip_nH + p.lip_nT;
-        if (p.lip_nH < 1 || p.lip_nT < 0 || ml < 2 || ml > 16) return fail(DPD_E_ARG, "lipids of 2..16 beads");
-        if (!(p.r_cat > 0.0) || p.syn_tries < 1 || p.syn_relax < 0 || p.syn_nN < 0 || p.syn_nN > ml)
-            return fail(DPD_E_ARG, "need r_cat > 0, syn_tries >= 1, syn_relax >= 0, 0 <= syn_nN <= mlen");
+        const int ml = M.mlen;
+        double ext = 0.0;  // the template's reach from its centroid
+        for (int b = 0; b < ml; b++) ext = std::max(ext, std::sqrt(M.px[b] * M.px[b] + M.py[b] * M.py[b]));
+        if (!(p.r_cat > 0.0) || p.syn_tries < 1 || p.syn_tries > DPD_CAT_MAXTR || p.syn_relax < 0 || p.syn_nN < 0 ||
+            p.syn_nN > ml)
+            return fail(DPD_E_ARG, "need r_cat > 0, 1 <= syn_tries <= %d, syn_relax >= 0, 0 <= syn_nN <= mlen",
+                        DPD_CAT_MAXTR);
         if (p.feed_mode < 0 || p.feed_mode > 2 || p.vent_kind < 0 || p.vent_kind > 2)
             return fail(DPD_E_ARG, "feed_mode 0..2, vent_kind 0..2");
         if (p.p_feed < 0.0 || p.p_feed > 1.0 || p.feed_cap < 0.0 || p.feed_cap >= 1.0)
@@ -212,15 +227,15 @@ static int make_rep(const dpd_params &p, int b0, int n, int c0, RepDev &R) {
         const double reach = 1.0 + 0.05 * p.syn_relax, ics = R.ncx / (double)R.L;
         const int wmax = std::max({(int)std::ceil((p.r_cat + 0.5) * ics), (int)std::ceil(1.5 * ics),
                                    (int)std::ceil((reach + 0.5) * ics)});
-        R.cat_E = (int)std::ceil((p.r_cat + 0.5 * (ml - 1) * p.r0) * ics) + 2 + wmax;
+        R.cat_E = (int)std::ceil((p.r_cat + ext) * ics) + 2 + wmax;
         if (2 * (int)std::ceil((reach + 0.5) * ics) + 1 > R.ncx)
             return fail(DPD_E_ARG, "box too small for the catalyst windows (L must exceed 2 (r_cat, reach) + 1)");
     }
     R.syn_tries = p.syn_tries;
     R.syn_relax = p.syn_relax;
     R.syn_nN = p.syn_nN;
-    R.lip_nH = p.lip_nH;
-    R.lip_nT = p.lip_nT;
+    R.lip_nH = M.nH;  // heads first, mlen beads (the template's, for every shape)
+    R.lip_nT = M.mlen - M.nH;
     R.feed_mode = p.feed_mode;
     R.vent_kind = p.vent_kind;
     R.r_cat = p.r_cat;
@@ -314,6 +329,7 @@ static int build_tiles(dpd_handle *h) {
 }
 
 static void enqueue_forces(dpd_handle *h, bool next_keys) {
+    if (h->any_mol) launch_mol_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     if (h->force_kernel == 0) launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
     else launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, next_keys, h->s);
 }
@@ -334,6 +350,7 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
             h->cat_period = a / std::gcd(a, c) * c;
         }
         h->any_stir = h->any_stir || params[r].stir_A != 0.0;
+        h->any_mol = h->any_mol || params[r].lip_arch != 0;
         b0 += n_beads[r];
         c0 += h->rh[r].ncell;
         h->nmax = std::max(h->nmax, (int)n_beads[r]);
@@ -405,6 +422,16 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.cat_near, N));
     TRY(dalloc(h, &b.cat_cell, N));
     TRY(dalloc(h, &b.cat_mark, C));
+    TRY(dalloc(h, &b.fmol, N));
+    {
+        std::vector<dpd_template> mols(nrep);
+        for (int r = 0; r < nrep; r++)
+            if (dpd_lipid_template(&h->params[r], &mols[r]) != DPD_OK) std::memset(&mols[r], 0, sizeof(dpd_template));
+        dpd_template *dm = nullptr;
+        TRY(dalloc(h, &dm, (size_t)nrep));
+        CK(cudaMemcpy(dm, mols.data(), (size_t)nrep * sizeof(dpd_template), cudaMemcpyHostToDevice));
+        b.mol = dm;
+    }
     CK(cudaMemset(b.resort, 0, ((size_t)nrep + 1) * sizeof(int32_t)));
     CK(cudaMemset(b.rng, 0, (size_t)4 * nrep * sizeof(uint64_t)));
     if (h->any_cat && catalyst_setup() != 0)
@@ -671,6 +698,7 @@ static int partial_forces(dpd_handle *h, int32_t r, bool pair, bool bond, float 
     // computed into the spare force buffer so the stored forces stay untouched
     Bufs b = h->b;
     b.f[h->cur] = h->b.f[h->cur ^ 1];
+    if (bond && h->any_mol) launch_mol_forces(b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     launch_forces(b, h->cur, h->d_rep, h->d_bch, h->nbch, pair, bond, false, h->s);
     CK(cudaGetLastError());
     const RepDev &R = h->rh[r];
@@ -1028,10 +1056,17 @@ extern "C" int dpd_set_params(dpd_handle *h, int32_t r, const dpd_params *p) {
     R.nch = old.nch;
     if ((p->chem && p->chem_kind == 1) != (h->params[r].chem && h->params[r].chem_kind == 1) && !h->any_cat)
         return fail(DPD_E_ARG, "dpd_set_params cannot switch the catalyst chemistry on: create the handle with it");
+    if (p->lip_arch != 0 && !h->any_mol)
+        return fail(DPD_E_ARG, "dpd_set_params cannot switch to branched lipids: create the handle with them");
     CK(cudaStreamSynchronize(h->s));
     h->rh[r] = R;
     h->params[r] = *p;
     CK(cudaMemcpy(h->d_rep + r, &R, sizeof R, cudaMemcpyHostToDevice));
+    {
+        dpd_template M;
+        if (dpd_lipid_template(p, &M) != DPD_OK) std::memset(&M, 0, sizeof M);
+        CK(cudaMemcpy((dpd_template *)h->b.mol + r, &M, sizeof M, cudaMemcpyHostToDevice));
+    }
     bool any = false;
     h->any_lipid = false;
     h->cat_period = 0;
@@ -1187,6 +1222,8 @@ static int check_window(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec,
         if (p.chem) return fail(DPD_E_ARG, "chemistry must be off inside a differentiated window");
         if (p.warmup > 0 && h->step < p.warm_end)
             return fail(DPD_E_ARG, "the repulsion warm-up must be over before a differentiated window");
+        if (p.lip_arch != 0)
+            return fail(DPD_E_ARG, "branched lipids are not differentiated (the force VJP has linear bonds only)");
         if (p.k_angle != 0.0 || p.stir_A != 0.0 || p.kT_amp != 0.0)
             return fail(DPD_E_ARG, "angle terms, stirring and the temperature cycle must be off in a differentiated "
                                    "window (the force VJP has no terms for them)");

@@ -33,6 +33,14 @@
 #define CAT_MAXRN 512    // relaxation neighbours of a new chain (the reference keeps 512)
 #define CAT_MARGIN 0.5   // oercel.c:1348
 #define CAT_WIN 1024     // catalysts per window of the walk
+#define CAT_MAXTR DPD_CAT_MAXTR
+#define CAT_SHUF_RUN 256 // swap partners drawn ahead by the shuffle's first warp
+// what the walk does with a catalyst: no draws (fewer than 2 N), the replication
+// draw, the synthesis and replication draws, or a visit by the whole CTA
+#define WALK_NONE 0
+#define WALK_REP 1
+#define WALK_SYN 2
+#define WALK_VISIT 3
 #define CAT_SHUF_MAX 49152  // catalysts per replica shuffled in shared memory (more: in place in global memory)
 
 // event kinds after the lipid chemistry's 0..2
@@ -66,11 +74,11 @@ struct CatSmem {
     uint64_t rng[4];
     int32_t go, k, var, ml;
     int32_t over;                        // a search found more than CAT_MAXNB candidates
+    double tux[CAT_MAXTR], tuy[CAT_MAXTR], tU[CAT_MAXTR];  // trial directions of a synthesis, their energies
     int32_t nchg;                        // beads whose type the current visit changed
     float2 chg[CAT_MAXML + 2];           // and their positions before the change
-    int32_t wk[CAT_WIN];                 // the window of the walk: catalyst slots,
-    uint32_t wnear[CAT_WIN];             // their packed candidate counts,
-    uint8_t wdirty[CAT_WIN];             // and whether an earlier event changed a bead near them
+    int32_t wk[CAT_WIN];                 // the window of the walk: catalyst slots and
+    uint8_t wcode[CAT_WIN];              // their actions: WALK_* | Kb << 2
     double xk, yk, ux, uy, cxm, cym;
 };
 
@@ -88,6 +96,13 @@ __device__ __forceinline__ uint64_t xo_next(uint64_t *s) {
     return r;
 }
 __device__ __forceinline__ double xo_unif(uint64_t *s) { return (double)(xo_next(s) >> 11) * 0x1.0p-53; }
+// xo_unif(s) < p  <=>  (xo_next(s) >> 11) < u01_threshold(p): the draw is k 2^-53
+// with an integer k < 2^53, and k < v <=> k < ceil(v) for real v = p 2^53
+__host__ __device__ __forceinline__ uint64_t u01_threshold(double p) {
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return 1ull << 53;
+    return (uint64_t)ceil(p * 0x1.0p53);
+}
 __device__ __forceinline__ long long xo_below(uint64_t *s, long long n) {
     const long long k = (long long)(xo_unif(s) * (double)n);
     return k >= n ? n - 1 : k;
@@ -131,27 +146,6 @@ __device__ __forceinline__ bool in_band(int c, int c0, int r, int n) {
 }
 
 // ---------------------------------------------------------------- block helpers
-
-// sum of v over the CTA, the same order every time; all threads get it
-__device__ __forceinline__ void block_sum2(CatSmem &S, double &a, double &b) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-    }
-    __syncthreads();
-    if (lane_id() == 0) {
-        S.red[0][threadIdx.x >> 5] = a;
-        S.red[1][threadIdx.x >> 5] = b;
-    }
-    __syncthreads();
-    a = 0.0;
-    b = 0.0;
-    for (int w = 0; w < CAT_WARPS; w++) {
-        a += S.red[0][w];
-        b += S.red[1][w];
-    }
-}
 
 __device__ __forceinline__ int block_excl_scan(CatSmem &S, int v, int &total) {
     const int lane = (int)lane_id(), w = (int)threadIdx.x >> 5;
@@ -284,6 +278,21 @@ __device__ void find_near(CatSmem &S, const RepDev &R, int kslot, double xk, dou
     __syncthreads();
 }
 
+// bead bb of a new lipid centred at (cx0, cy0) with long axis u: the linear
+// chain along u (oercel.c:1433-1436), or the template turned onto u
+// (oercel.c:1437-1440)
+__device__ __forceinline__ void place(const RepDev &R, const dpd_template &M, int bb, int ml, double cx0, double cy0,
+                                      double ux, double uy, double L, double &px, double &py) {
+    if (R.arch == 0) {
+        const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
+        px = dwrap(cx0 + off * ux, L);
+        py = dwrap(cy0 + off * uy, L);
+    } else {
+        px = dwrap(cx0 + (M.px[bb] * ux - M.py[bb] * uy), L);
+        py = dwrap(cy0 + (M.px[bb] * uy + M.py[bb] * ux), L);
+    }
+}
+
 __device__ __forceinline__ bool in_chain(const CatSmem &S, int i, int ml) {
     bool r = false;
     for (int q = 0; q < ml; q++) r |= S.sl[q] == i;
@@ -291,33 +300,44 @@ __device__ __forceinline__ bool in_chain(const CatSmem &S, int i, int ml) {
 }
 
 // overlap energy of the would-be straight chain (centre, direction u) with the
-// beads outside it (chain_overlap_energy, oercel.c:1425-1468)
-__device__ double chain_energy(CatSmem &S, const RepDev &R, double cx0, double cy0, double ux, double uy, int ml) {
+// beads outside it (chain_overlap_energy, oercel.c:1425-1468), for each trial
+// direction S.tu[tr] at once: trial tr on warp tr % CAT_WARPS, its lanes over
+// the staged beads; S.tU[tr] receives the energy
+__device__ void chain_energies(CatSmem &S, const RepDev &R, const dpd_template &M, double cx0, double cy0, int ntr,
+                               int ml) {
     const double L = (double)R.L;
     const int rx = (int)ceil((1.0 + CAT_MARGIN) * R.icsx), ry = (int)ceil((1.0 + CAT_MARGIN) * R.icsy);
-    double U = 0.0, dummy = 0.0;
-    for (int bb = 0; bb < ml; bb++) {
-        const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
-        const double px = dwrap(cx0 + off * ux, L), py = dwrap(cy0 + off * uy, L);
-        const int tb = bb < R.lip_nH ? 1 : 2;
-        int cx, cy;
-        dcell(R, px, py, cx, cy);
-        for (int i = (int)threadIdx.x; i < S.ns; i += CAT_TPB) {
-            if (!in_band(S.cx[i], cx, rx, R.ncx) || !in_band(S.cy[i], cy, ry, R.ncy) || in_chain(S, i, ml)) continue;
-            const double dx = dmin((double)S.pos[i].x - px, L), dy = dmin((double)S.pos[i].y - py, L);
-            const double r2 = dx * dx + dy * dy;
-            if (r2 >= 1.0) continue;
-            const double w = 1.0 - sqrt(r2);
-            U += 0.5 * (double)R.a[tb * DPD_MAXT + S.type[i]] * w * w;
+    const int lane = (int)lane_id(), warp = (int)threadIdx.x >> 5;
+    for (int tr = warp; tr < ntr; tr += CAT_WARPS) {
+        const double ux = S.tux[tr], uy = S.tuy[tr];
+        double U = 0.0;
+        for (int bb = 0; bb < ml; bb++) {
+            double px, py;
+            place(R, M, bb, ml, cx0, cy0, ux, uy, L, px, py);
+            const int tb = bb < R.lip_nH ? 1 : 2;
+            int cx, cy;
+            dcell(R, px, py, cx, cy);
+            for (int i = lane; i < S.ns; i += 32) {
+                if (!in_band(S.cx[i], cx, rx, R.ncx) || !in_band(S.cy[i], cy, ry, R.ncy) || in_chain(S, i, ml))
+                    continue;
+                const double dx = dmin((double)S.pos[i].x - px, L), dy = dmin((double)S.pos[i].y - py, L);
+                const double r2 = dx * dx + dy * dy;
+                if (r2 >= 1.0) continue;
+                const double w = 1.0 - sqrt(r2);
+                U += 0.5 * (double)R.a[tb * DPD_MAXT + S.type[i]] * w * w;
+            }
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) U += __shfl_down_sync(0xffffffffu, U, o);
+        if (lane == 0) S.tU[tr] = U;
     }
-    block_sum2(S, U, dummy);
-    return U;
+    __syncthreads();
 }
 
 // steepest-descent relaxation of the new chain S.px/py against its frozen
-// surroundings (relax_new_chain, oercel.c:1473-1560, the linear template)
-__device__ void relax_chain(CatSmem &S, const RepDev &R, int ml, bool &overflow) {
+// surroundings (relax_new_chain, oercel.c:1473-1560): pair repulsion, then the
+// chain's bonds and angles (the linear terms, or the template's)
+__device__ void relax_chain(CatSmem &S, const RepDev &R, const dpd_template &M, int ml, bool &overflow) {
     const double L = (double)R.L, cap = 0.05, alpha = 0.002;
     const double reach = 1.0 + cap * R.syn_relax, reach2 = reach * reach;
     const int rx = (int)ceil((reach + CAT_MARGIN) * R.icsx), ry = (int)ceil((reach + CAT_MARGIN) * R.icsy);
@@ -341,11 +361,13 @@ __device__ void relax_chain(CatSmem &S, const RepDev &R, int ml, bool &overflow)
     }
     if (base > CAT_MAXRN) overflow = true;
     const int nrn = min(base, CAT_MAXRN);
+    const int lane = (int)lane_id(), warp = (int)threadIdx.x >> 5;
     for (int it = 0; it < R.syn_relax; it++) {
-        for (int bb = 0; bb < ml; bb++) {
+        // chain bead bb: warp bb % CAT_WARPS, its lanes over the neighbours
+        for (int bb = warp; bb < ml; bb += CAT_WARPS) {
             const int ti = bb < R.lip_nH ? 1 : 2;
             double fx = 0.0, fy = 0.0;
-            for (int q = (int)threadIdx.x; q < nrn; q += CAT_TPB) {
+            for (int q = lane; q < nrn; q += 32) {
                 const int j = S.rn[q];
                 const double dx = dmin(S.px[bb] - (double)S.pos[j].x, L), dy = dmin(S.py[bb] - (double)S.pos[j].y, L);
                 const double r2 = dx * dx + dy * dy;
@@ -355,16 +377,49 @@ __device__ void relax_chain(CatSmem &S, const RepDev &R, int ml, bool &overflow)
                 fx += f * dx;
                 fy += f * dy;
             }
-            block_sum2(S, fx, fy);
-            if (threadIdx.x == 0) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                fx += __shfl_down_sync(0xffffffffu, fx, o);
+                fy += __shfl_down_sync(0xffffffffu, fy, o);
+            }
+            if (lane == 0) {
                 S.fx[bb] = fx;
                 S.fy[bb] = fy;
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0 && R.arch != 0) {
+            // the template's bonds and angles by position (mol_forces, oercel.c:1221-1257)
+            for (int q = 0; q < M.nb; q++) {
+                const int i = M.bi[q], j = M.bj[q];
+                const double dx = dmin(S.px[j] - S.px[i], L), dy = dmin(S.py[j] - S.py[i], L);
+                const double r = sqrt(dx * dx + dy * dy);
+                const double f = -R.kb_d * (r - M.br0[q]) / r;
+                S.fx[j] += f * dx;
+                S.fy[j] += f * dy;
+                S.fx[i] -= f * dx;
+                S.fy[i] -= f * dy;
+            }
+            for (int q = 0; q < M.na; q++) {
+                const int i = M.ai[q], j = M.aj[q], k = M.ak[q];
+                const double ax = dmin(S.px[j] - S.px[i], L), ay = dmin(S.py[j] - S.py[i], L);
+                const double cxv = dmin(S.px[k] - S.px[j], L), cyv = dmin(S.py[k] - S.py[j], L);
+                const double la = sqrt(ax * ax + ay * ay), lc = sqrt(cxv * cxv + cyv * cyv);
+                const double ilac = 1.0 / (la * lc), cs = (ax * cxv + ay * cyv) * ilac;
+                const double g = M.akind[q] == 0 ? -M.aK[q] : 2.0 * M.aK[q] * (cs - M.ac0[q]);
+                const double dUax = g * (cxv * ilac - cs * ax / (la * la)), dUay = g * (cyv * ilac - cs * ay / (la * la));
+                const double dUcx = g * (ax * ilac - cs * cxv / (lc * lc)), dUcy = g * (ay * ilac - cs * cyv / (lc * lc));
+                S.fx[i] += dUax;
+                S.fy[i] += dUay;
+                S.fx[j] += -dUax + dUcx;
+                S.fy[j] += -dUay + dUcy;
+                S.fx[k] -= dUcx;
+                S.fy[k] -= dUcy;
+            }
+        }
         if (threadIdx.x == 0) {
             double bx[CAT_MAXML], by[CAT_MAXML], bl[CAT_MAXML];
-            for (int bb = 0; bb < ml - 1; bb++) {
+            for (int bb = 0; bb < ml - 1 && R.arch == 0; bb++) {
                 bx[bb] = dmin(S.px[bb + 1] - S.px[bb], L);
                 by[bb] = dmin(S.py[bb + 1] - S.py[bb], L);
                 bl[bb] = sqrt(bx[bb] * bx[bb] + by[bb] * by[bb]);
@@ -374,7 +429,7 @@ __device__ void relax_chain(CatSmem &S, const RepDev &R, int ml, bool &overflow)
                 S.fx[bb] -= f * bx[bb];
                 S.fy[bb] -= f * by[bb];
             }
-            for (int bb = 0; bb < ml - 2 && R.ka_d != 0.0; bb++) {
+            for (int bb = 0; bb < ml - 2 && R.ka_d != 0.0 && R.arch == 0; bb++) {
                 const double ax = bx[bb], ay = by[bb], cxv = bx[bb + 1], cyv = by[bb + 1], la = bl[bb], lc = bl[bb + 1];
                 const double ilac = 1.0 / (la * lc), cs = (ax * cxv + ay * cyv) * ilac, ka = R.ka_d;
                 const double dUax = -ka * (cxv * ilac - cs * ax / (la * la)), dUay = -ka * (cyv * ilac - cs * ay / (la * la));
@@ -465,10 +520,18 @@ __global__ void __launch_bounds__(BEAD_TPB) k_cat_list(Bufs b, int cur, const Re
     const RepDev &R = reps[c.rep];
     const long long step = *b.step;
     if (!cat_due(R, step) || b.cat_cnt[blockIdx.x] == 0) return;
-    if (threadIdx.x == 0) {
-        int s = 0;
-        for (int k = R.ch0; k < (int)blockIdx.x; k++) s += b.cat_cnt[k];
-        pre = s;
+    {  // candidates of the replica's earlier chunks, summed by the whole block
+        int part = 0;
+        for (int k = R.ch0 + (int)threadIdx.x; k < (int)blockIdx.x; k += BEAD_TPB) part += b.cat_cnt[k];
+        part = __reduce_add_sync(0xffffffffu, part);
+        if (lane_id() == 0) ws[threadIdx.x >> 5] = part;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int s = 0;
+            for (int w = 0; w < BEAD_TPB / 32; w++) s += ws[w];
+            pre = s;
+        }
+        __syncthreads();
     }
     const int d = c.begin + (int)threadIdx.x;
     int v = 0;
@@ -504,69 +567,93 @@ __global__ void __launch_bounds__(BEAD_TPB) k_cat_list(Bufs b, int cur, const Re
 }
 
 // the catalyst list of one replica shuffled with its serial generator
-// (oercel.c:1571-1580): one warp per replica, the list in shared memory while
-// it fits (CAT_SHUF_MAX entries); also the replica's catalyst count
-__global__ void __launch_bounds__(32) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int shmax) {
+// (oercel.c:1571-1580), the list in shared memory while it fits (shmax
+// entries); also the replica's catalyst count.  Two warps pipeline the
+// Fisher-Yates loop: lane 0 of warp 0 draws the next CAT_SHUF_RUN swap
+// partners while lane 0 of warp 1 applies the previous run's swaps, so the
+// draws and the swaps are those of the serial loop.
+__global__ void __launch_bounds__(64) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int shmax) {
     extern __shared__ int32_t shl[];
+    __shared__ int32_t part[2][CAT_SHUF_RUN];
+    __shared__ int nks;
     const int rep = (int)blockIdx.x;
     const RepDev &R = reps[rep];
     if (!cat_due(R, *b.step)) return;
-    const int lane = (int)lane_id();
-    int nk = 0;
-    for (int k = lane; k < R.nch; k += 32) nk += b.cat_cnt[R.ch0 + k];
-    nk = __reduce_add_sync(0xffffffffu, nk);
+    const int tid = (int)threadIdx.x, warp = tid >> 5, lane = (int)lane_id();
+    if (warp == 0) {
+        int n = 0;
+        for (int k = lane; k < R.nch; k += 32) n += b.cat_cnt[R.ch0 + k];
+        n = __reduce_add_sync(0xffffffffu, n);
+        if (lane == 0) {
+            nks = n;
+            b.cat_nk[rep] = n;
+        }
+    }
+    __syncthreads();
+    const int nk = nks;
     int32_t *list = b.cat_list + R.b0;
     const bool sh = nk <= shmax;
     int32_t *a = sh ? shl : list;
     if (sh)
-        for (int i = lane; i < nk; i += 32) shl[i] = list[i];
-    __syncwarp();
-    if (lane == 0) {
-        b.cat_nk[rep] = nk;
-        uint64_t s[4];
-        for (int q = 0; q < 4; q++) s[q] = b.rng[4 * rep + q];
-        for (int i = nk - 1; i > 0; i--) {
-            const int c = (int)xo_below(s, i + 1);
-            const int t = a[i];
-            a[i] = a[c];
-            a[c] = t;
-        }
-        for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = s[q];
+        for (int i = tid; i < nk; i += 64) shl[i] = list[i];
+    // swaps i = nk-1 .. 1; run r holds i = nk-1 - r*RUN - j, j < RUN
+    const int nswap = nk > 1 ? nk - 1 : 0, nrun = (nswap + CAT_SHUF_RUN - 1) / CAT_SHUF_RUN;
+    uint64_t st[4];
+    if (tid == 0)
+        for (int q = 0; q < 4; q++) st[q] = b.rng[4 * rep + q];
+    for (int r = 0; r <= nrun; r++) {
+        if (tid == 0 && r < nrun)  // draw run r
+            for (int j = 0; j < CAT_SHUF_RUN; j++) {
+                const int i = nk - 1 - r * CAT_SHUF_RUN - j;
+                if (i <= 0) break;
+                part[r & 1][j] = (int)xo_below(st, i + 1);
+            }
+        if (tid == 32 && r > 0)  // apply run r - 1
+            for (int j = 0; j < CAT_SHUF_RUN; j++) {
+                const int i = nk - 1 - (r - 1) * CAT_SHUF_RUN - j;
+                if (i <= 0) break;
+                const int c = part[(r - 1) & 1][j];
+                const int t = a[i];
+                a[i] = a[c];
+                a[c] = t;
+            }
+        __syncthreads();
     }
-    __syncwarp();
+    if (tid == 0)
+        for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = st[q];
     if (sh)
-        for (int i = lane; i < nk; i += 32) list[i] = shl[i];
+        for (int i = tid; i < nk; i += 64) list[i] = shl[i];
 }
 
-// per catalyst (thread per list entry): the N and W counts its searches will
-// find (the candidate rules of find_near on the cell index of the last sort),
-// its type and its cell.  Packed: nn | nw << 16 | Kb << 31 (counts saturate).
-__global__ void __launch_bounds__(BEAD_TPB) k_cat_near(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                       const Chunk *__restrict__ ch) {
-    const Chunk c = ch[blockIdx.x];
-    const RepDev &R = reps[c.rep];
+// per catalyst (a warp each, its lanes over the cells of the search window):
+// the N and W counts its searches will find (the candidate rules of find_near
+// on the cell index of the last sort), its type and its cell.  Packed:
+// nn | nw << 16 | Kb << 31 (counts saturate).  Grid: blockIdx.y = replica,
+// the replica's blocks stride over its catalysts.
+__global__ void __launch_bounds__(BEAD_TPB) k_cat_near(Bufs b, int cur, const RepDev *__restrict__ reps) {
+    const int rep = (int)blockIdx.y;
+    const RepDev &R = reps[rep];
     if (!cat_due(R, *b.step)) return;
-    const int d = c.begin + (int)threadIdx.x;
-    if (d >= c.end || d - R.b0 >= b.cat_nk[c.rep]) return;
-    const int k = b.cat_list[d];
-    const float2 pk = b.pos[cur][k];
-    const int t = (int)(b.tg[cur][k] >> TYPE_SHIFT);
-    const double L = (double)R.L, xk = pk.x, yk = pk.y, r2c = R.r_cat * R.r_cat;
-    int cx, cy;
-    dcell(R, xk, yk, cx, cy);
+    const int nk = b.cat_nk[rep], lane = (int)lane_id();
     const int rx = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsx), ry = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsy);
     const int ncol = 2 * rx + 1 >= R.ncx ? R.ncx : 2 * rx + 1, nrow = 2 * ry + 1 >= R.ncy ? R.ncy : 2 * ry + 1;
-    const int x0 = 2 * rx + 1 >= R.ncx ? 0 : cx - rx, y0 = 2 * ry + 1 >= R.ncy ? 0 : cy - ry;
+    const double L = (double)R.L, r2c = R.r_cat * R.r_cat;
     const int32_t *cs = b.cstart + R.c0;
-    int nn = 0, nw = 0;
-    for (int u = 0; u < ncol; u++) {
-        int gx = x0 + u;
-        gx += gx < 0 ? R.ncx : (gx >= R.ncx ? -R.ncx : 0);
-        for (int v = 0; v < nrow; v++) {
-            int gy = y0 + v;
+    const int warps = (int)gridDim.x * (BEAD_TPB / 32);
+    for (int q = (int)blockIdx.x * (BEAD_TPB / 32) + (int)(threadIdx.x >> 5); q < nk; q += warps) {
+        const int k = b.cat_list[R.b0 + q];
+        const float2 pk = b.pos[cur][k];
+        const double xk = pk.x, yk = pk.y;
+        int cx, cy;
+        dcell(R, xk, yk, cx, cy);
+        const int x0 = 2 * rx + 1 >= R.ncx ? 0 : cx - rx, y0 = 2 * ry + 1 >= R.ncy ? 0 : cy - ry;
+        int nn = 0, nw = 0;
+        for (int e = lane; e < ncol * nrow; e += 32) {
+            int gx = x0 + e / nrow, gy = y0 + e % nrow;
+            gx += gx < 0 ? R.ncx : (gx >= R.ncx ? -R.ncx : 0);
             gy += gy < 0 ? R.ncy : (gy >= R.ncy ? -R.ncy : 0);
-            const int gc = gx * R.ncy + gy, e = cs[gc + 1];
-            for (int j = cs[gc]; j < e; j++) {
+            const int gc = gx * R.ncy + gy, end = cs[gc + 1];
+            for (int j = cs[gc]; j < end; j++) {
                 const int tj = (int)(b.tg[cur][j] >> TYPE_SHIFT);
                 if ((tj != 3 && tj != 0) || j == k) continue;
                 const float2 pj = b.pos[cur][j];
@@ -577,9 +664,15 @@ __global__ void __launch_bounds__(BEAD_TPB) k_cat_near(Bufs b, int cur, const Re
                 }
             }
         }
+        nn = __reduce_add_sync(0xffffffffu, nn);
+        nw = __reduce_add_sync(0xffffffffu, nw);
+        if (lane == 0) {
+            const int t = (int)(b.tg[cur][k] >> TYPE_SHIFT);
+            b.cat_near[R.b0 + q] =
+                (uint32_t)min(nn, 0x7FFF) | ((uint32_t)min(nw, 0x7FFF) << 16) | (t == 5 ? 0x80000000u : 0u);
+            b.cat_cell[R.b0 + q] = R.c0 + cx * R.ncy + cy;
+        }
     }
-    b.cat_near[d] = (uint32_t)min(nn, 0x7FFF) | ((uint32_t)min(nw, 0x7FFF) << 16) | (t == 5 ? 0x80000000u : 0u);
-    b.cat_cell[d] = R.c0 + cx * R.ncy + cy;
 }
 
 // One catalyst visit with the whole CTA (oercel.c:1582-1653): staging, the
@@ -589,6 +682,7 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
                       bool &overflow) {
     const int tid = (int)threadIdx.x, ml = R.lip_nH + R.lip_nT;
     const double L = (double)R.L;
+    const dpd_template &M = b.mol[rep];
     if (tid == 0) {
         const int t = (int)(__ldcg(b.tg[cur] + k) >> TYPE_SHIFT);
         const float2 pk = __ldcg(b.pos[cur] + k);
@@ -636,24 +730,28 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
             S.ux = 1.0;
             S.uy = 0.0;
         }
-        __syncthreads();
-        double ubest = INFINITY;
-        for (int tr = 0; tr < R.syn_tries; tr++) {
-            if (tid == 0) {
+        // the trial directions: consecutive draws, as in the reference's loop
+        const int ntr = R.syn_tries;
+        if (tid == 0)
+            for (int tr = 0; tr < ntr; tr++) {
                 const double phi = 2.0 * M_PI * xo_unif(S.rng);
-                S.fx[0] = cos(phi);
-                S.fy[0] = sin(phi);
+                S.tux[tr] = cos(phi);
+                S.tuy[tr] = sin(phi);
             }
-            __syncthreads();
-            const double cu = S.fx[0], su = S.fy[0];
-            const double U = R.syn_tries > 1 ? chain_energy(S, R, S.cxm, S.cym, cu, su, ml) : 0.0;
-            if (tid == 0 && U < ubest) {
-                ubest = U;
-                S.ux = cu;
-                S.uy = su;
+        __syncthreads();
+        if (ntr > 1) chain_energies(S, R, M, S.cxm, S.cym, ntr, ml);
+        if (tid == 0) {  // the first lowest energy wins
+            double ubest = INFINITY;
+            for (int tr = 0; tr < ntr; tr++) {
+                const double U = ntr > 1 ? S.tU[tr] : 0.0;
+                if (U < ubest) {
+                    ubest = U;
+                    S.ux = S.tux[tr];
+                    S.uy = S.tuy[tr];
+                }
             }
-            __syncthreads();
         }
+        __syncthreads();
         if (tid == 0) {
             double mvx = 0, mvy = 0, mtx = 0, mty = 0;
             for (int bb = 0; bb < ml; bb++) {
@@ -670,9 +768,7 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
             mty /= ml;
             for (int bb = 0; bb < ml; bb++) {
                 const int i = S.sl[bb], g = S.slot[i];
-                const double off = (bb - 0.5 * (ml - 1)) * R.r0_d;
-                S.px[bb] = dwrap(S.cxm + off * S.ux, L);
-                S.py[bb] = dwrap(S.cym + off * S.uy, L);
+                place(R, M, bb, ml, S.cxm, S.cym, S.ux, S.uy, L, S.px[bb], S.py[bb]);
                 b.vh[cur][g] = make_float2((float)mvx, (float)mvy);
                 b.vt[cur][g] = make_float2((float)mtx, (float)mty);
                 const int t = bb < R.lip_nH ? 1 : 2;
@@ -683,7 +779,7 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
             }
         }
         __syncthreads();
-        if (R.syn_relax > 0) relax_chain(S, R, ml, overflow);
+        if (R.syn_relax > 0) relax_chain(S, R, M, ml, overflow);
         if (tid == 0) {
             const float Lf = R.L;
             for (int bb = 0; bb < ml; bb++) {
@@ -714,6 +810,19 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
     __syncthreads();
 }
 
+// the walk's action for a catalyst from its packed counts and its cell mark
+__device__ __forceinline__ uint8_t walk_code(uint32_t v, uint8_t dirty, int nsynN, int ml) {
+    const int nn = (int)(v & 0x7FFF), nw = (int)((v >> 16) & 0x7FFF), var = (int)(v >> 31);
+    int code;
+    if (dirty || nn > CAT_MAXNB || nw > CAT_MAXNB) code = WALK_VISIT;
+    else if (nn < 2) code = WALK_NONE;
+    else {
+        const int nwe = nn >= nsynN && nsynN < ml ? nw : 0;
+        code = nn >= nsynN && nsynN + nwe >= ml ? WALK_SYN : WALK_REP;
+    }
+    return (uint8_t)(code | var << 2);
+}
+
 // The catalysts of one replica, one after the other in the shuffled order
 // (oercel.c:1582-1655).  Most visits end without an event: their decisions
 // need only the draws and the two candidate counts, which k_cat_near found
@@ -737,6 +846,8 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
     const uint32_t *near = b.cat_near + R.b0;
     const int32_t *cell = b.cat_cell + R.b0;
     uint8_t *mark = b.cat_mark;
+    const uint64_t tsyn[2] = {u01_threshold(R.p_syn_a), u01_threshold(R.p_syn_b)};
+    const uint64_t trep[2] = {u01_threshold(R.p_rep_a), u01_threshold(R.p_rep_b)};
     // marking reach: the search radius in cells (a changed bead within r_cat of a
     // catalyst lies within rx cells of it), plus one
     const int mx = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsx) + 1, my = (int)ceil((R.r_cat + CAT_MARGIN) * R.icsy) + 1;
@@ -751,8 +862,7 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
         __syncthreads();
         for (int i = tid; i < wn; i += CAT_TPB) {
             S.wk[i] = list[w0 + i];
-            S.wnear[i] = near[w0 + i];
-            S.wdirty[i] = __ldcg(mark + cell[w0 + i]);
+            S.wcode[i] = walk_code(near[w0 + i], __ldcg(mark + cell[w0 + i]), nsynN, ml);
         }
         __syncthreads();
         int i = 0;
@@ -760,15 +870,16 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
             if (tid == 0) {
                 uint64_t r[4] = {S.rng[0], S.rng[1], S.rng[2], S.rng[3]};
                 for (; i < wn; i++) {
-                    const uint32_t v = S.wnear[i];
-                    const int nn = (int)(v & 0x7FFF), nw = (int)((v >> 16) & 0x7FFF), var = (int)(v >> 31);
-                    if (S.wdirty[i] || nn > CAT_MAXNB || nw > CAT_MAXNB) break;
-                    if (nn < 2) continue;
+                    const int code = S.wcode[i], kind = code & 3, var = code >> 2;
+                    if (kind == WALK_NONE) continue;
+                    if (kind == WALK_VISIT) break;
                     uint64_t t[4] = {r[0], r[1], r[2], r[3]};
-                    const int nwe = nn >= nsynN && nsynN < ml ? nw : 0;
-                    if (nn >= nsynN && nsynN + nwe >= ml && xo_unif(t) < (var ? R.p_syn_b : R.p_syn_a)) break;
-                    if (xo_unif(t) < (var ? R.p_rep_b : R.p_rep_a)) break;
-                    for (int q = 0; q < 4; q++) r[q] = t[q];
+                    if (kind == WALK_SYN && (xo_next(t) >> 11) < tsyn[var]) break;
+                    if ((xo_next(t) >> 11) < trep[var]) break;
+                    r[0] = t[0];
+                    r[1] = t[1];
+                    r[2] = t[2];
+                    r[3] = t[3];
                 }
                 for (int q = 0; q < 4; q++) S.rng[q] = r[q];
                 S.k = i;
@@ -790,7 +901,8 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
                     mark[R.c0 + gx * R.ncy + gy] = 1;
                 }
                 __syncthreads();
-                for (int j = i + 1 + tid; j < wn; j += CAT_TPB) S.wdirty[j] |= __ldcg(mark + cell[w0 + j]);
+                for (int j = i + 1 + tid; j < wn; j += CAT_TPB)
+                    if (__ldcg(mark + cell[w0 + j])) S.wcode[j] = (uint8_t)(WALK_VISIT | (S.wcode[j] & 4));
                 __syncthreads();
             }
             i++;
@@ -917,8 +1029,8 @@ void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch
     const int shmax = std::min(nmax, CAT_SHUF_MAX);
     k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
     k_cat_list<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
-    k_cat_shuffle<<<nrep, 32, (size_t)shmax * sizeof(int32_t), s>>>(b, rep, shmax);
-    k_cat_near<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
+    k_cat_shuffle<<<nrep, 64, (size_t)shmax * sizeof(int32_t), s>>>(b, rep, shmax);
+    k_cat_near<<<dim3(std::max(1, 148 * 8 / nrep), nrep), BEAD_TPB, 0, s>>>(b, cur, rep);
     cudaMemsetAsync(b.cat_mark, 0, (size_t)C, s);
     k_cat_serial<<<nrep, CAT_TPB, sizeof(CatSmem), s>>>(b, cur, rep);
     k_cat_decay<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);

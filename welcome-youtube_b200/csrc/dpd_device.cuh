@@ -220,25 +220,35 @@ __device__ __forceinline__ void bead_pairs_direct(const PairCtx &pc, const RepDe
 
 // ---------------------------------------------------------------- angle terms and stirring
 
-// The outer shares of one angle term U = ka (1 - cos theta) of the chain
-// triplet (i, j, k), theta the angle between a = x_j - x_i and c = x_k - x_j
-// (chain_forces_linear, oercel.c:1290-1307), in fixed point: (qix, qiy) on
-// the end i, (qkx, qky) on the end k; the middle bead j takes -(qi + qk), so
-// the three shares cancel exactly.  Every rounding is explicit: each of the
-// three beads recomputes the term from the same positions and gets the same bits.
-__device__ __forceinline__ void angle_shares(float2 xi, float2 xj, float2 xk, float ka, float L, float h, int &qix,
-                                             int &qiy, int &qkx, int &qky) {
+// The outer shares of one angle term of the triplet (i, j, k), theta the angle
+// between a = x_j - x_i and c = x_k - x_j: kind 0, U = K (1 - cos theta) (the
+// chain terms, chain_forces_linear, oercel.c:1290-1307); kind 1,
+// U = K (cos theta - c0)^2 (the junction terms of branched lipids,
+// mol_forces, oercel.c:1237-1256).  In fixed point: (qix, qiy) on the end i,
+// (qkx, qky) on the end k; the middle bead j takes -(qi + qk), so the three
+// shares cancel exactly.  Every rounding is explicit: each of the three beads
+// recomputes the term from the same positions and gets the same bits.
+__device__ __forceinline__ void angle_shares_g(float2 xi, float2 xj, float2 xk, int kind, float K, float c0, float L,
+                                               float h, int &qix, int &qiy, int &qkx, int &qky) {
     const float ax = minimg(__fsub_rn(xj.x, xi.x), L, h), ay = minimg(__fsub_rn(xj.y, xi.y), L, h);
     const float cx = minimg(__fsub_rn(xk.x, xj.x), L, h), cy = minimg(__fsub_rn(xk.y, xj.y), L, h);
     const float la2 = __fmaf_rn(ax, ax, __fmul_rn(ay, ay)), lc2 = __fmaf_rn(cx, cx, __fmul_rn(cy, cy));
     const float ilac = __fdiv_rn(1.0f, __fmul_rn(__fsqrt_rn(la2), __fsqrt_rn(lc2)));
     const float cs = __fmul_rn(__fmaf_rn(ax, cx, __fmul_rn(ay, cy)), ilac);
     const float csa = __fdiv_rn(cs, la2), csc = __fdiv_rn(cs, lc2);
-    // on i: dU/da = -ka (c / (la lc) - cos a / la^2); on k: -dU/dc = ka (a / (la lc) - cos c / lc^2)
-    qix = f2fix16(__fmul_rn(-ka, __fsub_rn(__fmul_rn(cx, ilac), __fmul_rn(csa, ax))));
-    qiy = f2fix16(__fmul_rn(-ka, __fsub_rn(__fmul_rn(cy, ilac), __fmul_rn(csa, ay))));
-    qkx = f2fix16(__fmul_rn(ka, __fsub_rn(__fmul_rn(ax, ilac), __fmul_rn(csc, cx))));
-    qky = f2fix16(__fmul_rn(ka, __fsub_rn(__fmul_rn(ay, ilac), __fmul_rn(csc, cy))));
+    // g = dU/dcos: kind 0, U = K (1 - cos): -K; kind 1, U = K (cos - c0)^2: 2 K (cos - c0) (oercel.c:1243-1245)
+    // on i: dU/da = g (c / (la lc) - cos a / la^2); on k: -dU/dc = -g (a / (la lc) - cos c / lc^2)
+    const float g = kind == 0 ? -K : __fmul_rn(2.0f * K, __fsub_rn(cs, c0));
+    qix = f2fix16(__fmul_rn(g, __fsub_rn(__fmul_rn(cx, ilac), __fmul_rn(csa, ax))));
+    qiy = f2fix16(__fmul_rn(g, __fsub_rn(__fmul_rn(cy, ilac), __fmul_rn(csa, ay))));
+    qkx = f2fix16(__fmul_rn(-g, __fsub_rn(__fmul_rn(ax, ilac), __fmul_rn(csc, cx))));
+    qky = f2fix16(__fmul_rn(-g, __fsub_rn(__fmul_rn(ay, ilac), __fmul_rn(csc, cy))));
+}
+
+// the straight-chain term U = ka (1 - cos) of the linear lipids
+__device__ __forceinline__ void angle_shares(float2 xi, float2 xj, float2 xk, float ka, float L, float h, int &qix,
+                                             int &qiy, int &qkx, int &qky) {
+    angle_shares_g(xi, xj, xk, 0, ka, 0.0f, L, h, qix, qiy, qkx, qky);
 }
 
 // The angle shares of bead g at position pg with chain neighbours p (prev),

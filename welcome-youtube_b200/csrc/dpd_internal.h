@@ -18,6 +18,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/dpd.h"
+
 #define DPD_MAXT 8
 #define TYPE_SHIFT 29
 #define GID_MASK 0x1FFFFFFFu
@@ -37,6 +39,7 @@
 #define DPD_F_TILE 0x20u        // a cell tile held more beads than its shared-memory capacity
 #define DPD_F_FORCE 0x40u       // a single pair or bond force term above the fixed-point range
 #define DPD_F_CATALYST 0x80u    // a catalyst's neighbourhood exceeded the staging capacity
+#define DPD_CAT_MAXTR 64        // orientation trials of one lipid synthesis (syn_tries)
 
 struct RepDev {                 // constants of one replica, read by every kernel
     float L, halfL;
@@ -66,7 +69,8 @@ struct RepDev {                 // constants of one replica, read by every kerne
     // the reference's catalyst chemistry (chem_kind 1, dpd_catalyst.cu)
     int32_t chem_kind, syn_tries, syn_relax, syn_nN, lip_nH, lip_nT, feed_mode, vent_kind;
     int32_t ch0, nch;           // this replica's chunks in the bead chunk table
-    int32_t cat_E, pad3;        // half-width in cells of the window staged around a catalyst
+    int32_t cat_E;              // half-width in cells of the window staged around a catalyst
+    int32_t arch;               // lipid shape (0 linear: per-bead bond terms; else the template, k_mol_forces)
     double r_cat, p_syn_a, p_syn_b, p_rep_a, p_rep_b, mu, p_ld, p_kd, p_nd, p_feed, feed_cap;
     double vent_x, vent_y, vent_r, vent_w;
     double kb_d, r0_d, ka_d;    // FP64 bond and angle constants for the relaxation of new chains
@@ -153,6 +157,8 @@ struct Bufs {
     uint32_t *cat_near;         // per catalyst list entry: packed candidate counts (k_cat_near)
     int32_t *cat_cell;          // per catalyst list entry: its cell
     uint8_t *cat_mark;          // per cell: a bead near it changed type in the current check
+    const dpd_template *mol;    // per replica: its lipid template
+    int2 *fmol;                 // per bead: fixed-point bonded force of a branched lipid (k_mol_forces)
 };
 
 struct StateView {              // one stored configuration (slot order of its own step)
@@ -207,6 +213,7 @@ void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
 void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s);
+void launch_mol_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
                    int64_t C, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,

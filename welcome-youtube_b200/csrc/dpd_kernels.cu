@@ -500,7 +500,14 @@ __global__ void __launch_bounds__(BEAD_TPB) k_forces(Bufs b, int cur, const RepD
             // the stirring body force belongs to the pair forces, as in the reference (oercel.c:1159-1165)
             if (R.stir_A != 0.0f) ax += stir_force(R, pi.y, pc.gi, b.stir[c.rep]);
         }
-        if (BOND) {
+        if (BOND && R.arch != 0) {  // branched lipids: the template terms of k_mol_forces
+            const int2 lk = b.link[cur][d];
+            if (lk.x >= 0 || lk.y >= 0) {
+                const int2 q = b.fmol[d];
+                ax += q.x;
+                ay += q.y;
+            }
+        } else if (BOND) {
             const int2 lk = b.link[cur][d];
             const float h = R.halfL, kb = R.kb, r0 = R.r0;
             float2 pjs[2];

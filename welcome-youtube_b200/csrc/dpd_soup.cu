@@ -1,8 +1,9 @@
 // dpd_soup.cu -- host-side random soup of the reference (dpd_init_soup).
 //
-// init_soup + set_velocities of cel/engine/oercel.c:1757-1814 for the linear
-// lipid: the same xoshiro256** stream seeded as rng_seed (oercel.c:143-174),
-// drawn in the same order, so one seed gives the reference's initial state.
+// init_soup + set_velocities of cel/engine/oercel.c:1757-1814, for linear
+// lipids and for the branched templates (dpd_mol.cu): the same xoshiro256**
+// stream seeded as rng_seed (oercel.c:143-174), drawn in the same order, so
+// one seed gives the reference's initial state.
 #include <cmath>
 #include <cstdint>
 
@@ -60,8 +61,14 @@ double wrap(double v, double L) {
 extern "C" int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, double r0, int32_t nH, int32_t nT,
                              double f_lip, double f_Ka, double f_Kb, double c_N, double *x, double *y, double *vx,
                              double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads,
-                             uint64_t *rng_out) {
-    if (!x || !y || !vx || !vy || !type || N < 2 || nH < 1 || nT < 0 || !(L > 0.0) || !(kT > 0.0))
+                             uint64_t *rng_out, const dpd_template *mol) {
+    const bool branched = mol && mol->arch != 0;
+    if (branched) {
+        nH = mol->nH;
+        nT = mol->mlen - mol->nH;
+    }
+    if (!x || !y || !vx || !vy || !type || N < 2 || nH < 1 || nT < 0 || !(L > 0.0) || !(kT > 0.0) ||
+        nH + nT > DPD_MAXML)
         return DPD_E_ARG;
     const int ml = nH + nT;
     const long nlip = std::lround(f_lip * N / ml);
@@ -76,9 +83,15 @@ extern "C" int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, doub
     for (long m = 0; m < nlip; m++) {
         const double hx = L * rng.unif(), hy = L * rng.unif();
         const double phi = 2.0 * M_PI * rng.unif();
+        const double cph = std::cos(phi), sph = std::sin(phi);
         for (int b = 0; b < ml; b++) {
-            x[gi] = wrap(hx + b * r0 * std::cos(phi), L);
-            y[gi] = wrap(hy + b * r0 * std::sin(phi), L);
+            if (branched) {  // the template's soup offsets, turned by phi
+                x[gi] = wrap(hx + (mol->ix[b] * cph - mol->iy[b] * sph), L);
+                y[gi] = wrap(hy + (mol->ix[b] * sph + mol->iy[b] * cph), L);
+            } else {
+                x[gi] = wrap(hx + b * r0 * cph, L);
+                y[gi] = wrap(hy + b * r0 * sph, L);
+            }
             type[gi] = b < nH ? 1 : 2;
             if (next && b + 1 < ml) next[gi] = gi + 1;
             if (prev && b > 0) prev[gi] = gi - 1;

@@ -218,18 +218,26 @@ __device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepD
                                               long long qx, long long qy, int2 lk, const float2 (&pj)[2], float2 v,
                                               float &mb, uint32_t &key) {
     const float L = R.L, h = R.halfL, kb = R.kb, r0 = R.r0;
+    if (R.arch != 0) {  // branched lipids: the template terms of k_mol_forces
+        if (lk.x >= 0 || lk.y >= 0) {
+            const int2 q = b.fmol[g];
+            qx += q.x;
+            qy += q.y;
+        }
+    } else {
 #pragma unroll
-    for (int e = 0; e < 2; e++) {
-        const int j = e ? lk.y : lk.x;
-        if (j < 0) continue;
-        const float dx = minimg(__fsub_rn(pj[e].x, pi.x), L, h), dy = minimg(__fsub_rn(pj[e].y, pi.y), L, h);
-        const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
-        mb = fmaxf(mb, r);
-        const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
-        qx += f2fix16(__fmul_rn(fb, dx));
-        qy += f2fix16(__fmul_rn(fb, dy));
+        for (int e = 0; e < 2; e++) {
+            const int j = e ? lk.y : lk.x;
+            if (j < 0) continue;
+            const float dx = minimg(__fsub_rn(pj[e].x, pi.x), L, h), dy = minimg(__fsub_rn(pj[e].y, pi.y), L, h);
+            const float r = __fsqrt_rn(__fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+            mb = fmaxf(mb, r);
+            const float fb = __fdiv_rn(__fmul_rn(kb, __fsub_rn(r, r0)), r);
+            qx += f2fix16(__fmul_rn(fb, dx));
+            qy += f2fix16(__fmul_rn(fb, dy));
+        }
+        angle_terms(b, cur, R, pi, lk, pj[0], pj[1], qx, qy);
     }
-    angle_terms(b, cur, R, pi, lk, pj[0], pj[1], qx, qy);
     if (R.stir_A != 0.0f) qx += stir_force(R, pi.y, b.tg[cur][g] & GID_MASK, b.stir[rep]);
     const float2 fs = make_float2(fix16_to_f(qx), fix16_to_f(qy));
     if (!(isfinite(fs.x) && isfinite(fs.y))) raise_flag(b.status, DPD_F_NONFINITE);

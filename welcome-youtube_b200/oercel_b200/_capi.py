@@ -44,6 +44,23 @@ class DpdParams(C.Structure):
         ("p_rep_b", C.c_double), ("mu", C.c_double), ("p_ld", C.c_double), ("p_kd", C.c_double),
         ("p_nd", C.c_double), ("p_feed", C.c_double), ("feed_cap", C.c_double), ("vent_x", C.c_double),
         ("vent_y", C.c_double), ("vent_r", C.c_double), ("vent_w", C.c_double),
+        ("lip_arch", C.c_int32), ("lip_tie", C.c_int32), ("r0_head", C.c_double), ("k_head", C.c_double),
+        ("cos_head", C.c_double),
+    ]
+
+
+MAXML = 16
+MAXMB = 2 * MAXML
+
+
+class DpdTemplate(C.Structure):
+    _fields_ = [
+        ("arch", C.c_int32), ("mlen", C.c_int32), ("nH", C.c_int32), ("nb", C.c_int32), ("na", C.c_int32),
+        ("pad", C.c_int32), ("bi", C.c_int32 * MAXMB), ("bj", C.c_int32 * MAXMB), ("br0", C.c_double * MAXMB),
+        ("ai", C.c_int32 * MAXMB), ("aj", C.c_int32 * MAXMB), ("ak", C.c_int32 * MAXMB),
+        ("akind", C.c_int32 * MAXMB), ("aK", C.c_double * MAXMB), ("ac0", C.c_double * MAXMB),
+        ("px", C.c_double * MAXML), ("py", C.c_double * MAXML), ("ix", C.c_double * MAXML),
+        ("iy", C.c_double * MAXML),
     ]
 
 
@@ -70,7 +87,7 @@ EXPORTS = [
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
-    "dpd_set_rng", "dpd_get_rng",
+    "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template",
 ]
 NGRAD = 66
 
@@ -116,7 +133,8 @@ def load(path: str | None = None):
         "dpd_set_step": ([vp, i64], C.c_int),
         "dpd_step": ([vp, i64], C.c_int),
         "dpd_init_soup": ([dbl, i32, u64, dbl, dbl, i32, i32, dbl, dbl, dbl, dbl] + [fp] * 7
-                          + [C.POINTER(C.c_int32), fp], C.c_int),
+                          + [C.POINTER(C.c_int32), fp, C.POINTER(DpdTemplate)], C.c_int),
+        "dpd_lipid_template": ([C.POINTER(DpdParams), C.POINTER(DpdTemplate)], C.c_int),
         "dpd_set_rng": ([vp, i32, fp], C.c_int),
         "dpd_get_rng": ([vp, i32, fp], C.c_int),
         "dpd_build_cells": ([vp], C.c_int),

@@ -30,7 +30,7 @@ import time
 
 import numpy as np
 
-from .params import PDEFS, ParamError, Params, param_table, parse_override, read_ini
+from .params import ARCHS, PDEFS, ParamError, Params, param_table, parse_override, read_ini
 
 KINDS = ("grow", "brk", "bond", "syn", "rep", "mut", "dlip", "dK", "dN", "feed")
 CKPT_MAGIC = b"OCKB"
@@ -53,20 +53,54 @@ class Log:
         self.f.flush()
 
 
-def write_snapshot(path, state, step, time_, L):
-    """SPEC section 5: OCEL v1, positions and types in gid order, bonds (i < j)"""
+def template_bonds(state, mol):
+    """gid pairs of the template bonds of every molecule (a molecule starts at a
+    bead without prev and with next; its beads follow next in template order),
+    ordered by the gid of the bond's first template bead, then by template order
+    (write_snapshot, oercel.c:1859-1876)"""
+    g = state["gid"].astype(np.int64)
+    nx, pv = state["next"], state["prev"]
+    heads = np.nonzero((pv < 0) & (nx >= 0))[0]
+    ml = mol.mlen
+    sl = np.empty((len(heads), ml), np.int64)
+    sl[:, 0] = heads
+    for b in range(1, ml):
+        prevcol = sl[:, b - 1]
+        if np.any(nx[prevcol] < 0):
+            raise EngineError("broken lipid chain")
+        sl[:, b] = nx[prevcol]
+    keys, subs, lo, hi = [], [], [], []
+    for q in range(mol.nb):
+        gi, gj = g[sl[:, mol.bi[q]]], g[sl[:, mol.bj[q]]]
+        keys.append(gi)
+        subs.append(np.full(len(gi), q))
+        lo.append(np.minimum(gi, gj))
+        hi.append(np.maximum(gi, gj))
+    if not keys:
+        return np.zeros((0, 2), np.int32)
+    keys, subs, lo, hi = (np.concatenate(a) for a in (keys, subs, lo, hi))
+    order = np.lexsort((subs, keys))
+    return np.stack([lo[order], hi[order]], axis=1).astype(np.int32)
+
+
+def write_snapshot(path, state, step, time_, L, mol=None):
+    """SPEC section 5: OCEL v1, positions and types in gid order, bonds (i < j);
+    mol: the template of branched lipids (their bonds), None for linear chains"""
     n = len(state["x"])
     g = state["gid"].astype(np.int64)
     x = np.empty(n, np.float32)
     y = np.empty(n, np.float32)
     t = np.empty(n, np.uint8)
     x[g], y[g], t[g] = state["x"], state["y"], state["type"]
-    nx = state["next"]
-    has = nx >= 0
-    gi, gj = g[has], g[nx[has]]
-    order = np.lexsort((gj, gi))  # by the bond's chain-side (prev) bead, as the reference orders by template start
-    lo, hi = np.minimum(gi, gj)[order], np.maximum(gi, gj)[order]
-    bonds = np.stack([lo, hi], axis=1).astype(np.int32)
+    if mol is not None:
+        bonds = template_bonds(state, mol)
+    else:
+        nx = state["next"]
+        has = nx >= 0
+        gi, gj = g[has], g[nx[has]]
+        order = np.lexsort((gj, gi))  # by the bond's chain-side (prev) bead, as the reference orders by template start
+        lo, hi = np.minimum(gi, gj)[order], np.maximum(gi, gj)[order]
+        bonds = np.stack([lo, hi], axis=1).astype(np.int32)
     tmp = path + ".tmp"
     with open(tmp, "wb") as f:
         f.write(b"OCEL")
@@ -155,15 +189,17 @@ def read_ckpt(path):
 
 
 def read_reference_ckpt(path, b):
-    """the reference engine's checkpoint, version 2 (linear lipids; layout of
-    write_ckpt, oercel.c:1891-1936): continue a reference run on the GPU.  The
-    FP64 state is rounded to FP32; prev links are the inverse of nxt."""
+    """the reference engine's checkpoint, version 2 (linear lipids) or 3 (the
+    same with the lipid shape code after nH; layout of write_ckpt,
+    oercel.c:1891-1936): continue a reference run on the GPU.  The FP64 state
+    is rounded to FP32; prev links are the inverse of nxt."""
     ver, n, ml, nh = struct.unpack_from("<iiii", b, 4)
-    if ver != 2:
-        raise EngineError(f"{path}: reference checkpoint version {ver} (only version 2, linear lipids, is read)")
-    step, time_, L, seed = struct.unpack_from("<qddQ", b, 20)
-    rng = np.frombuffer(b, np.uint64, 4, 52).copy()
-    o = 20 + 32 + 32 + 8          # rng state, maxbond
+    if ver not in (2, 3):
+        raise EngineError(f"{path}: reference checkpoint version {ver} (versions 2 and 3 are read)")
+    arch, o0 = (struct.unpack_from("<i", b, 20)[0], 24) if ver == 3 else (0, 20)
+    step, time_, L, seed = struct.unpack_from("<qddQ", b, o0)
+    rng = np.frombuffer(b, np.uint64, 4, o0 + 32).copy()
+    o = o0 + 32 + 32 + 8          # rng state, maxbond
     warm_end, ta, sa, da = struct.unpack_from("<qdqd", b, o)
     o += 32 + 8                   # warm_end, anchors, soup seed
     gid = np.frombuffer(b, np.uint32, n, o).copy()
@@ -173,7 +209,7 @@ def read_reference_ckpt(path, b):
     nxt = np.frombuffer(b, np.int32, n, o).copy()
     o += 4 * n
     out = dict(N=n, step=step, time=time_, L=L, seed=seed, warm_end=warm_end, anchor=(ta, sa, da), gid=gid,
-               type=typ, next=nxt, rng=rng)
+               type=typ, next=nxt, rng=rng, arch=arch, mlen=ml, nH=nh)
     for k, ref in (("x", "x"), ("y", "y"), ("vhx", "vx"), ("vhy", "vy"), ("fx", "fx"), ("fy", "fy")):
         out[k] = np.frombuffer(b, np.float64, n, o).astype(np.float32)
         o += 8 * n
@@ -265,6 +301,8 @@ def _run(p, outdir, over):
             ck = read_ckpt(p.restart)
             if abs(ck["L"] - p.L) > 1e-12:
                 raise EngineError(f"checkpoint L={ck['L']:g} differs from parameter L={p.L:g}")
+            if "arch" in ck and (ck["arch"] != ARCHS.index(p.lip_arch) or ck["mlen"] != p.mlen()):
+                raise EngineError("checkpoint lipid architecture differs from parameters")
             seed = p.seed if p.restart_reseed else ck["seed"]
             if p.restart_reseed:
                 log(f"restart: reseeded with seed={p.seed} (branch, not an exact continuation)")
@@ -296,6 +334,7 @@ def _run(p, outdir, over):
     step0 = e.step_no
     n = e.n_beads[0]
     L = float(p.L)
+    mol = p.template() if p.lip_arch != "linear" else None  # the bonds of branched lipids in snapshots
     # params.ini (keep the previous one if a restart changed the parameters)
     pp = os.path.join(outdir, "params.ini")
     newp = pp + ".new"
@@ -363,11 +402,11 @@ def _run(p, outdir, over):
         if p.stats_every > 0:
             stats(0)
         if p.snap_every > 0:
-            write_snapshot(os.path.join(outdir, f"snap_{0:010d}.bin"), e.state(0), 0, 0.0, L)
+            write_snapshot(os.path.join(outdir, f"snap_{0:010d}.bin"), e.state(0), 0, 0.0, L, mol)
     elif p.snap_every > 0 and step0 % p.snap_every == 0:
         sp = os.path.join(outdir, f"snap_{step0:010d}.bin")
         if not os.path.exists(sp):
-            write_snapshot(sp, e.state(0), step0, tnow(step0), L)
+            write_snapshot(sp, e.state(0), step0, tnow(step0), L, mol)
     step = step0
     t_loop = time.time()
     t_last, step_last = t_loop, step
@@ -389,7 +428,7 @@ def _run(p, outdir, over):
             if not math.isfinite(o["T"]):
                 raise EngineError(f"non-finite temperature at step {step}")
         if p.snap_every > 0 and step % p.snap_every == 0:
-            write_snapshot(os.path.join(outdir, f"snap_{step:010d}.bin"), e.state(0), step, tnow(step), L)
+            write_snapshot(os.path.join(outdir, f"snap_{step:010d}.bin"), e.state(0), step, tnow(step), L, mol)
         if stop["flag"] is None and p.walltime > 0 and time.time() - t_start > p.walltime:
             stop["flag"] = "walltime"
         if (p.ckpt_every > 0 and step % p.ckpt_every == 0) or stop["flag"] or step >= p.steps:

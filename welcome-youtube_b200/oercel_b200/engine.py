@@ -20,9 +20,10 @@ from .params import Params
 EVENT_KINDS = ("grow", "brk", "bond", "syn", "rep", "mut", "dlip", "dK", "dN", "feed")
 
 
-def make_soup(L, N, seed, *, kT=1.0, r0=0.5, nH=1, nT=3, f_lip=0.10, f_Ka=0.0, f_Kb=0.0, c_N=0.12):
+def make_soup(L, N, seed, *, kT=1.0, r0=0.5, nH=1, nT=3, f_lip=0.10, f_Ka=0.0, f_Kb=0.0, c_N=0.12, mol=None):
     """The reference's random soup (same draws as init_soup/set_velocities) from
-    libdpd's host routine; float64 arrays in gid order."""
+    libdpd's host routine; float64 arrays in gid order.  mol: the lipid template
+    of a branched shape (Params.template()), None for linear lipids."""
     lib = load()
     x, y, vx, vy = (np.empty(N, np.float64) for _ in range(4))
     t = np.empty(N, np.uint8)
@@ -32,14 +33,16 @@ def make_soup(L, N, seed, *, kT=1.0, r0=0.5, nH=1, nT=3, f_lip=0.10, f_Ka=0.0, f
     rng = np.zeros(4, np.uint64)
     check(lib.dpd_init_soup(float(L), int(N), int(seed) & 0xFFFFFFFFFFFFFFFF, float(kT), float(r0), int(nH),
                             int(nT), float(f_lip), float(f_Ka), float(f_Kb), float(c_N), ptr(x), ptr(y), ptr(vx),
-                            ptr(vy), ptr(t), ptr(pv), ptr(nx), C.byref(nl), ptr(rng)))
+                            ptr(vy), ptr(t), ptr(pv), ptr(nx), C.byref(nl), ptr(rng),
+                            C.byref(mol) if mol is not None else None))
     return dict(x=x, y=y, vx=vx, vy=vy, type=t, prev=pv, next=nx, n_lipid_beads=nl.value, rng=rng)
 
 
 def soup_for(p: Params, seed=None):
     """soup of a parameter set (positions rounded to FP32 inside [0, L))"""
     s = make_soup(np.float32(p.L), p.n_beads(), p.seed if seed is None else seed, kT=p.kT, r0=p.r0,
-                  nH=p.lip_nH, nT=p.lip_nT, f_lip=p.f_lip, f_Ka=p.f_Ka, f_Kb=p.f_Kb, c_N=p.c_N)
+                  nH=p.lip_nH, nT=p.lip_nT, f_lip=p.f_lip, f_Ka=p.f_Ka, f_Kb=p.f_Kb, c_N=p.c_N,
+                  mol=p.template() if p.lip_arch != "linear" else None)
     L = np.float32(p.L)
     for k in ("x", "y"):
         v = s[k].astype(np.float32)

@@ -29,11 +29,12 @@ PDEFS = [
     ("k_angle", "float", "10", "angle constant, U = k (1 - cos theta) on consecutive chain triplets"),
     ("lip_nH", "int", "1", "head beads per lipid"),
     ("lip_nT", "int", "3", "tail beads per lipid"),
-    ("lip_arch", "str", "linear", "lipid shape (only linear is supported here)"),
-    ("r0_head", "float", "0.5", "branched lipids only (unused)"),
-    ("k_head", "float", "0", "branched lipids only (unused)"),
-    ("cos_head", "float", "0", "branched lipids only (unused)"),
-    ("lip_tie", "int", "0", "branched lipids only (unused)"),
+    ("lip_arch", "str", "linear", "lipid shape: linear, pi (two bonded heads, one tail each), y (one head, two "
+                                  "tails) or bola (a head pair and a third head joined by two tails)"),
+    ("r0_head", "float", "0.5", "pi / bola: rest length of the head-head bond and of pi's rungs"),
+    ("k_head", "float", "0", "pi / y / bola: junction angle term k_head (cos theta - cos_head)^2 (0 = none)"),
+    ("cos_head", "float", "0", "pi / y / bola: preferred cos of the junction angle"),
+    ("lip_tie", "int", "0", "pi / y / bola: rungs between the two tails (tail beads m = 1..lip_tie)"),
     ("syn_nN", "int", "0", "N consumed per new lipid (0 = one per lipid bead; the rest are the nearest W)"),
     ("steps", "long", "10000", "run until this step number"),
     ("snap_every", "long", "1000", "snapshot interval (0 = none)"),
@@ -91,6 +92,7 @@ PDEFS = [
     ("max_chain", "int", "12", "NEW longest chain growth may produce"),
 ]
 PKEYS = {k: (t, d, h) for k, t, d, h in PDEFS}
+ARCHS = ("linear", "pi", "y", "bola")
 REMOVED = {"seed_R", "seed_spacing", "seed_cN_in", "seed_nKa", "feed_every", "feed_grid", "feed_tmin"}
 
 
@@ -210,8 +212,12 @@ class Params:
             raise ParamError("dt must be > 0")
         if self.kT <= 0:
             raise ParamError("kT must be > 0")
-        if self.lip_arch != "linear":
-            raise ParamError("only lip_arch = linear is supported")
+        if self.lip_arch not in ARCHS:
+            raise ParamError("lip_arch must be linear, pi, y or bola")
+        if self.lip_arch != "linear" and self.lip_nT < 1:
+            raise ParamError("branched lipids need lip_nT >= 1")
+        if self.mlen() > 16:
+            raise ParamError("lipids of at most 16 beads")
         if self.k_angle < 0:
             raise ParamError("k_angle must be >= 0")
         if self.stir_n < 1:
@@ -234,10 +240,25 @@ class Params:
             raise ParamError("p_feed must be in [0, 1] and feed_cap in [0, 1)")
         if not (0 <= self.syn_nN <= self.lip_nH + self.lip_nT):
             raise ParamError("syn_nN must be 0..mlen")
+        if self.syn_tries > 64:
+            raise ParamError("syn_tries must be <= 64 (orientation trials held in shared memory)")
         return self
 
     def sigma(self):
         return math.sqrt(2.0 * self.gamma * self.kT)
+
+    def mlen(self):
+        """beads of one lipid (oercel.c:486-553)"""
+        nT = int(self.lip_nT)
+        return {"linear": int(self.lip_nH) + nT, "pi": 2 + 2 * nT, "y": 1 + 2 * nT, "bola": 3 + 2 * nT}.get(
+            self.lip_arch, int(self.lip_nH) + nT)
+
+    def template(self):
+        """the lipid molecule template (dpd_lipid_template): a DpdTemplate"""
+        from ._capi import DpdTemplate, check, load
+        t = DpdTemplate()
+        check(load().dpd_lipid_template(self.to_struct(), t))
+        return t
 
     def to_struct(self, seed=None, warm_end=None, t_anchor=0.0, step_anchor=0):
         from ._capi import DpdParams, load
@@ -270,6 +291,9 @@ class Params:
         s.chem_kind = 1 if self.chem_kind == "catalyst" else 0
         s.syn_tries, s.syn_relax, s.syn_nN = max(int(self.syn_tries), 1), int(self.syn_relax), int(self.syn_nN)
         s.lip_nH, s.lip_nT = int(self.lip_nH), int(self.lip_nT)
+        s.lip_arch = ARCHS.index(self.lip_arch) if self.lip_arch in ARCHS else -1
+        s.lip_tie = int(self.lip_tie)
+        s.r0_head, s.k_head, s.cos_head = float(self.r0_head), float(self.k_head), float(self.cos_head)
         s.feed_mode = {"none": 0, "0": 0, "uniform": 1, "vent": 2}[self.feed]
         s.vent_kind = {"disk": 0, "vstrip": 1, "hstrip": 2}[self.vent_shape]
         for k in ("r_cat", "p_syn_a", "p_syn_b", "p_rep_a", "p_rep_b", "mu", "p_ld", "p_kd", "p_nd", "p_feed",

@@ -72,6 +72,26 @@ def config5(n_replicas=64, seed=2027, a_wt=75.0):
             for b in range(n_replicas)]
 
 
+# The reference's big-soup experiment (cel/pc/plan.txt item 1: L = 512, a check every 10
+# steps, its chemistry rates and membranes.ini's composition) with linear H-T-T-T lipids,
+# the reference's default physics otherwise.  Every key is a reference key.
+CATALYST_PLAN = dict(L=512, chem=1, events=1, n_chem=10, lip_nH=1, lip_nT=3, f_lip=0.2, f_Ka=0.01, f_Kb=0.0,
+                     c_N=0.10, warmup=0, p_syn_a=3e-5, p_syn_b=1e-4, p_rep_a=1e-5, p_rep_b=1e-5, mu=0.02,
+                     p_ld=2e-6, p_kd=5e-6, p_nd=1e-6, feed="uniform", p_feed=1e-4, feed_cap=0.12)
+
+
+def catalyst_plan(seed=1, **kv):
+    """the catalyst chemistry workload: 786,432 beads, about 7,900 catalysts"""
+    return Params(**dict(CATALYST_PLAN, seed=seed, **kv))
+
+
+def catalyst_plan_ini(seed: int, steps: int, threads: int) -> str:
+    """the reference engine's ini for catalyst_plan(seed)"""
+    kv = dict(CATALYST_PLAN, seed=seed, steps=steps, threads=threads, snap_every=0, stats_every=steps,
+              ckpt_every=0, log_every=0)
+    return "".join(f"{k} = {v}\n" for k, v in kv.items())
+
+
 def reference_ini(p: Params, steps: int, threads: int) -> str:
     """the reference engine's ini for the physics of p (type 3 is its N; its
     catalyst chemistry is switched off: the lipid rules do not exist there)"""
