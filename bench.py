@@ -283,6 +283,29 @@ def batched_rates(torch, steps=64):
             "timing": "batched: CUDA events on the engine stream; one at a time: host clock around all engines"}
 
 
+def analysis_rates(eng, p, reps=5):
+    """tail-bead clusters and neighbour fraction of the bench box (the reference's
+    `snapcheck.py tclust`): dpd_type_clusters on the GPU against the CPU
+    restatement of the reference tool (scipy trees) on the same state"""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import analysis
+    eng.type_clusters(0, 2, 1.0)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        got = eng.type_clusters(0, 2, 1.0)
+    gpu_ms = (time.perf_counter() - t0) * 1000.0 / reps
+    st = eng.state(0)
+    t0 = time.perf_counter()
+    ref = analysis.type_clusters(st["x"], st["y"], st["type"], float(np.float32(p.L)), 2, 1.0)
+    cpu_ms = (time.perf_counter() - t0) * 1000.0
+    same = all(got[k] == ref[k] for k in ref)
+    return {"gpu_ms": gpu_ms, "cpu_ms": cpu_ms, "same_result": same, "beads": int(p.n_beads()), "t_beads": ref["n"],
+            "clusters": ref["clusters"], "timing": "host clock around each call (device synchronised); CPU: the "
+                                                    "oracle's restatement of the reference tool (scipy), 1 thread",
+            "kind": "port"}
+
+
 def catalyst_rates(torch, steps=200, ref_steps=40):
     """the reference's catalyst chemistry on its big-soup workload (786,432 beads,
     a check every 10 steps): bead-steps/s of whole steps, checks included, the
@@ -319,8 +342,9 @@ def catalyst_rates(torch, steps=200, ref_steps=40):
     ref_ms, t = run_reference(p, ref_steps, threads, workloads.catalyst_plan_ini(p.seed, ref_steps, threads))
     out = {"value": nb * 1000.0 / ms, "unit": UNIT, "ms_per_step": ms, "check_ms": check_ms, "steps": steps,
            "events": nev, "beads": nb, "catalysts": ncat,
-           "workload": "L=512 soup, linear H-T-T-T lipids, catalyst chemistry with the big-soup rates of the "
-                       "reference's experiment plan, a check every 10 steps (CUDA events, graphs)"}
+           "workload": "L=512 soup with the reference's membrane physics (membranes.ini: tied H2T2 pi lipids) and "
+                       "the big-soup chemistry rates of its experiment plan, a check every 10 steps (CUDA events, "
+                       "graphs)"}
     if ref_ms is not None:
         out["reference"] = {"value": nb * 1000.0 / ref_ms, "ms_per_step": ref_ms, "cores": threads,
                             "chem_ms_per_step": t["chem"],
@@ -437,6 +461,7 @@ def ours(args, rank, local_rank, ws):
     ach = KERNEL_BYTES[top] * nb / (kernels[top] / 1000.0) / 1e9
     traffic = profiled_traffic(top)
     n_plain, _ = eng.kernels_per_step()
+    ana = analysis_rates(eng, p) if (rank == 0 and not args.quick and not args.skip_cpu) else None
     eng.close()
     del flush
     res = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -458,6 +483,8 @@ def ours(args, rank, local_rank, ws):
         print(json.dumps(res))
         return
     if rank == 0:
+        if ana is not None:
+            res["analysis"] = ana
         res["e2e"] = e2e_rate(Engine, p, args.e2e_steps)
         if not args.skip_batched and ws == 1:
             res["batched"] = batched_rates(torch)

@@ -301,6 +301,17 @@ DPD_API int dpd_observables(dpd_handle *h, int32_t replica, double *out);
 /* the stats row only (out[3], the virial, is left 0): no pair loop */
 DPD_API int dpd_stats(dpd_handle *h, int32_t replica, double *out);
 
+/* Clusters of the beads of one type of replica r (the reference's analysis
+ * `snapcheck.py tclust`, cel/engine/tests/snapcheck.py:122-144): beads of the
+ * type within rcut (0 < rcut <= 1) of each other are joined; out[0] beads of
+ * the type, out[1] clusters, out[2] the largest, out[3] the sum of squared
+ * sizes (bead-weighted mean size = out[3] / out[0]), out[4] neighbours within
+ * 1.0 of the type's beads (any type, self excluded), out[5] those of the type
+ * (neighbour fraction = out[5] / out[4]).  Distances in FP64 from the FP32
+ * positions, <= as the reference's tree queries.  No counterpart call in the
+ * reference engine, whose analysis reads snapshots on the CPU. */
+DPD_API int dpd_type_clusters(dpd_handle *h, int32_t replica, int32_t type, double rcut, int64_t *out);
+
 /* Histogram (nbin bins on [0, rmax), rmax <= 3) of distances between beads of
  * types ta and tb of replica r, each unordered pair once. */
 DPD_API int dpd_pair_hist(dpd_handle *h, int32_t replica, int32_t ta, int32_t tb, double rmax, int32_t nbin, double *hist);

@@ -18,6 +18,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = "/root/reference"  # the reference checkout this generator reads (fixtures are made here only)
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import oracle as O  # noqa: E402
 
@@ -207,6 +208,32 @@ def mol_fixture(name, seed, **over):
     np.savez_compressed(os.path.join(HERE, name), **out)
 
 
+def tclust_fixture():
+    """the reference's `snapcheck.py tclust` output (its printed line) on the
+    reference snapshots of the run fixtures, with the snapshots' positions"""
+    import contextlib
+    import io
+    import tempfile
+    sys.path.insert(0, os.path.join(REF_ROOT, "cel", "engine", "tests"))
+    import snapcheck
+    out = {}
+    cases = [("run_L10_seed3.npz", "snap_24"), ("run_cat_L16_seed5.npz", "snap_24"), ("run_pi_L16_seed7.npz", "snap_24"),
+             ("run_extras_L10_seed4.npz", "snap_36")]
+    for k, (name, key) in enumerate(cases):
+        g = np.load(os.path.join(HERE, name))
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "s.bin")
+            with open(path, "wb") as f:
+                f.write(bytes(g[key]))
+            buf = io.StringIO()
+            with contextlib.redirect_stdout(buf):
+                snapcheck.cmd_tclust(path)
+            s = snapcheck.read_snap(path)
+        out[f"c{k}_line"] = np.frombuffer(buf.getvalue().strip().encode(), np.uint8)
+        out[f"c{k}_snap"] = g[key]
+    np.savez_compressed(os.path.join(HERE, "tclust.npz"), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -339,5 +366,6 @@ if __name__ == "__main__":
     catalyst_fixture("catalyst_L16_seed12.npz", 12, 21)
     catalyst_fixture("catalyst_vent_L16_seed13.npz", 13, 21, syn_nN=2, feed="vent", vent_shape="disk", vent_r=4,
                      feed_cap=0.3)
+    tclust_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -278,3 +278,26 @@ def test_template_bonded_forces_match_reference(name):
     assert np.abs(fx - g["fx"]).max() <= 1e-12 * scale and np.abs(fy - g["fy"]).max() <= 1e-12 * scale
     assert mb == pytest.approx(float(g["maxbond"]), rel=1e-14)
     assert abs(fx.sum()) < 1e-9 and abs(fy.sum()) < 1e-9
+
+
+def tclust_cases():
+    g = golden("tclust.npz")
+    k = 0
+    while f"c{k}_line" in g:
+        yield bytes(g[f"c{k}_line"]).decode(), bytes(g[f"c{k}_snap"])
+        k += 1
+
+
+@pytest.mark.parametrize("line, snap", list(tclust_cases()))
+def test_cluster_analysis_matches_the_reference_tool(tmp_path, line, snap):
+    """the restatement of `snapcheck.py tclust` against the reference tool's own
+    output on reference snapshots"""
+    import analysis
+    from oercel_b200 import cli
+    p = tmp_path / "s.bin"
+    p.write_bytes(snap)
+    s = cli.read_snapshot(str(p))
+    r = analysis.type_clusters(s["x"], s["y"], s["type"], s["L"])
+    mine = (f"step={s['step']} nT={r['n']} clusters={r['clusters']} largest={r['largest']} mean size "
+            f"(bead-weighted)={r['sum_sq'] / r['n']:.1f}  T-neighbour fraction={r['nb_same'] / r['nb_all']:.3f}")
+    assert mine == line

@@ -69,6 +69,9 @@ struct dpd_handle {
     int adj_nck = 0, adj_nseg = 0;
     // staging for state in/out
     char *stage = nullptr;
+    // cluster analysis scratch (allocated on first use): union-find parents, sizes, sums
+    int *ana_parent = nullptr, *ana_size = nullptr;
+    unsigned long long *ana_acc = nullptr;
     std::vector<void *> allocs;
 };
 
@@ -504,6 +507,7 @@ static int check_status(dpd_handle *h) {
     if (st.flags) {
         CK(cudaMemsetAsync(&h->b.status->flags, 0, sizeof(unsigned), h->s));
         CK(cudaStreamSynchronize(h->s));
+        if (st.flags & DPD_F_ANALYSIS) return fail(DPD_E_STATE, "cluster analysis did not converge");
         if (st.flags & DPD_F_CATALYST)
             return fail(DPD_E_STATE, "a catalyst's neighbourhood did not fit the staging area, or a search found "
                                      "more than 256 candidates or 512 relaxation neighbours (too crowded)");
@@ -944,6 +948,31 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     h->step += 1;
     *n_out = nk;
     return check_status(h);
+}
+
+extern "C" int dpd_type_clusters(dpd_handle *h, int32_t r, int32_t type, double rcut, int64_t *out) {
+    TRY(ensure_replica(h, r));
+    if (!out) return fail(DPD_E_ARG, "null output");
+    if (type < 0 || type >= DPD_MAXT) return fail(DPD_E_ARG, "type must be 0..%d", DPD_MAXT - 1);
+    if (!(rcut > 0.0 && rcut <= 1.0)) return fail(DPD_E_ARG, "rcut must be in (0, 1]");
+    if (!h->ana_parent) {
+        TRY(dalloc(h, &h->ana_parent, (size_t)h->N));
+        TRY(dalloc(h, &h->ana_size, (size_t)h->N));
+        TRY(dalloc(h, &h->ana_acc, 8));
+    }
+    launch_type_clusters(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, type, rcut, h->ana_parent, h->ana_size,
+                         h->ana_acc, h->s);
+    CK(cudaGetLastError());
+    unsigned long long acc[8];
+    CK(cudaMemcpyAsync(acc, h->ana_acc, sizeof acc, cudaMemcpyDeviceToHost, h->s));
+    TRY(check_status(h));
+    out[0] = (int64_t)acc[4];  // beads of the type (the sum of the cluster sizes)
+    out[1] = (int64_t)acc[2];  // clusters
+    out[2] = (int64_t)acc[5];  // largest cluster
+    out[3] = (int64_t)acc[3];  // sum of squared cluster sizes
+    out[4] = (int64_t)acc[0];  // neighbours within 1 of the type's beads, all types
+    out[5] = (int64_t)acc[1];  // the same, of the type
+    return DPD_OK;
 }
 
 extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out) {

@@ -40,6 +40,7 @@
 #define DPD_F_FORCE 0x40u       // a single pair or bond force term above the fixed-point range
 #define DPD_F_CATALYST 0x80u    // a catalyst's neighbourhood exceeded the staging capacity
 #define DPD_CAT_MAXTR 64        // orientation trials of one lipid synthesis (syn_tries)
+#define DPD_F_ANALYSIS 0x200u   // a cluster union kept losing its compare-and-swap (analysis result invalid)
 
 struct RepDev {                 // constants of one replica, read by every kernel
     float L, halfL;
@@ -214,6 +215,8 @@ void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s);
 void launch_mol_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
+void launch_type_clusters(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int t,
+                          double rcut, int *parent, int *size, unsigned long long *acc, cudaStream_t s);
 void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
                    int64_t C, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,

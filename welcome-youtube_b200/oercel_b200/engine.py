@@ -231,6 +231,15 @@ class Engine:
         return dict(T=o[0], px=o[1], py=o[2], virial=o[3], maxbond=o[4], n_chains=int(o[5]),
                     counts=o[8:16].astype(np.int64))
 
+    def type_clusters(self, replica=0, type=2, rcut=1.0):
+        """clusters of the beads of `type` joined within rcut, and their neighbour
+        fraction within 1.0 (the reference's `snapcheck.py tclust`)"""
+        out = np.zeros(6, np.int64)
+        check(self.lib.dpd_type_clusters(self.h, int(replica), int(type), float(rcut), ptr(out)))
+        n, nc, largest, sq, nb_all, nb_same = (int(v) for v in out)
+        return dict(n=n, clusters=nc, largest=largest, sum_sq=sq, mean_size=sq / max(n, 1), nb_all=nb_all,
+                    nb_same=nb_same, fraction=nb_same / max(nb_all, 1))
+
     def pair_hist(self, replica, ta, tb, rmax, nbin):
         h = np.zeros(nbin)
         check(self.lib.dpd_pair_hist(self.h, replica, ta, tb, float(rmax), nbin, ptr(h)))

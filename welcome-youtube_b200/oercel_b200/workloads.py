@@ -72,17 +72,21 @@ def config5(n_replicas=64, seed=2027, a_wt=75.0):
             for b in range(n_replicas)]
 
 
-# The reference's big-soup experiment (cel/pc/plan.txt item 1: L = 512, a check every 10
-# steps, its chemistry rates and membranes.ini's composition) with linear H-T-T-T lipids,
-# the reference's default physics otherwise.  Every key is a reference key.
-CATALYST_PLAN = dict(L=512, chem=1, events=1, n_chem=10, lip_nH=1, lip_nT=3, f_lip=0.2, f_Ka=0.01, f_Kb=0.0,
-                     c_N=0.10, warmup=0, p_syn_a=3e-5, p_syn_b=1e-4, p_rep_a=1e-5, p_rep_b=1e-5, mu=0.02,
-                     p_ld=2e-6, p_kd=5e-6, p_nd=1e-6, feed="uniform", p_feed=1e-4, feed_cap=0.12)
+# The reference's big-soup experiment (cel/pc/plan.txt item 1): a random soup of L = 512
+# with the membrane physics of cel/engine/params/membranes.ini (tied H2T2 pi lipids, the
+# demixing repulsions) and the plan's chemistry rates, a check every 10 steps.  Every key
+# is a reference key.
+CATALYST_PLAN = dict(L=512, dt=0.03, kT=1, gamma=4.5, warmup=3000, f_lip=0.20, f_Ka=0.01, f_Kb=0, c_N=0.10,
+                     lip_arch="pi", lip_nT=1, lip_tie=1, r0_head=0.7, k_head=0, k_bond=300, r0=0.5, k_angle=15,
+                     syn_nN=0, a_W_H=20, a_W_T=200, a_H_T=50, a_W_N=45, a_H_N=22, a_T_N=120, a_W_K=45, a_H_K=30,
+                     a_T_K=200, chem=1, events=1, n_chem=10, p_syn_a=3e-5, p_syn_b=1e-4, p_rep_a=1e-5,
+                     p_rep_b=1e-5, mu=0.02, p_ld=2e-6, p_kd=5e-6, p_nd=1e-6, feed="uniform", p_feed=1e-4,
+                     feed_cap=0.12)
 
 
 def catalyst_plan(seed=1, **kv):
     """the catalyst chemistry workload: 786,432 beads, about 7,900 catalysts"""
-    return Params(**dict(CATALYST_PLAN, seed=seed, **kv))
+    return Params().update([(k, str(v)) for k, v in dict(CATALYST_PLAN, seed=seed, **kv).items()])
 
 
 def catalyst_plan_ini(seed: int, steps: int, threads: int) -> str:
