@@ -263,6 +263,12 @@ DPD_API int dpd_init_soup(double L, int32_t N, uint64_t seed, double kT, double 
                           double *vy, uint8_t *type, int32_t *prev, int32_t *next, int32_t *n_lipid_beads,
                           uint64_t *rng_out, const dpd_template *mol);
 
+/* The xoshiro256** state n draws after `state` (out may equal state), by a
+ * jump through the generator's characteristic polynomial; the catalyst check
+ * uses the same jumps to draw its stream in parallel.  No counterpart call in
+ * the reference, which draws serially. */
+DPD_API int dpd_xoshiro_jump(const uint64_t *state, uint64_t n, uint64_t *out);
+
 /* The serial xoshiro256** state of the catalyst chemistry of replica r
  * (4 words; the reference's Sys.rng, checkpointed with the state). */
 DPD_API int dpd_set_rng(dpd_handle *h, int32_t replica, const uint64_t *state);

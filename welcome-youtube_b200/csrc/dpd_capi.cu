@@ -62,6 +62,7 @@ struct dpd_handle {
     // the reference's catalyst chemistry: replicas with chem_kind 1, the period of their checks
     bool any_cat = false, any_lipid = false;
     bool any_mol = false;       // some replica has branched lipids (k_mol_forces)
+    int stream_grid = 1;        // blocks per replica of the catalyst stream kernel
     int64_t cat_period = 0;
     // reverse-mode storage, grown on demand (full checkpoints, the states of one
     // recomputed segment, adjoint arrays in gid order)
@@ -426,6 +427,29 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.cat_cell, N));
     TRY(dalloc(h, &b.cat_mark, C));
     TRY(dalloc(h, &b.fmol, N));
+    if (h->any_cat) {
+        // the catalyst checks' draw streams: 3 n + 4096 draws per replica, 64-draw blocks
+        long long so = 0;
+        int nblk = 1;
+        for (int r = 0; r < nrep; r++) {
+            const int dcap = (int)((3ll * h->rh[r].n + 4096 + 63) / 64 * 64);
+            h->rh[r].so = so;
+            h->rh[r].dcap = dcap;
+            so += dcap;
+            nblk = std::max(nblk, dcap / 64);
+        }
+        CK(cudaMemcpy(h->d_rep, h->rh.data(), (size_t)nrep * sizeof(RepDev), cudaMemcpyHostToDevice));
+        std::vector<uint64_t> jt;
+        if (jump_table(nblk, jt) != 0) return fail(DPD_E_STATE, "xoshiro256** polynomial not found");
+        uint64_t *dj = nullptr;
+        TRY(dalloc(h, &dj, jt.size()));
+        CK(cudaMemcpy(dj, jt.data(), jt.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        b.jump = dj;
+        TRY(dalloc(h, &b.stream, (size_t)so));
+        TRY(dalloc(h, &b.sblock, (size_t)so / 16));
+        TRY(dalloc(h, &b.cat_dn, (size_t)nrep));
+        h->stream_grid = (nblk + 255) / 256;
+    }
     {
         std::vector<dpd_template> mols(nrep);
         for (int r = 0; r < nrep; r++)
@@ -754,7 +778,7 @@ extern "C" int dpd_chemistry(dpd_handle *h, int64_t step) {
     launch_chem_scan(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
     // the catalyst chemistry as the reference's chemistry(): no sort afterwards
-    if (h->any_cat) launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->s);
+    if (h->any_cat) launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->stream_grid, h->s);
     CK(cudaGetLastError());
     return check_status(h);
 }
@@ -791,7 +815,7 @@ static void enqueue_step(dpd_handle *h, int64_t s) {
     if (h->any_lipid) launch_chem_lists(h->b, h->cur, h->d_rep, -1, h->s);
     if (cat) {
         launch_resort(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->d_cch, h->ncch, h->C, h->s);
-        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->s);
+        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->stream_grid, h->s);
         enqueue_sort(h, PERM_SORT);
     }
     enqueue_forces(h, true);
@@ -935,7 +959,7 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
         }
     if (cat) {
         launch_resort(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->d_cch, h->ncch, h->C, h->s);
-        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->s);
+        launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->stream_grid, h->s);
         enqueue_sort(h, PERM_SORT);
         CK(cudaEventRecord(ev[k++], h->s));
     }
@@ -1083,6 +1107,8 @@ extern "C" int dpd_set_params(dpd_handle *h, int32_t r, const dpd_params *p) {
     if (R.ncx != old.ncx || R.L != old.L) return fail(DPD_E_ARG, "dpd_set_params cannot change the box size");
     R.ch0 = old.ch0;
     R.nch = old.nch;
+    R.so = old.so;
+    R.dcap = old.dcap;
     if ((p->chem && p->chem_kind == 1) != (h->params[r].chem && h->params[r].chem_kind == 1) && !h->any_cat)
         return fail(DPD_E_ARG, "dpd_set_params cannot switch the catalyst chemistry on: create the handle with it");
     if (p->lip_arch != 0 && !h->any_mol)

@@ -34,9 +34,9 @@
 #define CAT_MARGIN 0.5   // oercel.c:1348
 #define CAT_WIN 1024     // catalysts per window of the walk
 #define CAT_MAXTR DPD_CAT_MAXTR
-#define CAT_SHUF_RUN 256 // swap partners drawn ahead by the shuffle's first warp
 // what the walk does with a catalyst: no draws (fewer than 2 N), the replication
 // draw, the synthesis and replication draws, or a visit by the whole CTA
+#define CAT_SHUF_RUN 2048  // shuffle steps whose partners are staged at a time
 #define WALK_NONE 0
 #define WALK_REP 1
 #define WALK_SYN 2
@@ -74,6 +74,9 @@ struct CatSmem {
     uint64_t rng[4];
     int32_t go, k, var, ml;
     int32_t over;                        // a search found more than CAT_MAXNB candidates
+    int32_t nd;                          // draws of the current visit
+    int32_t serial, first, exhaust;      // walk state: serial mode, first stop of a segment, stop reason
+    long long P, fpos;                   // stream position of the walk, of the first stop
     double tux[CAT_MAXTR], tuy[CAT_MAXTR], tU[CAT_MAXTR];  // trial directions of a synthesis, their energies
     int32_t nchg;                        // beads whose type the current visit changed
     float2 chg[CAT_MAXML + 2];           // and their positions before the change
@@ -291,6 +294,12 @@ __device__ __forceinline__ void place(const RepDev &R, const dpd_template &M, in
         px = dwrap(cx0 + (M.px[bb] * ux - M.py[bb] * uy), L);
         py = dwrap(cy0 + (M.px[bb] * uy + M.py[bb] * ux), L);
     }
+}
+
+// a draw of the visit from the generator state S.rng, counted (thread 0)
+__device__ __forceinline__ double draw(CatSmem &S) {
+    S.nd++;
+    return xo_unif(S.rng);
 }
 
 __device__ __forceinline__ bool in_chain(const CatSmem &S, int i, int ml) {
@@ -566,63 +575,109 @@ __global__ void __launch_bounds__(BEAD_TPB) k_cat_list(Bufs b, int cur, const Re
     if (v) b.cat_list[R.b0 + before + __popc(m & ((1u << lane_id()) - 1u))] = d;
 }
 
-// the catalyst list of one replica shuffled with its serial generator
-// (oercel.c:1571-1580), the list in shared memory while it fits (shmax
-// entries); also the replica's catalyst count.  Two warps pipeline the
-// Fisher-Yates loop: lane 0 of warp 0 draws the next CAT_SHUF_RUN swap
-// partners while lane 0 of warp 1 applies the previous run's swaps, so the
-// draws and the swaps are those of the serial loop.
-__global__ void __launch_bounds__(64) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int shmax) {
+// The draws of one check (per replica): draw p is the output of T^p s0, s0
+// the generator state at the check's start, T one step.  One thread per block
+// of 64 draws starts at T^(64 m) s0 by the jump table (x^(64 m) mod the
+// generator's characteristic polynomial, dpd_jump.cu), then steps.  The
+// shuffle takes nk - 1 draws and the walk at most two per catalyst plus those
+// of its events; 3 nk + 4096 draws are made (the walk goes on serially past
+// them).  Block start states are kept for the walk's visits.
+__global__ void __launch_bounds__(256) k_cat_stream(Bufs b, const RepDev *__restrict__ reps) {
+    __shared__ int red[8];
+    const int rep = (int)blockIdx.y;
+    const RepDev &R = reps[rep];
+    if (!cat_due(R, *b.step)) return;
+    const int tid = (int)threadIdx.x;
+    int n = 0;
+    for (int k = tid; k < R.nch; k += 256) n += b.cat_cnt[R.ch0 + k];
+    n = __reduce_add_sync(0xffffffffu, n);
+    if (lane_id() == 0) red[tid >> 5] = n;
+    __syncthreads();
+    int nk = 0;
+    for (int w = 0; w < 8; w++) nk += red[w];
+    const long long D = min((long long)R.dcap, (3ll * nk + 4096 + 63) / 64 * 64);
+    if (blockIdx.x == 0 && tid == 0) {
+        b.cat_nk[rep] = nk;
+        b.cat_dn[rep] = D;
+    }
+    uint64_t s0[4];
+    for (int q = 0; q < 4; q++) s0[q] = b.rng[4 * rep + q];
+    for (long long m = (long long)blockIdx.x * 256 + tid; m < D / 64; m += (long long)gridDim.x * 256) {
+        const uint64_t *J = b.jump + 4 * m;
+        uint64_t t[4] = {s0[0], s0[1], s0[2], s0[3]}, acc[4] = {0, 0, 0, 0};
+        for (int w = 0; w < 4; w++) {
+            const uint64_t jw = J[w];
+            for (int bit = 0; bit < 64; bit++) {
+                if ((jw >> bit) & 1) {
+                    acc[0] ^= t[0];
+                    acc[1] ^= t[1];
+                    acc[2] ^= t[2];
+                    acc[3] ^= t[3];
+                }
+                xo_next(t);
+            }
+        }
+        uint64_t *bs = b.sblock + 4 * (R.so / 64 + m);
+        for (int q = 0; q < 4; q++) bs[q] = acc[q];
+        uint64_t *out = b.stream + R.so + 64 * m;
+        for (int j = 0; j < 64; j++) out[j] = xo_next(acc);
+    }
+}
+
+// the generator state at draw p of the replica's stream (p < its length)
+__device__ __forceinline__ void state_at(const Bufs &b, const RepDev &R, long long p, uint64_t *s) {
+    const uint64_t *bs = b.sblock + 4 * (R.so / 64 + p / 64);
+    for (int q = 0; q < 4; q++) s[q] = __ldcg(bs + q);
+    for (int k = 0; k < (int)(p % 64); k++) xo_next(s);
+}
+
+// the catalyst list of one replica shuffled as the serial generator does it
+// (oercel.c:1571-1580): step i = nk-1 .. 1 swaps entries i and xo_below(i + 1)
+// of draw nk-1-i.  The block computes the swap partners of a run of steps
+// from the stream into shared memory, then one thread applies them; the list
+// is in shared memory while it fits (shmax entries).
+__device__ __forceinline__ int swap_partner(const uint64_t *st, int nk, int i) {
+    const double u = (double)(__ldcg(st + (nk - 1 - i)) >> 11) * 0x1.0p-53;
+    const long long k = (long long)(u * (double)(i + 1));
+    return (int)(k >= i + 1 ? i : k);
+}
+
+__global__ void __launch_bounds__(256) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int shmax) {
     extern __shared__ int32_t shl[];
-    __shared__ int32_t part[2][CAT_SHUF_RUN];
-    __shared__ int nks;
+    __shared__ int32_t spart[CAT_SHUF_RUN];
     const int rep = (int)blockIdx.x;
     const RepDev &R = reps[rep];
     if (!cat_due(R, *b.step)) return;
-    const int tid = (int)threadIdx.x, warp = tid >> 5, lane = (int)lane_id();
-    if (warp == 0) {
-        int n = 0;
-        for (int k = lane; k < R.nch; k += 32) n += b.cat_cnt[R.ch0 + k];
-        n = __reduce_add_sync(0xffffffffu, n);
-        if (lane == 0) {
-            nks = n;
-            b.cat_nk[rep] = n;
-        }
-    }
-    __syncthreads();
-    const int nk = nks;
+    const int tid = (int)threadIdx.x;
+    const int nk = b.cat_nk[rep];
     int32_t *list = b.cat_list + R.b0;
+    const uint64_t *st = b.stream + R.so;
     const bool sh = nk <= shmax;
-    int32_t *a = sh ? shl : list;
     if (sh)
-        for (int i = tid; i < nk; i += 64) shl[i] = list[i];
-    // swaps i = nk-1 .. 1; run r holds i = nk-1 - r*RUN - j, j < RUN
-    const int nswap = nk > 1 ? nk - 1 : 0, nrun = (nswap + CAT_SHUF_RUN - 1) / CAT_SHUF_RUN;
-    uint64_t st[4];
-    if (tid == 0)
-        for (int q = 0; q < 4; q++) st[q] = b.rng[4 * rep + q];
-    for (int r = 0; r <= nrun; r++) {
-        if (tid == 0 && r < nrun)  // draw run r
-            for (int j = 0; j < CAT_SHUF_RUN; j++) {
-                const int i = nk - 1 - r * CAT_SHUF_RUN - j;
-                if (i <= 0) break;
-                part[r & 1][j] = (int)xo_below(st, i + 1);
+        for (int i = tid; i < nk; i += 256) shl[i] = list[i];
+    for (int hi = nk - 1; hi > 0; hi -= CAT_SHUF_RUN) {
+        const int lo = max(1, hi - CAT_SHUF_RUN + 1);
+        for (int i = lo + tid; i <= hi; i += 256) spart[i - lo] = swap_partner(st, nk, i);
+        __syncthreads();
+        if (tid == 0) {
+            if (sh) {
+                for (int i = hi; i >= lo; i--) {
+                    const int c = spart[i - lo], t = shl[i];
+                    shl[i] = shl[c];
+                    shl[c] = t;
+                }
+            } else {
+                for (int i = hi; i >= lo; i--) {
+                    const int c = spart[i - lo], t = list[i];
+                    list[i] = list[c];
+                    list[c] = t;
+                }
             }
-        if (tid == 32 && r > 0)  // apply run r - 1
-            for (int j = 0; j < CAT_SHUF_RUN; j++) {
-                const int i = nk - 1 - (r - 1) * CAT_SHUF_RUN - j;
-                if (i <= 0) break;
-                const int c = part[(r - 1) & 1][j];
-                const int t = a[i];
-                a[i] = a[c];
-                a[c] = t;
-            }
+        }
         __syncthreads();
     }
-    if (tid == 0)
-        for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = st[q];
     if (sh)
-        for (int i = tid; i < nk; i += 64) list[i] = shl[i];
+        for (int i = tid; i < nk; i += 256) list[i] = shl[i];
 }
 
 // per catalyst (a warp each, its lanes over the cells of the search window):
@@ -711,7 +766,7 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
     __syncthreads();
     const int nw = S.nw;
     int used = 0;
-    if (tid == 0) S.go = nn >= nsynN && nsynN + nw >= ml && xo_unif(S.rng) < (var ? R.p_syn_b : R.p_syn_a);
+    if (tid == 0) S.go = nn >= nsynN && nsynN + nw >= ml && draw(S) < (var ? R.p_syn_b : R.p_syn_a);
     __syncthreads();
     if (S.go) {
         // synthesis: the nsynN nearest N, then the nearest W
@@ -734,7 +789,7 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
         const int ntr = R.syn_tries;
         if (tid == 0)
             for (int tr = 0; tr < ntr; tr++) {
-                const double phi = 2.0 * M_PI * xo_unif(S.rng);
+                const double phi = 2.0 * M_PI * draw(S);
                 S.tux[tr] = cos(phi);
                 S.tuy[tr] = sin(phi);
             }
@@ -793,9 +848,9 @@ __device__ void visit(CatSmem &S, const Bufs &b, int cur, const RepDev &R, int r
         used = nsynN;
     }
     // replication onto the next two nearest N, with mutation
-    if (tid == 0 && nn - used >= 2 && xo_unif(S.rng) < (var ? R.p_rep_b : R.p_rep_a)) {
+    if (tid == 0 && nn - used >= 2 && draw(S) < (var ? R.p_rep_b : R.p_rep_a)) {
         int nv = var, mut = 0;
-        if (xo_unif(S.rng) < R.mu) {
+        if (draw(S) < R.mu) {
             nv = 1 - var;
             mut = 1;
         }
@@ -826,10 +881,14 @@ __device__ __forceinline__ uint8_t walk_code(uint32_t v, uint8_t dirty, int nsyn
 // The catalysts of one replica, one after the other in the shuffled order
 // (oercel.c:1582-1655).  Most visits end without an event: their decisions
 // need only the draws and the two candidate counts, which k_cat_near found
-// before the walk.  So thread 0 walks a window of the list on those counts with
-// a copy of the generator, and hands a catalyst to the whole CTA (visit(), the
-// generator state from before its draws) when its draws give an event, or when
-// an earlier event in this check changed a bead near it (cell marks).  The
+// before the walk.  A catalyst's draws are the next 0 (fewer than 2 N), 1
+// (replication) or 2 (synthesis, replication) of the check's stream, so a
+// block-wide prefix sum over a window of the walk gives every catalyst its
+// draw positions and the decisions are made in parallel; the first catalyst
+// whose draws give an event, or near which an earlier event changed a bead
+// (cell marks), is visited by the whole CTA (visit(), from the generator state
+// at its position), which counts the draws it takes, and the walk goes on
+// after it.  Past the end of the stream, thread 0 walks on serially.  The
 // draws, their order and every decision are those of visiting each catalyst
 // in full.
 __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const RepDev *__restrict__ reps) {
@@ -842,9 +901,11 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
     const int tid = (int)threadIdx.x;
     const int ml = R.lip_nH + R.lip_nT, nsynN = R.syn_nN > 0 ? R.syn_nN : ml;
     const int nk = b.cat_nk[rep];
+    const long long D = b.cat_dn[rep];
     const int32_t *list = b.cat_list + R.b0;
     const uint32_t *near = b.cat_near + R.b0;
     const int32_t *cell = b.cat_cell + R.b0;
+    const uint64_t *st = b.stream + R.so;
     uint8_t *mark = b.cat_mark;
     const uint64_t tsyn[2] = {u01_threshold(R.p_syn_a), u01_threshold(R.p_syn_b)};
     const uint64_t trep[2] = {u01_threshold(R.p_rep_a), u01_threshold(R.p_rep_b)};
@@ -854,7 +915,8 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
     const int mcol = 2 * mx + 1 >= R.ncx ? R.ncx : 2 * mx + 1, mrow = 2 * my + 1 >= R.ncy ? R.ncy : 2 * my + 1;
     if (tid == 0) {
         S.over = 0;
-        for (int q = 0; q < 4; q++) S.rng[q] = b.rng[4 * rep + q];
+        S.serial = 0;
+        S.P = nk > 0 ? nk - 1 : 0;  // after the shuffle's draws
     }
     bool overflow = false;
     for (int w0 = 0; w0 < nk; w0 += CAT_WIN) {
@@ -867,27 +929,91 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
         __syncthreads();
         int i = 0;
         while (true) {
-            if (tid == 0) {
-                uint64_t r[4] = {S.rng[0], S.rng[1], S.rng[2], S.rng[3]};
-                for (; i < wn; i++) {
-                    const int code = S.wcode[i], kind = code & 3, var = code >> 2;
-                    if (kind == WALK_NONE) continue;
-                    if (kind == WALK_VISIT) break;
-                    uint64_t t[4] = {r[0], r[1], r[2], r[3]};
-                    if (kind == WALK_SYN && (xo_next(t) >> 11) < tsyn[var]) break;
-                    if ((xo_next(t) >> 11) < trep[var]) break;
-                    r[0] = t[0];
-                    r[1] = t[1];
-                    r[2] = t[2];
-                    r[3] = t[3];
+            if (!S.serial) {
+                // entries i .. wn-1: CAT_WIN / CAT_TPB consecutive ones per thread
+                constexpr int PER = CAT_WIN / CAT_TPB;
+                const int q0 = i + tid * PER;
+                int nd[PER], tot = 0;
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    const int q = q0 + e, kind = q < wn ? S.wcode[q] & 3 : WALK_NONE;
+                    nd[e] = kind == WALK_SYN ? 2 : kind == WALK_REP ? 1 : 0;
+                    tot += nd[e];
                 }
-                for (int q = 0; q < 4; q++) S.rng[q] = r[q];
-                S.k = i;
+                int total;
+                long long pos = S.P + block_excl_scan(S, tot, total);
+                if (tid == 0) {
+                    S.first = wn;
+                    S.exhaust = 0;
+                }
+                __syncthreads();
+                int mine = wn;
+                long long mpos = 0;
+                bool mex = false;
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    const int q = q0 + e;
+                    if (q >= wn || mine < wn) break;
+                    const int code = S.wcode[q], kind = code & 3, var = code >> 2;
+                    bool stop = kind == WALK_VISIT;
+                    if (!stop && nd[e] > 0) {
+                        if (pos + 2 > D - 128) {
+                            stop = true;
+                            mex = true;
+                        } else {
+                            stop = (kind == WALK_SYN && (__ldcg(st + pos) >> 11) < tsyn[var]) ||
+                                   (__ldcg(st + pos + (kind == WALK_SYN)) >> 11) < trep[var];
+                        }
+                    }
+                    if (stop) {
+                        mine = q;
+                        mpos = pos;
+                    }
+                    pos += nd[e];
+                }
+                if (mine < wn) atomicMin(&S.first, mine);
+                __syncthreads();
+                if (mine < wn && mine == S.first) {
+                    S.fpos = mpos;
+                    S.exhaust = mex;
+                }
+                __syncthreads();
+                i = S.first;
+                if (i >= wn) {
+                    if (tid == 0) S.P += total;
+                    break;
+                }
+                if (tid == 0) {
+                    state_at(b, R, S.fpos, S.rng);
+                    S.nd = 0;
+                    if (S.exhaust) S.serial = 1;
+                }
+                __syncthreads();
+                if (S.serial) continue;  // walk on serially from catalyst i
+            } else {
+                if (tid == 0) {
+                    uint64_t r[4] = {S.rng[0], S.rng[1], S.rng[2], S.rng[3]};
+                    for (; i < wn; i++) {
+                        const int code = S.wcode[i], kind = code & 3, var = code >> 2;
+                        if (kind == WALK_NONE) continue;
+                        if (kind == WALK_VISIT) break;
+                        uint64_t t[4] = {r[0], r[1], r[2], r[3]};
+                        if (kind == WALK_SYN && (xo_next(t) >> 11) < tsyn[var]) break;
+                        if ((xo_next(t) >> 11) < trep[var]) break;
+                        r[0] = t[0];
+                        r[1] = t[1];
+                        r[2] = t[2];
+                        r[3] = t[3];
+                    }
+                    for (int q = 0; q < 4; q++) S.rng[q] = r[q];
+                    S.k = i;
+                }
+                __syncthreads();
+                i = S.k;
+                if (i >= wn) break;
             }
-            __syncthreads();
-            i = S.k;
-            if (i >= wn) break;
             visit(S, b, cur, R, rep, step, S.wk[i], overflow);
+            if (tid == 0 && !S.serial) S.P = S.fpos + S.nd;
             // mark the cells around the beads it changed; re-test the rest of the window
             const int nchg = S.nchg;
             if (nchg > 0) {
@@ -903,13 +1029,16 @@ __global__ void __launch_bounds__(CAT_TPB) k_cat_serial(Bufs b, int cur, const R
                 __syncthreads();
                 for (int j = i + 1 + tid; j < wn; j += CAT_TPB)
                     if (__ldcg(mark + cell[w0 + j])) S.wcode[j] = (uint8_t)(WALK_VISIT | (S.wcode[j] & 4));
-                __syncthreads();
             }
+            __syncthreads();
             i++;
         }
     }
-    if (tid == 0)
+    __syncthreads();
+    if (tid == 0) {
+        if (!S.serial) state_at(b, R, S.P, S.rng);
         for (int q = 0; q < 4; q++) b.rng[4 * rep + q] = S.rng[q];
+    }
     if ((overflow || S.over) && tid == 0) raise_flag(b.status, DPD_F_CATALYST);
 }
 
@@ -1020,16 +1149,17 @@ int catalyst_setup() {
         cudaFuncSetAttribute(k_cat_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CatSmem));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_cat_shuffle, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 CAT_SHUF_MAX * (int)sizeof(int32_t));
+                                 CAT_SHUF_MAX * (int)sizeof(int32_t));  // + CAT_SHUF_RUN static: 200 KB
     return e == cudaSuccess ? 0 : -1;
 }
 
 void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep, int64_t C,
-                     int nmax, cudaStream_t s) {
+                     int nmax, int stream_grid, cudaStream_t s) {
     const int shmax = std::min(nmax, CAT_SHUF_MAX);
     k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
     k_cat_list<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
-    k_cat_shuffle<<<nrep, 64, (size_t)shmax * sizeof(int32_t), s>>>(b, rep, shmax);
+    k_cat_stream<<<dim3(stream_grid, nrep), 256, 0, s>>>(b, rep);
+    k_cat_shuffle<<<nrep, 256, (size_t)shmax * sizeof(int32_t), s>>>(b, rep, shmax);
     k_cat_near<<<dim3(std::max(1, 148 * 8 / nrep), nrep), BEAD_TPB, 0, s>>>(b, cur, rep);
     cudaMemsetAsync(b.cat_mark, 0, (size_t)C, s);
     k_cat_serial<<<nrep, CAT_TPB, sizeof(CatSmem), s>>>(b, cur, rep);

@@ -16,6 +16,7 @@
 //     (placement cursor)
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/dpd.h"
@@ -72,6 +73,8 @@ struct RepDev {                 // constants of one replica, read by every kerne
     int32_t ch0, nch;           // this replica's chunks in the bead chunk table
     int32_t cat_E;              // half-width in cells of the window staged around a catalyst
     int32_t arch;               // lipid shape (0 linear: per-bead bond terms; else the template, k_mol_forces)
+    long long so;               // first draw of this replica's catalyst stream (a multiple of 64)
+    int32_t dcap, pad4;         // draws its stream holds (a multiple of 64)
     double r_cat, p_syn_a, p_syn_b, p_rep_a, p_rep_b, mu, p_ld, p_kd, p_nd, p_feed, feed_cap;
     double vent_x, vent_y, vent_r, vent_w;
     double kb_d, r0_d, ka_d;    // FP64 bond and angle constants for the relaxation of new chains
@@ -159,6 +162,10 @@ struct Bufs {
     int32_t *cat_cell;          // per catalyst list entry: its cell
     uint8_t *cat_mark;          // per cell: a bead near it changed type in the current check
     const dpd_template *mol;    // per replica: its lipid template
+    const uint64_t *jump;       // x^(64 m) mod the xoshiro256** polynomial, 4 words per m (dpd_jump.cu)
+    uint64_t *stream;           // the draws of a catalyst check, from RepDev::so per replica
+    uint64_t *sblock;           // the generator state at every 64th draw of the stream
+    long long *cat_dn;          // per replica: draws in the current check's stream
     int2 *fmol;                 // per bead: fixed-point bonded force of a branched lipid (k_mol_forces)
 };
 
@@ -194,7 +201,8 @@ inline void launch_pdl(void (*k)(KArgs...), unsigned grid, unsigned block, size_
 // the catalyst chemistry of one check (dpd_catalyst.cu): catalysts, decay, food supply
 int catalyst_setup();
 void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep, int64_t C,
-                     int nmax, cudaStream_t s);
+                     int nmax, int stream_grid, cudaStream_t s);
+int jump_table(int nblk, std::vector<uint64_t> &out);
 
 // launchers (dpd_kernels.cu, dpd_chem.cu, dpd_adjoint.cu); every launcher enqueues on stream s
 // PERM_KEEP: the step's update with the slot order kept (source = destination)

@@ -87,7 +87,7 @@ EXPORTS = [
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
-    "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters",
+    "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters", "dpd_xoshiro_jump",
 ]
 NGRAD = 66
 
@@ -136,6 +136,7 @@ def load(path: str | None = None):
                           + [C.POINTER(C.c_int32), fp, C.POINTER(DpdTemplate)], C.c_int),
         "dpd_lipid_template": ([C.POINTER(DpdParams), C.POINTER(DpdTemplate)], C.c_int),
         "dpd_type_clusters": ([vp, i32, i32, dbl, fp], C.c_int),
+        "dpd_xoshiro_jump": ([fp, u64, fp], C.c_int),
         "dpd_set_rng": ([vp, i32, fp], C.c_int),
         "dpd_get_rng": ([vp, i32, fp], C.c_int),
         "dpd_build_cells": ([vp], C.c_int),
