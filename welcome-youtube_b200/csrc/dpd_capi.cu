@@ -448,6 +448,8 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
         TRY(dalloc(h, &b.stream, (size_t)so));
         TRY(dalloc(h, &b.sblock, (size_t)so / 16));
         TRY(dalloc(h, &b.cat_dn, (size_t)nrep));
+        TRY(dalloc(h, &b.shuf, 8 * N));
+        b.shuf_n = (long long)N;
         h->stream_grid = (nblk + 255) / 256;
     }
     {

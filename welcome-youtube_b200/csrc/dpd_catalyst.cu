@@ -36,12 +36,11 @@
 #define CAT_MAXTR DPD_CAT_MAXTR
 // what the walk does with a catalyst: no draws (fewer than 2 N), the replication
 // draw, the synthesis and replication draws, or a visit by the whole CTA
-#define CAT_SHUF_RUN 2048  // shuffle steps whose partners are staged at a time
+#define CAT_SHUF_SH 11264  // catalysts per replica whose shuffle scratch fits in shared memory (5 x 44 KB)
 #define WALK_NONE 0
 #define WALK_REP 1
 #define WALK_SYN 2
 #define WALK_VISIT 3
-#define CAT_SHUF_MAX 49152  // catalysts per replica shuffled in shared memory (more: in place in global memory)
 
 // event kinds after the lipid chemistry's 0..2
 #define EV_SYN 3
@@ -632,52 +631,137 @@ __device__ __forceinline__ void state_at(const Bufs &b, const RepDev &R, long lo
 }
 
 // the catalyst list of one replica shuffled as the serial generator does it
-// (oercel.c:1571-1580): step i = nk-1 .. 1 swaps entries i and xo_below(i + 1)
-// of draw nk-1-i.  The block computes the swap partners of a run of steps
-// from the stream into shared memory, then one thread applies them; the list
-// is in shared memory while it fits (shmax entries).
+// (oercel.c:1571-1580): step i = nk-1 .. 1 swaps entries i and c_i =
+// xo_below(i + 1) of draw nk-1-i.  The swaps are resolved in parallel: the
+// entry that ends at position i >= 1 is the one that sat at c_i just before
+// step i, i.e. the one the latest earlier step (the smallest m > i with
+// c_m = c_i) moved there, else the original a[c_i]; what step m moved is the
+// entry that sat at m just before step m, i.e. the one moved there by the
+// smallest m' > m with c_m' = m, else a[m].  These "moved by" links point to
+// larger steps, so pointer jumping resolves them in O(log nk) rounds.  Position
+// 0 ends with what the smallest step m with c_m = 0 moved, else a[0].  The
+// steps are grouped by partner (a stable order within each group comes from
+// sorting the group, at most a few steps).
 __device__ __forceinline__ int swap_partner(const uint64_t *st, int nk, int i) {
     const double u = (double)(__ldcg(st + (nk - 1 - i)) >> 11) * 0x1.0p-53;
     const long long k = (long long)(u * (double)(i + 1));
     return (int)(k >= i + 1 ? i : k);
 }
 
-__global__ void __launch_bounds__(256) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int shmax) {
-    extern __shared__ int32_t shl[];
-    __shared__ int32_t spart[CAT_SHUF_RUN];
+__device__ __forceinline__ int block_excl_scan_1k(int v, int &total, int *ws) {
+    const int lane = (int)lane_id(), w = (int)threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = ws[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        ws[lane] = t;  // inclusive sums of the warps
+    }
+    __syncthreads();
+    total = ws[31];
+    return (w > 0 ? ws[w - 1] : 0) + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_cat_shuffle(Bufs b, const RepDev *__restrict__ reps, int sh) {
+    extern __shared__ int32_t shs[];
+    __shared__ int ws[32];
     const int rep = (int)blockIdx.x;
     const RepDev &R = reps[rep];
     if (!cat_due(R, *b.step)) return;
-    const int tid = (int)threadIdx.x;
-    const int nk = b.cat_nk[rep];
-    int32_t *list = b.cat_list + R.b0;
+    const int tid = (int)threadIdx.x, nk = b.cat_nk[rep];
+    if (nk < 2) return;
     const uint64_t *st = b.stream + R.so;
-    const bool sh = nk <= shmax;
-    if (sh)
-        for (int i = tid; i < nk; i += 256) shl[i] = list[i];
-    for (int hi = nk - 1; hi > 0; hi -= CAT_SHUF_RUN) {
-        const int lo = max(1, hi - CAT_SHUF_RUN + 1);
-        for (int i = lo + tid; i <= hi; i += 256) spart[i - lo] = swap_partner(st, nk, i);
-        __syncthreads();
-        if (tid == 0) {
-            if (sh) {
-                for (int i = hi; i >= lo; i--) {
-                    const int c = spart[i - lo], t = shl[i];
-                    shl[i] = shl[c];
-                    shl[c] = t;
-                }
-            } else {
-                for (int i = hi; i >= lo; i--) {
-                    const int c = spart[i - lo], t = list[i];
-                    list[i] = list[c];
-                    list[c] = t;
-                }
-            }
-        }
-        __syncthreads();
+    int32_t *list = b.cat_list + R.b0;
+    // scratch of nk entries each, in shared memory while it fits: bucket starts, fill (later the
+    // result), the steps sorted by partner, the next step with the same partner, the "moved by" link
+    int32_t *cnt, *fill, *occ, *nxt, *lnk;
+    if (nk <= sh) {  // the launch gave 5 sh entries of shared memory
+        cnt = shs;
+        fill = shs + sh;
+        occ = shs + 2 * sh;
+        nxt = shs + 3 * sh;
+        lnk = shs + 4 * sh;
+    } else {
+        cnt = b.shuf + 0 * b.shuf_n + R.b0;
+        fill = b.shuf + 1 * b.shuf_n + R.b0;
+        occ = b.shuf + 2 * b.shuf_n + R.b0;
+        nxt = b.shuf + 3 * b.shuf_n + R.b0;
+        lnk = b.shuf + 4 * b.shuf_n + R.b0;
     }
-    if (sh)
-        for (int i = tid; i < nk; i += 256) list[i] = shl[i];
+    for (int p = tid; p < nk; p += 1024) {
+        cnt[p] = 0;
+        fill[p] = 0;
+    }
+    __syncthreads();
+    for (int k = 1 + tid; k < nk; k += 1024) atomicAdd(cnt + swap_partner(st, nk, k), 1);
+    __syncthreads();
+    int base = 0;  // bucket starts: exclusive scan of cnt, in place
+    for (int p0 = 0; p0 < nk; p0 += 1024) {
+        const int p = p0 + tid, v = p < nk ? cnt[p] : 0;
+        int tot;
+        const int ex = block_excl_scan_1k(v, tot, ws);
+        if (p < nk) cnt[p] = base + ex;
+        base += tot;
+    }
+    __syncthreads();
+    for (int k = 1 + tid; k < nk; k += 1024) {
+        const int c = swap_partner(st, nk, k);
+        occ[cnt[c] + atomicAdd(fill + c, 1)] = k;
+    }
+    __syncthreads();
+    // each bucket in ascending step order; the next step of the same partner
+    for (int p = tid; p < nk; p += 1024) {
+        const int s0 = cnt[p], n = fill[p];
+        for (int a = 1; a < n; a++) {
+            const int t = occ[s0 + a];
+            int c = a - 1;
+            while (c >= 0 && occ[s0 + c] > t) {
+                occ[s0 + c + 1] = occ[s0 + c];
+                c--;
+            }
+            occ[s0 + c + 1] = t;
+        }
+        for (int a = 0; a < n; a++) nxt[occ[s0 + a]] = a + 1 < n ? occ[s0 + a + 1] : -1;
+    }
+    __syncthreads();
+    // step k moved what the first step m > k with c_m = k had moved there, else a[k]
+    for (int k = 1 + tid; k < nk; k += 1024) {
+        int m = fill[k] > 0 ? occ[cnt[k]] : -1;  // the smallest step with partner k (>= k)
+        if (m == k) m = nxt[k];
+        lnk[k] = m;
+    }
+    __syncthreads();
+    // what ends at position i: what the smallest step m > i with c_m = c_i moved (following the
+    // links, which only go to larger steps), else a[c_i]; position 0 likewise with partner 0.
+    // Into fill: only position 0 reads fill (fill[0], by the thread that writes it).
+    for (int i = tid; i < nk; i += 1024) {
+        int m, src;
+        if (i == 0) {
+            m = fill[0] > 0 ? occ[cnt[0]] : -1;
+            src = 0;
+        } else {
+            m = nxt[i];
+            src = swap_partner(st, nk, i);
+        }
+        for (int hop = 0; m >= 0 && hop < nk; hop++) {
+            src = m;
+            m = lnk[m];
+        }
+        fill[i] = list[src];
+    }
+    __syncthreads();
+    for (int i = tid; i < nk; i += 1024) list[i] = fill[i];
 }
 
 // per catalyst (a warp each, its lanes over the cells of the search window):
@@ -1149,17 +1233,18 @@ int catalyst_setup() {
         cudaFuncSetAttribute(k_cat_serial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CatSmem));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_cat_shuffle, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 CAT_SHUF_MAX * (int)sizeof(int32_t));  // + CAT_SHUF_RUN static: 200 KB
+                                 CAT_SHUF_SH * 5 * (int)sizeof(int32_t));
+
     return e == cudaSuccess ? 0 : -1;
 }
 
 void launch_catalyst(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int nrep, int64_t C,
                      int nmax, int stream_grid, cudaStream_t s) {
-    const int shmax = std::min(nmax, CAT_SHUF_MAX);
     k_cat_count<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
     k_cat_list<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, 0);
     k_cat_stream<<<dim3(stream_grid, nrep), 256, 0, s>>>(b, rep);
-    k_cat_shuffle<<<nrep, 256, (size_t)shmax * sizeof(int32_t), s>>>(b, rep, shmax);
+    const int sh = std::min(nmax, CAT_SHUF_SH);
+    k_cat_shuffle<<<nrep, 1024, (size_t)sh * 5 * sizeof(int32_t), s>>>(b, rep, sh);
     k_cat_near<<<dim3(std::max(1, 148 * 8 / nrep), nrep), BEAD_TPB, 0, s>>>(b, cur, rep);
     cudaMemsetAsync(b.cat_mark, 0, (size_t)C, s);
     k_cat_serial<<<nrep, CAT_TPB, sizeof(CatSmem), s>>>(b, cur, rep);

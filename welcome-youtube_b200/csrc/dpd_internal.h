@@ -166,6 +166,8 @@ struct Bufs {
     uint64_t *stream;           // the draws of a catalyst check, from RepDev::so per replica
     uint64_t *sblock;           // the generator state at every 64th draw of the stream
     long long *cat_dn;          // per replica: draws in the current check's stream
+    int32_t *shuf;              // 8 x shuf_n scratch of the parallel shuffle (per replica at b0)
+    long long shuf_n;
     int2 *fmol;                 // per bead: fixed-point bonded force of a branched lipid (k_mol_forces)
 };
 
