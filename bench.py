@@ -300,9 +300,29 @@ def analysis_rates(eng, p, reps=5):
     ref = analysis.type_clusters(st["x"], st["y"], st["type"], float(np.float32(p.L)), 2, 1.0)
     cpu_ms = (time.perf_counter() - t0) * 1000.0
     same = all(got[k] == ref[k] for k in ref)
+    # molecules and membrane aggregates (the first stages of the reference's cell detection)
+    eng.aggregates(0)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        agg = eng.aggregates(0, labels=True)
+    agg_gpu_ms = (time.perf_counter() - t0) * 1000.0 / reps
+    n = len(st["x"])
+    g = st["gid"].astype(np.int64)
+    x, y, t = np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.uint8)
+    x[g], y[g], t[g] = st["x"], st["y"], st["type"]
+    nx = st["next"]
+    bonds = np.stack([g[nx >= 0], g[nx[nx >= 0]]], axis=1)
+    t0 = time.perf_counter()
+    aref = analysis.aggregates(x, y, t, bonds, float(np.float32(p.L)), 1.0, 12)
+    agg_cpu_ms = (time.perf_counter() - t0) * 1000.0
+    agg_same = all(agg[k] == aref[k] for k in aref if k != "labels") and np.array_equal(agg["labels"], aref["labels"])
     return {"gpu_ms": gpu_ms, "cpu_ms": cpu_ms, "same_result": same, "beads": int(p.n_beads()), "t_beads": ref["n"],
-            "clusters": ref["clusters"], "timing": "host clock around each call (device synchronised); CPU: the "
-                                                    "oracle's restatement of the reference tool (scipy), 1 thread",
+            "clusters": ref["clusters"], "aggregates": {"gpu_ms": agg_gpu_ms, "cpu_ms": agg_cpu_ms,
+                                                        "same_result": bool(agg_same),
+                                                        "molecules": aref["n_molecules"],
+                                                        "membranes": aref["n_membranes"]},
+            "timing": "host clock around each call (device synchronised; the aggregates call includes the copy of "
+                      "the per-bead labels); CPU: the oracle's restatements of the reference tools (scipy), 1 thread",
             "kind": "port"}
 
 

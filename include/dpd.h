@@ -318,6 +318,19 @@ DPD_API int dpd_stats(dpd_handle *h, int32_t replica, double *out);
  * reference engine, whose analysis reads snapshots on the CPU. */
 DPD_API int dpd_type_clusters(dpd_handle *h, int32_t replica, int32_t type, double rcut, int64_t *out);
 
+/* Membrane aggregates of replica r: the first stages of the reference's cell
+ * detection (cel/tools/cells.py:64-86, 345-366, 605-608).  Molecules are the
+ * bonded components of lipid beads (H, T); aggregates join molecules whose
+ * tail beads lie within r_tail (0 < r_tail <= 1, distance <= r_tail).  out[0]
+ * molecules, out[1] aggregates, out[2] membranes (aggregates of at least
+ * min_lipids molecules), out[3] molecules in smaller aggregates, out[4] the
+ * largest aggregate in molecules.  agg_of_gid (n entries, may be NULL): per
+ * bead in gid order, the smallest gid of its aggregate, -1 for non-lipid
+ * beads.  Uses the cell index of the last sort.  No counterpart call in the
+ * reference engine, whose analysis reads snapshots on the CPU. */
+DPD_API int dpd_aggregates(dpd_handle *h, int32_t replica, double r_tail, int32_t min_lipids, int64_t *out,
+                           int32_t *agg_of_gid);
+
 /* Histogram (nbin bins on [0, rmax), rmax <= 3) of distances between beads of
  * types ta and tb of replica r, each unordered pair once. */
 DPD_API int dpd_pair_hist(dpd_handle *h, int32_t replica, int32_t ta, int32_t tb, double rmax, int32_t nbin, double *hist);

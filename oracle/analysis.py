@@ -32,3 +32,51 @@ def type_clusters(x, y, types, L, t=2, rcut=1.0):
     return dict(n=n, clusters=int(nclust) if n else 0, largest=int(sizes.max()) if n else 0,
                 sum_sq=int((sizes.astype(np.int64) ** 2).sum()), nb_all=int(near_all.sum()),
                 nb_same=int(near_same.sum()))
+
+
+def aggregates(x, y, types, bonds, L, r_tail=1.0, min_lipids=12):
+    """Molecules and membrane aggregates: the first stages of the reference's
+    cell detection (cel/tools/cells.py: lipid_molecules 68-86, detect 345-366,
+    summary 605-608).  Molecules are the components of the bonds between lipid
+    beads (H = 1, T = 2); aggregates join molecules whose T beads lie within
+    r_tail.  Returns the summary counts and, per bead, the smallest bead index
+    of its aggregate (-1 for other beads)."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    from scipy.spatial import cKDTree
+
+    types = np.asarray(types)
+    n = len(types)
+    lipid = (types == 1) | (types == 2)
+    bonds = np.asarray(bonds, np.int64).reshape(-1, 2)
+    bonds = bonds[lipid[bonds[:, 0]] & lipid[bonds[:, 1]]] if len(bonds) else bonds
+    tails = np.nonzero(types == 2)[0]
+    contacts = np.zeros((0, 2), np.int64)
+    if len(tails) > 1:
+        pts = np.stack([np.asarray(x, np.float64)[tails], np.asarray(y, np.float64)[tails]], axis=1) % L
+        pr = cKDTree(pts, boxsize=L).query_pairs(r_tail, output_type="ndarray")
+        contacts = tails[pr] if len(pr) else contacts
+    # molecules: components of the bond graph over the lipid beads
+    mol_graph = coo_matrix((np.ones(len(bonds)), (bonds[:, 0], bonds[:, 1])), shape=(n, n))
+    _, mol = connected_components(mol_graph, directed=False)
+    mol_ids, mol = np.unique(np.where(lipid, mol, -1), return_inverse=True)
+    mol = mol - (1 if mol_ids[0] == -1 else 0)
+    mol[~lipid] = -1
+    nmol = int(mol.max()) + 1 if lipid.any() else 0
+    # aggregates: components of the molecules joined by tail contacts
+    if nmol:
+        e = mol[contacts] if len(contacts) else np.zeros((0, 2), np.int64)
+        g = coo_matrix((np.ones(len(e)), (e[:, 0], e[:, 1])), shape=(nmol, nmol))
+        nagg, agg_of_mol = connected_components(g, directed=False)
+        size = np.bincount(agg_of_mol, minlength=nagg)
+    else:
+        nagg, agg_of_mol, size = 0, np.zeros(0, np.int64), np.zeros(0, np.int64)
+    label = np.full(n, -1, np.int64)
+    if nmol:
+        agg = agg_of_mol[mol[lipid]]
+        first = np.full(nagg, n, np.int64)
+        np.minimum.at(first, agg, np.nonzero(lipid)[0])
+        label[lipid] = first[agg]
+    return dict(n_molecules=nmol, n_aggregates=int(nagg), n_membranes=int((size >= min_lipids).sum()),
+                lipids_in_small_aggregates=int(size[size < min_lipids].sum()),
+                largest_aggregate=int(size.max()) if nmol else 0, labels=label)

@@ -234,6 +234,52 @@ def tclust_fixture():
     np.savez_compressed(os.path.join(HERE, "tclust.npz"), **out)
 
 
+# reference runs long enough to form membranes (tail aggregates of >= 12 molecules)
+MEMBRANE_RUNS = [dict(lip_arch="linear", lip_nH=1, lip_nT=3, f_lip=0.3, k_angle=10, a_W_T=100),
+                 dict(lip_arch="pi", lip_nT=2, lip_tie=1, f_lip=0.35, k_angle=15, a_W_T=200)]
+
+
+def aggregates_fixture():
+    """the reference cell detection's molecule and aggregate stages (its summary
+    and per-bead aggregate index) on the reference snapshots of tclust.npz and on
+    two 3000-step reference runs that form membranes"""
+    import subprocess
+    import tempfile
+    sys.path.insert(0, os.path.join(REF_ROOT, "cel", "tools"))
+    import cells
+    import ocio
+    g = np.load(os.path.join(HERE, "tclust.npz"))
+    snaps = []
+    k = 0
+    while f"c{k}_snap" in g.files:
+        snaps.append(bytes(g[f"c{k}_snap"]))
+        k += 1
+    exe = os.path.join(HERE, "..", "..", "oracle", "_ref", "oercel_portable")
+    for lip in MEMBRANE_RUNS:
+        kv = dict(L=24, dt=0.03, kT=1, gamma=4.5, warmup=200, f_Ka=0.0, f_Kb=0, c_N=0.05, chem=0, seed=11, threads=8,
+                  steps=3000, snap_every=3000, stats_every=3000, ckpt_every=0, log_every=0, **lip)
+        with tempfile.TemporaryDirectory() as td:
+            ini = os.path.join(td, "p.ini")
+            with open(ini, "w") as f:
+                f.write("".join(f"{k_} = {v}\n" for k_, v in kv.items()))
+            subprocess.run([exe, ini, os.path.join(td, "o")], check=True, capture_output=True)
+            with open(os.path.join(td, "o", "snap_0000003000.bin"), "rb") as f:
+                snaps.append(f.read())
+    out = {}
+    for k, raw in enumerate(snaps):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "s.bin")
+            with open(path, "wb") as f:
+                f.write(raw)
+            res = cells.detect(ocio.read_snapshot(path))
+        sm = res["summary"]
+        for key in ("n_molecules", "n_aggregates", "n_membranes", "lipids_in_small_aggregates", "largest_aggregate"):
+            out[f"c{k}_{key}"] = np.int64(sm[key])
+        out[f"c{k}_bead_agg"] = np.asarray(res["bead_agg"], np.int64)
+        out[f"c{k}_snap"] = np.frombuffer(raw, np.uint8)
+    np.savez_compressed(os.path.join(HERE, "aggregates.npz"), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -367,5 +413,6 @@ if __name__ == "__main__":
     catalyst_fixture("catalyst_vent_L16_seed13.npz", 13, 21, syn_nN=2, feed="vent", vent_shape="disk", vent_r=4,
                      feed_cap=0.3)
     tclust_fixture()
+    aggregates_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,8 +1,11 @@
-"""Cluster analysis on the GPU (dpd_type_clusters) against the oracle's
-restatement of the reference's `snapcheck.py tclust` (oracle/analysis.py,
-pinned to the tool's own output): on the reference snapshots of
-tests/golden/tclust.npz and on states the engine evolved, every count exact
-(beads, clusters, largest, sum of squared sizes, neighbour counts)."""
+"""Analysis on the GPU against the oracle's restatements (oracle/analysis.py,
+pinned to the reference tools' own output): tail-bead clusters
+(dpd_type_clusters, the reference's `snapcheck.py tclust`) on the reference
+snapshots of tests/golden/tclust.npz and on states the engine evolved, every
+count exact (beads, clusters, largest, sum of squared sizes, neighbour
+counts); molecules and membrane aggregates (dpd_aggregates, the first stages
+of the reference's cells.detect) on evolved boxes of linear and pi lipids,
+every count and every bead's aggregate exact."""
 import numpy as np
 import pytest
 
@@ -52,3 +55,35 @@ def test_clusters_of_an_evolved_box(cuda_ok, rcut):
     ref = analysis.type_clusters(st["x"], st["y"], st["type"], float(np.float32(p.L)), 2, rcut)
     assert {k_: got[k_] for k_ in KEYS} == ref
     assert got["n"] == int((st["type"] == 2).sum()) and got["clusters"] < got["n"]
+
+
+@pytest.mark.parametrize("arch", ["linear", "pi"])
+def test_aggregates_of_an_evolved_box(cuda_ok, arch):
+    """molecules and membrane aggregates (the first stages of the reference's
+    cell detection) on a 32 x 32 lipid box after 1500 steps, against the oracle
+    (pinned to the reference's cells.detect): every count and the aggregate
+    label of every bead"""
+    kv = dict(L=32, seed=23, chem=0, noise="philox", f_lip=0.3, warmup=0)
+    if arch == "linear":
+        p = params(a_W_T=100, lip_nT=3, k_angle=10, **kv)
+    else:
+        p = params(lip_arch="pi", lip_nT=2, lip_tie=1, r0_head=0.7, k_bond=300, k_angle=15, a_W_T=150, **kv)
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(1500)
+    st = e.state()
+    got = e.aggregates(0, 1.0, 12, labels=True)
+    if arch == "linear":
+        g, nx = st["gid"].astype(np.int64), st["next"]
+        bonds = np.stack([g[nx >= 0], g[nx[nx >= 0]]], axis=1)
+    else:
+        bonds = cli.template_bonds(st, p.template())
+    n = len(st["x"])
+    x, y, t = np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.uint8)
+    x[st["gid"]], y[st["gid"]], t[st["gid"]] = st["x"], st["y"], st["type"]
+    ref = analysis.aggregates(x, y, t, bonds, float(np.float32(p.L)), 1.0, 12)
+    for k in ("n_molecules", "n_aggregates", "n_membranes", "lipids_in_small_aggregates", "largest_aggregate"):
+        assert got[k] == ref[k], k
+    assert np.array_equal(got["labels"], ref["labels"])
+    assert got["n_membranes"] >= 1

@@ -301,3 +301,30 @@ def test_cluster_analysis_matches_the_reference_tool(tmp_path, line, snap):
     mine = (f"step={s['step']} nT={r['n']} clusters={r['clusters']} largest={r['largest']} mean size "
             f"(bead-weighted)={r['sum_sq'] / r['n']:.1f}  T-neighbour fraction={r['nb_same'] / r['nb_all']:.3f}")
     assert mine == line
+
+
+def aggregate_cases():
+    g = golden("aggregates.npz")
+    k = 0
+    while f"c{k}_snap" in g:
+        yield k, g
+        k += 1
+
+
+@pytest.mark.parametrize("k", [k for k, _ in aggregate_cases()])
+def test_aggregates_match_the_reference_cell_detection(tmp_path, k):
+    """molecules and membrane aggregates against the reference's cells.detect
+    (summary counts and the partition of the lipid beads into aggregates)"""
+    import analysis
+    from oercel_b200 import cli
+    g = golden("aggregates.npz")
+    p = tmp_path / "s.bin"
+    p.write_bytes(bytes(g[f"c{k}_snap"]))
+    s = cli.read_snapshot(str(p))
+    r = analysis.aggregates(s["x"], s["y"], s["type"], s["bonds"], s["L"])
+    for key in ("n_molecules", "n_aggregates", "n_membranes", "lipids_in_small_aggregates", "largest_aggregate"):
+        assert r[key] == int(g[f"c{k}_{key}"]), key
+    ref = g[f"c{k}_bead_agg"]
+    assert np.array_equal(ref < 0, r["labels"] < 0)
+    pairs = {(int(a), int(b)) for a, b in zip(ref[ref >= 0], r["labels"][ref >= 0])}
+    assert len(pairs) == len({a for a, _ in pairs}) == len({b for _, b in pairs})  # the same partition

@@ -71,7 +71,8 @@ struct dpd_handle {
     // staging for state in/out
     char *stage = nullptr;
     // cluster analysis scratch (allocated on first use): union-find parents, sizes, sums
-    int *ana_parent = nullptr, *ana_size = nullptr;
+    int *ana_parent = nullptr, *ana_size = nullptr, *ana_min = nullptr;
+    int32_t *ana_label = nullptr;
     unsigned long long *ana_acc = nullptr;
     std::vector<void *> allocs;
 };
@@ -998,6 +999,36 @@ extern "C" int dpd_type_clusters(dpd_handle *h, int32_t r, int32_t type, double 
     out[3] = (int64_t)acc[3];  // sum of squared cluster sizes
     out[4] = (int64_t)acc[0];  // neighbours within 1 of the type's beads, all types
     out[5] = (int64_t)acc[1];  // the same, of the type
+    return DPD_OK;
+}
+
+extern "C" int dpd_aggregates(dpd_handle *h, int32_t r, double r_tail, int32_t min_lipids, int64_t *out,
+                              int32_t *agg_of_gid) {
+    TRY(ensure_replica(h, r));
+    if (!out) return fail(DPD_E_ARG, "null output");
+    if (!(r_tail > 0.0 && r_tail <= 1.0)) return fail(DPD_E_ARG, "r_tail must be in (0, 1]");
+    if (!h->ana_parent) {
+        TRY(dalloc(h, &h->ana_parent, (size_t)h->N));
+        TRY(dalloc(h, &h->ana_size, (size_t)h->N));
+        TRY(dalloc(h, &h->ana_acc, 8));
+    }
+    if (!h->ana_min) {
+        TRY(dalloc(h, &h->ana_min, (size_t)h->N));
+        TRY(dalloc(h, &h->ana_label, (size_t)h->nmax));
+    }
+    const RepDev &R = h->rh[r];
+    launch_aggregates(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, R.n, r_tail, min_lipids, h->ana_parent,
+                      h->ana_size, h->ana_min, h->ana_acc, agg_of_gid ? h->ana_label : nullptr, h->s);
+    CK(cudaGetLastError());
+    unsigned long long acc[8];
+    CK(cudaMemcpyAsync(acc, h->ana_acc, sizeof acc, cudaMemcpyDeviceToHost, h->s));
+    if (agg_of_gid) CK(cudaMemcpyAsync(agg_of_gid, h->ana_label, (size_t)R.n * sizeof(int32_t), cudaMemcpyDefault, h->s));
+    TRY(check_status(h));
+    out[0] = (int64_t)acc[4];  // molecules
+    out[1] = (int64_t)acc[2];  // aggregates
+    out[2] = (int64_t)acc[3];  // membranes (aggregates of >= min_lipids molecules)
+    out[3] = (int64_t)acc[6];  // molecules in smaller aggregates
+    out[4] = (int64_t)acc[5];  // the largest aggregate (molecules)
     return DPD_OK;
 }
 

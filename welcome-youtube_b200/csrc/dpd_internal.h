@@ -227,6 +227,9 @@ void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s);
 void launch_mol_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_type_clusters(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int t,
                           double rcut, int *parent, int *size, unsigned long long *acc, cudaStream_t s);
+void launch_aggregates(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int n,
+                       double r_tail, int min_lipids, int *parent, int *size, int *minlab, unsigned long long *acc,
+                       int32_t *out_label, cudaStream_t s);
 void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
                    int64_t C, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,

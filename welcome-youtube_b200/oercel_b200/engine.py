@@ -240,6 +240,19 @@ class Engine:
         return dict(n=n, clusters=nc, largest=largest, sum_sq=sq, mean_size=sq / max(n, 1), nb_all=nb_all,
                     nb_same=nb_same, fraction=nb_same / max(nb_all, 1))
 
+    def aggregates(self, replica=0, r_tail=1.0, min_lipids=12, labels=False):
+        """molecules and membrane aggregates (the first stages of the reference's
+        cell detection); labels: per bead in gid order the smallest gid of its
+        aggregate (-1 for non-lipid beads)"""
+        out = np.zeros(5, np.int64)
+        lab = np.empty(self.n_beads[replica], np.int32) if labels else None
+        check(self.lib.dpd_aggregates(self.h, int(replica), float(r_tail), int(min_lipids), ptr(out), ptr(lab)))
+        res = dict(n_molecules=int(out[0]), n_aggregates=int(out[1]), n_membranes=int(out[2]),
+                   lipids_in_small_aggregates=int(out[3]), largest_aggregate=int(out[4]))
+        if labels:
+            res["labels"] = lab
+        return res
+
     def pair_hist(self, replica, ta, tb, rmax, nbin):
         h = np.zeros(nbin)
         check(self.lib.dpd_pair_hist(self.h, replica, ta, tb, float(rmax), nbin, ptr(h)))
