@@ -306,6 +306,13 @@ DPD_API int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *
 DPD_API int dpd_observables(dpd_handle *h, int32_t replica, double *out);
 /* the stats row only (out[3], the virial, is left 0): no pair loop */
 DPD_API int dpd_stats(dpd_handle *h, int32_t replica, double *out);
+/* dpd_stats without waiting: enqueues the row on the handle's stream and a
+ * copy of its 16 raw sums into raw (host memory, pinned for a true async copy),
+ * valid once the stream passes that point (dpd_sync); dpd_stats_decode turns
+ * the raw sums into the 16 values of dpd_stats.  No counterpart call in the
+ * reference, whose stats row is written by the step loop itself. */
+DPD_API int dpd_stats_async(dpd_handle *h, int32_t replica, uint64_t *raw);
+DPD_API int dpd_stats_decode(const dpd_handle *h, int32_t replica, const uint64_t *raw, double *out);
 
 /* Clusters of the beads of one type of replica r (the reference's analysis
  * `snapcheck.py tclust`, cel/engine/tests/snapcheck.py:122-144): beads of the

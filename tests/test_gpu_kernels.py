@@ -7,6 +7,7 @@ largest force (max |F_gpu - F_ref| <= 1e-5 max |F_ref|), FP32 against FP64.
 import numpy as np
 import pytest
 
+import oercel_b200 as ob
 import oracle as O
 from conftest import golden
 from gpu_util import (engine_with, links_from_next, oracle_params, oracle_state, params, rel_err)
@@ -221,3 +222,26 @@ def test_extras_tile_and_bead_kernels_agree(cuda_ok):
         e.forces(int(g["step"]))
         runs.append(e.state())
     assert np.array_equal(runs[0]["fx"], runs[1]["fx"]) and np.array_equal(runs[0]["fy"], runs[1]["fy"])
+
+
+def test_stats_async_equals_stats(cuda_ok):
+    """dpd_stats_async + dpd_stats_decode give the numbers of dpd_stats (two
+    identical engines: a stats read restarts the running max bond)"""
+    p = params(L=16, seed=5, chem=1, n_chem=1, p_grow=0.05, p_bond=0.3, p_break=0.02)
+    rows = []
+    for use_async in (False, True):
+        e = ob.Engine(p)
+        e.load_soup(0)
+        e.prime()
+        e.step(7)
+        if use_async:
+            raw = np.zeros(16, np.uint64)
+            e.stats_async(0, raw)
+            e.sync()
+            rows.append(e.stats_decode(0, raw))
+        else:
+            rows.append(e.observables(0, virial=False))
+    a, b = rows
+    for k in ("T", "px", "py", "maxbond", "n_chains"):
+        assert a[k] == b[k], k
+    assert np.array_equal(a["counts"], b["counts"])

@@ -1052,19 +1052,19 @@ extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_
     return DPD_OK;
 }
 
-static int observables_impl(dpd_handle *h, int32_t r, bool virial, double *out) {
-    TRY(ensure_replica(h, r));
-    if (!out) return fail(DPD_E_ARG, "null out");
+// the sums of a stats row on the stream, copied into v (OBS_N words) when the stream gets there
+static int enqueue_observables(dpd_handle *h, int32_t r, bool virial, unsigned long long *v) {
     unsigned long long *o = h->b.obs + (size_t)r * OBS_N;
     CK(cudaMemsetAsync(o, 0, 4 * sizeof(unsigned long long), h->s));
     CK(cudaMemsetAsync(o + 5, 0, (OBS_N - 5) * sizeof(unsigned long long), h->s));
     launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, h->s);
     CK(cudaGetLastError());
-    unsigned long long v[OBS_N];
-    CK(cudaMemcpyAsync(v, o, sizeof v, cudaMemcpyDeviceToHost, h->s));
-    CK(cudaStreamSynchronize(h->s));
+    CK(cudaMemcpyAsync(v, o, OBS_N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->s));
     CK(cudaMemsetAsync(o + 4, 0, sizeof(unsigned long long), h->s));  // max bond restarts per stats row
-    const RepDev &R = h->rh[r];
+    return DPD_OK;
+}
+
+static void decode_observables(const RepDev &R, const unsigned long long *v, double *out) {
     for (int k = 0; k < 16; k++) out[k] = 0.0;
     out[0] = (double)(long long)v[2] / OBS_FIX / (2.0 * R.n - 2.0);
     out[1] = (double)(long long)v[0] / OBS_FIX;
@@ -1076,7 +1076,28 @@ static int observables_impl(dpd_handle *h, int32_t r, bool virial, double *out) 
     out[4] = mb;
     out[5] = (double)v[5];
     for (int t = 0; t < 8; t++) out[8 + t] = (double)v[8 + t];
+}
+
+static int observables_impl(dpd_handle *h, int32_t r, bool virial, double *out) {
+    TRY(ensure_replica(h, r));
+    if (!out) return fail(DPD_E_ARG, "null out");
+    unsigned long long v[OBS_N];
+    TRY(enqueue_observables(h, r, virial, v));
     CK(cudaStreamSynchronize(h->s));
+    decode_observables(h->rh[r], v, out);
+    return DPD_OK;
+}
+
+extern "C" int dpd_stats_async(dpd_handle *h, int32_t r, uint64_t *raw) {
+    TRY(ensure_replica(h, r));
+    if (!raw) return fail(DPD_E_ARG, "null raw buffer");
+    return enqueue_observables(h, r, false, (unsigned long long *)raw);
+}
+
+extern "C" int dpd_stats_decode(const dpd_handle *h, int32_t r, const uint64_t *raw, double *out) {
+    if (!h || !raw || !out) return fail(DPD_E_ARG, "null argument");
+    if (r < 0 || r >= h->nrep) return fail(DPD_E_ARG, "replica %d out of range", r);
+    decode_observables(h->rh[r], (const unsigned long long *)raw, out);
     return DPD_OK;
 }
 

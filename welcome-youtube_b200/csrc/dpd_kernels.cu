@@ -11,6 +11,8 @@
 //                      cell of the next position and its atomic count
 // so the bead state is read and written once per kernel and the sort keys for
 // step n+1 come out of the force kernel of step n.
+#include <algorithm>
+
 #include "dpd_chem.cuh"
 
 // ---------------------------------------------------------------- keys (prime / build_cells)
@@ -606,71 +608,77 @@ __global__ void __launch_bounds__(BEAD_TPB) k_integrate(Bufs b, int cur, const R
 // ---------------------------------------------------------------- observables
 
 // per-bead sums (momentum, kinetic energy, type counts, chain heads) and the
-// conservative virial over each unordered pair once; fixed-point integer
-// atomics make the result independent of the launch shape.
+// conservative virial over each unordered pair once; fixed-point integer sums
+// make the result independent of the launch shape.  A grid-stride loop over
+// the replica's chunks keeps each thread's sums in registers; a block reduction
+// then leaves one atomic per quantity per block.
 template <bool VIRIAL>
 __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const Chunk *__restrict__ ch, int rep_index) {
-    const Chunk c = ch[blockIdx.x];
-    if (c.rep != rep_index) return;
-    const RepDev &R = reps[c.rep];
-    const int d = c.begin + (int)threadIdx.x;
-    const bool act = d < c.end;
+    __shared__ long long red[BEAD_TPB / 32][5 + DPD_MAXT];
+    const RepDev &R = reps[rep_index];
     long long sx = 0, sy = 0, s2 = 0, vir = 0, heads = 0;
-    int ty = -1;
-    if (act) {
+    int cnt[DPD_MAXT];
+#pragma unroll
+    for (int t = 0; t < DPD_MAXT; t++) cnt[t] = 0;
+    for (int k = (int)blockIdx.x; k < R.nch; k += (int)gridDim.x) {
+        const Chunk c = ch[R.ch0 + k];
+        const int d = c.begin + (int)threadIdx.x;
+        if (d >= c.end) continue;
         const float2 v = b.vh[cur][d], f = b.f[cur][d];
         const double vx = (double)v.x + (double)R.hdt * (double)f.x, vy = (double)v.y + (double)R.hdt * (double)f.y;
-        sx = __double2ll_rn(vx * OBS_FIX);
-        sy = __double2ll_rn(vy * OBS_FIX);
-        s2 = __double2ll_rn((vx * vx + vy * vy) * OBS_FIX);
+        sx += __double2ll_rn(vx * OBS_FIX);
+        sy += __double2ll_rn(vy * OBS_FIX);
+        s2 += __double2ll_rn((vx * vx + vy * vy) * OBS_FIX);
         const uint32_t tgi = b.tg[cur][d];
-        ty = (int)(tgi >> TYPE_SHIFT);
+        const int ty = (int)(tgi >> TYPE_SHIFT);
+#pragma unroll
+        for (int t = 0; t < DPD_MAXT; t++) cnt[t] += ty == t;
         const int2 lk = b.link[cur][d];
-        heads = (lk.x < 0 && lk.y >= 0) ? 1 : 0;
+        heads += (lk.x < 0 && lk.y >= 0) ? 1 : 0;
         // virial: pairs (d, j) with j > d inside the cutoff
         if (VIRIAL) {
-        const float2 *__restrict__ pos = b.pos[cur];
-        const float2 pi = pos[d];
-        const int ncx = R.ncx, ncy = R.ncy;
-        const int32_t *cs = b.cstart + R.c0;
-        int cx, cy;
-        cell_xy(R, pi.x, pi.y, cx, cy);
-        double accv = 0.0;
-        for (int ox = -1; ox <= 1; ox++)
-            for (int oy = -1; oy <= 1; oy++) {
-                const int nx = (cx + ox + ncx) % ncx, ny = (cy + oy + ncy) % ncy;
-                const int cc = nx * ncy + ny;
-                for (int j = cs[cc]; j < cs[cc + 1]; j++) {
-                    if (j <= d) continue;
-                    const float2 pj = pos[j];
-                    const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
-                    const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
-                    const double r2 = dx * dx + dy * dy;
-                    if (!(r2 < 1.0 && r2 > 1e-24)) continue;
-                    const double r = sqrt(r2);
-                    accv += (double)a_at(R, ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT), *b.step) * (1.0 - r) * r;
+            const float2 *__restrict__ pos = b.pos[cur];
+            const float2 pi = pos[d];
+            const int ncx = R.ncx, ncy = R.ncy;
+            const int32_t *cs = b.cstart + R.c0;
+            int cx, cy;
+            cell_xy(R, pi.x, pi.y, cx, cy);
+            double accv = 0.0;
+            for (int ox = -1; ox <= 1; ox++)
+                for (int oy = -1; oy <= 1; oy++) {
+                    const int nx = (cx + ox + ncx) % ncx, ny = (cy + oy + ncy) % ncy;
+                    const int cc = nx * ncy + ny;
+                    for (int j = cs[cc]; j < cs[cc + 1]; j++) {
+                        if (j <= d) continue;
+                        const float2 pj = pos[j];
+                        const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
+                        const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
+                        const double r2 = dx * dx + dy * dy;
+                        if (!(r2 < 1.0 && r2 > 1e-24)) continue;
+                        const double r = sqrt(r2);
+                        accv += (double)a_at(R, ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT), *b.step) * (1.0 - r) * r;
+                    }
                 }
-            }
-        vir = __double2ll_rn(accv * OBS_FIX);
+            vir += __double2ll_rn(accv * OBS_FIX);
         }
     }
-    unsigned long long *o = b.obs + (size_t)rep_index * OBS_N;
-    sx = warp_sum_ll(sx);
-    sy = warp_sum_ll(sy);
-    s2 = warp_sum_ll(s2);
-    vir = warp_sum_ll(vir);
-    heads = warp_sum_ll(heads);
-    if (lane_id() == 0) {
-        atomicAdd(o + 0, (unsigned long long)sx);
-        atomicAdd(o + 1, (unsigned long long)sy);
-        atomicAdd(o + 2, (unsigned long long)s2);
-        atomicAdd(o + 3, (unsigned long long)vir);
-        atomicAdd(o + 5, (unsigned long long)heads);
+    long long q[5 + DPD_MAXT] = {sx, sy, s2, vir, heads};
+#pragma unroll
+    for (int t = 0; t < DPD_MAXT; t++) q[5 + t] = cnt[t];
+    const int lane = (int)lane_id(), w = (int)threadIdx.x >> 5;
+#pragma unroll
+    for (int e = 0; e < 5 + DPD_MAXT; e++) {
+        const long long sum = warp_sum_ll(q[e]);
+        if (lane == 0) red[w][e] = sum;
     }
-    for (int t = 0; t < DPD_MAXT; t++) {
-        const unsigned m = __ballot_sync(0xffffffffu, ty == t);
-        if (lane_id() == 0 && m) atomicAdd(o + 8 + t, (unsigned long long)__popc(m));
+    __syncthreads();
+    if (threadIdx.x < 5 + DPD_MAXT) {
+        long long sum = 0;
+        for (int k = 0; k < BEAD_TPB / 32; k++) sum += red[k][threadIdx.x];
+        // slots: 0, 1 momentum, 2 kinetic, 3 virial, 5 heads, 8 + t type counts (4 is the running max bond)
+        const int slot = threadIdx.x < 4 ? (int)threadIdx.x : threadIdx.x == 4 ? 5 : 8 + (int)threadIdx.x - 5;
+        if (sum != 0) atomicAdd(b.obs + (size_t)rep_index * OBS_N + slot, (unsigned long long)sum);
     }
 }
 
@@ -854,8 +862,9 @@ void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bc
 
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
                         bool virial, cudaStream_t s) {
-    if (virial) k_observables<true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
-    else k_observables<false><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
+    const int grid = std::min(nbch, 148 * 4);  // grid-stride over the replica's chunks
+    if (virial) k_observables<true><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
+    else k_observables<false><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
 }
 
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,

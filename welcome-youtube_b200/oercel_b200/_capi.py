@@ -88,7 +88,7 @@ EXPORTS = [
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
     "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters", "dpd_xoshiro_jump",
-    "dpd_aggregates",
+    "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode",
 ]
 NGRAD = 66
 
@@ -139,6 +139,8 @@ def load(path: str | None = None):
         "dpd_type_clusters": ([vp, i32, i32, dbl, fp], C.c_int),
         "dpd_xoshiro_jump": ([fp, u64, fp], C.c_int),
         "dpd_aggregates": ([vp, i32, dbl, i32, fp, fp], C.c_int),
+        "dpd_stats_async": ([vp, i32, fp], C.c_int),
+        "dpd_stats_decode": ([vp, i32, fp, fp], C.c_int),
         "dpd_set_rng": ([vp, i32, fp], C.c_int),
         "dpd_get_rng": ([vp, i32, fp], C.c_int),
         "dpd_build_cells": ([vp], C.c_int),

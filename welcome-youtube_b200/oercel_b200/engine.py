@@ -231,6 +231,17 @@ class Engine:
         return dict(T=o[0], px=o[1], py=o[2], virial=o[3], maxbond=o[4], n_chains=int(o[5]),
                     counts=o[8:16].astype(np.int64))
 
+    def stats_async(self, replica, raw):
+        """enqueue the stats row; its 16 raw sums land in raw (a pinned uint64
+        array) once the stream passes (sync); stats_decode reads them"""
+        check(self.lib.dpd_stats_async(self.h, int(replica), ptr(raw)))
+
+    def stats_decode(self, replica, raw):
+        o = np.zeros(16)
+        check(self.lib.dpd_stats_decode(self.h, int(replica), ptr(np.ascontiguousarray(raw, np.uint64)), ptr(o)))
+        return dict(T=o[0], px=o[1], py=o[2], virial=o[3], maxbond=o[4], n_chains=int(o[5]),
+                    counts=o[8:16].astype(np.int64))
+
     def type_clusters(self, replica=0, type=2, rcut=1.0):
         """clusters of the beads of `type` joined within rcut, and their neighbour
         fraction within 1.0 (the reference's `snapcheck.py tclust`)"""
