@@ -165,3 +165,53 @@ def test_mixed_chemistries_in_one_batch_equal_solo_runs(cuda_ok):
         assert np.array_equal(both.rng(r), solo.rng(0))
         mine = sorted((x[:6] for x in ev_both if x[6] == r), key=repr)
         assert mine == sorted((x[:6] for x in ev_solo), key=repr) and mine, r
+
+
+def test_catalyst_replicas_of_uneven_size_equal_solo_runs(cuda_ok):
+    """three catalyst replicas of different sizes and settings in one engine
+    (their draw streams, lists and scratch at different offsets) give bit for
+    bit the runs of each alone"""
+    plist = [ob.Params(L=16, seed=7, n_chem=3, **CAT),
+             ob.Params(L=24, seed=8, n_chem=2, **dict(CAT, p_syn_a=0.2, p_rep_a=0.1)),
+             ob.Params(L=18, seed=9, n_chem=3, feed="vent", **CAT)]
+
+    def run(ps):
+        e = ob.Engine(ps)
+        for r in range(len(ps)):
+            e.load_soup(r)
+        e.prime()
+        e.step(24)
+        ev = [tuple(None if isinstance(v, float) and v != v else v for v in x) for x in e.events()]
+        return e, ev
+
+    both, ev_both = run(plist)
+    for r, p in enumerate(plist):
+        solo, ev_solo = run([p])
+        a, b = both.state(r), solo.state(0)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (r, k)
+        assert np.array_equal(both.rng(r), solo.rng(0))
+        mine = sorted((x[:6] for x in ev_both if x[6] == r), key=repr)
+        assert mine == sorted((x[:6] for x in ev_solo), key=repr) and mine, r
+
+
+def test_catalyst_check_with_the_shuffle_scratch_in_global_memory(cuda_ok):
+    """a 480 x 480 box with about 11,500 catalysts: more than the shuffle keeps
+    in shared memory; one check against the oracle"""
+    p = ob.Params(L=480, seed=3, n_chem=10, **dict(CAT, **LOW))
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(9)
+    s, cs, rng = e.state(), e.cells(), e.rng(0)
+    assert int(np.isin(s["type"], (4, 5)).sum()) > 11264
+    op, oc = oracle_blocks(p)
+    st = {k: s[k].copy() for k in ("x", "y", "vhx", "vhy", "vtx", "vty", "type", "gid", "prev", "next")}
+    orng = rng.copy()
+    _, oev = O.catalyst_chemistry(op, oc, st, cs.astype(np.int32), 10, orng, evcap=1 << 18)
+    e.chemistry(10)
+    g = e.state()
+    assert np.array_equal(e.rng(0), orng)
+    assert np.array_equal(g["type"], st["type"]) and np.array_equal(g["next"], st["next"])
+    got = sorted((ev[1], ev[2], ev[3] if ev[3] < 2**31 else ev[3] - 2**32) for ev in e.events())
+    assert got == sorted((ev[1], ev[2], ev[3]) for ev in oev)
