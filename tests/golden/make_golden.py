@@ -280,6 +280,42 @@ def aggregates_fixture():
     np.savez_compressed(os.path.join(HERE, "aggregates.npz"), **out)
 
 
+# catalyst chemistry rates over 300 steps (a check every 5), compared statistically
+RATES_INI = dict(L=24, dt=0.02, kT=1, gamma=4.5, warmup=50, f_lip=0.1, f_Ka=0.03, f_Kb=0.02, c_N=0.25, lip_nH=1,
+                 lip_nT=3, k_angle=10, chem=1, events=1, n_chem=5, p_syn_a=0.05, p_syn_b=0.08, p_rep_a=0.03,
+                 p_rep_b=0.03, mu=0.2, p_ld=0.005, p_kd=0.005, p_nd=0.004, feed="uniform", p_feed=0.01, feed_cap=0.3,
+                 threads=4, steps=300, snap_every=0, stats_every=100, ckpt_every=0, log_every=0)
+RATE_KINDS = ("syn", "rep", "mut", "dlip", "dK", "dN", "feed")
+
+
+def catalyst_rates_fixture(seeds=(1, 2, 3, 4)):
+    """the reference executable's event totals per kind (fed beads for feed)
+    and final stats rows over 300 steps, for several seeds"""
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "..", "..", "oracle", "_ref", "oercel_portable")
+    totals = np.zeros((len(seeds), len(RATE_KINDS)), np.int64)
+    finals = []
+    for a, seed in enumerate(seeds):
+        kv = dict(RATES_INI, seed=seed)
+        with tempfile.TemporaryDirectory() as td:
+            ini = os.path.join(td, "p.ini")
+            with open(ini, "w") as f:
+                f.write("".join(f"{k} = {v}\n" for k, v in kv.items()))
+            subprocess.run([exe, ini, os.path.join(td, "o")], check=True, capture_output=True)
+            with open(os.path.join(td, "o", "events.csv")) as f:
+                rows = [ln.split(",") for ln in f.read().strip().split("\n")[1:]]
+            with open(os.path.join(td, "o", "stats.csv")) as f:
+                finals.append([float(v) for v in f.read().strip().split("\n")[-1].split(",")])
+        for r in rows:
+            k = RATE_KINDS.index(r[1])
+            totals[a, k] += int(r[2]) if r[1] == "feed" else 1
+    ini = "".join(f"{k} = {v}\n" for k, v in RATES_INI.items())
+    np.savez_compressed(os.path.join(HERE, "catalyst_rates.npz"), seeds=np.array(seeds), totals=totals,
+                        finals=np.array(finals), kinds=np.frombuffer(",".join(RATE_KINDS).encode(), np.uint8),
+                        ini=np.frombuffer(ini.encode(), np.uint8))
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -414,5 +450,6 @@ if __name__ == "__main__":
                      feed_cap=0.3)
     tclust_fixture()
     aggregates_fixture()
+    catalyst_rates_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))
