@@ -338,8 +338,11 @@ DPD_API int dpd_type_clusters(dpd_handle *h, int32_t replica, int32_t type, doub
 DPD_API int dpd_aggregates(dpd_handle *h, int32_t replica, double r_tail, int32_t min_lipids, int64_t *out,
                            int32_t *agg_of_gid);
 
-/* Histogram (nbin bins on [0, rmax), rmax <= 3) of distances between beads of
- * types ta and tb of replica r, each unordered pair once. */
+/* Histogram (nbin bins on [0, rmax], rmax <= 3) of distances between beads of
+ * types ta and tb of replica r (ta < 0: all beads), each unordered pair once:
+ * the pair counts of the reference's `snapcheck.py rdf`
+ * (cel/engine/tests/snapcheck.py:86-107), distances in FP64 from the FP32
+ * positions, binned as np.histogram bins them. */
 DPD_API int dpd_pair_hist(dpd_handle *h, int32_t replica, int32_t ta, int32_t tb, double rmax, int32_t nbin, double *hist);
 
 /* the CUDA stream (cudaStream_t) this handle enqueues its work on */

@@ -80,3 +80,30 @@ def aggregates(x, y, types, bonds, L, r_tail=1.0, min_lipids=12):
     return dict(n_molecules=nmol, n_aggregates=int(nagg), n_membranes=int((size >= min_lipids).sum()),
                 lipids_in_small_aggregates=int(size[size < min_lipids].sum()),
                 largest_aggregate=int(size.max()) if nmol else 0, labels=label)
+
+
+def rdf_counts(x, y, types, L, t=None, rmax=3.0, nbin=30):
+    """Pair-distance counts of the reference's `snapcheck.py rdf`
+    (cel/engine/tests/snapcheck.py:86-107): the beads (of type t, or all),
+    positions in FP64 modulo L, the pairs within rmax of each other (periodic,
+    distance <= rmax), their minimum-image distances binned over [0, rmax]
+    into nbin bins.  Returns the counts and the number of beads."""
+    from scipy.spatial import cKDTree
+
+    pts = np.stack([np.asarray(x, np.float64), np.asarray(y, np.float64)], axis=1) % L
+    if t is not None:
+        pts = pts[np.asarray(types) == int(t)]
+    pairs = cKDTree(pts, boxsize=L).query_pairs(rmax, output_type="ndarray")
+    d = pts[pairs[:, 0]] - pts[pairs[:, 1]]
+    d -= L * np.round(d / L)
+    r = np.hypot(d[:, 0], d[:, 1])
+    counts, _ = np.histogram(r, bins=nbin, range=(0.0, rmax))
+    return counts, len(pts)
+
+
+def rdf_lines(counts, n, L, rmax=3.0, nbin=30):
+    """g(r) from the counts, printed as the reference tool prints it"""
+    edges = np.linspace(0.0, rmax, nbin + 1)
+    g = 2 * counts / (n * (n / L**2) * (np.pi * (edges[1:] ** 2 - edges[:-1] ** 2)))
+    rc = 0.5 * (edges[1:] + edges[:-1])
+    return [f"{r_:.3f} {g_:.4f} " + "#" * int(40 * g_ / max(g.max(), 1e-9)) for r_, g_ in zip(rc, g)]

@@ -316,6 +316,31 @@ def catalyst_rates_fixture(seeds=(1, 2, 3, 4)):
                         ini=np.frombuffer(ini.encode(), np.uint8))
 
 
+def rdf_fixture():
+    """the reference's `snapcheck.py rdf` output (all beads, and T beads) on the
+    snapshots of aggregates.npz"""
+    import contextlib
+    import io
+    import tempfile
+    sys.path.insert(0, os.path.join(REF_ROOT, "cel", "engine", "tests"))
+    import snapcheck
+    g = np.load(os.path.join(HERE, "aggregates.npz"))
+    out = {}
+    k = 0
+    while f"c{k}_snap" in g.files:
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "s.bin")
+            with open(path, "wb") as f:
+                f.write(bytes(g[f"c{k}_snap"]))
+            for tag, typ in (("all", None), ("T", 2)):
+                buf = io.StringIO()
+                with contextlib.redirect_stdout(buf):
+                    snapcheck.cmd_rdf([path], typ)
+                out[f"c{k}_{tag}"] = np.frombuffer(buf.getvalue().encode(), np.uint8)
+        k += 1
+    np.savez_compressed(os.path.join(HERE, "rdf.npz"), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -450,6 +475,7 @@ if __name__ == "__main__":
                      feed_cap=0.3)
     tclust_fixture()
     aggregates_fixture()
+    rdf_fixture()
     catalyst_rates_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -87,3 +87,23 @@ def test_aggregates_of_an_evolved_box(cuda_ok, arch):
         assert got[k] == ref[k], k
     assert np.array_equal(got["labels"], ref["labels"])
     assert got["n_membranes"] >= 1
+
+
+@pytest.mark.parametrize("k", range(6))
+def test_rdf_counts_of_reference_snapshots(cuda_ok, tmp_path, k):
+    """the pair-distance histogram (dpd_pair_hist, all beads and T beads, rmax 3,
+    30 bins) equals the oracle's restatement of the reference's `snapcheck.py
+    rdf` count for count on the reference snapshots (two with membranes)"""
+    g = golden("aggregates.npz")
+    p = tmp_path / "s.bin"
+    p.write_bytes(bytes(g[f"c{k}_snap"]))
+    s = cli.read_snapshot(str(p))
+    n = s["N"]
+    e = ob.Engine(ob.Params(L=s["L"], chem=0), n_beads=n)
+    z = np.zeros(n, np.float32)
+    e.set_state(0, s["x"], s["y"], z, z, s["type"])
+    e.build_cells()
+    for typ in (None, 2):
+        got = e.pair_hist(0, -1 if typ is None else typ, -1 if typ is None else typ, 3.0, 30)
+        ref, _ = analysis.rdf_counts(s["x"], s["y"], s["type"], s["L"], typ)
+        assert np.array_equal(got.astype(np.int64), ref), typ

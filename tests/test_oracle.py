@@ -328,3 +328,19 @@ def test_aggregates_match_the_reference_cell_detection(tmp_path, k):
     assert np.array_equal(ref < 0, r["labels"] < 0)
     pairs = {(int(a), int(b)) for a, b in zip(ref[ref >= 0], r["labels"][ref >= 0])}
     assert len(pairs) == len({a for a, _ in pairs}) == len({b for _, b in pairs})  # the same partition
+
+
+@pytest.mark.parametrize("k", range(6))
+@pytest.mark.parametrize("tag, typ", [("all", None), ("T", 2)])
+def test_rdf_counts_reproduce_the_reference_tool(tmp_path, k, tag, typ):
+    """the pair-distance counts of `snapcheck.py rdf`, printed as g(r), equal the
+    reference tool's own output line for line"""
+    import analysis
+    from oercel_b200 import cli
+    g, r = golden("aggregates.npz"), golden("rdf.npz")
+    p = tmp_path / "s.bin"
+    p.write_bytes(bytes(g[f"c{k}_snap"]))
+    s = cli.read_snapshot(str(p))
+    counts, n = analysis.rdf_counts(s["x"], s["y"], s["type"], s["L"], typ)
+    ref = bytes(r[f"c{k}_{tag}"]).decode().strip().split("\n")[1:]
+    assert analysis.rdf_lines(counts, n, s["L"]) == ref

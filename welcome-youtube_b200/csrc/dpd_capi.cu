@@ -1111,7 +1111,7 @@ extern "C" int dpd_pair_hist(dpd_handle *h, int32_t r, int32_t ta, int32_t tb, d
     if (!hist || nbin < 1 || nbin > 4096 || !(rmax > 0.0 && rmax <= 3.0))
         return fail(DPD_E_ARG, "need 1 <= nbin <= 4096 and 0 < rmax <= 3");
     CK(cudaMemsetAsync(h->b.hist, 0, nbin * sizeof(unsigned long long), h->s));
-    launch_pair_hist(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, ta, tb, (float)rmax, nbin, h->s);
+    launch_pair_hist(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, ta, tb, rmax, nbin, h->s);
     CK(cudaGetLastError());
     std::vector<unsigned long long> v(nbin);
     CK(cudaMemcpyAsync(v.data(), h->b.hist, nbin * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->s));

@@ -235,7 +235,7 @@ void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
                         bool virial, cudaStream_t s);
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
-                      int tb, float rmax, int nbin, cudaStream_t s);
+                      int tb, double rmax, int nbin, cudaStream_t s);
 void launch_pack(const Bufs &b, int cur, int b0, int n, const float *x, const float *y, const float *vx,
                  const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
                  const int32_t *next, cudaStream_t s);

@@ -682,23 +682,29 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
     }
 }
 
-// distances between types ta and tb within rmax (<= 3 cells), each unordered pair once
+// distances between types ta and tb (ta < 0: all beads) within rmax (<= 3
+// cells), each unordered pair once, binned as the reference's `snapcheck.py
+// rdf` bins them (np.histogram over [0, rmax] of pairs with d <= rmax,
+// cel/engine/tests/snapcheck.py:86-107): d in FP64 from the FP32 positions with
+// the minimum image, the bin from d * nbin / rmax corrected against the edges
+// k * (rmax / nbin), the last bin closed on the right
 __global__ void __launch_bounds__(BEAD_TPB) k_pair_hist(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                         const Chunk *__restrict__ ch, int rep_index, int ta, int tb,
-                                                        float rmax, int nbin) {
+                                                        double rmax, int nbin) {
     const Chunk c = ch[blockIdx.x];
     if (c.rep != rep_index) return;
     const RepDev &R = reps[c.rep];
     const int d = c.begin + (int)threadIdx.x;
     if (d >= c.end) return;
-    const uint32_t ti = b.tg[cur][d] >> TYPE_SHIFT;
-    if ((int)ti != ta && (int)ti != tb) return;
+    const int ti = (int)(b.tg[cur][d] >> TYPE_SHIFT);
+    if (ta >= 0 && ti != ta && ti != tb) return;
     const float2 *__restrict__ pos = b.pos[cur];
     const float2 pi = pos[d];
     const int ncx = R.ncx, ncy = R.ncy;
-    const int rc = (int)ceil((double)rmax * R.icsx);
+    const int rc = (int)ceil(rmax * R.icsx);
     const int rx = min(rc, (ncx - 1) / 2), ry = min(rc, (ncy - 1) / 2);
     const int32_t *cs = b.cstart + R.c0;
+    const double L = (double)R.L, norm = (double)nbin / rmax, step = rmax / (double)nbin;
     int cx, cy;
     cell_xy(R, pi.x, pi.y, cx, cy);
     for (int ox = -rx; ox <= rx; ox++)
@@ -707,14 +713,18 @@ __global__ void __launch_bounds__(BEAD_TPB) k_pair_hist(Bufs b, int cur, const R
             const int cc = nx * ncy + ny;
             for (int j = cs[cc]; j < cs[cc + 1]; j++) {
                 if (j <= d) continue;
-                const uint32_t tj = b.tg[cur][j] >> TYPE_SHIFT;
-                if (!(((int)ti == ta && (int)tj == tb) || ((int)ti == tb && (int)tj == ta))) continue;
+                const int tj = (int)(b.tg[cur][j] >> TYPE_SHIFT);
+                if (ta >= 0 && !((ti == ta && tj == tb) || (ti == tb && tj == ta))) continue;
                 const float2 pj = pos[j];
-                const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
-                const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
-                const double r = sqrt(dx * dx + dy * dy);
-                if (r >= (double)rmax) continue;
-                const int bin = (int)(r / (double)rmax * nbin);
+                double dx = (double)pi.x - (double)pj.x, dy = (double)pi.y - (double)pj.y;
+                dx -= L * rint(dx / L);
+                dy -= L * rint(dy / L);
+                const double r = hypot(dx, dy);
+                if (!(r <= rmax)) continue;
+                int bin = (int)(r * norm);
+                if (bin >= nbin) bin = nbin - 1;
+                if (r < bin * step) bin--;
+                else if (bin + 1 < nbin && r >= (bin + 1) * step) bin++;
                 if (bin >= 0 && bin < nbin) atomicAdd(b.hist + bin, 1ull);
             }
         }
@@ -868,7 +878,7 @@ void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *
 }
 
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
-                      int tb, float rmax, int nbin, cudaStream_t s) {
+                      int tb, double rmax, int nbin, cudaStream_t s) {
     k_pair_hist<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, ta, tb, rmax, nbin);
 }
 
