@@ -341,6 +341,34 @@ def rdf_fixture():
     np.savez_compressed(os.path.join(HERE, "rdf.npz"), **out)
 
 
+# membrane physics of cel/engine/params/membranes.ini (tied H2T2 pi lipids, k_bond 300, dt 0.03) on a small box
+MEMBRANE_INI = dict(L=24, dt=0.03, kT=1, gamma=4.5, warmup=200, f_lip=0.20, f_Ka=0.01, f_Kb=0, c_N=0.10, lip_arch="pi",
+                    lip_nT=1, lip_tie=1, r0_head=0.7, k_head=0, k_bond=300, r0=0.5, k_angle=15, a_W_H=20, a_W_T=200,
+                    a_H_T=50, a_W_N=45, a_H_N=22, a_T_N=120, a_W_K=45, a_H_K=30, a_T_K=200, chem=0, threads=8,
+                    steps=4000, snap_every=0, stats_every=10, ckpt_every=0, log_every=0)
+
+
+def membrane_stats_fixture(seeds=(5, 6)):
+    """the reference executable's stats rows (T_kin, max_bond every 10 steps)
+    over 4000 steps of the membrane physics, for two seeds"""
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "..", "..", "oracle", "_ref", "oercel_portable")
+    out = {}
+    for seed in seeds:
+        with tempfile.TemporaryDirectory() as td:
+            ini = os.path.join(td, "p.ini")
+            with open(ini, "w") as f:
+                f.write("".join(f"{k} = {v}\n" for k, v in dict(MEMBRANE_INI, seed=seed).items()))
+            subprocess.run([exe, ini, os.path.join(td, "o")], check=True, capture_output=True)
+            with open(os.path.join(td, "o", "stats.csv")) as f:
+                out[f"stats_{seed}"] = np.array([[float(v) for v in ln.split(",")]
+                                                 for ln in f.read().strip().split("\n")[1:]])
+    out["seeds"] = np.array(seeds)
+    out["ini"] = np.frombuffer("".join(f"{k} = {v}\n" for k, v in MEMBRANE_INI.items()).encode(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "membrane_stats.npz"), **out)
+
+
 def theta_fixture():
     lib = O.Ref.lib()
     rows = []
@@ -477,5 +505,6 @@ if __name__ == "__main__":
     aggregates_fixture()
     rdf_fixture()
     catalyst_rates_fixture()
+    membrane_stats_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))
