@@ -6,12 +6,16 @@ count exact (beads, clusters, largest, sum of squared sizes, neighbour
 counts); molecules and membrane aggregates (dpd_aggregates, the first stages
 of the reference's cells.detect) on evolved boxes of linear and pi lipids,
 every count and every bead's aggregate exact."""
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
 import analysis
 import oercel_b200 as ob
-from conftest import golden
+from conftest import PKG, golden
 from gpu_util import params
 from oercel_b200 import cli
 
@@ -107,3 +111,31 @@ def test_rdf_counts_of_reference_snapshots(cuda_ok, tmp_path, k):
         got = e.pair_hist(0, -1 if typ is None else typ, -1 if typ is None else typ, 3.0, 30)
         ref, _ = analysis.rdf_counts(s["x"], s["y"], s["type"], s["L"], typ)
         assert np.array_equal(got.astype(np.int64), ref), typ
+
+
+
+SNAPCHECK = os.path.join(PKG, "bin", "oercel_b200_snapcheck")
+
+
+@pytest.mark.parametrize("k", range(6))
+def test_snapcheck_drop_in_prints_what_the_reference_tool_prints(cuda_ok, tmp_path, k):
+    """`oercel_b200_snapcheck rdf|tclust SNAP` (GPU) prints the reference tool's
+    own output (tests/golden/rdf.npz, tclust.npz) byte for byte; g(r) of the
+    tail beads too, through the module's rdf(typ=2)"""
+    import io
+    from oercel_b200 import snapcheck
+    g, r = golden("aggregates.npz"), golden("rdf.npz")
+    p = tmp_path / "snap.bin"
+    p.write_bytes(bytes(g[f"c{k}_snap"]))
+    out = subprocess.run([sys.executable, SNAPCHECK, "rdf", str(p)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout == bytes(r[f"c{k}_all"]).decode()
+    buf = io.StringIO()
+    snapcheck.rdf([str(p)], 2, out=buf)
+    assert buf.getvalue() == bytes(r[f"c{k}_T"]).decode()
+    t = golden("tclust.npz")
+    if f"c{k}_line" in t.files:
+        out = subprocess.run([sys.executable, SNAPCHECK, "tclust", str(p)], capture_output=True, text=True,
+                             timeout=300)
+        assert out.returncode == 0, out.stderr[-2000:]
+        assert out.stdout.strip() == bytes(t[f"c{k}_line"]).decode()
