@@ -345,6 +345,44 @@ DPD_API int dpd_aggregates(dpd_handle *h, int32_t replica, double r_tail, int32_
  * positions, binned as np.histogram bins them. */
 DPD_API int dpd_pair_hist(dpd_handle *h, int32_t replica, int32_t ta, int32_t tb, double rmax, int32_t nbin, double *hist);
 
+/* ---- cell detection in one snapshot (the reference's cel/tools/cells.py) ----
+ * Stand-alone: no engine handle.  The thresholds of cells.py's DEFAULTS
+ * (cells.py:37-56), with the same names and meaning. */
+typedef struct {
+    double r_tail, h, r_stamp;
+    int32_t min_membrane_lipids, pad0;
+    double min_lumen_area, min_aqueous_frac, rho, pad, leaflet_in, leaflet_max, min_exposure, wall_extra;
+    double inner_frac_lo, inner_frac_hi;
+} dpd_cells_cfg;
+
+/* Columns of one detected cell, raw (unrounded) values:
+ * x, y (lumen centroid, wrapped), area, n_lipids, n_Ka, n_Kb, n_N, n_W, n_Z,
+ * agg, agg_lumens, agg_lipids, inner_heads, outer_heads, aspect, solidity
+ * (not capped at 1), extent, wraps_membrane (0/1), exposure, wall (inf when
+ * no distance to the bulk medium is finite).  Rounding as cells.py rounds its
+ * dict (cells.py:582-601) is left to the caller. */
+#define DPD_CELL_COLS 20
+typedef struct dpd_cells dpd_cells;
+
+DPD_API int dpd_cells_default(dpd_cells_cfg *cfg);
+/* detect(snap, cfg) (cells.py:331-611) on the GPU: x, y (n host values,
+ * already wrapped into [0, L), FP64 as the reference's snapshot reader gives
+ * them), type (n), bonds (nbond x 2 bead indices).  *out receives the result;
+ * free it with dpd_cells_free. */
+DPD_API int dpd_cells_detect(const dpd_cells_cfg *cfg, double L, int64_t n, const double *x, const double *y,
+                             const uint8_t *type, int64_t nbond, const int32_t *bonds, dpd_cells **out);
+/* info[0..5]: n_molecules, n_aggregates, n_membranes, lipids_in_small_aggregates,
+ * largest_aggregate, wrapping_membranes (the reference's summary); info[6] ng
+ * (label grid side), info[7] cells, info[8] membranes listed by
+ * dpd_cells_fetch's aggs; *h the pixel size. */
+DPD_API int dpd_cells_info(const dpd_cells *c, int64_t *info, double *h);
+/* Copies out (any pointer may be NULL): cells (cells x DPD_CELL_COLS), aggs
+ * (membranes x 4: agg, n_lipids, wraps, n_holes), label (ng x ng, -1 = no
+ * cell), bead_cell, mol and bead_agg (n each, as cells.py returns them). */
+DPD_API int dpd_cells_fetch(const dpd_cells *c, double *cells, int64_t *aggs, int32_t *label, int32_t *bead_cell,
+                            int32_t *mol, int32_t *bead_agg);
+DPD_API void dpd_cells_free(dpd_cells *c);
+
 /* the CUDA stream (cudaStream_t) this handle enqueues its work on */
 DPD_API int dpd_get_stream(const dpd_handle *h, void **stream);
 /* kernels one step of dpd_step launches: *n_plain in total, of which *n_chem

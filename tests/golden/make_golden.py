@@ -466,7 +466,61 @@ def run_fixture(name="run_L10_seed3.npz", **over):
                             ckpt_24=rd(f"{a}/ckpt.bin"))
 
 
+# hand-built scenes for cell detection (cell_scenes.py): (scene, seed, k x k tiling, configuration)
+CELL_CASES = [("vesicles", 1, 1, {}), ("vesicles", 2, 1, {}), ("vesicles", 3, 1, {}), ("network", 1, 1, {}),
+              ("network", 2, 1, {}), ("network", 3, 1, {}), ("vesicles", 1, 2, {}),
+              ("vesicles", 1, 1, dict(min_lumen_area=30.0)),
+              ("vesicles", 2, 1, dict(min_exposure=0.95, leaflet_in=1.2, r_stamp=0.8)),
+              ("network", 1, 1, dict(h=0.3)),
+              ("vesicles", 3, 1, dict(h=0.3, pad=1.0, min_membrane_lipids=20, inner_frac_range=(0.3, 0.5)))]
+
+
+def cells_fixture():
+    """every output of the reference's cells.detect (cells with their rounding,
+    label grid, per-bead maps, aggregates, summary) on the scenes of CELL_CASES,
+    with the snapshot files it read"""
+    import json
+    import tempfile
+    sys.path.insert(0, os.path.join(REF_ROOT, "cel", "tools"))
+    import cell_scenes as cs
+    import cells
+    import ocio
+
+    def js(v):
+        return np.frombuffer(json.dumps(v, default=lambda o: o.item()).encode(), np.uint8)
+
+    out = {}
+    for k, (name, seed, tile, cfg) in enumerate(CELL_CASES):
+        sc = cs.SCENES[name](seed)
+        L = sc.L
+        x, y, t, b = sc.arrays()
+        if tile > 1:
+            L, x, y, t, b = cs.tile(L, x, y, t, b, tile)
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "s.bin")
+            cs.write_snap(path, L, x, y, t, b)
+            with open(path, "rb") as f:
+                raw = f.read()
+            r = cells.detect(ocio.read_snapshot(path), cfg)
+        out[f"c{k}_snap"] = np.frombuffer(raw, np.uint8)
+        out[f"c{k}_cfg"] = js(cfg)
+        out[f"c{k}_cells"] = js(r["cells"])
+        out[f"c{k}_aggregates"] = js(r["aggregates"])
+        out[f"c{k}_summary"] = js(r["summary"])
+        out[f"c{k}_label"] = r["label"]
+        for key in ("bead_cell", "mol", "bead_agg"):
+            out[f"c{k}_{key}"] = np.asarray(r[key], np.int32)
+        out[f"c{k}_h"] = np.float64(r["h"])
+        out[f"c{k}_ng"] = np.int64(r["ng"])
+        print(name, seed, tile, cfg, r["summary"], len(r["cells"]), "cells")
+    np.savez_compressed(os.path.join(HERE, "cells.npz"), **out)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1:  # only the named fixtures, e.g. `make_golden.py cells`
+        for name in sys.argv[1:]:
+            globals()[f"{name}_fixture"]()
+        sys.exit(0)
     if not O.Ref.available():
         sys.exit("oracle/_ref/libref_oercel.so is missing: run make -C oracle with the reference sources present")
     soup_fixture()
@@ -506,5 +560,6 @@ if __name__ == "__main__":
     rdf_fixture()
     catalyst_rates_fixture()
     membrane_stats_fixture()
+    cells_fixture()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

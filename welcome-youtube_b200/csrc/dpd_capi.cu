@@ -27,6 +27,12 @@ static int fail(int code, const char *fmt, ...) {
     return code;
 }
 
+// the error message of a call made outside this file (dpd_cells.cu)
+int lib_error(int code, const char *msg) {
+    g_err = msg;
+    return code;
+}
+
 #define CK(call)                                                                                        \
     do {                                                                                                \
         cudaError_t e_ = (call);                                                                        \

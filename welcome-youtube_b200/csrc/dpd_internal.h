@@ -261,6 +261,7 @@ void launch_adj_gather(const uint32_t *tg, const RepDev *rep, const Chunk *bch, 
 void launch_adj_save(int n, const float2 *pos, const float2 *vt, const uint32_t *tg, const int2 *link, float2 *opos,
                      float2 *ovt, uint32_t *otg, int2 *olink, cudaStream_t s);
 int chem_kernel_count();
+int lib_error(int code, const char *msg);  // sets dpd_last_error() and returns code
 // the break stage and the candidate draws on the current sorted state (phase entry point)
 void launch_chem_scan(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 // the growth and bonding stages over the candidate lists (part 0..3, or all with part < 0)

@@ -74,6 +74,18 @@ class DpdRdfSpec(C.Structure):
                 ("rmax", C.c_double), ("sigma", C.c_double), ("horizon", C.c_int32), ("pad", C.c_int32)]
 
 
+class DpdCellsCfg(C.Structure):
+    _fields_ = [("r_tail", C.c_double), ("h", C.c_double), ("r_stamp", C.c_double),
+                ("min_membrane_lipids", C.c_int32), ("pad0", C.c_int32),
+                ("min_lumen_area", C.c_double), ("min_aqueous_frac", C.c_double), ("rho", C.c_double),
+                ("pad", C.c_double), ("leaflet_in", C.c_double), ("leaflet_max", C.c_double),
+                ("min_exposure", C.c_double), ("wall_extra", C.c_double), ("inner_frac_lo", C.c_double),
+                ("inner_frac_hi", C.c_double)]
+
+
+CELL_COLS = 20
+
+
 class DpdEvent(C.Structure):
     _fields_ = [("step", C.c_int64), ("kind", C.c_int32), ("gid", C.c_uint32), ("partner", C.c_uint32),
                 ("x", C.c_float), ("y", C.c_float), ("replica", C.c_int32)]
@@ -88,7 +100,8 @@ EXPORTS = [
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
     "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters", "dpd_xoshiro_jump",
-    "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode",
+    "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode", "dpd_cells_default", "dpd_cells_detect",
+    "dpd_cells_info", "dpd_cells_fetch", "dpd_cells_free",
 ]
 NGRAD = 66
 
@@ -167,6 +180,11 @@ def load(path: str | None = None):
         "dpd_sync": ([vp], C.c_int),
         "dpd_set_graph_steps": ([vp, i32], C.c_int),
         "dpd_profile_step": ([vp, C.POINTER(C.c_float), i32, C.POINTER(C.c_int32)], C.c_int),
+        "dpd_cells_default": ([C.POINTER(DpdCellsCfg)], C.c_int),
+        "dpd_cells_detect": ([C.POINTER(DpdCellsCfg), dbl, i64, fp, fp, fp, i64, fp, C.POINTER(vp)], C.c_int),
+        "dpd_cells_info": ([vp, fp, C.POINTER(C.c_double)], C.c_int),
+        "dpd_cells_fetch": ([vp, fp, fp, fp, fp, fp, fp], C.c_int),
+        "dpd_cells_free": ([vp], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
