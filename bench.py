@@ -316,7 +316,8 @@ def analysis_rates(eng, p, reps=5):
     aref = analysis.aggregates(x, y, t, bonds, float(np.float32(p.L)), 1.0, 12)
     agg_cpu_ms = (time.perf_counter() - t0) * 1000.0
     agg_same = all(agg[k] == aref[k] for k in aref if k != "labels") and np.array_equal(agg["labels"], aref["labels"])
-    return {"gpu_ms": gpu_ms, "cpu_ms": cpu_ms, "same_result": same, "beads": int(p.n_beads()), "t_beads": ref["n"],
+    cells = cell_rates()
+    return {"cells": cells, "gpu_ms": gpu_ms, "cpu_ms": cpu_ms, "same_result": same, "beads": int(p.n_beads()), "t_beads": ref["n"],
             "clusters": ref["clusters"], "aggregates": {"gpu_ms": agg_gpu_ms, "cpu_ms": agg_cpu_ms,
                                                         "same_result": bool(agg_same),
                                                         "molecules": aref["n_molecules"],
@@ -324,6 +325,34 @@ def analysis_rates(eng, p, reps=5):
             "timing": "host clock around each call (device synchronised; the aggregates call includes the copy of "
                       "the per-bead labels); CPU: the oracle's restatements of the reference tools (scipy), 1 thread",
             "kind": "port"}
+
+
+def cell_rates(reps=3):
+    """the reference's cell detection (cells.detect) on the GPU, end to end from
+    host arrays: a 56 x 56 scene of vesicles (free, across the edge, on the
+    corner, nested, dry, open) tiled k x k, L = 448 and 1792; a tiled box must
+    hold k^2 times the base box's cells"""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import cell_scenes as cs
+
+    from oercel_b200 import cells
+    sc = cs.vesicles(1)
+    x, y, t, b = sc.arrays()
+    base = len(cells.detect(cells.Snapshot(0, 0.0, sc.L, x.astype(np.float64), y.astype(np.float64), t, b))["cells"])
+    out = []
+    for k in (8, 32):
+        L, X, Y, T, B = cs.tile(sc.L, x, y, t, b, k)
+        s = cells.Snapshot(0, 0.0, L, X, Y, T, B)
+        r = cells.detect(s)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            cells.detect(s)
+            ts.append(time.perf_counter() - t0)
+        out.append({"L": L, "beads": int(len(T)), "grid": int(r["ng"]), "cells": len(r["cells"]),
+                    "k2_cells": len(r["cells"]) == k * k * base, "gpu_ms": round(1000.0 * min(ts), 2)})
+    return out
 
 
 def catalyst_rates(torch, steps=200, ref_steps=40):
