@@ -378,9 +378,11 @@ DPD_API int dpd_cells_detect(const dpd_cells_cfg *cfg, double L, int64_t n, cons
 DPD_API int dpd_cells_info(const dpd_cells *c, int64_t *info, double *h);
 /* Copies out (any pointer may be NULL): cells (cells x DPD_CELL_COLS), aggs
  * (membranes x 4: agg, n_lipids, wraps, n_holes), label (ng x ng, -1 = no
- * cell), bead_cell, mol and bead_agg (n each, as cells.py returns them). */
-DPD_API int dpd_cells_fetch(const dpd_cells *c, double *cells, int64_t *aggs, int32_t *label, int32_t *bead_cell,
-                            int32_t *mol, int32_t *bead_agg);
+ * cell; label_bytes 2 gives int16 as cells.py does below 32767 cells, 4 gives
+ * int32), bead_cell, mol and bead_agg (n each, as cells.py returns them).  The
+ * grid and the per-bead arrays stay on the device until fetched. */
+DPD_API int dpd_cells_fetch(const dpd_cells *c, double *cells, int64_t *aggs, void *label, int32_t label_bytes,
+                            int32_t *bead_cell, int32_t *mol, int32_t *bead_agg);
 DPD_API void dpd_cells_free(dpd_cells *c);
 
 /* the CUDA stream (cudaStream_t) this handle enqueues its work on */

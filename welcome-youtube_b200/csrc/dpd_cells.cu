@@ -49,11 +49,16 @@
 
 struct dpd_cells {
     double h = 0;
-    int64_t ng = 0;
+    int64_t ng = 0, n = 0;
     int64_t summary[6] = {0, 0, 0, 0, 0, 0};
     std::vector<int64_t> aggs;  // 4 per membrane
     std::vector<double> cells;  // DPD_CELL_COLS per cell
-    std::vector<int32_t> label, bead_cell, mol, bead_agg;
+    // on the device until fetched: label grid (ng x ng), per-bead cell, molecule, aggregate
+    int32_t *label = nullptr, *bead_cell = nullptr, *mol = nullptr, *bead_agg = nullptr;
+    ~dpd_cells() {
+        for (int32_t *p : {label, bead_cell, mol, bead_agg})
+            if (p) cudaFree(p);
+    }
 };
 
 namespace dpd_cells_impl {
@@ -85,14 +90,27 @@ struct Ctx {
     cudaStream_t s = nullptr;
     std::vector<void *> mem;
     int *err = nullptr;  // device flags: 1 union retries exhausted, 2 inconsistent torus roots, 4 key range
+    void *tmp = nullptr;  // CUB scratch, grown on demand and kept for the whole call
+    size_t tmp_bytes = 0;
+    long long *pin = nullptr;  // pinned host words for small read-backs
     void init() {
         CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        CU(cudaMallocHost((void **)&pin, 4 * sizeof(long long)));
         err = zeros<int>(1);
     }
     ~Ctx() {
         if (s) cudaStreamSynchronize(s);
         for (void *p : mem) cudaFree(p);
+        if (pin) cudaFreeHost(pin);
         if (s) cudaStreamDestroy(s);
+    }
+    void *scratch(size_t bytes) {
+        if (bytes > tmp_bytes) {
+            if (tmp) release(tmp);
+            tmp = alloc<char>(bytes + bytes / 2);
+            tmp_bytes = bytes + bytes / 2;
+        }
+        return tmp;
     }
     template <class T> T *alloc(size_t n) {
         void *p = nullptr;
@@ -103,6 +121,10 @@ struct Ctx {
         }
         mem.push_back(p);
         return (T *)p;
+    }
+    void adopt(void *p) {  // the caller keeps p: it is not freed with the context
+        auto it = std::find(mem.begin(), mem.end(), p);
+        if (it != mem.end()) mem.erase(it);
     }
     void release(void *p) {
         auto it = std::find(mem.begin(), mem.end(), p);
@@ -154,11 +176,27 @@ template <class T> T scan(Ctx &c, const T *in, T *out, long long n) {
     if (n <= 0) return 0;
     size_t tb = 0;
     CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, c.s));
-    void *t = c.alloc<char>(tb);
+    void *t = c.scratch(tb);
     CU(cub::DeviceScan::ExclusiveSum(t, tb, in, out, n, c.s));
-    const T a = c.get(out + n - 1), b = c.get(in + n - 1);
-    c.release(t);
-    return a + b;
+    T *h = (T *)c.pin;
+    CU(cudaMemcpyAsync(h, out + n - 1, sizeof(T), cudaMemcpyDeviceToHost, c.s));
+    CU(cudaMemcpyAsync(h + 1, in + n - 1, sizeof(T), cudaMemcpyDeviceToHost, c.s));
+    CU(cudaStreamSynchronize(c.s));
+    return h[0] + h[1];
+}
+
+struct MaxOp {
+    __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
+};
+
+// inclusive running maximum: with key[p] = p at the start of each run of a row
+// and -1 elsewhere, every pixel gets the first pixel of its run
+void max_scan(Ctx &c, const int *in, int *out, long long n) {
+    if (n <= 0) return;
+    size_t tb = 0;
+    CU(cub::DeviceScan::InclusiveScan(nullptr, tb, in, out, MaxOp(), n, c.s));
+    void *t = c.scratch(tb);
+    CU(cub::DeviceScan::InclusiveScan(t, tb, in, out, MaxOp(), n, c.s));
 }
 
 // the indices i < n with flag[i] == 1, increasing
@@ -180,11 +218,10 @@ void sort_pairs(Ctx &c, int *key, int *val, int n, int end_bit) {
     int *k2 = c.alloc<int>(n), *v2 = c.alloc<int>(n);
     size_t tb = 0;
     CU(cub::DeviceRadixSort::SortPairs(nullptr, tb, key, k2, val, v2, n, 0, end_bit, c.s));
-    void *t = c.alloc<char>(tb);
+    void *t = c.scratch(tb);
     CU(cub::DeviceRadixSort::SortPairs(t, tb, key, k2, val, v2, n, 0, end_bit, c.s));
     CU(cudaMemcpyAsync(key, k2, n * sizeof(int), cudaMemcpyDeviceToDevice, c.s));
     CU(cudaMemcpyAsync(val, v2, n * sizeof(int), cudaMemcpyDeviceToDevice, c.s));
-    c.release(t);
     c.release(k2);
     c.release(v2);
 }
@@ -194,10 +231,9 @@ void sort_keys(Ctx &c, unsigned long long *key, int n, int end_bit) {
     unsigned long long *k2 = c.alloc<unsigned long long>(n);
     size_t tb = 0;
     CU(cub::DeviceRadixSort::SortKeys(nullptr, tb, key, k2, n, 0, end_bit, c.s));
-    void *t = c.alloc<char>(tb);
+    void *t = c.scratch(tb);
     CU(cub::DeviceRadixSort::SortKeys(t, tb, key, k2, n, 0, end_bit, c.s));
     CU(cudaMemcpyAsync(key, k2, (size_t)n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, c.s));
-    c.release(t);
     c.release(k2);
 }
 
@@ -311,6 +347,13 @@ __device__ __forceinline__ void wunion(unsigned long long *par, int a, int b, in
         }
     }
     atomicOr(err, 1);
+}
+
+// counter[key] += 1 with one atomic per distinct key among the warp's active
+// threads: most pixels of a labelling pass add to the same few roots
+template <class T> __device__ __forceinline__ void agg_inc(T *counter, int key) {
+    const unsigned grp = __match_any_sync(__activemask(), key);
+    if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(counter + key, (T)__popc(grp));
 }
 
 __device__ __forceinline__ int find_seg(const long long *base, int nseg, long long p) {  // base[s] <= p < base[s+1]
@@ -722,17 +765,28 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
                 if (ii >= 0 && ii < s0 && jj >= 0 && jj < s1) memb[BB[b] + ii * s1 + jj] = 1;
             }
         });
-        int *lp = c.alloc<int>(P);
-        c.each(Pi, [=] __device__(long long p) { lp[p] = memb[p] ? -1 : (int)p; });
+        // every solvent pixel starts under the first pixel of its row run; a
+        // vertical union is needed only where an overlap of two runs begins
+        int *lp = c.alloc<int>(P), *rk = c.alloc<int>(P);
+        c.each(Pi, [=] __device__(long long p) {
+            const int b = find_seg(BB, nbox, p);
+            const long long j = (p - BB[b]) % BS1[b];
+            rk[p] = (memb[p] || j == 0 || memb[p - 1]) ? (int)p : -1;
+        });
+        max_scan(c, rk, lp, P);
+        c.each(Pi, [=] __device__(long long p) {
+            if (memb[p]) lp[p] = -1;
+        });
         c.each(Pi, [=] __device__(long long p) {
             if (memb[p]) return;
             const int b = find_seg(BB, nbox, p);
             const long long loc = p - BB[b];
             const int s0 = BS0[b], s1 = BS1[b];
             const long long i = loc / s1, j = loc % s1;
-            if (j + 1 < s1 && !memb[p + 1]) uf_union(lp, (int)p, (int)p + 1, err);
-            if (i + 1 < s0 && !memb[p + s1]) uf_union(lp, (int)p, (int)(p + s1), err);
+            if (i + 1 < s0 && !memb[p + s1] && (j == 0 || memb[p - 1] || memb[p - 1 + s1]))
+                uf_union(lp, (int)p, (int)(p + s1), err);
         });
+        c.release(rk);
         int *sz = c.zeros<int>(P), *bord = c.zeros<int>(P);
         c.each(Pi, [=] __device__(long long p) {
             if (memb[p]) return;
@@ -741,7 +795,7 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             const int s0 = BS0[b], s1 = BS1[b];
             const long long i = loc / s1, j = loc % s1;
             const int r = uf_find(lp, (int)p);
-            atomicAdd(sz + r, 1);
+            agg_inc(sz, r);
             if (i == 0 || i == s0 - 1 || j == 0 || j == s1 - 1) bord[r] = 1;
         });
         c.check_flags("local holes");
@@ -812,14 +866,26 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             const long long pi = pmod((long long)floor(X[i] / h), ngl), pj = pmod((long long)floor(Y[i] / h), ngl);
             for (int o = 0; o < noff; o++) memb[pmod(pi + OFF[o].x, ngl) * ngl + pmod(pj + OFF[o].y, ngl)] = 1;
         });
+        // row runs as in the boxes; unions (and the offset checks below) only on
+        // the edges that leave a run: across the box edge along a row, and where
+        // an overlap of two vertically adjacent runs begins.  Any other edge
+        // closes a square of edges whose offsets are already consistent.
         unsigned long long *wp = c.alloc<unsigned long long>(G);
-        c.each(Gi, [=] __device__(long long p) { wp[p] = memb[p] ? ~0ull : wpack((int)p, 0, 0); });
+        int *rk = c.alloc<int>(G), *rs = c.alloc<int>(G);
+        c.each(Gi, [=] __device__(long long p) {
+            const long long j = p % ngl;
+            rk[p] = (memb[p] || j == 0 || memb[p - 1]) ? (int)p : -1;
+        });
+        max_scan(c, rk, rs, G);
+        c.each(Gi, [=] __device__(long long p) { wp[p] = memb[p] ? ~0ull : wpack(rs[p], 0, 0); });
+        c.release(rk);
+        c.release(rs);
         c.each(Gi, [=] __device__(long long p) {
             if (memb[p]) return;
             const long long i = p / ngl, j = p % ngl;
-            const long long q1 = i * ngl + (j + 1 == ngl ? 0 : j + 1), q2 = (i + 1 == ngl ? 0 : i + 1) * ngl + j;
-            if (!memb[q1]) wunion(wp, (int)p, (int)q1, 0, j + 1 == ngl ? 1 : 0, err);
-            if (!memb[q2]) wunion(wp, (int)p, (int)q2, i + 1 == ngl ? 1 : 0, 0, err);
+            if (j + 1 == ngl && !memb[i * ngl]) wunion(wp, (int)p, (int)(i * ngl), 0, 1, err);
+            const long long q = (i + 1 == ngl ? 0 : i + 1) * ngl + j;
+            if (!memb[q] && (j == 0 || memb[p - 1] || memb[q - 1])) wunion(wp, (int)p, (int)q, i + 1 == ngl ? 1 : 0, 0, err);
         });
         int *wflag = c.zeros<int>(G), *cnt = c.zeros<int>(G);
         unsigned long long *si = c.zeros<unsigned long long>(G), *sj = c.zeros<unsigned long long>(G);
@@ -832,12 +898,14 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             const int sx[2] = {0, i + 1 == ngl ? 1 : 0}, sy[2] = {j + 1 == ngl ? 1 : 0, 0};
             for (int k = 0; k < 2; k++) {
                 if (memb[q[k]]) continue;
+                if (k == 0 && j + 1 != ngl) continue;                            // inside a run
+                if (k == 1 && j != 0 && !memb[p - 1] && !memb[q[1] - 1]) continue;  // inside an overlap
                 int qx, qy;
                 const int rq = wfind(wp, (int)q[k], qx, qy);
                 if (rq != r) atomicOr(err, 2);
                 if (qx != ox + sx[k] || qy != oy + sy[k]) wflag[r] = 1;
             }
-            atomicAdd(cnt + r, 1);
+            agg_inc(cnt, r);
             atomicAdd(si + r, (unsigned long long)(i + (long long)ox * ngl));
             atomicAdd(sj + r, (unsigned long long)(j + (long long)oy * ngl));
         });
@@ -955,10 +1023,16 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
     if (nent64 >= INT_MAX) throw Fail{DPD_E_ARG, "cell detection: lumens exceed 2^31 pixels"};
     const int nent = (int)nent64;
     int2 *LP = c.alloc<int2>(nent);
-    for (int k = 0; k < nl; k++)
-        if (lumens[k].cnt)
-            CU(cudaMemcpyAsync(LP + hloff[k], lumens[k].src, lumens[k].cnt * sizeof(int2), cudaMemcpyDeviceToDevice, c.s));
     const long long *LOFF = c.upload(hloff);
+    {  // one gather of every lumen's pixel list, in the sorted order
+        std::vector<unsigned long long> hsrc(std::max(nl, 1));
+        for (int k = 0; k < nl; k++) hsrc[k] = (unsigned long long)(uintptr_t)lumens[k].src;
+        const unsigned long long *SRC = c.upload(hsrc);
+        c.each(nent, [=] __device__(long long e) {
+            const int k = find_seg(LOFF, nl, e);
+            LP[e] = ((const int2 *)(uintptr_t)SRC[k])[e - LOFF[k]];
+        });
+    }
     int *lid = c.alloc<int>(nent);
     c.each(nent, [=] __device__(long long e) { lid[e] = find_seg(LOFF, nl, e); });
     const long long ngl = ng;
@@ -980,7 +1054,8 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
     });
     unsigned long long *apx = c.zeros<unsigned long long>(std::max(nl, 1));
     c.each(Gi, [=] __device__(long long p) {
-        if (label[p] >= 0) atomicAdd(apx + label[p], 1ull);
+        const int l = label[p];
+        if (l >= 0) agg_inc(apx, l);
     });
 
     // bulk medium and the lumen tests (cells.py:420-459)
@@ -1000,18 +1075,26 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             const long long pi = gflat[i] / ngl, pj = gflat[i] % ngl;
             for (int o = 0; o < noff; o++) memb[pmod(pi + OFF[o].x, ngl) * ngl + pmod(pj + OFF[o].y, ngl)] = 1;
         });
-        int *gp = c.alloc<int>(G);
-        c.each(Gi, [=] __device__(long long p) { gp[p] = memb[p] ? -1 : (int)p; });
+        int *gp = c.alloc<int>(G), *rk = c.alloc<int>(G);
+        c.each(Gi, [=] __device__(long long p) {
+            const long long j = p % ngl;
+            rk[p] = (memb[p] || j == 0 || memb[p - 1]) ? (int)p : -1;
+        });
+        max_scan(c, rk, gp, G);
+        c.release(rk);
+        c.each(Gi, [=] __device__(long long p) {
+            if (memb[p]) gp[p] = -1;
+        });
         c.each(Gi, [=] __device__(long long p) {
             if (memb[p]) return;
             const long long i = p / ngl, j = p % ngl;
-            const long long q1 = i * ngl + (j + 1 == ngl ? 0 : j + 1), q2 = (i + 1 == ngl ? 0 : i + 1) * ngl + j;
-            if (!memb[q1]) uf_union(gp, (int)p, (int)q1, err);
-            if (!memb[q2]) uf_union(gp, (int)p, (int)q2, err);
+            if (j + 1 == ngl && !memb[i * ngl]) uf_union(gp, (int)p, (int)(i * ngl), err);
+            const long long q = (i + 1 == ngl ? 0 : i + 1) * ngl + j;
+            if (!memb[q] && (j == 0 || memb[p - 1] || memb[q - 1])) uf_union(gp, (int)p, (int)q, err);
         });
         int *garea = c.zeros<int>(G);
         c.each(Gi, [=] __device__(long long p) {
-            if (!memb[p]) atomicAdd(garea + uf_find(gp, (int)p), 1);
+            if (!memb[p]) agg_inc(garea, uf_find(gp, (int)p));
         });
         c.check_flags("bulk medium");
         int *pf = c.alloc<int>(G);
@@ -1059,16 +1142,18 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             double d = INFINITY;
             if (oa) {
                 const long long pi = pmod(LP[e].x, ngl), pj = pmod(LP[e].y, ngl);
+                // rows and columns outward from the pixel, each scan stopped once
+                // it cannot beat the nearest found so far
                 long long best = LLONG_MAX;
-                for (int dx = -Mpx; dx <= Mpx; dx++) {
-                    const long long dx2 = (long long)dx * dx;
-                    if (dx2 >= best) continue;
-                    const long long row = pmod(pi + dx, ngl) * ngl;
-                    for (int dy = -Mpx; dy <= Mpx; dy++) {
-                        const long long d2 = dx2 + (long long)dy * dy;
-                        if (d2 < best && outside[row + pmod(pj + dy, ngl)]) best = d2;
+                for (int ax = 0; ax <= Mpx && (long long)ax * ax < best; ax++)
+                    for (int sx = 0; sx < (ax ? 2 : 1); sx++) {
+                        const long long row = pmod(pi + (sx ? -ax : ax), ngl) * ngl;
+                        for (int ay = 0; ay <= Mpx; ay++) {
+                            const long long d2 = (long long)ax * ax + (long long)ay * ay;
+                            if (d2 >= best) break;
+                            if (outside[row + pmod(pj + ay, ngl)] || outside[row + pmod(pj - ay, ngl)]) best = d2;
+                        }
                     }
-                }
                 if (best != LLONG_MAX) d = sqrt((double)best) * h;
             }
             dob[e] = d;
@@ -1092,16 +1177,20 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             keep.push_back(k);
     }
     // median distance of the kept lumens' boundary (numpy's median)
+    std::vector<double> hdob;
+    std::vector<uint8_t> hsel;
+    if (!keep.empty()) {
+        hdob = c.download(dob, nent);
+        hsel = c.download(sel, nent);
+    }
     for (int k : keep) {
         const long long o = hloff[k], m = lumens[k].cnt;
-        const std::vector<double> d = c.download(dob + o, m);
-        const std::vector<uint8_t> s = c.download(sel + o, m);
         std::vector<double> v;
         bool fin = false;
-        for (long long e = 0; e < m; e++)
-            if (s[e]) {
-                v.push_back(d[e]);
-                fin |= std::isfinite(d[e]);
+        for (long long e = o; e < o + m; e++)
+            if (hsel[e]) {
+                v.push_back(hdob[e]);
+                fin |= std::isfinite(hdob[e]);
             }
         if (!fin || v.empty()) continue;
         std::sort(v.begin(), v.end());
@@ -1341,11 +1430,13 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
     }
     out.summary[5] = nwrap;
     out.cells = rows;
-    out.label = c.download(label, G);
-    out.bead_cell = c.download(bcell, n);
-    out.mol = c.download(mol, n);
-    out.bead_agg = c.download(bagg, n);
+    out.n = n;
     CU(cudaStreamSynchronize(c.s));
+    for (void *p : {(void *)label, (void *)bcell, (void *)mol, (void *)bagg}) c.adopt(p);
+    out.label = label;
+    out.bead_cell = bcell;
+    out.mol = mol;
+    out.bead_agg = bagg;
 }
 
 }  // namespace dpd_cells_impl
@@ -1399,17 +1490,39 @@ extern "C" int dpd_cells_info(const dpd_cells *c, int64_t *info, double *h) {
     return DPD_OK;
 }
 
-extern "C" int dpd_cells_fetch(const dpd_cells *c, double *cells, int64_t *aggs, int32_t *label, int32_t *bead_cell,
-                               int32_t *mol, int32_t *bead_agg) {
+extern "C" int dpd_cells_fetch(const dpd_cells *c, double *cells, int64_t *aggs, void *label, int32_t label_bytes,
+                               int32_t *bead_cell, int32_t *mol, int32_t *bead_agg) {
     if (!c) return lib_error(DPD_E_ARG, "dpd_cells_fetch: null");
+    if (label && label_bytes != 4 && label_bytes != 2) return lib_error(DPD_E_ARG, "dpd_cells_fetch: label_bytes must be 2 or 4");
+    const int64_t ncell = (int64_t)(c->cells.size() / DPD_CELL_COLS);
+    if (label && label_bytes == 2 && ncell >= 32767)
+        return lib_error(DPD_E_ARG, "dpd_cells_fetch: 32767 or more cells need a 4-byte label grid");
     if (cells && !c->cells.empty()) std::memcpy(cells, c->cells.data(), c->cells.size() * sizeof(double));
     if (aggs && !c->aggs.empty()) std::memcpy(aggs, c->aggs.data(), c->aggs.size() * sizeof(int64_t));
-    if (label && !c->label.empty()) std::memcpy(label, c->label.data(), c->label.size() * sizeof(int32_t));
-    if (bead_cell && !c->bead_cell.empty())
-        std::memcpy(bead_cell, c->bead_cell.data(), c->bead_cell.size() * sizeof(int32_t));
-    if (mol && !c->mol.empty()) std::memcpy(mol, c->mol.data(), c->mol.size() * sizeof(int32_t));
-    if (bead_agg && !c->bead_agg.empty())
-        std::memcpy(bead_agg, c->bead_agg.data(), c->bead_agg.size() * sizeof(int32_t));
+    const long long G = c->ng * c->ng;
+    if (label && G) {
+        if (label_bytes == 4) {
+            if (cudaMemcpy(label, c->label, G * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return lib_error(DPD_E_CUDA, "dpd_cells_fetch: copy of the label grid failed");
+        } else {
+            int16_t *d = nullptr;
+            if (cudaMalloc(&d, G * sizeof(int16_t)) != cudaSuccess) {
+                cudaGetLastError();
+                return lib_error(DPD_E_NOMEM, "dpd_cells_fetch: device allocation failed");
+            }
+            const int32_t *src = c->label;
+            dpd_cells_impl::k_each<<<(unsigned)((G + dpd_cells_impl::TPB - 1) / dpd_cells_impl::TPB),
+                                     dpd_cells_impl::TPB>>>(G, [=] __device__(long long p) { d[p] = (int16_t)src[p]; });
+            const cudaError_t e = cudaMemcpy(label, d, G * sizeof(int16_t), cudaMemcpyDeviceToHost);
+            cudaFree(d);
+            if (e != cudaSuccess) return lib_error(DPD_E_CUDA, "dpd_cells_fetch: copy of the label grid failed");
+        }
+    }
+    const int32_t *src[3] = {c->bead_cell, c->mol, c->bead_agg};
+    int32_t *dst[3] = {bead_cell, mol, bead_agg};
+    for (int k = 0; k < 3; k++)
+        if (dst[k] && c->n && cudaMemcpy(dst[k], src[k], c->n * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return lib_error(DPD_E_CUDA, "dpd_cells_fetch: copy of a per-bead array failed");
     return DPD_OK;
 }
 

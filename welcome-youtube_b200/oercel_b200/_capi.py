@@ -183,7 +183,7 @@ def load(path: str | None = None):
         "dpd_cells_default": ([C.POINTER(DpdCellsCfg)], C.c_int),
         "dpd_cells_detect": ([C.POINTER(DpdCellsCfg), dbl, i64, fp, fp, fp, i64, fp, C.POINTER(vp)], C.c_int),
         "dpd_cells_info": ([vp, fp, C.POINTER(C.c_double)], C.c_int),
-        "dpd_cells_fetch": ([vp, fp, fp, fp, fp, fp, fp], C.c_int),
+        "dpd_cells_fetch": ([vp, fp, fp, fp, i32, fp, fp, fp], C.c_int),
         "dpd_cells_free": ([vp], None),
     }
     for name, (args, res) in sig.items():

@@ -141,11 +141,12 @@ def detect(snap, cfg=None):
         ng, ncell, nagg = int(info[6]), int(info[7]), int(info[8])
         rows = np.zeros((ncell, CELL_COLS))
         aggs = np.zeros((nagg, 4), np.int64)
-        label = np.empty((ng, ng), np.int32)
+        label = np.empty((ng, ng), np.int16 if ncell < INT16_LABELS else np.int32)
         bead_cell = np.empty(n, np.int32)
         mol = np.empty(n, np.int32)
         bead_agg = np.empty(n, np.int32)
-        check(lib.dpd_cells_fetch(h, ptr(rows), ptr(aggs), ptr(label), ptr(bead_cell), ptr(mol), ptr(bead_agg)))
+        check(lib.dpd_cells_fetch(h, ptr(rows), ptr(aggs), ptr(label), label.itemsize, ptr(bead_cell), ptr(mol),
+                                  ptr(bead_agg)))
     finally:
         lib.dpd_cells_free(h)
     cells = [_cell_dict(j, r) for j, r in enumerate(rows)]
@@ -153,6 +154,5 @@ def detect(snap, cfg=None):
                    lipids_in_small_aggregates=int(info[3]), largest_aggregate=int(info[4]),
                    wrapping_membranes=int(info[5]))
     agg_info = [dict(agg=int(a), n_lipids=int(k), wraps=bool(w), n_holes=int(nh)) for a, k, w, nh in aggs]
-    ldt = np.int16 if len(cells) < INT16_LABELS else np.int32
-    return dict(cells=cells, label=label.astype(ldt), bead_cell=bead_cell, h=float(hh.value), ng=ng,
+    return dict(cells=cells, label=label, bead_cell=bead_cell, h=float(hh.value), ng=ng,
                 aggregates=agg_info, summary=summary, mol=mol.astype(np.int64), bead_agg=bead_agg.astype(np.int64))
