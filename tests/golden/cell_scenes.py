@@ -121,7 +121,7 @@ class Scene:
             self.typ.append(t)
 
     def arrays(self):
-        p = np.asarray(self.pos, np.float64) % self.L
+        p = np.asarray(self.pos, np.float64).reshape(-1, 2) % self.L
         x = p[:, 0].astype(np.float32)
         y = p[:, 1].astype(np.float32)
         x[x >= np.float32(self.L)] = 0
@@ -192,4 +192,43 @@ def network(seed):
     return s
 
 
-SCENES = {"vesicles": vesicles, "network": network}
+def water(seed):
+    """L = 20: solvent only, no lipid"""
+    s = Scene(20, seed)
+    s.solvent()
+    return s
+
+
+def micelles(seed):
+    """L = 20: two micelles and free lipids, no membrane"""
+    s = Scene(20, seed)
+    s.micelle(5, 5, 8)
+    s.micelle(14, 14, 7)
+    s.free_lipids(5)
+    s.solvent()
+    return s
+
+
+def tiny(seed):
+    """L = 2.5, a box under three tail-contact cells wide: three lipids in water"""
+    s = Scene(2.5, seed)
+    s.free_lipids(3)
+    s.solvent()
+    return s
+
+
+def lone(seed):
+    """L = 16: one vesicle whose lumen is too small to count"""
+    s = Scene(16, seed)
+    s.ring(8, 8, 4.5)
+    s.solvent()
+    return s
+
+
+def empty(seed):
+    """L = 16 with no bead at all"""
+    return Scene(16, seed)
+
+
+SCENES = {"vesicles": vesicles, "network": network, "water": water, "micelles": micelles, "tiny": tiny,
+          "lone": lone, "empty": empty}
