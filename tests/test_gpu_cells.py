@@ -7,7 +7,9 @@ and on the corner, a nested pair, a dry and an open vesicle, micelles, free
 lipids; a membrane network that wraps the box and encloses lumens (one across
 the edge) with a vesicle fused onto it; a 2 x 2 tiling; and, under other
 configurations, a pixel size that is not a power of two (h = 0.3), another
-stamp radius, thresholds and padding.  The GPU must give
+stamp radius, thresholds and padding; and the edge cases: water only,
+micelles only, a box under three contact cells wide, a lumen too small to
+count, no beads at all.  The GPU must give
 the same summary, membrane list, label grid, per-bead maps and cells; every
 cell field equal after the reference's rounding, except the centroid (FP64
 sums in another order: 1e-9) and the shape fields computed through an
