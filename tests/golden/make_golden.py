@@ -477,10 +477,21 @@ CELL_CASES = [("vesicles", 1, 1, {}), ("vesicles", 2, 1, {}), ("vesicles", 3, 1,
               ("empty", 5, 1, {})]
 
 
+# reference runs that grow membranes (linear and tied pi lipids), L = 48, 30000 steps; their
+# snapshots at the listed steps are the evolved cases of cells_fixture
+EVOLVED_CELL_RUNS = {
+    "lin48": (dict(L=48, dt=0.03, kT=1, gamma=4.5, warmup=200, f_Ka=0.0, f_Kb=0, c_N=0.05, chem=0, seed=21,
+                   lip_arch="linear", lip_nH=1, lip_nT=3, f_lip=0.3, k_angle=10, a_W_T=100), (20000, 30000)),
+    "pi48": (dict(L=48, dt=0.03, kT=1, gamma=4.5, warmup=200, f_Ka=0.0, f_Kb=0, c_N=0.05, chem=0, seed=22,
+                  lip_arch="pi", lip_nT=2, lip_tie=1, f_lip=0.35, k_angle=15, a_W_T=200), (20000, 30000)),
+}
+
+
 def cells_fixture():
     """every output of the reference's cells.detect (cells with their rounding,
-    label grid, per-bead maps, aggregates, summary) on the scenes of CELL_CASES,
-    with the snapshot files it read"""
+    label grid, per-bead maps, aggregates, summary) on the scenes of CELL_CASES
+    and on snapshots of the reference engine's EVOLVED_CELL_RUNS, with the
+    snapshot files it read"""
     import json
     import tempfile
     sys.path.insert(0, os.path.join(REF_ROOT, "cel", "tools"))
@@ -515,6 +526,34 @@ def cells_fixture():
         out[f"c{k}_h"] = np.float64(r["h"])
         out[f"c{k}_ng"] = np.int64(r["ng"])
         print(name, seed, tile, cfg, r["summary"], len(r["cells"]), "cells")
+    import subprocess
+    exe = os.path.join(HERE, "..", "..", "oracle", "_ref", "oercel_portable")
+    k = len(CELL_CASES)
+    for name, (kv, steps) in EVOLVED_CELL_RUNS.items():
+        kv = dict(kv, threads=16, steps=max(steps), snap_every=10000, stats_every=max(steps), ckpt_every=0,
+                  log_every=0)
+        with tempfile.TemporaryDirectory() as td:
+            ini = os.path.join(td, "p.ini")
+            with open(ini, "w") as f:
+                f.write("".join(f"{a} = {v}\n" for a, v in kv.items()))
+            subprocess.run([exe, ini, os.path.join(td, "o")], check=True, capture_output=True)
+            for st in steps:
+                path = os.path.join(td, "o", f"snap_{st:010d}.bin")
+                with open(path, "rb") as f:
+                    raw = f.read()
+                r = cells.detect(ocio.read_snapshot(path))
+                out[f"c{k}_snap"] = np.frombuffer(raw, np.uint8)
+                out[f"c{k}_cfg"] = js({})
+                out[f"c{k}_cells"] = js(r["cells"])
+                out[f"c{k}_aggregates"] = js(r["aggregates"])
+                out[f"c{k}_summary"] = js(r["summary"])
+                out[f"c{k}_label"] = r["label"]
+                for key in ("bead_cell", "mol", "bead_agg"):
+                    out[f"c{k}_{key}"] = np.asarray(r[key], np.int32)
+                out[f"c{k}_h"] = np.float64(r["h"])
+                out[f"c{k}_ng"] = np.int64(r["ng"])
+                print(name, st, r["summary"], len(r["cells"]), "cells")
+                k += 1
     np.savez_compressed(os.path.join(HERE, "cells.npz"), **out)
 
 

@@ -9,7 +9,9 @@ the edge) with a vesicle fused onto it; a 2 x 2 tiling; and, under other
 configurations, a pixel size that is not a power of two (h = 0.3), another
 stamp radius, thresholds and padding; and the edge cases: water only,
 micelles only, a box under three contact cells wide, a lumen too small to
-count, no beads at all.  The GPU must give
+count, no beads at all; and four snapshots that the reference executable wrote
+after 20,000 and 30,000 steps of membrane-forming runs (one membrane wraps the
+box with eleven holes).  The GPU must give
 the same summary, membrane list, label grid, per-bead maps and cells; every
 cell field equal after the reference's rounding, except the centroid (FP64
 sums in another order: 1e-9) and the shape fields computed through an
