@@ -28,11 +28,12 @@ import sys
 import numpy as np
 import pytest
 
+import oercel_b200 as ob
 from conftest import GOLDEN, golden
 
 sys.path.insert(0, GOLDEN)
 import cell_scenes as cs  # noqa: E402
-from oercel_b200 import cells  # noqa: E402
+from oercel_b200 import cells, cli  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 EXACT = ("id", "area", "r_eq", "n_lipids", "n_Ka", "n_Kb", "n_N", "n_W", "n_Z", "agg", "agg_lumens", "agg_lipids",
@@ -90,3 +91,23 @@ def test_tiled_box_has_k2_times_the_cells(cuda_ok, k):
     assert sorted(c["area"] for c in big["cells"]) == sorted([c["area"] for c in base["cells"]] * (k * k))
     assert big["summary"]["n_membranes"] == k * k * base["summary"]["n_membranes"]
     assert big["label"].shape == (base["ng"] * k, base["ng"] * k)
+
+
+def test_engine_detect_cells_equals_its_snapshot_file(cuda_ok, tmp_path):
+    """Engine.detect_cells on a box of tied pi lipids after 3000 steps gives what
+    detect gives on the snapshot file the drop-in executable writes for it"""
+    p = ob.Params(L=48, dt=0.03, gamma=4.5, warmup=200, f_Ka=0.0, f_Kb=0.0, c_N=0.05, chem=0, seed=22,
+                  lip_arch="pi", lip_nT=2, lip_tie=1, f_lip=0.35, k_angle=15, a_W_T=200)
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(3000)
+    got = e.detect_cells()
+    path = str(tmp_path / "snap.bin")
+    cli.write_snapshot(path, e.state(0), e.step_no, 0.0, float(p.L), p.template())
+    ref = cells.detect(cells.read_snapshot(path))
+    assert got["summary"] == ref["summary"] and got["summary"]["n_membranes"] > 0
+    assert got["aggregates"] == ref["aggregates"]
+    for key in ("label", "bead_cell", "mol", "bead_agg"):
+        assert np.array_equal(got[key], ref[key]), key
+    assert got["cells"] == ref["cells"]

@@ -83,9 +83,10 @@ def template_bonds(state, mol):
     return np.stack([lo[order], hi[order]], axis=1).astype(np.int32)
 
 
-def write_snapshot(path, state, step, time_, L, mol=None):
-    """SPEC section 5: OCEL v1, positions and types in gid order, bonds (i < j);
-    mol: the template of branched lipids (their bonds), None for linear chains"""
+def snapshot_arrays(state, mol=None):
+    """the contents of a snapshot: positions and types in gid order, bonds (i < j)
+    in the reference's order; mol: the template of branched lipids (their
+    bonds), None for linear chains"""
     n = len(state["x"])
     g = state["gid"].astype(np.int64)
     x = np.empty(n, np.float32)
@@ -101,6 +102,14 @@ def write_snapshot(path, state, step, time_, L, mol=None):
         order = np.lexsort((gj, gi))  # by the bond's chain-side (prev) bead, as the reference orders by template start
         lo, hi = np.minimum(gi, gj)[order], np.maximum(gi, gj)[order]
         bonds = np.stack([lo, hi], axis=1).astype(np.int32)
+    return x, y, t, bonds
+
+
+def write_snapshot(path, state, step, time_, L, mol=None):
+    """SPEC section 5: OCEL v1, positions and types in gid order, bonds (i < j);
+    mol: the template of branched lipids (their bonds), None for linear chains"""
+    x, y, t, bonds = snapshot_arrays(state, mol)
+    n = len(t)
     tmp = path + ".tmp"
     with open(tmp, "wb") as f:
         f.write(b"OCEL")

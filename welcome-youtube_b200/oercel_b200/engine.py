@@ -264,6 +264,24 @@ class Engine:
             res["labels"] = lab
         return res
 
+    def snapshot(self, replica=0):
+        """the replica's current configuration as the reference's tools read a
+        snapshot file (oercel_b200.cells.Snapshot: FP64 positions in gid order,
+        wrapped into [0, L), types, bonds)"""
+        from . import cells, cli
+        p = self.params[replica]
+        mol = p.template() if p.lip_arch != "linear" else None
+        x, y, t, b = cli.snapshot_arrays(self.state(replica), mol)
+        L = float(p.L)
+        return cells.Snapshot(step=self.step_no, time=0.0, L=L, x=cells._wrap(x.astype(np.float64), L),
+                              y=cells._wrap(y.astype(np.float64), L), type=t, bonds=b.astype(np.int64))
+
+    def detect_cells(self, replica=0, cfg=None):
+        """the reference's cell detection (cells.detect) on the replica's current
+        configuration, without a snapshot file"""
+        from . import cells
+        return cells.detect(self.snapshot(replica), cfg)
+
     def pair_hist(self, replica, ta, tb, rmax, nbin):
         h = np.zeros(nbin)
         check(self.lib.dpd_pair_hist(self.h, replica, ta, tb, float(rmax), nbin, ptr(h)))
