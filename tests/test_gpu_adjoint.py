@@ -157,3 +157,48 @@ def test_fit_moves_repulsion_toward_target(cuda_ok):
     hist = fit.fit(e, ["a_W_T"], target[0], iters=6, window=60, ckpt=20, spec=spec, lr=2.0)
     assert hist[-1]["values"][0] > 60.0
     assert all(np.isfinite(h["loss"]) for h in hist)
+
+
+def test_batched_adjoint_rows_equal_solo_boxes(cuda_ok):
+    """configuration 5 at reduced size: 4 of its 64 boxes (L = 128, lipid
+    fraction U(0.1, 0.3)) in one engine; each replica's loss and gradient row
+    equal those of the same box run alone"""
+    from oercel_b200 import workloads
+    ps = workloads.config5(n_replicas=4)
+    spec = ob.Engine.rdf_spec(nbin=64, rmax=2.0, sigma=0.05, last_steps=10, horizon=10)
+    target = np.ones(64)
+    e = ob.Engine(ps)
+    for r in range(len(ps)):
+        e.load_soup(r)
+    e.prime()
+    e.step(50)
+    loss, grad, _ = e.window_adjoint(40, 20, spec, target)
+    for r, p in enumerate(ps):
+        s = ob.Engine(p)
+        s.load_soup(0)
+        s.prime()
+        s.step(50)
+        l1, g1, _ = s.window_adjoint(40, 20, spec, target)
+        assert loss[r] == pytest.approx(l1[0], rel=1e-9)
+        assert np.allclose(grad[r], g1[0], rtol=1e-6, atol=1e-9 * np.abs(g1[0]).max())
+        s.close()
+
+
+def test_batched_fit_moves_the_shared_repulsion(cuda_ok):
+    """configuration 5's pattern on 4 boxes: per-box targets g_TT(r) made at
+    a_W_T = 75, one a_W_T shared by every box fitted from 60 with the summed
+    gradient rows"""
+    from oercel_b200 import fit, workloads
+    truth = workloads.config5(n_replicas=4)
+    e = ob.Engine(truth)
+    for r in range(len(truth)):
+        e.load_soup(r)
+    e.prime()
+    e.step(200)
+    spec = ob.Engine.rdf_spec(nbin=32, rmax=2.0, sigma=0.1, last_steps=20, horizon=10)
+    _, target = e.window_loss(60, spec, np.zeros(32))
+    for r, p in enumerate(workloads.config5(n_replicas=4, a_wt=60.0)):
+        e.set_params(r, p)
+    hist = fit.fit(e, ["a_W_T"], target, iters=6, window=60, ckpt=20, spec=spec, lr=2.0)
+    assert hist[-1]["values"][0] > 60.0
+    assert all(np.isfinite(h["loss"]) for h in hist)
