@@ -612,7 +612,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=1000)
+    ap.add_argument("--e2e-steps", type=int, default=10000,
+                    help="steps of the end-to-end run (default: the 10^4 steps of the 1M-bead configuration)")
     ap.add_argument("--cpu-steps", type=int, default=100)
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

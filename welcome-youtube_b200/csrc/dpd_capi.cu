@@ -422,6 +422,8 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.status, 1));
     TRY(dalloc(h, &b.step, 1));
     TRY(dalloc(h, &b.obs, (size_t)nrep * OBS_N));
+    TRY(dalloc(h, &b.obs_out, (size_t)nrep * OBS_N));
+    TRY(dalloc(h, &b.obs_done, (size_t)nrep));
     TRY(dalloc(h, &b.hist, 4096));
     TRY(dalloc(h, &b.stir, (size_t)nrep));
     TRY(dalloc(h, &b.rng, (size_t)4 * nrep));
@@ -481,6 +483,7 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     CK(cudaMemset(b.status, 0, sizeof(DevStatus)));
     CK(cudaMemset(b.step, 0, sizeof(long long)));
     CK(cudaMemset(b.obs, 0, (size_t)nrep * OBS_N * sizeof(unsigned long long)));
+    CK(cudaMemset(b.obs_done, 0, (size_t)nrep * sizeof(unsigned int)));
     for (int k = 0; k < 2; k++) {
         CK(cudaMemset(b.pos[k], 0, N * sizeof(float2)));
         CK(cudaMemset(b.vh[k], 0, N * sizeof(float2)));
@@ -1058,15 +1061,14 @@ extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_
     return DPD_OK;
 }
 
-// the sums of a stats row on the stream, copied into v (OBS_N words) when the stream gets there
+// the sums of a stats row on the stream, copied into v (OBS_N words) when the
+// stream gets there: one kernel, whose last block hands the row over to obs_out
+// and clears the running sums (the max bond restarts per stats row), and one copy
 static int enqueue_observables(dpd_handle *h, int32_t r, bool virial, unsigned long long *v) {
-    unsigned long long *o = h->b.obs + (size_t)r * OBS_N;
-    CK(cudaMemsetAsync(o, 0, 4 * sizeof(unsigned long long), h->s));
-    CK(cudaMemsetAsync(o + 5, 0, (OBS_N - 5) * sizeof(unsigned long long), h->s));
     launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, h->s);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(v, o, OBS_N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->s));
-    CK(cudaMemsetAsync(o + 4, 0, sizeof(unsigned long long), h->s));  // max bond restarts per stats row
+    CK(cudaMemcpyAsync(v, h->b.obs_out + (size_t)r * OBS_N, OBS_N * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, h->s));
     return DPD_OK;
 }
 

@@ -149,7 +149,9 @@ struct Bufs {
     int32_t evcap;
     DevStatus *status;
     long long *step;            // step number of the forces being computed
-    unsigned long long *obs;    // OBS_N per replica
+    unsigned long long *obs;    // OBS_N per replica: the running sums (zero between stats rows)
+    unsigned long long *obs_out;  // OBS_N per replica: the last stats row, handed over by k_observables
+    unsigned int *obs_done;     // per replica: blocks of k_observables finished
     unsigned long long *hist;   // pair histogram scratch
     long long *stir;            // per replica: sum of the stirring terms (fixed point) of the current positions
     uint64_t *rng;              // per replica: the serial xoshiro256** state of the catalyst chemistry (4 words)

@@ -680,6 +680,19 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
         const int slot = threadIdx.x < 4 ? (int)threadIdx.x : threadIdx.x == 4 ? 5 : 8 + (int)threadIdx.x - 5;
         if (sum != 0) atomicAdd(b.obs + (size_t)rep_index * OBS_N + slot, (unsigned long long)sum);
     }
+    // the last block to finish hands the row over and clears the sums for the next one
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(b.obs_done + rep_index, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        if (threadIdx.x < OBS_N)
+            b.obs_out[(size_t)rep_index * OBS_N + threadIdx.x] =
+                atomicExch(b.obs + (size_t)rep_index * OBS_N + threadIdx.x, 0ull);
+        if (threadIdx.x == 0) b.obs_done[rep_index] = 0u;
+    }
 }
 
 // distances between types ta and tb (ta < 0: all beads) within rmax (<= 3
