@@ -237,6 +237,47 @@ def time_steps(torch, eng, K, flush):
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
 
+def reference_ensemble(steps=100):
+    """the reference CPU engine on the 256-replica ensemble, sweep style: one
+    single-threaded process per host core, each on a replica drawn evenly from
+    the ensemble's list, all at once; each process's rate from its own timing
+    line (step phases only), summed"""
+    import numpy as np
+
+    from oercel_b200 import workloads
+    from oercel_b200.workloads import reference_ini
+    exe, isa = reference_binary()
+    if exe is None:
+        return {"error": "oracle/_ref/oercel not built"}
+    reps = workloads.config3()
+    cores = os.cpu_count() or 1
+    idx = [int(i) for i in np.linspace(0, len(reps) - 1, min(cores, len(reps)))]
+    rates, beads = [], []
+    with tempfile.TemporaryDirectory() as td:
+        procs = []
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        for k, i in enumerate(idx):
+            p, _ = reps[i]
+            ini = os.path.join(td, f"p{k}.ini")
+            with open(ini, "w") as f:
+                f.write(reference_ini(p, steps, 1))
+            procs.append((subprocess.Popen([exe, ini, os.path.join(td, f"o{k}")], stdout=subprocess.PIPE,
+                                           stderr=subprocess.PIPE, text=True, env=env), p.n_beads()))
+        for pr, n in procs:
+            out, _ = pr.communicate(timeout=1800)
+            m = re.search(r"timing: (\d+) steps, [\d.]+ ms/step \(integrate ([\d.]+), sort ([\d.]+), pair ([\d.]+), "
+                          r"bonded ([\d.]+), chem ([\d.]+)", out)
+            if not m:
+                return {"error": out[-300:]}
+            ms = sum(float(v) for v in m.groups()[1:])
+            rates.append(n * 1000.0 / ms)
+            beads.append(n)
+    return {"value": float(sum(rates)), "unit": UNIT, "processes": len(idx), "cores": cores, "threads_each": 1,
+            "steps": steps, "beads_run": int(sum(beads)), "isa": isa,
+            "sample": f"{len(idx)} of the 256 replicas (evenly over the list), one single-threaded reference "
+                      f"process each, run together; chemistry off (the lipid rules do not exist in the reference)"}
+
+
 def batched_rates(torch, steps=64):
     """256-replica ensemble in one engine vs the same replicas one engine at a
     time; both run graphs of `steps` steps (captured before timing)"""
@@ -588,6 +629,8 @@ def ours(args, rank, local_rank, ws):
         res["e2e"] = e2e_rate(Engine, p, args.e2e_steps)
         if not args.skip_batched and ws == 1:
             res["batched"] = batched_rates(torch)
+            if not args.skip_cpu:
+                res["batched"]["cpu_reference"] = reference_ensemble()
             res["adjoint"] = adjoint_ratio(torch)
             res["batched_adjoint"] = batched_adjoint(torch)
             res["catalyst"] = catalyst_rates(torch)
