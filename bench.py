@@ -507,13 +507,14 @@ def batched_adjoint(torch, window=500, ckpt=25, last=50):
                       "loss; an optimizer iteration of the configuration is one adjoint call"}
 
 
-def e2e_rate(eng_cls, p, K):
+def e2e_rate(eng_cls, p, K, ws=1):
     """the public API from host memory: load the soup from pinned host buffers,
     prime, then K steps, each a one-step graph followed by its stats row copied
     into pinned host memory (dpd_stats_async) and an event; the host decodes the
     row of step k - 1 while step k runs (one step of pipelining); the event log
     read back every 20 steps and at the end, the final state read back; wall
-    clock around all of it (the graph capture included)"""
+    clock around all of it (the graph capture included).  With ws ranks, every
+    rank runs its own box at once and the slowest rank's clock counts."""
     import numpy as np
     import torch
 
@@ -534,6 +535,9 @@ def e2e_rate(eng_cls, p, K):
     stream = torch.cuda.ExternalStream(eng.stream())
     done = [torch.cuda.Event() for _ in range(2)]
     torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
     t0 = time.perf_counter()
     eng.set_state(0, pin["x"], pin["y"], pin["vx"], pin["vy"], pin["type"], None, pin["prev"], pin["next"])
     eng.prime()
@@ -555,13 +559,19 @@ def e2e_rate(eng_cls, p, K):
     st = eng.state(0)
     el = time.perf_counter() - t0
     eng.close()
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
     assert all(0.1 < t < 10.0 for t in temps)
     h2d = n * (4 * 4 + 1 + 4 + 4)
     d2h = nev * 32 + n * (8 * 4 + 1 + 3 * 4)
-    return {"value": n * K / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d / K),
-            "d2h_bytes_per_step": int(d2h / K + 16 * 8), "steps": K,
+    return {"value": n * K * ws / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d / K) * ws,
+            "d2h_bytes_per_step": int(d2h / K + 16 * 8) * ws, "steps": K,
             "note": "state upload and final read-back amortised over the steps; the stats row read back and decoded "
-                    "every step, one step behind the device; the events every 20 steps"}
+                    "every step, one step behind the device; the events every 20 steps; bytes and rate over all "
+                    "ranks, each with its own box"}
 
 
 def ours(args, rank, local_rank, ws):
@@ -620,13 +630,15 @@ def ours(args, rank, local_rank, ws):
                              "frac": value / ws * STEP_BYTES_CHEM / 1e9 / peak},
            "kernels_ms": kernels, "gpu_launches": n_plain * args.steps, "clocks": clk.summary(),
            "tuning": tuned}
-    if rank == 0 and args.quick:
-        print(json.dumps(res))
+    if args.quick:
+        if rank == 0:
+            print(json.dumps(res))
         return
+    e2e = e2e_rate(Engine, p, args.e2e_steps, ws)  # every rank, its own box
     if rank == 0:
         if ana is not None:
             res["analysis"] = ana
-        res["e2e"] = e2e_rate(Engine, p, args.e2e_steps)
+        res["e2e"] = e2e
         if not args.skip_batched and ws == 1:
             res["batched"] = batched_rates(torch)
             if not args.skip_cpu:
