@@ -473,6 +473,7 @@ CELL_CASES = [("vesicles", 1, 1, {}), ("vesicles", 2, 1, {}), ("vesicles", 3, 1,
               ("vesicles", 2, 1, dict(min_exposure=0.95, leaflet_in=1.2, r_stamp=0.8)),
               ("network", 1, 1, dict(h=0.3)),
               ("vesicles", 3, 1, dict(h=0.3, pad=1.0, min_membrane_lipids=20, inner_frac_range=(0.3, 0.5))),
+              ("vesicles", 1, 1, dict(min_lumen_area=30.0, inner_frac_range=(0.362, 0.62))),
               ("water", 1, 1, {}), ("micelles", 2, 1, {}), ("tiny", 3, 1, {}), ("lone", 4, 1, {}),
               ("empty", 5, 1, {})]
 
