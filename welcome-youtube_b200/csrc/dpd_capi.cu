@@ -1065,10 +1065,18 @@ extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_
 // stream gets there: one kernel, whose last block hands the row over to obs_out
 // and clears the running sums (the max bond restarts per stats row), and one copy
 static int enqueue_observables(dpd_handle *h, int32_t r, bool virial, unsigned long long *v) {
-    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, h->s);
+    // pinned host memory the device can reach: the kernel writes the row there itself
+    unsigned long long *direct = nullptr;
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, v) == cudaSuccess && pa.type == cudaMemoryTypeHost &&
+        pa.devicePointer == (void *)v)
+        direct = v;
+    cudaGetLastError();
+    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, direct, h->s);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(v, h->b.obs_out + (size_t)r * OBS_N, OBS_N * sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, h->s));
+    if (!direct)
+        CK(cudaMemcpyAsync(v, h->b.obs_out + (size_t)r * OBS_N, OBS_N * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, h->s));
     return DPD_OK;
 }
 

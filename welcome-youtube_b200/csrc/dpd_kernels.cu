@@ -279,6 +279,8 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
 
 // ---------------------------------------------------------------- permute (+ integrate)
 
+#define OBS_ITEMS 4  // chunks per round of k_observables
+
 #ifndef PERM_ITEMS
 #define PERM_ITEMS 1
 #endif
@@ -614,53 +616,82 @@ __global__ void __launch_bounds__(BEAD_TPB) k_integrate(Bufs b, int cur, const R
 // then leaves one atomic per quantity per block.
 template <bool VIRIAL>
 __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                          const Chunk *__restrict__ ch, int rep_index) {
+                                                          const Chunk *__restrict__ ch, int rep_index,
+                                                          unsigned long long *__restrict__ host_out) {
     __shared__ long long red[BEAD_TPB / 32][5 + DPD_MAXT];
     const RepDev &R = reps[rep_index];
     long long sx = 0, sy = 0, s2 = 0, vir = 0, heads = 0;
     int cnt[DPD_MAXT];
 #pragma unroll
     for (int t = 0; t < DPD_MAXT; t++) cnt[t] = 0;
-    for (int k = (int)blockIdx.x; k < R.nch; k += (int)gridDim.x) {
-        const Chunk c = ch[R.ch0 + k];
-        const int d = c.begin + (int)threadIdx.x;
-        if (d >= c.end) continue;
-        const float2 v = b.vh[cur][d], f = b.f[cur][d];
-        const double vx = (double)v.x + (double)R.hdt * (double)f.x, vy = (double)v.y + (double)R.hdt * (double)f.y;
-        sx += __double2ll_rn(vx * OBS_FIX);
-        sy += __double2ll_rn(vy * OBS_FIX);
-        s2 += __double2ll_rn((vx * vx + vy * vy) * OBS_FIX);
-        const uint32_t tgi = b.tg[cur][d];
-        const int ty = (int)(tgi >> TYPE_SHIFT);
+    // OBS_ITEMS chunks per round, their loads issued together (the chunk
+    // descriptor, then the bead, are two dependent loads: more in flight)
+    const int G = (int)gridDim.x;
+    for (int k0 = (int)blockIdx.x; k0 < R.nch; k0 += OBS_ITEMS * G) {
+        int d[OBS_ITEMS];
+        bool act[OBS_ITEMS];
 #pragma unroll
-        for (int t = 0; t < DPD_MAXT; t++) cnt[t] += ty == t;
-        const int2 lk = b.link[cur][d];
-        heads += (lk.x < 0 && lk.y >= 0) ? 1 : 0;
-        // virial: pairs (d, j) with j > d inside the cutoff
-        if (VIRIAL) {
-            const float2 *__restrict__ pos = b.pos[cur];
-            const float2 pi = pos[d];
-            const int ncx = R.ncx, ncy = R.ncy;
-            const int32_t *cs = b.cstart + R.c0;
-            int cx, cy;
-            cell_xy(R, pi.x, pi.y, cx, cy);
-            double accv = 0.0;
-            for (int ox = -1; ox <= 1; ox++)
-                for (int oy = -1; oy <= 1; oy++) {
-                    const int nx = (cx + ox + ncx) % ncx, ny = (cy + oy + ncy) % ncy;
-                    const int cc = nx * ncy + ny;
-                    for (int j = cs[cc]; j < cs[cc + 1]; j++) {
-                        if (j <= d) continue;
-                        const float2 pj = pos[j];
-                        const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
-                        const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
-                        const double r2 = dx * dx + dy * dy;
-                        if (!(r2 < 1.0 && r2 > 1e-24)) continue;
-                        const double r = sqrt(r2);
-                        accv += (double)a_at(R, ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT), *b.step) * (1.0 - r) * r;
+        for (int u = 0; u < OBS_ITEMS; u++) {
+            const int k = k0 + u * G;
+            act[u] = false;
+            d[u] = 0;
+            if (k < R.nch) {
+                const Chunk c = ch[R.ch0 + k];
+                d[u] = c.begin + (int)threadIdx.x;
+                act[u] = d[u] < c.end;
+            }
+        }
+        float2 v[OBS_ITEMS], f[OBS_ITEMS];
+        uint32_t tgv[OBS_ITEMS];
+        int2 lk[OBS_ITEMS];
+#pragma unroll
+        for (int u = 0; u < OBS_ITEMS; u++) {
+            if (!act[u]) continue;
+            v[u] = b.vh[cur][d[u]];
+            f[u] = b.f[cur][d[u]];
+            tgv[u] = b.tg[cur][d[u]];
+            lk[u] = b.link[cur][d[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < OBS_ITEMS; u++) {
+            if (!act[u]) continue;
+            const double vx = (double)v[u].x + (double)R.hdt * (double)f[u].x;
+            const double vy = (double)v[u].y + (double)R.hdt * (double)f[u].y;
+            sx += __double2ll_rn(vx * OBS_FIX);
+            sy += __double2ll_rn(vy * OBS_FIX);
+            s2 += __double2ll_rn((vx * vx + vy * vy) * OBS_FIX);
+            const int ty = (int)(tgv[u] >> TYPE_SHIFT);
+#pragma unroll
+            for (int t = 0; t < DPD_MAXT; t++) cnt[t] += ty == t;
+            heads += (lk[u].x < 0 && lk[u].y >= 0) ? 1 : 0;
+            // virial: pairs (d, j) with j > d inside the cutoff
+            if (VIRIAL) {
+                const int dd = d[u];
+                const float2 *__restrict__ pos = b.pos[cur];
+                const float2 pi = pos[dd];
+                const int ncx = R.ncx, ncy = R.ncy;
+                const int32_t *cs = b.cstart + R.c0;
+                int cx, cy;
+                cell_xy(R, pi.x, pi.y, cx, cy);
+                double accv = 0.0;
+                for (int ox = -1; ox <= 1; ox++)
+                    for (int oy = -1; oy <= 1; oy++) {
+                        const int nx = (cx + ox + ncx) % ncx, ny = (cy + oy + ncy) % ncy;
+                        const int cc = nx * ncy + ny;
+                        for (int j = cs[cc]; j < cs[cc + 1]; j++) {
+                            if (j <= dd) continue;
+                            const float2 pj = pos[j];
+                            const double dx = (double)minimg(__fsub_rn(pi.x, pj.x), R.L, R.halfL);
+                            const double dy = (double)minimg(__fsub_rn(pi.y, pj.y), R.L, R.halfL);
+                            const double r2 = dx * dx + dy * dy;
+                            if (!(r2 < 1.0 && r2 > 1e-24)) continue;
+                            const double r = sqrt(r2);
+                            accv += (double)a_at(R, ty * DPD_MAXT + (b.tg[cur][j] >> TYPE_SHIFT), *b.step) *
+                                    (1.0 - r) * r;
+                        }
                     }
-                }
-            vir += __double2ll_rn(accv * OBS_FIX);
+                vir += __double2ll_rn(accv * OBS_FIX);
+            }
         }
     }
     long long q[5 + DPD_MAXT] = {sx, sy, s2, vir, heads};
@@ -680,7 +711,9 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
         const int slot = threadIdx.x < 4 ? (int)threadIdx.x : threadIdx.x == 4 ? 5 : 8 + (int)threadIdx.x - 5;
         if (sum != 0) atomicAdd(b.obs + (size_t)rep_index * OBS_N + slot, (unsigned long long)sum);
     }
-    // the last block to finish hands the row over and clears the sums for the next one
+    // the last block to finish hands the row over (to obs_out and, when given,
+    // straight into the caller's pinned host buffer) and clears the sums for the
+    // next row
     __shared__ bool last;
     __threadfence();
     __syncthreads();
@@ -688,9 +721,11 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
     __syncthreads();
     if (last) {
         __threadfence();
-        if (threadIdx.x < OBS_N)
-            b.obs_out[(size_t)rep_index * OBS_N + threadIdx.x] =
-                atomicExch(b.obs + (size_t)rep_index * OBS_N + threadIdx.x, 0ull);
+        if (threadIdx.x < OBS_N) {
+            const unsigned long long v = atomicExch(b.obs + (size_t)rep_index * OBS_N + threadIdx.x, 0ull);
+            b.obs_out[(size_t)rep_index * OBS_N + threadIdx.x] = v;
+            if (host_out) host_out[threadIdx.x] = v;
+        }
         if (threadIdx.x == 0) b.obs_done[rep_index] = 0u;
     }
 }
@@ -884,10 +919,10 @@ void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bc
 }
 
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
-                        bool virial, cudaStream_t s) {
-    const int grid = std::min(nbch, 148 * 4);  // grid-stride over the replica's chunks
-    if (virial) k_observables<true><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
-    else k_observables<false><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index);
+                        bool virial, unsigned long long *host_out, cudaStream_t s) {
+    const int grid = std::min(nbch, 148 * 8);  // grid-stride over the replica's chunks
+    if (virial) k_observables<true><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, host_out);
+    else k_observables<false><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, host_out);
 }
 
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
