@@ -48,3 +48,18 @@ def test_cell_row_to_dict():
     assert d["solidity"] == 1.0 and d["aspect"] == 1.011 and d["extent"] == 15.57 and d["wall"] == 4.81
     row[19] = math.inf
     assert cells._cell_dict(0, row)["wall"] is None
+
+
+def test_detect_refuses_unwrapped_positions_and_bad_bonds():
+    """checked on the host before anything reaches the device"""
+    import pytest
+    from oercel_b200 import DpdError
+    x = np.array([1.0, 2.0, 3.0])
+    s = cells.Snapshot(0, 0.0, 8.0, x, np.array([1.0, 8.0, 2.0]), np.array([1, 2, 0], np.uint8),
+                       np.array([[0, 1]], np.int64))
+    with pytest.raises(DpdError, match="outside"):
+        cells.detect(s)
+    s.y = np.array([1.0, 2.0, 3.0])
+    s.bonds = np.array([[0, 5]], np.int64)
+    with pytest.raises(DpdError, match="bond index"):
+        cells.detect(s)

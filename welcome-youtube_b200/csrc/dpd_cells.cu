@@ -431,6 +431,9 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
     const int nbd = (int)nbond;
     for (long long e = 0; e < 2 * nbond; e++)
         if (hbond[e] < 0 || hbond[e] >= n) throw Fail{DPD_E_ARG, "cell detection: a bond index is out of range"};
+    for (int i = 0; i < n; i++)
+        if (!(hx[i] >= 0.0 && hx[i] < L && hy[i] >= 0.0 && hy[i] < L))
+            throw Fail{DPD_E_ARG, "cell detection: a position is outside [0, L) (wrap the snapshot's positions)"};
     const long long ng = (long long)std::nearbyint(L / cfg.h);  // round half to even, as Python's round
     if (ng < 4 || ng > 21845) throw Fail{DPD_E_ARG, "cell detection: the label grid side L/h must be 4..21845"};
     const double h = L / (double)ng;
