@@ -194,10 +194,13 @@ DPD_API int dpd_destroy(dpd_handle *h);
 /* sizes: total beads, beads of replica r, cells of replica r */
 DPD_API int dpd_sizes(const dpd_handle *h, int32_t replica, int64_t *n_total, int32_t *n_beads, int32_t *n_cells);
 
-/* Load replica r's state.  x, y in [0, L); vx, vy: velocity (see dpd_prime);
- * type in 0..7; gid: permanent bead ids 0..n-1 (NULL = 0..n-1); prev/next:
- * link slot indices within the replica, -1 = none (NULL = no links).  The
- * slot order is the caller's; dpd_prime or dpd_build_cells sorts it. */
+/* Load replica r's state.  x, y in [0, L) (finite values outside are wrapped
+ * in); vx, vy: velocity (see dpd_prime); type in 0..7; gid: permanent bead ids
+ * 0..n-1 (NULL = 0..n-1); prev/next: link slot indices within the replica,
+ * -1 = none (NULL = no links).  The slot order is the caller's; dpd_prime or
+ * dpd_build_cells sorts it.  A non-finite position, a type above 7, a gid >= n
+ * or a link out of range fails with DPD_E_ARG (checked on the device, so the
+ * arrays may be host or device memory). */
 DPD_API int dpd_set_state(dpd_handle *h, int32_t replica, const float *x, const float *y, const float *vx, const float *vy,
                   const uint8_t *type, const uint32_t *gid, const int32_t *prev, const int32_t *next);
 

@@ -245,3 +245,28 @@ def test_stats_async_equals_stats(cuda_ok):
     for k in ("T", "px", "py", "maxbond", "n_chains"):
         assert a[k] == b[k], k
     assert np.array_equal(a["counts"], b["counts"])
+
+
+def test_set_state_checks_its_input(cuda_ok):
+    """a type above 7, a link or gid out of range, a non-finite position: DPD_E_ARG,
+    nothing out of range stored; finite positions outside [0, L) are wrapped in"""
+    p = params(L=8, seed=3)
+    e = ob.Engine(p)
+    s = ob.make_soup(float(p.L), p.n_beads(), 3, nH=p.lip_nH, nT=p.lip_nT, f_lip=p.f_lip, c_N=p.c_N)
+    base = dict(x=s["x"], y=s["y"], vx=s["vx"], vy=s["vy"], type=s["type"], prev=s["prev"], next=s["next"])
+    for key, bad in (("type", 9), ("next", len(s["x"])), ("prev", -2), ("x", np.nan)):
+        kv = {k: v.copy() for k, v in base.items()}
+        kv[key][5] = bad
+        with pytest.raises(ob.DpdError, match="set_state"):
+            e.set_state(0, kv["x"], kv["y"], kv["vx"], kv["vy"], kv["type"], None, kv["prev"], kv["next"])
+    with pytest.raises(ob.DpdError, match="set_state"):
+        e.set_state(0, base["x"], base["y"], base["vx"], base["vy"], base["type"],
+                     np.full(len(s["x"]), len(s["x"]) + 3, np.uint32), base["prev"], base["next"])
+    kv = {k: v.copy() for k, v in base.items()}
+    kv["x"][0], kv["y"][1] = np.float32(p.L), np.float32(-0.5)
+    e.set_state(0, kv["x"], kv["y"], kv["vx"], kv["vy"], kv["type"], None, kv["prev"], kv["next"])
+    st = e.state()
+    assert np.all((st["x"] >= 0) & (st["x"] < p.L) & (st["y"] >= 0) & (st["y"] < p.L))
+    assert st["x"][0] == 0.0 and st["y"][1] == np.float32(p.L) - np.float32(0.5)
+    e.prime()
+    e.step(5)

@@ -588,11 +588,19 @@ extern "C" int dpd_set_state(dpd_handle *h, int32_t r, const float *x, const flo
     if (gid) CK(cudaMemcpyAsync(sg, gid, n * 4, cudaMemcpyDefault, h->s));
     if (prev) CK(cudaMemcpyAsync(sp, prev, n * 4, cudaMemcpyDefault, h->s));
     if (next) CK(cudaMemcpyAsync(sn, next, n * 4, cudaMemcpyDefault, h->s));
-    launch_pack(h->b, h->cur, R.b0, (int)n, sx, sy, svx, svy, st, gid ? sg : nullptr, prev ? sp : nullptr,
+    launch_pack(h->b, h->cur, R.b0, (int)n, R.L, sx, sy, svx, svy, st, gid ? sg : nullptr, prev ? sp : nullptr,
                 next ? sn : nullptr, h->s);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s));
     h->keys_valid = false;
+    unsigned flags = 0;
+    CK(cudaMemcpy(&flags, &h->b.status->flags, sizeof flags, cudaMemcpyDeviceToHost));
+    if (flags & DPD_F_INPUT) {
+        flags &= ~DPD_F_INPUT;
+        CK(cudaMemcpy(&h->b.status->flags, &flags, sizeof flags, cudaMemcpyHostToDevice));
+        return fail(DPD_E_ARG, "set_state: a non-finite position, a type >= %d, a gid >= n or a link outside "
+                               "[-1, n) (replica %d)", DPD_MAXT, r);
+    }
     return DPD_OK;
 }
 

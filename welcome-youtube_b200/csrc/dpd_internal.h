@@ -42,6 +42,8 @@
 #define DPD_F_CATALYST 0x80u    // a catalyst's neighbourhood exceeded the staging capacity
 #define DPD_CAT_MAXTR 64        // orientation trials of one lipid synthesis (syn_tries)
 #define DPD_F_ANALYSIS 0x200u   // a cluster union kept losing its compare-and-swap (analysis result invalid)
+#define DPD_F_INPUT 0x400u      // a state handed in had a non-finite position, a type >= DPD_MAXT, a gid >= n
+                                // or a link outside [-1, n): stored sanitised, the call fails
 
 struct RepDev {                 // constants of one replica, read by every kernel
     float L, halfL;
@@ -238,7 +240,7 @@ void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *
                         bool virial, unsigned long long *host_out, cudaStream_t s);
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
                       int tb, double rmax, int nbin, cudaStream_t s);
-void launch_pack(const Bufs &b, int cur, int b0, int n, const float *x, const float *y, const float *vx,
+void launch_pack(const Bufs &b, int cur, int b0, int n, float L, const float *x, const float *y, const float *vx,
                  const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
                  const int32_t *next, cudaStream_t s);
 void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, float *vhx, float *vhy, float *vtx,

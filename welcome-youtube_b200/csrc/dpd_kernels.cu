@@ -780,18 +780,53 @@ __global__ void __launch_bounds__(BEAD_TPB) k_pair_hist(Bufs b, int cur, const R
 
 // ---------------------------------------------------------------- state in/out
 
-__global__ void k_pack(Bufs b, int cur, int b0, int n, const float *x, const float *y, const float *vx, const float *vy,
-                       const uint8_t *type, const uint32_t *gid, const int32_t *prev, const int32_t *next) {
+// a bead handed in: a finite position is wrapped into [0, L) (values inside are
+// kept as they are; a float32 snapshot coordinate may round to exactly L);
+// a non-finite position, a type >= DPD_MAXT, a gid >= n or a link outside
+// [-1, n) is stored sanitised and flagged (DPD_F_INPUT), so nothing out of range
+// ever reaches the step's kernels
+__global__ void k_pack(Bufs b, int cur, int b0, int n, float L, const float *x, const float *y, const float *vx,
+                       const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
+                       const int32_t *next) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int d = b0 + k;
-    b.pos[cur][d] = make_float2(x[k], y[k]);
+    float px = x[k], py = y[k];
+    uint32_t t = type[k], g = gid ? gid[k] : (uint32_t)k;
+    int p = prev ? prev[k] : -1, q = next ? next[k] : -1;
+    bool bad = false;
+    if (!(isfinite(px) && isfinite(py))) {
+        px = py = 0.0f;
+        bad = true;
+    }
+    if (!(px >= 0.0f && px < L)) {
+        px = fmodf(px, L);
+        px = px < 0.0f ? px + L : px;
+        px = px >= L ? 0.0f : px;
+    }
+    if (!(py >= 0.0f && py < L)) {
+        py = fmodf(py, L);
+        py = py < 0.0f ? py + L : py;
+        py = py >= L ? 0.0f : py;
+    }
+    if (t >= (uint32_t)DPD_MAXT) {
+        t = 0;
+        bad = true;
+    }
+    if (g >= (uint32_t)n) {
+        g = (uint32_t)k;
+        bad = true;
+    }
+    if (p < -1 || p >= n || q < -1 || q >= n) {
+        p = q = -1;
+        bad = true;
+    }
+    if (bad) raise_flag(b.status, DPD_F_INPUT);
+    b.pos[cur][d] = make_float2(px, py);
     b.vh[cur][d] = make_float2(vx[k], vy[k]);
     b.vt[cur][d] = make_float2(vx[k], vy[k]);
     b.f[cur][d] = make_float2(0.0f, 0.0f);
-    const uint32_t g = gid ? gid[k] : (uint32_t)k;
-    b.tg[cur][d] = ((uint32_t)type[k] << TYPE_SHIFT) | (g & GID_MASK);
-    const int p = prev ? prev[k] : -1, q = next ? next[k] : -1;
+    b.tg[cur][d] = (t << TYPE_SHIFT) | (g & GID_MASK);
     b.link[cur][d] = make_int2(p >= 0 ? b0 + p : -1, q >= 0 ? b0 + q : -1);
 }
 
@@ -930,10 +965,10 @@ void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bc
     k_pair_hist<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, ta, tb, rmax, nbin);
 }
 
-void launch_pack(const Bufs &b, int cur, int b0, int n, const float *x, const float *y, const float *vx,
+void launch_pack(const Bufs &b, int cur, int b0, int n, float L, const float *x, const float *y, const float *vx,
                  const float *vy, const uint8_t *type, const uint32_t *gid, const int32_t *prev,
                  const int32_t *next, cudaStream_t s) {
-    k_pack<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, x, y, vx, vy, type, gid, prev, next);
+    k_pack<<<(n + 255) / 256, 256, 0, s>>>(b, cur, b0, n, L, x, y, vx, vy, type, gid, prev, next);
 }
 
 void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, float *vhx, float *vhy, float *vtx,
