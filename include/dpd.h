@@ -316,6 +316,14 @@ DPD_API int dpd_stats(dpd_handle *h, int32_t replica, double *out);
  * reference, whose stats row is written by the step loop itself. */
 DPD_API int dpd_stats_async(dpd_handle *h, int32_t replica, uint64_t *raw);
 DPD_API int dpd_stats_decode(const dpd_handle *h, int32_t replica, const uint64_t *raw, double *out);
+/* From now on every step (eager or inside a step graph) writes replica r's
+ * stats row into ring[(step % nslots) * 16 ...] itself, as dpd_stats_async's
+ * raw sums with word 6 set to the step number; ring: pinned host memory the
+ * device can write (cudaHostAlloc, cudaHostRegister), else DPD_E_ARG.  A row
+ * is complete once the stream has passed its step.  ring = NULL stops it.  A
+ * driver can then run multi-step graphs and still read every step's row.  The
+ * reference writes its stats row inside its own step loop (oercel.c:2262-2290). */
+DPD_API int dpd_stats_ring(dpd_handle *h, int32_t replica, uint64_t *ring, int32_t nslots);
 
 /* Clusters of the beads of one type of replica r (the reference's analysis
  * `snapcheck.py tclust`, cel/engine/tests/snapcheck.py:122-144): beads of the

@@ -270,3 +270,35 @@ def test_set_state_checks_its_input(cuda_ok):
     assert st["x"][0] == 0.0 and st["y"][1] == np.float32(p.L) - np.float32(0.5)
     e.prime()
     e.step(5)
+
+
+def test_stats_ring_rows_equal_stats_async(cuda_ok):
+    """rows the steps write into a pinned ring (4-step graphs) equal the rows of
+    dpd_stats_async after each eager step of the same run, word 6 the step; a
+    pageable ring is refused"""
+    import torch
+    p = params(L=16, seed=4)
+    a, b = ob.Engine(p), ob.Engine(p)
+    for e in (a, b):
+        e.load_soup(0)
+        e.prime()
+    ring = torch.zeros((8, 16), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    with pytest.raises(ob.DpdError, match="pinned"):
+        a.stats_ring(0, np.zeros((8, 16), np.uint64))
+    a.stats_ring(0, ring)
+    a.set_graph_steps(4)
+    b.set_graph_steps(1)
+    for _ in range(3):
+        a.step(4)
+        rows = {int(r[6]): r.copy() for r in ring}
+        for _ in range(4):
+            b.step(1)
+            raw = np.zeros(16, np.uint64)
+            b.stats_async(0, raw)
+            b.sync()
+            got = rows[b.step_no].copy()
+            got[6] = 0
+            assert np.array_equal(got, raw)
+    a.stats_ring(0, None)
+    a.step(4)
+    assert max(int(r[6]) for r in ring) == 12  # no row after the ring was stopped

@@ -63,6 +63,9 @@ struct dpd_handle {
     int64_t step = 0;
     // CUDA graphs of gsteps consecutive steps, one per starting buffer parity
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    // the stats ring: every step writes replica ring_rep's row into ring[step % ring_slots]
+    unsigned long long *ring = nullptr;
+    int32_t ring_rep = 0, ring_slots = 0;
     int gflip[2] = {0, 0};      // buffer parity change of one replay (steps + the extra sorts of catalyst checks)
     int gsteps = 0;
     // the reference's catalyst chemistry: replicas with chem_kind 1, the period of their checks
@@ -839,6 +842,9 @@ static void enqueue_step(dpd_handle *h, int64_t s) {
         enqueue_sort(h, PERM_SORT);
     }
     enqueue_forces(h, true);
+    if (h->ring)
+        launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->ring_rep, false, h->ring, h->ring_slots,
+                           h->s);
 }
 
 // capture gsteps steps starting from the current buffer parity and step s0
@@ -1080,7 +1086,7 @@ static int enqueue_observables(dpd_handle *h, int32_t r, bool virial, unsigned l
         pa.devicePointer == (void *)v)
         direct = v;
     cudaGetLastError();
-    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, direct, h->s);
+    launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, r, virial, direct, 0, h->s);
     CK(cudaGetLastError());
     if (!direct)
         CK(cudaMemcpyAsync(v, h->b.obs_out + (size_t)r * OBS_N, OBS_N * sizeof(unsigned long long),
@@ -1116,6 +1122,25 @@ extern "C" int dpd_stats_async(dpd_handle *h, int32_t r, uint64_t *raw) {
     TRY(ensure_replica(h, r));
     if (!raw) return fail(DPD_E_ARG, "null raw buffer");
     return enqueue_observables(h, r, false, (unsigned long long *)raw);
+}
+
+extern "C" int dpd_stats_ring(dpd_handle *h, int32_t r, uint64_t *ring, int32_t nslots) {
+    TRY(ensure_replica(h, r));
+    if (ring) {
+        if (nslots < 1) return fail(DPD_E_ARG, "the ring needs at least one slot");
+        cudaPointerAttributes pa;
+        const bool ok = cudaPointerGetAttributes(&pa, ring) == cudaSuccess && pa.type == cudaMemoryTypeHost &&
+                        pa.devicePointer == (void *)ring;
+        cudaGetLastError();
+        if (!ok) return fail(DPD_E_ARG, "the stats ring must be pinned host memory the device can write "
+                                        "(cudaHostAlloc, cudaHostRegister)");
+    }
+    CK(cudaStreamSynchronize(h->s));
+    h->ring = (unsigned long long *)ring;
+    h->ring_rep = ring ? r : 0;
+    h->ring_slots = ring ? nslots : 0;
+    drop_graphs(h);  // the step graphs are captured again with (or without) the row
+    return DPD_OK;
 }
 
 extern "C" int dpd_stats_decode(const dpd_handle *h, int32_t r, const uint64_t *raw, double *out) {

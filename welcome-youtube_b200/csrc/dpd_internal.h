@@ -237,7 +237,7 @@ void launch_aggregates(const Bufs &b, int cur, const RepDev *rep, const Chunk *b
 void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
                    int64_t C, cudaStream_t s);
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
-                        bool virial, unsigned long long *host_out, cudaStream_t s);
+                        bool virial, unsigned long long *host_out, int ring_slots, cudaStream_t s);
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,
                       int tb, double rmax, int nbin, cudaStream_t s);
 void launch_pack(const Bufs &b, int cur, int b0, int n, float L, const float *x, const float *y, const float *vx,

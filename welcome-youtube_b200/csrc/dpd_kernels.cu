@@ -617,7 +617,8 @@ __global__ void __launch_bounds__(BEAD_TPB) k_integrate(Bufs b, int cur, const R
 template <bool VIRIAL>
 __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const Chunk *__restrict__ ch, int rep_index,
-                                                          unsigned long long *__restrict__ host_out) {
+                                                          unsigned long long *__restrict__ host_out,
+                                                          int ring_slots) {
     __shared__ long long red[BEAD_TPB / 32][5 + DPD_MAXT];
     const RepDev &R = reps[rep_index];
     long long sx = 0, sy = 0, s2 = 0, vir = 0, heads = 0;
@@ -721,10 +722,14 @@ __global__ void __launch_bounds__(BEAD_TPB) k_observables(Bufs b, int cur, const
     __syncthreads();
     if (last) {
         __threadfence();
+        // a ring of rows in host memory: the slot of this step, its word 6 the step
+        unsigned long long *out = host_out;
+        const long long step = *b.step;
+        if (out && ring_slots > 0) out += (size_t)(step % ring_slots) * OBS_N;
         if (threadIdx.x < OBS_N) {
             const unsigned long long v = atomicExch(b.obs + (size_t)rep_index * OBS_N + threadIdx.x, 0ull);
             b.obs_out[(size_t)rep_index * OBS_N + threadIdx.x] = v;
-            if (host_out) host_out[threadIdx.x] = v;
+            if (out) out[threadIdx.x] = (ring_slots > 0 && threadIdx.x == 6) ? (unsigned long long)step : v;
         }
         if (threadIdx.x == 0) b.obs_done[rep_index] = 0u;
     }
@@ -954,10 +959,10 @@ void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bc
 }
 
 void launch_observables(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index,
-                        bool virial, unsigned long long *host_out, cudaStream_t s) {
+                        bool virial, unsigned long long *host_out, int ring_slots, cudaStream_t s) {
     const int grid = std::min(nbch, 148 * 8);  // grid-stride over the replica's chunks
-    if (virial) k_observables<true><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, host_out);
-    else k_observables<false><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, host_out);
+    if (virial) k_observables<true><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, host_out, ring_slots);
+    else k_observables<false><<<grid, BEAD_TPB, 0, s>>>(b, cur, rep, bch, rep_index, host_out, ring_slots);
 }
 
 void launch_pair_hist(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int ta,

@@ -100,7 +100,8 @@ EXPORTS = [
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
     "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters", "dpd_xoshiro_jump",
-    "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode", "dpd_cells_default", "dpd_cells_detect",
+    "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode", "dpd_stats_ring", "dpd_cells_default",
+    "dpd_cells_detect",
     "dpd_cells_info", "dpd_cells_fetch", "dpd_cells_free",
 ]
 NGRAD = 66
@@ -154,6 +155,7 @@ def load(path: str | None = None):
         "dpd_aggregates": ([vp, i32, dbl, i32, fp, fp], C.c_int),
         "dpd_stats_async": ([vp, i32, fp], C.c_int),
         "dpd_stats_decode": ([vp, i32, fp, fp], C.c_int),
+        "dpd_stats_ring": ([vp, i32, fp, i32], C.c_int),
         "dpd_set_rng": ([vp, i32, fp], C.c_int),
         "dpd_get_rng": ([vp, i32, fp], C.c_int),
         "dpd_build_cells": ([vp], C.c_int),

@@ -242,6 +242,19 @@ class Engine:
         return dict(T=o[0], px=o[1], py=o[2], virial=o[3], maxbond=o[4], n_chains=int(o[5]),
                     counts=o[8:16].astype(np.int64))
 
+    def stats_ring(self, replica, ring):
+        """every step writes the replica's stats row into ring[step % len(ring)]
+        (ring: pinned uint64 host memory, shape (slots, 16), e.g. a numpy view
+        of torch.empty(..., pin_memory=True); word 6 of a row holds its step);
+        None stops it"""
+        if ring is None:
+            check(self.lib.dpd_stats_ring(self.h, int(replica), None, 0))
+            self._ring = None
+            return
+        assert ring.dtype == np.uint64 and ring.ndim == 2 and ring.shape[1] == 16 and ring.flags.c_contiguous
+        check(self.lib.dpd_stats_ring(self.h, int(replica), ptr(ring), int(ring.shape[0])))
+        self._ring = ring  # kept alive while the device writes into it
+
     def type_clusters(self, replica=0, type=2, rcut=1.0):
         """clusters of the beads of `type` joined within rcut, and their neighbour
         fraction within 1.0 (the reference's `snapcheck.py tclust`)"""
