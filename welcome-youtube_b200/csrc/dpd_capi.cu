@@ -40,6 +40,28 @@ int lib_error(int code, const char *msg) {
                                            __FILE__, __LINE__);                                         \
     } while (0)
 
+// reverse-mode storage (defined here: the handle keeps it between windows)
+namespace {
+struct FullCk {  // a full configuration of the engine's current buffer
+    float2 *pos, *vh, *vt, *f;
+    uint32_t *tg;
+    int2 *link;
+    int32_t *cstart;
+};
+struct SegState {  // what a force VJP needs of one configuration
+    float2 *pos, *vt;
+    uint32_t *tg;
+    int2 *link;
+    int32_t *cstart;
+};
+struct AdjBufs {
+    std::vector<FullCk> ck;  // checkpoints + the end of the window (last)
+    std::vector<SegState> seg;
+    float2 *X, *V, *F, *g, *xb, *vb;
+    double *hist, *wgt, *grad;
+};
+}  // namespace
+
 struct dpd_handle {
     int nrep = 0;
     std::vector<dpd_params> params;
@@ -76,7 +98,8 @@ struct dpd_handle {
     // reverse-mode storage, grown on demand (full checkpoints, the states of one
     // recomputed segment, adjoint arrays in gid order)
     std::vector<void *> adj_allocs;
-    int adj_nck = 0, adj_nseg = 0;
+    int adj_nck = 0, adj_nseg = 0, adj_nbin = 0;  // capacity of adj (0: none yet)
+    AdjBufs adj;
     // staging for state in/out
     char *stage = nullptr;
     // cluster analysis scratch (allocated on first use): union-find parents, sizes, sums
@@ -307,7 +330,8 @@ static void drop_graphs(dpd_handle *h) {
 static void free_adj(dpd_handle *h) {
     for (void *p : h->adj_allocs) cudaFree(p);
     h->adj_allocs.clear();
-    h->adj_nck = h->adj_nseg = 0;
+    h->adj_nck = h->adj_nseg = h->adj_nbin = 0;
+    h->adj = AdjBufs();
 }
 
 static void free_all(dpd_handle *h) {
@@ -1257,26 +1281,6 @@ extern "C" int dpd_set_params(dpd_handle *h, int32_t r, const dpd_params *p) {
 
 // ---------------------------------------------------------------- reverse mode
 
-namespace {
-struct FullCk {  // a full configuration of the engine's current buffer
-    float2 *pos, *vh, *vt, *f;
-    uint32_t *tg;
-    int2 *link;
-    int32_t *cstart;
-};
-struct SegState {  // what a force VJP needs of one configuration
-    float2 *pos, *vt;
-    uint32_t *tg;
-    int2 *link;
-    int32_t *cstart;
-};
-struct AdjBufs {
-    std::vector<FullCk> ck;  // checkpoints + the end of the window (last)
-    std::vector<SegState> seg;
-    float2 *X, *V, *F, *g, *xb, *vb;
-    double *hist, *wgt, *grad;
-};
-}  // namespace
 
 template <typename T>
 static int adj_alloc(dpd_handle *h, T **p, size_t count) {
@@ -1289,9 +1293,22 @@ static int adj_alloc(dpd_handle *h, T **p, size_t count) {
 }
 
 static int adj_setup(dpd_handle *h, int nck, int nseg, int nbin, AdjBufs &A) {
-    // storage is rebuilt each call (cheap next to the window)
+    // storage kept on the handle and grown on demand: a window that fits reuses
+    // the buffers of the last one (freeing and allocating them every call costs a
+    // device synchronisation per buffer)
+    const int want_ck = nck, want_seg = nseg;
+    if (h->adj_nbin > 0 && nck <= h->adj_nck && nseg <= h->adj_nseg && nbin <= h->adj_nbin) {
+        A = h->adj;
+        A.ck.resize(want_ck);
+        A.seg.resize(want_seg);
+        return DPD_OK;
+    }
+    nck = std::max(nck, h->adj_nck);
+    nseg = std::max(nseg, h->adj_nseg);
+    nbin = std::max(nbin, h->adj_nbin);
     free_adj(h);
     const size_t N = (size_t)h->N, C = (size_t)h->C;
+    A = AdjBufs();
     A.ck.resize(nck);
     for (auto &c : A.ck) {
         TRY(adj_alloc(h, &c.pos, N));
@@ -1319,6 +1336,12 @@ static int adj_setup(dpd_handle *h, int nck, int nseg, int nbin, AdjBufs &A) {
     TRY(adj_alloc(h, &A.hist, (size_t)h->nrep * nbin));
     TRY(adj_alloc(h, &A.wgt, (size_t)h->nrep * nbin));
     TRY(adj_alloc(h, &A.grad, (size_t)h->nrep * DPD_NGRAD));
+    h->adj = A;
+    h->adj_nck = nck;
+    h->adj_nseg = nseg;
+    h->adj_nbin = nbin;
+    A.ck.resize(want_ck);
+    A.seg.resize(want_seg);
     return DPD_OK;
 }
 
