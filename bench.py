@@ -386,6 +386,7 @@ def cell_rates(reps=3):
         L, X, Y, T, B = cs.tile(sc.L, x, y, t, b, k)
         s = cells.Snapshot(0, 0.0, L, X, Y, T, B)
         r = cells.detect(s)
+        cells.detect(s)  # the memory pool settles over the first calls
         ts = []
         for _ in range(reps):
             t0 = time.perf_counter()

@@ -96,11 +96,21 @@ struct Ctx {
     void init() {
         CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         CU(cudaMallocHost((void **)&pin, 4 * sizeof(long long)));
+        // stream-ordered allocations from the device's default pool, which keeps
+        // freed memory for the next call instead of returning it (a free then
+        // needs no device synchronisation)
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            unsigned long long keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
         err = zeros<int>(1);
     }
     ~Ctx() {
+        for (void *p : mem) cudaFreeAsync(p, s);
         if (s) cudaStreamSynchronize(s);
-        for (void *p : mem) cudaFree(p);
         if (pin) cudaFreeHost(pin);
         if (s) cudaStreamDestroy(s);
     }
@@ -114,7 +124,7 @@ struct Ctx {
     }
     template <class T> T *alloc(size_t n) {
         void *p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+        if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), s) != cudaSuccess) {
             cudaGetLastError();
             throw Fail{DPD_E_NOMEM, "cell detection: device allocation of " + std::to_string(n * sizeof(T)) +
                                         " bytes failed"};
@@ -129,8 +139,7 @@ struct Ctx {
     void release(void *p) {
         auto it = std::find(mem.begin(), mem.end(), p);
         if (it == mem.end()) return;
-        CU(cudaStreamSynchronize(s));
-        cudaFree(p);
+        CU(cudaFreeAsync(p, s));
         mem.erase(it);
     }
     template <class T> T *fill(size_t n, int byte) {
