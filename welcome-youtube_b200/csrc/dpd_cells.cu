@@ -308,6 +308,19 @@ __device__ __forceinline__ void uf_union(int *par, int a, int b, int *err) {
     atomicOr(err, 1);
 }
 
+// after the unions: a run start points straight at its root (only this
+// thread writes entry i; the others' entries it reads only ever shorten), so a
+// pixel then reaches its root in two hops whatever the order of the links was
+__device__ __forceinline__ void uf_flatten(int *par, int i) {
+    int x = __ldcg(par + i);
+    for (int it = 0; it < MAXIT; it++) {
+        const int y = __ldcg(par + x);
+        if (y == x) break;
+        x = y;
+        par[i] = x;
+    }
+}
+
 // weighted union-find on the periodic grid: a word holds the parent (low 32
 // bits) and the node's image offset relative to it (two int16); a root's word
 // is (itself, 0, 0)
@@ -318,6 +331,22 @@ __device__ __forceinline__ unsigned long long wpack(int p, int ox, int oy) {
 __device__ __forceinline__ int wpar(unsigned long long w) { return (int)(unsigned)w; }
 __device__ __forceinline__ int wox(unsigned long long w) { return (short)(unsigned short)(w >> 32); }
 __device__ __forceinline__ int woy(unsigned long long w) { return (short)(unsigned short)(w >> 48); }
+
+// the weighted form of uf_flatten: entry i gets its root and its offset to it
+__device__ __forceinline__ void wflatten(unsigned long long *par, int i) {
+    unsigned long long w = __ldcg(par + i);
+    int x = (int)(unsigned)w, ox = (short)(unsigned short)(w >> 32), oy = (short)(unsigned short)(w >> 48);
+    for (int it = 0; it < MAXIT; it++) {
+        const unsigned long long v = __ldcg(par + x);
+        const int y = (int)(unsigned)v;
+        if (y == x) break;
+        ox += (short)(unsigned short)(v >> 32);
+        oy += (short)(unsigned short)(v >> 48);
+        x = y;
+        par[i] = (unsigned long long)(unsigned)x | ((unsigned long long)(unsigned short)(short)ox << 32) |
+                 ((unsigned long long)(unsigned short)(short)oy << 48);
+    }
+}
 
 __device__ __forceinline__ int wfind(unsigned long long *par, int i, int &ox, int &oy) {
     ox = 0;
@@ -798,6 +827,9 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             if (i + 1 < s0 && !memb[p + s1] && (j == 0 || memb[p - 1] || memb[p - 1 + s1]))
                 uf_union(lp, (int)p, (int)(p + s1), err);
         });
+        c.each(Pi, [=] __device__(long long p) {
+            if (rk[p] == (int)p && !memb[p]) uf_flatten(lp, (int)p);
+        });
         c.release(rk);
         int *sz = c.zeros<int>(P), *bord = c.zeros<int>(P);
         c.each(Pi, [=] __device__(long long p) {
@@ -898,6 +930,9 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             if (j + 1 == ngl && !memb[i * ngl]) wunion(wp, (int)p, (int)(i * ngl), 0, 1, err);
             const long long q = (i + 1 == ngl ? 0 : i + 1) * ngl + j;
             if (!memb[q] && (j == 0 || memb[p - 1] || memb[q - 1])) wunion(wp, (int)p, (int)q, i + 1 == ngl ? 1 : 0, 0, err);
+        });
+        c.each(Gi, [=] __device__(long long p) {
+            if (!memb[p] && (p % ngl == 0 || memb[p - 1])) wflatten(wp, (int)p);
         });
         int *wflag = c.zeros<int>(G), *cnt = c.zeros<int>(G);
         unsigned long long *si = c.zeros<unsigned long long>(G), *sj = c.zeros<unsigned long long>(G);
@@ -1103,6 +1138,9 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
             if (j + 1 == ngl && !memb[i * ngl]) uf_union(gp, (int)p, (int)(i * ngl), err);
             const long long q = (i + 1 == ngl ? 0 : i + 1) * ngl + j;
             if (!memb[q] && (j == 0 || memb[p - 1] || memb[q - 1])) uf_union(gp, (int)p, (int)q, err);
+        });
+        c.each(Gi, [=] __device__(long long p) {
+            if (!memb[p] && (p % ngl == 0 || memb[p - 1])) uf_flatten(gp, (int)p);
         });
         int *garea = c.zeros<int>(G);
         c.each(Gi, [=] __device__(long long p) {
