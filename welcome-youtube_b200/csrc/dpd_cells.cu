@@ -1296,31 +1296,48 @@ void detect(const dpd_cells_cfg &cfg, double L, long long n64, const double *hx,
         const double rmax = std::max(wall_max, cfg.leaflet_max);
         const int rb = ((int)std::ceil(rmax / h) + 1) / BK + 2;
         const bool all_blocks = 2 * rb + 1 >= nbk;
+        const int partial = ng % BK ? 1 : 0;
         double *bd = c.alloc<double>(n);
         int *bl = c.alloc<int>(n);
         c.each(n, [=] __device__(long long i) {
             if (mol[i] < 0 || !HASC[bagg[i]]) return;
             const int a = bagg[i];
             const long long bx = (gflat[i] / ngl) / BK, by = (gflat[i] % ngl) / BK;
-            const long long span = all_blocks ? nbk : 2 * rb + 1;
             double best = INFINITY;
             int bj = -1;
-            for (long long u = 0; u < span; u++)
-                for (long long v = 0; v < span; v++) {
-                    const long long cx = all_blocks ? u : pmod(bx - rb + u, nbk);
-                    const long long cy = all_blocks ? v : pmod(by - rb + v, nbk);
-                    const long long blk = cx * nbk + cy;
-                    for (int q = bo[blk]; q < bo[blk + 1]; q++) {
-                        const int3 t = bent[q];
-                        if (AGGC[t.x] != a) continue;
-                        const double px = ((double)t.y + 0.5) * h, py = ((double)t.z + 0.5) * h;
-                        const double d2 = sq2(kd_wrap(__dsub_rn(X[i], px), L), kd_wrap(__dsub_rn(Y[i], py), L));
-                        if (d2 < best || (d2 == best && t.x < bj)) {
-                            best = d2;
-                            bj = t.x;
-                        }
+            auto scan_block = [&](long long cx, long long cy) {
+                const long long blk = cx * nbk + cy;
+                for (int q = bo[blk]; q < bo[blk + 1]; q++) {
+                    const int3 t = bent[q];
+                    if (AGGC[t.x] != a) continue;
+                    const double px = ((double)t.y + 0.5) * h, py = ((double)t.z + 0.5) * h;
+                    const double d2 = sq2(kd_wrap(__dsub_rn(X[i], px), L), kd_wrap(__dsub_rn(Y[i], py), L));
+                    if (d2 < best || (d2 == best && t.x < bj)) {  // a tie: the lower lumen
+                        best = d2;
+                        bj = t.x;
                     }
                 }
+            };
+            if (all_blocks) {
+                for (long long u = 0; u < nbk; u++)
+                    for (long long v = 0; v < nbk; v++) scan_block(u, v);
+            } else {
+                // rings of blocks outward; every pixel of ring r lies more than (r - 1) BK
+                // pixels away (one block less where the grid ends in a partial block), so
+                // once that exceeds the nearest found, no nearer pixel and no tie remains
+                for (int r = 0; r <= rb; r++) {
+                    const int sure = r - 1 - partial;
+                    if (sure > 0) {
+                        const double dmin = (double)(sure * BK) * h;
+                        if (dmin * dmin > best) break;
+                    }
+                    for (int dx = -r; dx <= r; dx++)
+                        for (int dy = -r; dy <= r; dy++) {
+                            if (max(abs(dx), abs(dy)) != r) continue;
+                            scan_block(pmod(bx + dx, nbk), pmod(by + dy, nbk));
+                        }
+                }
+            }
             bd[i] = bj >= 0 ? sqrt(best) : INFINITY;
             bl[i] = bj;
         });
