@@ -50,6 +50,26 @@ def test_fused_step_equals_phases(cuda_ok, noise):
     assert np.array_equal(a.cells(), b.cells())
 
 
+def test_sort_falls_back_when_a_bead_jumps_cells(cuda_ok):
+    """a step in which one bead moves two cells gives the same stable sort (and
+    the same state) as dpd_integrate, dpd_build_cells and dpd_forces in turn"""
+    p, a = primed(noise="philox")
+    a.step(3)
+    b = clone(p, a)
+    s0 = a.step_no
+    for e in (a, b):
+        vhx = e.state()["vhx"].copy()
+        vhx[11] = 100.0  # dt 0.02: two cells in one step
+        e.set_dynamics(0, vhx=vhx)
+    a.step(1)
+    b.integrate()
+    b.build_cells()
+    b.forces(s0 + 1)
+    same_state(a.state(), b.state())
+    assert np.array_equal(a.cells(), b.cells())
+    a.step(2)
+
+
 def test_graph_replay_equals_eager(cuda_ok, monkeypatch):
     """a CUDA-graph replay of the step gives the same bits as eager launches"""
     p, a = primed(noise="philox")
