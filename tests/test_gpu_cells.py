@@ -93,18 +93,23 @@ def test_tiled_box_has_k2_times_the_cells(cuda_ok, k):
     assert big["label"].shape == (base["ng"] * k, base["ng"] * k)
 
 
-def test_engine_detect_cells_equals_its_snapshot_file(cuda_ok, tmp_path):
-    """Engine.detect_cells on a box of tied pi lipids after 3000 steps gives what
-    detect gives on the snapshot file the drop-in executable writes for it"""
-    p = ob.Params(L=48, dt=0.03, gamma=4.5, warmup=200, f_Ka=0.0, f_Kb=0.0, c_N=0.05, chem=0, seed=22,
-                  lip_arch="pi", lip_nT=2, lip_tie=1, f_lip=0.35, k_angle=15, a_W_T=200)
+LIPIDS = {"pi": dict(lip_arch="pi", lip_nT=2, lip_tie=1, f_lip=0.35, k_angle=15, a_W_T=200, seed=22),
+          "linear": dict(lip_arch="linear", lip_nH=1, lip_nT=3, f_lip=0.3, k_angle=10, a_W_T=100, seed=21)}
+
+
+@pytest.mark.parametrize("arch", list(LIPIDS))
+def test_engine_detect_cells_equals_its_snapshot_file(cuda_ok, tmp_path, arch):
+    """Engine.detect_cells on a box of lipids (tied pi: bonds from the template;
+    linear: from the chain links) after 3000 steps gives what detect gives on the
+    snapshot file the drop-in executable writes for it"""
+    p = ob.Params(L=48, dt=0.03, gamma=4.5, warmup=200, f_Ka=0.0, f_Kb=0.0, c_N=0.05, chem=0, **LIPIDS[arch])
     e = ob.Engine(p)
     e.load_soup(0)
     e.prime()
     e.step(3000)
     got = e.detect_cells()
     path = str(tmp_path / "snap.bin")
-    cli.write_snapshot(path, e.state(0), e.step_no, 0.0, float(p.L), p.template())
+    cli.write_snapshot(path, e.state(0), e.step_no, 0.0, float(p.L), p.template() if arch != "linear" else None)
     ref = cells.detect(cells.read_snapshot(path))
     assert got["summary"] == ref["summary"] and got["summary"]["n_membranes"] > 0
     assert got["aggregates"] == ref["aggregates"]
