@@ -1309,33 +1309,44 @@ static int adj_setup(dpd_handle *h, int nck, int nseg, int nbin, AdjBufs &A) {
     free_adj(h);
     const size_t N = (size_t)h->N, C = (size_t)h->C;
     A = AdjBufs();
+    // every buffer carved from one allocation (one cudaMalloc instead of a few hundred)
+    std::vector<std::pair<void **, size_t>> plan;
+    auto want = [&](auto **p, size_t count) { plan.push_back({(void **)p, count * sizeof(**p)}); };
     A.ck.resize(nck);
     for (auto &c : A.ck) {
-        TRY(adj_alloc(h, &c.pos, N));
-        TRY(adj_alloc(h, &c.vh, N));
-        TRY(adj_alloc(h, &c.vt, N));
-        TRY(adj_alloc(h, &c.f, N));
-        TRY(adj_alloc(h, &c.tg, N));
-        TRY(adj_alloc(h, &c.link, N));
-        TRY(adj_alloc(h, &c.cstart, C + 1));
+        want(&c.pos, N);
+        want(&c.vh, N);
+        want(&c.vt, N);
+        want(&c.f, N);
+        want(&c.tg, N);
+        want(&c.link, N);
+        want(&c.cstart, C + 1);
     }
     A.seg.resize(nseg);
     for (auto &c : A.seg) {
-        TRY(adj_alloc(h, &c.pos, N));
-        TRY(adj_alloc(h, &c.vt, N));
-        TRY(adj_alloc(h, &c.tg, N));
-        TRY(adj_alloc(h, &c.link, N));
-        TRY(adj_alloc(h, &c.cstart, C + 1));
+        want(&c.pos, N);
+        want(&c.vt, N);
+        want(&c.tg, N);
+        want(&c.link, N);
+        want(&c.cstart, C + 1);
     }
-    TRY(adj_alloc(h, &A.X, N));
-    TRY(adj_alloc(h, &A.V, N));
-    TRY(adj_alloc(h, &A.F, N));
-    TRY(adj_alloc(h, &A.g, N));
-    TRY(adj_alloc(h, &A.xb, N));
-    TRY(adj_alloc(h, &A.vb, N));
-    TRY(adj_alloc(h, &A.hist, (size_t)h->nrep * nbin));
-    TRY(adj_alloc(h, &A.wgt, (size_t)h->nrep * nbin));
-    TRY(adj_alloc(h, &A.grad, (size_t)h->nrep * DPD_NGRAD));
+    want(&A.X, N);
+    want(&A.V, N);
+    want(&A.F, N);
+    want(&A.g, N);
+    want(&A.xb, N);
+    want(&A.vb, N);
+    want(&A.hist, (size_t)h->nrep * nbin);
+    want(&A.wgt, (size_t)h->nrep * nbin);
+    want(&A.grad, (size_t)h->nrep * DPD_NGRAD);
+    size_t total = 0;
+    for (auto &q : plan) total += (q.second + 64 + 255) & ~(size_t)255;
+    char *base = nullptr;
+    TRY(adj_alloc(h, &base, total));
+    for (auto &q : plan) {
+        *q.first = base;
+        base += (q.second + 64 + 255) & ~(size_t)255;
+    }
     h->adj = A;
     h->adj_nck = nck;
     h->adj_nseg = nseg;
