@@ -237,6 +237,28 @@ def time_steps(torch, eng, K, flush):
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
 
+def noise_rate(torch, K=200):
+    """the headline box and step with the reference's mix13 pair hash in place of Philox4x32-10"""
+    from oercel_b200 import Engine, workloads
+    from oercel_b200.autotune import autotune
+    p = workloads.config2(seed=1, noise="mix13")
+    eng = Engine(p)
+    eng.load_soup(0)
+    eng.prime()
+    eng.step(3)
+    autotune(eng, use_cache=False)
+    eng.set_graph_steps(1)
+    eng.step(2)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ms = time_steps(torch, eng, K, flush)
+    nb = p.n_beads()
+    eng.close()
+    return {"noise": "mix13", "value": nb * K / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / K, "steps": K,
+            "note": "same box, chemistry and timing as the headline; the pair noise is the reference's own hash "
+                    "(cel/engine/oercel.c:131-141) instead of Philox4x32-10"}
+
+
 def reference_ensemble(steps=100):
     """the reference CPU engine on the 256-replica ensemble, sweep style: one
     single-threaded process per host core, each on a replica drawn evenly from
@@ -663,6 +685,7 @@ def ours(args, rank, local_rank, ws):
             res["adjoint"] = adjoint_ratio(torch)
             res["batched_adjoint"] = batched_adjoint(torch)
             res["catalyst"] = catalyst_rates(torch)
+            res["noise_mix13"] = noise_rate(torch)
         if ws == 1 and not args.skip_cpu:
             threads = os.cpu_count() or 1
             step_ms, t = run_reference(p, args.cpu_steps, threads)
