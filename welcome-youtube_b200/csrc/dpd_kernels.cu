@@ -293,9 +293,13 @@ __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__res
 // PERM_SORT moves everything unchanged.
 // ITEMS chunks per CTA, one bead of each per thread; the loads of all items
 // are issued phase by phase (slots, state, partner slots) so that each thread
-// has several independent gathers in flight.
+// has several independent gathers in flight.  The gathers wait on memory
+// (three dependent loads: slot, state, partner slots), so the kernel is held
+// to 32 registers for 8 CTAs (all 64 warps) per SM: 24.6 us a step on the
+// 1,048,576-bead box against 26.7 us at 6 CTAs; 2 or 4 ITEMS were slower
+// (29.7, 39.9 us).
 template <int MODE, int ITEMS>
-__global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
+__global__ void __launch_bounds__(BEAD_TPB, 8) k_permute(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                       const Chunk *__restrict__ ch, int nch,
                                                       const int32_t *__restrict__ gate) {
     pdl_begin();
@@ -391,13 +395,6 @@ __global__ void __launch_bounds__(BEAD_TPB) k_permute(Bufs b, int cur, const Rep
 
 // ---------------------------------------------------------------- pair + bond forces
 
-// Per bead d: F_d = sum_j w [a_ij - gamma w (rhat . vt_ij) + sigma theta_ij / sqrt(dt)] rhat
-// over the 3x3 neighbour cells (w = 1 - r, r < 1; oercel.c:970-981) plus the
-// harmonic bonds to prev/next (oercel.c:1272-1308).  Every pair is evaluated
-// by both of its beads with exactly negated operands and summed in fixed point,
-// so F_ij = -F_ji and sum F = 0 hold exactly and the result does not depend on
-// the order of the loops.  NEXTKEY: also the cell of x + dt vh + dt^2 F and
-// its count, i.e. the first half of the next step's sort.
 #define MAXHIT 32
 
 // Per bead d: F_d = sum_j w [a_ij - gamma w (rhat . vt_ij) + sigma theta_ij / sqrt(dt)] rhat
