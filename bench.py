@@ -34,7 +34,10 @@ sys.path.insert(0, os.path.join(ROOT, "welcome-youtube_b200"))
 
 METRIC = "DPD bead-steps/s at 1M beads & 256-replica batch; adjoint/forward time ratio"
 UNIT = "bead-steps/s"
-# algorithmic bytes per bead of each kernel of the step (FP32 SoA; derivation in DESIGN.md)
+# algorithmic bytes per bead of each kernel of the step: the FP32 SoA words each kernel must
+# read and write once per bead (permute: src 4, pos/vh/f/link 8 each, tg 4, partner dest ~2 in;
+# pos/vh/vt/link 8 each, tg 4 out; forces: the tile copy-in, links, partner positions and the
+# velocity in, the force and the next cell key out)
 KERNEL_BYTES = {"scan1": 3, "scan2": 2, "place": 13, "cellfix": 14, "permute": 88, "chem_grow": 0,
                 "chem_bond": 0, "forces": 54}
 KERNELS_PLAIN = ["scan1", "scan2", "place", "cellfix", "permute"]
