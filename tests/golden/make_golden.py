@@ -1,6 +1,6 @@
 """Generate the golden fixtures of this directory from the reference engine itself.
 
-    python tests/golden/make_golden.py
+    OERCEL_REF_ROOT=<reference checkout> python tests/golden/make_golden.py
 
 Runs the reference's own routines (cel/engine/oercel.c compiled by
 oracle/Makefile into oracle/_ref/libref_oercel.so with FMA contraction off) and
@@ -18,7 +18,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = "/root/reference"  # the reference checkout this generator reads (fixtures are made here only)
+REF_ROOT = os.environ.get("OERCEL_REF_ROOT", "")  # the reference checkout this generator reads
+if not REF_ROOT or not os.path.isdir(os.path.join(REF_ROOT, "cel", "engine")):
+    sys.exit("make_golden.py: set OERCEL_REF_ROOT to the reference checkout (the directory holding cel/engine)")
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import oracle as O  # noqa: E402
 
