@@ -96,6 +96,16 @@ double ora_theta(const ora_params *P, int64_t step, uint32_t gi, uint32_t gj) {
     return (double)(int32_t)u * (SQRT12 / 4294967296.0);
 }
 
+/* theta of every pair of n beads at one step (the test models' noise table):
+ * out[i n + j] = theta(gid[i], gid[j]), 0 on the diagonal */
+void ora_theta_matrix(const ora_params *P, int64_t step, int n, const uint32_t *gid, double *out) {
+    for (int i = 0; i < n; i++) {
+        out[(size_t)i * n + i] = 0.0;
+        for (int j = i + 1; j < n; j++)
+            out[(size_t)i * n + j] = out[(size_t)j * n + i] = ora_theta(P, step, gid[i], gid[j]);
+    }
+}
+
 /* keyed uniform decision word for the chemistry: Philox word 0 at counter
  * (gid, salt, step), key = seed.  Mechanism of oercel.c:819-826 (hash_key /
  * hash_u01: a pure function of seed, step, salt and gid). */

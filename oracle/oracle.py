@@ -82,6 +82,8 @@ def _load():
     lib.ora_step_seed.restype = C.c_uint64
     lib.ora_theta.argtypes = [P, C.c_int64, C.c_uint32, C.c_uint32]
     lib.ora_theta.restype = C.c_double
+    lib.ora_theta_matrix.argtypes = [P, C.c_int64, C.c_int, C.c_void_p, C.c_void_p]
+    lib.ora_theta_matrix.restype = None
     lib.ora_decision_word.argtypes = [C.c_uint64, C.c_int64, C.c_uint32, C.c_uint32]
     lib.ora_decision_word.restype = C.c_uint32
     lib.ora_cell_of.argtypes = [P, C.c_float, C.c_float]
@@ -148,6 +150,14 @@ def params(L, amat, *, dt=0.02, lam=0.65, gamma=4.5, kT=1.0, k_bond=100.0, r0=0.
         p.a[k] = v
     p.k_bond, p.r0, p.seed, p.noise = k_bond, r0, seed, noise
     return p
+
+
+def theta_matrix(p, step, gid):
+    """theta of every pair of the beads with these gids at one step (n x n, zero diagonal)"""
+    g = np.ascontiguousarray(gid, np.uint32)
+    out = np.empty((len(g), len(g)), np.float64)
+    lib().ora_theta_matrix(C.byref(p), int(step), len(g), g.ctypes.data, out.ctypes.data)
+    return out
 
 
 def f32consts(p):

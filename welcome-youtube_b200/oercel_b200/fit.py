@@ -1,11 +1,14 @@
 """Fitting interaction parameters to a structural target with the window adjoint.
 
-One iteration: every replica runs a differentiated window (dpd_window_adjoint:
-chemistry frozen, noise replayed, checkpoints every `ckpt` steps), the
-per-replica gradients of the smoothed pair-distribution loss are summed into
-one shared update (and over ranks with torch.distributed, one all-reduce of a
-few dozen floats), and Adam moves the chosen parameters.  The replicas then
-continue from the end of their window.
+One iteration: every replica runs a differentiated window through the
+torch.autograd Function of oercel_b200.autograd (dpd_window_adjoint: chemistry
+frozen, noise replayed, checkpoints every `ckpt` steps), the per-replica losses
+are summed, backward gives the gradient of the shared parameters (summed over
+ranks with torch.distributed when `distributed`: one all-reduce of a few
+floats, shard.reduce_gradients), and torch.optim.Adam moves them.  The
+replicas then continue from the end of their window.  The reference fits
+nothing (it has no reverse mode); its closest analogue is a sweep of
+independent runs (cel/pc/sweep.py:146-166).
 """
 from __future__ import annotations
 
@@ -38,67 +41,60 @@ def get_value(p, key):
     return float(p.a[i // MAXT][i % MAXT])
 
 
-def set_value(p, key, v):
-    if key in ("gamma", "k_bond"):
-        p.set(key, repr(float(v)))
-    else:
-        p.set(key, repr(float(v)))
+def shared_inputs(engine, keys, values):
+    """the window's inputs with `keys` set to `values` (a float64 tensor) in
+    every replica: per-replica repulsions (nrep, 8, 8) (the other entries kept
+    from each replica's own parameters), gamma and k_bond, or None where no
+    key touches them"""
+    import torch
+    nrep = engine.nrep
+    base = torch.tensor(np.array([np.array(p.a, dtype=np.float64) for p in engine.params]))
+    a = None
+    gamma = k_bond = None
+    for k, key in enumerate(keys):
+        if key == "gamma":
+            gamma = values[k]
+        elif key == "k_bond":
+            k_bond = values[k]
+        else:
+            idx = param_index(key)
+            m = torch.zeros(nrep, MAXT, MAXT, dtype=torch.float64)
+            m[:, idx // MAXT, idx % MAXT] = 1.0
+            a = (base if a is None else a) * (1.0 - m) + values[k] * m
+    return a, gamma, k_bond
 
 
-class Adam:
-    def __init__(self, n, lr, b1=0.9, b2=0.999, eps=1e-12):
-        self.m, self.v, self.t = np.zeros(n), np.zeros(n), 0
-        self.lr, self.b1, self.b2, self.eps = lr, b1, b2, eps
+def fit(engine, keys, target, *, iters=20, window=200, ckpt=20, spec=None, lr=1.0, distributed=False, log=None):
+    """torch.optim.Adam on `keys` (a_X_Y, gamma, k_bond; shared by every replica
+    of the engine) through the autograd Function; returns the history: per
+    iteration the summed loss (over replicas and ranks), the gradient and the
+    values the window ran with"""
+    import torch
 
-    def step(self, g):
-        self.t += 1
-        self.m = self.b1 * self.m + (1 - self.b1) * g
-        self.v = self.b2 * self.v + (1 - self.b2) * g * g
-        mh = self.m / (1 - self.b1 ** self.t)
-        vh = self.v / (1 - self.b2 ** self.t)
-        return -self.lr * mh / (np.sqrt(vh) + self.eps)
-
-
-def fit(engine, keys, target, *, iters=20, window=200, ckpt=20, spec=None, lr=1.0, reduce=None, log=None):
-    """Adam on `keys` (shared by every replica of the engine); returns the history"""
+    from . import autograd as AG
+    from .shard import reduce_gradients
     spec = spec or engine.rdf_spec()
-    opt = Adam(len(keys), lr)
-    idx = [param_index(k) for k in keys]
+    values = torch.tensor([get_value(engine.params[0], k) for k in keys], dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([values], lr=lr)
+    cfg = AG.WindowConfig(engine, window, spec, target, ckpt=ckpt)
     hist = []
     for it in range(iters):
-        loss, grad, _ = engine.window_adjoint(window, ckpt, spec, target)
-        g = grad[:, idx].sum(axis=0)
-        tot = float(loss.sum())
-        if reduce is not None:
-            g, tot = reduce(g, tot)
-        step = opt.step(g)
-        vals = []
-        for r, p in enumerate(engine.params):
-            for k, d in zip(keys, step):
-                set_value(p, k, get_value(p, k) + d)
-            engine.set_params(r, p)
-        vals = [get_value(engine.params[0], k) for k in keys]
-        hist.append(dict(iter=it, loss=tot, grad=g.tolist(), values=vals))
+        used = values.detach().tolist()
+        opt.zero_grad()
+        loss = AG.window_loss(cfg, *shared_inputs(engine, keys, values)).sum()
+        loss.backward()
+        tot = float(loss.detach())
+        if distributed:
+            buf = torch.cat([values.grad, torch.tensor([tot], dtype=torch.float64)])
+            reduce_gradients(buf)
+            values.grad.copy_(buf[:-1])
+            tot = float(buf[-1])
+        g = values.grad.tolist()
+        opt.step()
+        hist.append(dict(iter=it, loss=tot, grad=g, values=used))
         if log:
             log(hist[-1])
     return hist
-
-
-def torch_reduce():
-    """sum gradient and loss over ranks (NCCL or gloo): the one exchange of a batched fit"""
-    import torch
-    import torch.distributed as dist
-
-    def red(g, loss):
-        if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
-            return g, loss
-        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
-        t = torch.tensor(np.append(g, loss), dtype=torch.float64, device=dev)
-        dist.all_reduce(t)
-        out = t.cpu().numpy()
-        return out[:-1], float(out[-1])
-
-    return red
 
 
 NGRAD = _capi.NGRAD

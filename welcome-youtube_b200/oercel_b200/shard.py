@@ -28,8 +28,25 @@ def my_replicas(n_beads, rank, world_size):
 
 
 def reduce_gradients(grad, group=None):
-    """sum a gradient tensor over all ranks in place (NCCL for CUDA tensors, gloo for CPU)"""
+    """sum a tensor over all ranks in place: the one exchange of a batched fit
+    (the shared parameter gradient and the loss).  gloo reduces CPU tensors as
+    they are; under NCCL a CPU tensor travels through a CUDA copy."""
     import torch.distributed as dist
-    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return grad
+    if dist.get_backend(group) == "nccl" and not grad.is_cuda:
+        import torch
+        t = grad.to(torch.device("cuda", torch.cuda.current_device()))
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        grad.copy_(t.cpu())
+    else:
         dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
     return grad
+
+
+def replica_share(reps, rank, world_size):
+    """this rank's part of an ensemble given as (Params, n_beads) pairs: the
+    replicas shard_replicas assigns to it, in ensemble order, with their
+    indices in the whole ensemble"""
+    idx = my_replicas([n for _, n in reps], rank, world_size)
+    return idx, [reps[i] for i in idx]
