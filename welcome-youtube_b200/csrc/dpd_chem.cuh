@@ -187,9 +187,21 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 
 #define NONE_LIST_KEY 0xFFFFFFFFFFFFFFFFull
 
+// a bead that could be a growable end, judged from itself alone: a lone H,
+// or a T with a prev and no next (growable_end then walks its chain)
+__device__ __forceinline__ bool maybe_end(uint32_t tj, int2 lj) {
+    if (lj.y >= 0) return false;
+    const int t = type_of(tj);
+    return t == T_H ? lj.x < 0 : (t == T_T && lj.x >= 0);
+}
+
+#define GROW_KEEP 4  // candidate ends a lane keeps in registers (32 x 4 = 128 beads in the 3x3 cells)
+
 // stage 2 request of list entry k, by one whole warp: the listed P needs
 // >= n_t_min T beads within r_grow and claims its nearest growable end within
-// r_grow (req[k] = end or -1)
+// r_grow (req[k] = end or -1).  Each lane keeps the possible ends among its
+// candidates; the warp then takes them in increasing (distance, gid) order and
+// walks the chain of one at a time, so that usually a single walk decides.
 __device__ __forceinline__ void chem_grow_req_one(const Bufs &b, int cur, const RepDev *__restrict__ reps, int k,
                                                   int lane) {
     const uint32_t *tg = b.tg[cur];
@@ -202,8 +214,20 @@ __device__ __forceinline__ void chem_grow_req_one(const Bufs &b, int cur, const 
     const float L = R.L, h = R.halfL, r2 = R.r2_grow;
     const NbrRanges q = nbr_ranges(b, R, pi);
     int nt = 0;
-    unsigned long long best = NONE_LIST_KEY;
-    for (int f = lane; f < q.total; f += 32) {
+    unsigned long long key[GROW_KEEP];
+    int slot[GROW_KEEP];
+#pragma unroll
+    for (int m = 0; m < GROW_KEEP; m++) {
+        key[m] = NONE_LIST_KEY;
+        slot[m] = -1;
+    }
+    const bool kept = q.total <= 32 * GROW_KEEP;
+    unsigned long long best = NONE_LIST_KEY;  // the exhaustive path (a crowded neighbourhood)
+    int bj = -1;
+#pragma unroll
+    for (int m = 0; m < GROW_KEEP; m++) {
+        const int f = lane + 32 * m;
+        if (f >= q.total) break;
         const int j = nbr_slot(q, f);
         if (j == d) continue;
         const float2 pj = pos[j];
@@ -211,19 +235,70 @@ __device__ __forceinline__ void chem_grow_req_one(const Bufs &b, int cur, const 
         if (!(dd < r2)) continue;
         const uint32_t tj = tg[j];
         nt += type_of(tj) == T_T;
-        const unsigned long long key = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
-        if (key < best && growable_end(tg, link, j, R.max_chain)) best = key;
-    }
-    nt = (int)__reduce_add_sync(0xffffffffu, (unsigned)nt);
-    best = warp_min_u64(best);
-    int e = -1;
-    if (nt >= R.n_t_min && best != NONE_LIST_KEY) {
-        // the slot of the winning end: the lane that holds it reports it
-        for (int f = lane; f < q.total; f += 32) {
-            const int j = nbr_slot(q, f);
-            if (j != d && (tg[j] & GID_MASK) == (uint32_t)(best & 0xFFFFFFFFu)) e = j;
+        if (maybe_end(tj, link[j])) {
+            key[m] = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
+            slot[m] = j;
         }
-        e = (int)__reduce_max_sync(0xffffffffu, (unsigned)(e + 1)) - 1;
+    }
+    if (!kept)
+        for (int f = lane + 32 * GROW_KEEP; f < q.total; f += 32) {
+            const int j = nbr_slot(q, f);
+            if (j == d) continue;
+            const float2 pj = pos[j];
+            const float dd = dist2(pi.x, pi.y, pj.x, pj.y, L, h);
+            if (!(dd < r2)) continue;
+            const uint32_t tj = tg[j];
+            nt += type_of(tj) == T_T;
+            const unsigned long long kk = ((unsigned long long)__float_as_uint(dd) << 32) | (tj & GID_MASK);
+            if (kk < best && maybe_end(tj, link[j]) && growable_end(tg, link, j, R.max_chain)) {
+                best = kk;
+                bj = j;
+            }
+        }
+    nt = (int)__reduce_add_sync(0xffffffffu, (unsigned)nt);
+    const unsigned long long wb = warp_min_u64(best);  // the exhaustive path's nearest growable end
+    int e = -1;
+    if (nt >= R.n_t_min) {
+        // the kept candidates in increasing key order, one chain walk each, until one is growable
+        unsigned alive = 0;
+#pragma unroll
+        for (int m = 0; m < GROW_KEEP; m++) alive |= key[m] != NONE_LIST_KEY ? (1u << m) : 0u;
+        unsigned long long found = NONE_LIST_KEY;
+        int fslot = -1;
+        while (true) {
+            unsigned long long mine = NONE_LIST_KEY;
+            int mm = -1;
+#pragma unroll
+            for (int m = 0; m < GROW_KEEP; m++)
+                if ((alive >> m & 1u) && key[m] < mine) {
+                    mine = key[m];
+                    mm = m;
+                }
+            const unsigned long long w = warp_min_u64(mine);
+            if (w == NONE_LIST_KEY || w > wb) break;  // (the exhaustive path's end is nearer)
+            int ok = 0;
+            int sj = -1;
+            if (mine == w) {
+#pragma unroll
+                for (int m = 0; m < GROW_KEEP; m++)
+                    if (m == mm) sj = slot[m];
+                ok = growable_end(tg, link, sj, R.max_chain) ? 1 : 0;
+                if (!ok) alive &= ~(1u << mm);
+            }
+            const unsigned okm = __ballot_sync(0xffffffffu, ok != 0);
+            if (okm) {
+                found = w;
+                fslot = __shfl_sync(0xffffffffu, sj, __ffs(okm) - 1);
+                break;
+            }
+        }
+        // the exhaustive path's candidates compete too
+        if (wb < found) {
+            const unsigned hm = __ballot_sync(0xffffffffu, best == wb && wb != NONE_LIST_KEY);
+            found = wb;
+            fslot = __shfl_sync(0xffffffffu, bj, __ffs(hm) - 1);
+        }
+        e = found != NONE_LIST_KEY ? fslot : -1;
     }
     if (lane == 0) {
         b.req[k] = e;
