@@ -140,3 +140,86 @@ def test_snapshot_header_layout(tmp_path):
     assert b[:4] == b"OCEL" and struct.unpack_from("<iiiqdd", b, 4) == (1, 2, 1, 7, 0.14, 8.0)
     s = cli.read_snapshot(p)
     assert s["x"].tolist() == [0.25, 1.5] and s["type"].tolist() == [1, 2] and s["bonds"].tolist() == [[0, 1]]
+
+
+def _ref_ckpt_fields(b):
+    ver, n, ml, nh = struct.unpack_from("<iiii", b, 4)
+    o = 20 + (4 if ver == 3 else 0) + 32 + 32 + 48
+    head = b[:o]
+    out = {"head": head, "n": n}
+    for k, dt in (("gid", np.uint32), ("type", np.uint8), ("mpos", np.int8), ("nxt", np.int32)):
+        out[k] = np.frombuffer(b, dt, n, o)
+        o += n * np.dtype(dt).itemsize
+    for k in ("x", "y", "vx", "vy", "fx", "fy"):
+        out[k] = np.frombuffer(b, np.float64, n, o)
+        o += 8 * n
+    assert b[o:] == b"END!"
+    return out
+
+
+def test_reference_checkpoint_writer_round_trip(tmp_path):
+    """the reference's own checkpoint, read and written again: the same header,
+    the same gids, types, template positions and links in the same slot order
+    (the reference's cell order with nsub = 4), the state rounded to FP32.
+    From the beads in a shuffled slot order: the reference's cell order again
+    (within a cell the beads keep their given order; any order of a cell is a
+    sorted order) and the same beads"""
+    ref = fixture_bytes("ckpt_24")
+    path = tmp_path / "ref.bin"
+    path.write_bytes(ref)
+    ck = cli.read_ckpt(str(path))
+    a = _ref_ckpt_fields(ref)
+    for order in (np.arange(ck["N"]), np.random.default_rng(5).permutation(ck["N"])):
+        inv = np.empty_like(order)
+        inv[order] = np.arange(len(order))
+        st = {k: ck[k][order] for k in ("gid", "type", "x", "y", "vhx", "vhy", "fx", "fy")}
+        nx = ck["next"][order]
+        st["next"] = np.where(nx >= 0, inv[np.maximum(nx, 0)], -1).astype(np.int32)
+        pv = ck["prev"][order]
+        st["prev"] = np.where(pv >= 0, inv[np.maximum(pv, 0)], -1).astype(np.int32)
+        out = tmp_path / "out.bin"
+        cli.write_reference_ckpt(str(out), st, ck["step"], ck["time"], ck["L"], ck["seed"], ck["warm_end"],
+                                 ck["anchor"], ck["rng"], 0.0, ck["soup_seed"], ck["mlen"], ck["nH"], ck["arch"], 4)
+        b = _ref_ckpt_fields(out.read_bytes())
+        assert b["head"] == a["head"]
+        ncy = 10 * 4
+        key = np.minimum((b["x"] * 1.0).astype(int), 9) * ncy + np.minimum((b["y"] * 4.0).astype(int), ncy - 1)
+        assert np.all(np.diff(key) >= 0)
+        ga, gb = a["gid"].astype(np.int64), b["gid"].astype(np.int64)
+
+        def by_gid(f, g, k):
+            v = np.empty_like(f[k])
+            v[g] = f[k]
+            return v
+
+        for k in ("type", "mpos"):
+            assert np.array_equal(by_gid(b, gb, k), by_gid(a, ga, k)), k
+        nxa = np.where(a["nxt"] >= 0, ga[np.maximum(a["nxt"], 0)], -1)
+        nxb = np.where(b["nxt"] >= 0, gb[np.maximum(b["nxt"], 0)], -1)
+        assert np.array_equal(by_gid({"n": nxb}, gb, "n"), by_gid({"n": nxa}, ga, "n"))
+        for k in ("x", "y", "vx", "vy", "fx", "fy"):
+            assert np.array_equal(by_gid(b, gb, k), by_gid(a, ga, k).astype(np.float32).astype(np.float64)), k
+        if order[0] == 0 and np.all(order == np.arange(len(order))):
+            for k in ("gid", "type", "mpos", "nxt"):
+                assert np.array_equal(b[k], a[k]), k
+
+
+def test_reference_checkpoint_writer_refuses_grown_chains(tmp_path):
+    """a chain longer than the template (grown by the lipid chemistry) or a free
+    T has no form in the reference's checkpoint"""
+    path = tmp_path / "ref.bin"
+    path.write_bytes(fixture_bytes("ckpt_24"))
+    ck = cli.read_ckpt(str(path))
+    st = {k: ck[k].copy() for k in ("gid", "type", "x", "y", "vhx", "vhy", "fx", "fy", "prev", "next")}
+    w = int(np.nonzero(st["type"] == 0)[0][0])
+    tail = int(np.nonzero((st["type"] == 2) & (st["next"] < 0) & (st["prev"] >= 0))[0][0])
+    st["type"][w] = 2
+    st["next"][tail], st["prev"][w] = w, tail   # a W turned into a fourth chain bead
+    args = (ck["step"], ck["time"], ck["L"], ck["seed"], ck["warm_end"], ck["anchor"], ck["rng"], 0.0,
+            ck["soup_seed"], ck["mlen"], ck["nH"], ck["arch"], 4)
+    with pytest.raises(cli.EngineError, match="reference checkpoint"):
+        cli.write_reference_ckpt(str(tmp_path / "o.bin"), st, *args)
+    st2 = {k: ck[k].copy() for k in ("gid", "type", "x", "y", "vhx", "vhy", "fx", "fy", "prev", "next")}
+    st2["type"][w] = 2                                # a free T
+    with pytest.raises(cli.EngineError, match="reference checkpoint"):
+        cli.write_reference_ckpt(str(tmp_path / "o.bin"), st2, *args)

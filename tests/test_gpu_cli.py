@@ -192,3 +192,42 @@ def test_sigterm_stops_cleanly(cuda_ok, ini, tmp_path):
     log = (out / "log.txt").read_text()
     assert "(signal), checkpoint written" in log
     assert cli.read_ckpt(str(out / "ckpt.bin"))["step"] > 0
+
+
+REF_EXE = os.path.join(os.path.dirname(PKG), "oracle", "_ref", "oercel_portable")
+
+
+@pytest.mark.parametrize("name", [G, G_EXTRAS, G_CAT, G_PI])
+def test_reference_executable_continues_our_checkpoint(cuda_ok, tmp_path, name):
+    """ckpt_format = reference: this engine runs the first 24 steps and writes
+    the reference's own checkpoint (OCKP v2, v3 for pi lipids); the reference
+    executable (built from cel/engine/oercel.c, the build that made the
+    fixtures) continues it to step 36.  Its stats rows, events and final
+    snapshot must agree with the reference's continuation of its own run
+    within the criteria above."""
+    if not os.path.exists(REF_EXE):
+        pytest.skip("the reference executable is not built (oracle/Makefile with the reference sources)")
+    ini = write_ini(tmp_path, name)
+    out = tmp_path / "ours"
+    run_exe(ini, out, "noise=mix13", "ckpt_format=reference")
+    ck = out / "ckpt.bin"
+    assert ck.read_bytes()[:4] == b"OCKP"
+    assert cli.read_ckpt(str(ck))["step"] == 24
+    cont = tmp_path / "ref"
+    r = subprocess.run([REF_EXE, str(ini), str(cont), f"restart={ck}", "steps=36"], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, (r.stdout + r.stderr)[-2000:]
+    check_stats((cont / "stats.csv").read_text(), fixture_bytes("stats_b", name).decode())
+    if "events_b" in golden(name):
+        check_events((cont / "events.csv").read_text(), fixture_bytes("events_b", name).decode())
+    check_snapshot(str(cont / "snap_0000000036.bin"), "snap_36", name)
+
+
+def test_reference_checkpoint_refuses_grown_chains(cuda_ok, ini, tmp_path):
+    """the lipid chemistry grows and cuts chains, which the reference's
+    fixed-length templates cannot describe: a clear error, exit 1"""
+    out = tmp_path / "g"
+    r = subprocess.run([sys.executable, EXE, str(ini), str(out), *CHEM, "p_grow=0.5", "ckpt_format=reference"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 1
+    assert "oercel: error:" in r.stderr and "reference checkpoint" in r.stderr

@@ -12,6 +12,8 @@ so its Python driver can run this engine in its place (`longrun.py --engine
                       grow, brk, bond; variant "-")
   snap_<step>.bin     SPEC section 5 snapshot (cel/SPEC.md:116-130)
   ckpt.bin            this engine's checkpoint (format in write_ckpt below),
+                      or with ckpt_format = reference the reference's own
+                      (write_reference_ckpt), which its executable continues;
                       written atomically; ckpt_keep keeps ckpt_<step>.bin
   log.txt             progress lines, "timing: ..." and "done at step N"
 SIGTERM / SIGINT / walltime: finish the step, write the checkpoint, log
@@ -169,6 +171,105 @@ def write_ckpt(path, st, step, time_, L, seed, warm_end, anchor, keep_copy=None,
     os.replace(tmp, path)
 
 
+REF_CKPT_MAGIC = b"OCKP"
+
+
+def reference_mpos(st, mlen, nH):
+    """The reference's per-bead template position (mpos, oercel.c:800-806) from
+    this engine's prev/next links: every H and T bead must sit in a chain of
+    exactly mlen beads whose k-th bead is an H for k < nH and a T after, and no
+    other bead may be linked.  Anything else (chains grown or cut by the lipid
+    chemistry, free H or T beads) has no form in the reference's checkpoint:
+    EngineError."""
+    prev, nxt, ty = st["prev"], st["next"], st["type"]
+    n = len(ty)
+    mpos = np.full(n, -1, np.int8)
+    lipid = (ty == 1) | (ty == 2)
+    linked = (prev >= 0) | (nxt >= 0)
+    if np.any(linked & ~lipid):
+        raise EngineError("a bead other than H or T is bonded: not representable in the reference checkpoint")
+    for h in np.nonzero((prev < 0) & (nxt >= 0))[0]:
+        c, k = h, 0
+        while c >= 0:
+            if k >= mlen or ty[c] != (1 if k < nH else 2):
+                raise EngineError("a chain does not match the lipid template (grown or cut by the lipid chemistry): "
+                                  "not representable in the reference checkpoint")
+            mpos[c] = k
+            c = nxt[c]
+            k += 1
+        if k != mlen:
+            raise EngineError(f"a chain of {k} beads (the template has {mlen}): not representable in the reference "
+                              f"checkpoint")
+    if np.any(lipid & (mpos < 0)):
+        raise EngineError("a free H or T bead: not representable in the reference checkpoint")
+    return mpos
+
+
+def reference_order(x, y, L, nsub):
+    """the slot order the reference engine keeps: a stable sort by its cell
+    (floor(L) columns, floor(L) nsub rows, column-major, the index products in
+    FP64; cell_of_pos / sort_cells, oercel.c:739-745,779-786,832-933)"""
+    ncx = int(math.floor(L))
+    ncy = ncx * int(nsub)
+    cx = np.minimum((np.asarray(x, np.float64) * (ncx / L)).astype(np.int64), ncx - 1)
+    cy = np.minimum((np.asarray(y, np.float64) * (ncy / L)).astype(np.int64), ncy - 1)
+    return np.argsort(np.maximum(cx, 0) * ncy + np.maximum(cy, 0), kind="stable")
+
+
+def write_reference_ckpt(path, st, step, time_, L, seed, warm_end, anchor, rng, maxbond, soup_seed, mlen, nH, arch,
+                         nsub, keep_copy=None):
+    """The reference engine's checkpoint (write_ckpt, oercel.c:1891-1936),
+    version 2 for linear lipids and 3 (with the shape code) otherwise, so that
+    its executable can continue this run: little endian "OCKP", int32 version,
+    N, mlen, nH, [arch], int64 step, float64 time, L, uint64 seed, rng[4],
+    float64 maxbond, int64 warm_end, float64 t_anchor, int64 step_anchor,
+    float64 dt_anchor, uint64 soup_seed, then in slot order uint32 gid, uint8
+    type, int8 mpos, int32 nxt, float64 x, y, vx, vy, fx, fy (the FP32 state
+    widened; vx/vy the stored half-step velocity), "END!".  The beads are
+    written in the reference's own slot order (reference_order, with the
+    nsub of the run): its restart sorts the state once more but leaves the
+    forces where they are (sort_cells permutes every array except fx, fy), so
+    the file must already be in the order that sort keeps.  Written to a
+    temporary file, synced and renamed."""
+    n = len(st["x"])
+    if np.any(st["type"] >= 6):
+        raise EngineError("bead type Z or above: not representable in the reference checkpoint")
+    mpos = reference_mpos(st, mlen, nH)
+    perm = reference_order(st["x"], st["y"], float(L), nsub)
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    nx = np.asarray(st["next"], np.int64)[perm]
+    nxt = np.where(nx >= 0, inv[np.maximum(nx, 0)], -1).astype(np.int32)
+    st = {k: np.asarray(st[k])[perm] for k in ("gid", "type", "x", "y", "vhx", "vhy", "fx", "fy")}
+    mpos = mpos[perm]
+    ver = 2 if arch == 0 else 3
+    tmp = path + ".tmp"
+    with open(tmp, "wb") as f:
+        f.write(REF_CKPT_MAGIC)
+        f.write(struct.pack("<iiii", ver, n, int(mlen), int(nH)))
+        if ver == 3:
+            f.write(struct.pack("<i", int(arch)))
+        f.write(struct.pack("<qddQ", int(step), float(time_), float(L), int(seed) & (2**64 - 1)))
+        f.write(np.ascontiguousarray(rng, np.uint64).tobytes())
+        f.write(struct.pack("<dqdqdQ", float(maxbond), int(warm_end), float(anchor[0]), int(anchor[1]),
+                            float(anchor[2]), int(soup_seed) & (2**64 - 1)))
+        f.write(np.ascontiguousarray(st["gid"], np.uint32).tobytes())
+        f.write(np.ascontiguousarray(st["type"], np.uint8).tobytes())
+        f.write(mpos.tobytes())
+        f.write(nxt.tobytes())
+        for k in ("x", "y", "vhx", "vhy", "fx", "fy"):
+            f.write(np.ascontiguousarray(st[k], np.float64).tobytes())
+        f.write(b"END!")
+        f.flush()
+        os.fsync(f.fileno())
+    if keep_copy:
+        try:
+            os.link(tmp, keep_copy)
+        except OSError:
+            pass
+    os.replace(tmp, path)
+
+
 def read_ckpt(path):
     with open(path, "rb") as f:
         b = f.read()
@@ -209,7 +310,7 @@ def read_reference_ckpt(path, b):
     step, time_, L, seed = struct.unpack_from("<qddQ", b, o0)
     rng = np.frombuffer(b, np.uint64, 4, o0 + 32).copy()
     o = o0 + 32 + 32 + 8          # rng state, maxbond
-    warm_end, ta, sa, da = struct.unpack_from("<qdqd", b, o)
+    warm_end, ta, sa, da, soup_seed = struct.unpack_from("<qdqdQ", b, o)
     o += 32 + 8                   # warm_end, anchors, soup seed
     gid = np.frombuffer(b, np.uint32, n, o).copy()
     o += 4 * n
@@ -218,7 +319,7 @@ def read_reference_ckpt(path, b):
     nxt = np.frombuffer(b, np.int32, n, o).copy()
     o += 4 * n
     out = dict(N=n, step=step, time=time_, L=L, seed=seed, warm_end=warm_end, anchor=(ta, sa, da), gid=gid,
-               type=typ, next=nxt, rng=rng, arch=arch, mlen=ml, nH=nh)
+               type=typ, next=nxt, rng=rng, arch=arch, mlen=ml, nH=nh, soup_seed=soup_seed)
     for k, ref in (("x", "x"), ("y", "y"), ("vhx", "vx"), ("vhy", "vy"), ("fx", "fx"), ("fy", "fy")):
         out[k] = np.frombuffer(b, np.float64, n, o).astype(np.float32)
         o += 8 * n
@@ -318,6 +419,7 @@ def _run(p, outdir, over):
             elif seed != p.seed:
                 log(f"note: using checkpoint seed {seed} (ini seed {p.seed} ignored; set restart_reseed=1 to branch)")
             warm_end = ck["warm_end"]
+            soup_seed = ck.get("soup_seed", ck["seed"])
             ta, sa, da = ck["anchor"]
             anchor = (ta, sa, da) if da == p.dt else (ck["time"], ck["step"], p.dt)  # dt changed: new anchor
             e = Engine(p, n_beads=ck["N"])
@@ -337,6 +439,7 @@ def _run(p, outdir, over):
             e.set_rng(0, s["rng"])
             e.prime()
             warm_end, seed, anchor = p.warmup, p.seed, (0.0, 0, p.dt)
+            soup_seed = p.seed
             log(f"init soup: N={len(s['x'])} lipid beads={s['n_lipid_beads']}")
     except DpdError as err:
         raise EngineError(str(err)) from None
@@ -390,7 +493,14 @@ def _run(p, outdir, over):
     def ckpt(step):
         st = e.state(0)
         keep = os.path.join(outdir, f"ckpt_{step:010d}.bin") if p.ckpt_keep else None
-        write_ckpt(os.path.join(outdir, "ckpt.bin"), st, step, tnow(step), L, seed, warm_end, anchor, keep, e.rng(0))
+        path = os.path.join(outdir, "ckpt.bin")
+        if p.ckpt_format == "reference":
+            obs()  # the device's running max bond, folded into the row's maximum
+            t = p.template()
+            write_reference_ckpt(path, st, step, tnow(step), L, seed, warm_end, anchor, e.rng(0), mb["acc"],
+                                 soup_seed, t.mlen, t.nH, ARCHS.index(p.lip_arch), p.nsub, keep)
+        else:
+            write_ckpt(path, st, step, tnow(step), L, seed, warm_end, anchor, keep, e.rng(0))
 
     # max_bond of a stats row is the largest bond length since the previous row
     # (oercel.c:2365-2369); every device read restarts the device maximum

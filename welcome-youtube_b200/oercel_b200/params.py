@@ -90,6 +90,8 @@ PDEFS = [
     ("r_bond", "float", "0.6", "NEW bonding radius"),
     ("n_t_min", "int", "2", "NEW T beads a P needs within r_grow"),
     ("max_chain", "int", "12", "NEW longest chain growth may produce"),
+    ("ckpt_format", "str", "own", "NEW checkpoint format: own (exact FP32 continuation here) or reference (the "
+                                  "reference engine's OCKP v2/v3, which its executable can continue)"),
 ]
 PKEYS = {k: (t, d, h) for k, t, d, h in PDEFS}
 ARCHS = ("linear", "pi", "y", "bola")
@@ -230,6 +232,8 @@ class Params:
             raise ParamError("noise must be philox or mix13")
         if self.init not in ("soup", "restart"):
             raise ParamError("init must be soup or restart")
+        if self.ckpt_format not in ("own", "reference"):
+            raise ParamError("ckpt_format must be own or reference")
         if self.chem_kind not in ("catalyst", "lipid"):
             raise ParamError("chem_kind must be catalyst or lipid")
         if self.feed not in ("none", "0", "uniform", "vent"):
