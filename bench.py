@@ -188,7 +188,7 @@ def reference_arm(args, rank, ws):
     from oercel_b200 import workloads
     p = workloads.config2()
     threads = os.cpu_count() or 1
-    step_ms, t = run_reference(p, min(args.steps, 300), threads)
+    step_ms, t = run_reference(p, args.cpu_steps, threads)
     base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
@@ -200,10 +200,13 @@ def reference_arm(args, rank, ws):
         print(json.dumps(base))
         return
     v = p.n_beads() * 1000.0 / step_ms * 1.0  # one box, the reference runs on the host
-    base.update({"value": v, "ms_per_step": step_ms,
+    v_io = p.n_beads() * 1000.0 / (step_ms + t["io"])
+    base.update({"value": v, "ms_per_step": step_ms, "value_with_io": v_io, "ms_per_step_with_io": step_ms + t["io"],
                  "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                                  "sample": f"{int(t['steps'])} steps of the 1,048,576-bead box, "
-                                            f"ms/step of integrate+sort+pair+bonded ({t['isa']} build)"},
+                                  "sample": f"{int(t['steps'])} steps of the 1,048,576-bead box (the same count as "
+                                            f"the cpu_baseline leg of our arm), ms/step of "
+                                            f"integrate+sort+pair+bonded+chem ({t['isa']} build); value_with_io "
+                                            f"adds the io phase"},
                  "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                  "reference_timing_ms": t})
     print(json.dumps(base))
@@ -303,9 +306,13 @@ def reference_ensemble(steps=100):
                       f"process each, run together; chemistry off (the lipid rules do not exist in the reference)"}
 
 
-def batched_rates(torch, steps=64):
-    """256-replica ensemble in one engine vs the same replicas one engine at a
-    time; both run graphs of `steps` steps (captured before timing)"""
+def batched_rates(torch, steps=2000, graph=50):
+    """the 256-replica ensemble (configuration 3, its 2000 steps) in one engine
+    against the same replicas one engine at a time; both run graphs of `graph`
+    steps (captured before timing) and both are timed with CUDA events: the
+    one-at-a-time leg chains the engines' streams with events, so that each
+    engine starts when the previous one has finished, and its time runs from
+    the first engine's start event to the last engine's end event"""
     from oercel_b200 import Engine, workloads
     reps = workloads.config3()
     plist = [p for p, _ in reps]
@@ -315,8 +322,8 @@ def batched_rates(torch, steps=64):
     for r in range(len(plist)):
         e.load_soup(r)
     e.prime()
-    e.set_graph_steps(steps)
-    e.step(steps)
+    e.set_graph_steps(graph)
+    e.step(graph)
     stream = torch.cuda.ExternalStream(e.stream())
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -333,20 +340,99 @@ def batched_rates(torch, steps=64):
         s = Engine(p, n)
         s.load_soup(0)
         s.prime()
-        s.set_graph_steps(steps)
-        s.step(steps)
+        s.set_graph_steps(graph)
+        s.step(graph)
         singles.append(s)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for s in singles:  # strictly one replica after the other
+    streams = [torch.cuda.ExternalStream(s.stream()) for s in singles]
+    first, done = torch.cuda.Event(enable_timing=True), None
+    first.record(streams[0])
+    for s, st in zip(singles, streams):  # strictly one replica after the other
+        if done is not None:
+            st.wait_event(done)
         s.step_async(steps)
+        done = torch.cuda.Event(enable_timing=True)
+        done.record(st)
+    done.synchronize()
+    for s in singles:
         s.sync()
-    t_single = (time.perf_counter() - t0) * 1000.0
+    t_single = first.elapsed_time(done)
     for s in singles:
         s.close()
     return {"value": total * steps / (t_batched / 1000.0), "one_at_a_time": total * steps / (t_single / 1000.0),
             "ratio": t_single / t_batched, "replicas": len(reps), "beads": total, "steps": steps,
-            "timing": "batched: CUDA events on the engine stream; one at a time: host clock around all engines"}
+            "graph_steps": graph,
+            "timing": "both legs: CUDA events on the engines' streams; one at a time: the engines' streams chained "
+                      "by events, first start to last end"}
+
+
+def sharded_ensemble(torch, rank, ws, steps=2000, graph=50):
+    """configuration 3 split across the ranks (shard.replica_share: balanced
+    by bead count, no exchange inside the step): each rank runs its replicas
+    in one engine; CUDA events on the rank's engine stream, the slowest rank's
+    time; value = all replicas' bead-steps over that time"""
+    import torch.distributed as dist
+
+    from oercel_b200 import Engine, workloads
+    from oercel_b200.shard import replica_share
+    reps = workloads.config3()
+    idx, mine = replica_share(reps, rank, ws)
+    e = Engine([p for p, _ in mine], [n for _, n in mine])
+    for r in range(len(mine)):
+        e.load_soup(r)
+    e.prime()
+    e.set_graph_steps(graph)
+    e.step(graph)
+    stream = torch.cuda.ExternalStream(e.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    a.record(stream)
+    e.step_async(steps)
+    b.record(stream)
+    stream.synchronize()
+    e.sync()
+    t = torch.tensor([a.elapsed_time(b)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e.close()
+    total = sum(n for _, n in reps)
+    return {"value": total * steps / (float(t.item()) / 1000.0), "unit": UNIT, "replicas": len(reps),
+            "beads": total, "steps": steps, "ranks": ws, "replicas_this_rank": len(mine),
+            "scaling": "strong", "timing": "CUDA events on each rank's engine stream, max over ranks"}
+
+
+def sharded_fit(torch, rank, ws, iters=2, window=500, ckpt=25, last=50):
+    """configuration 5 split across the ranks: each rank holds its share of
+    the 64 boxes and the fit's shared a_W_T gradient is summed over ranks (one
+    all-reduce per optimizer iteration, fit.fit(distributed=True)); host clock
+    per iteration after one untimed iteration, max over ranks"""
+    import numpy as np
+    import torch.distributed as dist
+
+    from oercel_b200 import Engine, fit, workloads
+    from oercel_b200.shard import replica_share
+    ps = workloads.config5()
+    idx, mine = replica_share([(p, p.n_beads()) for p in ps], rank, ws)
+    e = Engine([p for p, _ in mine])
+    for r in range(len(mine)):
+        e.load_soup(r)
+    e.prime()
+    e.step(50)
+    spec = Engine.rdf_spec(nbin=64, rmax=2.0, sigma=0.05, last_steps=last, horizon=20)
+    target = np.ones(64)
+    fit.fit(e, ["a_W_T"], target, iters=1, window=window, ckpt=ckpt, spec=spec, distributed=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    hist = fit.fit(e, ["a_W_T"], target, iters=iters, window=window, ckpt=ckpt, spec=spec, distributed=True)
+    torch.cuda.synchronize()
+    t = torch.tensor([(time.perf_counter() - t0) / iters], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e.close()
+    return {"s_per_iteration": float(t.item()), "replicas": len(ps), "ranks": ws, "window": window,
+            "ckpt_every": ckpt, "finite": bool(all(np.isfinite(h["loss"]) for h in hist)),
+            "timing": "host clock around fit iterations (device synchronised), max over ranks; each iteration "
+                      "one window adjoint per rank plus one all-reduce of the shared gradient"}
 
 
 def analysis_rates(eng, p, reps=5):
@@ -497,6 +583,68 @@ def adjoint_ratio(torch, window=200, ckpt=20, last=50, reps=3):
     f, a = float(np.median(tf)), float(np.median(ta))
     return {"ratio": a / f, "forward_s": f, "adjoint_s": a, "window": window, "ckpt_every": ckpt, "beads": p.n_beads(),
             "timing": "host clock around each call, device synchronised; forward = the same window with its loss"}
+
+
+def adjoint_accuracy(torch, windows=(10, 20, 50, 100, 200), ckpt=20, last=50):
+    """the window gradient of configuration 4 (16,384 beads) against central
+    finite differences of the same window, for a_W_T: every window starts from
+    the same state (the autograd front end given it explicitly), the
+    differences are Richardson-extrapolated from steps 0.5 and 0.25
+    ((4 D(h/2) - D(h)) / 3); plus the error that a horizon of 20 steps
+    introduces into the 200-step gradient"""
+    import numpy as np
+
+    from oercel_b200 import Engine, autograd as AG, workloads
+    p = workloads.config4()
+    e = Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(200)
+    step0 = e.step_no
+    s = e.state()
+    g = s["gid"].astype(np.int64)
+
+    def col(a, b):
+        out = np.empty((len(g), 2), np.float64)
+        out[g, 0], out[g, 1] = s[a], s[b]
+        return torch.tensor(out)
+
+    x0, vh0, vt0 = col("x", "y"), col("vhx", "vhy"), col("vtx", "vty")
+    a0 = torch.tensor(np.array(p.a, dtype=np.float64))
+    rows = []
+    for W in windows:
+        spec = Engine.rdf_spec(nbin=64, rmax=2.0, sigma=0.05, last_steps=min(last, W))
+        target = np.ones(64)
+        cfg = AG.WindowConfig(e, W, spec, target, ckpt=min(ckpt, W), step0=step0)
+        a = a0.clone().requires_grad_(True)
+        loss = AG.window_loss(cfg, a, None, None, x0, vh0, vt0).sum()
+        grad = float(torch.autograd.grad(loss, [a])[0][0, 2])
+
+        def at(v):
+            b = a0.clone()
+            b[0, 2] = v
+            with torch.no_grad():
+                return float(AG.window_loss(cfg, b, None, None, x0, vh0, vt0).sum())
+
+        base = float(a0[0, 2])
+        d1 = (at(base + 0.5) - at(base - 0.5)) / 1.0
+        d2 = (at(base + 0.25) - at(base - 0.25)) / 0.5
+        fd = (4.0 * d2 - d1) / 3.0
+        rows.append({"window": W, "adjoint": grad, "fd": fd, "rel_err": abs(grad - fd) / max(abs(fd), 1e-300)})
+    ok = [r["window"] for r in rows if r["rel_err"] < 1e-3]
+    # the horizon's error on the 200-step gradient
+    W = windows[-1]
+    spec_full = Engine.rdf_spec(nbin=64, rmax=2.0, sigma=0.05, last_steps=last)
+    spec_h = Engine.rdf_spec(nbin=64, rmax=2.0, sigma=0.05, last_steps=last, horizon=20)
+    gfull = rows[-1]["adjoint"]
+    cfg = AG.WindowConfig(e, W, spec_h, np.ones(64), ckpt=ckpt, step0=step0)
+    a = a0.clone().requires_grad_(True)
+    gh = float(torch.autograd.grad(AG.window_loss(cfg, a, None, None, x0, vh0, vt0).sum(), [a])[0][0, 2])
+    e.close()
+    return {"rows": rows, "longest_window_within_1e-3": max(ok) if ok else None,
+            "horizon20_rel_diff_at_200": abs(gh - gfull) / max(abs(gfull), 1e-300),
+            "note": "gradient of the smoothed T-T g(r) loss with respect to a_W_T; finite differences of the same "
+                    "FP32 window (Richardson, h = 0.5, 0.25)"}
 
 
 def batched_adjoint(torch, window=500, ckpt=25, last=50):
@@ -677,7 +825,12 @@ def ours(args, rank, local_rank, ws):
             print(json.dumps(res))
         return
     e2e = e2e_rate(Engine, p, args.e2e_steps, ws)  # every rank, its own box
+    sharded = None
+    if ws > 1 and not args.skip_batched:  # every rank takes part in both
+        sharded = {"ensemble": sharded_ensemble(torch, rank, ws), "fit": sharded_fit(torch, rank, ws)}
     if rank == 0:
+        if sharded is not None:
+            res["sharded"] = sharded
         if ana is not None:
             res["analysis"] = ana
         res["e2e"] = e2e
@@ -686,6 +839,7 @@ def ours(args, rank, local_rank, ws):
             if not args.skip_cpu:
                 res["batched"]["cpu_reference"] = reference_ensemble()
             res["adjoint"] = adjoint_ratio(torch)
+            res["adjoint"]["accuracy"] = adjoint_accuracy(torch)
             res["batched_adjoint"] = batched_adjoint(torch)
             res["catalyst"] = catalyst_rates(torch)
             res["noise_mix13"] = noise_rate(torch)

@@ -169,12 +169,17 @@ typedef struct dpd_handle dpd_handle;
 /* Launch choices of a handle (the autotuner's knobs).  force_kernel 0: cell
  * tiles of tile_w x tile_h cells staged in shared memory, each pair evaluated
  * once (default); 1: one thread per bead over its 3x3 cells, each pair
- * evaluated by both beads.  Both give bit-identical forces.  graph_steps:
- * steps per captured CUDA graph. */
+ * evaluated by both beads; 2: the cell tiles of 0 staged into shared memory
+ * by bulk asynchronous copies, one per tile column (tile_w <= 30).  All give
+ * bit-identical forces.
+ * graph_steps: steps per captured CUDA graph.  sort_mode: the exclusive scan
+ * of the cell counts in two passes (0) or in one pass with decoupled
+ * look-back between blocks (1); the same cell starts. */
 typedef struct {
     int32_t force_kernel;
     int32_t tile_w, tile_h;   /* (tile_w + 2) * (tile_h + 2) <= 256 */
     int32_t graph_steps;
+    int32_t sort_mode;
 } dpd_tuning;
 
 /* message of the last failed call on this thread ("" if none) */
@@ -436,6 +441,17 @@ DPD_API int dpd_window_loss(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *s
  * of the window, as after dpd_window_loss. */
 DPD_API int dpd_window_adjoint(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
                                const double *target, double *loss, double *grad, double *rdf_out);
+/* dpd_window_adjoint plus the cotangents of the window's start state: the
+ * loss's gradient with respect to the positions (xbar), the stored half-step
+ * velocities (vhbar) and the predicted velocities (vtbar) the window starts
+ * from, the start forces being F(x, vt) of that state.  Each is 2 x N floats
+ * (x, y interleaved) over all replicas packed, replica r's bead of gid g at
+ * b0_r + g (b0_r = the bead counts of the replicas before r); any may be NULL.
+ * Needs spec->horizon == 0 (the full reverse pass), else DPD_E_ARG.  No
+ * counterpart in the reference (it has no reverse mode). */
+DPD_API int dpd_window_adjoint_state(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
+                                     const double *target, double *loss, double *grad, double *rdf_out, float *xbar,
+                                     float *vhbar, float *vtbar);
 /* Vector-Jacobian product of the pair + bond forces of replica r's current
  * configuration at `step` (noise key): given the force cotangent (gx, gy, slot
  * order), the gradients with respect to positions (xbar), predicted velocities
@@ -451,11 +467,18 @@ DPD_API int dpd_force_vjp(dpd_handle *h, int32_t replica, int64_t step, const fl
  * allowed: the stable cell sort of n positions (x, y: DEVICE arrays in [0, L))
  * with the cell grid of the handle API, writing cstart (floor(L)^2 + 1 DEVICE
  * entries) and order (n DEVICE entries: input index of each sorted slot).
+ * The grid side is floor((float)L); an L whose rounding to float changes its
+ * floor (31.9999999 -> 32.0f) is refused with DPD_E_ARG, so floor(L) is
+ * always the side.  Positions outside [0, L) are clamped into the edge cells.
+ * Any number of beads may share a cell (crowded cells are sorted by whole
+ * CTAs; the work stays bounded even with every bead in one cell).
  * Scratch lives in one fixed device array of the library (8.0 MiB per GPU):
  * n <= DPD_NOALLOC_MAX_BEADS and floor(L)^2 <= DPD_NOALLOC_MAX_CELLS, else
  * DPD_E_ARG.  Calls whose work overlaps on the GPU race on that array.  The
- * first call on a device looks up the array's address: make it before any
- * stream capture.  stream: a cudaStream_t (NULL = the default stream). */
+ * first call on a device looks up the array's address and keeps it for the
+ * life of the process: make it before any stream capture, and do not call
+ * this on a device after a cudaDeviceReset of it.  stream: a cudaStream_t
+ * (NULL = the default stream). */
 #define DPD_NOALLOC_MAX_BEADS 1048576
 #define DPD_NOALLOC_MAX_CELLS 524288
 DPD_API int dpd_sort_cells_noalloc(const float *x, const float *y, int32_t n, double L, int32_t *cstart,

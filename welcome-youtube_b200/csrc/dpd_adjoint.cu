@@ -223,6 +223,22 @@ __global__ void __launch_bounds__(BEAD_TPB) k_adj_gather(const uint32_t *__restr
     g[d] = F[(tg[d] & GID_MASK) + (uint32_t)reps[c.rep].b0];
 }
 
+// cotangents of the window's start state in gid order: x_bar(0) gains the part
+// that flows through the start forces (xb = J_x^T F_bar(0)), and the predicted
+// velocity's cotangent is that force VJP's vb; vh_bar(0) is V as it stands
+__global__ void __launch_bounds__(BEAD_TPB) k_adj_state(const uint32_t *__restrict__ tg, const RepDev *__restrict__ reps,
+                                                        const Chunk *__restrict__ ch, const float2 *__restrict__ xb,
+                                                        const float2 *__restrict__ vb, float2 *__restrict__ X,
+                                                        float2 *__restrict__ VT) {
+    const Chunk c = ch[blockIdx.x];
+    const int d = c.begin + (int)threadIdx.x;
+    if (d >= c.end) return;
+    const uint32_t g = (tg[d] & GID_MASK) + (uint32_t)reps[c.rep].b0;
+    const float2 x = X[g], a = xb[d];
+    X[g] = make_float2(x.x + a.x, x.y + a.y);
+    VT[g] = vb[d];
+}
+
 // copy a configuration out of the engine's buffers (for recomputation)
 __global__ void k_adj_save(int n, const float2 *pos, const float2 *vt, const uint32_t *tg, const int2 *link,
                            float2 *opos, float2 *ovt, uint32_t *otg, int2 *olink) {
@@ -259,6 +275,11 @@ void launch_adj_update(const uint32_t *tg, const RepDev *rep, const Chunk *bch, 
 void launch_adj_gather(const uint32_t *tg, const RepDev *rep, const Chunk *bch, int nbch, const float2 *F, float2 *g,
                        cudaStream_t s) {
     k_adj_gather<<<nbch, BEAD_TPB, 0, s>>>(tg, rep, bch, F, g);
+}
+
+void launch_adj_state(const uint32_t *tg, const RepDev *rep, const Chunk *bch, int nbch, const float2 *xb,
+                      const float2 *vb, float2 *X, float2 *VT, cudaStream_t s) {
+    k_adj_state<<<nbch, BEAD_TPB, 0, s>>>(tg, rep, bch, xb, vb, X, VT);
 }
 
 void launch_adj_save(int n, const float2 *pos, const float2 *vt, const uint32_t *tg, const int2 *link, float2 *opos,

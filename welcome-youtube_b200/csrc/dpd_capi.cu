@@ -75,7 +75,8 @@ struct dpd_handle {
     Bufs b{};
     int cur = 0;
     // force kernel: 0 = cell tiles in shared memory (half shell), 1 = one thread per bead (full shell)
-    int force_kernel = 0;
+    int force_kernel = 0;      // 0 cell tiles, 1 thread per bead, 2 cell tiles staged by bulk copies
+    int sort_mode = 0;         // cell-count scan: 0 two passes (k_scan1, k_scan2), 1 one pass (k_scan_lb)
     int tile_w = 8, tile_h = 16;
     TileDesc *d_tiles = nullptr;
     int ntiles = 0;
@@ -366,9 +367,16 @@ static int build_tiles(dpd_handle *h) {
     return DPD_OK;
 }
 
+// the exclusive scan of the cell counts, in the form the handle's tuning picked
+static void enqueue_scan(dpd_handle *h, bool step_inc) {
+    if (h->sort_mode == 1) launch_scan_lb(h->b, h->C, step_inc, h->s);
+    else launch_scan(h->b, h->C, step_inc, h->s);
+}
+
 static void enqueue_forces(dpd_handle *h, bool next_keys) {
     if (h->any_mol) launch_mol_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     if (h->force_kernel == 0) launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
+    else if (h->force_kernel == 2) launch_forces_bulk(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
     else launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, next_keys, h->s);
 }
 
@@ -411,7 +419,9 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     h->ncch = (int)cch.size();
     CK(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
     if (tile_setup() != 0) return fail(DPD_E_CUDA, "cannot reserve %zu bytes of shared memory per CTA", tile_smem_bytes());
-    if (const char *e = getenv("DPD_FORCES")) h->force_kernel = strcmp(e, "bead") == 0 ? 1 : 0;
+    if (const char *e = getenv("DPD_FORCES"))
+        h->force_kernel = strcmp(e, "bead") == 0 ? 1 : (strcmp(e, "bulk") == 0 ? 2 : 0);
+
     // default tile: 8 x 16 cells, smaller when that would leave SMs idle (at least ~4 tiles per SM)
     while (h->C / ((int64_t)h->tile_w * h->tile_h) < 4 * 148 && h->tile_w * h->tile_h > 4) {
         if (h->tile_h > h->tile_w) h->tile_h /= 2;
@@ -440,6 +450,10 @@ static int create_impl(dpd_handle *h, const dpd_params *params, int32_t nrep, co
     TRY(dalloc(h, &b.count, C + 4));
     TRY(dalloc(h, &b.cstart, C + 4));
     TRY(dalloc(h, &b.bsum, C / SCAN_PER_BLOCK + 2));
+    TRY(dalloc(h, &b.scan_state, C / SCAN_PER_BLOCK + 2));
+    TRY(dalloc(h, &b.scan_ticket, 1));
+    CK(cudaMemset(b.scan_state, 0, (C / SCAN_PER_BLOCK + 2) * sizeof(unsigned long long)));
+    CK(cudaMemset(b.scan_ticket, 0, sizeof(unsigned long long)));
     TRY(dalloc(h, &b.claim, N));
     TRY(dalloc(h, &b.req, N));
     TRY(dalloc(h, &b.grow_list, N));
@@ -570,6 +584,8 @@ static int check_status(dpd_handle *h) {
     if (st.flags) {
         CK(cudaMemsetAsync(&h->b.status->flags, 0, sizeof(unsigned), h->s));
         CK(cudaStreamSynchronize(h->s));
+        if (st.flags & DPD_F_WAIT)
+            return fail(DPD_E_TIMEOUT, "a bounded device wait gave up (bulk copies of the force kernel, or the scan)");
         if (st.flags & DPD_F_ANALYSIS) return fail(DPD_E_STATE, "cluster analysis did not converge");
         if (st.flags & DPD_F_CATALYST)
             return fail(DPD_E_STATE, "a catalyst's neighbourhood did not fit the staging area, or a search found "
@@ -688,7 +704,7 @@ static void enqueue_sort(dpd_handle *h, PermuteMode mode) {
     // counts of the CURRENT positions
     cudaMemsetAsync(h->b.count, 0, (size_t)(h->C + 4) * sizeof(uint32_t), h->s);
     launch_keys(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, false, h->s);
-    launch_scan(h->b, h->C, false, h->s);
+    enqueue_scan(h, false);
     launch_place(h->b, h->d_bch, h->nbch, h->s);
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     clear_stir(h);
@@ -850,7 +866,7 @@ static bool cat_at(const dpd_handle *h, int64_t s) {
 static void enqueue_step(dpd_handle *h, int64_t s) {
     const bool cat = cat_at(h, s);
     if (!cat) {
-        launch_scan(h->b, h->C, true, h->s);
+        enqueue_scan(h, true);
         launch_place(h->b, h->d_bch, h->nbch, h->s);
         launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     } else {
@@ -937,8 +953,11 @@ extern "C" int dpd_sync(dpd_handle *h) {
 
 extern "C" int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t) {
     if (!h || !t) return fail(DPD_E_ARG, "null argument");
-    if (t->force_kernel != 0 && t->force_kernel != 1) return fail(DPD_E_ARG, "force_kernel must be 0 or 1");
+    if (t->force_kernel < 0 || t->force_kernel > 2) return fail(DPD_E_ARG, "force_kernel must be 0, 1 or 2");
+    if (t->force_kernel == 2 && t->tile_w + 2 > 32)
+        return fail(DPD_E_ARG, "the bulk-staged force kernel takes tiles of at most 30 columns");
     if (t->graph_steps < 1) return fail(DPD_E_ARG, "graph_steps must be >= 1");
+    if (t->sort_mode < 0 || t->sort_mode > 1) return fail(DPD_E_ARG, "sort_mode must be 0 or 1");
     CK(cudaStreamSynchronize(h->s));
     const int ow = h->tile_w, oh = h->tile_h;
     h->tile_w = t->tile_w;
@@ -951,6 +970,7 @@ extern "C" int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t) {
         return r;
     }
     h->force_kernel = t->force_kernel;
+    h->sort_mode = t->sort_mode;
     h->gsteps = graph_len(h, t->graph_steps);
     drop_graphs(h);
     return DPD_OK;
@@ -962,6 +982,7 @@ extern "C" int dpd_get_tuning(const dpd_handle *h, dpd_tuning *t) {
     t->tile_w = h->tile_w;
     t->tile_h = h->tile_h;
     t->graph_steps = h->gsteps;
+    t->sort_mode = h->sort_mode;
     return DPD_OK;
 }
 
@@ -974,8 +995,8 @@ extern "C" int dpd_set_graph_steps(dpd_handle *h, int32_t steps) {
 }
 
 // One step launched kernel by kernel with CUDA events between the launches on
-// the handle's stream; ms[k] = device time of kernel k (scan1, scan2, place,
-// cellfix, permute, [2 chemistry], [catalyst check + its sort], forces).  The
+// the handle's stream; ms[k] = device time of kernel k (scan1 (the whole scan
+// with sort_mode 1), scan2 (0 ms with sort_mode 1), place, cellfix, permute, [2 chemistry], [catalyst check + its sort], forces).  The
 // step is a real step; on a step with a catalyst check the first entry is the
 // step counter's kernel, the next three are not launched (0 ms) and the
 // permute keeps the slot order.
@@ -989,10 +1010,14 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     for (auto &e : ev) CK(cudaEventCreate(&e));
     int k = 0;
     CK(cudaEventRecord(ev[k++], h->s));
-    if (!cat) launch_scan_part(h->b, h->C, true, 1, h->s);
-    else launch_step_begin(h->b, h->nrep, h->s);
+    if (!cat) {
+        if (h->sort_mode == 1) launch_scan_lb(h->b, h->C, true, h->s);
+        else launch_scan_part(h->b, h->C, true, 1, h->s);
+    } else {
+        launch_step_begin(h->b, h->nrep, h->s);
+    }
     CK(cudaEventRecord(ev[k++], h->s));
-    if (!cat) launch_scan_part(h->b, h->C, true, 2, h->s);
+    if (!cat && h->sort_mode == 0) launch_scan_part(h->b, h->C, true, 2, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
     if (!cat) launch_place(h->b, h->d_bch, h->nbch, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
@@ -1395,7 +1420,7 @@ static StateView view_cur(dpd_handle *h) {
 }
 
 static void enqueue_plain_step(dpd_handle *h) {  // one step without chemistry (windows require chem off)
-    launch_scan(h->b, h->C, true, h->s);
+    enqueue_scan(h, true);
     launch_place(h->b, h->d_bch, h->nbch, h->s);
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
     clear_stir(h);
@@ -1457,9 +1482,14 @@ static int count_pairs(dpd_handle *h, const dpd_rdf_spec *spec, std::vector<long
     return DPD_OK;
 }
 
+// state_out (optional): the cotangents of the start state, gid order packed by
+// replica, x/y interleaved: [0] positions, [1] stored half-step velocities,
+// [2] predicted velocities (2 N floats each; host or device memory)
 static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rdf_spec *spec, const double *target,
-                       double *loss, double *grad, double *rdf_out, bool backward) {
+                       double *loss, double *grad, double *rdf_out, bool backward, float *const *state_out = nullptr) {
     TRY(check_window(h, nsteps, spec, target));
+    if (state_out && spec->horizon > 0)
+        return fail(DPD_E_ARG, "start-state cotangents need the full reverse pass (horizon 0)");
     if (ckpt < 1) ckpt = (int32_t)nsteps;
     const int nseg = (int)((nsteps + ckpt - 1) / ckpt);
     const int nb = spec->nbin;
@@ -1527,6 +1557,12 @@ static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rd
     launch_adj_gather(v0.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
     launch_force_vjp(v0, step0 + k_stop, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
     CK(cudaGetLastError());
+    if (state_out) {
+        launch_adj_state(v0.tg, h->d_rep, h->d_bch, h->nbch, A.xb, A.vb, A.X, A.g, h->s);
+        const float2 *src[3] = {A.X, A.V, A.g};
+        for (int k = 0; k < 3; k++)
+            if (state_out[k]) CK(cudaMemcpyAsync(state_out[k], src[k], N * sizeof(float2), cudaMemcpyDefault, h->s));
+    }
     if (grad) {
         CK(cudaMemcpyAsync(grad, A.grad, (size_t)h->nrep * DPD_NGRAD * sizeof(double), cudaMemcpyDeviceToHost, h->s));
     }
@@ -1548,6 +1584,14 @@ extern "C" int dpd_window_adjoint(dpd_handle *h, int64_t nsteps, int32_t ckpt_ev
                                   const double *target, double *loss, double *grad, double *rdf_out) {
     if (!h) return fail(DPD_E_ARG, "null handle");
     return window_impl(h, nsteps, ckpt_every, spec, target, loss, grad, rdf_out, true);
+}
+
+extern "C" int dpd_window_adjoint_state(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
+                                        const double *target, double *loss, double *grad, double *rdf_out,
+                                        float *xbar, float *vhbar, float *vtbar) {
+    if (!h) return fail(DPD_E_ARG, "null handle");
+    float *const out[3] = {xbar, vhbar, vtbar};
+    return window_impl(h, nsteps, ckpt_every, spec, target, loss, grad, rdf_out, true, out);
 }
 
 extern "C" int dpd_force_vjp(dpd_handle *h, int32_t r, int64_t step, const float *gx, const float *gy, float *xbar_x,

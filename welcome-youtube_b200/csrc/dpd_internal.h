@@ -42,6 +42,7 @@
 #define DPD_F_CATALYST 0x80u    // a catalyst's neighbourhood exceeded the staging capacity
 #define DPD_CAT_MAXTR 64        // orientation trials of one lipid synthesis (syn_tries)
 #define DPD_F_ANALYSIS 0x200u   // a cluster union kept losing its compare-and-swap (analysis result invalid)
+#define DPD_F_WAIT 0x800u       // a bounded device wait (an mbarrier, a look-back of the scan) gave up
 #define DPD_F_INPUT 0x400u      // a state handed in had a non-finite position, a type >= DPD_MAXT, a gid >= n
                                 // or a link outside [-1, n): stored sanitised, the call fails
 
@@ -143,6 +144,8 @@ struct Bufs {
     uint32_t *count;
     int32_t *cstart;            // C + 1
     int32_t *bsum;              // scan block totals
+    unsigned long long *scan_state;   // single-pass scan: per block (epoch | flag | value), see k_scan_lb
+    unsigned long long *scan_ticket;  // single-pass scan: block tickets taken so far (never reset)
     uint32_t *claim;            // per bead, 0xFFFFFFFF when unclaimed
     int32_t *req;               // per candidate chemistry request target (-1 none)
     int2 *grow_list;            // (slot, replica) of P beads whose growth draw succeeded
@@ -219,6 +222,8 @@ void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, in
 void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s);
 
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s);
+// the same exclusive scan in one pass (decoupled look-back between blocks)
+void launch_scan_lb(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s);
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s);
 void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
@@ -252,6 +257,9 @@ void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDes
                         bool next_keys, cudaStream_t s);
 int tile_setup();
 size_t tile_smem_bytes();
+size_t bulk_smem_bytes();
+void launch_forces_bulk(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
+                        bool next_keys, cudaStream_t s);
 void launch_force_vjp(const StateView &sv, long long step, const RepDev *rep, const Chunk *bch, int nbch,
                       const float2 *g, float2 *xbar, float2 *vbar, double *grad, cudaStream_t s);
 void launch_rdf(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,
@@ -262,6 +270,8 @@ void launch_adj_update(const uint32_t *tg, const RepDev *rep, const Chunk *bch, 
                        const float2 *vb, float2 *X, float2 *V, float2 *F, cudaStream_t s);
 void launch_adj_gather(const uint32_t *tg, const RepDev *rep, const Chunk *bch, int nbch, const float2 *F, float2 *g,
                        cudaStream_t s);
+void launch_adj_state(const uint32_t *tg, const RepDev *rep, const Chunk *bch, int nbch, const float2 *xb,
+                      const float2 *vb, float2 *X, float2 *VT, cudaStream_t s);
 void launch_adj_save(int n, const float2 *pos, const float2 *vt, const uint32_t *tg, const int2 *link, float2 *opos,
                      float2 *ovt, uint32_t *otg, int2 *olink, cudaStream_t s);
 int chem_kernel_count();

@@ -160,6 +160,132 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan2(int32_t *__restrict__ cstart
     if ((int)blockIdx.x == nblocks - 1 && threadIdx.x == 0) cstart[C] = prefix + bsum[nblocks - 1];
 }
 
+// Single pass (decoupled look-back, after Merrill and Garland's single-pass
+// prefix scan): a block scans its 1024 counts, publishes its total, then sums
+// its predecessors' published values, stopping at the first inclusive prefix.
+// Blocks take their index from a ticket counter that is never reset, so a
+// block waits only on blocks that are already running, and the launch's epoch
+// (ticket / blocks) tags every published word: words of earlier launches read
+// as not yet published, and nothing has to be cleared between launches.
+// Published word: epoch (30 bits) | flag (2 bits: 1 block total, 2 inclusive
+// prefix) | value (32 bits).  Waits on a predecessor are bounded; a block that
+// gives up raises DPD_F_WAIT.
+#define LB_AGG 1ull
+#define LB_INC 2ull
+#define LB_SPIN_LIMIT (1 << 22)
+
+__device__ __forceinline__ unsigned long long lb_load(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void lb_store(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(SCAN_TPB) k_scan_lb(uint32_t *__restrict__ count, int32_t *__restrict__ cstart,
+                                                      uint32_t *__restrict__ fill, unsigned long long *state,
+                                                      unsigned long long *ticket, long long C, int nblocks,
+                                                      long long *__restrict__ step, int step_inc,
+                                                      DevStatus *__restrict__ status) {
+    pdl_begin();
+    __shared__ unsigned long long sh_ticket;
+    __shared__ int sh_excl;
+    if (threadIdx.x == 0) sh_ticket = atomicAdd(ticket, 1ull);
+    __syncthreads();
+    const int id = (int)(sh_ticket % (unsigned long long)nblocks);
+    const unsigned long long epoch = (sh_ticket / (unsigned long long)nblocks) & 0x3FFFFFFFull;
+    const long long base = (long long)id * SCAN_PER_BLOCK + (long long)threadIdx.x * SCAN_PER_THREAD;
+    int v[SCAN_PER_THREAD];
+    int sum = 0;
+    if (base + SCAN_PER_THREAD <= C) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(count + base);
+        v[0] = (int)q.x;
+        v[1] = (int)q.y;
+        v[2] = (int)q.z;
+        v[3] = (int)q.w;
+        *reinterpret_cast<uint4 *>(count + base) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; k++) {
+            v[k] = base + k < C ? (int)count[base + k] : 0;
+            if (base + k < C) count[base + k] = 0u;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; k++) sum += v[k];
+    int total;
+    int ex = block_exclusive_scan(sum, &total);
+    // publish this block's total, then find the sum of all earlier blocks
+    if (threadIdx.x == 0) {
+        lb_store(state + id, epoch << 34 | (id == 0 ? LB_INC : LB_AGG) << 32 | (unsigned)total);
+        if (step_inc && id == 0) {
+            *step += 1;
+            status->n_grow = 0u;  // the chemistry candidate lists of the new step start empty
+            status->n_bond = 0u;
+        }
+    }
+    if (threadIdx.x < 32) {
+        const int lane = (int)threadIdx.x;
+        int excl = 0;
+        bool gave_up = false;
+        for (int j = id - 1; j >= 0;) {
+            // lane k looks at block j - k; wait until each of them has published in this launch
+            const int jj = j - lane;
+            unsigned long long w = 0;
+            if (jj >= 0) {
+                int spins = 0;
+                while (true) {
+                    w = lb_load(state + jj);
+                    if ((w >> 34) == epoch && ((w >> 32) & 3ull) != 0ull) break;
+                    if (++spins > LB_SPIN_LIMIT) {
+                        gave_up = true;
+                        w = epoch << 34 | LB_INC << 32;  // stop here: the result is flagged as invalid
+                        break;
+                    }
+                }
+            }
+            const bool inc = jj >= 0 && ((w >> 32) & 3ull) == LB_INC;
+            const unsigned incm = __ballot_sync(0xffffffffu, inc);
+            const int stop = incm ? __ffs(incm) - 1 : 31;  // the nearest inclusive prefix ends the walk
+            int val = (jj >= 0 && lane <= stop) ? (int)(unsigned)(w & 0xFFFFFFFFull) : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+            excl += val;
+            if (incm) break;
+            j -= 32;
+        }
+        if (__any_sync(0xffffffffu, gave_up) && lane == 0) raise_flag(status, DPD_F_WAIT);
+        if (lane == 0) {
+            sh_excl = excl;
+            if (id > 0) lb_store(state + id, epoch << 34 | LB_INC << 32 | (unsigned)(excl + total));
+        }
+    }
+    __syncthreads();
+    const int prefix = sh_excl;
+    ex += prefix;
+    if (base + SCAN_PER_THREAD <= C) {
+        int4 o;
+        o.x = ex;
+        o.y = ex + v[0];
+        o.z = o.y + v[1];
+        o.w = o.z + v[2];
+        *reinterpret_cast<int4 *>(cstart + base) = o;
+        *reinterpret_cast<int4 *>(fill + base) = o;
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_PER_THREAD; k++) {
+            if (base + k < C) {
+                cstart[base + k] = ex;
+                fill[base + k] = (uint32_t)ex;
+            }
+            ex += v[k];
+        }
+    }
+    if (id == nblocks - 1 && threadIdx.x == 0) cstart[C] = prefix + total;
+}
+
 // ---------------------------------------------------------------- placement and the stable fix-up
 
 // The beads of a warp that go to the same cell share one atomic on its cursor
@@ -890,6 +1016,12 @@ static void scan_part(const Bufs &b, int64_t C, bool step_inc, int part, const i
 
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s) {
     scan_part(b, C, step_inc, part, nullptr, s);
+}
+
+void launch_scan_lb(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
+    const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
+    launch_pdl(k_scan_lb, nb, SCAN_TPB, 0, s, b.count, b.cstart, b.fill, b.scan_state, b.scan_ticket, (long long)C, nb,
+               b.step, step_inc ? 1 : 0, b.status);
 }
 
 void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {

@@ -24,6 +24,8 @@
 // HBM, and the cell of the next position with its count (the first half of
 // the next step's sort).  A tile whose beads do not fit in shared memory
 // computes its owned beads straight from HBM instead (bead_pairs_direct).
+#include <algorithm>
+
 #include "dpd_device.cuh"
 
 #define TILE_TPB 256
@@ -32,22 +34,28 @@
 #define TILE_MAXC 256
 #define TILE_QCAP 128  // per-warp ring; < 64 entries wait between drains, at most 64 arrive per round
 
-struct TileSmem {
+struct __align__(16) TileBead {    // one tile's staged beads and their local layout
     float2 pos[TILE_MAXB];
     float2 vt[TILE_MAXB];
     uint32_t tg[TILE_MAXB];
     int32_t accx[TILE_MAXB];      // fixed-point force sums (separate arrays: 32 banks for the atomics)
     int32_t accy[TILE_MAXB];
-    uint16_t lxy[TILE_MAXB];      // local cell of each bead: lx << 8 | ly
+    uint16_t lxy[TILE_MAXB];      // local cell of each bead: lx << 8 | ly (TILE_PAD: a padding slot)
     uint8_t img[TILE_MAXB];       // periodic image code: (ix + 1) | (iy + 1) << 2
     int32_t lcs[TILE_MAXC + 1];   // local cell starts (column-major over (w+2) x (h+2))
     int32_t gst[TILE_MAXC];       // global slot of each local cell's first bead
-    uint32_t q[TILE_WARPS][TILE_QCAP];
     float a[DPD_MAXT * DPD_MAXT];
-    int32_t scan[TILE_WARPS];
     int32_t n;
+};
+
+struct TileSmem {
+    TileBead t;
+    uint32_t q[TILE_WARPS][TILE_QCAP];
+    int32_t scan[TILE_WARPS];
     int32_t next_chunk;           // source chunks are handed to warps as they finish their last one
 };
+
+#define TILE_PAD 0xFFFFu          // lxy of a slot that holds no bead of the tile (bulk-copy padding)
 
 // periodic image shift of a pair along one axis: (code_s - code_t) L, exactly 0 or +-L
 __device__ __forceinline__ float img_shift(int dc, float L) { return dc == 0 ? 0.0f : (dc > 0 ? L : -L); }
@@ -59,7 +67,7 @@ struct PairConst {
 
 // the pair force on s from t as fixed-point terms (a queued pair: inside the cutoff)
 template <bool WRAP, int NOISE>
-__device__ __forceinline__ void tile_pair(const TileSmem &S, const PairConst &pc, int s, int t, int &qx, int &qy,
+__device__ __forceinline__ void tile_pair(const TileBead &S, const PairConst &pc, int s, int t, int &qx, int &qy,
                                           float &fmax) {
     const float2 ps = S.pos[s], pt = S.pos[t];
     float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
@@ -95,7 +103,7 @@ __device__ __forceinline__ void tile_pair(const TileSmem &S, const PairConst &pc
 }
 
 // +q to s, -q to t; halo accumulators take their share too and are ignored
-__device__ __forceinline__ void tile_add(TileSmem &S, uint32_t v, int qx, int qy) {
+__device__ __forceinline__ void tile_add(TileBead &S, uint32_t v, int qx, int qy) {
     const int s = (int)(v >> 16), t = (int)(v & 0xFFFFu);
     atomicAdd(&S.accx[s], qx);
     atomicAdd(&S.accy[s], qy);
@@ -105,7 +113,7 @@ __device__ __forceinline__ void tile_add(TileSmem &S, uint32_t v, int qx, int qy
 
 // evaluate ring entries [head, head + cnt), cnt <= 64: two independent chains per lane
 template <bool WRAP, int NOISE>
-__device__ __forceinline__ void drain(TileSmem &S, const PairConst &pc, const uint32_t *q, int head, int cnt,
+__device__ __forceinline__ void drain(TileBead &S, const PairConst &pc, const uint32_t *q, int head, int cnt,
                                       int lane, float &fmax) {
     const int e1 = lane, e2 = lane + 32;
     const bool has1 = e1 < cnt, has2 = e2 < cnt;
@@ -122,7 +130,7 @@ __device__ __forceinline__ void drain(TileSmem &S, const PairConst &pc, const ui
 }
 
 // rows [lo, hi] of local column c that hold owned cells, as a bead index range
-__device__ __forceinline__ void owned_rows(const TileSmem &S, int c, int LH, int tw, int th, int &b0, int &b1) {
+__device__ __forceinline__ void owned_rows(const TileBead &S, int c, int LH, int tw, int th, int &b0, int &b1) {
     if (c >= 1 && c <= tw) {
         b0 = S.lcs[c * LH + 1];
         b1 = S.lcs[c * LH + th + 1];
@@ -131,21 +139,25 @@ __device__ __forceinline__ void owned_rows(const TileSmem &S, int c, int LH, int
     }
 }
 
+// The screened pairs of the staged tile S, evaluated on full warps.  q: this
+// warp's ring; next_chunk: the CTA's chunk counter (starts at the warp count);
+// first: this warp's first chunk of 32 sources.
 template <bool WRAP, int NOISE>
-__device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int tw, int th, DevStatus *status) {
-    const int lane = (int)lane_id(), wq = (int)threadIdx.x >> 5;
+__device__ void tile_pairs(TileBead &S, uint32_t *q, int *next_chunk, int first, const PairConst &pc, int LW, int LH,
+                           int tw, int th, DevStatus *status) {
+    const int lane = (int)lane_id();
     const uint32_t below = (1u << lane) - 1u;
-    uint32_t *q = S.q[wq];
     const int nsrc = S.lcs[(LW - 1) * LH];  // the last column (right halo) holds no sources
     int head = 0, tail = 0;
     float fmax = 0.0f;
-    for (int base = wq * 32; base < nsrc;) {
+    for (int base = first * 32; base < nsrc;) {
         const int s = base + lane;
         int r1s = 0, len1 = 0, r2s = 0, len = 0;
         float2 ps = make_float2(0.0f, 0.0f);
         int is = 0;
-        if (s < nsrc) {
-            const int v = S.lxy[s], lx = v >> 8, ly = v & 255, l = lx * LH + ly;
+        const int v = s < nsrc ? S.lxy[s] : (int)TILE_PAD;
+        if (v != (int)TILE_PAD) {
+            const int lx = v >> 8, ly = v & 255, l = lx * LH + ly;
             ps = S.pos[s];
             if (WRAP) is = S.img[s];
             int r1e = S.lcs[l + (ly + 1 < LH ? 2 : 1)];
@@ -199,7 +211,7 @@ __device__ void tile_pairs(TileSmem &S, const PairConst &pc, int LW, int LH, int
             }
         }
         int nxt = 0;
-        if (lane == 0) nxt = atomicAdd(&S.next_chunk, 1);
+        if (lane == 0) nxt = atomicAdd(next_chunk, 1);
         base = __shfl_sync(0xffffffffu, nxt, 0) * 32;
     }
     while (tail > head) {
@@ -263,16 +275,139 @@ __device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev
 
 #define EPI_ITEMS 2  // owned beads per thread per round of the epilogue
 
+// The owned beads of tile td straight from HBM (full-shell sums, bonds, force,
+// next key): the path for a tile too crowded for shared memory (rare; the
+// same bits).  arow: the tile's a_ij table in shared memory.
+template <bool NEXTKEY>
+__device__ void tile_direct(const Bufs &b, int cur, const RepDev &R, const TileDesc &td, const float *a, long long step,
+                            float &mb) {
+    const int ncy = R.ncy, tid = (int)threadIdx.x;
+    const int32_t *__restrict__ cs = b.cstart + R.c0;
+    PairConst pk;
+    pk.nk = make_noise_key(R, step);
+    for (int c = 1; c <= td.w; c++) {
+        const int gx = td.cx0 + c - 1, g0 = cs[gx * ncy + td.cy0], g1 = cs[gx * ncy + td.cy0 + td.h];
+        for (int base = g0; base < g1; base += blockDim.x) {
+            const int g = base + tid;
+            const bool act = g < g1;
+            uint32_t key = 0;
+            if (act) {
+                PairCtx pc;
+                pc.pos = b.pos[cur];
+                pc.vt = b.vt[cur];
+                pc.tg = b.tg[cur];
+                pc.pi = pc.pos[g];
+                pc.vi = pc.vt[g];
+                const uint32_t tgi = pc.tg[g];
+                pc.gi = tgi & GID_MASK;
+                pc.arow = a + (tgi >> TYPE_SHIFT) * DPD_MAXT;
+                pc.nk = pk.nk;
+                pc.L = R.L;
+                pc.h = R.halfL;
+                pc.gam = R.gamma;
+                pc.sdt = sdt_at(R, step);
+                long long ax = 0, ay = 0;
+                bead_pairs_direct(pc, R, cs, g, ax, ay);
+                finish_bead<NEXTKEY>(b, cur, R, td.rep, g, pc.pi, ax, ay, mb, key);
+            }
+            if (NEXTKEY) {
+                count_key(b.count, key, act);
+                if (act) b.key[g] = key;
+            }
+        }
+    }
+}
+
+// The pairs of a staged tile: the screen and the ring, one instantiation per
+// image mode and noise generator
+__device__ __forceinline__ void tile_pairs_any(TileBead &S, uint32_t *q, int *next_chunk, int first,
+                                               const RepDev &R, const TileDesc &td, long long step,
+                                               DevStatus *status) {
+    PairConst pc;
+    pc.nk = make_noise_key(R, step);
+    pc.L = R.L;
+    pc.gam = R.gamma;
+    pc.sdt = sdt_at(R, step);
+    const int LW = td.w + 2, LH = td.h + 2;
+    const bool wrap = td.cx0 == 0 || td.cy0 == 0 || td.cx0 + td.w >= R.ncx || td.cy0 + td.h >= R.ncy;
+    if (R.noise == 1) {
+        if (wrap) tile_pairs<true, 1>(S, q, next_chunk, first, pc, LW, LH, td.w, td.h, status);
+        else tile_pairs<false, 1>(S, q, next_chunk, first, pc, LW, LH, td.w, td.h, status);
+    } else {
+        if (wrap) tile_pairs<true, 0>(S, q, next_chunk, first, pc, LW, LH, td.w, td.h, status);
+        else tile_pairs<false, 0>(S, q, next_chunk, first, pc, LW, LH, td.w, td.h, status);
+    }
+}
+
+// The epilogue of a staged tile: over the local index range of the owned
+// columns, every owned bead (halo rows and padding slots in that range are
+// skipped) gets its bonds, its force written to HBM and its next cell key.
+// The loads of a round are issued first.
+template <bool NEXTKEY>
+__device__ __forceinline__ void tile_epilogue(const Bufs &b, int cur, const RepDev &R, const TileDesc &td,
+                                              const TileBead &S, float &mb) {
+    const int LH = td.h + 2, tid = (int)threadIdx.x;
+    const int e0 = S.lcs[LH + 1], e1 = S.lcs[td.w * LH + td.h + 1];
+    const float2 *__restrict__ gpos = b.pos[cur];
+    for (int base = e0; base < e1; base += EPI_ITEMS * blockDim.x) {
+        int gg[EPI_ITEMS];
+        bool own[EPI_ITEMS];
+#pragma unroll
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            const int k = base + j * (int)blockDim.x + tid;
+            own[j] = false;
+            gg[j] = 0;
+            if (k < e1) {
+                const int v = S.lxy[k], ly = v & 255, l = (v >> 8) * LH + ly;
+                own[j] = v != (int)TILE_PAD && ly >= 1 && ly <= td.h;
+                if (own[j]) gg[j] = S.gst[l] + (k - S.lcs[l]);
+            }
+        }
+        int2 lk[EPI_ITEMS];
+        float2 vv[EPI_ITEMS];
+#pragma unroll
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            lk[j] = own[j] ? b.link[cur][gg[j]] : make_int2(-1, -1);
+            vv[j] = (NEXTKEY && own[j]) ? b.vh[cur][gg[j]] : make_float2(0.0f, 0.0f);
+        }
+        float2 pj[EPI_ITEMS][2];
+#pragma unroll
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            pj[j][0] = lk[j].x >= 0 ? gpos[lk[j].x] : make_float2(0.0f, 0.0f);
+            pj[j][1] = lk[j].y >= 0 ? gpos[lk[j].y] : make_float2(0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            const int k = base + j * (int)blockDim.x + tid;
+            uint32_t key = 0;
+            if (own[j])
+                finish_loaded<NEXTKEY>(b, cur, R, td.rep, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j], vv[j],
+                                       mb, key);
+            if (NEXTKEY) {
+                count_key(b.count, key, own[j]);
+                if (own[j]) b.key[gg[j]] = key;
+            }
+        }
+    }
+}
+
+// the running max bond of a tile's replica (one atomic per warp)
+__device__ __forceinline__ void max_bond_out(const Bufs &b, int rep, float mb) {
+    const unsigned mbb = __reduce_max_sync(0xffffffffu, __float_as_uint(mb));
+    if (lane_id() == 0 && mbb != 0u) atomicMax(b.obs + (size_t)rep * OBS_N + 4, (unsigned long long)mbb);
+}
+
 template <bool NEXTKEY>
 __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const TileDesc *__restrict__ tiles) {
     pdl_begin();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    TileSmem &S = *reinterpret_cast<TileSmem *>(smem_raw);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    TileSmem &SS = *reinterpret_cast<TileSmem *>(smem_raw);
+    TileBead &S = SS.t;
     const TileDesc td = tiles[blockIdx.x];
     const RepDev &R = reps[td.rep];
     const int ncx = R.ncx, ncy = R.ncy;
-    const int LW = td.w + 2, LH = td.h + 2, nl = LW * LH;
+    const int LH = td.h + 2, nl = (td.w + 2) * LH;
     const int32_t *__restrict__ cs = b.cstart + R.c0;
     const int tid = (int)threadIdx.x, lane = (int)lane_id(), wq = tid >> 5;
     const long long step = *b.step;
@@ -299,10 +434,10 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
-        if (lane == 31) S.scan[wq] = x;
+        if (lane == 31) SS.scan[wq] = x;
         __syncthreads();
         before = 0;
-        for (int k = 0; k < wq; k++) before += S.scan[k];
+        for (int k = 0; k < wq; k++) before += SS.scan[k];
         before += x - cnt;
         if (tid < nl) S.lcs[tid] = before;
         if (tid == TILE_TPB - 1) {
@@ -314,40 +449,7 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
     const int n = S.n;
     float mb = 0.0f;
     if (n > TILE_MAXB) {
-        // too crowded for shared memory: the owned beads straight from HBM (rare; same bits)
-        PairConst pk;
-        pk.nk = make_noise_key(R, step);
-        for (int c = 1; c <= td.w; c++) {
-            const int gx = td.cx0 + c - 1, g0 = cs[gx * ncy + td.cy0], g1 = cs[gx * ncy + td.cy0 + td.h];
-            for (int base = g0; base < g1; base += TILE_TPB) {
-                const int g = base + tid;
-                const bool act = g < g1;
-                uint32_t key = 0;
-                if (act) {
-                    PairCtx pc;
-                    pc.pos = b.pos[cur];
-                    pc.vt = b.vt[cur];
-                    pc.tg = b.tg[cur];
-                    pc.pi = pc.pos[g];
-                    pc.vi = pc.vt[g];
-                    const uint32_t tgi = pc.tg[g];
-                    pc.gi = tgi & GID_MASK;
-                    pc.arow = S.a + (tgi >> TYPE_SHIFT) * DPD_MAXT;
-                    pc.nk = pk.nk;
-                    pc.L = R.L;
-                    pc.h = R.halfL;
-                    pc.gam = R.gamma;
-                    pc.sdt = sdt_at(R, step);
-                    long long ax = 0, ay = 0;
-                    bead_pairs_direct(pc, R, cs, g, ax, ay);
-                    finish_bead<NEXTKEY>(b, cur, R, td.rep, g, pc.pi, ax, ay, mb, key);
-                }
-                if (NEXTKEY) {
-                    count_key(b.count, key, act);
-                    if (act) b.key[g] = key;
-                }
-            }
-        }
+        tile_direct<NEXTKEY>(b, cur, R, td, S.a, step, mb);
     } else {
         // per local cell: its beads' cell and image code
         if (tid < nl)
@@ -366,79 +468,351 @@ __global__ void __launch_bounds__(TILE_TPB) k_forces_tile(Bufs b, int cur, const
             S.accx[k] = 0;
             S.accy[k] = 0;
         }
-        if (tid == 0) S.next_chunk = TILE_WARPS;  // chunks 0..7 go to warps 0..7 first
+        if (tid == 0) SS.next_chunk = TILE_WARPS;  // chunks 0..7 go to warps 0..7 first
         __syncthreads();
-        // ---- screened pairs, evaluated on full warps
-        PairConst pc;
-        pc.nk = make_noise_key(R, step);
-        pc.L = R.L;
-        pc.gam = R.gamma;
-        pc.sdt = sdt_at(R, step);
-        const bool wrap = td.cx0 == 0 || td.cy0 == 0 || td.cx0 + td.w >= ncx || td.cy0 + td.h >= ncy;
-        if (R.noise == 1) {
-            if (wrap) tile_pairs<true, 1>(S, pc, LW, LH, td.w, td.h, b.status);
-            else tile_pairs<false, 1>(S, pc, LW, LH, td.w, td.h, b.status);
-        } else {
-            if (wrap) tile_pairs<true, 0>(S, pc, LW, LH, td.w, td.h, b.status);
-            else tile_pairs<false, 0>(S, pc, LW, LH, td.w, td.h, b.status);
+        tile_pairs_any(S, SS.q[wq], &SS.next_chunk, wq, R, td, step, b.status);
+        __syncthreads();
+        tile_epilogue<NEXTKEY>(b, cur, R, td, S, mb);
+    }
+    max_bond_out(b, td.rep, mb);
+}
+
+// ---------------------------------------------------------------- the bulk-staged kernel
+//
+// k_forces_bulk computes the same sums as k_forces_tile, one CTA per tile, but
+// stages the tile's beads with bulk asynchronous copies (cp.async.bulk, global
+// -> shared, completion counted on an mbarrier) instead of per-bead loads and
+// stores.  Cells are column-major, so a local column of the tile and its halo
+// is one contiguous slot range (two where the rows wrap around the box): warp
+// 0 issues one bulk copy per array and range as soon as it has the ranges'
+// ends, while the other threads load the per-cell starts.  A bulk copy moves
+// 16-byte aligned blocks, so each range is widened to a multiple of 4 slots;
+// the extra slots are padding, marked with TILE_PAD and placed far away, so
+// that no screen ever hits them.  All copies read this GPU's own memory; no
+// copy uses cluster multicast.  The epilogue takes a bond partner's position
+// from shared memory when the partner is staged (almost always: bonds are
+// shorter than a cell), else from HBM.
+//
+// The wait on the mbarrier is bounded (STAGE_WAIT_NS of global time); a CTA
+// that gives up raises DPD_F_WAIT (the call returns DPD_E_TIMEOUT), waits once
+// more, bounded, for its copies, and returns.
+
+#define STAGE_MAXP 64                 // column ranges of one tile (w + 2 <= 32 columns, at most 2 ranges each)
+#define STAGE_MAXLW 32
+#define STAGE_WAIT_NS 200000000ull    // 0.2 s
+#define STAGE_FAR 1.0e18f             // padding slots sit here: no distance to them is below the cutoff
+
+struct StagePiece {                   // one contiguous slot range of a local column, staged by bulk copies
+    int32_t a4, n4;                   // first global slot copied (a multiple of 4), slots copied (a multiple of 4)
+    int32_t sm;                       // local slot of a4
+    int32_t lo, hi;                   // the tile's beads in the range: global slots [lo, hi)
+};
+
+struct BulkSmem {
+    TileBead t;
+    StagePiece pc[STAGE_MAXP];
+    int32_t np;                       // ranges of the tile
+    int8_t colp[STAGE_MAXLW];         // first range of each local column
+    int8_t split[STAGE_MAXLW];        // local rows in that first range (the rest are in the next)
+    uint32_t q[TILE_WARPS][TILE_QCAP];
+    int32_t next_chunk;
+    int32_t fail;
+    unsigned long long mbar;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *m, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *m, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *m, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(m)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait for the phase of parity `parity` of m to complete, at most STAGE_WAIT_NS
+__device__ __forceinline__ bool mbar_wait(unsigned long long *m, unsigned parity) {
+    if (mbar_try_wait(m, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(m, parity))
+        if (global_ns() - t0 > STAGE_WAIT_NS) return false;
+    return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *m) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(m))
+                 : "memory");
+}
+
+// Warp 0: the tile's column ranges, their local slots and the bulk copies of
+// the bead data (none if the tile does not fit: T.n > TILE_MAXB)
+__device__ void stage_ranges(BulkSmem &S, const TileDesc &td, const Bufs &b, int cur, const RepDev &R) {
+    const int lane = (int)lane_id();
+    TileBead &T = S.t;
+    const int ncx = R.ncx, ncy = R.ncy, LW = td.w + 2, LH = td.h + 2;
+    const int32_t *__restrict__ cs = b.cstart + R.c0;
+    // lane = local column; its rows cy0 - 1 .. cy0 + h wrap at most once (h + 2 <= ncy)
+    int nr = 0, sp = LH;
+    StagePiece p0 = {0, 0, 0, 0, 0}, p1 = {0, 0, 0, 0, 0};
+    if (lane < LW) {
+        int gx = td.cx0 - 1 + lane;
+        gx = gx < 0 ? gx + ncx : (gx >= ncx ? gx - ncx : gx);
+        const int gy0 = td.cy0 - 1, col = gx * ncy;
+        if (gy0 < 0) sp = 1;                       // row ncy - 1, then rows 0 .. h
+        else if (gy0 + LH > ncy) sp = ncy - gy0;   // rows gy0 .. ncy - 1, then row 0 ..
+        const int ya = gy0 < 0 ? ncy - 1 : gy0;
+        p0.lo = cs[col + ya];
+        p0.hi = cs[col + ya + sp];
+        nr = 1;
+        if (sp < LH) {
+            p1.lo = cs[col];
+            p1.hi = cs[col + LH - sp];
+            nr = 2;
         }
-        __syncthreads();
-        // ---- epilogue over the local index range of the owned columns; halo beads
-        // (rows 0 and h + 1) in that range are skipped.  Loads of a round first.
-        const int e0 = S.lcs[LH + 1], e1 = S.lcs[td.w * LH + td.h + 1];
-        const float2 *__restrict__ gpos = b.pos[cur];
-        for (int base = e0; base < e1; base += EPI_ITEMS * TILE_TPB) {
-            int gg[EPI_ITEMS];
-            bool own[EPI_ITEMS];
+    }
+    int slots = 0;
+    StagePiece *pp[2] = {&p0, &p1};
 #pragma unroll
-            for (int j = 0; j < EPI_ITEMS; j++) {
-                const int k = base + j * TILE_TPB + tid;
-                own[j] = false;
-                gg[j] = 0;
-                if (k < e1) {
-                    const int v = S.lxy[k], ly = v & 255, l = (v >> 8) * LH + ly;
-                    own[j] = ly >= 1 && ly <= td.h;
-                    gg[j] = S.gst[l] + (k - S.lcs[l]);
+    for (int k = 0; k < 2; k++) {
+        StagePiece &q = *pp[k];
+        const bool any = k < nr && q.hi > q.lo;
+        q.a4 = any ? q.lo & ~3 : q.lo;  // an empty range copies nothing; its cells start at its local slot
+        q.n4 = any ? ((q.hi + 3) & ~3) - q.a4 : 0;
+        slots += q.n4;
+    }
+    // local slot of each range and index of each column's first range: exclusive warp scans
+    int x = slots, y = nr;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, x, o), v = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) {
+            x += u;
+            y += v;
+        }
+    }
+    const int total = __shfl_sync(0xffffffffu, x, 31), np = __shfl_sync(0xffffffffu, y, 31);
+    p0.sm = x - slots;
+    p1.sm = p0.sm + p0.n4;
+    const int pidx = y - nr;
+    if (lane < LW) {
+        S.pc[pidx] = p0;
+        if (nr == 2) S.pc[pidx + 1] = p1;
+        S.colp[lane] = (int8_t)pidx;
+        S.split[lane] = (int8_t)sp;
+    }
+    if (lane == 0) {
+        S.np = np;
+        T.n = total;
+    }
+    const bool fits = total <= TILE_MAXB;
+    __syncwarp();
+    if (lane == 0) mbar_arrive_tx(&S.mbar, fits ? (unsigned)total * 20u : 0u);
+    __syncwarp();
+    if (fits && lane < LW) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const StagePiece &q = *pp[k];
+            if (k >= nr || q.n4 == 0) continue;
+            bulk_g2s(&T.pos[q.sm], b.pos[cur] + q.a4, (unsigned)q.n4 * 8u, &S.mbar);
+            bulk_g2s(&T.vt[q.sm], b.vt[cur] + q.a4, (unsigned)q.n4 * 8u, &S.mbar);
+            bulk_g2s(&T.tg[q.sm], b.tg[cur] + q.a4, (unsigned)q.n4 * 4u, &S.mbar);
+        }
+    }
+}
+
+// local slot of a staged bead of column lx - 1 .. lx + 1 from its global slot g (-1: not staged)
+__device__ __forceinline__ int staged_slot(const BulkSmem &S, int lx, int LW, int LH, int g) {
+    for (int c = max(lx - 1, 0); c <= min(lx + 1, LW - 1); c++) {
+        const int k0 = S.colp[c], nk = S.split[c] < LH ? 2 : 1;
+        for (int k = k0; k < k0 + nk; k++) {
+            const StagePiece &q = S.pc[k];
+            if (g >= q.lo && g < q.hi) return q.sm + (g - q.a4);
+        }
+    }
+    return -1;
+}
+
+// the epilogue of a bulk-staged tile: tile_epilogue with the bond partners'
+// positions taken from shared memory where staged
+template <bool NEXTKEY>
+__device__ __forceinline__ void bulk_epilogue(const Bufs &b, int cur, const RepDev &R, const TileDesc &td,
+                                              const BulkSmem &S, float &mb) {
+    const TileBead &T = S.t;
+    const int LH = td.h + 2, LW = td.w + 2, tid = (int)threadIdx.x;
+    const int e0 = T.lcs[LH + 1], e1 = T.lcs[td.w * LH + td.h + 1];
+    const float2 *__restrict__ gpos = b.pos[cur];
+    for (int base = e0; base < e1; base += EPI_ITEMS * blockDim.x) {
+        int gg[EPI_ITEMS], lx[EPI_ITEMS];
+        bool own[EPI_ITEMS];
+#pragma unroll
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            const int k = base + j * (int)blockDim.x + tid;
+            own[j] = false;
+            gg[j] = 0;
+            lx[j] = 0;
+            if (k < e1) {
+                const int v = T.lxy[k], ly = v & 255, l = (v >> 8) * LH + ly;
+                own[j] = v != (int)TILE_PAD && ly >= 1 && ly <= td.h;
+                if (own[j]) {
+                    gg[j] = T.gst[l] + (k - T.lcs[l]);
+                    lx[j] = v >> 8;
                 }
             }
-            int2 lk[EPI_ITEMS];
-            float2 vv[EPI_ITEMS];
+        }
+        int2 lk[EPI_ITEMS];
+        float2 vv[EPI_ITEMS];
 #pragma unroll
-            for (int j = 0; j < EPI_ITEMS; j++) {
-                lk[j] = own[j] ? b.link[cur][gg[j]] : make_int2(-1, -1);
-                vv[j] = (NEXTKEY && own[j]) ? b.vh[cur][gg[j]] : make_float2(0.0f, 0.0f);
-            }
-            float2 pj[EPI_ITEMS][2];
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            lk[j] = own[j] ? b.link[cur][gg[j]] : make_int2(-1, -1);
+            vv[j] = (NEXTKEY && own[j]) ? b.vh[cur][gg[j]] : make_float2(0.0f, 0.0f);
+        }
+        float2 pj[EPI_ITEMS][2];
 #pragma unroll
-            for (int j = 0; j < EPI_ITEMS; j++) {
-                pj[j][0] = lk[j].x >= 0 ? gpos[lk[j].x] : make_float2(0.0f, 0.0f);
-                pj[j][1] = lk[j].y >= 0 ? gpos[lk[j].y] : make_float2(0.0f, 0.0f);
-            }
+        for (int j = 0; j < EPI_ITEMS; j++)
 #pragma unroll
-            for (int j = 0; j < EPI_ITEMS; j++) {
-                const int k = base + j * TILE_TPB + tid;
-                uint32_t key = 0;
-                if (own[j])
-                    finish_loaded<NEXTKEY>(b, cur, R, td.rep, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j],
-                                           vv[j], mb, key);
-                if (NEXTKEY) {
-                    count_key(b.count, key, own[j]);
-                    if (own[j]) b.key[gg[j]] = key;
+            for (int e = 0; e < 2; e++) {
+                const int g = e ? lk[j].y : lk[j].x;
+                pj[j][e] = make_float2(0.0f, 0.0f);
+                if (g >= 0) {
+                    const int ks = staged_slot(S, lx[j], LW, LH, g);
+                    pj[j][e] = ks >= 0 ? T.pos[ks] : gpos[g];
                 }
+            }
+#pragma unroll
+        for (int j = 0; j < EPI_ITEMS; j++) {
+            const int k = base + j * (int)blockDim.x + tid;
+            uint32_t key = 0;
+            if (own[j])
+                finish_loaded<NEXTKEY>(b, cur, R, td.rep, gg[j], T.pos[k], T.accx[k], T.accy[k], lk[j], pj[j], vv[j],
+                                       mb, key);
+            if (NEXTKEY) {
+                count_key(b.count, key, own[j]);
+                if (own[j]) b.key[gg[j]] = key;
             }
         }
     }
-    const unsigned mbb = __reduce_max_sync(0xffffffffu, __float_as_uint(mb));
-    if (lane == 0 && mbb != 0u) atomicMax(b.obs + (size_t)td.rep * OBS_N + 4, (unsigned long long)mbb);
+}
+
+template <bool NEXTKEY>
+__global__ void __launch_bounds__(TILE_TPB) k_forces_bulk(Bufs b, int cur, const RepDev *__restrict__ reps,
+                                                          const TileDesc *__restrict__ tiles) {
+    pdl_begin();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    BulkSmem &S = *reinterpret_cast<BulkSmem *>(smem_raw);
+    TileBead &T = S.t;
+    const int tid = (int)threadIdx.x, wq = tid >> 5;
+    const TileDesc td = tiles[blockIdx.x];
+    const RepDev &R = reps[td.rep];
+    const int ncx = R.ncx, ncy = R.ncy, LH = td.h + 2, nl = (td.w + 2) * LH;
+    const int32_t *__restrict__ cs = b.cstart + R.c0;
+    const long long step = *b.step;
+    if (tid == 0) {
+        mbar_init(&S.mbar, 1);
+        S.fail = 0;
+        S.next_chunk = TILE_WARPS;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (tid < DPD_MAXT * DPD_MAXT) T.a[tid] = a_at(R, tid, step);
+    // every thread of a local cell loads its cell starts while warp 0 starts the copies
+    int lx = 0, ly = 0, code = 0, s0 = 0, s1 = 0;
+    if (tid < nl) {
+        lx = tid / LH;
+        ly = tid - lx * LH;
+        int gx = td.cx0 - 1 + lx, gy = td.cy0 - 1 + ly;
+        const int ix = gx < 0 ? -1 : (gx >= ncx ? 1 : 0), iy = gy < 0 ? -1 : (gy >= ncy ? 1 : 0);
+        gx -= ix * ncx;
+        gy -= iy * ncy;
+        code = (ix + 1) | ((iy + 1) << 2);
+        const int gc = gx * ncy + gy;
+        s0 = cs[gc];
+        s1 = cs[gc + 1];
+    }
+    __syncthreads();  // the mbarrier is initialised
+    if (wq == 0) stage_ranges(S, td, b, cur, R);
+    __syncthreads();  // ranges known
+    const bool fits = T.n <= TILE_MAXB;
+    if (tid < nl) {
+        const StagePiece &q = S.pc[S.colp[lx] + (ly < S.split[lx] ? 0 : 1)];
+        const int k0 = q.sm + (s0 - q.a4);
+        T.lcs[tid] = k0;
+        T.gst[tid] = s0;
+        if (fits)
+            for (int k = k0; k < k0 + (s1 - s0); k++) {
+                T.lxy[k] = (uint16_t)((lx << 8) | ly);
+                T.img[k] = (uint8_t)code;
+            }
+    }
+    if (tid == 0) T.lcs[nl] = T.n;
+    if (fits)
+        for (int k = tid; k < S.np; k += blockDim.x) {  // padding slots: no bead
+            const StagePiece q = S.pc[k];
+            for (int j = q.sm; j < q.sm + (q.lo - q.a4); j++) T.lxy[j] = (uint16_t)TILE_PAD;
+            for (int j = q.sm + (q.hi - q.a4); j < q.sm + q.n4; j++) T.lxy[j] = (uint16_t)TILE_PAD;
+        }
+    // the staged beads
+    if (!mbar_wait(&S.mbar, 0u)) S.fail = 1;
+    if (fits) {
+        for (int k = tid; k < S.np; k += blockDim.x) {  // padding slots sit far away
+            const StagePiece q = S.pc[k];
+            for (int j = q.sm; j < q.sm + (q.lo - q.a4); j++) T.pos[j] = make_float2(STAGE_FAR, STAGE_FAR);
+            for (int j = q.sm + (q.hi - q.a4); j < q.sm + q.n4; j++) T.pos[j] = make_float2(STAGE_FAR, STAGE_FAR);
+        }
+        for (int k = tid; k < T.n; k += blockDim.x) {
+            T.accx[k] = 0;
+            T.accy[k] = 0;
+        }
+    }
+    __syncthreads();
+    if (S.fail) {
+        // a copy never completed: report it, wait once more (bounded) so that none is
+        // still writing when the CTA ends, and return
+        if (tid == 0) raise_flag(b.status, DPD_F_WAIT);
+        mbar_wait(&S.mbar, 0u);
+        return;
+    }
+    float mb = 0.0f;
+    if (fits) {
+        tile_pairs_any(T, S.q[wq], &S.next_chunk, wq, R, td, step, b.status);
+        __syncthreads();
+        bulk_epilogue<NEXTKEY>(b, cur, R, td, S, mb);
+    } else {
+        tile_direct<NEXTKEY>(b, cur, R, td, T.a, step, mb);
+    }
+    max_bond_out(b, td.rep, mb);
 }
 
 size_t tile_smem_bytes() { return sizeof(TileSmem); }
+size_t bulk_smem_bytes() { return sizeof(BulkSmem); }
 
 int tile_setup() {
-    const size_t bytes = sizeof(TileSmem);
+    const size_t bytes = sizeof(TileSmem), bbytes = sizeof(BulkSmem);
     cudaError_t e = cudaFuncSetAttribute(k_forces_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_forces_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_forces_bulk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bbytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_forces_bulk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bbytes);
     return e == cudaSuccess ? 0 : -1;
 }
 
@@ -447,4 +821,11 @@ void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDes
     const size_t bytes = sizeof(TileSmem);
     if (next_keys) launch_pdl(k_forces_tile<true>, ntiles, TILE_TPB, bytes, s, b, cur, rep, tiles);
     else k_forces_tile<false><<<ntiles, TILE_TPB, bytes, s>>>(b, cur, rep, tiles);
+}
+
+void launch_forces_bulk(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
+                        bool next_keys, cudaStream_t s) {
+    const size_t bytes = sizeof(BulkSmem);
+    if (next_keys) launch_pdl(k_forces_bulk<true>, ntiles, TILE_TPB, bytes, s, b, cur, rep, tiles);
+    else k_forces_bulk<false><<<ntiles, TILE_TPB, bytes, s>>>(b, cur, rep, tiles);
 }

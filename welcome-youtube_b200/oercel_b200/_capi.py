@@ -66,7 +66,7 @@ class DpdTemplate(C.Structure):
 
 class DpdTuning(C.Structure):
     _fields_ = [("force_kernel", C.c_int32), ("tile_w", C.c_int32), ("tile_h", C.c_int32),
-                ("graph_steps", C.c_int32)]
+                ("graph_steps", C.c_int32), ("sort_mode", C.c_int32)]
 
 
 class DpdRdfSpec(C.Structure):
@@ -98,7 +98,8 @@ EXPORTS = [
     "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events",
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
-    "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_force_vjp",
+    "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_window_adjoint_state",
+    "dpd_force_vjp",
     "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters", "dpd_xoshiro_jump",
     "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode", "dpd_stats_ring", "dpd_cells_default",
     "dpd_cells_detect",
@@ -174,6 +175,7 @@ def load(path: str | None = None):
         "dpd_set_params": ([vp, i32, C.POINTER(DpdParams)], C.c_int),
         "dpd_window_loss": ([vp, i64, C.POINTER(DpdRdfSpec), fp, fp, fp], C.c_int),
         "dpd_window_adjoint": ([vp, i64, i32, C.POINTER(DpdRdfSpec), fp, fp, fp, fp], C.c_int),
+        "dpd_window_adjoint_state": ([vp, i64, i32, C.POINTER(DpdRdfSpec), fp, fp, fp, fp, fp, fp, fp], C.c_int),
         "dpd_force_vjp": ([vp, i32, i64, fp, fp, fp, fp, fp, fp, fp], C.c_int),
         "dpd_pair_hist": ([vp, i32, i32, i32, dbl, i32, fp], C.c_int),
         "dpd_get_stream": ([vp, C.POINTER(vp)], C.c_int),

@@ -1,9 +1,10 @@
 """Autotuner of the launch choices of an Engine.
 
 The knobs are those of dpd_tuning (include/dpd.h): which force kernel runs
-(cell tiles in shared memory, one pair evaluation per pair; or one thread per
-bead over its 3x3 cells), the tile shape in cells, and the steps per captured
-CUDA graph.  Every candidate is timed on the live engine with real steps
+(cell tiles in shared memory, one pair evaluation per pair, staged by per-bead
+loads or by bulk asynchronous copies; or one thread per bead over its 3x3
+cells), the tile shape in cells, and the
+steps per captured CUDA graph.  Every candidate is timed on the live engine with real steps
 (dpd_profile_step: CUDA events around each kernel of one step), so tuning
 advances the simulation by a few steps; do it during equilibration.  Results
 are cached per system shape in a JSON file.
@@ -23,7 +24,15 @@ FORCE_CANDIDATES = [
     dict(force_kernel=0, tile_w=10, tile_h=18),
     dict(force_kernel=0, tile_w=4, tile_h=8),
     dict(force_kernel=0, tile_w=2, tile_h=4),
+    dict(force_kernel=2, tile_w=14, tile_h=14),
+    dict(force_kernel=2, tile_w=8, tile_h=16),
+    dict(force_kernel=2, tile_w=6, tile_h=30),
+    dict(force_kernel=2, tile_w=10, tile_h=18),
+    dict(force_kernel=2, tile_w=4, tile_h=8),
 ]
+
+# the exclusive scan of the cell counts: 0 two passes, 1 one pass with decoupled look-back
+SORT_CANDIDATES = [0, 1]
 
 
 def _key(engine):
@@ -60,7 +69,19 @@ def autotune(engine, repeats=3, candidates=None, cache_path=None, use_cache=True
         if best is None or ms < best[1]:
             best = (cand, ms)
     engine.set_tuning(**best[0])
-    out = {"tuning": engine.tuning(), "forces_ms": best[1], "timings": timings}
+    # the scan of the cell counts: two passes or one pass with look-back (the
+    # first four kernel times of a step: scan1, scan2, place, cellfix)
+    sort_best, sort_timings = None, []
+    for mode in SORT_CANDIDATES:
+        engine.set_tuning(sort_mode=mode)
+        engine.profile_step()
+        ms = float(np.median([sum(engine.profile_step()[:4]) for _ in range(repeats)]))
+        sort_timings.append(dict(sort_mode=mode, sort_ms=ms))
+        if sort_best is None or ms < sort_best[1]:
+            sort_best = (mode, ms)
+    engine.set_tuning(sort_mode=sort_best[0])
+    out = {"tuning": engine.tuning(), "forces_ms": best[1], "timings": timings, "sort_ms": sort_best[1],
+           "sort_timings": sort_timings}
     if use_cache:
         cache[key] = out
         try:

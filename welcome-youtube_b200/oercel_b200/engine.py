@@ -164,12 +164,14 @@ class Engine:
     def tuning(self):
         t = _capi.DpdTuning()
         check(self.lib.dpd_get_tuning(self.h, C.byref(t)))
-        return dict(force_kernel=t.force_kernel, tile_w=t.tile_w, tile_h=t.tile_h, graph_steps=t.graph_steps)
+        return dict(force_kernel=t.force_kernel, tile_w=t.tile_w, tile_h=t.tile_h, graph_steps=t.graph_steps,
+                    sort_mode=t.sort_mode)
 
     def set_tuning(self, **kv):
         cur = self.tuning()
         cur.update(kv)
-        t = _capi.DpdTuning(int(cur["force_kernel"]), int(cur["tile_w"]), int(cur["tile_h"]), int(cur["graph_steps"]))
+        t = _capi.DpdTuning(int(cur["force_kernel"]), int(cur["tile_w"]), int(cur["tile_h"]), int(cur["graph_steps"]),
+                            int(cur["sort_mode"]))
         check(self.lib.dpd_set_tuning(self.h, C.byref(t)))
 
     def profile_step(self):
@@ -329,6 +331,20 @@ class Engine:
         check(self.lib.dpd_window_adjoint(self.h, int(nsteps), int(ckpt_every), C.byref(spec), ptr(tgt), ptr(loss),
                                           ptr(grad), ptr(rdf)))
         return loss, grad, rdf
+
+    def window_adjoint_state(self, nsteps, ckpt_every, spec, target):
+        """window_adjoint plus the cotangents of the start state (horizon 0):
+        (loss, grad, rdf, xbar, vhbar, vtbar), the last three (N_total, 2) in gid
+        order packed by replica (replica r's gid g at row sum(n_beads[:r]) + g)"""
+        tgt = np.ascontiguousarray(np.broadcast_to(target, (self.nrep, spec.nbin)), np.float64)
+        loss = np.zeros(self.nrep)
+        rdf = np.zeros((self.nrep, spec.nbin))
+        grad = np.zeros((self.nrep, _capi.NGRAD))
+        N = int(sum(self.n_beads))
+        st = [np.zeros((N, 2), np.float32) for _ in range(3)]
+        check(self.lib.dpd_window_adjoint_state(self.h, int(nsteps), int(ckpt_every), C.byref(spec), ptr(tgt),
+                                                ptr(loss), ptr(grad), ptr(rdf), *[ptr(a) for a in st]))
+        return loss, grad, rdf, st[0], st[1], st[2]
 
     def force_vjp(self, replica, step, gx, gy):
         n = self.n_beads[replica]
