@@ -94,27 +94,72 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed loop"""
+    """SM clock and throttle reasons sampled during a timed region: NVML read
+    from a background thread as fast as it answers (a timed loop of a few
+    milliseconds still gets many samples), nvidia-smi as the fallback.  The
+    sampler is running before the region starts and stops after it ends."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.p = None
+        self.thread = None
+        self.stop = False
+        self.samples = []  # (sm MHz, max MHz, set of reason names)
+        self.source = None
+
+    def _nvml_loop(self, nv, h, started):
+        bits = {"hw_slowdown": nv.nvmlClocksThrottleReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksThrottleReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksThrottleReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksThrottleReasonSwPowerCap}
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.samples.append((float(sm), float(smax), {k for k, b in bits.items() if r & b}))
+            started.set()
+            time.sleep(0.0005)
 
     def __enter__(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            try:  # the CUDA device's own NVML handle, by UUID (NVML numbers every GPU of the machine)
+                import torch
+                u = str(torch.cuda.get_device_properties(self.index).uuid)
+                h = nv.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            except Exception:
+                h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            started = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, started), daemon=True)
+            self.thread.start()
+            started.wait(5.0)
+            self.source = "nvml"
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi"
         except OSError:
             self.p = None
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        self.stop = True
+        if self.thread is not None:
+            self.thread.join(timeout=5)
         if self.p:
             self.p.terminate()
             try:
@@ -122,27 +167,23 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.p.kill()
                 out, _ = self.p.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            for l in out.splitlines():
+                f = [x.strip() for x in l.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.samples.append((float(f[1]), float(f[2]),
+                                         {n for n, v in zip(self.NAMES, f[5:9]) if v.lower().startswith("active")}))
+                except ValueError:
+                    continue
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": self.source}
+        sm = sorted(s[0] for s in self.samples)
+        reasons = set().union(*[s[2] for s in self.samples])
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.samples[-1][1], "reasons": sorted(reasons),
+                "samples": len(sm), "source": self.source}
 
 
 def reference_binary():

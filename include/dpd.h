@@ -172,9 +172,12 @@ typedef struct dpd_handle dpd_handle;
  * evaluated by both beads; 2: the cell tiles of 0 staged into shared memory
  * by bulk asynchronous copies, one per tile column (tile_w <= 30).  All give
  * bit-identical forces.
- * graph_steps: steps per captured CUDA graph.  sort_mode: the exclusive scan
- * of the cell counts in two passes (0) or in one pass with decoupled
- * look-back between blocks (1); the same cell starts. */
+ * graph_steps: steps per captured CUDA graph.  sort_mode: the cell sort's
+ * exclusive scan of the cell counts in two passes (0), in one pass with
+ * decoupled look-back between blocks (1), or as a block-local pass whose
+ * block prefixes the placement and fix-up kernels add themselves (2: one
+ * kernel fewer; boxes of up to 4,194,304 cells, else as 0); the same cell
+ * starts and order. */
 typedef struct {
     int32_t force_kernel;
     int32_t tile_w, tile_h;   /* (tile_w + 2) * (tile_h + 2) <= 256 */

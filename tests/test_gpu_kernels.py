@@ -117,12 +117,13 @@ def test_integrate_bit_exact_against_fp32_oracle(cuda_ok):
         assert np.array_equal(after[k], st[k]), k
 
 
-@pytest.mark.parametrize("sort_mode", [0, 1])
+@pytest.mark.parametrize("sort_mode", [0, 1, 2])
 def test_sort_at_one_million_beads(cuda_ok, sort_mode):
     """size-independent properties at the 1M-bead size: the sort is the oracle's
     stable counting sort, bit for bit, and every bead lies in its cell; with
-    the two-pass scan and with the one-pass look-back scan (256 blocks, each
-    waiting on its predecessors)"""
+    the two-pass scan, the one-pass look-back scan (256 blocks, each waiting on
+    its predecessors) and the block-local scan whose prefixes the placement
+    adds"""
     import oercel_b200 as ob
     p = params(L=512, seed=1)
     s = ob.soup_for(p)
@@ -138,21 +139,22 @@ def test_sort_at_one_million_beads(cuda_ok, sort_mode):
 
 
 def test_scan_forms_give_the_same_steps(cuda_ok):
-    """the production step with the two-pass and the one-pass scan: bit-identical
+    """the production step with each form of the sort: bit-identical
     trajectories (with the lipid chemistry), through CUDA graphs of 4 steps"""
     import oercel_b200 as ob
     p = params(L=48, seed=12, noise="philox", chem=1, n_chem=1, p_grow=0.05, p_bond=0.2, p_break=0.01)
     runs = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         e = ob.Engine(p)
         e.set_tuning(sort_mode=mode, graph_steps=4)
         e.load_soup(0)
         e.prime()
         e.step(40)
         runs.append((e.state(), e.cells()))
-    for k in ("x", "y", "vhx", "fx", "type", "gid", "prev", "next"):
-        assert np.array_equal(runs[0][0][k], runs[1][0][k]), k
-    assert np.array_equal(runs[0][1], runs[1][1])
+    for r in runs[1:]:
+        for k in ("x", "y", "vhx", "fx", "type", "gid", "prev", "next"):
+            assert np.array_equal(runs[0][0][k], r[0][k]), k
+        assert np.array_equal(runs[0][1], r[1])
 
 
 def a_eff(a, warmup, warm_end, step):

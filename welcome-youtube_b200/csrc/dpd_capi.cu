@@ -76,7 +76,7 @@ struct dpd_handle {
     int cur = 0;
     // force kernel: 0 = cell tiles in shared memory (half shell), 1 = one thread per bead (full shell)
     int force_kernel = 0;      // 0 cell tiles, 1 thread per bead, 2 cell tiles staged by bulk copies
-    int sort_mode = 0;         // cell-count scan: 0 two passes (k_scan1, k_scan2), 1 one pass (k_scan_lb)
+    int sort_mode = 2;         // 0 two scan passes, 1 one scan pass (k_scan_lb), 2 no second pass (block prefixes in place/cellfix)
     int tile_w = 8, tile_h = 16;
     TileDesc *d_tiles = nullptr;
     int ntiles = 0;
@@ -371,6 +371,17 @@ static int build_tiles(dpd_handle *h) {
 static void enqueue_scan(dpd_handle *h, bool step_inc) {
     if (h->sort_mode == 1) launch_scan_lb(h->b, h->C, step_inc, h->s);
     else launch_scan(h->b, h->C, step_inc, h->s);
+}
+
+// the sort of the counted keys into cell order (cell starts, src, dest)
+static void enqueue_cell_sort(dpd_handle *h, bool step_inc) {
+    if (h->sort_mode == 2 && sort_pfx_fits(h->C)) {
+        launch_sort_pfx(h->b, h->C, step_inc, h->d_bch, h->nbch, h->d_cch, h->ncch, -1, h->s);
+        return;
+    }
+    enqueue_scan(h, step_inc);
+    launch_place(h->b, h->d_bch, h->nbch, h->s);
+    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
 }
 
 static void enqueue_forces(dpd_handle *h, bool next_keys) {
@@ -704,9 +715,7 @@ static void enqueue_sort(dpd_handle *h, PermuteMode mode) {
     // counts of the CURRENT positions
     cudaMemsetAsync(h->b.count, 0, (size_t)(h->C + 4) * sizeof(uint32_t), h->s);
     launch_keys(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, false, h->s);
-    enqueue_scan(h, false);
-    launch_place(h->b, h->d_bch, h->nbch, h->s);
-    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    enqueue_cell_sort(h, false);
     clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, mode, h->s);
     h->cur ^= 1;
@@ -866,9 +875,7 @@ static bool cat_at(const dpd_handle *h, int64_t s) {
 static void enqueue_step(dpd_handle *h, int64_t s) {
     const bool cat = cat_at(h, s);
     if (!cat) {
-        enqueue_scan(h, true);
-        launch_place(h->b, h->d_bch, h->nbch, h->s);
-        launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+        enqueue_cell_sort(h, true);
     } else {
         launch_step_begin(h->b, h->nrep, h->s);
     }
@@ -957,7 +964,7 @@ extern "C" int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t) {
     if (t->force_kernel == 2 && t->tile_w + 2 > 32)
         return fail(DPD_E_ARG, "the bulk-staged force kernel takes tiles of at most 30 columns");
     if (t->graph_steps < 1) return fail(DPD_E_ARG, "graph_steps must be >= 1");
-    if (t->sort_mode < 0 || t->sort_mode > 1) return fail(DPD_E_ARG, "sort_mode must be 0 or 1");
+    if (t->sort_mode < 0 || t->sort_mode > 2) return fail(DPD_E_ARG, "sort_mode must be 0, 1 or 2");
     CK(cudaStreamSynchronize(h->s));
     const int ow = h->tile_w, oh = h->tile_h;
     h->tile_w = t->tile_w;
@@ -996,7 +1003,8 @@ extern "C" int dpd_set_graph_steps(dpd_handle *h, int32_t steps) {
 
 // One step launched kernel by kernel with CUDA events between the launches on
 // the handle's stream; ms[k] = device time of kernel k (scan1 (the whole scan
-// with sort_mode 1), scan2 (0 ms with sort_mode 1), place, cellfix, permute, [2 chemistry], [catalyst check + its sort], forces).  The
+// with sort_mode 1, the block-local scan with 2), scan2 (0 ms with sort_mode 1
+// and 2), place, cellfix, permute, [2 chemistry], [catalyst check + its sort], forces).  The
 // step is a real step; on a step with a catalyst check the first entry is the
 // step counter's kernel, the next three are not launched (0 ms) and the
 // permute keeps the slot order.
@@ -1010,8 +1018,10 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     for (auto &e : ev) CK(cudaEventCreate(&e));
     int k = 0;
     CK(cudaEventRecord(ev[k++], h->s));
+    const bool pfx = h->sort_mode == 2 && sort_pfx_fits(h->C);
     if (!cat) {
-        if (h->sort_mode == 1) launch_scan_lb(h->b, h->C, true, h->s);
+        if (pfx) launch_sort_pfx(h->b, h->C, true, h->d_bch, h->nbch, h->d_cch, h->ncch, 0, h->s);
+        else if (h->sort_mode == 1) launch_scan_lb(h->b, h->C, true, h->s);
         else launch_scan_part(h->b, h->C, true, 1, h->s);
     } else {
         launch_step_begin(h->b, h->nrep, h->s);
@@ -1019,9 +1029,15 @@ extern "C" int dpd_profile_step(dpd_handle *h, float *ms, int32_t cap, int32_t *
     CK(cudaEventRecord(ev[k++], h->s));
     if (!cat && h->sort_mode == 0) launch_scan_part(h->b, h->C, true, 2, h->s);
     CK(cudaEventRecord(ev[k++], h->s));
-    if (!cat) launch_place(h->b, h->d_bch, h->nbch, h->s);
+    if (!cat) {
+        if (pfx) launch_sort_pfx(h->b, h->C, true, h->d_bch, h->nbch, h->d_cch, h->ncch, 1, h->s);
+        else launch_place(h->b, h->d_bch, h->nbch, h->s);
+    }
     CK(cudaEventRecord(ev[k++], h->s));
-    if (!cat) launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    if (!cat) {
+        if (pfx) launch_sort_pfx(h->b, h->C, true, h->d_bch, h->nbch, h->d_cch, h->ncch, 2, h->s);
+        else launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    }
     CK(cudaEventRecord(ev[k++], h->s));
     clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, cat ? PERM_KEEP : PERM_STEP, h->s);
@@ -1420,9 +1436,7 @@ static StateView view_cur(dpd_handle *h) {
 }
 
 static void enqueue_plain_step(dpd_handle *h) {  // one step without chemistry (windows require chem off)
-    enqueue_scan(h, true);
-    launch_place(h->b, h->d_bch, h->nbch, h->s);
-    launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
+    enqueue_cell_sort(h, true);
     clear_stir(h);
     launch_permute(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, PERM_STEP, h->s);
     h->cur ^= 1;

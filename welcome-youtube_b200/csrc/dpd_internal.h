@@ -224,6 +224,11 @@ void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s);
 void launch_scan_part(const Bufs &b, int64_t C, bool step_inc, int part, cudaStream_t s);
 // the same exclusive scan in one pass (decoupled look-back between blocks)
 void launch_scan_lb(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s);
+// the sort of a step in three kernels (block-local scan, placement and fix-up
+// adding the block prefixes themselves); part 0..2 or all with part < 0
+bool sort_pfx_fits(int64_t C);
+void launch_sort_pfx(const Bufs &b, int64_t C, bool step_inc, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
+                     int part, cudaStream_t s);
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s);
 void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,

@@ -73,6 +73,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *total) {
 }
 
 // block-local exclusive scan; counts are consumed and zeroed for the next step
+// ZERO: the counts are consumed and zeroed here; without it they stay for
+// k_place<true>, which consumes them as its placement cursors.
+template <bool ZERO>
 __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count, int32_t *__restrict__ cstart,
                                                     int32_t *__restrict__ bsum, long long C,
                                                     long long *__restrict__ step, int step_inc,
@@ -88,12 +91,12 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan1(uint32_t *__restrict__ count
         v[1] = (int)q.y;
         v[2] = (int)q.z;
         v[3] = (int)q.w;
-        *reinterpret_cast<uint4 *>(count + base) = make_uint4(0u, 0u, 0u, 0u);
+        if (ZERO) *reinterpret_cast<uint4 *>(count + base) = make_uint4(0u, 0u, 0u, 0u);
     } else {
 #pragma unroll
         for (int k = 0; k < SCAN_PER_THREAD; k++) {
             v[k] = base + k < C ? (int)count[base + k] : 0;
-            if (base + k < C) count[base + k] = 0u;
+            if (ZERO && base + k < C) count[base + k] = 0u;
         }
     }
 #pragma unroll
@@ -294,11 +297,38 @@ __global__ void __launch_bounds__(SCAN_TPB) k_scan_lb(uint32_t *__restrict__ cou
 #define PLACE_ITEMS 4
 #endif
 
+// The sort without the second scan pass (sort_mode 2): k_scan1<false> leaves
+// each cell's start within its scan block in `fill` and the counts in place;
+// k_place<true> and k_cellfix<true> add the block prefixes themselves (every
+// CTA scans the block totals into shared memory), k_place<true> takes the
+// places by counting each cell's count down to zero (so the counts are clear
+// for the next step's force epilogue), and k_cellfix<true> writes the final
+// cell starts.
+#define PFX_MAX 4096  // scan blocks whose prefixes a CTA holds: C <= 4,194,304 cells
+
+// exclusive prefix of the scan's block totals, into shared memory (blockDim = SCAN_TPB)
+__device__ __forceinline__ void block_prefixes(const int32_t *__restrict__ bsum, int nb, int *pfx) {
+    const int per = (nb + SCAN_TPB - 1) / SCAN_TPB;
+    const int lo = (int)threadIdx.x * per, hi = min(lo + per, nb);
+    int s = 0;
+    for (int k = lo; k < hi; k++) s += bsum[k];
+    int total;
+    int ex = block_exclusive_scan(s, &total);
+    for (int k = lo; k < hi; k++) {
+        pfx[k] = ex;
+        ex += bsum[k];
+    }
+    __syncthreads();
+}
+
 // PLACE_ITEMS chunks per CTA: all keys are loaded before the first atomic
+template <bool PFX>
 __global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restrict__ ch, int nch,
-                                                    const int32_t *__restrict__ gate) {
+                                                    const int32_t *__restrict__ gate, int nb) {
     pdl_begin();
     if (gate && !*gate) return;
+    __shared__ int pfx[PFX ? PFX_MAX : 1];
+    if (PFX) block_prefixes(b.bsum, nb, pfx);
     const unsigned lane = lane_id();
     uint32_t key[PLACE_ITEMS];
     int idx[PLACE_ITEMS];
@@ -319,7 +349,14 @@ __global__ void __launch_bounds__(BEAD_TPB) k_place(Bufs b, const Chunk *__restr
         const unsigned grp = __match_any_sync(0xffffffffu, key[k]);
         const int leader = __ffs(grp) - 1;
         uint32_t base = 0;
-        if (act && (int)lane == leader) base = atomicAdd(b.fill + key[k], (unsigned)__popc(grp));
+        if (act && (int)lane == leader) {
+            if (PFX) {
+                const unsigned n = (unsigned)__popc(grp), left = atomicSub(b.count + key[k], n);
+                base = b.fill[key[k]] + (uint32_t)pfx[key[k] / SCAN_PER_BLOCK] + left - n;
+            } else {
+                base = atomicAdd(b.fill + key[k], (unsigned)__popc(grp));
+            }
+        }
         base = __shfl_sync(0xffffffffu, base, leader);
         if (act) b.src[base + __popc(grp & ((1u << lane) - 1u))] = idx[k];
     }
@@ -366,8 +403,7 @@ __device__ __forceinline__ void fix_cell(int32_t *__restrict__ src, int32_t *__r
 // Beads that land in one cell keep their old slot order (the reference's
 // stable counting sort, oercel.c:832-933): the atomics gave each bead some
 // place in its cell; here every cell orders its beads by old slot.
-__device__ __forceinline__ void cellfix_one(const Bufs &b, int cell) {
-    const int s = b.cstart[cell], m = b.cstart[cell + 1] - s;
+__device__ __forceinline__ void cellfix_range(const Bufs &b, int s, int m) {
     if (m <= 1) {
         if (m == 1) b.dest[b.src[s]] = s;
         return;
@@ -394,13 +430,27 @@ __device__ __forceinline__ void cellfix_one(const Bufs &b, int cell) {
     }
 }
 
+template <bool PFX>
 __global__ void __launch_bounds__(CELL_TPB) k_cellfix(Bufs b, const Chunk *__restrict__ ch,
-                                                      const int32_t *__restrict__ gate) {
+                                                      const int32_t *__restrict__ gate, int nb, long long C) {
     pdl_begin();
     if (gate && !*gate) return;
+    __shared__ int pfx[PFX ? PFX_MAX : 1];
+    if (PFX) block_prefixes(b.bsum, nb, pfx);
     const Chunk c = ch[blockIdx.x];
     const int cell = c.begin + (int)threadIdx.x;
-    if (cell < c.end) cellfix_one(b, cell);
+    if (cell >= c.end) return;
+    int s, e;
+    if (PFX) {  // the final cell starts: block-local start + block prefix
+        s = (int)b.fill[cell] + pfx[cell / SCAN_PER_BLOCK];
+        e = cell + 1 < C ? (int)b.fill[cell + 1] + pfx[(cell + 1) / SCAN_PER_BLOCK] : pfx[nb - 1] + b.bsum[nb - 1];
+        b.cstart[cell] = s;
+        if (cell + 1 == C) b.cstart[C] = e;
+    } else {
+        s = b.cstart[cell];
+        e = b.cstart[cell + 1];
+    }
+    cellfix_range(b, s, e - s);
 }
 
 // ---------------------------------------------------------------- permute (+ integrate)
@@ -1009,8 +1059,8 @@ void launch_keys(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, in
 static void scan_part(const Bufs &b, int64_t C, bool step_inc, int part, const int32_t *gate, cudaStream_t s) {
     const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
     if (part == 1)
-        launch_pdl(k_scan1, nb, SCAN_TPB, 0, s, b.count, b.cstart, b.bsum, (long long)C, b.step, step_inc ? 1 : 0,
-                   b.status, gate);
+        launch_pdl(k_scan1<true>, nb, SCAN_TPB, 0, s, b.count, b.cstart, b.bsum, (long long)C, b.step,
+                   step_inc ? 1 : 0, b.status, gate);
     else launch_pdl(k_scan2, nb, SCAN_TPB, 0, s, b.cstart, b.fill, b.bsum, (long long)C, nb, gate);
 }
 
@@ -1030,12 +1080,26 @@ void launch_scan(const Bufs &b, int64_t C, bool step_inc, cudaStream_t s) {
 }
 
 void launch_place(const Bufs &b, const Chunk *bch, int nbch, cudaStream_t s) {
-    launch_pdl(k_place, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch,
-               (const int32_t *)nullptr);
+    launch_pdl(k_place<false>, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch,
+               (const int32_t *)nullptr, 0);
 }
 
 void launch_cellfix(const Bufs &b, const Chunk *cch, int ncch, cudaStream_t s) {
-    launch_pdl(k_cellfix, ncch, CELL_TPB, 0, s, b, cch, (const int32_t *)nullptr);
+    launch_pdl(k_cellfix<false>, ncch, CELL_TPB, 0, s, b, cch, (const int32_t *)nullptr, 0, 0ll);
+}
+
+bool sort_pfx_fits(int64_t C) { return (C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK <= PFX_MAX; }
+
+void launch_sort_pfx(const Bufs &b, int64_t C, bool step_inc, const Chunk *bch, int nbch, const Chunk *cch, int ncch,
+                     int part, cudaStream_t s) {
+    const int nb = (int)((C + SCAN_PER_BLOCK - 1) / SCAN_PER_BLOCK);
+    const int32_t *no = nullptr;
+    if (part < 0 || part == 0)
+        launch_pdl(k_scan1<false>, nb, SCAN_TPB, 0, s, b.count, (int32_t *)b.fill, b.bsum, (long long)C, b.step,
+                   step_inc ? 1 : 0, b.status, no);
+    if (part < 0 || part == 1)
+        launch_pdl(k_place<true>, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch, no, nb);
+    if (part < 0 || part == 2) launch_pdl(k_cellfix<true>, ncch, CELL_TPB, 0, s, b, cch, no, nb, (long long)C);
 }
 
 void launch_permute(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, PermuteMode mode,
@@ -1061,8 +1125,8 @@ void launch_resort(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
     k_keys<false, true><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
     scan_part(b, C, false, 1, gate, s);
     scan_part(b, C, false, 2, gate, s);
-    launch_pdl(k_place, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch, gate);
-    launch_pdl(k_cellfix, ncch, CELL_TPB, 0, s, b, cch, gate);
+    launch_pdl(k_place<false>, (nbch + PLACE_ITEMS - 1) / PLACE_ITEMS, BEAD_TPB, 0, s, b, bch, nbch, gate, 0);
+    launch_pdl(k_cellfix<false>, ncch, CELL_TPB, 0, s, b, cch, gate, 0, 0ll);
     k_permute<PERM_SORT, 1><<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch, nbch, gate);
     k_copy_back<<<nbch, BEAD_TPB, 0, s>>>(b, cur, bch);
 }

@@ -31,8 +31,9 @@ FORCE_CANDIDATES = [
     dict(force_kernel=2, tile_w=4, tile_h=8),
 ]
 
-# the exclusive scan of the cell counts: 0 two passes, 1 one pass with decoupled look-back
-SORT_CANDIDATES = [0, 1]
+# the cell sort: 0 two scan passes, 1 one scan pass with decoupled look-back, 2 a block-local
+# scan whose block prefixes the placement and fix-up kernels add themselves
+SORT_CANDIDATES = [0, 1, 2]
 
 
 def _key(engine):
