@@ -817,7 +817,11 @@ def ours(args, rank, local_rank, ws):
     eng.prime()
     eng.step(max(args.warmup, 3))
     from oercel_b200.autotune import autotune
-    tuned = autotune(eng, use_cache=False)
+    if args.tuning:  # a fixed launch choice (profiler runs: a known sequence of launches)
+        eng.set_tuning(**json.loads(args.tuning))
+        tuned = {"tuning": eng.tuning(), "fixed": True}
+    else:
+        tuned = autotune(eng, use_cache=False)
     eng.set_graph_steps(1)
     eng.step(2)  # capture the one-step graphs of both buffer parities before timing
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -911,6 +915,8 @@ def main():
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--quick", action="store_true", help="timed loop and kernel profile only (for profiler runs)")
+    ap.add_argument("--tuning", default="", help='fixed tuning instead of the autotuner, e.g. \'{"force_kernel": 0, '
+                                              '"tile_w": 10, "tile_h": 18}\'')
     args = ap.parse_args()
     rank, local_rank, ws = dist_init()
     try:

@@ -177,12 +177,15 @@ typedef struct dpd_handle dpd_handle;
  * decoupled look-back between blocks (1), or as a block-local pass whose
  * block prefixes the placement and fix-up kernels add themselves (2: one
  * kernel fewer; boxes of up to 4,194,304 cells, else as 0); the same cell
- * starts and order. */
+ * starts and order.  tile_threads: threads per CTA of force_kernel 0, 256
+ * (four CTAs per SM) or 512 (two per SM, tiles of up to 512 cells with their
+ * halo, so less halo per owned cell). */
 typedef struct {
     int32_t force_kernel;
-    int32_t tile_w, tile_h;   /* (tile_w + 2) * (tile_h + 2) <= 256 */
+    int32_t tile_w, tile_h;   /* (tile_w + 2) * (tile_h + 2) <= 256, or <= tile_threads with force_kernel 0 */
     int32_t graph_steps;
     int32_t sort_mode;
+    int32_t tile_threads;
 } dpd_tuning;
 
 /* message of the last failed call on this thread ("" if none) */

@@ -102,7 +102,11 @@ def test_window_adjoint_matches_finite_differences(cuda_ok):
     s0, step0 = e.state(), e.step_no
     spec = ob.Engine.rdf_spec(ta=2, tb=2, nbin=32, rmax=2.0, sigma=0.1, last_steps=5)
     target = np.linspace(0.5, 1.5, 32)
-    nsteps, ckpt = 12, 5
+    # 6 steps (a checkpoint at 5): over longer windows of this dense box the FP32
+    # trajectories of nearby parameter values part enough that central
+    # differences scatter by about 3e-3 across step sizes (12 steps), which
+    # would hide a 1e-3 error of the adjoint; at 6 steps they agree to 1e-4
+    nsteps, ckpt = 6, 5
     e = _window_engine(base, s0, step0)
     loss, grad, rdf = e.window_adjoint(nsteps, ckpt, spec, target)
     assert loss[0] > 0 and np.all(np.isfinite(grad))
@@ -116,11 +120,14 @@ def test_window_adjoint_matches_finite_differences(cuda_ok):
         pp = params(L=12.0, seed=5, noise="philox", f_lip=0.3, c_N=0.1, **kv)
         return _window_engine(pp, s0, step0).window_loss(nsteps, spec, target)[0][0]
 
-    checks = [("a_W_T", 75.0, 0.5, 0 * 8 + 2), ("a_H_T", 50.0, 0.5, 1 * 8 + 2), ("gamma", 4.5, 0.05, 64),
-              ("k_bond", 100.0, 1.0, 65)]
-    for key, val, h, idx in checks:
+    # central differences with steps of 4 % of each value: the loss is smooth on
+    # that scale, and the step keeps the FP32 rounding of the two runs small
+    # against their difference
+    checks = [("a_W_T", 75.0, 0 * 8 + 2), ("a_H_T", 50.0, 1 * 8 + 2), ("gamma", 4.5, 64), ("k_bond", 100.0, 65)]
+    for key, val, idx in checks:
+        h = 0.04 * val
         fd = (loss_at(**{key: val + h}) - loss_at(**{key: val - h})) / (2 * h)
-        assert grad[0][idx] == pytest.approx(fd, rel=0.05, abs=1e-3 * np.abs(grad[0]).max()), key
+        assert grad[0][idx] == pytest.approx(fd, rel=1e-3, abs=1e-5 * np.abs(grad[0]).max()), key
 
 
 def test_horizon_truncates_the_reverse_pass(cuda_ok):

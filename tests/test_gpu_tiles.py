@@ -125,3 +125,29 @@ def test_bulk_staged_kernel_in_a_batch(cuda_ok):
     for a, b in zip(*runs):
         for k in ("x", "y", "fx", "fy", "type", "prev", "next"):
             assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("L", [9.0, 33.5, 64.0])
+@pytest.mark.parametrize("shape", [(20, 20), (14, 30), (10, 40)])
+def test_wide_tile_forces_equal_bead_forces(cuda_ok, L, shape):
+    """512-thread CTAs with tiles of up to 512 cells (tile and halo): the same
+    bits as the per-bead kernel"""
+    p = params(L=L, seed=int(L * 7), noise="philox")
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(5)
+    e.set_tuning(force_kernel=1)
+    e.forces(321)
+    a = e.state()
+    e.set_tuning(force_kernel=0, tile_w=shape[0], tile_h=shape[1], tile_threads=512)
+    e.forces(321)
+    b = e.state()
+    assert np.array_equal(a["fx"], b["fx"]) and np.array_equal(a["fy"], b["fy"])
+    nc = int(np.floor(np.float32(L)))
+    w, h = min(shape[0], nc - 2), min(shape[1], nc - 2)
+    if (w + 2) * (h + 2) > 256:
+        with pytest.raises(ob.DpdError):
+            e.set_tuning(tile_threads=256)  # a tile of more than 256 cells does not fit 256 threads
+    with pytest.raises(ob.DpdError):
+        e.set_tuning(tile_threads=384)

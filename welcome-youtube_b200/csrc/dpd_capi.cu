@@ -76,7 +76,8 @@ struct dpd_handle {
     int cur = 0;
     // force kernel: 0 = cell tiles in shared memory (half shell), 1 = one thread per bead (full shell)
     int force_kernel = 0;      // 0 cell tiles, 1 thread per bead, 2 cell tiles staged by bulk copies
-    int sort_mode = 2;         // 0 two scan passes, 1 one scan pass (k_scan_lb), 2 no second pass (block prefixes in place/cellfix)
+    int sort_mode = 2;
+    int tile_threads = 256;    // threads per CTA of the tile kernel (256 or 512: tiles of up to that many local cells)         // 0 two scan passes, 1 one scan pass (k_scan_lb), 2 no second pass (block prefixes in place/cellfix)
     int tile_w = 8, tile_h = 16;
     TileDesc *d_tiles = nullptr;
     int ntiles = 0;
@@ -346,8 +347,9 @@ static void free_all(dpd_handle *h) {
 // cell tiles of every replica: w x h cells (narrower boxes get narrower tiles,
 // so that a tile and its halo never hold the same column or row twice)
 static int build_tiles(dpd_handle *h) {
-    if (h->tile_w < 1 || h->tile_h < 1 || (h->tile_w + 2) * (h->tile_h + 2) > 256)
-        return fail(DPD_E_ARG, "tile shape %dx%d: need (w+2)(h+2) <= 256", h->tile_w, h->tile_h);
+    const int maxc = h->force_kernel == 0 ? h->tile_threads : 256;
+    if (h->tile_w < 1 || h->tile_h < 1 || (h->tile_w + 2) * (h->tile_h + 2) > maxc)
+        return fail(DPD_E_ARG, "tile shape %dx%d: need (w+2)(h+2) <= %d", h->tile_w, h->tile_h, maxc);
     std::vector<TileDesc> t;
     for (int r = 0; r < h->nrep; r++) {
         const RepDev &R = h->rh[r];
@@ -386,7 +388,8 @@ static void enqueue_cell_sort(dpd_handle *h, bool step_inc) {
 
 static void enqueue_forces(dpd_handle *h, bool next_keys) {
     if (h->any_mol) launch_mol_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
-    if (h->force_kernel == 0) launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
+    if (h->force_kernel == 0)
+        launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, h->tile_threads, next_keys, h->s);
     else if (h->force_kernel == 2) launch_forces_bulk(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
     else launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, next_keys, h->s);
 }
@@ -965,18 +968,22 @@ extern "C" int dpd_set_tuning(dpd_handle *h, const dpd_tuning *t) {
         return fail(DPD_E_ARG, "the bulk-staged force kernel takes tiles of at most 30 columns");
     if (t->graph_steps < 1) return fail(DPD_E_ARG, "graph_steps must be >= 1");
     if (t->sort_mode < 0 || t->sort_mode > 2) return fail(DPD_E_ARG, "sort_mode must be 0, 1 or 2");
+    if (t->tile_threads != 256 && t->tile_threads != 512) return fail(DPD_E_ARG, "tile_threads must be 256 or 512");
     CK(cudaStreamSynchronize(h->s));
-    const int ow = h->tile_w, oh = h->tile_h;
+    const int ow = h->tile_w, oh = h->tile_h, ofk = h->force_kernel, ott = h->tile_threads;
     h->tile_w = t->tile_w;
     h->tile_h = t->tile_h;
+    h->force_kernel = t->force_kernel;
+    h->tile_threads = t->tile_threads;
     const int r = build_tiles(h);
     if (r != DPD_OK) {
         h->tile_w = ow;
         h->tile_h = oh;
+        h->force_kernel = ofk;
+        h->tile_threads = ott;
         build_tiles(h);
         return r;
     }
-    h->force_kernel = t->force_kernel;
     h->sort_mode = t->sort_mode;
     h->gsteps = graph_len(h, t->graph_steps);
     drop_graphs(h);
@@ -990,6 +997,7 @@ extern "C" int dpd_get_tuning(const dpd_handle *h, dpd_tuning *t) {
     t->tile_h = h->tile_h;
     t->graph_steps = h->gsteps;
     t->sort_mode = h->sort_mode;
+    t->tile_threads = h->tile_threads;
     return DPD_OK;
 }
 
@@ -1578,7 +1586,7 @@ static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rd
             if (state_out[k]) CK(cudaMemcpyAsync(state_out[k], src[k], N * sizeof(float2), cudaMemcpyDefault, h->s));
     }
     if (grad) {
-        CK(cudaMemcpyAsync(grad, A.grad, (size_t)h->nrep * DPD_NGRAD * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+        CK(cudaMemcpyAsync(grad, A.grad, (size_t)h->nrep * DPD_NGRAD * sizeof(double), cudaMemcpyDefault, h->s));
     }
     // back to the end of the window
     h->cur = cur_end;
@@ -1638,7 +1646,7 @@ extern "C" int dpd_force_vjp(dpd_handle *h, int32_t r, int64_t step, const float
     CK(cudaGetLastError());
     for (int k = 0; k < 4; k++)
         if (outs[k]) CK(cudaMemcpyAsync(outs[k], st[k], n * 4, cudaMemcpyDefault, h->s));
-    if (grad) CK(cudaMemcpyAsync(grad, A.grad + (size_t)r * DPD_NGRAD, DPD_NGRAD * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    if (grad) CK(cudaMemcpyAsync(grad, A.grad + (size_t)r * DPD_NGRAD, DPD_NGRAD * sizeof(double), cudaMemcpyDefault, h->s));
     CK(cudaStreamSynchronize(h->s));
     return DPD_OK;
 }

@@ -258,7 +258,7 @@ void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, fl
                    cudaStream_t s);
 void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
                          const float *fx, const float *fy, const float *vtx, const float *vty, cudaStream_t s);
-void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
+void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles, int threads,
                         bool next_keys, cudaStream_t s);
 int tile_setup();
 size_t tile_smem_bytes();

@@ -15,8 +15,8 @@
 // (lx, ly) its half-shell partners are two contiguous index ranges of the
 // local arrays: the rest of its own cell plus the cell above, and cells
 // ly-1..ly+1 of the next column.  A lane owns one source and walks its two
-// ranges; hits (r < 1) go through a warp ballot into a per-warp ring buffer,
-// which is drained 64 pairs at a time (two per lane), so the noise and force
+// ranges; hits (r < 1) go through a warp ballot into a per-warp queue, which
+// is drained 64 pairs at a time (two per lane), so the noise and force
 // arithmetic always runs on full warps.  Halo sources only pair with owned
 // beads: their ranges are clipped to the owned rows of the column.
 //
@@ -32,26 +32,37 @@
 #define TILE_WARPS (TILE_TPB / 32)
 #define TILE_MAXB 1408
 #define TILE_MAXC 256
-#define TILE_QCAP 128  // per-warp ring; < 64 entries wait between drains, at most 64 arrive per round
+#define TILE_QCAP 128  // per-warp queue; < 64 entries wait between drains, at most 64 arrive per round
 
-struct __align__(16) TileBead {    // one tile's staged beads and their local layout
-    float2 pos[TILE_MAXB];
-    float2 vt[TILE_MAXB];
-    uint32_t tg[TILE_MAXB];
-    int32_t accx[TILE_MAXB];      // fixed-point force sums (separate arrays: 32 banks for the atomics)
-    int32_t accy[TILE_MAXB];
-    uint16_t lxy[TILE_MAXB];      // local cell of each bead: lx << 8 | ly (TILE_PAD: a padding slot)
-    uint8_t img[TILE_MAXB];       // periodic image code: (ix + 1) | (iy + 1) << 2
-    int32_t lcs[TILE_MAXC + 1];   // local cell starts (column-major over (w+2) x (h+2))
-    int32_t gst[TILE_MAXC];       // global slot of each local cell's first bead
+// one tile's staged beads and their local layout, for tiles of up to MAXC local
+// cells (tile and halo) and MAXB beads
+template <int MAXB, int MAXC>
+struct __align__(16) TileBeadT {
+    static constexpr int maxb = MAXB;
+    float2 pos[MAXB];
+    float2 vt[MAXB];
+    uint32_t tg[MAXB];
+    int32_t accx[MAXB];           // fixed-point force sums (separate arrays: 32 banks for the atomics)
+    int32_t accy[MAXB];
+    uint16_t lxy[MAXB];           // local cell of each bead: lx << 8 | ly (TILE_PAD: a padding slot)
+    uint8_t img[MAXB];            // periodic image code: (ix + 1) | (iy + 1) << 2
+    int32_t lcs[MAXC + 1];        // local cell starts (column-major over (w+2) x (h+2))
+    int32_t gst[MAXC];            // global slot of each local cell's first bead
     float a[DPD_MAXT * DPD_MAXT];
     int32_t n;
+    // The screen reads pos[t] and img[t] for t < 2 MAXB (past a range's end,
+    // masked out): pos is followed by vt, and img by at least MAXB bytes.
+    static_assert((MAXC + 1) * 4 + MAXC * 4 >= MAXB, "img must be followed by MAXB bytes of the tile");
 };
+using TileBead = TileBeadT<TILE_MAXB, TILE_MAXC>;
 
-struct TileSmem {
-    TileBead t;
-    uint32_t q[TILE_WARPS][TILE_QCAP];
-    int32_t scan[TILE_WARPS];
+// the shared memory of k_forces_tile with TPB threads: tiles of up to TPB
+// local cells, and beads in proportion
+template <int TPB>
+struct TileSmemT {
+    TileBeadT<TILE_MAXB * (TPB / 256), TPB> t;
+    uint32_t q[TPB / 32][TILE_QCAP];
+    int32_t scan[TPB / 32];
     int32_t next_chunk;           // source chunks are handed to warps as they finish their last one
 };
 
@@ -66,8 +77,8 @@ struct PairConst {
 };
 
 // the pair force on s from t as fixed-point terms (a queued pair: inside the cutoff)
-template <bool WRAP, int NOISE>
-__device__ __forceinline__ void tile_pair(const TileBead &S, const PairConst &pc, int s, int t, int &qx, int &qy,
+template <bool WRAP, int NOISE, class TB>
+__device__ __forceinline__ void tile_pair(const TB &S, const PairConst &pc, int s, int t, int &qx, int &qy,
                                           float &fmax) {
     const float2 ps = S.pos[s], pt = S.pos[t];
     float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
@@ -103,7 +114,8 @@ __device__ __forceinline__ void tile_pair(const TileBead &S, const PairConst &pc
 }
 
 // +q to s, -q to t; halo accumulators take their share too and are ignored
-__device__ __forceinline__ void tile_add(TileBead &S, uint32_t v, int qx, int qy) {
+template <class TB>
+__device__ __forceinline__ void tile_add(TB &S, uint32_t v, int qx, int qy) {
     const int s = (int)(v >> 16), t = (int)(v & 0xFFFFu);
     atomicAdd(&S.accx[s], qx);
     atomicAdd(&S.accy[s], qy);
@@ -111,15 +123,15 @@ __device__ __forceinline__ void tile_add(TileBead &S, uint32_t v, int qx, int qy
     atomicAdd(&S.accy[t], -qy);
 }
 
-// evaluate ring entries [head, head + cnt), cnt <= 64: two independent chains per lane
-template <bool WRAP, int NOISE>
-__device__ __forceinline__ void drain(TileBead &S, const PairConst &pc, const uint32_t *q, int head, int cnt,
-                                      int lane, float &fmax) {
+// evaluate queue entries [0, cnt), cnt <= 64: two independent chains per lane
+template <bool WRAP, int NOISE, class TB>
+__device__ __forceinline__ void drain(TB &S, const PairConst &pc, const uint32_t *q, int cnt, int lane,
+                                      float &fmax) {
     const int e1 = lane, e2 = lane + 32;
     const bool has1 = e1 < cnt, has2 = e2 < cnt;
     if (has1) {
-        const uint32_t v1 = q[(head + e1) & (TILE_QCAP - 1)];
-        const uint32_t v2 = q[(head + (has2 ? e2 : e1)) & (TILE_QCAP - 1)];
+        const uint32_t v1 = q[e1];
+        const uint32_t v2 = q[has2 ? e2 : e1];
         int qx1, qy1, qx2, qy2;
         tile_pair<WRAP, NOISE>(S, pc, (int)(v1 >> 16), (int)(v1 & 0xFFFFu), qx1, qy1, fmax);
         tile_pair<WRAP, NOISE>(S, pc, (int)(v2 >> 16), (int)(v2 & 0xFFFFu), qx2, qy2, fmax);
@@ -130,7 +142,8 @@ __device__ __forceinline__ void drain(TileBead &S, const PairConst &pc, const ui
 }
 
 // rows [lo, hi] of local column c that hold owned cells, as a bead index range
-__device__ __forceinline__ void owned_rows(const TileBead &S, int c, int LH, int tw, int th, int &b0, int &b1) {
+template <class TB>
+__device__ __forceinline__ void owned_rows(const TB &S, int c, int LH, int tw, int th, int &b0, int &b1) {
     if (c >= 1 && c <= tw) {
         b0 = S.lcs[c * LH + 1];
         b1 = S.lcs[c * LH + th + 1];
@@ -139,45 +152,55 @@ __device__ __forceinline__ void owned_rows(const TileBead &S, int c, int LH, int
     }
 }
 
+// The half-shell partners of source s (local cell code v) as two local index
+// ranges, [r1s, r1s + len1) and [s2m + len1, s2m + len): the rest of its own
+// cell with the cell above, and rows ly-1..ly+1 of the next column.  A halo
+// source keeps its owned partners only.  Returns len.
+template <class TB>
+__device__ __forceinline__ int src_ranges(const TB &S, int s, int v, int LH, int tw, int th, int &r1s, int &len1,
+                                          int &s2m) {
+    const int lx = v >> 8, ly = v & 255, l = lx * LH + ly;
+    int r1e = S.lcs[l + (ly + 1 < LH ? 2 : 1)];
+    r1s = s + 1;
+    const int c2 = (lx + 1) * LH;
+    int r2s = S.lcs[c2 + (ly > 0 ? ly - 1 : 0)];
+    int r2e = S.lcs[c2 + (ly + 1 < LH ? ly + 1 : LH - 1) + 1];
+    if (!(lx >= 1 && lx <= tw && ly >= 1 && ly <= th)) {  // halo source: owned partners only
+        int o0, o1;
+        owned_rows(S, lx, LH, tw, th, o0, o1);
+        r1s = max(r1s, o0);
+        r1e = min(r1e, o1);
+        owned_rows(S, lx + 1, LH, tw, th, o0, o1);
+        r2s = max(r2s, o0);
+        r2e = min(r2e, o1);
+    }
+    len1 = max(r1e - r1s, 0);
+    s2m = r2s - len1;
+    return len1 + max(r2e - r2s, 0);
+}
+
 // The screened pairs of the staged tile S, evaluated on full warps.  q: this
-// warp's ring; next_chunk: the CTA's chunk counter (starts at the warp count);
+// warp's queue; next_chunk: the CTA's chunk counter (starts at the warp count);
 // first: this warp's first chunk of 32 sources.
-template <bool WRAP, int NOISE>
-__device__ void tile_pairs(TileBead &S, uint32_t *q, int *next_chunk, int first, const PairConst &pc, int LW, int LH,
+template <bool WRAP, int NOISE, class TB>
+__device__ void tile_pairs(TB &S, uint32_t *q, int *next_chunk, int first, const PairConst &pc, int LW, int LH,
                            int tw, int th, DevStatus *status) {
     const int lane = (int)lane_id();
     const uint32_t below = (1u << lane) - 1u;
     const int nsrc = S.lcs[(LW - 1) * LH];  // the last column (right halo) holds no sources
-    int head = 0, tail = 0;
+    int tail = 0;  // queued pairs: fewer than 64 between rounds
     float fmax = 0.0f;
     for (int base = first * 32; base < nsrc;) {
         const int s = base + lane;
-        int r1s = 0, len1 = 0, r2s = 0, len = 0;
+        int r1s = 0, len1 = 0, s2m = 0, len = 0;
         float2 ps = make_float2(0.0f, 0.0f);
         int is = 0;
         const int v = s < nsrc ? S.lxy[s] : (int)TILE_PAD;
         if (v != (int)TILE_PAD) {
-            const int lx = v >> 8, ly = v & 255, l = lx * LH + ly;
             ps = S.pos[s];
             if (WRAP) is = S.img[s];
-            int r1e = S.lcs[l + (ly + 1 < LH ? 2 : 1)];
-            r1s = s + 1;
-            const int c2 = (lx + 1) * LH;
-            r2s = S.lcs[c2 + (ly > 0 ? ly - 1 : 0)];
-            int r2e = S.lcs[c2 + (ly + 1 < LH ? ly + 1 : LH - 1) + 1];
-            if (!(lx >= 1 && lx <= tw && ly >= 1 && ly <= th)) {  // halo source: owned partners only
-                int o0, o1;
-                owned_rows(S, lx, LH, tw, th, o0, o1);
-                r1s = max(r1s, o0);
-                r1e = min(r1e, o1);
-                owned_rows(S, lx + 1, LH, tw, th, o0, o1);
-                r2s = max(r2s, o0);
-                r2e = min(r2e, o1);
-            }
-            len1 = max(r1e - r1s, 0);
-            len = len1 + max(r2e - r2s, 0);
+            len = src_ranges(S, s, v, LH, tw, th, r1s, len1, s2m);
         }
-        const int s2m = r2s - len1;
         const int maxlen = __reduce_max_sync(0xffffffffu, len);
         for (int k = 0; k < maxlen; k += 2) {
             bool hit[2];
@@ -187,7 +210,7 @@ __device__ void tile_pairs(TileBead &S, uint32_t *q, int *next_chunk, int first,
                 const int kk = k + u;
                 const int t = kk + (kk < len1 ? r1s : s2m);
                 tt[u] = t;
-                const int tc = kk < len ? t : 0;  // past the end: a harmless in-range read
+                const int tc = t;  // past the end (t < 2 MAXB): an in-bounds read, masked out below
                 const float2 pt = S.pos[tc];
                 float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
                 if (WRAP) {
@@ -201,24 +224,27 @@ __device__ void tile_pairs(TileBead &S, uint32_t *q, int *next_chunk, int first,
 #pragma unroll
             for (int u = 0; u < 2; u++) {
                 const uint32_t hm = __ballot_sync(0xffffffffu, hit[u]);
-                if (hit[u]) q[(tail + __popc(hm & below)) & (TILE_QCAP - 1)] = ((uint32_t)s << 16) | (uint32_t)tt[u];
+                if (hit[u]) q[tail + __popc(hm & below)] = ((uint32_t)s << 16) | (uint32_t)tt[u];
                 tail += __popc(hm);
             }
-            __syncwarp();
-            if (tail - head >= 64) {
-                drain<WRAP, NOISE>(S, pc, q, head, 64, lane, fmax);
-                head += 64;
+            if (tail >= 64) {  // uniform over the warp
+                __syncwarp();
+                drain<WRAP, NOISE>(S, pc, q, 64, lane, fmax);
+                // move the rest, fewer than 64, to the front
+                const int rest = tail - 64;
+                const uint32_t m1 = q[64 + lane], m2 = q[96 + lane];
+                if (lane < rest) q[lane] = m1;
+                if (lane + 32 < rest) q[lane + 32] = m2;
+                tail = rest;
+                __syncwarp();
             }
         }
         int nxt = 0;
         if (lane == 0) nxt = atomicAdd(next_chunk, 1);
         base = __shfl_sync(0xffffffffu, nxt, 0) * 32;
     }
-    while (tail > head) {
-        const int cnt = min(tail - head, 64);
-        drain<WRAP, NOISE>(S, pc, q, head, cnt, lane, fmax);
-        head += cnt;
-    }
+    __syncwarp();
+    if (tail > 0) drain<WRAP, NOISE>(S, pc, q, tail, lane, fmax);
     if (fmax > 2048.0f) raise_flag(status, DPD_F_FORCE);
 }
 
@@ -323,9 +349,10 @@ __device__ void tile_direct(const Bufs &b, int cur, const RepDev &R, const TileD
     }
 }
 
-// The pairs of a staged tile: the screen and the ring, one instantiation per
+// The pairs of a staged tile: the screen and the queue, one instantiation per
 // image mode and noise generator
-__device__ __forceinline__ void tile_pairs_any(TileBead &S, uint32_t *q, int *next_chunk, int first,
+template <class TB>
+__device__ __forceinline__ void tile_pairs_any(TB &S, uint32_t *q, int *next_chunk, int first,
                                                const RepDev &R, const TileDesc &td, long long step,
                                                DevStatus *status) {
     PairConst pc;
@@ -348,9 +375,9 @@ __device__ __forceinline__ void tile_pairs_any(TileBead &S, uint32_t *q, int *ne
 // columns, every owned bead (halo rows and padding slots in that range are
 // skipped) gets its bonds, its force written to HBM and its next cell key.
 // The loads of a round are issued first.
-template <bool NEXTKEY>
+template <bool NEXTKEY, class TB>
 __device__ __forceinline__ void tile_epilogue(const Bufs &b, int cur, const RepDev &R, const TileDesc &td,
-                                              const TileBead &S, float &mb) {
+                                              const TB &S, float &mb) {
     const int LH = td.h + 2, tid = (int)threadIdx.x;
     const int e0 = S.lcs[LH + 1], e1 = S.lcs[td.w * LH + td.h + 1];
     const float2 *__restrict__ gpos = b.pos[cur];
@@ -402,13 +429,14 @@ __device__ __forceinline__ void max_bond_out(const Bufs &b, int rep, float mb) {
     if (lane_id() == 0 && mbb != 0u) atomicMax(b.obs + (size_t)rep * OBS_N + 4, (unsigned long long)mbb);
 }
 
-template <bool NEXTKEY>
-__global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
+template <bool NEXTKEY, int TPB>
+__global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const TileDesc *__restrict__ tiles) {
     pdl_begin();
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    TileSmem &SS = *reinterpret_cast<TileSmem *>(smem_raw);
-    TileBead &S = SS.t;
+    TileSmemT<TPB> &SS = *reinterpret_cast<TileSmemT<TPB> *>(smem_raw);
+    auto &S = SS.t;
+    constexpr int MAXB = TILE_MAXB * (TPB / 256);
     const TileDesc td = tiles[blockIdx.x];
     const RepDev &R = reps[td.rep];
     const int ncx = R.ncx, ncy = R.ncy;
@@ -432,7 +460,7 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_tile(Bufs b, int
         cnt = cs[gc + 1] - cs[gc];
     }
     int before;
-    {   // block exclusive scan of cnt (nl <= TILE_TPB)
+    {   // block exclusive scan of cnt (nl <= TPB)
         int x = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -445,7 +473,7 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_tile(Bufs b, int
         for (int k = 0; k < wq; k++) before += SS.scan[k];
         before += x - cnt;
         if (tid < nl) S.lcs[tid] = before;
-        if (tid == TILE_TPB - 1) {
+        if (tid == TPB - 1) {
             S.n = before + cnt;
             S.lcs[nl] = before + cnt;
         }
@@ -453,7 +481,7 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_tile(Bufs b, int
     }
     const int n = S.n;
     float mb = 0.0f;
-    if (n > TILE_MAXB) {
+    if (n > MAXB) {
         tile_direct<NEXTKEY>(b, cur, R, td, S.a, step, mb);
     } else {
         // per local cell: its beads' cell and image code
@@ -464,7 +492,7 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_tile(Bufs b, int
             }
         __syncthreads();
         // copy in: consecutive beads of a column are consecutive in HBM (coalesced)
-        for (int k = tid; k < n; k += TILE_TPB) {
+        for (int k = tid; k < n; k += TPB) {
             const int v = S.lxy[k], l = (v >> 8) * LH + (v & 255);
             const int g = S.gst[l] + (k - S.lcs[l]);
             S.pos[k] = b.pos[cur][g];
@@ -473,7 +501,7 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_tile(Bufs b, int
             S.accx[k] = 0;
             S.accy[k] = 0;
         }
-        if (tid == 0) SS.next_chunk = TILE_WARPS;  // chunks 0..7 go to warps 0..7 first
+        if (tid == 0) SS.next_chunk = TPB / 32;  // chunk w goes to warp w first
         __syncthreads();
         tile_pairs_any(S, SS.q[wq], &SS.next_chunk, wq, R, td, step, b.status);
         __syncthreads();
@@ -806,14 +834,19 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_bulk(Bufs b, int
     max_bond_out(b, td.rep, mb);
 }
 
-size_t tile_smem_bytes() { return sizeof(TileSmem); }
+size_t tile_smem_bytes() { return sizeof(TileSmemT<512>); }
 size_t bulk_smem_bytes() { return sizeof(BulkSmem); }
 
 int tile_setup() {
-    const size_t bytes = sizeof(TileSmem), bbytes = sizeof(BulkSmem);
-    cudaError_t e = cudaFuncSetAttribute(k_forces_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    const size_t bytes = sizeof(TileSmemT<256>), bytes2 = sizeof(TileSmemT<512>), bbytes = sizeof(BulkSmem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_forces_tile<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_forces_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        e = cudaFuncSetAttribute(k_forces_tile<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_forces_tile<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes2);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_forces_tile<false, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes2);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_forces_bulk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bbytes);
     if (e == cudaSuccess)
@@ -821,11 +854,17 @@ int tile_setup() {
     return e == cudaSuccess ? 0 : -1;
 }
 
-void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
+void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles, int threads,
                         bool next_keys, cudaStream_t s) {
-    const size_t bytes = sizeof(TileSmem);
-    if (next_keys) launch_pdl(k_forces_tile<true>, ntiles, TILE_TPB, bytes, s, b, cur, rep, tiles);
-    else k_forces_tile<false><<<ntiles, TILE_TPB, bytes, s>>>(b, cur, rep, tiles);
+    if (threads == 512) {
+        const size_t bytes = sizeof(TileSmemT<512>);
+        if (next_keys) launch_pdl(k_forces_tile<true, 512>, ntiles, 512, bytes, s, b, cur, rep, tiles);
+        else k_forces_tile<false, 512><<<ntiles, 512, bytes, s>>>(b, cur, rep, tiles);
+        return;
+    }
+    const size_t bytes = sizeof(TileSmemT<256>);
+    if (next_keys) launch_pdl(k_forces_tile<true, 256>, ntiles, 256, bytes, s, b, cur, rep, tiles);
+    else k_forces_tile<false, 256><<<ntiles, 256, bytes, s>>>(b, cur, rep, tiles);
 }
 
 void launch_forces_bulk(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,

@@ -66,7 +66,7 @@ class DpdTemplate(C.Structure):
 
 class DpdTuning(C.Structure):
     _fields_ = [("force_kernel", C.c_int32), ("tile_w", C.c_int32), ("tile_h", C.c_int32),
-                ("graph_steps", C.c_int32), ("sort_mode", C.c_int32)]
+                ("graph_steps", C.c_int32), ("sort_mode", C.c_int32), ("tile_threads", C.c_int32)]
 
 
 class DpdRdfSpec(C.Structure):

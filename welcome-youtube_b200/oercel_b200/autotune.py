@@ -18,12 +18,15 @@ import numpy as np
 
 FORCE_CANDIDATES = [
     dict(force_kernel=1),
-    dict(force_kernel=0, tile_w=8, tile_h=16),
-    dict(force_kernel=0, tile_w=14, tile_h=14),
-    dict(force_kernel=0, tile_w=6, tile_h=30),
-    dict(force_kernel=0, tile_w=10, tile_h=18),
-    dict(force_kernel=0, tile_w=4, tile_h=8),
-    dict(force_kernel=0, tile_w=2, tile_h=4),
+    dict(force_kernel=0, tile_w=8, tile_h=16, tile_threads=256),
+    dict(force_kernel=0, tile_w=14, tile_h=14, tile_threads=256),
+    dict(force_kernel=0, tile_w=6, tile_h=30, tile_threads=256),
+    dict(force_kernel=0, tile_w=10, tile_h=18, tile_threads=256),
+    dict(force_kernel=0, tile_w=4, tile_h=8, tile_threads=256),
+    dict(force_kernel=0, tile_w=2, tile_h=4, tile_threads=256),
+    dict(force_kernel=0, tile_w=20, tile_h=20, tile_threads=512),
+    dict(force_kernel=0, tile_w=14, tile_h=30, tile_threads=512),
+    dict(force_kernel=0, tile_w=10, tile_h=40, tile_threads=512),
     dict(force_kernel=2, tile_w=14, tile_h=14),
     dict(force_kernel=2, tile_w=8, tile_h=16),
     dict(force_kernel=2, tile_w=6, tile_h=30),

@@ -165,13 +165,13 @@ class Engine:
         t = _capi.DpdTuning()
         check(self.lib.dpd_get_tuning(self.h, C.byref(t)))
         return dict(force_kernel=t.force_kernel, tile_w=t.tile_w, tile_h=t.tile_h, graph_steps=t.graph_steps,
-                    sort_mode=t.sort_mode)
+                    sort_mode=t.sort_mode, tile_threads=t.tile_threads)
 
     def set_tuning(self, **kv):
         cur = self.tuning()
         cur.update(kv)
         t = _capi.DpdTuning(int(cur["force_kernel"]), int(cur["tile_w"]), int(cur["tile_h"]), int(cur["graph_steps"]),
-                            int(cur["sort_mode"]))
+                            int(cur["sort_mode"]), int(cur["tile_threads"]))
         check(self.lib.dpd_set_tuning(self.h, C.byref(t)))
 
     def profile_step(self):
