@@ -68,6 +68,19 @@ struct TileSmemT {
 
 #define TILE_PAD 0xFFFFu          // lxy of a slot that holds no bead of the tile (bulk-copy padding)
 
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// asynchronous global -> shared copies of one 8- or 4-byte element
+// (cp.async, completed by cp.async.wait_all): a thread keeps all of its
+// elements in flight at once, with no registers held for them
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // periodic image shift of a pair along one axis: (code_s - code_t) L, exactly 0 or +-L
 __device__ __forceinline__ float img_shift(int dc, float L) { return dc == 0 ? 0.0f : (dc > 0 ? L : -L); }
 
@@ -491,17 +504,19 @@ __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs
                 S.img[k] = (uint8_t)code;
             }
         __syncthreads();
-        // copy in: consecutive beads of a column are consecutive in HBM (coalesced)
+        // copy in: consecutive beads of a column are consecutive in HBM
+        // (coalesced); every copy of a thread is issued before it waits
         for (int k = tid; k < n; k += TPB) {
             const int v = S.lxy[k], l = (v >> 8) * LH + (v & 255);
             const int g = S.gst[l] + (k - S.lcs[l]);
-            S.pos[k] = b.pos[cur][g];
-            S.vt[k] = b.vt[cur][g];
-            S.tg[k] = b.tg[cur][g];
+            cp_async8(&S.pos[k], b.pos[cur] + g);
+            cp_async8(&S.vt[k], b.vt[cur] + g);
+            cp_async4(&S.tg[k], b.tg[cur] + g);
             S.accx[k] = 0;
             S.accy[k] = 0;
         }
         if (tid == 0) SS.next_chunk = TPB / 32;  // chunk w goes to warp w first
+        cp_async_wait_all();
         __syncthreads();
         tile_pairs_any(S, SS.q[wq], &SS.next_chunk, wq, R, td, step, b.status);
         __syncthreads();
@@ -553,7 +568,6 @@ struct BulkSmem {
     unsigned long long mbar;
 };
 
-__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(unsigned long long *m, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(m)), "r"(count) : "memory");
