@@ -312,9 +312,11 @@ __device__ __forceinline__ void angle_terms(const Bufs &b, int cur, const RepDev
 // (launch_pdl): a kernel may be scheduled while its predecessor drains.  It
 // waits for the predecessor's completion (and its memory) before touching
 // anything, and lets its own successor be scheduled once all its CTAs run.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_begin() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    pdl_wait();
+    pdl_trigger();
 }
 
 // ---------------------------------------------------------------- grid helpers

@@ -445,7 +445,10 @@ __device__ __forceinline__ void max_bond_out(const Bufs &b, int rep, float mb) {
 template <bool NEXTKEY, int TPB>
 __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
                                                           const TileDesc *__restrict__ tiles) {
-    pdl_begin();
+    // The successor may be scheduled only once this grid's CTAs reach their
+    // epilogue: scheduled earlier, its waiting CTAs would hold SM slots that
+    // later tiles need (1 % of the step at 1M beads).
+    pdl_wait();
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmemT<TPB> &SS = *reinterpret_cast<TileSmemT<TPB> *>(smem_raw);
     auto &S = SS.t;
@@ -520,6 +523,7 @@ __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs
         __syncthreads();
         tile_pairs_any(S, SS.q[wq], &SS.next_chunk, wq, R, td, step, b.status);
         __syncthreads();
+        pdl_trigger();
         tile_epilogue<NEXTKEY>(b, cur, R, td, S, mb);
     }
     max_bond_out(b, td.rep, mb);

@@ -22,6 +22,8 @@ FORCE_CANDIDATES = [
     dict(force_kernel=0, tile_w=14, tile_h=14, tile_threads=256),
     dict(force_kernel=0, tile_w=6, tile_h=30, tile_threads=256),
     dict(force_kernel=0, tile_w=10, tile_h=18, tile_threads=256),
+    dict(force_kernel=0, tile_w=12, tile_h=13, tile_threads=256),
+    dict(force_kernel=0, tile_w=9, tile_h=17, tile_threads=256),
     dict(force_kernel=0, tile_w=4, tile_h=8, tile_threads=256),
     dict(force_kernel=0, tile_w=2, tile_h=4, tile_threads=256),
     dict(force_kernel=0, tile_w=20, tile_h=20, tile_threads=512),
@@ -33,6 +35,9 @@ FORCE_CANDIDATES = [
     dict(force_kernel=2, tile_w=10, tile_h=18),
     dict(force_kernel=2, tile_w=4, tile_h=8),
 ]
+
+# 12 x 13 and 9 x 17 cells give 1720 and 1767 tiles on a 512 x 512 grid, just under three full
+# rounds of 4 CTAs on 148 SMs (1776)
 
 # the cell sort: 0 two scan passes, 1 one scan pass with decoupled look-back, 2 a block-local
 # scan whose block prefixes the placement and fix-up kernels add themselves
