@@ -356,7 +356,7 @@ static int build_tiles(dpd_handle *h) {
         const int w = std::min(h->tile_w, R.ncx - 2), hh = std::min(h->tile_h, R.ncy - 2);
         for (int cx = 0; cx < R.ncx; cx += w)
             for (int cy = 0; cy < R.ncy; cy += hh)
-                t.push_back({r, cx, cy, std::min(w, R.ncx - cx), std::min(hh, R.ncy - cy), 0, 0, 0});
+                t.push_back({r, cx, cy, std::min(w, R.ncx - cx), std::min(hh, R.ncy - cy), (int32_t)R.c0, R.ncx, R.ncy});
     }
     if (h->d_tiles) {
         cudaFree(h->d_tiles);

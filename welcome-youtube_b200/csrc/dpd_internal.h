@@ -107,7 +107,8 @@ struct Chunk {                  // one CTA's work: packed indices [begin, end) o
 };
 
 struct TileDesc {               // one CTA of the tiled force kernel: cells [cx0, cx0+w) x [cy0, cy0+h)
-    int32_t rep, cx0, cy0, w, h, pad0, pad1, pad2;
+    int32_t rep, cx0, cy0, w, h;
+    int32_t c0, ncx, ncy;       // the replica's first cell and grid (its RepDev's), read with the tile
 };
 
 struct DevStatus {

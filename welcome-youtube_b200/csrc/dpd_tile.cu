@@ -455,9 +455,9 @@ __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs
     constexpr int MAXB = TILE_MAXB * (TPB / 256);
     const TileDesc td = tiles[blockIdx.x];
     const RepDev &R = reps[td.rep];
-    const int ncx = R.ncx, ncy = R.ncy;
+    const int ncx = td.ncx, ncy = td.ncy;  // from the tile: the cell starts need no load of R first
     const int LH = td.h + 2, nl = (td.w + 2) * LH;
-    const int32_t *__restrict__ cs = b.cstart + R.c0;
+    const int32_t *__restrict__ cs = b.cstart + td.c0;
     const int tid = (int)threadIdx.x, lane = (int)lane_id(), wq = tid >> 5;
     const long long step = *b.step;
     if (tid < DPD_MAXT * DPD_MAXT) S.a[tid] = a_at(R, tid, step);
