@@ -438,7 +438,9 @@ typedef struct {
                         symmetric pair's total), d loss / d gamma, d loss / d k_bond */
 
 /* Advance every replica nsteps steps (chemistry must be off) and return the
- * loss (nrep values) and, if rdf_out, the averaged g(r) (nrep x nbin). */
+ * loss (nrep values) and, if rdf_out, the averaged g(r) (nrep x nbin).  The
+ * differentiated terms are those of the forces (dpd_force_vjp), the noise
+ * amplitude following the temperature cycle. */
 DPD_API int dpd_window_loss(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec, const double *target,
                             double *loss, double *rdf_out);
 /* The same window, then its adjoint: the pair noise is replayed from its key,
@@ -458,10 +460,12 @@ DPD_API int dpd_window_adjoint(dpd_handle *h, int64_t nsteps, int32_t ckpt_every
 DPD_API int dpd_window_adjoint_state(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
                                      const double *target, double *loss, double *grad, double *rdf_out, float *xbar,
                                      float *vhbar, float *vtbar);
-/* Vector-Jacobian product of the pair + bond forces of replica r's current
- * configuration at `step` (noise key): given the force cotangent (gx, gy, slot
- * order), the gradients with respect to positions (xbar), predicted velocities
- * (vbar) and parameters (grad, DPD_NGRAD values). */
+/* Vector-Jacobian product of the forces of replica r's current configuration
+ * at `step` (noise key and kT(t)): pair terms, bonds and angle terms (linear
+ * chains and the templates of the branched shapes) and stirring.  Given the
+ * force cotangent (gx, gy, slot order), the gradients with respect to
+ * positions (xbar), predicted velocities (vbar) and parameters (grad,
+ * DPD_NGRAD values). */
 DPD_API int dpd_force_vjp(dpd_handle *h, int32_t replica, int64_t step, const float *gx, const float *gy,
                           float *xbar_x, float *xbar_y, float *vbar_x, float *vbar_y, double *grad);
 

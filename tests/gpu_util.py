@@ -68,3 +68,23 @@ def links_by_gid(s):
     P[g] = pv
     Nn[g] = nx
     return P, Nn
+
+
+def naive_chain_and_stir_forces(torch, x, prv, nxt, ka, L, stir_A, stir_n):
+    """angle terms U = ka (1 - cos) of every chain triplet (oercel.c:1237-1256) and the
+    stirring body force A sin(2 pi n y / L) less its mean (oercel.c:1183-1195), float64"""
+    F = torch.zeros_like(x)
+    j = np.nonzero((prv >= 0) & (nxt >= 0))[0]
+    if ka != 0.0 and len(j):
+        p_, n_ = prv[j], nxt[j]
+        a = x[j] - x[p_]
+        a = a - L * torch.round(a / L)
+        c = x[n_] - x[j]
+        c = c - L * torch.round(c / L)
+        cos = (a * c).sum(-1) / (a.norm(dim=-1) * c.norm(dim=-1))
+        U = (ka * (1.0 - cos)).sum()
+        F = F - torch.autograd.grad(U, x, create_graph=True)[0]
+    if stir_A != 0.0:
+        f = stir_A * torch.sin(2.0 * np.pi * stir_n * x[:, 1] / L)
+        F = F + torch.stack([f - f.mean(), torch.zeros_like(f)], -1)
+    return F

@@ -8,7 +8,7 @@ import pytest
 
 import oracle as O
 import oercel_b200 as ob
-from gpu_util import engine_with, oracle_params, params
+from gpu_util import engine_with, naive_chain_and_stir_forces, oracle_params, params
 
 pytestmark = pytest.mark.gpu
 
@@ -41,6 +41,194 @@ def naive_forces(torch, x, v, P, gamma, kb, types, theta, nxt, L, kT, dt, r0):
     F = F.index_add(0, torch.as_tensor(i), fb)
     F = F.index_add(0, torch.as_tensor(j), -fb)
     return F
+
+
+def _theta_table(p, s, step):
+    """the pair noise theta of every pair of the state at `step`, from the oracle"""
+    op = oracle_params(p)
+    n = len(s["x"])
+    th = np.zeros((n, n))
+    for a_ in range(n):
+        for b_ in range(a_ + 1, n):
+            th[a_, b_] = th[b_, a_] = O.lib().ora_theta(C.byref(op), step, int(s["gid"][a_]), int(s["gid"][b_]))
+    return th
+
+
+def test_force_vjp_with_angles_stirring_and_temperature_cycle(cuda_ok):
+    """every term together: pairs with the noise at kT(t), bonds, angle terms and
+    stirring, against torch autograd of the all-pairs model"""
+    import torch
+    p = params(L=8.0, seed=23, noise="philox", f_lip=0.3, c_N=0.1, k_angle=10.0, stir_A=0.5, stir_n=2, kT_amp=0.3,
+               kT_period=0.5)
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(5)
+    step = e.step_no
+    s = e.state()
+    n = len(s["x"])
+    rng = np.random.default_rng(0)
+    gx, gy = rng.normal(size=(2, n)).astype(np.float32)
+    xbx, xby, vbx, vby, grad = e.force_vjp(0, step, gx, gy)
+    th = _theta_table(p, s, step)
+    dt = torch.float64
+    x = torch.tensor(np.c_[s["x"], s["y"]], dtype=dt, requires_grad=True)
+    v = torch.tensor(np.c_[s["vtx"], s["vty"]], dtype=dt, requires_grad=True)
+    P = torch.tensor(np.array(p.a, dtype=np.float64), dtype=dt, requires_grad=True)
+    gam = torch.tensor(p.gamma, dtype=dt, requires_grad=True)
+    kb = torch.tensor(p.k_bond, dtype=dt, requires_grad=True)
+    L = float(np.float32(p.L))
+    kT = p.kT + p.kT_amp * np.sin(2.0 * np.pi * step * p.dt / p.kT_period)  # t = step dt
+    F = naive_forces(torch, x, v, P, gam, kb, torch.as_tensor(s["type"].astype(np.int64)), torch.tensor(th), s["next"],
+                     L, kT, p.dt, p.r0)
+    F = F + naive_chain_and_stir_forces(torch, x, s["prev"], s["next"], p.k_angle, L, p.stir_A, p.stir_n)
+    assert np.abs(F.detach().numpy() - np.c_[s["fx"], s["fy"]]).max() < 1e-5 * np.abs(F.detach().numpy()).max()
+    lam = (F * torch.tensor(np.c_[gx, gy], dtype=dt)).sum()
+    gxv, gvv, gP, gg, gk = torch.autograd.grad(lam, [x, v, P, gam, kb])
+
+    def rel(a, b):
+        return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-30)
+
+    assert rel(np.c_[xbx, xby], gxv.numpy()) < 1e-3
+    assert rel(np.c_[vbx, vby], gvv.numpy()) < 1e-3
+    gP = gP.numpy()
+    up = np.array([[gP[i, j] if i <= j else 0.0 for j in range(MAXT)] for i in range(MAXT)])
+    assert rel(grad[:64].reshape(MAXT, MAXT), up) < 1e-3
+    assert grad[64] == pytest.approx(gg.item(), rel=1e-3)
+    assert grad[65] == pytest.approx(gk.item(), rel=1e-3)
+
+
+def test_force_vjp_terms_one_at_a_time(cuda_ok):
+    """each term's own share of the VJP, the VJP with the term on less the VJP
+    with it off on the same configuration, against torch autograd of that term
+    alone: the angle terms, stirring, and the temperature cycle's noise"""
+    import torch
+    kv = dict(L=8.0, seed=25, noise="philox", f_lip=0.4, c_N=0.1)
+    on = dict(k_angle=30.0, stir_A=2.0, stir_n=2, kT_amp=0.5, kT_period=0.5)
+    full = params(**kv, **on)
+    e = ob.Engine(full)
+    e.load_soup(0)
+    e.prime()
+    e.step(5)
+    step = e.step_no
+    s = e.state()
+    n = len(s["x"])
+    rng = np.random.default_rng(4)
+    gx, gy = rng.normal(size=(2, n)).astype(np.float32)
+
+    def vjp(**off):
+        e.set_params(0, params(**kv, **{**on, **off}))
+        xbx, xby, vbx, vby, grad = e.force_vjp(0, step, gx, gy)
+        return np.c_[xbx, xby].astype(np.float64), np.c_[vbx, vby].astype(np.float64), grad
+
+    x_all, v_all, g_all = vjp()
+    dt = torch.float64
+    L = float(np.float32(full.L))
+    g = torch.tensor(np.c_[gx, gy], dtype=dt)
+
+    def share(F, x):
+        return torch.autograd.grad((F * g).sum(), x)[0].numpy()
+
+    def rel(a, b):
+        return np.abs(a - b).max() / np.abs(b).max()
+
+    x = torch.tensor(np.c_[s["x"], s["y"]], dtype=dt, requires_grad=True)
+    want = share(naive_chain_and_stir_forces(torch, x, s["prev"], s["next"], on["k_angle"], L, 0.0, 1), x)
+    assert np.abs(want).max() > 0
+    assert rel(x_all - vjp(k_angle=0.0)[0], want) < 1e-4
+    x = torch.tensor(np.c_[s["x"], s["y"]], dtype=dt, requires_grad=True)
+    want = share(naive_chain_and_stir_forces(torch, x, s["prev"], s["next"], 0.0, L, on["stir_A"], on["stir_n"]), x)
+    assert rel(x_all - vjp(stir_A=0.0)[0], want) < 1e-4
+    # the noise at kT(t) less the noise at kT: through the positions and gamma
+    th = _theta_table(full, s, step)
+    x = torch.tensor(np.c_[s["x"], s["y"]], dtype=dt, requires_grad=True)
+    v = torch.tensor(np.c_[s["vtx"], s["vty"]], dtype=dt, requires_grad=True)
+    gam = torch.tensor(full.gamma, dtype=dt, requires_grad=True)
+    P = torch.tensor(np.array(full.a, dtype=np.float64), dtype=dt)
+    kb = torch.tensor(full.k_bond, dtype=dt)
+    kTt = full.kT + on["kT_amp"] * np.sin(2.0 * np.pi * step * full.dt / on["kT_period"])
+    args = (torch.as_tensor(s["type"].astype(np.int64)), torch.tensor(th), s["next"], L)
+    F = naive_forces(torch, x, v, P, gam, kb, *args, kTt, full.dt, full.r0) - \
+        naive_forces(torch, x, v, P, gam, kb, *args, full.kT, full.dt, full.r0)
+    wx, wv, wg = torch.autograd.grad((F * g).sum(), [x, v, gam], allow_unused=True)
+    x_off, v_off, g_off = vjp(kT_amp=0.0)
+    assert rel(x_all - x_off, wx.numpy()) < 1e-3
+    # the noise term does not depend on the velocities: their share is zero (torch's to rounding)
+    assert wv is None or np.abs(wv.numpy()).max() <= 1e-12 * np.abs(wx.numpy()).max()
+    assert np.abs(v_all - v_off).max() <= 1e-6 * np.abs(v_all).max()
+    assert g_all[64] - g_off[64] == pytest.approx(wg.item(), rel=1e-3)
+
+
+def naive_template_forces(torch, x, prv, nxt, tmpl, kb, L):
+    """bonded forces of branched lipids from their template (mol_forces,
+    oercel.c:1221-1257): each molecule is the chain of next links from a bead
+    without prev; bonds kb (r - r0) toward each other, angles K (1 - cos) or
+    K (cos - c0)^2 of (x_j - x_i, x_k - x_j); float64"""
+    starts = np.nonzero((prv < 0) & (nxt >= 0))[0]
+    mols = []
+    for s0 in starts:
+        m = [s0]
+        while nxt[m[-1]] >= 0 and len(m) < tmpl.mlen:
+            m.append(nxt[m[-1]])
+        assert len(m) == tmpl.mlen
+        mols.append(m)
+    M = torch.as_tensor(np.array(mols))
+    U = x.new_zeros(())
+
+    def vec(i, j):
+        d = x[M[:, j]] - x[M[:, i]]
+        return d - L * torch.round(d / L)
+    for q in range(tmpl.nb):
+        r = vec(tmpl.bi[q], tmpl.bj[q]).norm(dim=-1)
+        U = U + 0.5 * kb * ((r - tmpl.br0[q]) ** 2).sum()
+    for q in range(tmpl.na):
+        a, c = vec(tmpl.ai[q], tmpl.aj[q]), vec(tmpl.aj[q], tmpl.ak[q])
+        cos = (a * c).sum(-1) / (a.norm(dim=-1) * c.norm(dim=-1))
+        K, c0 = float(tmpl.aK[q]), float(tmpl.ac0[q])
+        U = U + (K * (1.0 - cos) if tmpl.akind[q] == 0 else K * (cos - c0) ** 2).sum()
+    return -torch.autograd.grad(U, x, create_graph=True)[0]
+
+
+def test_force_vjp_of_branched_lipids(cuda_ok):
+    """the template bonds and both kinds of angle term of pi lipids, against torch autograd"""
+    import torch
+    p = params(L=8.0, seed=24, noise="philox", f_lip=0.4, c_N=0.05, lip_arch="pi", lip_nT=2, lip_tie=1, r0_head=0.7,
+               k_bond=300, k_angle=15, k_head=20, cos_head=-0.2)
+    tmpl = p.template()
+    assert any(tmpl.akind[q] == 1 for q in range(tmpl.na))
+    e = ob.Engine(p)
+    e.load_soup(0)
+    e.prime()
+    e.step(5)
+    step = e.step_no
+    s = e.state()
+    n = len(s["x"])
+    rng = np.random.default_rng(3)
+    gx, gy = rng.normal(size=(2, n)).astype(np.float32)
+    xbx, xby, vbx, vby, grad = e.force_vjp(0, step, gx, gy)
+    th = _theta_table(p, s, step)
+    dt = torch.float64
+    x = torch.tensor(np.c_[s["x"], s["y"]], dtype=dt, requires_grad=True)
+    v = torch.tensor(np.c_[s["vtx"], s["vty"]], dtype=dt, requires_grad=True)
+    P = torch.tensor(np.array(p.a, dtype=np.float64), dtype=dt, requires_grad=True)
+    gam = torch.tensor(p.gamma, dtype=dt, requires_grad=True)
+    kb = torch.tensor(p.k_bond, dtype=dt, requires_grad=True)
+    L = float(np.float32(p.L))
+    none = -np.ones(n, dtype=np.int64)  # no linear bonds: the template's terms instead
+    F = naive_forces(torch, x, v, P, gam, kb, torch.as_tensor(s["type"].astype(np.int64)), torch.tensor(th), none, L,
+                     p.kT, p.dt, p.r0)
+    F = F + naive_template_forces(torch, x, s["prev"], s["next"], tmpl, kb, L)
+    assert np.abs(F.detach().numpy() - np.c_[s["fx"], s["fy"]]).max() < 1e-5 * np.abs(F.detach().numpy()).max()
+    lam = (F * torch.tensor(np.c_[gx, gy], dtype=dt)).sum()
+    gxv, gvv, gP, gg, gk = torch.autograd.grad(lam, [x, v, P, gam, kb])
+
+    def rel(a, b):
+        return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-30)
+
+    assert rel(np.c_[xbx, xby], gxv.numpy()) < 1e-3
+    assert rel(np.c_[vbx, vby], gvv.numpy()) < 1e-3
+    assert grad[64] == pytest.approx(gg.item(), rel=1e-3)
+    assert grad[65] == pytest.approx(gk.item(), rel=1e-3)
 
 
 def test_force_vjp_matches_torch_autograd(cuda_ok):
@@ -127,6 +315,39 @@ def test_window_adjoint_matches_finite_differences(cuda_ok):
     for key, val, idx in checks:
         h = 0.04 * val
         fd = (loss_at(**{key: val + h}) - loss_at(**{key: val - h})) / (2 * h)
+        assert grad[0][idx] == pytest.approx(fd, rel=1e-3, abs=1e-5 * np.abs(grad[0]).max()), key
+
+
+def test_window_adjoint_with_angles_stirring_and_temperature_cycle(cuda_ok):
+    """the window adjoint through the angle, stirring and kT(t) terms against
+    central differences.  These terms bend the loss more over the 4 % steps of
+    the test above, so the differences are Richardson-extrapolated from steps of
+    2 % and 1 %: (4 D(h/2) - D(h)) / 3.  gamma is left to the exact check against
+    the unrolled torch model (test_gpu_autograd.py): it scales the noise
+    amplitude too, and its differences scatter by a few 1e-3 on this box."""
+    kv = dict(L=12.0, seed=7, noise="philox", f_lip=0.3, c_N=0.1, k_angle=10.0, stir_A=0.5, stir_n=2, kT_amp=0.3,
+              kT_period=2.0)
+    base = params(**kv)
+    e = ob.Engine(base)
+    e.load_soup(0)
+    e.prime()
+    e.step(40)
+    s0, step0 = e.state(), e.step_no
+    spec = ob.Engine.rdf_spec(ta=2, tb=2, nbin=32, rmax=2.0, sigma=0.1, last_steps=5)
+    target = np.linspace(0.5, 1.5, 32)
+    nsteps, ckpt = 6, 5
+    loss, grad, rdf = _window_engine(base, s0, step0).window_adjoint(nsteps, ckpt, spec, target)
+    assert loss[0] > 0 and np.all(np.isfinite(grad))
+
+    def loss_at(**over):
+        return _window_engine(params(**{**kv, **over}), s0, step0).window_loss(nsteps, spec, target)[0][0]
+
+    def d(key, val, h):
+        return (loss_at(**{key: val + h}) - loss_at(**{key: val - h})) / (2 * h)
+
+    for key, val, idx in [("a_W_T", 75.0, 2), ("a_H_T", 50.0, 10), ("k_bond", 100.0, 65)]:
+        h = 0.02 * val
+        fd = (4.0 * d(key, val, h / 2) - d(key, val, h)) / 3.0
         assert grad[0][idx] == pytest.approx(fd, rel=1e-3, abs=1e-5 * np.abs(grad[0]).max()), key
 
 

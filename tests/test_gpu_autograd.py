@@ -14,7 +14,7 @@ import pytest
 
 import oracle as O
 import oercel_b200 as ob
-from gpu_util import oracle_params, params
+from gpu_util import naive_chain_and_stir_forces, oracle_params, params
 
 pytestmark = pytest.mark.gpu
 
@@ -67,7 +67,9 @@ def smoothed_pairs(torch, x, sel, L, nbin, rmax, sigma):
     return torch.where(inside, k, torch.zeros_like(k)).sum(0)
 
 
-def unrolled_window_loss(torch, p, step0, nsteps, x0, vh0, vt0, P, gamma, kb, types, bi, bj, spec, target):
+def unrolled_window_loss(torch, p, step0, nsteps, x0, vh0, vt0, P, gamma, kb, types, bi, bj, spec, target,
+                         prv=None, nxt=None):
+    """prv, nxt (gid order): the chains, for the angle terms and stirring when p has them"""
     op = oracle_params(p)
     L = float(np.float32(p.L))
     dt = float(np.float32(p.dt))
@@ -80,7 +82,13 @@ def unrolled_window_loss(torch, p, step0, nsteps, x0, vh0, vt0, P, gamma, kb, ty
 
     def forces(x, v, step):
         th = torch.as_tensor(O.theta_matrix(op, step, gid))
-        return pair_forces_all(torch, x, v, asym, gamma, kb, types, th, bi, bj, L, p.kT, dt, p.r0)
+        kT = p.kT
+        if p.kT_amp != 0:  # the temperature cycle of the noise, t = step dt
+            kT = p.kT + p.kT_amp * np.sin(2.0 * np.pi * step * p.dt / p.kT_period)
+        F = pair_forces_all(torch, x, v, asym, gamma, kb, types, th, bi, bj, L, kT, dt, p.r0)
+        if p.k_angle != 0 or p.stir_A != 0:
+            F = F + naive_chain_and_stir_forces(torch, x, prv, nxt, p.k_angle, L, p.stir_A, p.stir_n)
+        return F
 
     x, vh, vt = x0, vh0, vt0
     f = forces(x, vt, step0)
@@ -122,11 +130,15 @@ def rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("nsteps,seed", [(12, 31), (20, 32)])
-def test_window_gradient_matches_unrolled_torch_autograd(cuda_ok, nsteps, seed):
+EXTRA = dict(k_angle=10.0, stir_A=0.5, stir_n=2, kT_amp=0.3, kT_period=2.0)
+
+
+@pytest.mark.parametrize("nsteps,seed,extra", [(12, 31, {}), (20, 32, {}), (12, 34, EXTRA)])
+def test_window_gradient_matches_unrolled_torch_autograd(cuda_ok, nsteps, seed, extra):
+    """extra: the angle terms of the chains, stirring and the temperature cycle as well"""
     import torch
     from oercel_b200 import autograd as AG
-    p = params(L=8.0, seed=seed, noise="philox", f_lip=0.3, c_N=0.1)
+    p = params(L=8.0, seed=seed, noise="philox", f_lip=0.3, c_N=0.1, **extra)
     e = ob.Engine(p)
     e.load_soup(0)
     e.prime()
@@ -150,7 +162,11 @@ def test_window_gradient_matches_unrolled_torch_autograd(cuda_ok, nsteps, seed):
     types = torch.as_tensor(s["type"].astype(np.int64))
     bi = torch.as_tensor(np.nonzero(s["next"] >= 0)[0])
     bj = torch.as_tensor(s["next"][s["next"] >= 0])
-    lm = unrolled_window_loss(torch, p, step0, nsteps, x0, vh0, vt0, P, gam, kb, types, bi, bj, spec, target)
+    nxt = s["next"]
+    prv = np.full(len(nxt), -1, np.int64)
+    prv[nxt[nxt >= 0]] = np.nonzero(nxt >= 0)[0]
+    lm = unrolled_window_loss(torch, p, step0, nsteps, x0, vh0, vt0, P, gam, kb, types, bi, bj, spec, target, prv,
+                              nxt)
     want = torch.autograd.grad(lm, [x0, vh0, vt0, P, gam, kb])
     assert float(loss.detach()[0]) == pytest.approx(float(lm.detach()), rel=1e-4)
     names = ["x0", "vh0", "vt0"]

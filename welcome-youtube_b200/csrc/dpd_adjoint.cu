@@ -19,17 +19,119 @@
 //   d(c.f)/da_ij = (c.d) w / r,  d(c.f)/dgamma = (c.d) w (-w rv + s theta / (2 gamma)) / r
 // with c = g_i - g_j for the pair (i, j).  Every bead sums over its 3x3 cells
 // (each pair from both ends; the two halves are exact negatives), the
-// parameter gradients count each pair once.
+// parameter gradients count each pair once.  s follows the temperature cycle
+// (s(step) = sqrt(2 gamma kT(t) / dt)), as the forward forces do.
+//
+// Angle terms (U = K (1 - cos), or K (cos - c0)^2 at the junctions of the
+// branched shapes, per triplet i-j-k, a = x_j - x_i, c = x_k - x_j): with
+// F = -grad U the VJP on bead m is -d phi / d x_m, phi = sum over beads of
+// g . dU/dx = D U(a, c)[da, dc], da = g_j - g_i, dc = g_k - g_j.  dphi/da and
+// dphi/dc are Hessian-vector products of U, written out in angle_hvp; then
+// d/dx_i = -d/da, d/dx_j = d/da - d/dc, d/dx_k = d/dc.  Linear chains: each
+// bead gathers the triplets it is part of (as middle, as last of its prev's,
+// as first of its next's), so no two threads write one bead.  Branched
+// shapes: k_mol_vjp, one thread per molecule.
+//
+// Stirring (f_x,i = A sin(2 pi k y_i) minus its replica mean): the VJP on y_m
+// is A 2 pi k cos(2 pi k y_m) (g_x,m - mean of g_x), the mean from k_gsum.
 #include "dpd_device.cuh"
 
 #define NGRAD DPD_NGRAD
 
 __device__ __forceinline__ float theta_of(const NoiseKey &nk, uint32_t gi, uint32_t gj) { return pair_theta(nk, gi, gj); }
 
+__device__ __forceinline__ float dot2(float2 u, float2 v) { return u.x * v.x + u.y * v.y; }
+
+// dphi/da (pa) and dphi/dc (pc) of phi = D U(a, c)[da, dc] for an angle term
+// U(cos) of kind 0, U = K (1 - cos) (U' = -K, U'' = 0), or kind 1,
+// U = K (cos - c0)^2 (U' = 2 K (cos - c0), U'' = 2 K):
+//   cos = (a.c) / (|a| |c|),  Dcos = q / AC - cos (a.da) / A2 - cos (c.dc) / C2,  q = da.c + a.dc
+//   dDcos/da = dc / AC - q a / (AC A2) - gca ((a.da) / A2 + (c.dc) / C2) - cos (da / A2 - 2 (a.da) a / A2^2)
+//   dDcos/dc = da / AC - q c / (AC C2) - gcc ((a.da) / A2 + (c.dc) / C2) - cos (dc / C2 - 2 (c.dc) c / C2^2)
+// with gca = dcos/da = c / AC - cos a / A2, gcc = dcos/dc = a / AC - cos c / C2;
+// phi = U' Dcos, so dphi/da = U'' Dcos gca + U' dDcos/da (and likewise for c)
+__device__ __forceinline__ void angle_hvp(float2 a, float2 c, float2 da, float2 dc, int kind, float K, float c0,
+                                          float2 &pa, float2 &pc) {
+    const float A2 = dot2(a, a), C2 = dot2(c, c);
+    const float iac = rsqrtf(A2 * C2), iA2 = 1.0f / A2, iC2 = 1.0f / C2;
+    const float cs = dot2(a, c) * iac;
+    const float q = dot2(da, c) + dot2(a, dc), ada = dot2(a, da), cdc = dot2(c, dc);
+    const float m = ada * iA2 + cdc * iC2;
+    const float2 gca = make_float2(c.x * iac - cs * a.x * iA2, c.y * iac - cs * a.y * iA2);
+    const float2 gcc = make_float2(a.x * iac - cs * c.x * iC2, a.y * iac - cs * c.y * iC2);
+    const float ta = q * iac * iA2, tc = q * iac * iC2;
+    const float ka2 = 2.0f * ada * iA2 * iA2, kc2 = 2.0f * cdc * iC2 * iC2;
+    const float u1 = kind == 0 ? -K : 2.0f * K * (cs - c0), u2 = kind == 0 ? 0.0f : 2.0f * K;
+    const float dcos = q * iac - cs * m;
+    pa = make_float2(u2 * dcos * gca.x + u1 * (dc.x * iac - ta * a.x - gca.x * m - cs * (da.x * iA2 - ka2 * a.x)),
+                     u2 * dcos * gca.y + u1 * (dc.y * iac - ta * a.y - gca.y * m - cs * (da.y * iA2 - ka2 * a.y)));
+    pc = make_float2(u2 * dcos * gcc.x + u1 * (da.x * iac - tc * c.x - gcc.x * m - cs * (dc.x * iC2 - kc2 * c.x)),
+                     u2 * dcos * gcc.y + u1 * (da.y * iac - tc * c.y - gcc.y * m - cs * (dc.y * iC2 - kc2 * c.y)));
+}
+
+// the angle-term VJP of a bead of a linear chain at pi with cotangent gi and
+// links lk (x_bar increment): the triplets (p, d, n), (pp, p, d) and
+// (d, n, nn) of its chain, where they exist
+__device__ __forceinline__ float2 angle_vjp(const StateView &sv, const float2 *__restrict__ g, const RepDev &R, float2 pi,
+                                           float2 gi, int2 lk) {
+    const float L = R.L, h = R.halfL, ka = R.ka;
+    float2 out = make_float2(0.0f, 0.0f);
+    auto vec = [&](float2 u, float2 v) {  // v - u, minimum image
+        return make_float2(minimg(v.x - u.x, L, h), minimg(v.y - u.y, L, h));
+    };
+    auto dif = [](float2 u, float2 v) { return make_float2(v.x - u.x, v.y - u.y); };
+    float2 pp_ = pi, pn = pi, gp = gi, gn = gi;
+    if (lk.x >= 0) {
+        pp_ = sv.pos[lk.x];
+        gp = g[lk.x];
+    }
+    if (lk.y >= 0) {
+        pn = sv.pos[lk.y];
+        gn = g[lk.y];
+    }
+    float2 pa, pc;
+    if (lk.x >= 0 && lk.y >= 0) {  // the bead in the middle: -(dphi/da - dphi/dc)
+        angle_hvp(vec(pp_, pi), vec(pi, pn), dif(gp, gi), dif(gi, gn), 0, ka, 0.0f, pa, pc);
+        out.x -= pa.x - pc.x;
+        out.y -= pa.y - pc.y;
+    }
+    if (lk.x >= 0) {
+        const int q = sv.link[lk.x].x;
+        if (q >= 0) {  // (q, p, d): the bead last, -dphi/dc
+            const float2 pq = sv.pos[q], gq = g[q];
+            angle_hvp(vec(pq, pp_), vec(pp_, pi), dif(gq, gp), dif(gp, gi), 0, ka, 0.0f, pa, pc);
+            out.x -= pc.x;
+            out.y -= pc.y;
+        }
+    }
+    if (lk.y >= 0) {
+        const int q = sv.link[lk.y].y;
+        if (q >= 0) {  // (d, n, q): the bead first, +dphi/da
+            const float2 pq = sv.pos[q], gq = g[q];
+            angle_hvp(vec(pi, pn), vec(pn, pq), dif(gi, gn), dif(gn, gq), 0, ka, 0.0f, pa, pc);
+            out.x += pa.x;
+            out.y += pa.y;
+        }
+    }
+    return out;
+}
+
+// per replica, the sum of the x cotangents (the stirring term's mean)
+__global__ void __launch_bounds__(BEAD_TPB) k_gsum(const RepDev *__restrict__ reps, const Chunk *__restrict__ ch,
+                                                   const float2 *__restrict__ g, double *__restrict__ gsum) {
+    const Chunk c = ch[blockIdx.x];
+    if (reps[c.rep].stir_A == 0.0f) return;
+    const int d = c.begin + (int)threadIdx.x;
+    double v = d < c.end ? (double)g[d].x : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane_id() == 0 && v != 0.0) atomicAdd(gsum + c.rep, v);
+}
+
 __global__ void __launch_bounds__(BEAD_TPB) k_force_vjp(StateView sv, long long step, const RepDev *__restrict__ reps,
                                                         const Chunk *__restrict__ ch, const float2 *__restrict__ g,
                                                         float2 *__restrict__ xbar, float2 *__restrict__ vbar,
-                                                        double *__restrict__ grad) {
+                                                        double *__restrict__ grad, const double *__restrict__ gsum) {
     __shared__ double sgrad[NGRAD];
     for (int k = threadIdx.x; k < NGRAD; k += blockDim.x) sgrad[k] = 0.0;
     __syncthreads();
@@ -40,7 +142,7 @@ __global__ void __launch_bounds__(BEAD_TPB) k_force_vjp(StateView sv, long long 
         const float2 pi = sv.pos[d], vi = sv.vt[d], gi2 = g[d];
         const uint32_t tgi = sv.tg[d], gi = tgi & GID_MASK;
         const int ti = (int)(tgi >> TYPE_SHIFT);
-        const float L = R.L, h = R.halfL, gam = R.gamma, s = R.sdt;
+        const float L = R.L, h = R.halfL, gam = R.gamma, s = sdt_at(R, step);
         const NoiseKey nk = make_noise_key(R, step);
         const int ncx = R.ncx, ncy = R.ncy;
         const int32_t *cs = sv.cstart + R.c0;
@@ -85,8 +187,9 @@ __global__ void __launch_bounds__(BEAD_TPB) k_force_vjp(StateView sv, long long 
                     }
                 }
             }
-        // bonds: f_i = kb (1 - r0/r) d with d = x_p - x_i
-        const int2 lk = sv.link[d];
+        // bonds: f_i = kb (1 - r0/r) d with d = x_p - x_i (linear chains; the
+        // branched shapes' bonds and angles are k_mol_vjp's)
+        const int2 lk = R.arch == 0 ? sv.link[d] : make_int2(-1, -1);
         double gkb = 0.0;
         for (int q = 0; q < 2; q++) {
             const int p = q ? lk.y : lk.x;
@@ -101,6 +204,16 @@ __global__ void __launch_bounds__(BEAD_TPB) k_force_vjp(StateView sv, long long 
             xbx -= k0 * dx + R.kb * u * cxv;
             xby -= k0 * dy + R.kb * u * cyv;
             if (q == 1) gkb += (double)(u * cd);  // each bond once, from its prev end
+        }
+        if (R.ka != 0.0f && (lk.x >= 0 || lk.y >= 0)) {
+            const float2 t = angle_vjp(sv, g, R, pi, gi2, lk);
+            xbx += t.x;
+            xby += t.y;
+        }
+        if (R.stir_A != 0.0f) {
+            const double w2 = 2.0 * R.stir_k;
+            const double dfy = (double)R.stir_A * M_PI * w2 * cospi(w2 * (double)pi.y);
+            xby += (float)(dfy * ((double)gi2.x - gsum[c.rep] / (double)R.n));
         }
         xbar[d] = make_float2(xbx, xby);
         vbar[d] = make_float2(vbx, vby);
@@ -250,9 +363,87 @@ __global__ void k_adj_save(int n, const float2 *pos, const float2 *vt, const uin
     olink[k] = link[k];
 }
 
+// The bonded terms of the branched shapes (the template terms of
+// k_mol_forces): one thread per molecule (its first bead) adds each of its
+// beads' share to x_bar after k_force_vjp, so no two threads write one bead.
+// Bond (i, j), d = x_j - x_i, F_i = kb (1 - r0/r) d = -F_j, c = g_i - g_j:
+//   d(c.F_i)/dd = kb ((1 - r0/r) c + r0 (c.d) d / r^3),  d(c.F_i)/dkb = (1 - r0/r) (c.d)
+// Angle (i, j, k): x_bar_i += dphi/da, x_bar_j -= dphi/da - dphi/dc, x_bar_k -= dphi/dc.
+__global__ void __launch_bounds__(BEAD_TPB) k_mol_vjp(StateView sv, const RepDev *__restrict__ reps,
+                                                      const Chunk *__restrict__ ch, const dpd_template *__restrict__ mol,
+                                                      const float2 *__restrict__ g, float2 *__restrict__ xbar,
+                                                      double *__restrict__ grad) {
+    const Chunk c = ch[blockIdx.x];
+    const RepDev &R = reps[c.rep];
+    if (R.arch == 0) return;
+    const int d = c.begin + (int)threadIdx.x;
+    double gkb = 0.0;
+    if (d < c.end) {
+        const int2 lk0 = sv.link[d];
+        if (lk0.x < 0 && lk0.y >= 0) {
+            const dpd_template &M = mol[c.rep];
+            const int ml = M.mlen;
+            int sl[DPD_MAXML];
+            float2 p[DPD_MAXML], gg[DPD_MAXML], xb[DPD_MAXML];
+            int n = 0;
+            for (int q = d; q >= 0 && n < ml; q = sv.link[q].y) {
+                sl[n] = q;
+                p[n] = sv.pos[q];
+                gg[n] = g[q];
+                xb[n] = make_float2(0.0f, 0.0f);
+                n++;
+            }
+            if (n == ml) {  // (an incomplete molecule raised DPD_F_CHAIN in the forward pass)
+                const float L = R.L, h = R.halfL, kb = R.kb;
+                for (int q = 0; q < M.nb; q++) {
+                    const int i = M.bi[q], j = M.bj[q];
+                    const float dx = minimg(p[j].x - p[i].x, L, h), dy = minimg(p[j].y - p[i].y, L, h);
+                    const float r = sqrtf(dx * dx + dy * dy), r0 = (float)M.br0[q];
+                    const float cx = gg[i].x - gg[j].x, cy = gg[i].y - gg[j].y, cd = cx * dx + cy * dy;
+                    const float u = 1.0f - r0 / r, k3 = kb * r0 * cd / (r * r * r);
+                    const float tx = kb * u * cx + k3 * dx, ty = kb * u * cy + k3 * dy;  // d(c.F_i)/dd
+                    xb[i].x -= tx;
+                    xb[i].y -= ty;
+                    xb[j].x += tx;
+                    xb[j].y += ty;
+                    gkb += (double)(u * cd);
+                }
+                for (int q = 0; q < M.na; q++) {
+                    const int i = M.ai[q], j = M.aj[q], k = M.ak[q];
+                    const float2 a = make_float2(minimg(p[j].x - p[i].x, L, h), minimg(p[j].y - p[i].y, L, h));
+                    const float2 cc = make_float2(minimg(p[k].x - p[j].x, L, h), minimg(p[k].y - p[j].y, L, h));
+                    const float2 da = make_float2(gg[j].x - gg[i].x, gg[j].y - gg[i].y);
+                    const float2 dc = make_float2(gg[k].x - gg[j].x, gg[k].y - gg[j].y);
+                    float2 pa, pc;
+                    angle_hvp(a, cc, da, dc, M.akind[q], (float)M.aK[q], (float)M.ac0[q], pa, pc);
+                    xb[i].x += pa.x;
+                    xb[i].y += pa.y;
+                    xb[j].x -= pa.x - pc.x;
+                    xb[j].y -= pa.y - pc.y;
+                    xb[k].x -= pc.x;
+                    xb[k].y -= pc.y;
+                }
+                for (int e = 0; e < ml; e++) {
+                    const float2 o = xbar[sl[e]];
+                    xbar[sl[e]] = make_float2(o.x + xb[e].x, o.y + xb[e].y);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) gkb += __shfl_down_sync(0xffffffffu, gkb, o);
+    if (lane_id() == 0 && gkb != 0.0) atomicAdd(&grad[(size_t)c.rep * NGRAD + DPD_MAXT * DPD_MAXT + 1], gkb);
+}
+
 void launch_force_vjp(const StateView &sv, long long step, const RepDev *rep, const Chunk *bch, int nbch,
-                      const float2 *g, float2 *xbar, float2 *vbar, double *grad, cudaStream_t s) {
-    k_force_vjp<<<nbch, BEAD_TPB, 0, s>>>(sv, step, rep, bch, g, xbar, vbar, grad);
+                      const float2 *g, float2 *xbar, float2 *vbar, double *grad, double *gsum, int nrep, bool stir,
+                      const dpd_template *mol, cudaStream_t s) {
+    if (stir) {
+        cudaMemsetAsync(gsum, 0, (size_t)nrep * sizeof(double), s);
+        k_gsum<<<nbch, BEAD_TPB, 0, s>>>(rep, bch, g, gsum);
+    }
+    k_force_vjp<<<nbch, BEAD_TPB, 0, s>>>(sv, step, rep, bch, g, xbar, vbar, grad, gsum);
+    if (mol) k_mol_vjp<<<nbch, BEAD_TPB, 0, s>>>(sv, rep, bch, mol, g, xbar, grad);
 }
 
 void launch_rdf(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,

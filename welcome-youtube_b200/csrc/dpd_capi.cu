@@ -59,6 +59,7 @@ struct AdjBufs {
     std::vector<SegState> seg;
     float2 *X, *V, *F, *g, *xb, *vb;
     double *hist, *wgt, *grad;
+    double *gsum;            // per replica: the sum of the x cotangents (stirring)
 };
 }  // namespace
 
@@ -1388,6 +1389,7 @@ static int adj_setup(dpd_handle *h, int nck, int nseg, int nbin, AdjBufs &A) {
     want(&A.hist, (size_t)h->nrep * nbin);
     want(&A.wgt, (size_t)h->nrep * nbin);
     want(&A.grad, (size_t)h->nrep * DPD_NGRAD);
+    want(&A.gsum, (size_t)h->nrep);
     size_t total = 0;
     for (auto &q : plan) total += (q.second + 64 + 255) & ~(size_t)255;
     char *base = nullptr;
@@ -1461,11 +1463,6 @@ static int check_window(dpd_handle *h, int64_t nsteps, const dpd_rdf_spec *spec,
         if (p.chem) return fail(DPD_E_ARG, "chemistry must be off inside a differentiated window");
         if (p.warmup > 0 && h->step < p.warm_end)
             return fail(DPD_E_ARG, "the repulsion warm-up must be over before a differentiated window");
-        if (p.lip_arch != 0)
-            return fail(DPD_E_ARG, "branched lipids are not differentiated (the force VJP has linear bonds only)");
-        if (p.k_angle != 0.0 || p.stir_A != 0.0 || p.kT_amp != 0.0)
-            return fail(DPD_E_ARG, "angle terms, stirring and the temperature cycle must be off in a differentiated "
-                                   "window (the force VJP has no terms for them)");
     }
     return DPD_OK;
 }
@@ -1570,14 +1567,16 @@ static int window_impl(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rd
             if (k >= first_loss)
                 launch_rdf_vjp(v, h->d_rep, h->d_bch, h->nbch, spec->ta, spec->tb, nb, rmax, sig, A.wgt, A.X, h->s);
             launch_adj_gather(v.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
-            launch_force_vjp(v, step0 + k, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+            launch_force_vjp(v, step0 + k, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, A.gsum, h->nrep,
+                     h->any_stir, h->any_mol ? h->b.mol : nullptr, h->s);
             launch_adj_update(v.tg, h->d_rep, h->d_bch, h->nbch, A.xb, A.vb, A.X, A.V, A.F, h->s);
         }
     }
     // the forces stored at step k_stop (the window start without a horizon) depend on the parameters too
     const StateView v0 = view_of(A.seg[stop_slot]);
     launch_adj_gather(v0.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
-    launch_force_vjp(v0, step0 + k_stop, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+    launch_force_vjp(v0, step0 + k_stop, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, A.gsum, h->nrep,
+                     h->any_stir, h->any_mol ? h->b.mol : nullptr, h->s);
     CK(cudaGetLastError());
     if (state_out) {
         launch_adj_state(v0.tg, h->d_rep, h->d_bch, h->nbch, A.xb, A.vb, A.X, A.g, h->s);
@@ -1633,7 +1632,8 @@ extern "C" int dpd_force_vjp(dpd_handle *h, int32_t r, int64_t step, const float
     Bufs u = h->b;
     u.f[h->cur] = A.g;
     launch_set_dynamics(u, h->cur, R.b0, (int)n, nullptr, nullptr, sx, sy, nullptr, nullptr, h->s);
-    launch_force_vjp(view_cur(h), step, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, h->s);
+    launch_force_vjp(view_cur(h), step, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, A.gsum, h->nrep,
+                     h->any_stir, h->any_mol ? h->b.mol : nullptr, h->s);
     CK(cudaGetLastError());
     float *outs[4] = {xbar_x, xbar_y, vbar_x, vbar_y};
     float *st[4];

@@ -266,8 +266,11 @@ size_t tile_smem_bytes();
 size_t bulk_smem_bytes();
 void launch_forces_bulk(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
                         bool next_keys, cudaStream_t s);
+// gsum: nrep doubles of scratch (the mean x cotangent of the stirring term), used when stir;
+// mol: the replicas' lipid templates when some replica has branched lipids, else null
 void launch_force_vjp(const StateView &sv, long long step, const RepDev *rep, const Chunk *bch, int nbch,
-                      const float2 *g, float2 *xbar, float2 *vbar, double *grad, cudaStream_t s);
+                      const float2 *g, float2 *xbar, float2 *vbar, double *grad, double *gsum, int nrep, bool stir,
+                      const dpd_template *mol, cudaStream_t s);
 void launch_rdf(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,
                 float rmax, float sigma, double *hist, cudaStream_t s);
 void launch_rdf_vjp(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,
