@@ -327,3 +327,36 @@ def test_stats_ring_rows_equal_stats_async(cuda_ok):
     a.stats_ring(0, None)
     a.step(4)
     assert max(int(r[6]) for r in ring) == 12  # no row after the ring was stopped
+
+
+@pytest.mark.parametrize("rho", [4, 7])
+def test_stats_ring_of_one_replica_in_a_batch(cuda_ok, rho):
+    """the tile force kernel assembles the ring's row itself: replica 1 of a
+    two-box engine gives the rows that dpd_stats_async gives for it; at rho 7 the
+    14 x 14 tiles hold more beads than shared memory does and take the direct
+    path"""
+    import torch
+    ps = [params(L=24, seed=6, rho=rho), params(L=20, seed=7, rho=rho)]
+    ns = [p.n_beads() for p in ps]
+    a, b = ob.Engine(ps, n_beads=ns), ob.Engine(ps, n_beads=ns)
+    for e in (a, b):
+        for r in range(2):
+            e.load_soup(r)
+        e.prime()
+        e.set_tuning(force_kernel=0, tile_w=14, tile_h=14, tile_threads=256)
+    ring = torch.zeros((8, 16), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    a.stats_ring(1, ring)
+    a.set_graph_steps(2)
+    b.set_graph_steps(1)
+    for _ in range(3):
+        a.step(2)
+        rows = {int(r[6]): r.copy() for r in ring}
+        for _ in range(2):
+            b.step(1)
+            raw = np.zeros(16, np.uint64)
+            b.stats_async(1, raw)
+            b.sync()
+            got = rows[b.step_no].copy()
+            got[6] = 0
+            assert np.array_equal(got, raw)
+    a.stats_ring(1, None)

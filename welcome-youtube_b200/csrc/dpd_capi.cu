@@ -387,10 +387,12 @@ static void enqueue_cell_sort(dpd_handle *h, bool step_inc) {
     launch_cellfix(h->b, h->d_cch, h->ncch, h->s);
 }
 
-static void enqueue_forces(dpd_handle *h, bool next_keys) {
+// row: a stats row the tile kernel assembles on the way (the other kernels
+// leave it to the caller)
+static void enqueue_forces(dpd_handle *h, bool next_keys, RowOut row = RowOut{-1, 0, nullptr}) {
     if (h->any_mol) launch_mol_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->s);
     if (h->force_kernel == 0)
-        launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, h->tile_threads, next_keys, h->s);
+        launch_forces_tile(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, h->tile_threads, next_keys, h->s, row);
     else if (h->force_kernel == 2) launch_forces_bulk(h->b, h->cur, h->d_rep, h->d_tiles, h->ntiles, next_keys, h->s);
     else launch_forces(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, true, true, next_keys, h->s);
 }
@@ -892,10 +894,16 @@ static void enqueue_step(dpd_handle *h, int64_t s) {
         launch_catalyst(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->nrep, h->C, h->nmax, h->stream_grid, h->s);
         enqueue_sort(h, PERM_SORT);
     }
-    enqueue_forces(h, true);
-    if (h->ring)
-        launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->ring_rep, false, h->ring, h->ring_slots,
-                           h->s);
+    // the step's stats row into the ring: assembled by the tile force kernel's
+    // epilogue from the beads it holds anyway, else by a pass of its own
+    if (h->ring && h->force_kernel == 0) {
+        enqueue_forces(h, true, RowOut{h->ring_rep, h->ring_slots, h->ring});
+    } else {
+        enqueue_forces(h, true);
+        if (h->ring)
+            launch_observables(h->b, h->cur, h->d_rep, h->d_bch, h->nbch, h->ring_rep, false, h->ring, h->ring_slots,
+                               h->s);
+    }
 }
 
 // capture gsteps steps starting from the current buffer parity and step s0

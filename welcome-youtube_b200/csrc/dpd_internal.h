@@ -259,8 +259,16 @@ void launch_unpack(const Bufs &b, int cur, int b0, int n, float *x, float *y, fl
                    cudaStream_t s);
 void launch_set_dynamics(const Bufs &b, int cur, int b0, int n, const float *vhx, const float *vhy,
                          const float *fx, const float *fy, const float *vtx, const float *vty, cudaStream_t s);
+// A stats row that the tile force kernel assembles in its epilogue, in place
+// of a separate pass over the beads: replica rep's row of this step (rep < 0:
+// none), handed over to obs_out and, when host is set, into the ring
+// host[step % slots] (the step in word 6), as k_observables does.
+struct RowOut {
+    int32_t rep, slots;
+    unsigned long long *host;
+};
 void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles, int threads,
-                        bool next_keys, cudaStream_t s);
+                        bool next_keys, cudaStream_t s, RowOut row = RowOut{-1, 0, nullptr});
 int tile_setup();
 size_t tile_smem_bytes();
 size_t bulk_smem_bytes();

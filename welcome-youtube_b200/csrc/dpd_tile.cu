@@ -64,6 +64,9 @@ struct TileSmemT {
     uint32_t q[TPB / 32][TILE_QCAP];
     int32_t scan[TPB / 32];
     int32_t next_chunk;           // source chunks are handed to warps as they finish their last one
+    long long rsum[TPB / 32][3];  // per warp, the stats-row sums of the tile's owned beads (RowAcc)
+    uint32_t rcnt[TPB / 32][DPD_MAXT / 2 + 1];
+    int32_t rlast;                // this CTA hands the row over
 };
 
 #define TILE_PAD 0xFFFFu          // lxy of a slot that holds no bead of the tile (bulk-copy padding)
@@ -265,9 +268,9 @@ __device__ void tile_pairs(TB &S, uint32_t *q, int *next_chunk, int first, const
 // links lk, its bond partners' positions pj[2] and its half-step velocity v
 // (loaded by the caller)
 template <bool NEXTKEY>
-__device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepDev &R, int rep, int g, float2 pi,
-                                              long long qx, long long qy, int2 lk, const float2 (&pj)[2], float2 v,
-                                              float &mb, uint32_t &key) {
+__device__ __forceinline__ float2 finish_loaded(const Bufs &b, int cur, const RepDev &R, int rep, int g, float2 pi,
+                                                long long qx, long long qy, int2 lk, const float2 (&pj)[2], float2 v,
+                                                float &mb, uint32_t &key) {
     const float L = R.L, h = R.halfL, kb = R.kb, r0 = R.r0;
     if (R.arch != 0) {  // branched lipids: the template terms of k_mol_forces
         if (lk.x >= 0 || lk.y >= 0) {
@@ -298,18 +301,57 @@ __device__ __forceinline__ void finish_loaded(const Bufs &b, int cur, const RepD
         key = (uint32_t)(R.c0 + cell_xy(R, advance1(pi.x, v.x, fs.x, R.dt, R.dt2, L),
                                         advance1(pi.y, v.y, fs.y, R.dt, R.dt2, L), cx, cy));
     }
+    return fs;
 }
+
+// The stats-row terms of a thread's owned beads, as k_observables sums them:
+// momentum and kinetic energy of v = vh + dt/2 F in fixed point, the bead
+// count of each type (16-bit fields, two types per word) and the molecule
+// heads.  flush() adds the warp's sums into its slot of the CTA's sums in
+// shared memory (all lanes of the warp call it; the slot starts at zero).
+struct RowAcc {
+    long long sx = 0, sy = 0, s2 = 0;
+    uint32_t c[DPD_MAXT / 2] = {0, 0, 0, 0};
+    uint32_t heads = 0;
+    __device__ __forceinline__ void add(const RepDev &R, float2 v, float2 f, uint32_t tg, int2 lk) {
+        const double vx = (double)v.x + (double)R.hdt * (double)f.x;
+        const double vy = (double)v.y + (double)R.hdt * (double)f.y;
+        sx += __double2ll_rn(vx * OBS_FIX);
+        sy += __double2ll_rn(vy * OBS_FIX);
+        s2 += __double2ll_rn((vx * vx + vy * vy) * OBS_FIX);
+        const int ty = (int)(tg >> TYPE_SHIFT);
+#pragma unroll
+        for (int w = 0; w < DPD_MAXT / 2; w++)
+            c[w] += ty == 2 * w ? 1u : (ty == 2 * w + 1 ? 0x10000u : 0u);
+        heads += (lk.x < 0 && lk.y >= 0) ? 1u : 0u;
+    }
+    __device__ __forceinline__ void flush(long long (*rs)[3], uint32_t (*rc)[DPD_MAXT / 2 + 1]) {
+        const long long a = warp_sum_ll(sx), bb = warp_sum_ll(sy), d = warp_sum_ll(s2);
+        uint32_t cw[DPD_MAXT / 2 + 1];
+#pragma unroll
+        for (int w = 0; w < DPD_MAXT / 2; w++) cw[w] = __reduce_add_sync(0xffffffffu, c[w]);
+        cw[DPD_MAXT / 2] = __reduce_add_sync(0xffffffffu, heads);
+        if (lane_id() == 0) {  // the warp's own slot: no other thread writes it
+            const int w = (int)threadIdx.x >> 5;
+            rs[w][0] += a;
+            rs[w][1] += bb;
+            rs[w][2] += d;
+#pragma unroll
+            for (int k = 0; k < DPD_MAXT / 2 + 1; k++) rc[w][k] += cw[k];
+        }
+    }
+};
 
 // the same with its own loads (the crowded-tile path)
 template <bool NEXTKEY>
-__device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev &R, int rep, int g, float2 pi,
-                                            long long qx, long long qy, float &mb, uint32_t &key) {
+__device__ __forceinline__ float2 finish_bead(const Bufs &b, int cur, const RepDev &R, int rep, int g, float2 pi,
+                                              long long qx, long long qy, float &mb, uint32_t &key) {
     const int2 lk = b.link[cur][g];
     float2 pj[2];
     pj[0] = lk.x >= 0 ? b.pos[cur][lk.x] : pi;
     pj[1] = lk.y >= 0 ? b.pos[cur][lk.y] : pi;
     const float2 v = NEXTKEY ? b.vh[cur][g] : make_float2(0.0f, 0.0f);
-    finish_loaded<NEXTKEY>(b, cur, R, rep, g, pi, qx, qy, lk, pj, v, mb, key);
+    return finish_loaded<NEXTKEY>(b, cur, R, rep, g, pi, qx, qy, lk, pj, v, mb, key);
 }
 
 #define EPI_ITEMS 2   // owned beads per thread per round of the epilogue
@@ -324,7 +366,7 @@ __device__ __forceinline__ void finish_bead(const Bufs &b, int cur, const RepDev
 // same bits).  arow: the tile's a_ij table in shared memory.
 template <bool NEXTKEY>
 __device__ void tile_direct(const Bufs &b, int cur, const RepDev &R, const TileDesc &td, const float *a, long long step,
-                            float &mb) {
+                            float &mb, long long (*rs)[3], uint32_t (*rc)[DPD_MAXT / 2 + 1]) {
     const int ncy = R.ncy, tid = (int)threadIdx.x;
     const int32_t *__restrict__ cs = b.cstart + R.c0;
     PairConst pk;
@@ -332,9 +374,11 @@ __device__ void tile_direct(const Bufs &b, int cur, const RepDev &R, const TileD
     for (int c = 1; c <= td.w; c++) {
         const int gx = td.cx0 + c - 1, g0 = cs[gx * ncy + td.cy0], g1 = cs[gx * ncy + td.cy0 + td.h];
         for (int base = g0; base < g1; base += blockDim.x) {
+            RowAcc acc;  // this round's row terms
             const int g = base + tid;
             const bool act = g < g1;
             uint32_t key = 0;
+            float2 fs = make_float2(0.0f, 0.0f);
             if (act) {
                 PairCtx pc;
                 pc.pos = b.pos[cur];
@@ -352,8 +396,10 @@ __device__ void tile_direct(const Bufs &b, int cur, const RepDev &R, const TileD
                 pc.sdt = sdt_at(R, step);
                 long long ax = 0, ay = 0;
                 bead_pairs_direct(pc, R, cs, g, ax, ay);
-                finish_bead<NEXTKEY>(b, cur, R, td.rep, g, pc.pi, ax, ay, mb, key);
+                fs = finish_bead<NEXTKEY>(b, cur, R, td.rep, g, pc.pi, ax, ay, mb, key);
             }
+            if (rs && act) acc.add(R, b.vh[cur][g], fs, b.tg[cur][g], b.link[cur][g]);
+            if (rs) acc.flush(rs, rc);  // (uniform over the CTA)
             if (NEXTKEY) {
                 count_key(b.count, key, act);
                 if (act) b.key[g] = key;
@@ -390,11 +436,13 @@ __device__ __forceinline__ void tile_pairs_any(TB &S, uint32_t *q, int *next_chu
 // The loads of a round are issued first.
 template <bool NEXTKEY, class TB>
 __device__ __forceinline__ void tile_epilogue(const Bufs &b, int cur, const RepDev &R, const TileDesc &td,
-                                              const TB &S, float &mb) {
+                                              const TB &S, float &mb, long long (*rs)[3],
+                                              uint32_t (*rc)[DPD_MAXT / 2 + 1]) {
     const int LH = td.h + 2, tid = (int)threadIdx.x;
     const int e0 = S.lcs[LH + 1], e1 = S.lcs[td.w * LH + td.h + 1];
     const float2 *__restrict__ gpos = b.pos[cur];
     for (int base = e0; base < e1; base += EPI_ITEMS * blockDim.x) {
+        RowAcc acc;  // this round's row terms
         int gg[EPI_ITEMS];
         bool own[EPI_ITEMS];
 #pragma unroll
@@ -425,15 +473,61 @@ __device__ __forceinline__ void tile_epilogue(const Bufs &b, int cur, const RepD
         for (int j = 0; j < EPI_ITEMS; j++) {
             const int k = base + j * (int)blockDim.x + tid;
             uint32_t key = 0;
+            float2 fs = make_float2(0.0f, 0.0f);
             if (own[j])
-                finish_loaded<NEXTKEY>(b, cur, R, td.rep, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j], vv[j],
-                                       mb, key);
+                fs = finish_loaded<NEXTKEY>(b, cur, R, td.rep, gg[j], S.pos[k], S.accx[k], S.accy[k], lk[j], pj[j],
+                                            vv[j], mb, key);
             if (NEXTKEY) {
                 count_key(b.count, key, own[j]);
                 if (own[j]) b.key[gg[j]] = key;
             }
+            if (rs && own[j]) acc.add(R, vv[j], fs, S.tg[k], lk[j]);
         }
+        if (rs) acc.flush(rs, rc);  // (uniform over the CTA)
     }
+}
+
+// The end of a launch that assembles a stats row: the CTA's row sums go to
+// the replica's running sums (the slots of k_observables: 0, 1 momentum,
+// 2 kinetic, 5 heads, 8 + t type counts; 4, the max bond, is max_bond_out's),
+// and the last CTA of the grid hands the row over, to obs_out and into the
+// host ring, and clears the sums for the next row, as k_observables does.
+__device__ __forceinline__ void row_handover(const Bufs &b, const RowOut &row, const long long (*rs)[3],
+                                             const uint32_t (*rc)[DPD_MAXT / 2 + 1], bool mine, int32_t *last) {
+    __syncthreads();
+    unsigned long long *obs = b.obs + (size_t)row.rep * OBS_N;
+    const int tid = (int)threadIdx.x, nw = (int)blockDim.x >> 5;
+    if (mine && tid < 3 + DPD_MAXT + 1) {  // the warps' sums: 3 fixed-point sums, the type counts, the heads
+        unsigned long long v = 0;
+        int slot;
+        if (tid < 3) {
+            for (int w = 0; w < nw; w++) v += (unsigned long long)rs[w][tid];
+            slot = tid;
+        } else if (tid < 3 + DPD_MAXT) {
+            const int t = tid - 3;
+            for (int w = 0; w < nw; w++) v += (rc[w][t >> 1] >> (16 * (t & 1))) & 0xFFFFu;
+            slot = 8 + t;
+        } else {
+            for (int w = 0; w < nw; w++) v += rc[w][DPD_MAXT / 2];
+            slot = 5;
+        }
+        if (v != 0) atomicAdd(obs + slot, v);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) *last = atomicAdd(b.obs_done + row.rep, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!*last) return;
+    __threadfence();
+    unsigned long long *out = row.host;
+    const long long step = *b.step;
+    if (out && row.slots > 0) out += (size_t)(step % row.slots) * OBS_N;
+    if (tid < OBS_N) {
+        const unsigned long long v = atomicExch(obs + tid, 0ull);
+        b.obs_out[(size_t)row.rep * OBS_N + tid] = v;
+        if (out) out[tid] = (row.slots > 0 && tid == 6) ? (unsigned long long)step : v;
+    }
+    if (tid == 0) b.obs_done[row.rep] = 0u;
 }
 
 // the running max bond of a tile's replica (one atomic per warp)
@@ -444,7 +538,7 @@ __device__ __forceinline__ void max_bond_out(const Bufs &b, int rep, float mb) {
 
 template <bool NEXTKEY, int TPB>
 __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs b, int cur, const RepDev *__restrict__ reps,
-                                                          const TileDesc *__restrict__ tiles) {
+                                                          const TileDesc *__restrict__ tiles, RowOut row) {
     // The successor may be scheduled only once this grid's CTAs reach their
     // epilogue: scheduled earlier, its waiting CTAs would hold SM slots that
     // later tiles need (1 % of the step at 1M beads).
@@ -461,6 +555,13 @@ __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs
     const int tid = (int)threadIdx.x, lane = (int)lane_id(), wq = tid >> 5;
     const long long step = *b.step;
     if (tid < DPD_MAXT * DPD_MAXT) S.a[tid] = a_at(R, tid, step);
+    const bool want_row = NEXTKEY && row.rep == td.rep;  // this tile's beads enter the step's stats row
+    long long(*rs)[3] = want_row ? SS.rsum : nullptr;
+    uint32_t(*rc)[DPD_MAXT / 2 + 1] = want_row ? SS.rcnt : nullptr;
+    if (want_row && lane == 0) {  // each warp's slot of the row sums (only that warp's lane 0 writes it)
+        SS.rsum[wq][0] = SS.rsum[wq][1] = SS.rsum[wq][2] = 0;
+        for (int k = 0; k < DPD_MAXT / 2 + 1; k++) SS.rcnt[wq][k] = 0;
+    }
     // ---- phase 0: local cells, their bead counts, exclusive scan
     int cnt = 0, lx = 0, ly = 0, code = 0;
     if (tid < nl) {
@@ -498,7 +599,7 @@ __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs
     const int n = S.n;
     float mb = 0.0f;
     if (n > MAXB) {
-        tile_direct<NEXTKEY>(b, cur, R, td, S.a, step, mb);
+        tile_direct<NEXTKEY>(b, cur, R, td, S.a, step, mb, rs, rc);
     } else {
         // per local cell: its beads' cell and image code
         if (tid < nl)
@@ -524,9 +625,10 @@ __global__ void __launch_bounds__(TPB, TILE_MINB * 256 / TPB) k_forces_tile(Bufs
         tile_pairs_any(S, SS.q[wq], &SS.next_chunk, wq, R, td, step, b.status);
         __syncthreads();
         pdl_trigger();
-        tile_epilogue<NEXTKEY>(b, cur, R, td, S, mb);
+        tile_epilogue<NEXTKEY>(b, cur, R, td, S, mb, rs, rc);
     }
     max_bond_out(b, td.rep, mb);
+    if (NEXTKEY && row.rep >= 0) row_handover(b, row, SS.rsum, SS.rcnt, want_row, &SS.rlast);
 }
 
 // ---------------------------------------------------------------- the bulk-staged kernel
@@ -847,7 +949,7 @@ __global__ void __launch_bounds__(TILE_TPB, TILE_MINB) k_forces_bulk(Bufs b, int
         __syncthreads();
         bulk_epilogue<NEXTKEY>(b, cur, R, td, S, mb);
     } else {
-        tile_direct<NEXTKEY>(b, cur, R, td, T.a, step, mb);
+        tile_direct<NEXTKEY>(b, cur, R, td, T.a, step, mb, nullptr, nullptr);
     }
     max_bond_out(b, td.rep, mb);
 }
@@ -873,16 +975,17 @@ int tile_setup() {
 }
 
 void launch_forces_tile(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles, int threads,
-                        bool next_keys, cudaStream_t s) {
+                        bool next_keys, cudaStream_t s, RowOut row) {
+    if (!next_keys) row.rep = -1;
     if (threads == 512) {
         const size_t bytes = sizeof(TileSmemT<512>);
-        if (next_keys) launch_pdl(k_forces_tile<true, 512>, ntiles, 512, bytes, s, b, cur, rep, tiles);
-        else k_forces_tile<false, 512><<<ntiles, 512, bytes, s>>>(b, cur, rep, tiles);
+        if (next_keys) launch_pdl(k_forces_tile<true, 512>, ntiles, 512, bytes, s, b, cur, rep, tiles, row);
+        else k_forces_tile<false, 512><<<ntiles, 512, bytes, s>>>(b, cur, rep, tiles, row);
         return;
     }
     const size_t bytes = sizeof(TileSmemT<256>);
-    if (next_keys) launch_pdl(k_forces_tile<true, 256>, ntiles, 256, bytes, s, b, cur, rep, tiles);
-    else k_forces_tile<false, 256><<<ntiles, 256, bytes, s>>>(b, cur, rep, tiles);
+    if (next_keys) launch_pdl(k_forces_tile<true, 256>, ntiles, 256, bytes, s, b, cur, rep, tiles, row);
+    else k_forces_tile<false, 256><<<ntiles, 256, bytes, s>>>(b, cur, rep, tiles, row);
 }
 
 void launch_forces_bulk(const Bufs &b, int cur, const RepDev *rep, const TileDesc *tiles, int ntiles,
