@@ -311,6 +311,16 @@ DPD_API int dpd_chemistry(dpd_handle *h, int64_t step);
  * dropped and reported as DPD_E_EVENT_OVERFLOW).  out == NULL only reports
  * the pending count in *n_out and clears nothing. */
 DPD_API int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out);
+/* dpd_get_events without waiting: enqueues on the handle's stream a copy of
+ * the events recorded since the last read into out (at most cap) and of
+ * their count into *n_out (all that were recorded: more than cap means the
+ * rest were dropped), then clears the log.  out and n_out must be pinned host
+ * memory the device can write (cudaHostAlloc, cudaHostRegister), else
+ * DPD_E_ARG; they are valid once the stream has passed this point.  A driver
+ * can read the events this way between steps without draining the stream.  No
+ * counterpart call in the reference, which appends events.csv inside its step
+ * loop (oercel.c:788-798). */
+DPD_API int dpd_events_async(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out);
 
 /* Observables of replica r (reference stats row, oercel.c:2364-2372):
  * out[0] T_kin = sum v^2 / (2N - 2) with v = vh + dt/2 f; out[1..2] total

@@ -360,3 +360,42 @@ def test_stats_ring_of_one_replica_in_a_batch(cuda_ok, rho):
             got[6] = 0
             assert np.array_equal(got, raw)
     a.stats_ring(1, None)
+
+
+def test_events_async_equal_get_events(cuda_ok):
+    """events read without a wait (dpd_events_async into pinned memory) are the
+    events dpd_get_events returns for a twin run, every 5 steps (as sets: the
+    order in which the device appends them may differ); a buffer too small
+    keeps some of them and reports the full count"""
+    import torch
+    p = params(L=24, seed=11, noise="philox", chem=1, n_chem=1, p_grow=0.05, p_bond=0.2, p_break=0.01, f_lip=0.3,
+               c_N=0.1)
+    a, b = ob.Engine(p), ob.Engine(p)
+    for e in (a, b):
+        e.load_soup(0)
+        e.prime()
+    cap = 4096
+    buf = torch.empty(cap * ob.Engine.EVENT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True).numpy()
+    buf = buf.view(ob.Engine.EVENT_DTYPE)
+    cnt = torch.zeros(1, dtype=torch.int32, pin_memory=True).numpy()
+    total = 0
+    for _ in range(4):
+        a.step(5)
+        want = a.events()
+        b.step_async(5)
+        b.events_async(buf, cnt)
+        b.sync()
+        assert int(cnt[0]) == len(want)
+        assert sorted(ob.Engine.event_tuples(buf, cnt[0])) == sorted(want)
+        total += len(want)
+    assert total > 0
+    a.step(5)
+    want = a.events()
+    assert len(want) > 2
+    b.step(5)
+    b.events_async(buf[:2], cnt)
+    b.sync()
+    got = ob.Engine.event_tuples(buf[:2], cnt[0])
+    assert int(cnt[0]) == len(want) and len(got) == 2 and set(got) <= set(want)
+    with pytest.raises(ob.DpdError, match="pinned"):
+        b.events_async(np.zeros(8, ob.Engine.EVENT_DTYPE), cnt)

@@ -1157,6 +1157,27 @@ extern "C" int dpd_get_events(dpd_handle *h, dpd_event *out, int32_t cap, int32_
     return DPD_OK;
 }
 
+// host memory the device can write through the same address (pinned, mapped)
+static bool device_writable_host(const void *p) {
+    cudaPointerAttributes pa;
+    const bool ok = cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost &&
+                    pa.devicePointer == p;
+    cudaGetLastError();
+    return ok;
+}
+
+extern "C" int dpd_events_async(dpd_handle *h, dpd_event *out, int32_t cap, int32_t *n_out) {
+    if (!h || !out || !n_out) return fail(DPD_E_ARG, "null argument");
+    if (cap < 1) return fail(DPD_E_ARG, "the event buffer needs room for at least one event");
+    static_assert(sizeof(dpd_event) == sizeof(EventDev), "dpd_event and the device log agree");
+    if (!device_writable_host(out) || !device_writable_host(n_out))
+        return fail(DPD_E_ARG, "the event buffer and its count must be pinned host memory the device can write "
+                               "(cudaHostAlloc, cudaHostRegister)");
+    launch_events_out(h->b, (EventDev *)out, cap, (int *)n_out, h->s);
+    CK(cudaGetLastError());
+    return DPD_OK;
+}
+
 // the sums of a stats row on the stream, copied into v (OBS_N words) when the
 // stream gets there: one kernel, whose last block hands the row over to obs_out
 // and clears the running sums (the max bond restarts per stats row), and one copy

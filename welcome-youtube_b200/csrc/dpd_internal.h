@@ -239,6 +239,7 @@ void launch_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, 
 void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_integrate(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s);
+void launch_events_out(const Bufs &b, EventDev *out, int cap, int *n_out, cudaStream_t s);
 void launch_mol_forces(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, cudaStream_t s);
 void launch_type_clusters(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch, int nbch, int rep_index, int t,
                           double rcut, int *parent, int *size, unsigned long long *acc, cudaStream_t s);

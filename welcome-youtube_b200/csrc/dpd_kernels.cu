@@ -1143,6 +1143,27 @@ void launch_halfkick(const Bufs &b, int cur, const RepDev *rep, const Chunk *bch
     k_halfkick<<<nbch, BEAD_TPB, 0, s>>>(b, cur, rep, bch);
 }
 
+// The event log read without a wait: the events recorded since the last read
+// are copied into the caller's host buffer (at most cap of them, the device can
+// write it), then k_events_done writes how many were recorded (cap exceeded
+// too) and clears the log.  Both run on the stream, after the steps before them.
+__global__ void k_events_out(const EventDev *__restrict__ ev, const DevStatus *__restrict__ st, int evcap,
+                             EventDev *__restrict__ out, int cap) {
+    const int m = min((int)min(st->nevents, (unsigned)evcap), cap);
+    for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < m; i += (int)(gridDim.x * blockDim.x))
+        out[i] = ev[i];
+}
+
+__global__ void k_events_done(DevStatus *__restrict__ st, int *__restrict__ n_out) {
+    *n_out = (int)st->nevents;
+    st->nevents = 0u;
+}
+
+void launch_events_out(const Bufs &b, EventDev *out, int cap, int *n_out, cudaStream_t s) {
+    k_events_out<<<16, 256, 0, s>>>(b.events, b.status, b.evcap, out, cap);
+    k_events_done<<<1, 1, 0, s>>>(b.status, n_out);
+}
+
 void launch_step_begin(const Bufs &b, int nrep, cudaStream_t s) {
     k_step_begin<<<1, 128, 0, s>>>(b.step, b.status, b.resort, nrep);
 }

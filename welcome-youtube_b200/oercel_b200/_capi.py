@@ -95,7 +95,7 @@ EXPORTS = [
     "dpd_last_error", "dpd_version", "dpd_params_default", "dpd_create", "dpd_destroy", "dpd_sizes",
     "dpd_set_state", "dpd_get_state", "dpd_set_dynamics", "dpd_prime", "dpd_resume", "dpd_get_step",
     "dpd_set_step", "dpd_step", "dpd_init_soup", "dpd_build_cells", "dpd_get_cells", "dpd_forces",
-    "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events",
+    "dpd_pair_forces", "dpd_bond_forces", "dpd_integrate", "dpd_chemistry", "dpd_get_events", "dpd_events_async",
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_window_adjoint_state",
@@ -167,6 +167,7 @@ def load(path: str | None = None):
         "dpd_integrate": ([vp], C.c_int),
         "dpd_chemistry": ([vp, i64], C.c_int),
         "dpd_get_events": ([vp, C.POINTER(DpdEvent), i32, C.POINTER(C.c_int32)], C.c_int),
+        "dpd_events_async": ([vp, vp, i32, vp], C.c_int),
         "dpd_observables": ([vp, i32, fp], C.c_int),
         "dpd_stats": ([vp, i32, fp], C.c_int),
         "dpd_set_tuning": ([vp, C.POINTER(DpdTuning)], C.c_int),

@@ -226,6 +226,27 @@ class Engine:
         check(self.lib.dpd_get_events(self.h, buf, cap, C.byref(n)))
         return [(e.step, e.kind, e.gid, e.partner, e.x, e.y, e.replica) for e in buf[: n.value]]
 
+    # a DpdEvent as a numpy record (the layout of dpd_event)
+    EVENT_DTYPE = np.dtype([("step", np.int64), ("kind", np.int32), ("gid", np.uint32), ("partner", np.uint32),
+                            ("x", np.float32), ("y", np.float32), ("replica", np.int32)])
+
+    def events_async(self, buf, count):
+        """enqueue a read of the events since the last read into buf (pinned
+        host memory with EVENT_DTYPE records, e.g. a numpy view of
+        torch.empty(..., pin_memory=True)) and their number into count (a
+        pinned int32 array of one element; more than len(buf) means the rest
+        were dropped); both are valid once the stream has passed this point
+        (sync, or an event recorded after it).  Nothing waits."""
+        assert buf.dtype == self.EVENT_DTYPE and buf.ndim == 1 and buf.flags.c_contiguous
+        assert count.dtype == np.int32 and count.size >= 1 and count.flags.c_contiguous
+        check(self.lib.dpd_events_async(self.h, buf.ctypes.data, int(buf.shape[0]), count.ctypes.data))
+
+    @staticmethod
+    def event_tuples(buf, n):
+        """records of an events_async read as (step, kind, gid, partner gid, x, y, replica), like events()"""
+        return [(int(e["step"]), int(e["kind"]), int(e["gid"]), int(e["partner"]), float(e["x"]), float(e["y"]),
+                 int(e["replica"])) for e in buf[:min(int(n), len(buf))]]
+
     def observables(self, replica=0, virial=True):
         o = np.zeros(16)
         f = self.lib.dpd_observables if virial else self.lib.dpd_stats
