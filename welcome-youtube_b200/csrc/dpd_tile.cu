@@ -22,8 +22,11 @@
 //
 // Epilogue per owned bead: harmonic bonds to prev/next, the force written to
 // HBM, and the cell of the next position with its count (the first half of
-// the next step's sort).  A tile whose beads do not fit in shared memory
-// computes its owned beads straight from HBM instead (bead_pairs_direct).
+// the next step's sort).  When the step's stats row is wanted (the stats ring),
+// the epilogue also sums the row's terms of the beads it holds, and the last
+// CTA hands the row over (RowAcc, row_handover).  A tile whose beads do not
+// fit in shared memory computes its owned beads straight from HBM instead
+// (bead_pairs_direct).
 #include <algorithm>
 
 #include "dpd_device.cuh"
