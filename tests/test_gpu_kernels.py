@@ -329,14 +329,17 @@ def test_stats_ring_rows_equal_stats_async(cuda_ok):
     assert max(int(r[6]) for r in ring) == 12  # no row after the ring was stopped
 
 
-@pytest.mark.parametrize("rho", [4, 7])
-def test_stats_ring_of_one_replica_in_a_batch(cuda_ok, rho):
+@pytest.mark.parametrize("rho,chem", [(4, 0), (7, 0), (4, 1)])
+def test_stats_ring_of_one_replica_in_a_batch(cuda_ok, rho, chem):
     """the tile force kernel assembles the ring's row itself: replica 1 of a
     two-box engine gives the rows that dpd_stats_async gives for it; at rho 7 the
     14 x 14 tiles hold more beads than shared memory does and take the direct
-    path"""
+    path; with the lipid chemistry every step the types and chains change under
+    the rows"""
     import torch
-    ps = [params(L=24, seed=6, rho=rho), params(L=20, seed=7, rho=rho)]
+    kv = dict(noise="philox", chem=1, n_chem=1, p_grow=0.05, p_bond=0.2, p_break=0.01, f_lip=0.3, c_N=0.1) \
+        if chem else {}
+    ps = [params(L=24, seed=6, rho=rho, **kv), params(L=20, seed=7, rho=rho, **kv)]
     ns = [p.n_beads() for p in ps]
     a, b = ob.Engine(ps, n_beads=ns), ob.Engine(ps, n_beads=ns)
     for e in (a, b):
