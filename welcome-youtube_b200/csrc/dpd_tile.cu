@@ -15,10 +15,11 @@
 // (lx, ly) its half-shell partners are two contiguous index ranges of the
 // local arrays: the rest of its own cell plus the cell above, and cells
 // ly-1..ly+1 of the next column.  A lane owns one source and walks its two
-// ranges; hits (r < 1) go through a warp ballot into a per-warp queue, which
-// is drained 64 pairs at a time (two per lane), so the noise and force
-// arithmetic always runs on full warps.  Halo sources only pair with owned
-// beads: their ranges are clipped to the owned rows of the column.
+// ranges, four candidates a round; hits (r < 1) go through a warp ballot into
+// a per-warp queue, which is drained 64 pairs at a time (two per lane), so the
+// noise and force arithmetic always runs on full warps.  Halo sources only
+// pair with owned beads: their ranges are clipped to the owned rows of the
+// column.
 //
 // Epilogue per owned bead: harmonic bonds to prev/next, the force written to
 // HBM, and the cell of the next position with its count (the first half of
@@ -35,7 +36,7 @@
 #define TILE_WARPS (TILE_TPB / 32)
 #define TILE_MAXB 1408
 #define TILE_MAXC 256
-#define TILE_QCAP 128  // per-warp queue; < 64 entries wait between drains, at most 64 arrive per round
+#define TILE_QCAP 192  // per-warp queue; < 64 entries wait between drains, at most 128 arrive per round
 
 // one tile's staged beads and their local layout, for tiles of up to MAXC local
 // cells (tile and halo) and MAXB beads
@@ -53,9 +54,10 @@ struct __align__(16) TileBeadT {
     int32_t gst[MAXC];            // global slot of each local cell's first bead
     float a[DPD_MAXT * DPD_MAXT];
     int32_t n;
-    // The screen reads pos[t] and img[t] for t < 2 MAXB (past a range's end,
-    // masked out): pos is followed by vt, and img by at least MAXB bytes.
-    static_assert((MAXC + 1) * 4 + MAXC * 4 >= MAXB, "img must be followed by MAXB bytes of the tile");
+    // The screen reads pos[t] and img[t] for t <= 2 MAXB + 2 (past a range's
+    // end, masked out): pos is followed by vt and tg, and img by at least
+    // MAXB + 8 bytes.
+    static_assert((MAXC + 1) * 4 + MAXC * 4 >= MAXB + 8, "img must be followed by MAXB + 8 bytes of the tile");
 };
 using TileBead = TileBeadT<TILE_MAXB, TILE_MAXC>;
 
@@ -221,15 +223,15 @@ __device__ void tile_pairs(TB &S, uint32_t *q, int *next_chunk, int first, const
             len = src_ranges(S, s, v, LH, tw, th, r1s, len1, s2m);
         }
         const int maxlen = __reduce_max_sync(0xffffffffu, len);
-        for (int k = 0; k < maxlen; k += 2) {
-            bool hit[2];
-            int tt[2];
+        for (int k = 0; k < maxlen; k += 4) {
+            bool hit[4];
+            int tt[4];
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < 4; u++) {
                 const int kk = k + u;
                 const int t = kk + (kk < len1 ? r1s : s2m);
                 tt[u] = t;
-                const int tc = t;  // past the end (t < 2 MAXB): an in-bounds read, masked out below
+                const int tc = t;  // past the end (t <= 2 MAXB + 2): an in-bounds read, masked out below
                 const float2 pt = S.pos[tc];
                 float dx = __fsub_rn(ps.x, pt.x), dy = __fsub_rn(ps.y, pt.y);
                 if (WRAP) {
@@ -241,19 +243,23 @@ __device__ void tile_pairs(TB &S, uint32_t *q, int *next_chunk, int first, const
                 hit[u] = kk < len && r2 < 1.0f && r2 > 1e-24f;
             }
 #pragma unroll
-            for (int u = 0; u < 2; u++) {
+            for (int u = 0; u < 4; u++) {
                 const uint32_t hm = __ballot_sync(0xffffffffu, hit[u]);
                 if (hit[u]) q[tail + __popc(hm & below)] = ((uint32_t)s << 16) | (uint32_t)tt[u];
                 tail += __popc(hm);
             }
-            if (tail >= 64) {  // uniform over the warp
+            while (tail >= 64) {  // uniform over the warp
                 __syncwarp();
                 drain<WRAP, NOISE>(S, pc, q, 64, lane, fmax);
-                // move the rest, fewer than 64, to the front
+                // move the rest, fewer than 128, to the front (all read before any is written)
                 const int rest = tail - 64;
-                const uint32_t m1 = q[64 + lane], m2 = q[96 + lane];
-                if (lane < rest) q[lane] = m1;
-                if (lane + 32 < rest) q[lane + 32] = m2;
+                uint32_t m[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) m[e] = 64 + lane + 32 * e < 192 ? q[64 + lane + 32 * e] : 0u;
+                __syncwarp();
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    if (lane + 32 * e < rest) q[lane + 32 * e] = m[e];
                 tail = rest;
                 __syncwarp();
             }
