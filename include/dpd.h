@@ -470,6 +470,27 @@ DPD_API int dpd_window_adjoint(dpd_handle *h, int64_t nsteps, int32_t ckpt_every
 DPD_API int dpd_window_adjoint_state(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
                                      const double *target, double *loss, double *grad, double *rdf_out, float *xbar,
                                      float *vhbar, float *vtbar);
+/* A fit of repulsions shared by every replica, run as one captured CUDA graph
+ * replayed iters times: each iteration is the differentiated window of
+ * dpd_window_adjoint (nsteps, ckpt_every, spec, target as there), its loss
+ * and gradient computed on the device, the gradient of the fitted a_ij summed
+ * over the replicas, and an Adam step (as torch.optim.Adam takes it, without
+ * weight decay) that sets a_ij = a_ji in every replica.  The replicas continue
+ * from the end of each window.  No host step comes between the iterations.
+ * slot[k] = i * 8 + j (i <= j) names the fitted entries; they must start equal
+ * in every replica.  Outputs (any may be NULL): loss (iters x nrep), grad
+ * (iters x n, the summed gradient) and values ((iters + 1) x n: the values
+ * each window ran with, then the last values).  Afterwards the handle holds
+ * the last values, as if set by dpd_set_params.  No counterpart in the reference (it has no reverse mode). */
+typedef struct {
+    int32_t n, pad;
+    int32_t slot[64];
+    double lr, beta1, beta2, eps;
+} dpd_fit_spec;
+DPD_API int dpd_fit_graph(dpd_handle *h, int64_t nsteps, int32_t ckpt_every, const dpd_rdf_spec *spec,
+                          const double *target, const dpd_fit_spec *fit, int32_t iters, double *loss, double *grad,
+                          double *values);
+
 /* Vector-Jacobian product of the forces of replica r's current configuration
  * at `step` (noise key and kT(t)): pair terms, bonds and angle terms (linear
  * chains and the templates of the branched shapes) and stirring.  Given the

@@ -430,3 +430,46 @@ def test_batched_fit_moves_the_shared_repulsion(cuda_ok):
     hist = fit.fit(e, ["a_W_T"], target, iters=6, window=60, ckpt=20, spec=spec, lr=2.0)
     assert hist[-1]["values"][0] > 60.0
     assert all(np.isfinite(h["loss"]) for h in hist)
+
+
+def test_fit_graph_equals_the_eager_fit(cuda_ok):
+    """dpd_fit_graph (windows, losses, gradients and Adam steps all on the
+    device, one captured iteration replayed) against the same fit driven from
+    the host: window_adjoint per iteration, the replicas' gradients summed, the
+    Adam step of torch.optim.Adam in numpy, set_params"""
+    def boxes():  # each engine its own parameter objects
+        return [params(L=12.0, seed=41, noise="philox", f_lip=0.3, c_N=0.1, a_W_T=60.0),
+                params(L=10.0, seed=42, noise="philox", f_lip=0.2, c_N=0.1, a_W_T=60.0)]
+    ns = [p.n_beads() for p in boxes()]
+    a, b = ob.Engine(boxes(), n_beads=ns), ob.Engine(boxes(), n_beads=ns)
+    for e in (a, b):
+        for r in range(2):
+            e.load_soup(r)
+        e.prime()
+        e.step(20)
+    spec = ob.Engine.rdf_spec(ta=2, tb=2, nbin=32, rmax=2.0, sigma=0.1, last_steps=4)
+    target = np.linspace(0.5, 1.5, 32)
+    nsteps, ckpt, iters, lr = 10, 5, 3, 0.5
+    loss_g, grad_g, vals_g = a.fit_graph(["a_W_T"], nsteps, ckpt, spec, target, iters, lr=lr)
+    b1, b2, eps = 0.9, 0.999, 1e-8
+    val, m, v = 60.0, 0.0, 0.0
+    for it in range(iters):
+        assert vals_g[it, 0] == pytest.approx(val, rel=1e-9)
+        loss, grad, _ = b.window_adjoint(nsteps, ckpt, spec, target)
+        g = float(grad[0][2] + grad[1][2])
+        tol = 1e-9 if it == 0 else 1e-4  # (later windows start from values equal to rounding)
+        assert loss_g[it] == pytest.approx(loss, rel=tol)
+        assert grad_g[it, 0] == pytest.approx(g, rel=max(tol, 1e-9))
+        t = it + 1
+        m = m + (1 - b1) * (g - m)
+        v = b2 * v + (1 - b2) * g * g
+        val = val - lr / (1 - b1 ** t) * m / (np.sqrt(v) / np.sqrt(1 - b2 ** t) + eps)
+        for r in range(2):
+            p = b.params[r]
+            p.a[0][2] = p.a[2][0] = val
+            b.set_params(r, p)
+    assert vals_g[iters, 0] == pytest.approx(val, rel=1e-6)
+    assert a.params[0].a[0][2] == vals_g[iters, 0]
+    assert a.step_no == b.step_no
+    sa, sb = a.state(0), b.state(0)
+    assert np.allclose(sa["x"], sb["x"], atol=1e-3)

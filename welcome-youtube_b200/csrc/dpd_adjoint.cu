@@ -131,7 +131,9 @@ __global__ void __launch_bounds__(BEAD_TPB) k_gsum(const RepDev *__restrict__ re
 __global__ void __launch_bounds__(BEAD_TPB) k_force_vjp(StateView sv, long long step, const RepDev *__restrict__ reps,
                                                         const Chunk *__restrict__ ch, const float2 *__restrict__ g,
                                                         float2 *__restrict__ xbar, float2 *__restrict__ vbar,
-                                                        double *__restrict__ grad, const double *__restrict__ gsum) {
+                                                        double *__restrict__ grad, const double *__restrict__ gsum,
+                                                        const long long *__restrict__ step_base) {
+    if (step_base) step += *step_base;  // the step relative to a step number kept on the device
     __shared__ double sgrad[NGRAD];
     for (int k = threadIdx.x; k < NGRAD; k += blockDim.x) sgrad[k] = 0.0;
     __syncthreads();
@@ -437,12 +439,12 @@ __global__ void __launch_bounds__(BEAD_TPB) k_mol_vjp(StateView sv, const RepDev
 
 void launch_force_vjp(const StateView &sv, long long step, const RepDev *rep, const Chunk *bch, int nbch,
                       const float2 *g, float2 *xbar, float2 *vbar, double *grad, double *gsum, int nrep, bool stir,
-                      const dpd_template *mol, cudaStream_t s) {
+                      const dpd_template *mol, cudaStream_t s, const long long *step_base) {
     if (stir) {
         cudaMemsetAsync(gsum, 0, (size_t)nrep * sizeof(double), s);
         k_gsum<<<nbch, BEAD_TPB, 0, s>>>(rep, bch, g, gsum);
     }
-    k_force_vjp<<<nbch, BEAD_TPB, 0, s>>>(sv, step, rep, bch, g, xbar, vbar, grad, gsum);
+    k_force_vjp<<<nbch, BEAD_TPB, 0, s>>>(sv, step, rep, bch, g, xbar, vbar, grad, gsum, step_base);
     if (mol) k_mol_vjp<<<nbch, BEAD_TPB, 0, s>>>(sv, rep, bch, mol, g, xbar, grad);
 }
 
@@ -476,4 +478,100 @@ void launch_adj_state(const uint32_t *tg, const RepDev *rep, const Chunk *bch, i
 void launch_adj_save(int n, const float2 *pos, const float2 *vt, const uint32_t *tg, const int2 *link, float2 *opos,
                      float2 *ovt, uint32_t *otg, int2 *olink, cudaStream_t s) {
     k_adj_save<<<(n + 255) / 256, 256, 0, s>>>(n, pos, vt, tg, link, opos, ovt, otg, olink);
+}
+
+// ---------------------------------------------------------------- a fit iteration without the host
+//
+// dpd_fit_graph captures one optimizer iteration (the window, its adjoint, the
+// loss and the parameter update) as a CUDA graph and replays it: every value
+// that changes from one iteration to the next lives on the device (FitDev).
+
+__global__ void k_fit_begin(const long long *__restrict__ step, FitDev *__restrict__ fd) { fd->base = *step; }
+
+__global__ void k_set_step_rel(long long *__restrict__ step, const FitDev *__restrict__ fd, long long off) {
+    *step = fd->base + off;
+}
+
+// The smoothed-RDF loss of each replica (one block each) and the weights dL/dh
+// of its bins, as the host computes them for dpd_window_adjoint:
+// g = h / last_steps * L^2 / (npairs 2 pi r_b dr), loss = mean over bins of
+// (g - target)^2, w = 2 (g - target) / nbin * L^2 / (npairs 2 pi r_b dr) / last_steps.
+// The loss goes to loss_out[iter * nrep + replica].
+__global__ void k_rdf_loss(const RepDev *__restrict__ reps, const double *__restrict__ hist,
+                           const long long *__restrict__ npairs, const double *__restrict__ target, int nbin,
+                           double rmax, int last_steps, double *__restrict__ loss_out, double *__restrict__ wgt,
+                           const FitDev *__restrict__ fd) {
+    __shared__ double red[32];
+    const int r = (int)blockIdx.x, nrep = (int)gridDim.x;
+    const double L = (double)reps[r].L, area = L * L, dr = rmax / nbin;
+    const long long np = npairs[r];
+    double sum = 0.0;
+    for (int b = (int)threadIdx.x; b < nbin; b += (int)blockDim.x) {
+        const double rb = (b + 0.5) * dr;
+        const double norm = np > 0 ? area / ((double)np * 2.0 * M_PI * rb * dr) : 0.0;
+        const double g = hist[(size_t)r * nbin + b] / last_steps * norm;
+        const double e = g - target[(size_t)r * nbin + b];
+        sum += e * e;
+        wgt[(size_t)r * nbin + b] = 2.0 * e / nbin * norm / last_steps;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+    if (lane_id() == 0) red[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        loss_out[(size_t)fd->iter * nrep + r] = t / nbin;
+    }
+}
+
+// The optimizer step of the shared a_ij (one thread per fitted slot): the
+// gradient summed over the replicas in replica order, then Adam as
+// torch.optim.Adam takes it (no weight decay): m += (1 - b1)(g - m),
+// v = b2 v + (1 - b2) g^2, a -= lr / (1 - b1^t) m / (sqrt(v) / sqrt(1 - b2^t) + eps).
+// The new value goes into a_ij and a_ji of every replica; the gradient and the
+// value the window ran with go to grad_out / value_out[iter * nfit + k].
+__global__ void k_fit_update(RepDev *__restrict__ reps, int nrep, const double *__restrict__ grad,
+                             FitDev *__restrict__ fd, double *__restrict__ grad_out, double *__restrict__ value_out) {
+    const int k = (int)threadIdx.x, it = fd->iter;
+    if (k < fd->nfit) {
+        const int slot = fd->slot[k];
+        double g = 0.0;
+        for (int r = 0; r < nrep; r++) g += grad[(size_t)r * NGRAD + slot];
+        const double t = (double)(it + 1);
+        const double m = fd->m[k] + (1.0 - fd->beta1) * (g - fd->m[k]);
+        const double v = fd->beta2 * fd->v[k] + (1.0 - fd->beta2) * g * g;
+        fd->m[k] = m;
+        fd->v[k] = v;
+        const double bc1 = 1.0 - pow(fd->beta1, t), bc2 = 1.0 - pow(fd->beta2, t);
+        const double denom = sqrt(v) / sqrt(bc2) + fd->eps;
+        const double val = fd->value[k] - fd->lr / bc1 * m / denom;
+        grad_out[(size_t)it * fd->nfit + k] = g;
+        value_out[(size_t)it * fd->nfit + k] = fd->value[k];
+        fd->value[k] = val;
+        const int i = slot / DPD_MAXT, j = slot % DPD_MAXT;
+        for (int r = 0; r < nrep; r++) {
+            reps[r].a[i * DPD_MAXT + j] = (float)val;
+            reps[r].a[j * DPD_MAXT + i] = (float)val;
+        }
+    }
+    __syncthreads();
+    if (k == 0) fd->iter = it + 1;
+}
+
+void launch_fit_begin(long long *step, FitDev *fd, cudaStream_t s) { k_fit_begin<<<1, 1, 0, s>>>(step, fd); }
+
+void launch_set_step_rel(long long *step, const FitDev *fd, long long off, cudaStream_t s) {
+    k_set_step_rel<<<1, 1, 0, s>>>(step, fd, off);
+}
+
+void launch_rdf_loss(const RepDev *rep, int nrep, const double *hist, const long long *npairs, const double *target,
+                     int nbin, double rmax, int last_steps, double *loss_out, double *wgt, const FitDev *fd,
+                     cudaStream_t s) {
+    k_rdf_loss<<<nrep, 256, 0, s>>>(rep, hist, npairs, target, nbin, rmax, last_steps, loss_out, wgt, fd);
+}
+
+void launch_fit_update(RepDev *rep, int nrep, const double *grad, FitDev *fd, double *grad_out, double *value_out,
+                       cudaStream_t s) {
+    k_fit_update<<<1, DPD_MAXT * DPD_MAXT, 0, s>>>(rep, nrep, grad, fd, grad_out, value_out);
 }

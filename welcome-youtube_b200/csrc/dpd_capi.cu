@@ -1644,6 +1644,201 @@ extern "C" int dpd_window_adjoint_state(dpd_handle *h, int64_t nsteps, int32_t c
     return window_impl(h, nsteps, ckpt_every, spec, target, loss, grad, rdf_out, true, out);
 }
 
+// ---------------------------------------------------------------- a fit as one captured graph
+//
+// One optimizer iteration of a shared-a_ij fit, enqueued without any host
+// step: the window (full checkpoints every ckpt steps), the loss and its bin
+// weights (k_rdf_loss), the reverse pass (the steps relative to the window's
+// first, kept on the device), and the update (k_fit_update).  The iteration
+// ends with the window's last state in the buffers of the parity it started
+// from, so the captured graph can be replayed for the next iteration.
+struct FitArgs {
+    int64_t nsteps;
+    int ckpt, nseg, nb;
+    const dpd_rdf_spec *spec;
+    FitDev *fd;
+    const long long *npairs;
+    const double *target;
+    double *loss, *grad, *value;  // iters x nrep, iters x nfit, iters x nfit
+};
+
+static void enqueue_fit_iteration(dpd_handle *h, AdjBufs &A, const FitArgs &a) {
+    const dpd_rdf_spec *spec = a.spec;
+    const int nb = a.nb, ckpt = a.ckpt, nseg = a.nseg;
+    const int64_t nsteps = a.nsteps;
+    const float rmax = (float)spec->rmax, sig = (float)spec->sigma;
+    const int cur0 = h->cur;
+    launch_fit_begin(h->b.step, a.fd, h->s);
+    cudaMemsetAsync(A.hist, 0, (size_t)h->nrep * nb * sizeof(double), h->s);
+    enqueue_next_keys(h);
+    const int64_t first_loss = nsteps - spec->last_steps + 1;
+    for (int64_t k = 1; k <= nsteps; k++) {
+        if ((k - 1) % ckpt == 0) ck_save(h, A.ck[(k - 1) / ckpt]);
+        enqueue_plain_step(h);
+        if (k >= first_loss) launch_rdf(view_cur(h), h->d_rep, h->d_bch, h->nbch, spec->ta, spec->tb, nb, rmax, sig, A.hist, h->s);
+    }
+    const FullCk &end = A.ck[nseg];
+    ck_save(h, end);
+    launch_rdf_loss(h->d_rep, h->nrep, A.hist, a.npairs, a.target, nb, spec->rmax, spec->last_steps, a.loss, A.wgt,
+                    a.fd, h->s);
+    const size_t N = (size_t)h->N;
+    cudaMemsetAsync(A.X, 0, N * sizeof(float2), h->s);
+    cudaMemsetAsync(A.V, 0, N * sizeof(float2), h->s);
+    cudaMemsetAsync(A.F, 0, N * sizeof(float2), h->s);
+    cudaMemsetAsync(A.grad, 0, (size_t)h->nrep * DPD_NGRAD * sizeof(double), h->s);
+    const long long *base = &a.fd->base;
+    const int64_t k_stop = spec->horizon > 0 ? std::max<int64_t>(0, first_loss - 1 - spec->horizon) : 0;
+    const int sg_stop = (int)(k_stop / ckpt);
+    int stop_slot = 0;
+    const dpd_template *mol = h->any_mol ? h->b.mol : nullptr;
+    for (int sg = nseg - 1; sg >= sg_stop; sg--) {
+        const int64_t k0 = (int64_t)sg * ckpt;
+        const int len = (int)std::min<int64_t>(ckpt, nsteps - k0);
+        ck_restore(h, A.ck[sg]);
+        launch_set_step_rel(h->b.step, a.fd, k0, h->s);
+        enqueue_next_keys(h);
+        seg_save(h, A.seg[0]);
+        for (int s = 1; s <= len; s++) {
+            enqueue_plain_step(h);
+            seg_save(h, A.seg[s]);
+        }
+        const int s_low = sg == sg_stop ? (int)(k_stop - k0) : 0;
+        stop_slot = s_low;
+        for (int s = len; s > s_low; s--) {
+            const int64_t k = k0 + s;
+            const StateView v = view_of(A.seg[s]);
+            if (k >= first_loss)
+                launch_rdf_vjp(v, h->d_rep, h->d_bch, h->nbch, spec->ta, spec->tb, nb, rmax, sig, A.wgt, A.X, h->s);
+            launch_adj_gather(v.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
+            launch_force_vjp(v, k, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, A.gsum, h->nrep, h->any_stir,
+                             mol, h->s, base);
+            launch_adj_update(v.tg, h->d_rep, h->d_bch, h->nbch, A.xb, A.vb, A.X, A.V, A.F, h->s);
+        }
+    }
+    const StateView v0 = view_of(A.seg[stop_slot]);
+    launch_adj_gather(v0.tg, h->d_rep, h->d_bch, h->nbch, A.F, A.g, h->s);
+    launch_force_vjp(v0, k_stop, h->d_rep, h->d_bch, h->nbch, A.g, A.xb, A.vb, A.grad, A.gsum, h->nrep, h->any_stir,
+                     mol, h->s, base);
+    // the window's end into the starting parity's buffers, the step after the window
+    h->cur = cur0;
+    ck_restore(h, end);
+    launch_set_step_rel(h->b.step, a.fd, nsteps, h->s);
+    launch_fit_update(h->d_rep, h->nrep, A.grad, a.fd, a.grad, a.value, h->s);
+}
+
+extern "C" int dpd_fit_graph(dpd_handle *h, int64_t nsteps, int32_t ckpt, const dpd_rdf_spec *spec,
+                             const double *target, const dpd_fit_spec *fit, int32_t iters, double *loss, double *grad,
+                             double *values) {
+    TRY(check_window(h, nsteps, spec, target));
+    if (!fit || fit->n < 1 || fit->n > DPD_MAXT * DPD_MAXT) return fail(DPD_E_ARG, "fit: 1 to 64 slots");
+    if (iters < 1) return fail(DPD_E_ARG, "fit: at least one iteration");
+    if (!(fit->lr > 0.0) || !(fit->beta1 >= 0.0 && fit->beta1 < 1.0) || !(fit->beta2 >= 0.0 && fit->beta2 < 1.0) ||
+        !(fit->eps > 0.0))
+        return fail(DPD_E_ARG, "fit: lr > 0, 0 <= beta < 1, eps > 0");
+    FitDev F;
+    std::memset(&F, 0, sizeof F);
+    F.nfit = fit->n;
+    F.lr = fit->lr;
+    F.beta1 = fit->beta1;
+    F.beta2 = fit->beta2;
+    F.eps = fit->eps;
+    for (int k = 0; k < fit->n; k++) {
+        const int s = fit->slot[k], i = s / DPD_MAXT, j = s % DPD_MAXT;
+        if (s < 0 || s >= DPD_MAXT * DPD_MAXT || i > j)
+            return fail(DPD_E_ARG, "fit: slot %d is not i * 8 + j with i <= j", s);
+        for (int q = 0; q < k; q++)
+            if (fit->slot[q] == s) return fail(DPD_E_ARG, "fit: slot %d twice", s);
+        F.slot[k] = s;
+        F.value[k] = h->params[0].a[s];
+        for (int r = 1; r < h->nrep; r++)
+            if (h->params[r].a[s] != F.value[k])
+                return fail(DPD_E_ARG, "fit: a shared slot (%d) must start equal in every replica", s);
+    }
+    if (ckpt < 1) ckpt = (int32_t)nsteps;
+    const int nseg = (int)((nsteps + ckpt - 1) / ckpt), nb = spec->nbin, nrep = h->nrep;
+    std::vector<long long> npairs;
+    TRY(count_pairs(h, spec, npairs));
+    AdjBufs A;
+    TRY(adj_setup(h, nseg + 1, ckpt + 1, nb, A));
+    // the fit's own device memory, freed before returning
+    char *mem = nullptr;
+    const size_t o_np = ((sizeof(FitDev) + 255) / 256) * 256, o_tg = o_np + (((size_t)nrep * 8 + 255) / 256) * 256;
+    const size_t o_loss = o_tg + (((size_t)nrep * nb * 8 + 255) / 256) * 256;
+    const size_t o_grad = o_loss + (((size_t)iters * nrep * 8 + 255) / 256) * 256;
+    const size_t o_val = o_grad + (((size_t)iters * fit->n * 8 + 255) / 256) * 256;
+    const size_t total = o_val + (((size_t)iters * fit->n * 8 + 255) / 256) * 256;
+    if (cudaMalloc(&mem, total) != cudaSuccess) return fail(DPD_E_NOMEM, "cudaMalloc(%zu) for the fit", total);
+    FitArgs a;
+    a.nsteps = nsteps;
+    a.ckpt = ckpt;
+    a.nseg = nseg;
+    a.nb = nb;
+    a.spec = spec;
+    a.fd = (FitDev *)mem;
+    a.npairs = (const long long *)(mem + o_np);
+    a.target = (const double *)(mem + o_tg);
+    a.loss = (double *)(mem + o_loss);
+    a.grad = (double *)(mem + o_grad);
+    a.value = (double *)(mem + o_val);
+    int rc = DPD_OK;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    const int cur0 = h->cur;
+    do {
+        if (cudaMemcpy(mem, &F, sizeof F, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(mem + o_np, npairs.data(), nrep * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(mem + o_tg, target, (size_t)nrep * nb * sizeof(double), cudaMemcpyDefault) != cudaSuccess) {
+            rc = fail(DPD_E_CUDA, "fit: copies to the device: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (cudaStreamSynchronize(h->s) != cudaSuccess ||
+            cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            rc = fail(DPD_E_CUDA, "fit: capture: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        enqueue_fit_iteration(h, A, a);
+        const cudaError_t e = cudaStreamEndCapture(h->s, &g);
+        h->cur = cur0;
+        if (e != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
+            rc = fail(DPD_E_CUDA, "fit: graph: %s", cudaGetErrorString(e != cudaSuccess ? e : cudaGetLastError()));
+            break;
+        }
+        for (int it = 0; it < iters && rc == DPD_OK; it++)
+            if (cudaGraphLaunch(ge, h->s) != cudaSuccess) rc = fail(DPD_E_CUDA, "fit: launch");
+        if (rc != DPD_OK) break;
+        if (cudaStreamSynchronize(h->s) != cudaSuccess) {
+            rc = fail(DPD_E_CUDA, "fit: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if ((rc = check_status(h)) != DPD_OK) break;
+        FitDev out;
+        if (cudaMemcpy(&out, mem, sizeof out, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            (loss && cudaMemcpy(loss, a.loss, (size_t)iters * nrep * 8, cudaMemcpyDefault) != cudaSuccess) ||
+            (grad && cudaMemcpy(grad, a.grad, (size_t)iters * fit->n * 8, cudaMemcpyDefault) != cudaSuccess) ||
+            (values && cudaMemcpy(values, a.value, (size_t)iters * fit->n * 8, cudaMemcpyDefault) != cudaSuccess)) {
+            rc = fail(DPD_E_CUDA, "fit: copies from the device");
+            break;
+        }
+        if (values)
+            for (int k = 0; k < fit->n; k++) values[(size_t)iters * fit->n + k] = out.value[k];
+        // the host's view of the handle: the steps taken, the fitted values in every replica
+        h->step += (int64_t)iters * nsteps;
+        h->keys_valid = false;
+        for (int r = 0; r < nrep && rc == DPD_OK; r++) {
+            dpd_params p = h->params[r];
+            for (int k = 0; k < fit->n; k++) {
+                const int s = fit->slot[k], i = s / DPD_MAXT, j = s % DPD_MAXT;
+                p.a[i * DPD_MAXT + j] = p.a[j * DPD_MAXT + i] = out.value[k];
+            }
+            rc = dpd_set_params(h, r, &p);
+        }
+    } while (false);
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    cudaFree(mem);
+    return rc;
+}
+
 extern "C" int dpd_force_vjp(dpd_handle *h, int32_t r, int64_t step, const float *gx, const float *gy, float *xbar_x,
                              float *xbar_y, float *vbar_x, float *vbar_y, double *grad) {
     TRY(ensure_replica(h, r));

@@ -279,7 +279,23 @@ void launch_forces_bulk(const Bufs &b, int cur, const RepDev *rep, const TileDes
 // mol: the replicas' lipid templates when some replica has branched lipids, else null
 void launch_force_vjp(const StateView &sv, long long step, const RepDev *rep, const Chunk *bch, int nbch,
                       const float2 *g, float2 *xbar, float2 *vbar, double *grad, double *gsum, int nrep, bool stir,
-                      const dpd_template *mol, cudaStream_t s);
+                      const dpd_template *mol, cudaStream_t s, const long long *step_base = nullptr);
+// the device side of a fit iteration that runs without the host (dpd_fit_graph); FitDev is in device memory
+struct FitDev {
+    long long base;             // the device step at the start of the iteration's window
+    int iter;                   // iterations done
+    int nfit;                   // fitted a_ij slots (i * DPD_MAXT + j, i <= j), shared by every replica
+    int slot[DPD_MAXT * DPD_MAXT];
+    double value[DPD_MAXT * DPD_MAXT], m[DPD_MAXT * DPD_MAXT], v[DPD_MAXT * DPD_MAXT];
+    double lr, beta1, beta2, eps;
+};
+void launch_fit_begin(long long *step, FitDev *fd, cudaStream_t s);
+void launch_set_step_rel(long long *step, const FitDev *fd, long long off, cudaStream_t s);
+void launch_rdf_loss(const RepDev *rep, int nrep, const double *hist, const long long *npairs, const double *target,
+                     int nbin, double rmax, int last_steps, double *loss_out, double *wgt, const FitDev *fd,
+                     cudaStream_t s);
+void launch_fit_update(RepDev *rep, int nrep, const double *grad, FitDev *fd, double *grad_out, double *value_out,
+                       cudaStream_t s);
 void launch_rdf(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,
                 float rmax, float sigma, double *hist, cudaStream_t s);
 void launch_rdf_vjp(const StateView &sv, const RepDev *rep, const Chunk *bch, int nbch, int ta, int tb, int nbin,

@@ -69,6 +69,11 @@ class DpdTuning(C.Structure):
                 ("graph_steps", C.c_int32), ("sort_mode", C.c_int32), ("tile_threads", C.c_int32)]
 
 
+class DpdFitSpec(C.Structure):
+    _fields_ = [("n", C.c_int32), ("pad", C.c_int32), ("slot", C.c_int32 * 64), ("lr", C.c_double),
+                ("beta1", C.c_double), ("beta2", C.c_double), ("eps", C.c_double)]
+
+
 class DpdRdfSpec(C.Structure):
     _fields_ = [("ta", C.c_int32), ("tb", C.c_int32), ("nbin", C.c_int32), ("last_steps", C.c_int32),
                 ("rmax", C.c_double), ("sigma", C.c_double), ("horizon", C.c_int32), ("pad", C.c_int32)]
@@ -99,6 +104,7 @@ EXPORTS = [
     "dpd_observables", "dpd_pair_hist", "dpd_get_stream", "dpd_kernels_per_step", "dpd_step_async",
     "dpd_sync", "dpd_set_graph_steps", "dpd_profile_step", "dpd_stats", "dpd_set_tuning", "dpd_get_tuning",
     "dpd_sort_cells_noalloc", "dpd_set_params", "dpd_window_loss", "dpd_window_adjoint", "dpd_window_adjoint_state",
+    "dpd_fit_graph",
     "dpd_force_vjp",
     "dpd_set_rng", "dpd_get_rng", "dpd_lipid_template", "dpd_type_clusters", "dpd_xoshiro_jump",
     "dpd_aggregates", "dpd_stats_async", "dpd_stats_decode", "dpd_stats_ring", "dpd_cells_default",
@@ -177,6 +183,7 @@ def load(path: str | None = None):
         "dpd_window_loss": ([vp, i64, C.POINTER(DpdRdfSpec), fp, fp, fp], C.c_int),
         "dpd_window_adjoint": ([vp, i64, i32, C.POINTER(DpdRdfSpec), fp, fp, fp, fp], C.c_int),
         "dpd_window_adjoint_state": ([vp, i64, i32, C.POINTER(DpdRdfSpec), fp, fp, fp, fp, fp, fp, fp], C.c_int),
+        "dpd_fit_graph": ([vp, i64, i32, C.POINTER(DpdRdfSpec), fp, C.POINTER(DpdFitSpec), i32, fp, fp, fp], C.c_int),
         "dpd_force_vjp": ([vp, i32, i64, fp, fp, fp, fp, fp, fp, fp], C.c_int),
         "dpd_pair_hist": ([vp, i32, i32, i32, dbl, i32, fp], C.c_int),
         "dpd_get_stream": ([vp, C.POINTER(vp)], C.c_int),

@@ -353,6 +353,33 @@ class Engine:
                                           ptr(grad), ptr(rdf)))
         return loss, grad, rdf
 
+    def fit_graph(self, keys, nsteps, ckpt_every, spec, target, iters, lr=1.0, betas=(0.9, 0.999), eps=1e-8):
+        """iters optimizer iterations of the repulsions `keys` (a_X_Y, shared by
+        every replica) replayed as one captured CUDA graph (dpd_fit_graph): each a
+        differentiated window and an Adam step on the device.  Returns (loss
+        (iters x nrep), summed gradient (iters x len(keys)), values the windows
+        ran with, then the last values ((iters + 1) x len(keys))); the engine
+        keeps the last values."""
+        from .fit import param_index
+        f = _capi.DpdFitSpec()
+        f.n = len(keys)
+        for k, key in enumerate(keys):
+            f.slot[k] = param_index(key)
+            if f.slot[k] >= 64:
+                raise ValueError(f"{key}: only repulsions a_X_Y are fitted this way")
+        f.lr, f.beta1, f.beta2, f.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
+        tgt = np.ascontiguousarray(np.broadcast_to(target, (self.nrep, spec.nbin)), np.float64)
+        loss = np.zeros((iters, self.nrep))
+        grad = np.zeros((iters, len(keys)))
+        vals = np.zeros((iters + 1, len(keys)))
+        check(self.lib.dpd_fit_graph(self.h, int(nsteps), int(ckpt_every), C.byref(spec), ptr(tgt), C.byref(f),
+                                     int(iters), ptr(loss), ptr(grad), ptr(vals)))
+        for r in range(self.nrep):  # the host copies of the parameters follow the handle's
+            for k, key in enumerate(keys):
+                i, j = divmod(int(f.slot[k]), 8)
+                self.params[r].a[i][j] = self.params[r].a[j][i] = float(vals[-1, k])
+        return loss, grad, vals
+
     def window_adjoint_state(self, nsteps, ckpt_every, spec, target):
         """window_adjoint plus the cotangents of the start state (horizon 0):
         (loss, grad, rdf, xbar, vhbar, vtbar), the last three (N_total, 2) in gid
