@@ -65,3 +65,38 @@ def test_errors_are_reported_not_fatal():
     p.a[1] = 30.0  # a_01 != a_10
     rc = lib.dpd_create(p, 1, n, C.byref(h))
     assert rc == -1 and b"symmetric" in lib.dpd_last_error()
+
+
+def test_struct_layouts_agree_with_the_header(tmp_path):
+    """the ctypes mirrors of the header's structs (and the numpy record of an
+    event) have the C compiler's sizes and field offsets"""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    fields = {"dpd_event": ["step", "kind", "gid", "partner", "x", "y", "replica"],
+              "dpd_fit_spec": ["n", "slot", "lr", "beta1", "beta2", "eps"],
+              "dpd_rdf_spec": ["ta", "tb", "nbin", "last_steps", "rmax", "sigma", "horizon"],
+              "dpd_tuning": ["force_kernel", "tile_w", "tile_h", "graph_steps", "sort_mode", "tile_threads"]}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dpd.h"', "int main(void) {"]
+    for st, fs in fields.items():
+        lines.append(f'printf("{st} %zu\\n", sizeof({st}));')
+        for f in fs:
+            lines.append(f'printf("{st}.{f} %zu\\n", offsetof({st}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    mirrors = {"dpd_event": _capi.DpdEvent, "dpd_fit_spec": _capi.DpdFitSpec, "dpd_rdf_spec": _capi.DpdRdfSpec,
+               "dpd_tuning": _capi.DpdTuning}
+    for st, cls in mirrors.items():
+        assert int(got[st]) == C.sizeof(cls), st
+        for f in fields[st]:
+            assert int(got[f"{st}.{f}"]) == getattr(cls, f).offset, (st, f)
+    rec = ob.Engine.EVENT_DTYPE
+    assert rec.itemsize == C.sizeof(_capi.DpdEvent)
+    for f in fields["dpd_event"]:
+        assert rec.fields[f][1] == getattr(_capi.DpdEvent, f).offset, f
